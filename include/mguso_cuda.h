@@ -1,0 +1,133 @@
+/*
+ * mguso_cuda.h -- C ABI of the B200-native (sm_100a) mguso implicit-step library.
+ *
+ * This is the drop-in boundary for the reference engine's implicit IPC step
+ * (SeedeXR/nguo-3d, core-engine). Every entry point takes plain pointers and sizes,
+ * returns an int status (MGUSO_OK = 0) and records a message readable through
+ * mguso_last_error(). Handles are opaque; one handle is used by one thread at a time
+ * (the reference's LinearSolver is not Sync either: linsolve.rs:415-442).
+ *
+ * Pointer conventions: arguments documented as "host" are caller-owned host memory;
+ * arguments documented as "device" are device pointers on the context's GPU, used on
+ * the given CUDA stream (NULL = the legacy default stream).
+ */
+#ifndef MGUSO_CUDA_H
+#define MGUSO_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------ */
+#define MGUSO_OK 0
+#define MGUSO_ERR_INVALID_ARG 1   /* bad pointer, size or parameter */
+#define MGUSO_ERR_OOM 2           /* device allocation failed */
+#define MGUSO_ERR_NONFINITE 3     /* a step produced NaN/Inf and was rejected */
+#define MGUSO_ERR_PCG_CAP 4       /* PCG hit max_iter before reaching tol */
+#define MGUSO_ERR_CCD_CAP 5       /* a CCD root solve hit its iteration cap */
+#define MGUSO_ERR_PAIR_OVERFLOW 6 /* candidate-pair buffer too small (count still reported) */
+#define MGUSO_ERR_BVH_STACK 7     /* LBVH traversal stack overflow */
+#define MGUSO_ERR_CUDA 8          /* a CUDA runtime call failed */
+#define MGUSO_ERR_TIMEOUT 9       /* a bounded device wait gave up */
+#define MGUSO_ERR_UNSUPPORTED 10  /* configuration not supported */
+
+/* Preconditioners (linsolve.rs:67-76). */
+#define MGUSO_PRECOND_BLOCK_JACOBI 1
+#define MGUSO_PRECOND_SCHWARZ 2
+
+/* Arithmetic of the PCG reductions: FP32 everywhere, or FP64 dots/norms (MIXED). */
+#define MGUSO_PRECISION_FP32 0
+#define MGUSO_PRECISION_MIXED 1
+
+typedef struct mguso_ctx mguso_ctx;
+typedef struct mguso_bsr mguso_bsr;
+typedef struct mguso_schwarz mguso_schwarz;
+typedef struct mguso_linear_solver mguso_linear_solver;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int mguso_version(void);
+
+/* Copies the calling thread's last error message (NUL-terminated, truncated to len).
+ * Returns the full message length. */
+size_t mguso_last_error(char* buf, size_t len);
+
+/* GPU context: selects `device` and owns a stream. The reference's GpuContext::new()
+ * (engine-gpu/src/lib.rs:91-126). */
+int mguso_ctx_create(int device, mguso_ctx** out);
+int mguso_ctx_destroy(mguso_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t). */
+void* mguso_ctx_stream(mguso_ctx* ctx);
+
+/* Scalar CSR as the reference builds it (CsrMatrix, engine-core/src/csr.rs:9-14): square
+ * n x n, n = 3 * vertices, columns sorted within each row. All pointers host. */
+typedef struct {
+  uint32_t n;
+  const uint32_t* row_ptr; /* n + 1 */
+  const uint32_t* col_idx; /* row_ptr[n] */
+  const float* values;     /* row_ptr[n] */
+} mguso_csr;
+
+typedef struct {
+  uint32_t iters;   /* PCG iterations performed */
+  double residual;  /* final relative residual ||r|| / ||b|| */
+  int status;       /* MGUSO_OK, or MGUSO_ERR_PCG_CAP when max_iter was reached */
+} mguso_lin_stats;
+
+/* ---- LinearSolver (replaces engine_core::LinearSolver, linsolve.rs:21-28) ----------- */
+/* A stateful solver like SchwarzCpu (linsolve.rs:463-520): caches the block pattern,
+ * BSR layout and Schwarz domains while the sparsity is unchanged. `domain` is the
+ * Schwarz domain size in vertices (ignored for block Jacobi). */
+int mguso_linear_solver_create(mguso_ctx* ctx, int precond, uint32_t domain, int precision,
+                               mguso_linear_solver** out);
+int mguso_linear_solver_destroy(mguso_linear_solver* s);
+/* solve(a, b, tol, max_iter) -> x  (LinearSolver::solve). a, b, x host; x has a->n
+ * entries. Stats as LinearSolver::last_stats. Reaching max_iter is reported in
+ * stats->status; the return value is still MGUSO_OK and x holds the last iterate, as in
+ * the reference, which returns the best x without failing. */
+int mguso_linear_solve(mguso_linear_solver* s, const mguso_csr* a, const float* b, float tol,
+                       uint32_t max_iter, float* x, mguso_lin_stats* stats);
+
+/* ---- Device-resident 3x3 BSR operator ----------------------------------------------- */
+/* Builds a device BSR from a host scalar CSR whose 3x3 block structure is implied by the
+ * vertex grouping (every vertex pair contributes 9 entries, implicit.rs:2394-3103).
+ * Missing entries inside a present block are stored as 0. */
+int mguso_bsr_create_from_csr(mguso_ctx* ctx, const mguso_csr* a, mguso_bsr** out);
+/* Builds a device BSR directly from host block arrays: nb block rows, row_ptr (nb+1),
+ * col (nnzb) sorted per row, val (9*nnzb, row-major 3x3 per block). */
+int mguso_bsr_create(mguso_ctx* ctx, uint32_t nb, const uint32_t* row_ptr, const uint32_t* col,
+                     const float* val, mguso_bsr** out);
+int mguso_bsr_destroy(mguso_bsr* a);
+int mguso_bsr_info(const mguso_bsr* a, uint32_t* nb, uint32_t* nnzb);
+/* y = A x with x, y device (3*nb floats each), on `stream`. */
+int mguso_bsr_spmv(mguso_bsr* a, const float* x, float* y, void* stream);
+/* y = A x with x, y host: copies in, multiplies, copies out (synchronous). */
+int mguso_bsr_spmv_host(mguso_bsr* a, const float* x, float* y);
+/* Selects the SpMV kernel variant: 0 = auto (autotuned), 1 = TMA-staged tiles,
+ * 2 = direct thread-per-row. Returns the variant in use through *active. */
+int mguso_bsr_set_kernel(mguso_bsr* a, int variant, int* active);
+/* Runs the SpMV autotuner on this matrix (times every variant and tile shape with CUDA
+ * events) and keeps the fastest. *best_us gets its time per apply. */
+int mguso_bsr_autotune(mguso_bsr* a, float* best_us);
+
+/* ---- One-level additive Schwarz preconditioner (linsolve.rs:126-258) --------------- */
+/* Domains are greedy BFS aggregates of <= `domain` vertices over the block graph of `a`
+ * (linsolve.rs:152-173). Each domain's dense block is Cholesky-factored in FP64 and its
+ * inverse stored packed in FP32; the apply is a dense symmetric matvec per domain. */
+int mguso_schwarz_create(mguso_bsr* a, uint32_t domain, mguso_schwarz** out);
+int mguso_schwarz_destroy(mguso_schwarz* s);
+int mguso_schwarz_info(const mguso_schwarz* s, uint32_t* ndomains, uint64_t* factor_bytes);
+/* Re-factors every domain from the current values of `a` (device, on `stream`). */
+int mguso_schwarz_factor(mguso_schwarz* s, void* stream);
+/* z = M^-1 r with r, z device (3*nb floats), on `stream`. */
+int mguso_schwarz_apply(mguso_schwarz* s, const float* r, float* z, void* stream);
+/* Domain id of every vertex (host, nb entries). */
+int mguso_schwarz_domains(const mguso_schwarz* s, uint32_t* dom_of_vertex);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MGUSO_CUDA_H */

@@ -1,0 +1,135 @@
+// Internal object layouts behind the opaque C-ABI handles.
+#pragma once
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+
+struct mguso_ctx {
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+};
+
+namespace mg {
+
+// SpMV kernel variants (mguso_bsr_set_kernel).
+enum SpmvVariant : int { SPMV_AUTO = 0, SPMV_TMA = 1, SPMV_DIRECT = 2 };
+
+// One TMA-staged tiling of a BSR matrix: tiles of <= `rows` block rows and <= `cap`
+// blocks; each tile's value and column ranges are staged into shared memory by 1-D bulk
+// copies (rounded out to 16-byte boundaries).
+struct SpmvTiling {
+  int rows = 0;     // block rows per tile (= threads per CTA)
+  int stages = 0;   // pipeline depth
+  uint32_t cap = 0; // max blocks per tile
+  uint32_t ntiles = 0;
+  uint32_t val_stage_bytes = 0, col_stage_bytes = 0;
+  int grid = 0;     // persistent CTAs
+  DevBuf<uint32_t> tile_row;  // ntiles + 1
+  bool ok = false;  // false when some row is longer than `cap`
+};
+
+}  // namespace mg
+
+struct mguso_bsr {
+  mguso_ctx* ctx = nullptr;
+  uint32_t nb = 0, nnzb = 0;
+  std::vector<uint32_t> h_row_ptr, h_col;  // host copy of the pattern
+  mg::DevBuf<uint32_t> row_ptr, col;
+  mg::DevBuf<float> val;
+  int variant = mg::SPMV_AUTO;
+  int tiling_choice = 0;  // index into tilings when variant == TMA
+  std::vector<std::unique_ptr<mg::SpmvTiling>> tilings;
+  mg::DevBuf<uint32_t> status;
+  mg::DevBuf<float> hx, hy;  // staging for spmv_host
+};
+
+struct mguso_schwarz {
+  mguso_bsr* a = nullptr;
+  uint32_t domain = 32;
+  uint32_t ndom = 0;
+  uint32_t max_m = 0;
+  std::vector<uint32_t> h_dom_start, h_dom_verts, h_dom_of;
+  mg::DevBuf<uint32_t> dom_start;  // ndom + 1 (vertex offsets)
+  mg::DevBuf<uint32_t> dom_verts;  // nb
+  mg::DevBuf<uint32_t> dom_of;     // nb
+  mg::DevBuf<uint32_t> loc;        // nb: local index of a vertex inside its domain
+  mg::DevBuf<uint64_t> fac_off;    // ndom + 1 (float offsets, 4-float aligned)
+  mg::DevBuf<float> fac;           // packed lower-triangular FP32 inverse per domain
+  uint64_t fac_floats = 0;
+  mg::DevBuf<uint32_t> status;
+};
+
+namespace mg {
+
+// ---- BSR -------------------------------------------------------------------------------
+int bsr_build_host_from_csr(const mguso_csr* a, uint32_t& nb, std::vector<uint32_t>& row_ptr,
+                            std::vector<uint32_t>& col, std::vector<float>& val);
+int bsr_upload(mguso_bsr* m, uint32_t nb, const std::vector<uint32_t>& row_ptr, const std::vector<uint32_t>& col,
+               const float* val_host);
+int bsr_prepare_tilings(mguso_bsr* m);
+// y = A x; optional fused dot(x, y) partial reduction into `dot` (see Reduce).
+struct DotSink;
+int bsr_spmv(mguso_bsr* m, const float* x, float* y, cudaStream_t s, const DotSink* dot);
+int bsr_autotune(mguso_bsr* m, float* best_us);
+
+// ---- Schwarz ---------------------------------------------------------------------------
+int schwarz_build(mguso_schwarz* s);
+int schwarz_factor(mguso_schwarz* s, cudaStream_t st);
+int schwarz_apply(mguso_schwarz* s, const float* r, float* z, cudaStream_t st, const DotSink* dot);
+
+// ---- deterministic grid reductions ----------------------------------------------------
+// Kernels that produce a dot product write one partial per CTA into `partials`; the last
+// CTA to finish (counted through `counter`) sums the partials in index order and runs the
+// `finish` step, so results do not depend on CTA scheduling.
+enum DotFinish : int {
+  FIN_STORE = 0,   // out = sum
+  FIN_PAP = 1,     // pap = sum; alpha = rz / pap; breakdown when pap <= 0 or NaN
+  FIN_RR = 2,      // residual = sqrt(sum)/bnorm; ++iters; done when residual <= tol or iters == max
+  FIN_RZ = 3,      // beta = sum / rz; rz = sum
+  FIN_RZ0 = 4,     // rz = sum (setup)
+  FIN_BNORM = 5,   // bnorm = max(sqrt(sum), 1e-30)
+  FIN_RR0 = 6,     // residual = sqrt(sum) / bnorm (setup)
+};
+
+struct PcgScalars {
+  double rz, pap, alpha, beta, bnorm, residual, tol, out;
+  uint32_t iters, max_iter, done, status;
+  uint32_t counter;
+  uint32_t pad[3];
+};
+
+struct DotSink {
+  PcgScalars* sc;     // device
+  void* partials;     // device, >= max grid entries (double or float per `mixed`)
+  int finish;
+  bool mixed;         // accumulate in FP64
+};
+
+constexpr int MAX_PARTIALS = 4096;
+
+}  // namespace mg
+
+struct mguso_linear_solver {
+  mguso_ctx* ctx = nullptr;
+  int precond = MGUSO_PRECOND_SCHWARZ;
+  uint32_t domain = 32;
+  int precision = MGUSO_PRECISION_MIXED;
+  // cached pattern (rebuild BSR/domains only when the scalar sparsity changes)
+  std::vector<uint32_t> csr_row_ptr, csr_col;
+  std::unique_ptr<mguso_bsr> bsr;
+  std::unique_ptr<mguso_schwarz> schwarz;
+  mg::DevBuf<float> bjinv;  // 9 per vertex (block Jacobi)
+  mg::DevBuf<float> b, x, r, z, p, ap;
+  mg::DevBuf<mg::PcgScalars> sc;
+  mg::DevBuf<double> partials;
+  mg::PcgScalars* h_sc = nullptr;  // pinned
+  std::vector<uint32_t> map_val;   // scalar CSR entry -> BSR value slot
+  std::vector<float> h_val;
+};
+
+namespace mg {
+int pcg_solve(mguso_linear_solver* s, float tol, uint32_t max_iter, mguso_lin_stats* st);
+int blockjacobi_factor(mguso_bsr* a, float* inv, cudaStream_t s);
+}  // namespace mg

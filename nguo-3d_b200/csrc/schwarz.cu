@@ -1,0 +1,381 @@
+// One-level additive Schwarz preconditioner and 3x3 block Jacobi on the GPU.
+//
+// Reference: SchwarzTopology::{build, factorize, apply} (engine-core/src/linsolve.rs:
+// 126-258): greedy BFS domains of <= D vertices over the block graph, per-domain dense
+// block with the diagonal floor 1e-6*(tr/m) + 1e-8, Cholesky in f64 (fallback to the
+// diagonal when a pivot is <= 1e-14), and z = (L L^T)^-1 r per domain.
+//
+// B200 layout: factorisation is one CTA per domain in FP64 shared memory (right-looking
+// Cholesky, then L^-1 and M^-1 = L^-T L^-1), and what is stored is M^-1 itself, packed
+// lower-triangular in FP32 (16-byte aligned per domain). The apply is then a dense
+// symmetric matvec per domain with no sequential triangular sweeps: one warp per domain
+// stages its packed inverse into shared memory with a single 1-D TMA bulk copy.
+#include <algorithm>
+#include <deque>
+
+#include "reduce.cuh"
+
+namespace mg {
+
+int schwarz_configure();
+
+// ---------------------------------------------------------------------------------------
+// Host: BFS domains over the block pattern (linsolve.rs:152-173).
+// ---------------------------------------------------------------------------------------
+int schwarz_build(mguso_schwarz* s) {
+  mguso_bsr* a = s->a;
+  uint32_t nb = a->nb;
+  const auto& rp = a->h_row_ptr;
+  const auto& cl = a->h_col;
+  std::vector<uint8_t> assigned(nb, 0);
+  s->h_dom_start.assign(1, 0);
+  s->h_dom_verts.clear();
+  s->h_dom_verts.reserve(nb);
+  s->h_dom_of.assign(nb, 0);
+  std::vector<uint32_t> loc(nb, 0);
+  uint32_t D = std::max<uint32_t>(s->domain, 1);
+  uint32_t max_m = 0;
+  for (uint32_t seed = 0; seed < nb; ++seed) {
+    if (assigned[seed]) continue;
+    size_t base = s->h_dom_verts.size();
+    s->h_dom_verts.push_back(seed);
+    assigned[seed] = 1;
+    size_t fi = base;
+    while (s->h_dom_verts.size() - base < D && fi < s->h_dom_verts.size()) {
+      uint32_t v = s->h_dom_verts[fi++];
+      // block columns are sorted and unique per row: the reference's sorted, deduped
+      // adjacency minus the vertex itself.
+      for (uint32_t k = rp[v]; k < rp[v + 1]; ++k) {
+        uint32_t nbv = cl[k];
+        if (nbv == v) continue;
+        if (!assigned[nbv] && s->h_dom_verts.size() - base < D) {
+          assigned[nbv] = 1;
+          s->h_dom_verts.push_back(nbv);
+        }
+      }
+    }
+    uint32_t d = (uint32_t)s->h_dom_start.size() - 1;
+    for (size_t i = base; i < s->h_dom_verts.size(); ++i) {
+      s->h_dom_of[s->h_dom_verts[i]] = d;
+      loc[s->h_dom_verts[i]] = (uint32_t)(i - base);
+    }
+    s->h_dom_start.push_back((uint32_t)s->h_dom_verts.size());
+    max_m = std::max<uint32_t>(max_m, 3 * (uint32_t)(s->h_dom_verts.size() - base));
+  }
+  s->ndom = (uint32_t)s->h_dom_start.size() - 1;
+  s->max_m = max_m;
+  std::vector<uint64_t> off(s->ndom + 1, 0);
+  for (uint32_t d = 0; d < s->ndom; ++d) {
+    uint64_t m = 3ull * (s->h_dom_start[d + 1] - s->h_dom_start[d]);
+    uint64_t packed = m * (m + 1) / 2;
+    off[d + 1] = off[d] + ((packed + 3) & ~3ull);
+  }
+  s->fac_floats = off[s->ndom];
+  cudaStream_t st = a->ctx->stream;
+  MG_TRY(s->dom_start.upload(s->h_dom_start.data(), s->h_dom_start.size(), st));
+  MG_TRY(s->dom_verts.upload(s->h_dom_verts.data(), s->h_dom_verts.size(), st));
+  MG_TRY(s->dom_of.upload(s->h_dom_of.data(), nb, st));
+  MG_TRY(s->loc.upload(loc.data(), nb, st));
+  MG_TRY(s->fac_off.upload(off.data(), off.size(), st));
+  MG_TRY(s->fac.reserve(std::max<uint64_t>(s->fac_floats, 4)));
+  MG_TRY(s->status.reserve(4));
+  MG_CUDA(cudaMemsetAsync(s->status.p, 0, 16, st));
+  MG_CUDA(cudaStreamSynchronize(st));
+  MG_TRY(schwarz_configure());
+  return MGUSO_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Factorisation: one CTA per domain. Shared: A (m x m, f64) + diag of L^-1 (m).
+// After the Cholesky sweep the lower triangle holds L; L^-1 is accumulated transposed in
+// the upper triangle (X[i][c] at A[c][i], i > c) with its diagonal in xd[].
+// ---------------------------------------------------------------------------------------
+__global__ void k_schwarz_factor(const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ col,
+                                 const float* __restrict__ val, const uint32_t* __restrict__ dom_start,
+                                 const uint32_t* __restrict__ dom_verts, const uint32_t* __restrict__ dom_of,
+                                 const uint32_t* __restrict__ loc, const uint64_t* __restrict__ fac_off,
+                                 float* __restrict__ fac, uint32_t* status) {
+  extern __shared__ __align__(16) double sA[];
+  __shared__ double s_floor;
+  __shared__ int s_fail;
+  const uint32_t d = blockIdx.x;
+  const uint32_t vs = dom_start[d], nvd = dom_start[d + 1] - vs;
+  const int m = 3 * (int)nvd;
+  double* xd = sA + (size_t)m * m;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int i = tid; i < m * m; i += nt) sA[i] = 0.0;
+  __syncthreads();
+  // gather this domain's dense block (each (p, q) block appears once per BSR row)
+  const int lane = tid & 31, w = tid >> 5, nw = nt >> 5;
+  for (uint32_t p = w; p < nvd; p += nw) {
+    uint32_t v = dom_verts[vs + p];
+    for (uint32_t k = row_ptr[v] + lane; k < row_ptr[v + 1]; k += 32) {
+      uint32_t c = col[k];
+      if (dom_of[c] != d) continue;
+      uint32_t q = loc[c];
+      const float* b = val + 9 * (size_t)k;
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) sA[(3 * p + i) * m + 3 * q + j] = (double)b[3 * i + j];
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double tr = 0.0;
+    for (int k = 0; k < m; ++k) tr += sA[k * m + k];
+    s_floor = 1e-6 * (tr / (double)m) + 1e-8;
+    s_fail = 0;
+  }
+  __syncthreads();
+  for (int k = tid; k < m; k += nt) sA[k * m + k] += s_floor;
+  __syncthreads();
+  // right-looking Cholesky on the lower triangle
+  for (int k = 0; k < m; ++k) {
+    if (tid == 0) {
+      double piv = sA[k * m + k];
+      if (!(piv > 1e-14)) s_fail = 1;
+      sA[k * m + k] = sqrt(fmax(piv, 1e-300));
+    }
+    __syncthreads();
+    if (s_fail) break;
+    double lkk = sA[k * m + k];
+    for (int i = k + 1 + tid; i < m; i += nt) sA[i * m + k] /= lkk;
+    __syncthreads();
+    int rem = m - k - 1;
+    int tot = rem * (rem + 1) / 2;
+    for (int e = tid; e < tot; e += nt) {
+      // e -> (i, j) with k < j <= i < m, row-major over the trailing lower triangle
+      int ii = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
+      while ((ii + 1) * (ii + 2) / 2 <= e) ++ii;
+      while (ii * (ii + 1) / 2 > e) --ii;
+      int jj = e - ii * (ii + 1) / 2;
+      int i = k + 1 + ii, j = k + 1 + jj;
+      sA[i * m + j] -= sA[i * m + k] * sA[j * m + k];
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  float* out = fac + fac_off[d];
+  if (s_fail) {
+    // reference fallback: L = diag(sqrt(ad_pp)) (1 where ad_pp <= 1e-14), so
+    // M^-1 = diag(1 / ad_pp). The diagonal was overwritten by the failed sweep, so it is
+    // re-gathered here.
+    for (int e = tid; e < m * (m + 1) / 2; e += nt) out[e] = 0.0f;
+    __syncthreads();
+    for (uint32_t p = w; p < nvd; p += nw) {
+      uint32_t v = dom_verts[vs + p];
+      for (uint32_t k = row_ptr[v] + lane; k < row_ptr[v + 1]; k += 32) {
+        if (col[k] != v) continue;
+        const float* b = val + 9 * (size_t)k;
+        for (int i = 0; i < 3; ++i) {
+          double a = (double)b[4 * i] + s_floor;
+          int r = 3 * p + i;
+          out[r * (r + 1) / 2 + r] = (float)(a > 1e-14 ? 1.0 / a : 1.0);
+        }
+      }
+    }
+    if (tid == 0) atomicOr(status, 1u << 8);
+    return;
+  }
+  // X = L^-1: zero the strict upper triangle, xd = 1, then right-looking row sweep.
+  for (int e = tid; e < m * m; e += nt) {
+    int i = e / m, j = e % m;
+    if (j > i) sA[e] = 0.0;
+  }
+  for (int i = tid; i < m; i += nt) xd[i] = 1.0;
+  __syncthreads();
+  for (int k = 0; k < m; ++k) {
+    double lkk = sA[k * m + k];
+    // finalise row k of X: X[k][c] /= L_kk, c <= k
+    for (int c = tid; c <= k; c += nt) {
+      if (c == k)
+        xd[k] /= lkk;
+      else
+        sA[c * m + k] /= lkk;
+    }
+    __syncthreads();
+    int rows = m - k - 1, cols = k + 1;
+    for (int e = tid; e < rows * cols; e += nt) {
+      int i = k + 1 + e / cols, c = e % cols;
+      double xkc = (c == k) ? xd[k] : sA[c * m + k];
+      sA[c * m + i] -= sA[i * m + k] * xkc;
+    }
+    __syncthreads();
+  }
+  // M^-1[i][j] = sum_{k >= i} X[k][i] X[k][j] for i >= j, packed row-major lower.
+  for (int e = tid; e < m * (m + 1) / 2; e += nt) {
+    int i = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
+    while ((i + 1) * (i + 2) / 2 <= e) ++i;
+    while (i * (i + 1) / 2 > e) --i;
+    int j = e - i * (i + 1) / 2;
+    double s = 0.0;
+    for (int k = i; k < m; ++k) {
+      double xki = (k == i) ? xd[i] : sA[i * m + k];
+      double xkj = (k == j) ? xd[j] : sA[j * m + k];
+      s += xki * xkj;
+    }
+    out[e] = (float)s;
+  }
+}
+
+int schwarz_factor(mguso_schwarz* s, cudaStream_t st) {
+  if (s->ndom == 0) return MGUSO_OK;
+  mguso_bsr* a = s->a;
+  size_t smem = sizeof(double) * ((size_t)s->max_m * s->max_m + s->max_m);
+  k_schwarz_factor<<<s->ndom, 128, smem, st>>>(a->row_ptr.p, a->col.p, a->val.p, s->dom_start.p, s->dom_verts.p,
+                                               s->dom_of.p, s->loc.p, s->fac_off.p, s->fac.p, s->status.p);
+  MG_CUDA(cudaGetLastError());
+  return MGUSO_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Apply: one warp per domain. Per-warp shared slice: mbarrier, the packed inverse (bulk
+// copied), and the gathered residual.
+// ---------------------------------------------------------------------------------------
+template <int WARPS, class Acc>
+__global__ void __launch_bounds__(32 * WARPS) k_schwarz_apply(
+    const uint32_t* __restrict__ dom_start, const uint32_t* __restrict__ dom_verts,
+    const uint64_t* __restrict__ fac_off, const float* __restrict__ fac, const float* __restrict__ r,
+    float* __restrict__ z, uint32_t ndom, uint32_t slice_floats, uint32_t* status, DotSink dot, int with_dot) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  if (with_dot && dot.sc->done) return;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint64_t* bar = (uint64_t*)(smem + 16 * w);
+  float* buf = (float*)(smem + 128 + (size_t)w * slice_floats * 4);
+  float* rd = buf + (slice_floats - 96);
+  const uint32_t d = blockIdx.x * WARPS + w;
+  Acc acc = 0;
+  bool ok = true;
+  if (d < ndom) {
+    const uint32_t vs = dom_start[d], nvd = dom_start[d + 1] - vs;
+    const int m = 3 * (int)nvd;
+    const uint64_t off = fac_off[d];
+    const uint32_t bytes = (uint32_t)((fac_off[d + 1] - off) * 4);
+    if (lane == 0) {
+      mbar_init(bar, 1);
+      fence_mbar_init();
+    }
+    __syncwarp();
+    if (lane == 0) {
+      fence_proxy_async();
+      mbar_arrive_expect_tx(bar, bytes);
+      bulk_g2s(buf, fac + off, bytes, bar);
+    }
+    for (int i = lane; i < m; i += 32) {
+      uint32_t v = dom_verts[vs + i / 3];
+      rd[i] = r[3 * v + i % 3];
+    }
+    __syncwarp();
+    ok = mbar_wait(bar, 0);
+    if (ok) {
+      for (int i = lane; i < m; i += 32) {
+        float s = 0.f;
+        const int ri = i * (i + 1) / 2;
+        for (int j = 0; j <= i; ++j) s = fmaf(buf[ri + j], rd[j], s);
+        for (int j = i + 1; j < m; ++j) s = fmaf(buf[j * (j + 1) / 2 + i], rd[j], s);
+        uint32_t v = dom_verts[vs + i / 3];
+        z[3 * v + i % 3] = s;
+        acc += (Acc)rd[i] * (Acc)s;
+      }
+    } else if (lane == 0) {
+      atomicOr(status, ST_WAIT_TIMEOUT);
+    }
+  }
+  if (with_dot) grid_dot_commit<Acc>(dot, acc);
+}
+
+// Shared-memory opt-in for the largest domain (32 vertices, m = 96), set once outside any
+// stream capture.
+int schwarz_configure() {
+  static bool done = false;
+  if (done) return MGUSO_OK;
+  constexpr int WARPS = 4;
+  size_t fsm = sizeof(double) * (96 * 96 + 96);
+  MG_CUDA(cudaFuncSetAttribute(k_schwarz_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
+  uint32_t slice = ((96 * 97 / 2 + 3) & ~3u) + 96;
+  slice = (slice + 31) & ~31u;
+  size_t asmem = 128 + (size_t)WARPS * slice * 4;
+  MG_CUDA(cudaFuncSetAttribute(k_schwarz_apply<WARPS, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)asmem));
+  MG_CUDA(cudaFuncSetAttribute(k_schwarz_apply<WARPS, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)asmem));
+  done = true;
+  return MGUSO_OK;
+}
+
+int schwarz_apply(mguso_schwarz* s, const float* r, float* z, cudaStream_t st, const DotSink* dot) {
+  constexpr int WARPS = 4;
+  DotSink d{};
+  int with_dot = dot ? 1 : 0;
+  if (dot) d = *dot;
+  bool mixed = dot && dot->mixed;
+  uint32_t mm = std::max<uint32_t>(s->max_m, 3);
+  uint32_t packed = (mm * (mm + 1) / 2 + 3) & ~3u;
+  uint32_t slice = packed + 96;  // factor + gathered residual (m <= 96 floats)
+  slice = (slice + 31) & ~31u;
+  size_t smem = 128 + (size_t)WARPS * slice * 4;
+  uint32_t grid = ceil_div(s->ndom, WARPS);
+  if (with_dot && grid > (uint32_t)MAX_PARTIALS) {
+    set_error("Schwarz apply with fused dot: too many domains for one partial per CTA");
+    return MGUSO_ERR_UNSUPPORTED;
+  }
+  if (mm > 96) {
+    set_error("Schwarz domain larger than 32 vertices");
+    return MGUSO_ERR_UNSUPPORTED;
+  }
+  void* fn = mixed ? (void*)k_schwarz_apply<WARPS, double> : (void*)k_schwarz_apply<WARPS, float>;
+  const uint32_t* a0 = s->dom_start.p;
+  const uint32_t* a1 = s->dom_verts.p;
+  const uint64_t* a2 = s->fac_off.p;
+  const float* a3 = s->fac.p;
+  uint32_t nd = s->ndom;
+  uint32_t* stp = s->status.p;
+  void* args[] = {(void*)&a0, (void*)&a1, (void*)&a2, (void*)&a3, (void*)&r, (void*)&z,
+                  (void*)&nd, (void*)&slice, (void*)&stp, (void*)&d, (void*)&with_dot};
+  if (grid == 0) return MGUSO_OK;
+  MG_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(32 * WARPS), args, smem, st));
+  return MGUSO_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Block Jacobi (linsolve.rs:294-315): per-vertex 3x3 inverse in f64, stored as 9 floats;
+// a singular block (|det| < 1e-20) falls back to 1/diagonal (1 where the diagonal is 0).
+// ---------------------------------------------------------------------------------------
+__global__ void k_bj_factor(const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ col,
+                            const float* __restrict__ val, uint32_t nb, float* __restrict__ inv) {
+  uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nb) return;
+  double m[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (uint32_t k = row_ptr[v]; k < row_ptr[v + 1]; ++k)
+    if (col[k] == v)
+      for (int e = 0; e < 9; ++e) m[e] = (double)val[9 * (size_t)k + e];
+  double det = m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
+               m[2] * (m[3] * m[7] - m[4] * m[6]);
+  double o[9];
+  if (fabs(det) < 1e-20) {
+    for (int e = 0; e < 9; ++e) o[e] = 0.0;
+    for (int i = 0; i < 3; ++i) o[4 * i] = m[4 * i] != 0.0 ? 1.0 / m[4 * i] : 1.0;
+  } else {
+    double id = 1.0 / det;
+    o[0] = (m[4] * m[8] - m[5] * m[7]) * id;
+    o[1] = (m[2] * m[7] - m[1] * m[8]) * id;
+    o[2] = (m[1] * m[5] - m[2] * m[4]) * id;
+    o[3] = (m[5] * m[6] - m[3] * m[8]) * id;
+    o[4] = (m[0] * m[8] - m[2] * m[6]) * id;
+    o[5] = (m[2] * m[3] - m[0] * m[5]) * id;
+    o[6] = (m[3] * m[7] - m[4] * m[6]) * id;
+    o[7] = (m[1] * m[6] - m[0] * m[7]) * id;
+    o[8] = (m[0] * m[4] - m[1] * m[3]) * id;
+  }
+  for (int e = 0; e < 9; ++e) inv[9 * (size_t)v + e] = (float)o[e];
+}
+
+int blockjacobi_factor(mguso_bsr* a, float* inv, cudaStream_t s) {
+  if (a->nb == 0) return MGUSO_OK;
+  k_bj_factor<<<ceil_div(a->nb, 128), 128, 0, s>>>(a->row_ptr.p, a->col.p, a->val.p, a->nb, inv);
+  MG_CUDA(cudaGetLastError());
+  return MGUSO_OK;
+}
+
+}  // namespace mg

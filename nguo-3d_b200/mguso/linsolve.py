@@ -1,0 +1,207 @@
+"""Host-side mirror of the reference's linear-solver seam.
+
+Mirrors ``engine_core::LinearSolver`` (core-engine/crates/engine-core/src/linsolve.rs:21-28):
+``solve(a, b, tol, max_iter) -> x`` plus ``last_stats()``, with the solve running on the
+GPU through the C ABI. ``CsrMatrix`` mirrors ``engine_core::CsrMatrix`` (csr.rs:9-14).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, ptr
+
+
+@dataclass
+class CsrMatrix:
+    """Square scalar CSR, ``n`` rows (3 per vertex), columns sorted per row."""
+
+    n: int
+    row_ptr: np.ndarray
+    col_idx: np.ndarray
+    values: np.ndarray
+
+    def nnz(self) -> int:
+        return int(self.values.size)
+
+
+@dataclass
+class LinearStats:
+    """``engine_core::LinearStats`` (linsolve.rs:12-18)."""
+
+    iters: int = 0
+    residual: float = 0.0
+    status: int = 0
+
+
+class Context:
+    """One GPU (``GpuContext::new``, engine-gpu/src/lib.rs:91-126)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        check(self.lib.mguso_ctx_create(device, C.byref(h)))
+        self.h = h
+        self.device = device
+
+    @property
+    def stream(self) -> int:
+        return self.lib.mguso_ctx_stream(self.h)
+
+    def close(self):
+        if self.h:
+            self.lib.mguso_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CudaLinearSolver:
+    """A ``LinearSolver`` whose solve is the device PCG.
+
+    ``precond`` is ``"schwarz"`` (SchwarzCpu(domain), linsolve.rs:463-520) or ``"block"``
+    (CgCpu's block Jacobi, linsolve.rs:413-442). ``precision`` is ``"mixed"`` (FP64 dot
+    products and norms) or ``"fp32"``.
+    """
+
+    def __init__(self, ctx: Context, precond: str = "schwarz", domain: int = 32, precision: str = "mixed"):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        pc = {"schwarz": _lib.PRECOND_SCHWARZ, "block": _lib.PRECOND_BLOCK_JACOBI}[precond]
+        pr = {"mixed": _lib.PRECISION_MIXED, "fp32": _lib.PRECISION_FP32}[precision]
+        h = C.c_void_p()
+        check(self.lib.mguso_linear_solver_create(ctx.h, pc, domain, pr, C.byref(h)))
+        self.h = h
+        self._stats = LinearStats()
+
+    def solve(self, a: CsrMatrix, b: np.ndarray, tol: float, max_iter: int) -> np.ndarray:
+        assert b.shape == (a.n,)
+        desc, keep = _lib.csr_desc(a.n, a.row_ptr, a.col_idx, a.values)
+        bb = np.ascontiguousarray(b, dtype=np.float32)
+        x = np.zeros(a.n, dtype=np.float32)
+        st = _lib.LinStats()
+        check(self.lib.mguso_linear_solve(self.h, C.byref(desc), ptr(bb), C.c_float(tol), max_iter, ptr(x),
+                                          C.byref(st)))
+        self._stats = LinearStats(int(st.iters), float(st.residual), int(st.status))
+        del keep
+        return x
+
+    def last_stats(self) -> LinearStats:
+        return self._stats
+
+    def close(self):
+        if self.h:
+            self.lib.mguso_linear_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Bsr:
+    """A device-resident 3x3 BSR operator."""
+
+    def __init__(self, ctx: Context, nb: int, row_ptr: np.ndarray, col: np.ndarray, val: np.ndarray):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        rp = np.ascontiguousarray(row_ptr, dtype=np.uint32)
+        cl = np.ascontiguousarray(col, dtype=np.uint32)
+        vl = np.ascontiguousarray(val, dtype=np.float32).reshape(-1)
+        assert rp.size == nb + 1 and vl.size == 9 * cl.size
+        h = C.c_void_p()
+        check(self.lib.mguso_bsr_create(ctx.h, nb, ptr(rp), ptr(cl) if cl.size else None,
+                                        ptr(vl) if vl.size else None, C.byref(h)))
+        self.h = h
+        self.nb = nb
+        self.nnzb = int(cl.size)
+
+    @classmethod
+    def from_csr(cls, ctx: Context, a: CsrMatrix) -> "Bsr":
+        self = cls.__new__(cls)
+        self.ctx = ctx
+        self.lib = ctx.lib
+        desc, keep = _lib.csr_desc(a.n, a.row_ptr, a.col_idx, a.values)
+        h = C.c_void_p()
+        check(self.lib.mguso_bsr_create_from_csr(ctx.h, C.byref(desc), C.byref(h)))
+        self.h = h
+        nb, nnzb = C.c_uint32(), C.c_uint32()
+        check(self.lib.mguso_bsr_info(h, C.byref(nb), C.byref(nnzb)))
+        self.nb, self.nnzb = nb.value, nnzb.value
+        return self
+
+    def spmv(self, x_dev: int, y_dev: int, stream: int = 0) -> None:
+        """y = A x on device pointers."""
+        check(self.lib.mguso_bsr_spmv(self.h, x_dev, y_dev, stream))
+
+    def spmv_host(self, x: np.ndarray) -> np.ndarray:
+        xx = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.empty(3 * self.nb, dtype=np.float32)
+        check(self.lib.mguso_bsr_spmv_host(self.h, ptr(xx), ptr(y)))
+        return y
+
+    def set_kernel(self, variant: int) -> int:
+        act = C.c_int()
+        check(self.lib.mguso_bsr_set_kernel(self.h, variant, C.byref(act)))
+        return act.value
+
+    def autotune(self) -> float:
+        us = C.c_float()
+        check(self.lib.mguso_bsr_autotune(self.h, C.byref(us)))
+        return us.value
+
+    def close(self):
+        if self.h:
+            self.lib.mguso_bsr_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Schwarz:
+    """One-level additive Schwarz over a device BSR (linsolve.rs:126-258)."""
+
+    def __init__(self, a: Bsr, domain: int = 32):
+        self.a = a
+        self.lib = a.lib
+        h = C.c_void_p()
+        check(self.lib.mguso_schwarz_create(a.h, domain, C.byref(h)))
+        self.h = h
+        nd, fb = C.c_uint32(), C.c_uint64()
+        check(self.lib.mguso_schwarz_info(h, C.byref(nd), C.byref(fb)))
+        self.ndomains, self.factor_bytes = nd.value, fb.value
+
+    def factor(self, stream: int = 0) -> None:
+        check(self.lib.mguso_schwarz_factor(self.h, stream))
+
+    def apply(self, r_dev: int, z_dev: int, stream: int = 0) -> None:
+        check(self.lib.mguso_schwarz_apply(self.h, r_dev, z_dev, stream))
+
+    def domains(self) -> np.ndarray:
+        out = np.empty(self.a.nb, dtype=np.uint32)
+        check(self.lib.mguso_schwarz_domains(self.h, ptr(out)))
+        return out
+
+    def close(self):
+        if self.h:
+            self.lib.mguso_schwarz_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

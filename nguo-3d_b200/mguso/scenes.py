@@ -1,0 +1,120 @@
+"""Seeded synthetic inputs for the benchmark and parity configurations.
+
+No public dataset is involved: every workload is generated here from a seed with the shapes,
+sizes and value distributions of the configurations it stands for.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def grid_edges(n: int) -> np.ndarray:
+    """Undirected edges of an n x n vertex grid triangulated along one diagonal per quad
+    (the stiffness pattern of a cloth grid: 6 neighbours per interior vertex)."""
+    idx = np.arange(n * n, dtype=np.int64).reshape(n, n)  # [j, i]
+    h = np.stack([idx[:, :-1].ravel(), idx[:, 1:].ravel()], 1)
+    v = np.stack([idx[:-1, :].ravel(), idx[1:, :].ravel()], 1)
+    d = np.stack([idx[:-1, :-1].ravel(), idx[1:, 1:].ravel()], 1)
+    return np.concatenate([h, v, d], 0)
+
+
+def grid_tris(n: int) -> np.ndarray:
+    """Triangles of the n x n grid, split along the (i,j)-(i+1,j+1) diagonal, wound
+    consistently."""
+    idx = np.arange(n * n, dtype=np.int64).reshape(n, n)
+    a = idx[:-1, :-1].ravel()
+    b = idx[:-1, 1:].ravel()
+    c = idx[1:, 1:].ravel()
+    d = idx[1:, :-1].ravel()
+    t1 = np.stack([a, b, c], 1)
+    t2 = np.stack([a, c, d], 1)
+    return np.concatenate([t1, t2], 0).astype(np.uint32)
+
+
+def grid_bsr(n: int, seed: int = 2):
+    """Operator microbenchmark matrix: the block pattern of an n x n cloth grid
+    (n^2 vertices, 7 blocks per interior row: the vertex, its 4 axis neighbours and its 2
+    neighbours along the quad diagonal), 3x3 blocks with FP32 values drawn N(0,1),
+    symmetric (A_ji = A_ij^T) and made strictly diagonally dominant
+    (a_rr = |a_rr| + sum_{k != r} |a_rk| + 1), hence SPD.
+
+    Built directly in row order (no global sort): row v's columns are
+    v-n-1, v-n, v-1, v, v+1, v+n, v+n+1 where they exist.
+    Returns (nb, row_ptr u32[nb+1], col u32[nnzb], val f32[nnzb, 3, 3]).
+    """
+    rng = np.random.default_rng(seed)
+    nb = n * n
+    # one block per undirected edge, indexed by its lower vertex: horizontal (v, v+1),
+    # vertical (v, v+n), diagonal (v, v+n+1); plus a symmetric diagonal block per vertex
+    gh = rng.standard_normal((nb, 3, 3), dtype=np.float32)
+    gv = rng.standard_normal((nb, 3, 3), dtype=np.float32)
+    gd = rng.standard_normal((nb, 3, 3), dtype=np.float32)
+    dg = rng.standard_normal((nb, 3, 3), dtype=np.float32)
+    dg = 0.5 * (dg + dg.transpose(0, 2, 1))
+    i = np.tile(np.arange(n), n)
+    j = np.repeat(np.arange(n), n)
+    valid = np.stack([(i > 0) & (j > 0), j > 0, i > 0, np.ones(nb, bool), i < n - 1, j < n - 1,
+                      (i < n - 1) & (j < n - 1)], 1)
+    offs = np.array([-n - 1, -n, -1, 0, 1, n, n + 1], dtype=np.int64)
+    full = np.zeros((nb, 7, 3, 3), dtype=np.float32)
+    full[n + 1:, 0] = gd[:-(n + 1)].transpose(0, 2, 1)
+    full[n:, 1] = gv[:-n].transpose(0, 2, 1)
+    full[1:, 2] = gh[:-1].transpose(0, 2, 1)
+    full[:, 3] = dg
+    full[:, 4] = gh
+    full[:, 5] = gv
+    full[:, 6] = gd
+    full *= valid[:, :, None, None]
+    absrow = np.abs(full).sum(axis=(1, 3), dtype=np.float64)  # (nb, 3) incl. the diagonal entry
+    d_vals = np.stack([full[:, 3, k, k] for k in range(3)], 1)
+    absrow -= np.abs(d_vals)
+    for k in range(3):
+        full[:, 3, k, k] = (np.abs(d_vals[:, k]) + absrow[:, k] + 1.0).astype(np.float32)
+    cnt = valid.sum(1)
+    row_ptr = np.zeros(nb + 1, dtype=np.int64)
+    row_ptr[1:] = np.cumsum(cnt)
+    vflat = valid.reshape(-1)
+    cols = (np.arange(nb, dtype=np.int64)[:, None] + offs[None, :]).reshape(-1)[vflat]
+    val = full.reshape(-1, 3, 3)[vflat]
+    return nb, row_ptr.astype(np.uint32), cols.astype(np.uint32), np.ascontiguousarray(val)
+
+
+def bsr_to_csr(nb: int, row_ptr: np.ndarray, col: np.ndarray, val: np.ndarray):
+    """Expands a 3x3 BSR into the reference's scalar CSR (n = 3 nb)."""
+    row_ptr = row_ptr.astype(np.int64)
+    nblk = np.diff(row_ptr)
+    n = 3 * nb
+    srp = np.zeros(n + 1, dtype=np.int64)
+    per_row = np.repeat(3 * nblk, 3)
+    srp[1:] = np.cumsum(per_row)
+    # scalar row (v, i) lists blocks k in row v, then j in 0..2
+    blk_of_row = np.repeat(np.arange(nb), nblk)
+    # For each scalar row (v,i): entries ordered by (k, j)
+    k_idx = np.arange(col.size)
+    # build arrays of shape (nnzb, 3 rows, 3 cols) -> reorder to rows
+    cols3 = (3 * col.astype(np.int64))[:, None] + np.arange(3)[None, :]  # (nnzb, 3)
+    out_cols = np.empty(9 * col.size, dtype=np.uint32)
+    out_vals = np.empty(9 * col.size, dtype=np.float32)
+    # position of entry (k, i, j) in the scalar CSR
+    base = 9 * row_ptr[blk_of_row]  # start of vertex row block
+    local = k_idx - row_ptr[blk_of_row]
+    for i in range(3):
+        pos = base + 3 * i * nblk[blk_of_row] + 3 * local
+        for j in range(3):
+            out_cols[pos + j] = cols3[:, j]
+            out_vals[pos + j] = val[:, i, j]
+    return n, srp.astype(np.uint32), out_cols, out_vals
+
+
+def bsr_spmv_f64(row_ptr: np.ndarray, col: np.ndarray, val: np.ndarray, x: np.ndarray) -> np.ndarray:
+    """y = A x in float64 (the reference value for size-independent SpMV checks)."""
+    nb = row_ptr.size - 1
+    xb = x.reshape(-1, 3).astype(np.float64)
+    rp = row_ptr.astype(np.int64)
+    prod = np.einsum("kij,kj->ki", val.astype(np.float64), xb[col.astype(np.int64)])
+    y = np.zeros((nb, 3), dtype=np.float64)
+    nonempty = rp[1:] > rp[:-1]
+    if prod.shape[0]:
+        sums = np.add.reduceat(prod, rp[:-1][nonempty], axis=0)
+        y[nonempty] = sums
+    return y.reshape(-1)
