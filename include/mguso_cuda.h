@@ -114,8 +114,9 @@ int mguso_bsr_autotune(mguso_bsr* a, float* best_us);
 
 /* ---- One-level additive Schwarz preconditioner (linsolve.rs:126-258) --------------- */
 /* Domains are greedy BFS aggregates of <= `domain` vertices over the block graph of `a`
- * (linsolve.rs:152-173). Each domain's dense block is Cholesky-factored in FP64 and its
- * inverse stored packed in FP32; the apply is a dense symmetric matvec per domain. */
+ * (linsolve.rs:152-173). Each domain's dense block (with the reference's diagonal floor)
+ * is inverted in FP64 and the inverse stored packed in FP32; the apply is a dense
+ * symmetric matvec per domain. */
 int mguso_schwarz_create(mguso_bsr* a, uint32_t domain, mguso_schwarz** out);
 int mguso_schwarz_destroy(mguso_schwarz* s);
 int mguso_schwarz_info(const mguso_schwarz* s, uint32_t* ndomains, uint64_t* factor_bytes);
@@ -125,6 +126,42 @@ int mguso_schwarz_factor(mguso_schwarz* s, void* stream);
 int mguso_schwarz_apply(mguso_schwarz* s, const float* r, float* z, void* stream);
 /* Domain id of every vertex (host, nb entries). */
 int mguso_schwarz_domains(const mguso_schwarz* s, uint32_t* dom_of_vertex);
+
+/* ---- LBVH broad phase (engine-gpu/src/{morton,radix,karras,bvh_aabb,bvh_traverse}.rs) */
+/* Triangle BVH: 30-bit (u32) or 63-bit (u64) Morton codes of the centroids normalised by
+ * the centroid box (morton.rs:21-63), a stable onesweep radix sort of (code, triangle),
+ * the Karras tree (karras.rs:24-88) and exact min/max node boxes (bvh_aabb.rs:28-56). */
+typedef struct mguso_lbvh mguso_lbvh;
+int mguso_lbvh_create(mguso_ctx* ctx, mguso_lbvh** out);
+int mguso_lbvh_destroy(mguso_lbvh* b);
+/* positions f32[3*nv], tris u32[3*nt] device; key_bits 30 or 63. */
+int mguso_lbvh_build(mguso_lbvh* b, const float* positions, uint32_t nv, const uint32_t* tris, uint32_t nt,
+                     int key_bits, void* stream);
+/* Emits (query, triangle) for every leaf box overlapping [p - dhat, p + dhat]
+ * (bvh_traverse.wgsl:64-92): points f32[3*np], pairs u32[2*cap], *count (u64) device.
+ * *count receives the total even when it exceeds cap (then status = PAIR_OVERFLOW).
+ * Queries are visited in Morton order so a warp walks neighbouring points together. */
+int mguso_lbvh_query_points(mguso_lbvh* b, const float* points, uint32_t np, float dhat, uint32_t* pairs,
+                            uint64_t cap, uint64_t* count, void* stream);
+/* Host copies of the last build: keys (zero-extended to u64), perm, left/right (nt-1),
+ * node boxes f32[6*(nt-1)] as [lo.xyz, hi.xyz]. Any pointer may be NULL. */
+int mguso_lbvh_download(mguso_lbvh* b, uint64_t* keys, uint32_t* perm, uint32_t* left, uint32_t* right,
+                        float* node_boxes);
+/* Device status of the last build/query: MGUSO_OK, MGUSO_ERR_PAIR_OVERFLOW,
+ * MGUSO_ERR_BVH_STACK or MGUSO_ERR_TIMEOUT (synchronises the context stream). */
+int mguso_lbvh_status(mguso_lbvh* b);
+/* enable != 0 records per-stage events; ms6 receives the last build+query's stage times:
+ * morton, sort, karras, refit, query preparation, traversal (ms). */
+int mguso_lbvh_stage_times(mguso_lbvh* b, int enable, float* ms6);
+/* Host-buffer convenience over build + point query (the operator entry point a binding
+ * calls): out_keys (u64[nt]), out_perm (u32[nt]) and out_pairs (u32[2*cap]) may be NULL. */
+int mguso_lbvh_build_query(mguso_ctx* ctx, const float* positions, uint32_t nv, const uint32_t* tris,
+                           uint32_t nt, int key_bits, float dhat, uint64_t* out_keys, uint32_t* out_perm,
+                           uint32_t* out_pairs, uint64_t cap, uint64_t* count);
+/* Stable onesweep LSD radix sort of (key, u32 payload) pairs in place (device pointers):
+ * u32 keys when key_bits <= 32, u64 keys otherwise. Replaces GpuRadixSort::sort_pairs
+ * (radix.rs:112-352), which is limited to 65 536 keys. */
+int mguso_radix_sort_pairs(mguso_ctx* ctx, void* keys, uint32_t* vals, uint32_t n, int key_bits, void* stream);
 
 #ifdef __cplusplus
 }

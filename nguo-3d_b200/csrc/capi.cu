@@ -2,7 +2,7 @@
 #include <algorithm>
 #include <cstring>
 
-#include "internal.cuh"
+#include "lbvh.cuh"
 
 namespace mg {
 static thread_local std::string g_err;
@@ -52,6 +52,7 @@ int mguso_ctx_destroy(mguso_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     cudaStreamDestroy(ctx->stream);
   }
+  delete ctx->sort_scratch;
   delete ctx;
   return MGUSO_OK;
 }

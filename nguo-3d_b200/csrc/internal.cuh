@@ -5,10 +5,15 @@
 
 #include "common.cuh"
 
+namespace mg {
+struct Lbvh;
+}
+
 struct mguso_ctx {
   int device = 0;
   int sm_count = 148;
   cudaStream_t stream = nullptr;
+  mg::Lbvh* sort_scratch = nullptr;  // scratch for mguso_radix_sort_pairs
 };
 
 namespace mg {

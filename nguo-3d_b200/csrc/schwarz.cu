@@ -86,26 +86,33 @@ int schwarz_build(mguso_schwarz* s) {
 }
 
 // ---------------------------------------------------------------------------------------
-// Factorisation: one CTA per domain. Shared: A (m x m, f64) + diag of L^-1 (m).
-// After the Cholesky sweep the lower triangle holds L; L^-1 is accumulated transposed in
-// the upper triangle (X[i][c] at A[c][i], i > c) with its diagonal in xd[].
+// Factorisation: one CTA per domain, FP64 in shared memory. The dense block (with the
+// reference's diagonal floor) is inverted by Gauss-Jordan elimination without pivoting,
+// ping-ponging between two m x ld buffers so every step is one data-parallel pass and one
+// barrier. For an SPD block the k-th Gauss-Jordan pivot is the k-th Schur-complement
+// diagonal, i.e. exactly the value the reference's Cholesky tests against 1e-14 before
+// taking its square root (linsolve.rs:88-92), so the same blocks fall back to the
+// diagonal. ld = m + 1 keeps column accesses free of bank conflicts.
 // ---------------------------------------------------------------------------------------
-__global__ void k_schwarz_factor(const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ col,
-                                 const float* __restrict__ val, const uint32_t* __restrict__ dom_start,
-                                 const uint32_t* __restrict__ dom_verts, const uint32_t* __restrict__ dom_of,
-                                 const uint32_t* __restrict__ loc, const uint64_t* __restrict__ fac_off,
-                                 float* __restrict__ fac, uint32_t* status) {
+constexpr int FACTOR_THREADS = 256;
+
+__global__ void __launch_bounds__(FACTOR_THREADS) k_schwarz_factor(
+    const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ col, const float* __restrict__ val,
+    const uint32_t* __restrict__ dom_start, const uint32_t* __restrict__ dom_verts,
+    const uint32_t* __restrict__ dom_of, const uint32_t* __restrict__ loc, const uint64_t* __restrict__ fac_off,
+    float* __restrict__ fac, uint32_t* status) {
   extern __shared__ __align__(16) double sA[];
   __shared__ double s_floor;
   __shared__ int s_fail;
   const uint32_t d = blockIdx.x;
   const uint32_t vs = dom_start[d], nvd = dom_start[d + 1] - vs;
   const int m = 3 * (int)nvd;
-  double* xd = sA + (size_t)m * m;
+  const int ld = m + 1;
+  double* A = sA;
+  double* B = sA + (size_t)m * ld;
   const int tid = threadIdx.x, nt = blockDim.x;
-  for (int i = tid; i < m * m; i += nt) sA[i] = 0.0;
+  for (int i = tid; i < m * ld; i += nt) A[i] = 0.0;
   __syncthreads();
-  // gather this domain's dense block (each (p, q) block appears once per BSR row)
   const int lane = tid & 31, w = tid >> 5, nw = nt >> 5;
   for (uint32_t p = w; p < nvd; p += nw) {
     uint32_t v = dom_verts[vs + p];
@@ -117,50 +124,48 @@ __global__ void k_schwarz_factor(const uint32_t* __restrict__ row_ptr, const uin
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int j = 0; j < 3; ++j) sA[(3 * p + i) * m + 3 * q + j] = (double)b[3 * i + j];
+        for (int j = 0; j < 3; ++j) A[(3 * p + i) * ld + 3 * q + j] = (double)b[3 * i + j];
     }
   }
   __syncthreads();
   if (tid == 0) {
     double tr = 0.0;
-    for (int k = 0; k < m; ++k) tr += sA[k * m + k];
+    for (int k = 0; k < m; ++k) tr += A[k * ld + k];
     s_floor = 1e-6 * (tr / (double)m) + 1e-8;
     s_fail = 0;
   }
   __syncthreads();
-  for (int k = tid; k < m; k += nt) sA[k * m + k] += s_floor;
-  __syncthreads();
-  // right-looking Cholesky on the lower triangle
-  for (int k = 0; k < m; ++k) {
-    if (tid == 0) {
-      double piv = sA[k * m + k];
-      if (!(piv > 1e-14)) s_fail = 1;
-      sA[k * m + k] = sqrt(fmax(piv, 1e-300));
-    }
-    __syncthreads();
-    if (s_fail) break;
-    double lkk = sA[k * m + k];
-    for (int i = k + 1 + tid; i < m; i += nt) sA[i * m + k] /= lkk;
-    __syncthreads();
-    int rem = m - k - 1;
-    int tot = rem * (rem + 1) / 2;
-    for (int e = tid; e < tot; e += nt) {
-      // e -> (i, j) with k < j <= i < m, row-major over the trailing lower triangle
-      int ii = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
-      while ((ii + 1) * (ii + 2) / 2 <= e) ++ii;
-      while (ii * (ii + 1) / 2 > e) --ii;
-      int jj = e - ii * (ii + 1) / 2;
-      int i = k + 1 + ii, j = k + 1 + jj;
-      sA[i * m + j] -= sA[i * m + k] * sA[j * m + k];
-    }
-    __syncthreads();
-  }
+  for (int k = tid; k < m; k += nt) A[k * ld + k] += s_floor;
   __syncthreads();
   float* out = fac + fac_off[d];
+  const int total = m * m;
+  for (int k = 0; k < m; ++k) {
+    const double p = A[k * ld + k];
+    if (!(p > 1e-14)) {  // uniform: every thread reads the same pivot
+      if (tid == 0) s_fail = 1;
+      break;
+    }
+    const double ip = 1.0 / p;
+    for (int e = tid; e < total; e += nt) {
+      int i = e / m, j = e - i * m;
+      double r;
+      if (i == k)
+        r = (j == k) ? ip : A[k * ld + j] * ip;
+      else if (j == k)
+        r = -A[i * ld + k] * ip;
+      else
+        r = A[i * ld + j] - A[i * ld + k] * (A[k * ld + j] * ip);
+      B[i * ld + j] = r;
+    }
+    __syncthreads();
+    double* t = A;
+    A = B;
+    B = t;
+  }
+  __syncthreads();
   if (s_fail) {
     // reference fallback: L = diag(sqrt(ad_pp)) (1 where ad_pp <= 1e-14), so
-    // M^-1 = diag(1 / ad_pp). The diagonal was overwritten by the failed sweep, so it is
-    // re-gathered here.
+    // M^-1 = diag(1 / ad_pp); the floored diagonal is re-gathered from the matrix.
     for (int e = tid; e < m * (m + 1) / 2; e += nt) out[e] = 0.0f;
     __syncthreads();
     for (uint32_t p = w; p < nvd; p += nw) {
@@ -178,52 +183,17 @@ __global__ void k_schwarz_factor(const uint32_t* __restrict__ row_ptr, const uin
     if (tid == 0) atomicOr(status, 1u << 8);
     return;
   }
-  // X = L^-1: zero the strict upper triangle, xd = 1, then right-looking row sweep.
-  for (int e = tid; e < m * m; e += nt) {
-    int i = e / m, j = e % m;
-    if (j > i) sA[e] = 0.0;
-  }
-  for (int i = tid; i < m; i += nt) xd[i] = 1.0;
-  __syncthreads();
-  for (int k = 0; k < m; ++k) {
-    double lkk = sA[k * m + k];
-    // finalise row k of X: X[k][c] /= L_kk, c <= k
-    for (int c = tid; c <= k; c += nt) {
-      if (c == k)
-        xd[k] /= lkk;
-      else
-        sA[c * m + k] /= lkk;
-    }
-    __syncthreads();
-    int rows = m - k - 1, cols = k + 1;
-    for (int e = tid; e < rows * cols; e += nt) {
-      int i = k + 1 + e / cols, c = e % cols;
-      double xkc = (c == k) ? xd[k] : sA[c * m + k];
-      sA[c * m + i] -= sA[i * m + k] * xkc;
-    }
-    __syncthreads();
-  }
-  // M^-1[i][j] = sum_{k >= i} X[k][i] X[k][j] for i >= j, packed row-major lower.
-  for (int e = tid; e < m * (m + 1) / 2; e += nt) {
-    int i = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
-    while ((i + 1) * (i + 2) / 2 <= e) ++i;
-    while (i * (i + 1) / 2 > e) --i;
-    int j = e - i * (i + 1) / 2;
-    double s = 0.0;
-    for (int k = i; k < m; ++k) {
-      double xki = (k == i) ? xd[i] : sA[i * m + k];
-      double xkj = (k == j) ? xd[j] : sA[j * m + k];
-      s += xki * xkj;
-    }
-    out[e] = (float)s;
-  }
+  // packed row-major lower triangle of the (symmetric) inverse; the two triangles are
+  // averaged so rounding asymmetry does not leak into the preconditioner
+  for (int i = w; i < m; i += nw)
+    for (int j = lane; j <= i; j += 32) out[i * (i + 1) / 2 + j] = (float)(0.5 * (A[i * ld + j] + A[j * ld + i]));
 }
 
 int schwarz_factor(mguso_schwarz* s, cudaStream_t st) {
   if (s->ndom == 0) return MGUSO_OK;
   mguso_bsr* a = s->a;
-  size_t smem = sizeof(double) * ((size_t)s->max_m * s->max_m + s->max_m);
-  k_schwarz_factor<<<s->ndom, 128, smem, st>>>(a->row_ptr.p, a->col.p, a->val.p, s->dom_start.p, s->dom_verts.p,
+  size_t smem = sizeof(double) * 2 * (size_t)s->max_m * (s->max_m + 1);
+  k_schwarz_factor<<<s->ndom, FACTOR_THREADS, smem, st>>>(a->row_ptr.p, a->col.p, a->val.p, s->dom_start.p, s->dom_verts.p,
                                                s->dom_of.p, s->loc.p, s->fac_off.p, s->fac.p, s->status.p);
   MG_CUDA(cudaGetLastError());
   return MGUSO_OK;
@@ -291,7 +261,7 @@ int schwarz_configure() {
   static bool done = false;
   if (done) return MGUSO_OK;
   constexpr int WARPS = 4;
-  size_t fsm = sizeof(double) * (96 * 96 + 96);
+  size_t fsm = sizeof(double) * 2 * 96 * 97;
   MG_CUDA(cudaFuncSetAttribute(k_schwarz_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
   uint32_t slice = ((96 * 97 / 2 + 3) & ~3u) + 96;
   slice = (slice + 31) & ~31u;

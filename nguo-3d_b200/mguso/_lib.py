@@ -85,6 +85,15 @@ def load() -> C.CDLL:
         "mguso_schwarz_factor": (i32, [vp, vp]),
         "mguso_schwarz_apply": (i32, [vp, vp, vp, vp]),
         "mguso_schwarz_domains": (i32, [vp, vp]),
+        "mguso_lbvh_create": (i32, [vp, P(vp)]),
+        "mguso_lbvh_destroy": (i32, [vp]),
+        "mguso_lbvh_build": (i32, [vp, vp, u32, vp, u32, i32, vp]),
+        "mguso_lbvh_query_points": (i32, [vp, vp, u32, f32, vp, u64, vp, vp]),
+        "mguso_lbvh_download": (i32, [vp, vp, vp, vp, vp, vp]),
+        "mguso_lbvh_status": (i32, [vp]),
+        "mguso_lbvh_stage_times": (i32, [vp, i32, vp]),
+        "mguso_lbvh_build_query": (i32, [vp, vp, u32, vp, u32, i32, f32, vp, vp, vp, u64, P(u64)]),
+        "mguso_radix_sort_pairs": (i32, [vp, vp, vp, u32, i32, vp]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)

@@ -118,3 +118,15 @@ def bsr_spmv_f64(row_ptr: np.ndarray, col: np.ndarray, val: np.ndarray, x: np.nd
         sums = np.add.reduceat(prod, rp[:-1][nonempty], axis=0)
         y[nonempty] = sums
     return y.reshape(-1)
+
+
+def triangle_soup(nt: int, seed: int = 3, edge: float = 2.0e-3):
+    """LBVH microbenchmark input: `nt` triangles with centroids uniform in the unit cube and
+    unshared vertices at centroid + offsets uniform in [-edge/2, edge/2]^3 (edge-length
+    scale `edge`, 2 mm by default). Returns (positions f32[3nt, 3], tris u32[nt, 3])."""
+    rng = np.random.default_rng(seed)
+    c = rng.random((nt, 3), dtype=np.float32)
+    off = (rng.random((nt, 3, 3), dtype=np.float32) - np.float32(0.5)) * np.float32(edge)
+    pos = (c[:, None, :] + off).reshape(-1, 3)
+    tris = np.arange(3 * nt, dtype=np.uint32).reshape(nt, 3)
+    return np.ascontiguousarray(pos), tris

@@ -73,32 +73,37 @@ template <class R> inline R rclamp(R v, R lo, R hi) { return v < lo ? lo : (v > 
 // ---------------------------------------------------------------------------------------
 // CSR (engine-core/src/csr.rs:9-14)
 // ---------------------------------------------------------------------------------------
-struct Triplet {
+template <class R>
+struct TripletT {
   uint32_t r, c;
-  float v;
+  R v;
 };
 
-struct Csr {
+template <class R>
+struct CsrT {
   size_t n = 0;
   std::vector<uint32_t> row_ptr, col_idx;
-  std::vector<float> values;
+  std::vector<R> values;
   size_t nnz() const { return values.size(); }
 };
+using Triplet = TripletT<float>;
+using Csr = CsrT<float>;
 
 // Sort one row's (col, value) entries by column and coalesce duplicates (csr.rs:63-84).
 // The reference uses an unstable sort; a stable sort is used here so duplicate cells are
 // summed in push order (the Rust order of equal keys is implementation-defined, so the
 // two agree up to the summation order of duplicates).
-inline void sort_coalesce_row(std::vector<std::pair<uint32_t, float>>& flat, size_t lo, size_t hi,
-                              std::vector<uint32_t>& col_idx, std::vector<float>& values) {
+template <class R>
+inline void sort_coalesce_row(std::vector<std::pair<uint32_t, R>>& flat, size_t lo, size_t hi,
+                              std::vector<uint32_t>& col_idx, std::vector<R>& values) {
   std::stable_sort(flat.begin() + lo, flat.begin() + hi,
-                   [](const std::pair<uint32_t, float>& a, const std::pair<uint32_t, float>& b) {
+                   [](const std::pair<uint32_t, R>& a, const std::pair<uint32_t, R>& b) {
                      return a.first < b.first;
                    });
   size_t j = lo;
   while (j < hi) {
     uint32_t c = flat[j].first;
-    float sum = 0.0f;
+    R sum = R(0);
     while (j < hi && flat[j].first == c) {
       sum += flat[j].second;
       ++j;
@@ -109,14 +114,15 @@ inline void sort_coalesce_row(std::vector<std::pair<uint32_t, float>>& flat, siz
 }
 
 // CsrMatrix::from_triplets (csr.rs:37-91): counting sort by row, per-row sort + coalesce.
-inline Csr csr_from_triplets(size_t n, const Triplet* t, size_t nt) {
+template <class R>
+inline CsrT<R> csr_from_triplets(size_t n, const TripletT<R>* t, size_t nt) {
   std::vector<uint32_t> starts(n + 1, 0);
   for (size_t k = 0; k < nt; ++k) starts[t[k].r + 1] += 1;
   for (size_t k = 0; k < n; ++k) starts[k + 1] += starts[k];
   std::vector<uint32_t> cursor(starts.begin(), starts.end() - 1);
-  std::vector<std::pair<uint32_t, float>> flat(nt);
+  std::vector<std::pair<uint32_t, R>> flat(nt);
   for (size_t k = 0; k < nt; ++k) flat[cursor[t[k].r]++] = {t[k].c, t[k].v};
-  Csr m;
+  CsrT<R> m;
   m.n = n;
   m.row_ptr.reserve(n + 1);
   m.row_ptr.push_back(0);
@@ -128,7 +134,8 @@ inline Csr csr_from_triplets(size_t n, const Triplet* t, size_t nt) {
 }
 
 // merge_csr (csr.rs:420-461): out = a + b, a's partial sums first.
-inline void merge_csr(const Csr& a, const Csr& b, Csr& out) {
+template <class R>
+inline void merge_csr(const CsrT<R>& a, const CsrT<R>& b, CsrT<R>& out) {
   size_t n = a.n;
   out.n = n;
   out.row_ptr.clear();
@@ -160,14 +167,15 @@ inline void merge_csr(const Csr& a, const Csr& b, Csr& out) {
 
 // TripletSink (csr.rs:205-416): streaming chunked accumulator, CHUNK_MIN = 2^14 growing by
 // doubling to CHUNK_MAX = 2^21, then folding; `finish` applies the Dirichlet filter.
-struct TripletSink {
+template <class R>
+struct TripletSinkT {
   static constexpr size_t CHUNK_MIN = size_t(1) << 14;
   static constexpr size_t CHUNK_MAX = size_t(1) << 21;
   size_t n = 0;
-  std::vector<Triplet> buf;
+  std::vector<TripletT<R>> buf;
   size_t flush_at = CHUNK_MIN;
   size_t pushed = 0, flushes = 0;
-  Csr acc, scratch, chunk;
+  CsrT<R> acc, scratch, chunk;
   bool acc_empty = true;
 
   void begin(size_t n_) {
@@ -175,11 +183,11 @@ struct TripletSink {
     buf.clear();
     pushed = 0;
     flushes = 0;
-    acc = Csr();
+    acc = CsrT<R>();
     acc.n = n;
     acc_empty = true;
   }
-  void push(const Triplet& t) {
+  void push(const TripletT<R>& t) {
     ++pushed;
     buf.push_back(t);
     if (buf.size() >= flush_at) {
@@ -204,16 +212,16 @@ struct TripletSink {
     ++flushes;
   }
   // `pinned` indexed by vertex (dof / 3); empty pins nothing (csr.rs:385-415).
-  Csr finish(const std::vector<uint8_t>& pinned) {
+  CsrT<R> finish(const std::vector<uint8_t>& pinned) {
     flush();
-    Csr out;
+    CsrT<R> out;
     out.n = n;
     out.row_ptr.push_back(0);
     auto pin = [&](size_t dof) { return dof / 3 < pinned.size() && pinned[dof / 3]; };
     for (size_t r = 0; r < n; ++r) {
       if (pin(r)) {
         out.col_idx.push_back((uint32_t)r);
-        out.values.push_back(1.0f);
+        out.values.push_back(R(1));
       } else if (!acc_empty) {
         for (size_t k = acc.row_ptr[r]; k < acc.row_ptr[r + 1]; ++k) {
           uint32_t c = acc.col_idx[k];
@@ -228,19 +236,22 @@ struct TripletSink {
     return out;
   }
 };
+using TripletSink = TripletSinkT<float>;
 
-// CsrMatrix::spmv_cpu (csr.rs:98-111), f32 accumulation.
-inline void spmv_f32(const Csr& a, const float* x, float* y) {
+// CsrMatrix::spmv_cpu (csr.rs:98-111), accumulation in the value type.
+template <class R>
+inline void spmv_f32(const CsrT<R>& a, const R* x, R* y) {
   for (size_t r = 0; r < a.n; ++r) {
-    float s = 0.0f;
+    R s = R(0);
     for (size_t k = a.row_ptr[r]; k < a.row_ptr[r + 1]; ++k) s += a.values[k] * x[a.col_idx[k]];
     y[r] = s;
   }
 }
 
 // CsrMatrix::diagonal (csr.rs:113-124).
-inline std::vector<float> csr_diagonal(const Csr& a) {
-  std::vector<float> d(a.n, 0.0f);
+template <class R>
+inline std::vector<R> csr_diagonal(const CsrT<R>& a) {
+  std::vector<R> d(a.n, R(0));
   for (size_t r = 0; r < a.n; ++r)
     for (size_t k = a.row_ptr[r]; k < a.row_ptr[r + 1]; ++k)
       if (a.col_idx[k] == r) d[r] = a.values[k];
@@ -336,7 +347,8 @@ inline std::vector<std::vector<uint32_t>> bfs_domains(const std::vector<std::vec
   return domains;
 }
 
-inline std::vector<std::vector<uint32_t>> vertex_adjacency(const Csr& a) {
+template <class R>
+inline std::vector<std::vector<uint32_t>> vertex_adjacency(const CsrT<R>& a) {
   size_t nv = a.n / 3;
   std::vector<std::vector<uint32_t>> adj(nv);
   for (size_t row = 0; row < a.n; ++row) {
@@ -357,7 +369,8 @@ struct SchwarzTopology {
   std::vector<std::vector<uint32_t>> domains;
   std::vector<std::vector<int64_t>> gather;  // -1 = structurally absent
 
-  static SchwarzTopology build(const Csr& a, size_t domain_size) {
+  template <class R>
+  static SchwarzTopology build(const CsrT<R>& a, size_t domain_size) {
     SchwarzTopology t;
     t.domains = bfs_domains(vertex_adjacency(a), domain_size);
     auto find_idx = [&](size_t row, size_t col) -> int64_t {
@@ -380,7 +393,8 @@ struct SchwarzTopology {
 
   // factorize (linsolve.rs:204-237): diagonal floor 1e-6*(tr/m) + 1e-8, then Cholesky;
   // a non-PD block falls back to sqrt of the floored diagonal.
-  std::vector<std::vector<double>> factorize(const Csr& a) const {
+  template <class R>
+  std::vector<std::vector<double>> factorize(const CsrT<R>& a) const {
     std::vector<std::vector<double>> factors;
     factors.reserve(domains.size());
     for (size_t di = 0; di < domains.size(); ++di) {
@@ -420,9 +434,9 @@ struct SchwarzTopology {
 };
 
 // cg_run (linsolve.rs:350-411): f64 PCG, x0 = 0, relative residual stop, pAp <= 0 break.
-template <class PrecondFn>
-inline LinearStats cg_run(const Csr& a, const float* b, float tol, uint32_t max_iter, PrecondFn precond,
-                          float* x_out) {
+template <class R, class PrecondFn>
+inline LinearStats cg_run(const CsrT<R>& a, const R* b, R tol, uint32_t max_iter, PrecondFn precond,
+                          R* x_out) {
   size_t n = a.n;
   auto spmv = [&](const std::vector<double>& x, std::vector<double>& out) {
     for (size_t row = 0; row < n; ++row) {
@@ -464,20 +478,21 @@ inline LinearStats cg_run(const Csr& a, const float* b, float tol, uint32_t max_
     for (size_t i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
     rz = rz_new;
   }
-  for (size_t i = 0; i < n; ++i) x_out[i] = (float)x[i];
+  for (size_t i = 0; i < n; ++i) x_out[i] = (R)x[i];
   return st;
 }
 
 // cg_cpu_precond (linsolve.rs:272-346) with an explicit preconditioner kind.
-inline LinearStats cg_precond(const Csr& a, const float* b, float tol, uint32_t max_iter, Precond kind_in,
-                              size_t domain, float* x_out) {
+template <class R>
+inline LinearStats cg_precond(const CsrT<R>& a, const R* b, R tol, uint32_t max_iter, Precond kind_in,
+                              size_t domain, R* x_out) {
   size_t n = a.n;
   bool block3 = n % 3 == 0;
   Precond kind = kind_in;
   if ((kind == Precond::Block || kind == Precond::Schwarz) && !block3) kind = Precond::Diagonal;
-  std::vector<float> dg = csr_diagonal(a);
+  std::vector<R> dg = csr_diagonal(a);
   std::vector<double> inv_diag(n);
-  for (size_t i = 0; i < n; ++i) inv_diag[i] = dg[i] != 0.0f ? 1.0 / (double)dg[i] : 1.0;
+  for (size_t i = 0; i < n; ++i) inv_diag[i] = dg[i] != R(0) ? 1.0 / (double)dg[i] : 1.0;
   std::vector<std::array<double, 9>> binv;
   if (kind == Precond::Block) {
     size_t nv = n / 3;
@@ -525,8 +540,9 @@ inline LinearStats cg_precond(const Csr& a, const float* b, float tol, uint32_t 
 }
 
 // relative_residual (linsolve.rs:445-455).
-inline double relative_residual(const Csr& a, const float* x, const float* b) {
-  std::vector<float> ax(a.n);
+template <class R>
+inline double relative_residual(const CsrT<R>& a, const R* x, const R* b) {
+  std::vector<R> ax(a.n);
   spmv_f32(a, x, ax.data());
   double num = 0.0, den = 0.0;
   for (size_t i = 0; i < a.n; ++i) {
@@ -543,7 +559,8 @@ struct LinearSolver {
   Precond kind = Precond::Block;
   size_t domain = 32;
   LinearStats last;
-  void solve(const Csr& a, const float* b, float tol, uint32_t max_iter, float* x) {
+  template <class R>
+  void solve(const CsrT<R>& a, const R* b, R tol, uint32_t max_iter, R* x) {
     if (kind == Precond::Schwarz && a.n % 3 == 0) {
       last = cg_precond(a, b, tol, max_iter, Precond::Schwarz, domain, x);
     } else {
