@@ -106,7 +106,8 @@ int mguso_bsr_spmv(mguso_bsr* a, const float* x, float* y, void* stream);
 /* y = A x with x, y host: copies in, multiplies, copies out (synchronous). */
 int mguso_bsr_spmv_host(mguso_bsr* a, const float* x, float* y);
 /* Selects the SpMV kernel variant: 0 = auto (autotuned), 1 = TMA-staged tiles,
- * 2 = direct thread-per-row. Returns the variant in use through *active. */
+ * 2 = direct thread-per-row, 3 = sliced ELL (32-row slices, coalesced 128-byte loads;
+ * builds the sliced copy on first use). Returns the variant in use through *active. */
 int mguso_bsr_set_kernel(mguso_bsr* a, int variant, int* active);
 /* Runs the SpMV autotuner on this matrix (times every variant and tile shape with CUDA
  * events) and keeps the fastest. *best_us gets its time per apply. */

@@ -77,6 +77,8 @@ int bsr_upload(mguso_bsr* m, uint32_t nb, const std::vector<uint32_t>& row_ptr, 
   MG_TRY(m->status.reserve(4));
   MG_CUDA(cudaMemsetAsync(m->status.p, 0, 16, s));
   m->tilings.clear();
+  m->sell.ready = false;
+  if (m->nnzb) m->h_val_keep.assign(val_host, val_host + (size_t)9 * m->nnzb);
   MG_TRY(bsr_prepare_tilings(m));
   MG_CUDA(cudaStreamSynchronize(s));
   return MGUSO_OK;
@@ -223,6 +225,86 @@ __global__ void k_spmv_direct(const uint32_t* __restrict__ row_ptr, const uint32
   if (with_dot) grid_dot_commit<Acc>(dot, acc.v);
 }
 
+// Sliced-ELL variant: one block row per thread, 32 rows per warp-aligned slice; values and
+// columns are streamed with evict-first loads, x is gathered through the read-only path.
+template <class Acc>
+__global__ void __launch_bounds__(256) k_spmv_sell(const uint32_t* __restrict__ slice_base,
+                                                   const uint32_t* __restrict__ scol, const float* __restrict__ sval,
+                                                   uint32_t nb, const float* __restrict__ x, float* __restrict__ y,
+                                                   DotSink dot, int with_dot) {
+  if (with_dot && dot.sc->done) return;
+  DotAcc<Acc> acc;
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < ((nb + 31u) & ~31u); r += gridDim.x * blockDim.x) {
+    const uint32_t sl = r >> 5, lane = r & 31u;
+    const uint32_t b0 = slice_base[sl], b1 = slice_base[sl + 1];
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+    const uint32_t* cp = scol + (size_t)b0 * 32 + lane;
+    const float* vp = sval + (size_t)b0 * 288 + lane;
+#pragma unroll 2
+    for (uint32_t k = b0; k < b1; ++k) {
+      uint32_t c = __ldcs(cp);
+      float a0 = __ldcs(vp), a1 = __ldcs(vp + 32), a2 = __ldcs(vp + 64);
+      float a3 = __ldcs(vp + 96), a4 = __ldcs(vp + 128), a5 = __ldcs(vp + 160);
+      float a6 = __ldcs(vp + 192), a7 = __ldcs(vp + 224), a8 = __ldcs(vp + 256);
+      float x0 = __ldg(x + 3 * c), x1 = __ldg(x + 3 * c + 1), x2 = __ldg(x + 3 * c + 2);
+      s0 = fmaf(a0, x0, s0); s0 = fmaf(a1, x1, s0); s0 = fmaf(a2, x2, s0);
+      s1 = fmaf(a3, x0, s1); s1 = fmaf(a4, x1, s1); s1 = fmaf(a5, x2, s1);
+      s2 = fmaf(a6, x0, s2); s2 = fmaf(a7, x1, s2); s2 = fmaf(a8, x2, s2);
+      cp += 32;
+      vp += 288;
+    }
+    if (r < nb) {
+      y[3 * r] = s0;
+      y[3 * r + 1] = s1;
+      y[3 * r + 2] = s2;
+      if (with_dot) {
+        acc.add(x[3 * r], s0);
+        acc.add(x[3 * r + 1], s1);
+        acc.add(x[3 * r + 2], s2);
+      }
+    }
+  }
+  if (with_dot) grid_dot_commit<Acc>(dot, acc.v);
+}
+
+int bsr_build_sell(mguso_bsr* m) {
+  SellLayout& L = m->sell;
+  if (L.ready) return MGUSO_OK;
+  const uint32_t nb = m->nb;
+  L.nslices = (nb + 31) / 32;
+  std::vector<uint32_t> base(L.nslices + 1, 0);
+  for (uint32_t sl = 0; sl < L.nslices; ++sl) {
+    uint32_t mx = 0;
+    for (uint32_t r = sl * 32; r < std::min(nb, sl * 32 + 32); ++r)
+      mx = std::max(mx, m->h_row_ptr[r + 1] - m->h_row_ptr[r]);
+    base[sl + 1] = base[sl] + mx;
+  }
+  L.total_k = base[L.nslices];
+  std::vector<uint32_t> col((size_t)32 * L.total_k, 0);
+  std::vector<float> val((size_t)288 * L.total_k, 0.0f);
+  for (uint32_t r = 0; r < L.nslices * 32; ++r) {
+    uint32_t sl = r >> 5, lane = r & 31;
+    uint32_t len = base[sl + 1] - base[sl];
+    uint32_t kb = r < nb ? m->h_row_ptr[r] : 0, ke = r < nb ? m->h_row_ptr[r + 1] : 0;
+    for (uint32_t k = 0; k < len; ++k) {
+      size_t g = (size_t)base[sl] + k;
+      if (kb + k < ke) {
+        col[g * 32 + lane] = m->h_col[kb + k];
+        for (int e = 0; e < 9; ++e) val[(g * 9 + e) * 32 + lane] = m->h_val_keep[9 * (size_t)(kb + k) + e];
+      } else {
+        col[g * 32 + lane] = r < nb ? r : 0;
+      }
+    }
+  }
+  cudaStream_t s = m->ctx->stream;
+  MG_TRY(L.slice_base.upload(base.data(), base.size(), s));
+  MG_TRY(L.col.upload(col.data(), col.size(), s));
+  MG_TRY(L.val.upload(val.data(), val.size(), s));
+  MG_CUDA(cudaStreamSynchronize(s));
+  L.ready = true;
+  return MGUSO_OK;
+}
+
 // ---------------------------------------------------------------------------------------
 // Tilings
 // ---------------------------------------------------------------------------------------
@@ -293,6 +375,18 @@ static int launch_spmv(mguso_bsr* m, int variant, int tiling, const float* x, fl
   if (dot) d = *dot;
   bool mixed = dot && dot->mixed;
   if (m->nb == 0) return MGUSO_OK;
+  if (variant == SPMV_SELL && m->sell.ready) {
+    int threads = 256;
+    uint32_t rows = m->sell.nslices * 32;
+    int grid = (int)std::min<uint64_t>(ceil_div(rows, threads), with_dot ? MAX_PARTIALS : 1u << 20);
+    const SellLayout& L = m->sell;
+    if (mixed)
+      k_spmv_sell<double><<<grid, threads, 0, s>>>(L.slice_base.p, L.col.p, L.val.p, m->nb, x, y, d, with_dot);
+    else
+      k_spmv_sell<float><<<grid, threads, 0, s>>>(L.slice_base.p, L.col.p, L.val.p, m->nb, x, y, d, with_dot);
+    MG_CUDA(cudaGetLastError());
+    return MGUSO_OK;
+  }
   if (variant == SPMV_TMA && tiling >= 0 && m->tilings[tiling]->ok) {
     SpmvTiling& t = *m->tilings[tiling];
     size_t smem = 128 + (size_t)t.stages * (t.val_stage_bytes + t.col_stage_bytes);
@@ -349,6 +443,13 @@ int bsr_autotune(mguso_bsr* m, float* best_us) {
   };
   float us = time_it(SPMV_DIRECT, -1);
   best = us;
+  if (bsr_build_sell(m) == MGUSO_OK) {
+    us = time_it(SPMV_SELL, -1);
+    if (us < best) {
+      best = us;
+      best_var = SPMV_SELL;
+    }
+  }
   for (size_t i = 0; i < m->tilings.size(); ++i) {
     if (!m->tilings[i]->ok) continue;
     us = time_it(SPMV_TMA, (int)i);

@@ -132,7 +132,8 @@ int mguso_bsr_spmv_host(mguso_bsr* a, const float* x, float* y) {
 }
 
 int mguso_bsr_set_kernel(mguso_bsr* a, int variant, int* active) {
-  MG_CHECK_ARG(a && variant >= 0 && variant <= 2, "bad variant");
+  MG_CHECK_ARG(a && variant >= 0 && variant <= 3, "bad variant");
+  if (variant == SPMV_SELL) MG_TRY(bsr_build_sell(a));
   a->variant = variant;
   if (active) *active = (variant == SPMV_AUTO) ? (a->tiling_choice >= 0 ? SPMV_TMA : SPMV_DIRECT) : variant;
   return MGUSO_OK;

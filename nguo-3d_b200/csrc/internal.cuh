@@ -19,7 +19,21 @@ struct mguso_ctx {
 namespace mg {
 
 // SpMV kernel variants (mguso_bsr_set_kernel).
-enum SpmvVariant : int { SPMV_AUTO = 0, SPMV_TMA = 1, SPMV_DIRECT = 2 };
+enum SpmvVariant : int { SPMV_AUTO = 0, SPMV_TMA = 1, SPMV_DIRECT = 2, SPMV_SELL = 3 };
+
+// Sliced-ELL copy of a BSR matrix: 32 block rows per slice, each slice padded to its
+// longest row; within a slice, block k of lane l keeps its column at
+// col[(base + k) * 32 + l] and entry e of its 3x3 block at val[((base + k) * 9 + e) * 32 + l],
+// so every warp-wide load is one contiguous 128-byte line. Padding blocks are zero with
+// the row's own column.
+struct SellLayout {
+  uint32_t nslices = 0;
+  uint64_t total_k = 0;           // sum over slices of the padded length
+  DevBuf<uint32_t> slice_base;    // nslices + 1 (in units of 32-block groups)
+  DevBuf<uint32_t> col;           // 32 * total_k
+  DevBuf<float> val;              // 9 * 32 * total_k
+  bool ready = false;
+};
 
 // One TMA-staged tiling of a BSR matrix: tiles of <= `rows` block rows and <= `cap`
 // blocks; each tile's value and column ranges are staged into shared memory by 1-D bulk
@@ -46,6 +60,8 @@ struct mguso_bsr {
   int variant = mg::SPMV_AUTO;
   int tiling_choice = 0;  // index into tilings when variant == TMA
   std::vector<std::unique_ptr<mg::SpmvTiling>> tilings;
+  mg::SellLayout sell;
+  std::vector<float> h_val_keep;  // host values kept for building the sliced copy lazily
   mg::DevBuf<uint32_t> status;
   mg::DevBuf<float> hx, hy;  // staging for spmv_host
 };
@@ -78,6 +94,7 @@ int bsr_prepare_tilings(mguso_bsr* m);
 struct DotSink;
 int bsr_spmv(mguso_bsr* m, const float* x, float* y, cudaStream_t s, const DotSink* dot);
 int bsr_autotune(mguso_bsr* m, float* best_us);
+int bsr_build_sell(mguso_bsr* m);
 
 // ---- Schwarz ---------------------------------------------------------------------------
 int schwarz_build(mguso_schwarz* s);

@@ -130,3 +130,67 @@ def triangle_soup(nt: int, seed: int = 3, edge: float = 2.0e-3):
     pos = (c[:, None, :] + off).reshape(-1, 3)
     tris = np.arange(3 * nt, dtype=np.uint32).reshape(nt, 3)
     return np.ascontiguousarray(pos), tris
+
+
+# ---------------------------------------------------------------------------------------
+# Drape scenes (the implicit step's inputs). A scene is a dict of numpy arrays plus
+# `params`, the solver knobs named as in the reference's ImplicitParams
+# (engine-core/src/implicit.rs:30-229).
+# ---------------------------------------------------------------------------------------
+def lame_from_young_poisson(young: float, poisson: float):
+    """material::lame_from_young_poisson (engine-core/src/material.rs:31-45), in f32."""
+    nu = np.float32(min(max(poisson, 1.0e-6), 0.5 - 1.0e-4))
+    y = np.float32(young)
+    mu = y / (np.float32(2.0) * (np.float32(1.0) + nu))
+    lam = y * nu / ((np.float32(1.0) + nu) * (np.float32(1.0) - np.float32(2.0) * nu))
+    return float(mu), float(lam)
+
+
+def default_params(**kw):
+    p = dict(dt=1.0 / 60.0, gravity=(0.0, -9.8, 0.0), newton_iters=32, stiffness=0.0, bend_stiffness=1.0e-5,
+             max_dx=float("inf"), target_toi=0.0, min_newton_steps=0, ccd_max_iter=256, eiganalysis_eps=1.0e-6,
+             contact_dhat=1.0e-3, contact_kappa=1.0e2, contact_dynamic=0.0, shell_mu=0.0, shell_lambda=0.0,
+             friction=0.0, friction_eps=1.0e-3, barrier_kind=0, contact_rayleigh=1, self_collision=1,
+             cg_tol=1.0e-4, cg_max_iter=2000, floor_y=float("-inf"), newton_tol=0.0, precond=2,
+             schwarz_domain=32)
+    p.update(kw)
+    return p
+
+
+def uniform_mass(positions: np.ndarray, tris: np.ndarray, density: float) -> float:
+    """Scene::lower's lumped mass: total area * density / vertex count
+    (engine-api/src/scene.rs:128-131), floored at 1e-6."""
+    p = positions.astype(np.float64)
+    t = tris.astype(np.int64)
+    area = 0.5 * np.linalg.norm(np.cross(p[t[:, 1]] - p[t[:, 0]], p[t[:, 2]] - p[t[:, 0]]), axis=1).sum()
+    return max(float(area * density / max(p.shape[0], 1)), 1.0e-6)
+
+
+def _empty_stitches():
+    return (np.zeros((0, 6), np.uint32), np.zeros((0, 6), np.float32), np.zeros((0, 3), np.float32))
+
+
+def sheet_on_sphere(n: int = 64, side: float = 1.0, height: float = 0.5, jitter: float = 1.0e-3, seed: int = 0,
+                    radius: float = 0.3, young: float = 1.0e5, poisson: float = 0.3, thickness: float = 5.0e-4,
+                    bend: float = 1.0e-5, density: float = 0.2, dhat: float = 1.0e-3, dt: float = 1.0 / 60.0,
+                    newton_tol_mps: float = 1.0e-3, **kw):
+    """Square cloth sheet as an n x n vertex grid (side `side`, horizontal at y = height,
+    every vertex jittered by a seeded uniform +-jitter per axis), StVK membrane from
+    (E * thickness, nu), hinge bending k_b, uniform lumped mass from the areal density,
+    dropped under gravity onto an analytic sphere of `radius` at the origin.
+    newton_tol_mps * dt is the added Newton termination on the step taken (metres)."""
+    rng = np.random.default_rng(seed)
+    s = np.linspace(-0.5 * side, 0.5 * side, n, dtype=np.float64)
+    X, Z = np.meshgrid(s, s)  # [j, i]
+    pos = np.stack([X, np.full_like(X, height), Z], -1).reshape(-1, 3)
+    pos = (pos + rng.uniform(-jitter, jitter, pos.shape)).astype(np.float32)
+    tris = grid_tris(n)
+    mu, lam = lame_from_young_poisson(young * thickness, poisson)
+    m = uniform_mass(pos, tris, density)
+    si, sw, skl = _empty_stitches()
+    params = default_params(dt=dt, bend_stiffness=bend, contact_dhat=dhat, shell_mu=mu, shell_lambda=lam,
+                            newton_tol=newton_tol_mps * dt, **kw)
+    return dict(positions=pos, velocities=np.zeros_like(pos), inv_mass=np.full(pos.shape[0], 1.0 / m, np.float32),
+                tris=tris, shell_faces=tris.copy(), static_mask=None, stitch_idx=si, stitch_w=sw, stitch_kl=skl,
+                colliders=np.array([[1, 0, 0, 0, 0, 0, 0, radius]], np.float32), params=params,
+                name=f"{n}x{n} sheet on r={radius} sphere")

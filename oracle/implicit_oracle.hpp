@@ -18,6 +18,7 @@
 // taken, max_i |t dx_i| < newton_tol (0 disables it).
 #pragma once
 #include <functional>
+#include <map>
 #include <unordered_map>
 
 #include "mguso_oracle.hpp"

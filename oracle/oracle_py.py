@@ -182,3 +182,221 @@ def lbvh(pos, tris, bits, dhat, cap=None):
     cnt = lib.oracle_lbvh(_p(p), nv, _p(t), nt, bits, dhat, _p(keys), _p(perm), _p(left), _p(right), _p(node),
                           _p(pairs), cap)
     return keys, perm, left[:max(nt - 1, 0)], right[:max(nt - 1, 0)], node[:max(nt - 1, 0)], pairs[:min(cnt, cap)]
+
+
+# ---- implicit step ---------------------------------------------------------------------
+class OracleParams(C.Structure):
+    _fields_ = [("dt", C.c_float), ("gravity", C.c_float * 3), ("newton_iters", C.c_uint32),
+                ("stiffness", C.c_float), ("bend_stiffness", C.c_float), ("max_dx", C.c_float),
+                ("target_toi", C.c_float), ("min_newton_steps", C.c_uint32), ("ccd_max_iter", C.c_uint32),
+                ("eiganalysis_eps", C.c_float), ("contact_dhat", C.c_float), ("contact_kappa", C.c_float),
+                ("contact_dynamic", C.c_float), ("shell_mu", C.c_float), ("shell_lambda", C.c_float),
+                ("friction", C.c_float), ("friction_eps", C.c_float), ("barrier_kind", C.c_int),
+                ("contact_rayleigh", C.c_int), ("self_collision", C.c_int), ("cg_tol", C.c_float),
+                ("cg_max_iter", C.c_uint32), ("floor_y", C.c_float), ("newton_tol", C.c_float),
+                ("precond", C.c_int), ("schwarz_domain", C.c_uint32)]
+
+
+class OracleStats(C.Structure):
+    _fields_ = [("newton_iters", C.c_uint32), ("max_cg_iters", C.c_uint32), ("num_contacts", C.c_uint32),
+                ("stencils", C.c_uint32), ("ccd_cap_hits", C.c_uint32), ("max_reresid", C.c_double),
+                ("t_min", C.c_double), ("penetration_free", C.c_int), ("all_finite", C.c_int)]
+
+
+def _step_sigs(lib):
+    vp, u32, i32, f32 = C.c_void_p, C.c_uint32, C.c_int, C.c_float
+    P = C.POINTER
+    sigs = {
+        "oracle_solver_new": (vp, [i32, u32, vp, vp, vp, u32, vp, vp, u32, vp, u32, vp, vp, vp, u32, vp,
+                                   P(OracleParams)]),
+        "oracle_solver_free": (None, [vp]),
+        "oracle_solver_step": (i32, [vp, i32, i32, vp]),
+        "oracle_solver_state": (None, [vp, vp, vp]),
+        "oracle_solver_set_state": (None, [vp, vp, vp]),
+        "oracle_solver_counts": (None, [vp, vp]),
+        "oracle_solver_stencils": (u32, [vp, vp, vp, u32]),
+        "oracle_solver_assemble": (vp, [vp, vp, vp, vp]),
+        "oracle_solver_ccd": (f32, [vp, vp]),
+        "oracle_point_tri": (f32, [vp, vp, vp]),
+        "oracle_seg_seg": (f32, [vp, vp, vp]),
+        "oracle_accd": (f32, [vp, vp, f32, f32, f32, u32, i32]),
+        "oracle_barrier": (i32, [i32, C.c_double, C.c_double, C.c_double, i32, vp]),
+        "oracle_rayleigh": (f32, [i32, vp, vp, vp, vp, f32]),
+        "oracle_shell": (i32, [i32, vp, vp, C.c_double, C.c_double, C.c_double, vp, vp, vp]),
+        "oracle_hinge": (C.c_double, [i32, vp, vp, vp]),
+        "oracle_stitch": (None, [vp, vp, C.c_double, C.c_double, vp, vp]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+def params_struct(p: dict) -> OracleParams:
+    s = OracleParams()
+    for k, v in p.items():
+        if k == "gravity":
+            s.gravity[:] = list(v)
+        elif hasattr(s, k):
+            setattr(s, k, v)
+    return s
+
+
+class OracleSolver:
+    """The reference's ImplicitSolver restated on the CPU (float) or as the FP64 oracle."""
+
+    def __init__(self, scene: dict, precision: str = "f32"):
+        lib = load()
+        _step_sigs(lib)
+        self.lib = lib
+        sc = scene
+        self.keep = [np.ascontiguousarray(sc[k]) for k in ("positions", "velocities", "inv_mass", "tris",
+                                                          "shell_faces", "stitch_idx", "stitch_w", "stitch_kl",
+                                                          "colliders")]
+        pos, vel, im, tris, sf, si, sw, skl, cols = self.keep
+        mask = sc.get("static_mask")
+        self.mask = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+        self.params = params_struct(sc["params"])
+        self.nv = pos.shape[0]
+        self.h = lib.oracle_solver_new(0 if precision == "f32" else 1, self.nv, _p(pos), _p(vel), _p(im),
+                                       tris.shape[0], _p(tris), _p(self.mask), sf.shape[0], _p(sf), si.shape[0],
+                                       _p(si), _p(sw), _p(skl), cols.shape[0], _p(cols), C.byref(self.params))
+
+    def step(self, n: int = 1, check_intersection: bool = True):
+        out = (OracleStats * n)()
+        self.lib.oracle_solver_step(self.h, n, 1 if check_intersection else 0, out)
+        return [{f: getattr(o, f) for f, _ in OracleStats._fields_} for o in out]
+
+    def positions(self) -> np.ndarray:
+        p = np.empty((self.nv, 3), np.float64)
+        self.lib.oracle_solver_state(self.h, _p(p), None)
+        return p
+
+    def velocities(self) -> np.ndarray:
+        v = np.empty((self.nv, 3), np.float64)
+        self.lib.oracle_solver_state(self.h, None, _p(v))
+        return v
+
+    def set_state(self, pos, vel):
+        p = np.ascontiguousarray(pos, np.float64)
+        v = np.ascontiguousarray(vel, np.float64)
+        self.lib.oracle_solver_set_state(self.h, _p(p), _p(v))
+
+    def counts(self):
+        out = np.zeros(4, np.uint32)
+        self.lib.oracle_solver_counts(self.h, _p(out))
+        return dict(zip(["hinges", "shells", "edges", "collider_tris"], out.tolist()))
+
+    def stencils(self, cap=1 << 20):
+        idx = np.empty((cap, 4), np.uint32)
+        d = np.empty(cap, np.float32)
+        n = self.lib.oracle_solver_stencils(self.h, _p(idx), _p(d), cap)
+        return idx[:min(n, cap)], d[:min(n, cap)]
+
+    def assemble(self, x=None, x_tilde=None):
+        n = 3 * self.nv
+        rhs = np.empty(n, np.float32)
+        xx = None if x is None else np.ascontiguousarray(x, np.float32)
+        xt = None if x_tilde is None else np.ascontiguousarray(x_tilde, np.float32)
+        h = self.lib.oracle_solver_assemble(self.h, _p(xx), _p(xt), _p(rhs))
+        nnz = self.lib.oracle_csr_nnz(h)
+        rp = np.empty(n + 1, np.uint32)
+        ci = np.empty(nnz, np.uint32)
+        vv = np.empty(nnz, np.float32)
+        self.lib.oracle_csr_copy(h, _p(rp), _p(ci), _p(vv))
+        self.lib.oracle_csr_free(h)
+        return (rp, ci, vv), rhs
+
+    def ccd(self, dx):
+        d = np.ascontiguousarray(dx, np.float32)
+        return float(self.lib.oracle_solver_ccd(self.h, _p(d)))
+
+    def close(self):
+        if self.h:
+            self.lib.oracle_solver_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _lib_elem():
+    lib = load()
+    _step_sigs(lib)
+    return lib
+
+
+def point_tri(p4):
+    lib = _lib_elem()
+    p = np.ascontiguousarray(p4, np.float32).reshape(12)
+    g = np.empty(12, np.float32)
+    w = np.empty(3, np.float32)
+    d = lib.oracle_point_tri(_p(p), _p(g), _p(w))
+    return d, g.reshape(4, 3), w
+
+
+def seg_seg(p4):
+    lib = _lib_elem()
+    p = np.ascontiguousarray(p4, np.float32).reshape(12)
+    g = np.empty(12, np.float32)
+    plain = C.c_float()
+    pl = np.empty(1, np.float32)
+    d = lib.oracle_seg_seg(_p(p), _p(g), _p(pl))
+    return d, g.reshape(4, 3), float(pl[0])
+
+
+def accd(x4, dx4, offset=0.0, max_t=1.25, reduction=0.01, max_iter=256, kind="pt"):
+    lib = _lib_elem()
+    x = np.ascontiguousarray(x4, np.float32).reshape(12)
+    d = np.ascontiguousarray(dx4, np.float32).reshape(12)
+    return lib.oracle_accd(_p(x), _p(d), offset, max_t, reduction, max_iter, 0 if kind == "pt" else 1)
+
+
+def barrier(d, dhat, kappa, kind="log", f64=False):
+    lib = _lib_elem()
+    out = np.zeros(3, np.float64)
+    on = lib.oracle_barrier(0 if kind == "log" else 1, d, dhat, kappa, 1 if f64 else 0, _p(out))
+    return (tuple(out.tolist()) if on else None)
+
+
+def rayleigh(elastic, mass, weights, e, offset=0.0):
+    lib = _lib_elem()
+    n = len(mass)
+    el = np.ascontiguousarray(elastic, np.float32).reshape(n * n * 9)
+    m = np.ascontiguousarray(mass, np.float32)
+    w = np.ascontiguousarray(weights, np.float32)
+    ee = np.ascontiguousarray(e, np.float32)
+    return lib.oracle_rayleigh(n, _p(el), _p(m), _p(w), _p(ee), offset)
+
+
+def shell(rest, p, mu, lam, eps=1e-6, f64=True):
+    lib = _lib_elem()
+    r = np.ascontiguousarray(rest, np.float64).reshape(9)
+    q = np.ascontiguousarray(p, np.float64).reshape(9)
+    e = np.zeros(1, np.float64)
+    g = np.zeros(9, np.float64)
+    h = np.zeros(81, np.float64)
+    ok = lib.oracle_shell(1 if f64 else 0, _p(r), _p(q), mu, lam, eps, _p(e), _p(g), _p(h))
+    return (float(e[0]), g.reshape(3, 3), h.reshape(9, 9)) if ok else None
+
+
+def hinge(p4, f64=True):
+    lib = _lib_elem()
+    q = np.ascontiguousarray(p4, np.float64).reshape(12)
+    g = np.zeros(12, np.float64)
+    gf = np.zeros(12, np.float64)
+    th = lib.oracle_hinge(1 if f64 else 0, _p(q), _p(g), _p(gf))
+    return th, g.reshape(4, 3), gf.reshape(4, 3)
+
+
+def stitch(x6, w6, l0, lcap):
+    lib = _lib_elem()
+    x = np.ascontiguousarray(x6, np.float64).reshape(18)
+    w = np.ascontiguousarray(w6, np.float64)
+    g = np.zeros(18, np.float64)
+    h = np.zeros(324, np.float64)
+    lib.oracle_stitch(_p(x), _p(w), l0, lcap, _p(g), _p(h))
+    return g.reshape(6, 3), h.reshape(18, 18)

@@ -1,0 +1,386 @@
+// C entry points over the implicit-step oracle (TEST INFRASTRUCTURE ONLY): whole steps in
+// float (the reference's f32 path) or double (the FP64 oracle), and the element-level
+// functions the reference's unit tests pin (distances, ACCD, barriers, shells, hinges,
+// stitches, Rayleigh stiffness).
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "implicit_oracle.hpp"
+
+using namespace mo;
+
+extern "C" {
+
+// Scene description shared with the CUDA library's mguso_scene_desc (same field meaning).
+struct OracleParams {
+  float dt, gravity[3];
+  uint32_t newton_iters;
+  float stiffness, bend_stiffness, max_dx, target_toi;
+  uint32_t min_newton_steps, ccd_max_iter;
+  float eiganalysis_eps, contact_dhat, contact_kappa, contact_dynamic;
+  float shell_mu, shell_lambda, friction, friction_eps;
+  int barrier_kind, contact_rayleigh, self_collision;
+  float cg_tol;
+  uint32_t cg_max_iter;
+  float floor_y, newton_tol;
+  int precond;
+  uint32_t schwarz_domain;
+};
+
+struct OracleStats {
+  uint32_t newton_iters, max_cg_iters, num_contacts, stencils, ccd_cap_hits;
+  double max_reresid, t_min;
+  int penetration_free, all_finite;
+};
+
+}  // extern "C"
+
+namespace {
+
+struct AnySolver {
+  int prec;  // 0 float, 1 double
+  std::unique_ptr<ImplicitSolver<float>> f;
+  std::unique_ptr<ImplicitSolver<double>> d;
+};
+
+template <class R>
+std::unique_ptr<ImplicitSolver<R>> make_solver(uint32_t nv, const float* pos, const float* vel, const float* inv_mass,
+                                               uint32_t nt, const uint32_t* tris, const uint8_t* static_mask,
+                                               uint32_t nshell, const uint32_t* shell_faces, uint32_t nstitch,
+                                               const uint32_t* st_idx, const float* st_w, const float* st_kl,
+                                               uint32_t ncol, const float* cols, const OracleParams* p) {
+  auto s = std::make_unique<ImplicitSolver<R>>();
+  std::vector<Vt<R>> P(nv), Vv(nv);
+  std::vector<R> im(nv);
+  for (uint32_t i = 0; i < nv; ++i) {
+    P[i] = Vt<R>(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+    Vv[i] = vel ? Vt<R>(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]) : Vt<R>();
+    im[i] = inv_mass[i];
+  }
+  std::vector<std::array<uint32_t, 3>> T(nt);
+  for (uint32_t t = 0; t < nt; ++t) T[t] = {tris[3 * t], tris[3 * t + 1], tris[3 * t + 2]};
+  Params<R> q;
+  q.dt = p->dt;
+  q.gravity = Vt<R>(p->gravity[0], p->gravity[1], p->gravity[2]);
+  q.newton_iters = p->newton_iters;
+  q.stiffness = p->stiffness;
+  q.bend_stiffness = p->bend_stiffness;
+  q.max_dx = p->max_dx;
+  q.target_toi = p->target_toi;
+  q.min_newton_steps = p->min_newton_steps;
+  q.ccd_max_iter = p->ccd_max_iter;
+  q.eiganalysis_eps = p->eiganalysis_eps;
+  q.contact_dhat = p->contact_dhat;
+  q.contact_kappa = p->contact_kappa;
+  q.contact_dynamic = p->contact_dynamic;
+  q.shell_mu = p->shell_mu;
+  q.shell_lambda = p->shell_lambda;
+  q.friction = p->friction;
+  q.friction_eps = p->friction_eps;
+  q.barrier_kind = (BarrierKind)p->barrier_kind;
+  q.contact_rayleigh = p->contact_rayleigh != 0;
+  q.self_collision = p->self_collision != 0;
+  q.cg_tol = p->cg_tol;
+  q.cg_max_iter = p->cg_max_iter;
+  q.floor_y = p->floor_y;
+  q.newton_tol = p->newton_tol;
+  q.precond = p->precond;
+  q.schwarz_domain = p->schwarz_domain;
+  s->init(P, Vv, im, T, q);
+  std::vector<std::array<uint32_t, 3>> SF(nshell);
+  for (uint32_t i = 0; i < nshell; ++i) SF[i] = {shell_faces[3 * i], shell_faces[3 * i + 1], shell_faces[3 * i + 2]};
+  s->set_shell_faces(SF);
+  for (uint32_t i = 0; i < nstitch; ++i) {
+    Stitch<R> st;
+    for (int k = 0; k < 6; ++k) {
+      st.index[k] = st_idx[6 * i + k];
+      st.weight[k] = st_w[6 * i + k];
+    }
+    st.stiffness = st_kl[3 * i];
+    st.l0 = st_kl[3 * i + 1];
+    st.l_cap = st_kl[3 * i + 2];
+    s->stitches.push_back(st);
+  }
+  for (uint32_t i = 0; i < ncol; ++i) {
+    const float* c = cols + 8 * i;
+    Collider<R> col;
+    col.kind = (int)c[0];
+    col.a = Vt<R>(c[1], c[2], c[3]);
+    col.n = Vt<R>(c[4], c[5], c[6]);
+    col.radius = c[7];
+    s->colliders.push_back(col);
+  }
+  if (static_mask) s->set_static_collider_verts(std::vector<uint8_t>(static_mask, static_mask + nv));
+  return s;
+}
+
+template <class R>
+void fill_stats(const StepStats& s, OracleStats* o) {
+  o->newton_iters = s.newton_iters;
+  o->max_cg_iters = s.max_cg_iters;
+  o->num_contacts = s.num_contacts;
+  o->stencils = s.stencils;
+  o->ccd_cap_hits = s.ccd_cap_hits;
+  o->max_reresid = s.max_reresid;
+  o->t_min = s.t_min;
+  o->penetration_free = s.penetration_free;
+  o->all_finite = s.all_finite;
+}
+
+// StVK shell element built from rest positions; returns 0 if the rest triangle is degenerate.
+template <class R>
+int shell_eval(const double* rest9, const double* p9, double mu, double lambda, double eps, double* energy,
+                      double* grad9, double* hess81) {
+  ShellEl<R> el;
+  Vt<R> r[3], p[3];
+  for (int k = 0; k < 3; ++k) {
+    r[k] = Vt<R>((R)rest9[3 * k], (R)rest9[3 * k + 1], (R)rest9[3 * k + 2]);
+    p[k] = Vt<R>((R)p9[3 * k], (R)p9[3 * k + 1], (R)p9[3 * k + 2]);
+  }
+  if (!build_shell(r[0], r[1], r[2], R(1.0e-12), el)) return 0;
+  Vt<R> g[3];
+  shell_gradient(p, el, (R)mu, (R)lambda, g);
+  R h[81];
+  shell_hessian(p, el, (R)mu, (R)lambda, (R)eps, h);
+  *energy = shell_energy(p, el, (R)mu, (R)lambda);
+  for (int k = 0; k < 3; ++k)
+    for (int c = 0; c < 3; ++c) grad9[3 * k + c] = g[k][c];
+  for (int k = 0; k < 81; ++k) hess81[k] = h[k];
+  return 1;
+}
+
+}  // namespace
+
+extern "C" {
+
+void* oracle_solver_new(int precision, uint32_t nv, const float* pos, const float* vel, const float* inv_mass,
+                        uint32_t nt, const uint32_t* tris, const uint8_t* static_mask, uint32_t nshell,
+                        const uint32_t* shell_faces, uint32_t nstitch, const uint32_t* st_idx, const float* st_w,
+                        const float* st_kl, uint32_t ncol, const float* cols, const OracleParams* p) {
+  auto* a = new AnySolver();
+  a->prec = precision;
+  if (precision == 0)
+    a->f = make_solver<float>(nv, pos, vel, inv_mass, nt, tris, static_mask, nshell, shell_faces, nstitch, st_idx,
+                              st_w, st_kl, ncol, cols, p);
+  else
+    a->d = make_solver<double>(nv, pos, vel, inv_mass, nt, tris, static_mask, nshell, shell_faces, nstitch, st_idx,
+                               st_w, st_kl, ncol, cols, p);
+  return a;
+}
+
+void oracle_solver_free(void* h) { delete (AnySolver*)h; }
+
+int oracle_solver_step(void* h, int nsteps, int check_intersection, OracleStats* out) {
+  auto* a = (AnySolver*)h;
+  for (int k = 0; k < nsteps; ++k) {
+    if (a->prec == 0) {
+      StepStats s = a->f->step(check_intersection != 0);
+      if (out) fill_stats<float>(s, out + k);
+    } else {
+      StepStats s = a->d->step(check_intersection != 0);
+      if (out) fill_stats<double>(s, out + k);
+    }
+  }
+  return 0;
+}
+
+// positions / velocities as f64 (whichever precision the solver runs in)
+void oracle_solver_state(void* h, double* pos, double* vel) {
+  auto* a = (AnySolver*)h;
+  size_t n = a->prec == 0 ? a->f->positions.size() : a->d->positions.size();
+  for (size_t i = 0; i < n; ++i)
+    for (int c = 0; c < 3; ++c) {
+      if (a->prec == 0) {
+        if (pos) pos[3 * i + c] = a->f->positions[i][c];
+        if (vel) vel[3 * i + c] = a->f->velocities[i][c];
+      } else {
+        if (pos) pos[3 * i + c] = a->d->positions[i][c];
+        if (vel) vel[3 * i + c] = a->d->velocities[i][c];
+      }
+    }
+}
+
+void oracle_solver_set_state(void* h, const double* pos, const double* vel) {
+  auto* a = (AnySolver*)h;
+  size_t n = a->prec == 0 ? a->f->positions.size() : a->d->positions.size();
+  for (size_t i = 0; i < n; ++i)
+    for (int c = 0; c < 3; ++c) {
+      if (a->prec == 0) {
+        if (pos) a->f->positions[i][c] = (float)pos[3 * i + c];
+        if (vel) a->f->velocities[i][c] = (float)vel[3 * i + c];
+      } else {
+        if (pos) a->d->positions[i][c] = pos[3 * i + c];
+        if (vel) a->d->velocities[i][c] = vel[3 * i + c];
+      }
+    }
+}
+
+// Element counts: hinges, shells, edges, exclusion entries.
+void oracle_solver_counts(void* h, uint32_t* out4) {
+  auto* a = (AnySolver*)h;
+  if (a->prec == 0) {
+    out4[0] = (uint32_t)a->f->hinges.size();
+    out4[1] = (uint32_t)a->f->shells.size();
+    out4[2] = (uint32_t)a->f->edges.size();
+    out4[3] = (uint32_t)a->f->collider_tris.size();
+  } else {
+    out4[0] = (uint32_t)a->d->hinges.size();
+    out4[1] = (uint32_t)a->d->shells.size();
+    out4[2] = (uint32_t)a->d->edges.size();
+    out4[3] = (uint32_t)a->d->collider_tris.size();
+  }
+}
+
+// Active self-contact stencils at the current positions: idx u32[4*cap], d f32[cap].
+uint32_t oracle_solver_stencils(void* h, uint32_t* idx, float* d, uint32_t cap) {
+  auto* a = (AnySolver*)h;
+  if (a->prec != 0) return 0;
+  auto st = a->f->self_collision_stencils(a->f->positions);
+  for (size_t i = 0; i < st.size() && i < cap; ++i) {
+    for (int k = 0; k < 4; ++k) idx[4 * i + k] = st[i].idx[k];
+    d[i] = st[i].d;
+  }
+  return (uint32_t)st.size();
+}
+
+// One assembly at the current positions (x = x_tilde = positions unless given):
+// returns the scalar CSR through the oracle_csr_* handle API and rhs f32[3n].
+void* oracle_solver_assemble(void* h, const float* x_in, const float* xt_in, float* rhs_out) {
+  auto* a = (AnySolver*)h;
+  auto& s = *a->f;
+  size_t n = s.positions.size();
+  std::vector<Vt<float>> x = s.positions, xt = s.positions;
+  for (size_t i = 0; i < n; ++i) {
+    if (x_in) x[i] = Vt<float>(x_in[3 * i], x_in[3 * i + 1], x_in[3 * i + 2]);
+    if (xt_in) xt[i] = Vt<float>(xt_in[3 * i], xt_in[3 * i + 1], xt_in[3 * i + 2]);
+  }
+  float h2 = s.params.dt * s.params.dt;
+  std::vector<float> rhs;
+  auto* m = new Csr(s.assemble(x, xt, 1.0f / h2, rhs, nullptr));
+  std::memcpy(rhs_out, rhs.data(), 4 * rhs.size());
+  return m;
+}
+
+// CCD step fraction for the current positions and a search direction dx f32[3n].
+float oracle_solver_ccd(void* h, const float* dx_in) {
+  auto* a = (AnySolver*)h;
+  auto& s = *a->f;
+  size_t n = s.positions.size();
+  std::vector<Vt<float>> dx(n);
+  for (size_t i = 0; i < n; ++i) dx[i] = Vt<float>(dx_in[3 * i], dx_in[3 * i + 1], dx_in[3 * i + 2]);
+  uint32_t caps = 0;
+  return s.ccd_max_step(s.positions, dx, &caps);
+}
+
+// ---- element-level functions (float) --------------------------------------------------
+float oracle_point_tri(const float* p12, float* g12, float* bary3) {
+  Vt<float> p[4];
+  for (int k = 0; k < 4; ++k) p[k] = Vt<float>(p12[3 * k], p12[3 * k + 1], p12[3 * k + 2]);
+  Vt<float> g[4];
+  float d = point_tri_distance_grad(p[0], p[1], p[2], p[3], g);
+  for (int k = 0; k < 4; ++k)
+    for (int c = 0; c < 3; ++c) g12[3 * k + c] = g[k][c];
+  float w[3];
+  closest_point_bary(p[0], p[1], p[2], p[3], w);
+  for (int k = 0; k < 3; ++k) bary3[k] = w[k];
+  return d;
+}
+
+float oracle_seg_seg(const float* p12, float* g12, float* plain) {
+  Vt<float> p[4];
+  for (int k = 0; k < 4; ++k) p[k] = Vt<float>(p12[3 * k], p12[3 * k + 1], p12[3 * k + 2]);
+  Vt<float> g[4];
+  float d = segment_segment_distance_grad(p[0], p[1], p[2], p[3], g);
+  for (int k = 0; k < 4; ++k)
+    for (int c = 0; c < 3; ++c) g12[3 * k + c] = g[k][c];
+  *plain = segment_segment_distance(p[0], p[1], p[2], p[3]);
+  return d;
+}
+
+// kind 0 = point-triangle, 1 = edge-edge
+float oracle_accd(const float* x12, const float* dx12, float offset, float max_t, float reduction, uint32_t max_iter,
+                  int kind) {
+  Vt<float> x0[4], dx[4];
+  for (int k = 0; k < 4; ++k) {
+    x0[k] = Vt<float>(x12[3 * k], x12[3 * k + 1], x12[3 * k + 2]);
+    dx[k] = Vt<float>(dx12[3 * k], dx12[3 * k + 1], dx12[3 * k + 2]);
+  }
+  if (kind == 0)
+    return accd_toi<float>(x0, dx, offset, max_t, reduction, max_iter, [](const Vt<float>* p) {
+      float d = point_triangle_distance(p[0], p[1], p[2], p[3]);
+      return d * d;
+    });
+  return accd_toi<float>(x0, dx, offset, max_t, reduction, max_iter, [](const Vt<float>* p) {
+    float d = segment_segment_distance(p[0], p[1], p[2], p[3]);
+    return d * d;
+  });
+}
+
+int oracle_barrier(int kind, double d, double dhat, double kappa, int f64, double* egh) {
+  if (f64) {
+    double e, g, h;
+    bool on = barrier_of<double>((BarrierKind)kind, d, dhat, kappa, e, g, h);
+    egh[0] = e; egh[1] = g; egh[2] = h;
+    return on;
+  }
+  float e, g, h;
+  bool on = barrier_of<float>((BarrierKind)kind, (float)d, (float)dhat, (float)kappa, e, g, h);
+  egh[0] = e; egh[1] = g; egh[2] = h;
+  return on;
+}
+
+float oracle_rayleigh(int n, const float* elastic, const float* mass, const float* weights, const float* e3,
+                      float offset) {
+  float el[16][9];
+  for (int i = 0; i < n * n; ++i)
+    for (int q = 0; q < 9; ++q) el[i][q] = elastic[9 * i + q];
+  return rayleigh_stiffness<float>(el, mass, weights, n, Vt<float>(e3[0], e3[1], e3[2]), offset);
+}
+
+int oracle_shell(int f64, const double* rest9, const double* p9, double mu, double lambda, double eps, double* energy,
+                 double* grad9, double* hess81) {
+  return f64 ? shell_eval<double>(rest9, p9, mu, lambda, eps, energy, grad9, hess81)
+             : shell_eval<float>(rest9, p9, mu, lambda, eps, energy, grad9, hess81);
+}
+
+double oracle_hinge(int f64, const double* p12, double* grad12, double* grad_fd12) {
+  if (f64) {
+    Vt<double> p[4], g[4], gf[4];
+    for (int k = 0; k < 4; ++k) p[k] = Vt<double>(p12[3 * k], p12[3 * k + 1], p12[3 * k + 2]);
+    dihedral_grad(p, g);
+    dihedral_grad_fd(p, gf);
+    for (int k = 0; k < 4; ++k)
+      for (int c = 0; c < 3; ++c) {
+        grad12[3 * k + c] = g[k][c];
+        grad_fd12[3 * k + c] = gf[k][c];
+      }
+    return dihedral_angle(p);
+  }
+  Vt<float> p[4], g[4], gf[4];
+  for (int k = 0; k < 4; ++k) p[k] = Vt<float>((float)p12[3 * k], (float)p12[3 * k + 1], (float)p12[3 * k + 2]);
+  dihedral_grad(p, g);
+  dihedral_grad_fd(p, gf);
+  for (int k = 0; k < 4; ++k)
+    for (int c = 0; c < 3; ++c) {
+      grad12[3 * k + c] = g[k][c];
+      grad_fd12[3 * k + c] = gf[k][c];
+    }
+  return dihedral_angle(p);
+}
+
+void oracle_stitch(const double* x18, const double* w6, double l0, double lcap, double* grad18, double* hess324) {
+  Vt<double> x[6], g[6];
+  double w[6];
+  for (int k = 0; k < 6; ++k) {
+    x[k] = Vt<double>(x18[3 * k], x18[3 * k + 1], x18[3 * k + 2]);
+    w[k] = w6[k];
+  }
+  stitch_force_hessian(x, w, l0, lcap, g, hess324);
+  for (int k = 0; k < 6; ++k)
+    for (int c = 0; c < 3; ++c) grad18[3 * k + c] = g[k][c];
+}
+
+}  // extern "C"

@@ -20,7 +20,7 @@ def small_grid(n=12, seed=5):
     return nb, rp, col, val, N, srp, sci, svv
 
 
-@pytest.mark.parametrize("variant", [1, 2])
+@pytest.mark.parametrize("variant", [1, 2, 3])
 def test_spmv_matches_oracle_small(ctx, variant):
     nb, rp, col, val, N, srp, sci, svv = small_grid(37)
     a = Bsr(ctx, nb, rp, col, val)
@@ -57,7 +57,7 @@ def test_spmv_edge_cases(ctx):
     x = np.random.default_rng(2).standard_normal(3 * nb).astype(np.float32)
     want = scenes.bsr_spmv_f64(rp, col, val, x)
     bound = scenes.bsr_spmv_f64(rp, col, np.abs(val), np.abs(x))
-    for variant in (1, 2):
+    for variant in (1, 2, 3):
         a.set_kernel(variant)
         assert np.all(np.abs(a.spmv_host(x) - want) <= 1e-5 * bound + 1e-30)
 

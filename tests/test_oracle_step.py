@@ -1,0 +1,253 @@
+"""Pins the implicit-step oracle against the reference's own unit tests
+(engine-core/src/contact.rs, shell_model.rs, bending.rs, stitch.rs, implicit.rs tests)."""
+import numpy as np
+import oracle_py as O
+import pytest
+
+from mguso import scenes
+
+
+def fd(pts, f, h=1e-3):
+    pts = np.array(pts, np.float64)
+    g = np.zeros_like(pts)
+    for i in range(pts.shape[0]):
+        for c in range(3):
+            pp, pm = pts.copy(), pts.copy()
+            pp[i, c] += h
+            pm[i, c] -= h
+            g[i, c] = (f(pp) - f(pm)) / (2 * h)
+    return g
+
+
+def pt_dist(q):
+    return O.point_tri(q)[0]
+
+
+def test_point_triangle_gradient_matches_fd_in_every_branch():  # contact.rs:1238-1268
+    a, b, c = (0, 0, 0), (1, 0, 0), (0, 1, 0)
+    for p in [(0.25, 0.25, 0.4), (0.5, -0.3, 0.3), (-0.3, 0.5, 0.3), (0.8, 0.8, 0.3), (-0.4, -0.4, 0.2),
+              (1.6, -0.4, 0.2), (-0.4, 1.6, 0.2)]:
+        pts = [p, a, b, c]
+        d, g, _ = O.point_tri(pts)
+        assert d > 0.05
+        want = fd(pts, pt_dist)
+        assert np.abs(g - want).max() < 2e-3
+        assert abs(np.linalg.norm(g[0]) - 1.0) < 1e-4
+
+
+def test_closest_point_weights_are_a_partition_of_unity():  # contact.rs:1271-1303
+    rng = np.random.default_rng(1)
+    for _ in range(200):
+        pts = rng.uniform(-1, 1, (4, 3))
+        _, _, w = O.point_tri(pts)
+        assert abs(w.sum() - 1.0) < 1e-5 and np.all(w >= -1e-6)
+
+
+def test_segment_gradient_matches_fd():  # contact.rs:1356-1404
+    cases = [[(-1, 0, 0), (1, 0, 0), (0, 0.5, -1), (0, 0.5, 1)],
+             [(0, 0, 0), (1, 0, 0), (2, 0.6, -1), (2, 0.6, 1)],
+             [(0, 0, 0), (1, 0, 0), (2, 0.7, 0), (3, 0.7, 0)]]
+    for pts in cases:
+        d, g, plain = O.seg_seg(pts)
+        assert d > 0.05 and abs(d - plain) < 1e-5
+        want = fd(pts, lambda q: O.seg_seg(q)[2])
+        assert np.abs(g - want).max() < 2e-3
+
+
+def test_distance_known_answers():  # contact.rs:1800-1814, 1935-1969
+    a, b, c = (0, 0, 0), (1, 0, 0), (0, 1, 0)
+    assert abs(O.point_tri([(0.25, 0.25, 0.7), a, b, c])[0] - 0.7) < 1e-5
+    assert abs(O.point_tri([(-1, -1, 0), a, b, c])[0] - np.sqrt(2)) < 1e-5
+    assert abs(O.point_tri([(0.5, -0.3, 0), a, b, c])[0] - 0.3) < 1e-5
+    assert O.seg_seg([(-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0)])[2] < 1e-5
+
+
+def test_accd_edge_through_edge():  # contact.rs:1971-1996
+    x0 = [(-1, 0.5, 0), (1, 0.5, 0), (0, 0, -1), (0, 0, 1)]
+    dx = [(0, -2, 0), (0, -2, 0), (0, 0, 0), (0, 0, 0)]
+    toi = O.accd(x0, dx, kind="ee")
+    assert toi < 1.25
+    m = np.array(x0, np.float32)
+    m[:2] += np.array(dx[:2], np.float32) * np.float32(toi)
+    assert O.seg_seg(m)[2] > 0
+
+
+def test_accd_point_into_triangle():  # contact.rs:1998-2025
+    x0 = [(0.25, 0.25, 1.0), (0, 0, 0), (1, 0, 0), (0, 1, 0)]
+    dx = [(0, 0, -2), (0, 0, 0), (0, 0, 0), (0, 0, 0)]
+    toi = O.accd(x0, dx)
+    assert 0.40 <= toi < 0.55
+    moved = np.array(x0, np.float32)
+    moved[0] += np.array(dx[0], np.float32) * np.float32(toi)
+    assert O.point_tri(moved)[0] > 0
+
+
+def test_accd_no_relative_motion():  # contact.rs:2027-2043
+    x0 = [(0.25, 0.25, 1.0), (0, 0, 0), (1, 0, 0), (0, 1, 0)]
+    v = (0, 0, -5)
+    assert O.accd(x0, [v] * 4) == np.float32(1.25)
+
+
+def test_rayleigh_reduces_to_inertial_term():  # contact.rs:1664-1696
+    e = np.array([0, 0.03, 0], np.float32)
+    g = 0.03
+    for n in (2, 3, 4):
+        w = np.full(n, 1.0 / (n - 1), np.float32)
+        w[0] = -1.0
+        k = O.rayleigh(np.zeros((n * n, 9)), np.full(n, 0.7), w, e)
+        assert abs(k - 0.7 / g ** 2) < 1e-3 * 0.7 / g ** 2
+    w = np.array([-1, 1], np.float32)
+    far = O.rayleigh(np.zeros((4, 9)), [0.7, 0.7], w, e)
+    near = O.rayleigh(np.zeros((4, 9)), [0.7, 0.7], w, e * 0.5)
+    assert abs(near / far - 4.0) < 1e-2
+
+
+def test_rayleigh_substitutes_static_side_mass():  # contact.rs:1698-1722
+    e = np.array([0, 0.04, 0], np.float32)
+    w = np.array([-1, 1], np.float32)
+    both = O.rayleigh(np.zeros((4, 9)), [0.9, 0.9], w, e)
+    one = O.rayleigh(np.zeros((4, 9)), [0.9, 0.0], w, e)
+    assert abs(both - one) < 1e-4 * both
+
+
+def test_log_barrier_is_c2_at_dhat_and_blows_up_near_zero():  # contact.rs:1784-1798
+    assert O.barrier(0.1, 0.1, 1.0) is None and O.barrier(0.2, 0.1, 1.0) is None
+    e_edge, g_edge, _ = O.barrier(0.0999, 0.1, 1.0)
+    assert 0 < e_edge < 1e-3 and abs(g_edge) < 1e-2
+    e_near, g_near, _ = O.barrier(1e-4, 0.1, 1.0)
+    assert e_near > 100 * e_edge and g_near < 0
+
+
+def test_cubic_barrier_derivatives_match_fd():  # contact.rs:1591-1630
+    for gap in (-0.02, 0.0, 0.03, 0.07):
+        e, g, h = O.barrier(gap, 0.1, 2.0, kind="cubic", f64=True)
+        hh = 1e-6
+        ep = O.barrier(gap + hh, 0.1, 2.0, kind="cubic", f64=True)
+        em = O.barrier(gap - hh, 0.1, 2.0, kind="cubic", f64=True)
+        assert abs((ep[0] - em[0]) / (2 * hh) - g) < 1e-5 * max(1, abs(g))
+        assert abs((ep[1] - em[1]) / (2 * hh) - h) < 1e-4 * max(1, abs(h))
+        assert g < 0 and h > 0
+
+
+def test_stvk_shell_gradient_matches_fd_and_hessian_is_psd():  # shell_model.rs:1077-1250
+    rng = np.random.default_rng(3)
+    rest = np.array([[0, 0, 0], [1, 0, 0], [0.2, 0.9, 0]], np.float64)
+    mu, lam = scenes.lame_from_young_poisson(1e5 * 5e-4, 0.3)
+    for _ in range(10):
+        p = rest @ np.diag([1.3, 0.8, 1.0]) + rng.normal(0, 0.05, (3, 3))
+        e, g, h = O.shell(rest, p, mu, lam)
+        want = fd(p, lambda q: O.shell(rest, q, mu, lam)[0], h=1e-6)
+        assert np.abs(g - want).max() < 1e-5 * max(1.0, np.abs(want).max())
+        assert np.abs(h - h.T).max() < 1e-9 * max(1.0, np.abs(h).max())
+        assert np.linalg.eigvalsh(h).min() > -1e-9 * max(1.0, np.abs(h).max())
+    # rest state: zero energy and gradient
+    e, g, _ = O.shell(rest, rest, mu, lam)
+    assert abs(e) < 1e-12 and np.abs(g).max() < 1e-9
+
+
+def test_hinge_analytic_gradient_matches_fd():  # bending.rs:228-260
+    rng = np.random.default_rng(5)
+    for _ in range(20):
+        p = np.array([[0, 1, 0], [0, 0, 0], [1, 0, 0], [0.5, -1, 0.3]], np.float64) + rng.normal(0, 0.1, (4, 3))
+        th, g, gf = O.hinge(p)
+        assert np.abs(g - gf).max() < 1e-4 * max(1.0, np.abs(gf).max())
+        assert np.abs(g.sum(0)).max() < 1e-9
+
+
+def test_flat_hinge_reads_zero():  # bending.rs:27-48
+    p = np.array([[0, 1, 0], [0, 0, 0], [1, 0, 0], [0.5, -1, 0]], np.float64)
+    th, _, _ = O.hinge(p)
+    assert abs(th) < 1e-12
+    q = np.array([[0, 1, 0], [0, 0, 0], [1, 0, 0], [1, 1, 0]], np.float64)  # folded shut
+    assert abs(abs(O.hinge(q)[0]) - np.pi) < 1e-12
+
+
+def test_stitch_gradient_matches_fd_and_hessian_is_psd():  # stitch.rs:138-230
+    rng = np.random.default_rng(7)
+    w = np.array([0.2, 0.3, 0.5, 0.6, 0.4, 0.0])
+    l0, lcap = 1e-3, 0.05
+    for _ in range(10):
+        x = rng.normal(0, 0.01, (6, 3))
+        x[3:] += 0.02
+
+        def energy(q):
+            t = (w[:3, None] * q[:3]).sum(0) - (w[3:, None] * q[3:]).sum(0)
+            e = np.linalg.norm(t) - l0
+            return 0.5 * e * e / l0
+
+        g, h = O.stitch(x, w, l0, lcap)
+        want = fd(x, energy, h=1e-7)
+        assert np.abs(g - want).max() < 1e-5 * max(1.0, np.abs(want).max())
+        assert np.linalg.eigvalsh(0.5 * (h + h.T)).min() > -1e-9
+
+
+def small_sheet(n=12, **kw):
+    return scenes.sheet_on_sphere(n, side=0.4, **kw)
+
+
+def test_cloth_drapes_over_sphere_without_penetration():  # implicit.rs:4595-4632
+    sc = small_sheet(12, height=0.33)
+    s = O.OracleSolver(sc)
+    stats = s.step(20)
+    p = s.positions()
+    assert all(st["all_finite"] and st["penetration_free"] for st in stats)
+    r = np.linalg.norm(p, axis=1)
+    assert r.min() >= 0.3 - 1e-3 * 1e-3 - 1e-6
+    assert p[:, 1].min() < 0.33 - 0.01  # it fell
+
+
+def test_implicit_is_deterministic():  # implicit.rs:4929-4949
+    sc = small_sheet(10)
+    a, b = O.OracleSolver(sc), O.OracleSolver(sc)
+    a.step(6)
+    b.step(6)
+    assert np.array_equal(a.positions(), b.positions())
+
+
+def test_f64_oracle_tracks_f32_oracle():
+    sc = small_sheet(10)
+    a, b = O.OracleSolver(sc, "f32"), O.OracleSolver(sc, "f64")
+    for _ in range(8):
+        a.step(1)
+        b.step(1)
+    pa, pb = a.positions(), b.positions()
+    assert np.abs(pa - pb).max() < 1e-3 * np.abs(pb).max()
+
+
+def test_self_contact_stencils_are_exact_predicate():
+    """Stencils = every (v, t) with 1-ring excluded and d < dhat, plus every edge pair with
+    no shared vertex and d < dhat (implicit.rs:678-753), independent of the hash grid."""
+    rng = np.random.default_rng(2)
+    n = 6
+    sc = scenes.sheet_on_sphere(n, side=0.05, jitter=0.0, dhat=5e-3)
+    # fold a second layer just above the first
+    pos = sc["positions"].copy()
+    top = pos.copy()
+    top[:, 1] += 2e-3
+    top += rng.uniform(-5e-4, 5e-4, top.shape).astype(np.float32)
+    sc["positions"] = np.concatenate([pos, top]).astype(np.float32)
+    sc["velocities"] = np.zeros_like(sc["positions"])
+    sc["tris"] = np.concatenate([sc["tris"], sc["tris"] + n * n]).astype(np.uint32)
+    sc["shell_faces"] = sc["tris"].copy()
+    sc["inv_mass"] = np.concatenate([sc["inv_mass"], sc["inv_mass"]])
+    s = O.OracleSolver(sc)
+    idx, d = s.stencils()
+    P = sc["positions"]
+    T = sc["tris"]
+    dh = np.float32(5e-3)
+    ring = [set() for _ in range(P.shape[0])]
+    for t in T:
+        for a in t:
+            ring[a] |= set(int(x) for x in t)
+    want_vt = set()
+    for v in range(P.shape[0]):
+        for ti, t in enumerate(T):
+            if ring[v] & set(int(x) for x in t) or v in t:
+                continue
+            dd, _, _ = O.point_tri([P[v], P[t[0]], P[t[1]], P[t[2]]])
+            if dd < dh:
+                want_vt.add((v, int(t[0]), int(t[1]), int(t[2])))
+    got = set(map(tuple, idx.tolist()))
+    got_vt = {g for g in got if any(g == w for w in want_vt) or (g[0], g[1], g[2], g[3]) in want_vt}
+    assert want_vt <= got
+    assert len(got) > len(want_vt)  # edge-edge stencils too
