@@ -164,6 +164,92 @@ int mguso_lbvh_build_query(mguso_ctx* ctx, const float* positions, uint32_t nv, 
  * (radix.rs:112-352), which is limited to 65 536 keys. */
 int mguso_radix_sort_pairs(mguso_ctx* ctx, void* keys, uint32_t* vals, uint32_t n, int key_bits, void* stream);
 
+/* ---- Implicit step: scene build -> step -> readback --------------------------------- */
+/* Solver knobs, named and defaulted as ImplicitParams (implicit.rs:30-229). Fields that
+ * the reference does not have: newton_tol (Newton stops once the largest per-vertex step
+ * actually taken is below it, 0 = off), precond/schwarz_domain (the LinearSolver choice)
+ * and precision (MGUSO_PRECISION_FP32, or MIXED = FP64 PCG dots and norms, FP64 contact
+ * distances/barriers and FP64 CCD root solves). barrier_kind: 0 log, 1 cubic. */
+typedef struct {
+  float dt;
+  float gravity[3];
+  uint32_t newton_iters;
+  float stiffness;      /* stretch-spring k on the unique mesh edges */
+  float bend_stiffness; /* hinge k_b (hinge weight w = 1) */
+  float max_dx;         /* search-direction cap (INFINITY = off) */
+  float target_toi;
+  uint32_t min_newton_steps;
+  uint32_t ccd_max_iter;
+  float eiganalysis_eps;
+  float contact_dhat;
+  float contact_kappa;
+  float contact_dynamic;
+  float shell_mu;
+  float shell_lambda;
+  float friction;
+  float friction_eps;
+  int barrier_kind;
+  int contact_rayleigh;
+  int self_collision;
+  float cg_tol;
+  uint32_t cg_max_iter;
+  float floor_y; /* -INFINITY = off */
+  float newton_tol;
+  int precond;
+  uint32_t schwarz_domain;
+  int precision;
+} mguso_params;
+
+/* One scene (Scene::build_implicit + the set_* calls of implicit.rs). All pointers host;
+ * they are copied, the caller keeps ownership. */
+typedef struct {
+  uint32_t nv;
+  const float* positions;   /* f32[3*nv] */
+  const float* velocities;  /* f32[3*nv] or NULL (zero) */
+  const float* inv_mass;    /* f32[nv]; 0 = pinned / static */
+  uint32_t nt;
+  const uint32_t* tris;     /* u32[3*nt]: every triangle (cloth and bodies): hinges, springs and collision */
+  const uint8_t* static_mask; /* u8[nv] static mesh collider vertices, or NULL (set_static_collider_verts) */
+  uint32_t nshell;
+  const uint32_t* shell_faces; /* u32[3*nshell] StVK shell faces (set_shell_faces) */
+  uint32_t nstitch;
+  const uint32_t* stitch_idx;  /* u32[6*nstitch] (Stitch::index) */
+  const float* stitch_w;       /* f32[6*nstitch] (Stitch::weight) */
+  const float* stitch_kl;      /* f32[3*nstitch]: stiffness, l0, l_cap */
+  uint32_t ncollider;
+  const float* colliders;      /* f32[8*ncollider]: kind (0 half-space, 1 sphere), point/center xyz,
+                                  normal xyz, radius (Collider, contact.rs:21-31) */
+  mguso_params params;
+} mguso_scene_desc;
+
+typedef struct {
+  uint32_t newton_iters;
+  uint32_t max_cg_iters;
+  uint32_t num_contacts;   /* free vertices within dhat of an analytic collider */
+  uint32_t stencils;       /* largest active self-contact stencil count over the Newton iterations */
+  uint32_t ccd_cap_hits;   /* CCD root solves that hit ccd_max_iter */
+  double max_reresid;
+  double t_min;            /* smallest CCD step fraction of the step */
+  int penetration_free;
+  int all_finite;
+  int status;              /* MGUSO_OK, MGUSO_ERR_NONFINITE (step rejected), ... */
+} mguso_step_stats;
+
+typedef struct mguso_scene mguso_scene;
+int mguso_scene_create(mguso_ctx* ctx, const mguso_scene_desc* desc, mguso_scene** out);
+int mguso_scene_destroy(mguso_scene* s);
+/* Advances nsteps implicit steps (ImplicitSolver::step, implicit.rs:1951-2191). stats has
+ * nsteps entries or is NULL. A non-finite step is rejected exactly as the reference does
+ * (positions kept, velocities zeroed) and reported as MGUSO_ERR_NONFINITE in its stats. */
+int mguso_step(mguso_scene* s, int nsteps, mguso_step_stats* stats);
+int mguso_read_positions(mguso_scene* s, float* out);   /* f32[3*nv] host */
+int mguso_write_positions(mguso_scene* s, const float* in);
+int mguso_read_velocities(mguso_scene* s, float* out);
+int mguso_write_velocities(mguso_scene* s, const float* in);
+/* Element counts: hinges, shells, unique edges, static collider triangles,
+ * system blocks (free-free pattern), pinned-pattern blocks. */
+int mguso_scene_info(mguso_scene* s, uint32_t* out6);
+
 #ifdef __cplusplus
 }
 #endif

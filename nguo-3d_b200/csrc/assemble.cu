@@ -1,0 +1,747 @@
+// Hessian and gradient assembly of the implicit step on the GPU
+// (ImplicitSolver::assemble, implicit.rs:2280-3155).
+//
+// 1. Element kernels (one thread per element) write local 3x3 blocks and gradient entries
+//    into contribution buffers at push-order positions: inertia (:2394-2405), stitches
+//    (:2456-2485), stretch springs (:2488-2530), StVK shells (:2608-2652), hinges
+//    (:2699-2740). Elements whose vertices are all pinned are constant and computed once.
+// 2. A gather kernel sums each slot's contributions in push order (no atomics), into the
+//    system pattern Ps or the pinned pattern Pp, and each vertex's gradient entries.
+// 3. Analytic colliders (:2954-3021) read the gathered diagonal block for the Rayleigh
+//    stiffness and add their block and gradient after everything elastic.
+// 4. Self contact (:3026-3103): per stencil, the Rayleigh stiffness from the gathered
+//    blocks, the barrier, friction, 16 (+16) blocks and 4 (+4) gradient entries; the
+//    entries are sorted by (row, col) keeping stencil order and added in that order onto
+//    Ps, or collected into the contact matrix C when the block lies outside Ps.
+// This file is compiled without FMA contraction so FP32 products round as the
+// reference's scalar f32 code does.
+#include <algorithm>
+
+#include "elements.cuh"
+#include "reduce.cuh"
+#include "scene.cuh"
+
+namespace mg {
+
+__device__ __forceinline__ void put_block(float* dst, const float* h, int ld, int r0, int c0, float scale) {
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) dst[3 * r + c] = scale * h[(r0 + r) * ld + c0 + c];
+}
+
+// ---- inertia ---------------------------------------------------------------------------
+__global__ void k_inertia(const uint32_t* __restrict__ free_verts, uint32_t n_free, const float* __restrict__ im,
+                          const float* __restrict__ x, const float* __restrict__ xt, float inv_h2,
+                          float* __restrict__ cb, float* __restrict__ ge) {
+  uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= n_free) return;
+  uint32_t i = free_verts[f];
+  float m = (1.0f / im[i]) * inv_h2;
+  float* b = cb + 9 * (size_t)f;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) b[k] = (k % 4 == 0) ? m : 0.f;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) ge[3 * (size_t)f + c] = m * (x[3 * i + c] - xt[3 * i + c]);
+}
+
+// ---- stitches (stitch.rs:57-107 at the stitch's stiffness) ------------------------------
+__global__ void k_stitch(const uint32_t* __restrict__ act, uint32_t n, const uint32_t* __restrict__ sidx,
+                         const float* __restrict__ sw, const float* __restrict__ skl, const float* __restrict__ x,
+                         float* __restrict__ cb, float* __restrict__ ge) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  uint32_t e = act[k];
+  const uint32_t* ix = sidx + 6 * (size_t)e;
+  float w[6], swt[6];
+  for (int q = 0; q < 6; ++q) {
+    w[q] = sw[6 * (size_t)e + q];
+    swt[q] = q < 3 ? w[q] : -w[q];
+  }
+  float stiff = skl[3 * e], l0 = skl[3 * e + 1], lcap = skl[3 * e + 2];
+  V3<float> t;
+  for (int q = 0; q < 6; ++q) t += ld3<float>(x, ix[q]) * swt[q];
+  float tn = t.length();
+  float* blk = cb + 9 * 36 * (size_t)e;
+  float* g = ge + 18 * (size_t)e;
+  if (tn < 1e-12f || l0 <= 0.f) {
+    for (int q = 0; q < 36 * 9; ++q) blk[q] = 0.f;
+    for (int q = 0; q < 18; ++q) g[q] = 0.f;
+    return;
+  }
+  float l = fminf(tn, lcap);
+  V3<float> nn = t / l;
+  V3<float> dedt = nn * (l / l0 - 1.0f);
+  for (int q = 0; q < 6; ++q) {
+    V3<float> gq = dedt * swt[q];
+    g[3 * q] = stiff * gq.x;
+    g[3 * q + 1] = stiff * gq.y;
+    g[3 * q + 2] = stiff * gq.z;
+  }
+  float r = (l - l0) / l;
+  float c0 = fmaxf(1.0f - r, 0.f) / l0;
+  float c1 = fmaxf(r / l0, 0.f);
+  for (int a = 0; a < 6; ++a) {
+    V3<float> ga = nn * swt[a];
+    for (int b = 0; b < 6; ++b) {
+      V3<float> gb = nn * swt[b];
+      float iden = c1 * swt[a] * swt[b];
+      float* o = blk + 9 * (6 * a + b);
+      for (int rr = 0; rr < 3; ++rr)
+        for (int cc = 0; cc < 3; ++cc) {
+          float v = c0 * ga[rr] * gb[cc];
+          if (rr == cc) v += iden;
+          o[3 * rr + cc] = stiff * v;
+        }
+    }
+  }
+}
+
+// ---- stretch springs (spring_block, implicit.rs:3240-3263) --------------------------------
+__global__ void k_spring(const uint32_t* __restrict__ act, uint32_t n, const uint32_t* __restrict__ sv,
+                         const float* __restrict__ rest, float k, const float* __restrict__ x, float* __restrict__ cb,
+                         float* __restrict__ ge) {
+  uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  uint32_t e = act[q];
+  uint32_t a = sv[2 * e], b = sv[2 * e + 1];
+  V3<float> d = ld3<float>(x, a) - ld3<float>(x, b);
+  float l = d.length();
+  float h[9];
+  V3<float> ga;
+  if (l < 1e-9f) {
+    for (int i = 0; i < 9; ++i) h[i] = (i % 4 == 0) ? k : 0.f;
+  } else {
+    V3<float> nrm = d / l;
+    float ct = fmaxf(1.0f - rest[e] / l, 0.f);
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        float nnt = nrm[i] * nrm[j];
+        h[3 * i + j] = k * (nnt + ct * ((i == j ? 1.f : 0.f) - nnt));
+      }
+    ga = nrm * (k * (l - rest[e]));
+  }
+  float* blk = cb + 36 * (size_t)e;
+  for (int i = 0; i < 9; ++i) {
+    blk[i] = h[i];
+    blk[9 + i] = h[i];
+    blk[18 + i] = -h[i];
+    blk[27 + i] = -h[i];
+  }
+  float* g = ge + 6 * (size_t)e;
+  g[0] = ga.x; g[1] = ga.y; g[2] = ga.z;
+  g[3] = -ga.x; g[4] = -ga.y; g[5] = -ga.z;
+}
+
+// ---- StVK shells ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_shell(const uint32_t* __restrict__ act, uint32_t n,
+                                               const uint32_t* __restrict__ sv, const float* __restrict__ dm,
+                                               const float* __restrict__ area, const float* __restrict__ mu,
+                                               const float* __restrict__ lam, float eps, const float* __restrict__ x,
+                                               float* __restrict__ cb, float* __restrict__ ge) {
+  uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  uint32_t e = act[q];
+  V3<float> p[3] = {ld3<float>(x, sv[3 * e]), ld3<float>(x, sv[3 * e + 1]), ld3<float>(x, sv[3 * e + 2])};
+  M2<float> D{dm[4 * e], dm[4 * e + 1], dm[4 * e + 2], dm[4 * e + 3]};
+  V3<float> g[3];
+  float h[81];
+  shell_grad_hess<float>(p, D, area[e], mu[e], lam[e], eps, g, h);
+  float* blk = cb + 81 * (size_t)e;
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) put_block(blk + 9 * (3 * a + b), h, 9, 3 * a, 3 * b, 1.0f);
+  float* gg = ge + 9 * (size_t)e;
+  for (int a = 0; a < 3; ++a) {
+    gg[3 * a] = g[a].x;
+    gg[3 * a + 1] = g[a].y;
+    gg[3 * a + 2] = g[a].z;
+  }
+}
+
+// ---- hinges ----------------------------------------------------------------------------------
+__global__ void k_hinge(const uint32_t* __restrict__ act, uint32_t n, const uint32_t* __restrict__ hv,
+                        const float* __restrict__ rest, float kb, const float* __restrict__ x, float* __restrict__ cb,
+                        float* __restrict__ ge) {
+  uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  uint32_t e = act[q];
+  V3<float> p[4];
+  for (int a = 0; a < 4; ++a) p[a] = ld3<float>(x, hv[4 * e + a]);
+  float theta = dihedral_angle<float>(p);
+  V3<float> g[4];
+  dihedral_grad<float>(p, g);
+  float kwt = kb * 1.0f;  // hinge weight w = 1 (bending.rs:150-156)
+  float gval = theta - rest[e];
+  float* gg = ge + 12 * (size_t)e;
+  for (int a = 0; a < 4; ++a)
+    for (int c = 0; c < 3; ++c) gg[3 * a + c] = kwt * gval * g[a][c];
+  float* blk = cb + 144 * (size_t)e;
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b)
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) blk[9 * (4 * a + b) + 3 * r + c] = kwt * g[a][r] * g[b][c];
+}
+
+// ---- gathers ---------------------------------------------------------------------------------
+__global__ void k_gather_blocks(const uint32_t* __restrict__ slot_ptr, const uint32_t* __restrict__ slot_list,
+                                const float* __restrict__ cb, uint32_t nslots, uint32_t nnz_s,
+                                float* __restrict__ vals, float* __restrict__ valp) {
+  uint32_t sl = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sl >= nslots) return;
+  float acc[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) acc[k] = 0.f;
+  for (uint32_t j = slot_ptr[sl]; j < slot_ptr[sl + 1]; ++j) {
+    const float* c = cb + 9 * (size_t)slot_list[j];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) acc[k] += c[k];
+  }
+  float* out = sl < nnz_s ? vals + 9 * (size_t)sl : valp + 9 * (size_t)(sl - nnz_s);
+#pragma unroll
+  for (int k = 0; k < 9; ++k) out[k] = acc[k];
+}
+
+__global__ void k_gather_grad(const uint32_t* __restrict__ gv_ptr, const uint32_t* __restrict__ gv_list,
+                              const float* __restrict__ ge, uint32_t nv, float* __restrict__ grad) {
+  uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+  for (uint32_t j = gv_ptr[v]; j < gv_ptr[v + 1]; ++j) {
+    const float* g = ge + 3 * (size_t)gv_list[j];
+    a0 += g[0];
+    a1 += g[1];
+    a2 += g[2];
+  }
+  grad[3 * v] = a0;
+  grad[3 * v + 1] = a1;
+  grad[3 * v + 2] = a2;
+}
+
+__global__ void k_pinned_identity(const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ col,
+                                  const uint8_t* __restrict__ pinned, uint32_t nv, float* __restrict__ vals) {
+  uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv || !pinned[v]) return;
+  for (uint32_t k = row_ptr[v]; k < row_ptr[v + 1]; ++k)
+    if (col[k] == v)
+      for (int q = 0; q < 9; ++q) vals[9 * (size_t)k + q] = (q % 4 == 0) ? 1.f : 0.f;
+}
+
+int assemble_elastic(Scene& s) {
+  cudaStream_t st = s.st;
+  const float h = s.p.dt, inv_h2 = 1.0f / (h * h);
+  auto grid = [](uint32_t n) { return std::max<uint32_t>(ceil_div(n, 128), 1u); };
+  float* cb = s.cblocks.p;
+  float* ge = s.gentries.p;
+  if (s.n_free)
+    k_inertia<<<grid(s.n_free), 128, 0, st>>>(s.free_verts.p, s.n_free, s.inv_mass.p, s.x.p, s.xt.p, inv_h2,
+                                            cb + 9 * s.cb_inertia, ge + 3 * s.gb_inertia);
+  // all-pinned elements once (their contributions never change), then the active ones
+  if (!s.static_done) {
+    // the full element lists, built from identity index arrays
+    std::vector<uint32_t> ids(std::max({s.n_stitch, s.n_spring, s.n_shell, s.n_hinge, 1u}));
+    for (uint32_t i = 0; i < ids.size(); ++i) ids[i] = i;
+    DevBuf<uint32_t> all;
+    MG_TRY(all.upload(ids.data(), ids.size(), st));
+    if (s.n_stitch)
+      k_stitch<<<grid(s.n_stitch), 128, 0, st>>>(all.p, s.n_stitch, s.stitch_idx.p, s.stitch_w.p, s.stitch_kl.p,
+                                                 s.x.p, cb + 9 * s.cb_stitch, ge + 3 * s.gb_stitch);
+    if (s.n_spring)
+      k_spring<<<grid(s.n_spring), 128, 0, st>>>(all.p, s.n_spring, s.spring_v.p, s.spring_rest.p, s.p.stiffness,
+                                                 s.x.p, cb + 9 * s.cb_spring, ge + 3 * s.gb_spring);
+    if (s.n_shell)
+      k_shell<<<grid(s.n_shell), 128, 0, st>>>(all.p, s.n_shell, s.shell_v.p, s.shell_dm.p, s.shell_area.p,
+                                               s.shell_mu.p, s.shell_lam.p, s.p.eiganalysis_eps, s.x.p,
+                                               cb + 9 * s.cb_shell, ge + 3 * s.gb_shell);
+    if (s.n_hinge)
+      k_hinge<<<grid(s.n_hinge), 128, 0, st>>>(all.p, s.n_hinge, s.hinge_v.p, s.hinge_rest.p, s.p.bend_stiffness,
+                                               s.x.p, cb + 9 * s.cb_hinge, ge + 3 * s.gb_hinge);
+    MG_CUDA(cudaGetLastError());
+    MG_CUDA(cudaStreamSynchronize(st));
+    s.static_done = true;
+  } else {
+    if (s.n_act_stitch)
+      k_stitch<<<grid(s.n_act_stitch), 128, 0, st>>>(s.act_stitch.p, s.n_act_stitch, s.stitch_idx.p, s.stitch_w.p,
+                                                     s.stitch_kl.p, s.x.p, cb + 9 * s.cb_stitch, ge + 3 * s.gb_stitch);
+    if (s.n_act_spring)
+      k_spring<<<grid(s.n_act_spring), 128, 0, st>>>(s.act_spring.p, s.n_act_spring, s.spring_v.p, s.spring_rest.p,
+                                                     s.p.stiffness, s.x.p, cb + 9 * s.cb_spring, ge + 3 * s.gb_spring);
+    if (s.n_act_shell)
+      k_shell<<<grid(s.n_act_shell), 128, 0, st>>>(s.act_shell.p, s.n_act_shell, s.shell_v.p, s.shell_dm.p,
+                                                   s.shell_area.p, s.shell_mu.p, s.shell_lam.p, s.p.eiganalysis_eps,
+                                                   s.x.p, cb + 9 * s.cb_shell, ge + 3 * s.gb_shell);
+    if (s.n_act_hinge)
+      k_hinge<<<grid(s.n_act_hinge), 128, 0, st>>>(s.act_hinge.p, s.n_act_hinge, s.hinge_v.p, s.hinge_rest.p,
+                                                   s.p.bend_stiffness, s.x.p, cb + 9 * s.cb_hinge, ge + 3 * s.gb_hinge);
+  }
+  MG_CUDA(cudaGetLastError());
+  uint32_t nslots = s.Ps.nnz + s.Pp.nnz;
+  k_gather_blocks<<<grid(nslots), 128, 0, st>>>(s.slot_ptr.p, s.slot_list.p, cb, nslots, s.Ps.nnz, s.A->val.p,
+                                                s.valp.p);
+  k_gather_grad<<<grid(s.nv), 128, 0, st>>>(s.gv_ptr.p, s.gv_list.p, ge, s.nv, s.grad.p);
+  k_pinned_identity<<<grid(s.nv), 128, 0, st>>>(s.Ps.row_ptr.p, s.Ps.col.p, s.pinned.p, s.nv, s.A->val.p);
+  MG_CUDA(cudaGetLastError());
+  return MGUSO_OK;
+}
+
+// ---- analytic colliders (vertex_contact_full, contact.rs:1082-1125) -------------------------
+template <class R>
+__global__ void k_colliders(const uint32_t* __restrict__ free_verts, uint32_t n_free, const float* __restrict__ im,
+                            const float* __restrict__ x, const float* __restrict__ x_start,
+                            const float* __restrict__ cols, uint32_t ncol, const uint32_t* __restrict__ diag_slot,
+                            float* __restrict__ vals, float* __restrict__ grad, float dhat, float kappa,
+                            float coupling, int barrier_kind, int rayleigh, float mu, float feps) {
+  uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= n_free) return;
+  uint32_t i = free_verts[f];
+  R m = R(1) / (R)im[i];
+  V3<R> xi = ld3<R>(x, i);
+  float* dblk = vals + 9 * (size_t)diag_slot[i];
+  R el[1][9];
+  for (int q = 0; q < 9; ++q) el[0][q] = (R)dblk[q];
+  V3<R> gsum;
+  R hs[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (uint32_t c = 0; c < ncol; ++c) {
+    const float* cc = cols + 8 * c;
+    R d;
+    V3<R> n;
+    V3<R> a((R)cc[1], (R)cc[2], (R)cc[3]);
+    if (cc[0] == 0.f) {
+      n = V3<R>((R)cc[4], (R)cc[5], (R)cc[6]);
+      d = (xi - a).dot(n);
+    } else {
+      V3<R> v = xi - a;
+      R l = v.length();
+      if (l < R(1.0e-9)) {
+        d = -(R)cc[7];
+        n = V3<R>(0, 1, 0);
+      } else {
+        d = l - (R)cc[7];
+        n = v / l;
+      }
+    }
+    R k;
+    if (rayleigh) {
+      R one = 1;
+      k = rayleigh_stiffness<R>(el, &m, &one, 1, n * d);
+    } else {
+      k = (R)kappa;
+      if (coupling > 0 && m > 0) {
+        R dd = rmax(rmax(d, R(0.1) * (R)dhat), R(1.0e-6));
+        k = (R)kappa * (R(1) + (R)coupling * m / (dd * dd));
+      }
+    }
+    R g, h;
+    if (!barrier_of<R>(barrier_kind, d, (R)dhat, k, g, h)) continue;
+    V3<R> f_c = n * g;
+    gsum += f_c;
+    R hp = rmax(h, R(0));
+    for (int r = 0; r < 3; ++r)
+      for (int c2 = 0; c2 < 3; ++c2) hs[3 * r + c2] += hp * n[r] * n[c2];
+    if (mu > 0) {
+      V3<R> fg;
+      R fh[9];
+      if (friction<R>(f_c, xi - ld3<R>(x_start, i), n, (R)mu, (R)feps, fg, fh)) {
+        gsum += fg;
+        for (int q = 0; q < 9; ++q) hs[q] += fh[q];
+      }
+    }
+  }
+  for (int q = 0; q < 9; ++q)
+    if (hs[q] != 0) dblk[q] += (float)hs[q];
+  grad[3 * i] += (float)gsum.x;
+  grad[3 * i + 1] += (float)gsum.y;
+  grad[3 * i + 2] += (float)gsum.z;
+}
+
+int assemble_colliders(Scene& s) {
+  if (!s.n_col || !s.n_free) return MGUSO_OK;
+  unsigned g = ceil_div(s.n_free, 128);
+  float mu = s.p.friction;  // collider friction unset: the vertex coefficient stands
+  if (s.mixed)
+    k_colliders<double><<<g, 128, 0, s.st>>>(s.free_verts.p, s.n_free, s.inv_mass.p, s.x.p, s.x0.p, s.colliders.p,
+                                             s.n_col, s.diag_slot.p, s.A->val.p, s.grad.p, s.p.contact_dhat,
+                                             s.p.contact_kappa, s.p.contact_dynamic, s.p.barrier_kind,
+                                             s.p.contact_rayleigh, mu, s.p.friction_eps);
+  else
+    k_colliders<float><<<g, 128, 0, s.st>>>(s.free_verts.p, s.n_free, s.inv_mass.p, s.x.p, s.x0.p, s.colliders.p,
+                                            s.n_col, s.diag_slot.p, s.A->val.p, s.grad.p, s.p.contact_dhat,
+                                            s.p.contact_kappa, s.p.contact_dynamic, s.p.barrier_kind,
+                                            s.p.contact_rayleigh, mu, s.p.friction_eps);
+  MG_CUDA(cudaGetLastError());
+  return MGUSO_OK;
+}
+
+// ---- self contact ------------------------------------------------------------------------------
+// block (va, vb) of the gathered (pre-contact) Hessian: Ps when both vertices are free,
+// else Pp; absent blocks read as zero.
+__device__ __forceinline__ const float* find_block(uint32_t va, uint32_t vb, const uint8_t* pinned,
+                                                   const uint32_t* ps_rp, const uint32_t* ps_col, const float* vals,
+                                                   const uint32_t* pp_rp, const uint32_t* pp_col, const float* valp) {
+  bool sys = !pinned[va] && !pinned[vb];
+  const uint32_t* rp = sys ? ps_rp : pp_rp;
+  const uint32_t* cl = sys ? ps_col : pp_col;
+  uint32_t lo = rp[va], hi = rp[va + 1];
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (cl[mid] < vb)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  if (lo < rp[va + 1] && cl[lo] == vb) return (sys ? vals : valp) + 9 * (size_t)lo;
+  return nullptr;
+}
+
+constexpr unsigned long long INVALID_KEY = ~0ull;
+
+template <class R>
+__global__ void k_contact_assemble(const Stencil* __restrict__ sts, uint32_t nst, const float* __restrict__ im,
+                                   const uint8_t* __restrict__ pinned, const float* __restrict__ x,
+                                   const float* __restrict__ x_start, const uint32_t* __restrict__ ps_rp,
+                                   const uint32_t* __restrict__ ps_col, const float* __restrict__ vals,
+                                   const uint32_t* __restrict__ pp_rp, const uint32_t* __restrict__ pp_col,
+                                   const float* __restrict__ valp, float kappa, int barrier_kind, float mu, float feps,
+                                   float* __restrict__ ccb, unsigned long long* __restrict__ ckeys,
+                                   uint32_t* __restrict__ cids, float* __restrict__ cge,
+                                   unsigned long long* __restrict__ gkeys, uint32_t* __restrict__ gids) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nst) return;
+  const Stencil& S = sts[s];
+  V3<R> g[4];
+  for (int a = 0; a < 4; ++a) g[a] = V3<R>((R)S.g[3 * a], (R)S.g[3 * a + 1], (R)S.g[3 * a + 2]);
+  R d = (R)S.d;
+  // self_contact_rayleigh (implicit.rs:755-795)
+  R k;
+  R nlen = g[0].length();
+  if (nlen < R(1.0e-12)) {
+    k = (R)kappa;
+  } else {
+    V3<R> nrm = g[0] / nlen;
+    R wts[4], mass[4];
+    R el[16][9];
+    for (int a = 0; a < 4; ++a) {
+      wts[a] = g[a].dot(nrm);
+      R imv = (R)im[S.idx[a]];
+      mass[a] = imv > 0 ? R(1) / imv : R(0);
+    }
+    for (int ia = 0; ia < 4; ++ia)
+      for (int ib = 0; ib < 4; ++ib) {
+        const float* b = find_block(S.idx[ia], S.idx[ib], pinned, ps_rp, ps_col, vals, pp_rp, pp_col, valp);
+        for (int q = 0; q < 9; ++q) el[ia * 4 + ib][q] = b ? (R)b[q] : R(0);
+      }
+    k = rayleigh_stiffness<R>(el, mass, wts, 4, nrm * d);
+    if (!(k > 0)) k = (R)kappa;
+  }
+  int kind = d < 0 ? 1 : barrier_kind;
+  R bg = 0, bh = 0;
+  bool active = barrier_of<R>(kind, d, (R)S.ghat, k, bg, bh);
+  R hp = rmax(bh, R(0));
+  // friction (stencil_friction, contact.rs:659-705)
+  bool fr = false;
+  V3<R> fg;
+  R fh[9];
+  R w[4];
+  if (active && mu > 0 && nlen >= R(1.0e-12)) {
+    V3<R> n = g[0] / nlen;
+    V3<R> slip;
+    for (int a = 0; a < 4; ++a) {
+      w[a] = g[a].dot(n);
+      slip += (ld3<R>(x, S.idx[a]) - ld3<R>(x_start, S.idx[a])) * w[a];
+    }
+    fr = friction<R>(n * bg, slip, n, (R)mu, (R)feps, fg, fh);
+    if (fr && fg.x == 0 && fg.y == 0 && fg.z == 0) fr = false;
+  }
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b) {
+      uint32_t ra = S.idx[a], cbv = S.idx[b];
+      bool keep = !pinned[ra] && !pinned[cbv];
+      size_t id = 32 * (size_t)s + 4 * a + b;
+      float* o = ccb + 9 * id;
+      bool any = false;
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+          float vh = active ? (float)(hp * g[a][r] * g[b][c]) : 0.f;
+          o[3 * r + c] = vh;
+          any = any || vh != 0.f;
+        }
+      ckeys[id] = (keep && any) ? (((unsigned long long)ra << 32) | cbv) : INVALID_KEY;
+      cids[id] = (uint32_t)id;
+      size_t id2 = id + 16;
+      float* o2 = ccb + 9 * id2;
+      bool any2 = false;
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+          float vh = fr ? (float)(w[a] * w[b] * fh[3 * r + c]) : 0.f;
+          if (fr && w[a] * w[b] == 0) vh = 0.f;
+          o2[3 * r + c] = vh;
+          any2 = any2 || vh != 0.f;
+        }
+      ckeys[id2] = (keep && any2) ? (((unsigned long long)ra << 32) | cbv) : INVALID_KEY;
+      cids[id2] = (uint32_t)id2;
+    }
+  for (int a = 0; a < 4; ++a) {
+    size_t id = 8 * (size_t)s + a;
+    V3<R> gb = g[a] * bg;
+    cge[3 * id] = active ? (float)gb.x : 0.f;
+    cge[3 * id + 1] = active ? (float)gb.y : 0.f;
+    cge[3 * id + 2] = active ? (float)gb.z : 0.f;
+    gkeys[id] = active ? S.idx[a] : INVALID_KEY;
+    gids[id] = (uint32_t)id;
+    size_t id2 = id + 4;
+    V3<R> ff = fr ? fg * w[a] : V3<R>();
+    cge[3 * id2] = (float)ff.x;
+    cge[3 * id2 + 1] = (float)ff.y;
+    cge[3 * id2 + 2] = (float)ff.z;
+    gkeys[id2] = fr ? S.idx[a] : INVALID_KEY;
+    gids[id2] = (uint32_t)id2;
+  }
+}
+
+// Segment heads of the sorted block keys: add onto Ps when the block exists there, else
+// flag a new C entry (rank computed by the scan below).
+__global__ void k_contact_heads(const unsigned long long* __restrict__ keys, const uint32_t* __restrict__ ids,
+                                uint32_t m, const float* __restrict__ ccb, const uint32_t* __restrict__ ps_rp,
+                                const uint32_t* __restrict__ ps_col, float* __restrict__ vals,
+                                uint32_t* __restrict__ is_new) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  unsigned long long k = keys[i];
+  bool head = k != INVALID_KEY && (i == 0 || keys[i - 1] != k);
+  is_new[i] = 0;
+  if (!head) return;
+  uint32_t r = (uint32_t)(k >> 32), c = (uint32_t)k;
+  uint32_t lo = ps_rp[r], hi = ps_rp[r + 1];
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (ps_col[mid] < c)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  if (lo < ps_rp[r + 1] && ps_col[lo] == c) {
+    float* v = vals + 9 * (size_t)lo;
+    float a[9];
+    for (int q = 0; q < 9; ++q) a[q] = v[q];
+    for (uint32_t j = i; j < m && keys[j] == k; ++j) {
+      const float* cc = ccb + 9 * (size_t)ids[j];
+      for (int q = 0; q < 9; ++q)
+        if (cc[q] != 0.f) a[q] += cc[q];
+    }
+    for (int q = 0; q < 9; ++q) v[q] = a[q];
+  } else {
+    is_new[i] = 1;
+  }
+}
+
+__global__ void k_contact_new(const unsigned long long* __restrict__ keys, const uint32_t* __restrict__ ids,
+                              uint32_t m, const float* __restrict__ ccb, const uint32_t* __restrict__ is_new,
+                              const uint32_t* __restrict__ rank, uint32_t* __restrict__ c_row,
+                              uint32_t* __restrict__ c_col, float* __restrict__ c_val) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m || !is_new[i]) return;
+  unsigned long long k = keys[i];
+  uint32_t o = rank[i];
+  float a[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (uint32_t j = i; j < m && keys[j] == k; ++j) {
+    const float* cc = ccb + 9 * (size_t)ids[j];
+    for (int q = 0; q < 9; ++q)
+      if (cc[q] != 0.f) a[q] += cc[q];
+  }
+  c_row[o] = (uint32_t)(k >> 32);
+  c_col[o] = (uint32_t)k;
+  for (int q = 0; q < 9; ++q) c_val[9 * (size_t)o + q] = a[q];
+}
+
+__global__ void k_row_ptr_from_sorted(const uint32_t* __restrict__ rows, const uint32_t* __restrict__ count,
+                                      uint32_t nv, uint32_t* __restrict__ row_ptr) {
+  uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r > nv) return;
+  uint32_t n = *count;
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (rows[mid] < r)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  row_ptr[r] = lo;
+}
+
+__global__ void k_contact_grad(const unsigned long long* __restrict__ keys, const uint32_t* __restrict__ ids,
+                               uint32_t m, const float* __restrict__ cge, float* __restrict__ grad) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  unsigned long long k = keys[i];
+  if (k == INVALID_KEY || (i > 0 && keys[i - 1] == k)) return;
+  uint32_t v = (uint32_t)k;
+  float a0 = grad[3 * v], a1 = grad[3 * v + 1], a2 = grad[3 * v + 2];
+  for (uint32_t j = i; j < m && keys[j] == k; ++j) {
+    const float* g = cge + 3 * (size_t)ids[j];
+    a0 += g[0];
+    a1 += g[1];
+    a2 += g[2];
+  }
+  grad[3 * v] = a0;
+  grad[3 * v + 1] = a1;
+  grad[3 * v + 2] = a2;
+}
+
+// exclusive scan of u32 flags (n <= 2^30), three passes
+__global__ void k_scan_block(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint32_t n,
+                             uint32_t* __restrict__ block_sums) {
+  __shared__ uint32_t s[1024];
+  uint32_t i = blockIdx.x * 1024 + threadIdx.x;
+  uint32_t v = i < n ? in[i] : 0;
+  s[threadIdx.x] = v;
+  __syncthreads();
+  for (uint32_t o = 1; o < 1024; o <<= 1) {
+    uint32_t t = threadIdx.x >= o ? s[threadIdx.x - o] : 0;
+    __syncthreads();
+    s[threadIdx.x] += t;
+    __syncthreads();
+  }
+  if (i < n) out[i] = s[threadIdx.x] - v;
+  if (threadIdx.x == 1023) block_sums[blockIdx.x] = s[1023];
+}
+
+__global__ void k_scan_sums(uint32_t* __restrict__ sums, uint32_t nb, uint32_t* __restrict__ total) {
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0;
+    for (uint32_t b = 0; b < nb; ++b) {
+      uint32_t v = sums[b];
+      sums[b] = acc;
+      acc += v;
+    }
+    *total = acc;
+  }
+}
+
+__global__ void k_scan_add(uint32_t* __restrict__ out, uint32_t n, const uint32_t* __restrict__ sums) {
+  uint32_t i = blockIdx.x * 1024 + threadIdx.x;
+  if (i < n) out[i] += sums[blockIdx.x];
+}
+
+static int scan_u32(Scene& s, const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* total, DevBuf<uint32_t>& tmp) {
+  uint32_t nb = std::max<uint32_t>(ceil_div(n, 1024), 1);
+  MG_TRY(tmp.reserve(nb + 1));
+  if (n) k_scan_block<<<nb, 1024, 0, s.st>>>(in, out, n, tmp.p);
+  else MG_CUDA(cudaMemsetAsync(tmp.p, 0, 4, s.st));
+  k_scan_sums<<<1, 32, 0, s.st>>>(tmp.p, n ? nb : 1, total);
+  if (n) k_scan_add<<<nb, 1024, 0, s.st>>>(out, n, tmp.p);
+  MG_CUDA(cudaGetLastError());
+  return MGUSO_OK;
+}
+
+int assemble_contacts(Scene& s, uint32_t nst) {
+  cudaStream_t st = s.st;
+  // C starts empty every iteration
+  MG_CUDA(cudaMemsetAsync(s.c_count.p, 0, 4, st));
+  if (nst == 0) {
+    MG_CUDA(cudaMemsetAsync(s.c_row_ptr.p, 0, 4 * ((size_t)s.nv + 1), st));
+    return MGUSO_OK;
+  }
+  const uint32_t mb = 32 * nst, mg_ = 8 * nst;
+  MG_TRY(s.ccblocks.reserve(9 * (size_t)mb));
+  MG_TRY(s.ckeys.reserve(mb));
+  MG_TRY(s.cids.reserve(mb));
+  MG_TRY(s.cgentries.reserve(3 * (size_t)mg_));
+  MG_TRY(s.gkeys.reserve(mg_));
+  MG_TRY(s.gids.reserve(mg_));
+  unsigned g = ceil_div(nst, 64);
+  if (s.mixed)
+    k_contact_assemble<double><<<g, 64, 0, st>>>(s.stencils_sorted.p, nst, s.inv_mass.p, s.pinned.p, s.x.p, s.x0.p,
+                                                 s.Ps.row_ptr.p, s.Ps.col.p, s.A->val.p, s.Pp.row_ptr.p, s.Pp.col.p,
+                                                 s.valp.p, s.p.contact_kappa, s.p.barrier_kind, s.p.friction,
+                                                 s.p.friction_eps, s.ccblocks.p, s.ckeys.p, s.cids.p, s.cgentries.p,
+                                                 s.gkeys.p, s.gids.p);
+  else
+    k_contact_assemble<float><<<g, 64, 0, st>>>(s.stencils_sorted.p, nst, s.inv_mass.p, s.pinned.p, s.x.p, s.x0.p,
+                                                s.Ps.row_ptr.p, s.Ps.col.p, s.A->val.p, s.Pp.row_ptr.p, s.Pp.col.p,
+                                                s.valp.p, s.p.contact_kappa, s.p.barrier_kind, s.p.friction,
+                                                s.p.friction_eps, s.ccblocks.p, s.ckeys.p, s.cids.p, s.cgentries.p,
+                                                s.gkeys.p, s.gids.p);
+  MG_CUDA(cudaGetLastError());
+  // blocks: stable sort by (row, col); stencil order survives within equal keys
+  MG_TRY(radix_sort_pairs(&s.tri_bvh, s.ckeys.p, s.cids.p, mb, 64, st));
+  DevBuf<uint32_t>& is_new = s.is_new;
+  DevBuf<uint32_t>& rank = s.rank;
+  DevBuf<uint32_t>& tmp = s.scan_tmp;
+  MG_TRY(is_new.reserve(mb));
+  MG_TRY(rank.reserve(mb));
+  k_contact_heads<<<ceil_div(mb, 256), 256, 0, st>>>(s.ckeys.p, s.cids.p, mb, s.ccblocks.p, s.Ps.row_ptr.p,
+                                                    s.Ps.col.p, s.A->val.p, is_new.p);
+  MG_TRY(scan_u32(s, is_new.p, rank.p, mb, s.c_count.p, tmp));
+  uint32_t nc = 0;
+  MG_CUDA(cudaMemcpyAsync(&nc, s.c_count.p, 4, cudaMemcpyDeviceToHost, st));
+  MG_CUDA(cudaStreamSynchronize(st));
+  if (nc > s.cap_c || !s.c_col.p) {
+    s.cap_c = std::max(nc, s.cap_c) * 2;
+    s.work.drop_graph();
+  }
+  MG_TRY(s.c_row.reserve(s.cap_c));
+  MG_TRY(s.c_col.reserve(s.cap_c));
+  MG_TRY(s.c_val.reserve(9 * (size_t)s.cap_c));
+  k_contact_new<<<ceil_div(mb, 256), 256, 0, st>>>(s.ckeys.p, s.cids.p, mb, s.ccblocks.p, is_new.p, rank.p,
+                                                  s.c_row.p, s.c_col.p, s.c_val.p);
+  k_row_ptr_from_sorted<<<ceil_div(s.nv + 1, 256), 256, 0, st>>>(s.c_row.p, s.c_count.p, s.nv, s.c_row_ptr.p);
+  // gradient entries: stable sort by vertex, then add in stencil order
+  MG_TRY(radix_sort_pairs(&s.tri_bvh, s.gkeys.p, s.gids.p, mg_, 64, st));
+  k_contact_grad<<<ceil_div(mg_, 256), 256, 0, st>>>(s.gkeys.p, s.gids.p, mg_, s.cgentries.p, s.grad.p);
+  MG_CUDA(cudaGetLastError());
+  return MGUSO_OK;
+}
+
+__global__ void k_rhs(const float* __restrict__ grad, const uint8_t* __restrict__ pinned, uint32_t nv,
+                      float* __restrict__ rhs) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 3 * nv) return;
+  rhs[i] = pinned[i / 3] ? 0.f : -grad[i];
+}
+
+int finish_rhs(Scene& s) {
+  k_rhs<<<ceil_div(3 * s.nv, 256), 256, 0, s.st>>>(s.grad.p, s.pinned.p, s.nv, s.work.b.p);
+  MG_CUDA(cudaGetLastError());
+  return MGUSO_OK;
+}
+
+// y += C x over C's rows, then the fused dot(x, y) over every row.
+template <class Acc>
+__global__ void k_c_add_dot(const uint32_t* __restrict__ c_rp, const uint32_t* __restrict__ c_col,
+                            const float* __restrict__ c_val, uint32_t nv, const float* __restrict__ x,
+                            float* __restrict__ y, DotSink dot, int with_dot) {
+  if (with_dot && dot.sc->done) return;
+  Acc acc = 0;
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < nv; r += gridDim.x * blockDim.x) {
+    float y0 = y[3 * r], y1 = y[3 * r + 1], y2 = y[3 * r + 2];
+    for (uint32_t k = c_rp[r]; k < c_rp[r + 1]; ++k) {
+      uint32_t c = c_col[k];
+      const float* a = c_val + 9 * (size_t)k;
+      float x0 = x[3 * c], x1 = x[3 * c + 1], x2 = x[3 * c + 2];
+      y0 += a[0] * x0 + a[1] * x1 + a[2] * x2;
+      y1 += a[3] * x0 + a[4] * x1 + a[5] * x2;
+      y2 += a[6] * x0 + a[7] * x1 + a[8] * x2;
+    }
+    y[3 * r] = y0;
+    y[3 * r + 1] = y1;
+    y[3 * r + 2] = y2;
+    acc += (Acc)x[3 * r] * (Acc)y0 + (Acc)x[3 * r + 1] * (Acc)y1 + (Acc)x[3 * r + 2] * (Acc)y2;
+  }
+  if (with_dot) grid_dot_commit<Acc>(dot, acc);
+}
+
+int system_spmv(Scene& s, const float* p, float* ap, cudaStream_t st, const DotSink* d) {
+  MG_TRY(bsr_spmv(s.A.get(), p, ap, st, nullptr));
+  int grid = vec_grid(s.nv, 256, s.ctx->sm_count);
+  DotSink dd = d ? *d : DotSink{};
+  if (d && d->mixed)
+    k_c_add_dot<double><<<grid, 256, 0, st>>>(s.c_row_ptr.p, s.c_col.p ? s.c_col.p : s.c_row_ptr.p, s.c_val.p,
+                                              s.nv, p, ap, dd, d ? 1 : 0);
+  else
+    k_c_add_dot<float><<<grid, 256, 0, st>>>(s.c_row_ptr.p, s.c_col.p ? s.c_col.p : s.c_row_ptr.p, s.c_val.p, s.nv,
+                                             p, ap, dd, d ? 1 : 0);
+  MG_CUDA(cudaGetLastError());
+  return MGUSO_OK;
+}
+
+}  // namespace mg

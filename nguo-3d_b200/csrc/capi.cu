@@ -203,7 +203,6 @@ int mguso_linear_solver_create(mguso_ctx* ctx, int precond, uint32_t domain, int
 
 int mguso_linear_solver_destroy(mguso_linear_solver* s) {
   if (!s) return MGUSO_OK;
-  if (s->h_sc) cudaFreeHost(s->h_sc);
   delete s;
   return MGUSO_OK;
 }
@@ -238,6 +237,7 @@ int mguso_linear_solve(mguso_linear_solver* s, const mguso_csr* a, const float* 
     }
     s->csr_row_ptr.assign(a->row_ptr, a->row_ptr + a->n + 1);
     s->csr_col.assign(a->col_idx, a->col_idx + nnz);
+    s->generation++;
     if (s->precond == MGUSO_PRECOND_SCHWARZ) {
       s->schwarz = std::make_unique<mguso_schwarz>();
       s->schwarz->a = s->bsr.get();
@@ -250,7 +250,8 @@ int mguso_linear_solve(mguso_linear_solver* s, const mguso_csr* a, const float* 
     MG_CUDA(cudaMemcpyAsync(s->bsr->val.p, s->h_val.data(), 4 * s->h_val.size(), cudaMemcpyHostToDevice, st));
   }
   uint32_t n = a->n;
-  MG_TRY(s->b.upload(b, n, st));
+  MG_TRY(s->work.reserve(n));
+  MG_CUDA(cudaMemcpyAsync(s->work.b.p, b, 4 * (size_t)n, cudaMemcpyHostToDevice, st));
   if (s->precond == MGUSO_PRECOND_SCHWARZ) {
     MG_TRY(schwarz_factor(s->schwarz.get(), st));
   } else {
@@ -259,7 +260,7 @@ int mguso_linear_solve(mguso_linear_solver* s, const mguso_csr* a, const float* 
   }
   mguso_lin_stats local{};
   MG_TRY(pcg_solve(s, tol, max_iter, &local));
-  MG_CUDA(cudaMemcpyAsync(x, s->x.p, 4 * (size_t)n, cudaMemcpyDeviceToHost, st));
+  MG_CUDA(cudaMemcpyAsync(x, s->work.x.p, 4 * (size_t)n, cudaMemcpyDeviceToHost, st));
   MG_CUDA(cudaStreamSynchronize(st));
   if (stats) *stats = local;
   return MGUSO_OK;

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <cstdio>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -71,12 +72,23 @@ struct DevBuf {
   }
   int upload(const T* h, size_t n, cudaStream_t s) {
     MG_TRY(reserve(n));
-    if (n) MG_CUDA(cudaMemcpyAsync(p, h, n * sizeof(T), cudaMemcpyHostToDevice, s));
+    if (n && h) MG_CUDA(cudaMemcpyAsync(p, h, n * sizeof(T), cudaMemcpyHostToDevice, s));
     return MGUSO_OK;
   }
 };
 
 inline unsigned ceil_div(size_t a, size_t b) { return (unsigned)((a + b - 1) / b); }
+
+inline unsigned int f2u_host(float f) {
+  unsigned int u;
+  std::memcpy(&u, &f, 4);
+  return u;
+}
+inline float u2f_host(unsigned int u) {
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
 
 int device_sm_count();
 

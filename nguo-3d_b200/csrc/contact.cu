@@ -1,0 +1,463 @@
+// Self contact on the GPU: LBVH candidates, static-collider sides, the active stencil set
+// and the CCD step filter.
+//
+// Reference: self_collision_stencils (implicit.rs:678-753), collider_sides
+// (implicit.rs:1431-1475) and ccd_max_step (implicit.rs:1690-1947), whose broad phase is a
+// uniform hash grid (broadphase.rs:263-526). Here candidates come from two LBVHs built over
+// the current positions (triangles, and edges as degenerate triangles), with the exact box
+// predicate the grid over-approximates: a vertex against a triangle's box grown by the
+// search radius, an edge's box grown by it against another edge's box. Every stencil the
+// grid finds within its activation gap is found here (the gap test is exact), with the
+// same 1-ring exclusion, movability filter and shared-vertex rule. Stencils are sorted by
+// (kind, primitive, primitive) to reproduce the reference's sorted, deduplicated order.
+#include <algorithm>
+
+#include "elements.cuh"
+#include "scene.cuh"
+
+namespace mg {
+
+__device__ __forceinline__ bool excluded(const uint32_t* ex_ptr, const uint32_t* ex_list, uint32_t v, uint32_t a,
+                                         uint32_t b, uint32_t c) {
+  for (uint32_t k = ex_ptr[v]; k < ex_ptr[v + 1]; ++k) {
+    uint32_t e = ex_list[k];
+    if (e == a || e == b || e == c) return true;
+  }
+  return false;
+}
+
+struct BvhView {
+  const uint32_t *left, *right, *prim;
+  const float4 *node, *leaf;
+  uint32_t n;
+};
+
+static BvhView view(const Lbvh& b) {
+  return BvhView{b.left.p, b.right.p, b.perm.p, (const float4*)b.node.p, (const float4*)b.leaf.p, b.nt};
+}
+
+template <class F>
+__device__ __forceinline__ bool visit(const BvhView& bv, float4 lo, float4 hi, F&& f) {
+  return lbvh_visit(bv.left, bv.right, bv.node, bv.leaf, bv.prim, bv.n, lo, hi, f);
+}
+
+__device__ __forceinline__ void point_box(const float* x, uint32_t v, float pad, float4& lo, float4& hi) {
+  float a = x[3 * v], b = x[3 * v + 1], c = x[3 * v + 2];
+  lo = make_float4(__fsub_rn(a, pad), __fsub_rn(b, pad), __fsub_rn(c, pad), 0.f);
+  hi = make_float4(__fadd_rn(a, pad), __fadd_rn(b, pad), __fadd_rn(c, pad), 0.f);
+}
+
+__device__ __forceinline__ void edge_box(const float* x, uint32_t a, uint32_t b, float pad, float4& lo, float4& hi) {
+  float l[3], h[3];
+  for (int c = 0; c < 3; ++c) {
+    float p = x[3 * a + c], q = x[3 * b + c];
+    l[c] = __fsub_rn(fminf(p, q), pad);
+    h[c] = __fadd_rn(fmaxf(p, q), pad);
+  }
+  lo = make_float4(l[0], l[1], l[2], 0.f);
+  hi = make_float4(h[0], h[1], h[2], 0.f);
+}
+
+int build_bvhs(Scene& s, const float* x) {
+  MG_TRY(lbvh_build(&s.tri_bvh, x, s.nv, s.tris.p, s.nt, 30, s.st));
+  MG_TRY(lbvh_build(&s.edge_bvh, x, s.nv, s.edge_tris.p, s.n_edge, 30, s.st));
+  return MGUSO_OK;
+}
+
+// ---- collider sides ------------------------------------------------------------------
+// best (d2 bits, triangle) per non-static vertex over collider triangles within dhat; ties
+// go to the lowest triangle index, which is the first one the reference's triangle-major
+// visit reaches.
+__global__ void k_side_best(BvhView bv, const float* __restrict__ x, const uint32_t* __restrict__ tris,
+                            const uint8_t* __restrict__ ctri, const uint8_t* __restrict__ svert,
+                            const float* __restrict__ im, const uint32_t* __restrict__ ex_ptr,
+                            const uint32_t* __restrict__ ex_list, uint32_t nv, float dhat,
+                            unsigned long long* __restrict__ best, uint32_t* __restrict__ status) {
+  uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  unsigned long long b = ~0ull;
+  if (!svert[v] && im[v] > 0.f) {
+    float4 lo, hi;
+    point_box(x, v, dhat, lo, hi);
+    V3<float> p = ld3<float>(x, v);
+    bool ok = visit(bv, lo, hi, [&](uint32_t t) {
+      if (!ctri[t]) return;
+      uint32_t a = tris[3 * t], bb = tris[3 * t + 1], c = tris[3 * t + 2];
+      if (excluded(ex_ptr, ex_list, v, a, bb, c)) return;
+      float w[3];
+      V3<float> q = closest_point_bary(p, ld3<float>(x, a), ld3<float>(x, bb), ld3<float>(x, c), w);
+      float d2 = (p - q).length_squared();
+      unsigned long long k = ((unsigned long long)__float_as_uint(d2) << 32) | t;
+      if (k < b) b = k;
+    });
+    if (!ok) atomicOr(status, ST_STACK_OVERFLOW);
+  }
+  best[v] = b;
+}
+
+__device__ __forceinline__ float side_of(uint32_t v, const unsigned long long* best, const float* x,
+                                         const uint32_t* tris, const float* pn, float dhat) {
+  unsigned long long b = best[v];
+  if (b == ~0ull) return 1.f;
+  float d2 = __uint_as_float((uint32_t)(b >> 32));
+  if (d2 >= dhat * dhat) return 1.f;
+  uint32_t t = (uint32_t)b;
+  uint32_t ia = tris[3 * t], ib = tris[3 * t + 1], ic = tris[3 * t + 2];
+  V3<float> a = ld3<float>(x, ia), bb = ld3<float>(x, ib), c = ld3<float>(x, ic), p = ld3<float>(x, v);
+  float l[3];
+  V3<float> q = closest_point_bary(p, a, bb, c, l);
+  V3<float> e = p - q;
+  V3<float> pnv[3] = {ld3<float>(pn, ia), ld3<float>(pn, ib), ld3<float>(pn, ic)};
+  V3<float> n = surface_normal_at(l, (bb - a).cross(c - a).normalize_or_zero(), pnv);
+  return e.dot(n) < 0.f ? -1.f : 1.f;
+}
+
+// ---- stencils ------------------------------------------------------------------------------
+__device__ __forceinline__ void emit_stencil(Stencil* out, unsigned long long* keys, uint32_t* ids,
+                                             unsigned long long* counter, uint32_t cap, uint32_t* status,
+                                             uint32_t kind, uint32_t pa, uint32_t pb, const uint32_t idx[4], double d,
+                                             double ghat, const double g[12]) {
+  unsigned long long at = atomicAdd(counter, 1ull);
+  if (at >= cap) {
+    atomicOr(status, ST_CAPACITY);
+    return;
+  }
+  Stencil& S = out[at];
+  for (int k = 0; k < 4; ++k) S.idx[k] = idx[k];
+  S.kind = kind;
+  S.pad = 0;
+  S.d = d;
+  S.ghat = ghat;
+  for (int k = 0; k < 12; ++k) S.g[k] = g[k];
+  keys[at] = ((unsigned long long)kind << 62) | ((unsigned long long)pa << 31) | pb;
+  ids[at] = (uint32_t)at;
+}
+
+template <class R>
+__device__ __forceinline__ R vt_distance(const float* x, const uint32_t idx[4], bool collider, bool inside, R g[12]) {
+  V3<R> gg[4];
+  R d = point_tri_distance_grad<R>(ld3<R>(x, idx[0]), ld3<R>(x, idx[1]), ld3<R>(x, idx[2]), ld3<R>(x, idx[3]),
+                                   collider && inside, gg);
+  for (int a = 0; a < 4; ++a)
+    for (int c = 0; c < 3; ++c) g[3 * a + c] = gg[a][c];
+  return d;
+}
+
+template <class R>
+__device__ __forceinline__ R ee_distance(const float* x, const uint32_t idx[4], R g[12]) {
+  V3<R> gg[4];
+  R d = segment_segment_distance_grad<R>(ld3<R>(x, idx[0]), ld3<R>(x, idx[1]), ld3<R>(x, idx[2]), ld3<R>(x, idx[3]),
+                                         gg);
+  for (int a = 0; a < 4; ++a)
+    for (int c = 0; c < 3; ++c) g[3 * a + c] = gg[a][c];
+  return d;
+}
+
+__global__ void k_vt_stencils(BvhView bv, const float* __restrict__ x, const uint32_t* __restrict__ tris,
+                              const uint8_t* __restrict__ ctri, const float* __restrict__ im,
+                              const uint32_t* __restrict__ ex_ptr, const uint32_t* __restrict__ ex_list,
+                              const unsigned long long* __restrict__ best, const float* __restrict__ pn, int has_static,
+                              uint32_t nv, float dhat, int mixed, Stencil* out, unsigned long long* keys, uint32_t* ids,
+                              unsigned long long* counter, uint32_t cap, uint32_t* status) {
+  uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  float4 lo, hi;
+  point_box(x, v, dhat, lo, hi);
+  bool vmov = im[v] > 0.f;
+  float side = 2.f;  // computed lazily
+  bool ok = visit(bv, lo, hi, [&](uint32_t t) {
+    uint32_t a = tris[3 * t], b = tris[3 * t + 1], c = tris[3 * t + 2];
+    bool tmov = im[a] > 0.f || im[b] > 0.f || im[c] > 0.f;
+    if (!tmov && !vmov) return;
+    if (excluded(ex_ptr, ex_list, v, a, b, c)) return;
+    uint32_t idx[4] = {v, a, b, c};
+    bool collider = has_static && ctri[t];
+    if (collider && side == 2.f) side = side_of(v, best, x, tris, pn, dhat);
+    bool inside = collider && side < 0.f;
+    double g[12];
+    float gf[12];
+    float df = vt_distance<float>(x, idx, collider, inside, gf);
+    double d = df;
+    for (int k = 0; k < 12; ++k) g[k] = gf[k];
+    if (mixed && df < 10.f * dhat) d = vt_distance<double>(x, idx, collider, inside, g);
+    if (!(d < (double)dhat)) return;
+    emit_stencil(out, keys, ids, counter, cap, status, 0, v, t, idx, d, dhat, g);
+  });
+  if (!ok) atomicOr(status, ST_STACK_OVERFLOW);
+}
+
+__global__ void k_ee_stencils(BvhView bv, const float* __restrict__ x, const uint32_t* __restrict__ edges,
+                              const float* __restrict__ im, uint32_t ne, float search, float dhat, int mixed,
+                              Stencil* out, unsigned long long* keys, uint32_t* ids, unsigned long long* counter,
+                              uint32_t cap, uint32_t* status) {
+  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ne) return;
+  uint32_t b0 = edges[2 * j], b1 = edges[2 * j + 1];
+  float4 lo, hi;
+  edge_box(x, b0, b1, search, lo, hi);
+  bool jmov = im[b0] > 0.f || im[b1] > 0.f;
+  bool ok = visit(bv, lo, hi, [&](uint32_t i) {
+    if (i >= j) return;
+    uint32_t a0 = edges[2 * i], a1 = edges[2 * i + 1];
+    if (!(jmov || im[a0] > 0.f || im[a1] > 0.f)) return;
+    if (a0 == b0 || a0 == b1 || a1 == b0 || a1 == b1) return;
+    uint32_t idx[4] = {a0, a1, b0, b1};
+    double g[12];
+    float gf[12];
+    float df = ee_distance<float>(x, idx, gf);
+    double d = df;
+    for (int k = 0; k < 12; ++k) g[k] = gf[k];
+    if (mixed && df < 10.f * dhat) d = ee_distance<double>(x, idx, g);
+    double ghat = (double)(0.5f * (dhat + dhat));
+    if (!(d < ghat)) return;
+    emit_stencil(out, keys, ids, counter, cap, status, 1, i, j, idx, d, ghat, g);
+  });
+  if (!ok) atomicOr(status, ST_STACK_OVERFLOW);
+}
+
+__global__ void k_permute_stencils(const Stencil* __restrict__ in, const uint32_t* __restrict__ ids, uint32_t n,
+                                   Stencil* __restrict__ out) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = in[ids[i]];
+}
+
+int collect_stencils(Scene& s, uint32_t* nst_out) {
+  cudaStream_t st = s.st;
+  const float dhat = s.p.contact_dhat;
+  BvhView tv = view(s.tri_bvh), ev = view(s.edge_bvh);
+  if (s.has_static) {
+    k_side_best<<<ceil_div(s.nv, 128), 128, 0, st>>>(tv, s.x.p, s.tris.p, s.collider_tri.p, s.static_vert.p,
+                                                   s.inv_mass.p, s.ex_ptr.p, s.ex_list.p, s.nv, dhat, s.side_best.p,
+                                                   s.status.p);
+  }
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    MG_TRY(s.stencils.reserve(s.cap_stencils));
+    MG_TRY(s.stencils_sorted.reserve(s.cap_stencils));
+    MG_TRY(s.st_keys.reserve(s.cap_stencils));
+    MG_TRY(s.st_ids.reserve(s.cap_stencils));
+    MG_CUDA(cudaMemsetAsync(s.counters.p, 0, 8 * 8, st));
+    k_vt_stencils<<<ceil_div(s.nv, 128), 128, 0, st>>>(tv, s.x.p, s.tris.p, s.collider_tri.p, s.inv_mass.p,
+                                                     s.ex_ptr.p, s.ex_list.p, s.side_best.p, s.collider_pn.p,
+                                                     s.has_static ? 1 : 0, s.nv, dhat, s.mixed ? 1 : 0, s.stencils.p,
+                                                     s.st_keys.p, s.st_ids.p, s.counters.p, s.cap_stencils,
+                                                     s.status.p);
+    if (s.n_edge)
+      k_ee_stencils<<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, s.x.p, s.edges.p, s.inv_mass.p, s.n_edge, dhat, dhat,
+                                                           s.mixed ? 1 : 0, s.stencils.p, s.st_keys.p, s.st_ids.p,
+                                                           s.counters.p, s.cap_stencils, s.status.p);
+    MG_CUDA(cudaGetLastError());
+    unsigned long long cnt = 0;
+    MG_CUDA(cudaMemcpyAsync(&cnt, s.counters.p, 8, cudaMemcpyDeviceToHost, st));
+    MG_CUDA(cudaStreamSynchronize(st));
+    if (cnt <= s.cap_stencils) {
+      uint32_t n = (uint32_t)cnt;
+      if (n > 1) MG_TRY(radix_sort_pairs(&s.tri_bvh, s.st_keys.p, s.st_ids.p, n, 64, st));
+      if (n) k_permute_stencils<<<ceil_div(n, 128), 128, 0, st>>>(s.stencils.p, s.st_ids.p, n, s.stencils_sorted.p);
+      MG_CUDA(cudaGetLastError());
+      *nst_out = n;
+      return MGUSO_OK;
+    }
+    s.cap_stencils = (uint32_t)std::min<unsigned long long>(2 * cnt + 1024, 1ull << 28);
+    MG_CUDA(cudaMemsetAsync(s.status.p, 0, 4, st));  // clear the capacity flag and retry
+  }
+  set_error("stencil buffer growth did not converge");
+  return MGUSO_ERR_PAIR_OVERFLOW;
+}
+
+// ---- CCD -----------------------------------------------------------------------------------
+__device__ __forceinline__ void atomic_min_pos(unsigned int* addr, float v) {
+  atomicMin(addr, __float_as_uint(fmaxf(v, 0.f)));
+}
+
+__global__ void k_max_norm(const float* __restrict__ dx, uint32_t nv, unsigned int* __restrict__ out) {
+  float m = 0.f;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x) {
+    V3<float> d = ld3<float>(dx, i);
+    m = fmaxf(m, d.length());
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+}
+
+// analytic colliders: keep >= 20% of the current gap (implicit.rs:1795-1818)
+__global__ void k_ccd_colliders(const uint32_t* __restrict__ free_verts, uint32_t n_free, const float* __restrict__ x,
+                                const float* __restrict__ dx, const float* __restrict__ cols, uint32_t ncol,
+                                unsigned int* __restrict__ tmin) {
+  uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= n_free) return;
+  uint32_t i = free_verts[f];
+  V3<float> xi = ld3<float>(x, i), di = ld3<float>(dx, i);
+  const float GAP = 0.2f;
+  float t = 1.f;
+  for (uint32_t c = 0; c < ncol; ++c) {
+    const float* cc = cols + 8 * c;
+    V3<float> a(cc[1], cc[2], cc[3]);
+    float d0;
+    V3<float> n;
+    if (cc[0] == 0.f) {
+      n = V3<float>(cc[4], cc[5], cc[6]);
+      d0 = (xi - a).dot(n);
+    } else {
+      V3<float> v = xi - a;
+      float l = v.length();
+      if (l < 1e-9f) {
+        d0 = -cc[7];
+      } else {
+        d0 = l - cc[7];
+        n = v / l;
+      }
+    }
+    if (d0 <= 0.f) continue;
+    if (cc[0] == 0.f) {
+      float rate = di.dot(n);
+      if (rate < 0.f) t = fminf(t, (GAP - 1.0f) * d0 / rate);
+    } else {
+      float l = di.length();
+      if (l > 1e-12f) t = fminf(t, (1.0f - GAP) * d0 / l);
+    }
+  }
+  if (t < 1.f) atomic_min_pos(tmin, t);
+}
+
+template <class R>
+__global__ void k_ccd_vt(BvhView bv, const float* __restrict__ x, const float* __restrict__ dx,
+                         const uint32_t* __restrict__ tris, const uint8_t* __restrict__ ctri,
+                         const float* __restrict__ im, const uint32_t* __restrict__ ex_ptr,
+                         const uint32_t* __restrict__ ex_list, const unsigned long long* __restrict__ best,
+                         const float* __restrict__ pn, int has_static, uint32_t nv, float search, float dhat,
+                         uint32_t max_iter, unsigned int* __restrict__ tmin, unsigned int* __restrict__ caps,
+                         uint32_t* __restrict__ status) {
+  uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  float4 lo, hi;
+  point_box(x, v, search, lo, hi);
+  bool vmov = im[v] > 0.f;
+  float side = 2.f;
+  float tloc = 1.f;
+  uint32_t ncap = 0;
+  bool ok = visit(bv, lo, hi, [&](uint32_t t) {
+    uint32_t a = tris[3 * t], b = tris[3 * t + 1], c = tris[3 * t + 2];
+    bool tmov = im[a] > 0.f || im[b] > 0.f || im[c] > 0.f;
+    if (!tmov && !vmov) return;
+    if (excluded(ex_ptr, ex_list, v, a, b, c)) return;
+    if (has_static && ctri[t]) {
+      if (side == 2.f) side = side_of(v, best, x, tris, pn, dhat);
+      if (side < 0.f) return;
+    }
+    uint32_t idx[4] = {v, a, b, c};
+    V3<R> x0[4], dd[4];
+    for (int k = 0; k < 4; ++k) {
+      x0[k] = ld3<R>(x, idx[k]);
+      dd[k] = ld3<R>(dx, idx[k]);
+    }
+    bool cap = false;
+    R toi = accd_toi<R>(x0, dd, R(0), R(1.25), R(0.01), max_iter, 0, &cap);
+    ncap += cap ? 1u : 0u;
+    tloc = fminf(tloc, (float)(toi / R(1.25)));
+  });
+  if (!ok) atomicOr(status, ST_STACK_OVERFLOW);
+  if (tloc < 1.f) atomic_min_pos(tmin, tloc);
+  if (ncap) atomicAdd(caps, ncap);
+}
+
+template <class R>
+__global__ void k_ccd_ee(BvhView bv, const float* __restrict__ x, const float* __restrict__ dx,
+                         const uint32_t* __restrict__ edges, const float* __restrict__ im, uint32_t ne, float search,
+                         uint32_t max_iter, unsigned int* __restrict__ tmin, unsigned int* __restrict__ caps,
+                         uint32_t* __restrict__ status) {
+  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ne) return;
+  uint32_t b0 = edges[2 * j], b1 = edges[2 * j + 1];
+  float4 lo, hi;
+  edge_box(x, b0, b1, search, lo, hi);
+  bool jmov = im[b0] > 0.f || im[b1] > 0.f;
+  float tloc = 1.f;
+  uint32_t ncap = 0;
+  bool ok = visit(bv, lo, hi, [&](uint32_t i) {
+    if (i >= j) return;
+    uint32_t a0 = edges[2 * i], a1 = edges[2 * i + 1];
+    if (!(jmov || im[a0] > 0.f || im[a1] > 0.f)) return;
+    if (a0 == b0 || a0 == b1 || a1 == b0 || a1 == b1) return;
+    uint32_t idx[4] = {a0, a1, b0, b1};
+    V3<R> x0[4], dd[4];
+    for (int k = 0; k < 4; ++k) {
+      x0[k] = ld3<R>(x, idx[k]);
+      dd[k] = ld3<R>(dx, idx[k]);
+    }
+    bool cap = false;
+    R toi = accd_toi<R>(x0, dd, R(0), R(1.25), R(0.01), max_iter, 1, &cap);
+    ncap += cap ? 1u : 0u;
+    tloc = fminf(tloc, (float)(toi / R(1.25)));
+  });
+  if (!ok) atomicOr(status, ST_STACK_OVERFLOW);
+  if (tloc < 1.f) atomic_min_pos(tmin, tloc);
+  if (ncap) atomicAdd(caps, ncap);
+}
+
+// ccd_max_step (implicit.rs:1690-1947) without strain limiting or pins. The search
+// direction is s.dx; red[0] = max |dx|, red[1] = collider t, red[2] = self t, red[3] = caps.
+int ccd_step(Scene& s, float* t_out, uint32_t* cap_hits) {
+  cudaStream_t st = s.st;
+  if (s.n_col == 0 && !s.p.self_collision) {
+    *t_out = 1.f;
+    return MGUSO_OK;
+  }
+  unsigned int init[4] = {0u, f2u_host(1.f), 0u, 0u};
+  MG_CUDA(cudaMemcpyAsync(s.red.p, init, sizeof(init), cudaMemcpyHostToDevice, st));
+  int sms = s.ctx->sm_count;
+  k_max_norm<<<std::min<uint32_t>(ceil_div(s.nv, 256), sms * 4), 256, 0, st>>>(s.dx.p, s.nv, s.red.p);
+  if (s.n_col && s.n_free)
+    k_ccd_colliders<<<ceil_div(s.n_free, 128), 128, 0, st>>>(s.free_verts.p, s.n_free, s.x.p, s.dx.p, s.colliders.p,
+                                                           s.n_col, s.red.p + 1);
+  MG_CUDA(cudaGetLastError());
+  unsigned int h[4];
+  MG_CUDA(cudaMemcpyAsync(h, s.red.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+  MG_CUDA(cudaStreamSynchronize(st));
+  float max_disp = u2f_host(h[0]);
+  float t = u2f_host(h[1]);
+  if (s.p.self_collision) {
+    const float dhat = s.p.contact_dhat;
+    const float fixed = dhat;  // max_edge_gap() + 2 * max_edge_offset() for face edges
+    float allowed = std::max(std::min(0.5f * s.char_len, max_disp), 1.0e-9f);
+    uint32_t iters = std::max<uint32_t>(s.p.ccd_max_iter, 1);
+    BvhView tv = view(s.tri_bvh), ev = view(s.edge_bvh);
+    for (int pass = 0; pass < 64; ++pass) {
+      bool full = allowed >= max_disp;
+      float search = fixed + 2.0f * allowed;
+      unsigned int one = f2u_host(1.f);
+      MG_CUDA(cudaMemcpyAsync(s.red.p + 2, &one, 4, cudaMemcpyHostToDevice, st));
+      if (s.mixed) {
+        k_ccd_vt<double><<<ceil_div(s.nv, 128), 128, 0, st>>>(
+            tv, s.x.p, s.dx.p, s.tris.p, s.collider_tri.p, s.inv_mass.p, s.ex_ptr.p, s.ex_list.p, s.side_best.p,
+            s.collider_pn.p, s.has_static ? 1 : 0, s.nv, search, dhat, iters, s.red.p + 2, s.red.p + 3, s.status.p);
+        if (s.n_edge)
+          k_ccd_ee<double><<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, s.x.p, s.dx.p, s.edges.p, s.inv_mass.p,
+                                                                   s.n_edge, search, iters, s.red.p + 2, s.red.p + 3,
+                                                                   s.status.p);
+      } else {
+        k_ccd_vt<float><<<ceil_div(s.nv, 128), 128, 0, st>>>(
+            tv, s.x.p, s.dx.p, s.tris.p, s.collider_tri.p, s.inv_mass.p, s.ex_ptr.p, s.ex_list.p, s.side_best.p,
+            s.collider_pn.p, s.has_static ? 1 : 0, s.nv, search, dhat, iters, s.red.p + 2, s.red.p + 3, s.status.p);
+        if (s.n_edge)
+          k_ccd_ee<float><<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, s.x.p, s.dx.p, s.edges.p, s.inv_mass.p,
+                                                                  s.n_edge, search, iters, s.red.p + 2, s.red.p + 3,
+                                                                  s.status.p);
+      }
+      MG_CUDA(cudaGetLastError());
+      unsigned int hs[2];
+      MG_CUDA(cudaMemcpyAsync(hs, s.red.p + 2, 8, cudaMemcpyDeviceToHost, st));
+      MG_CUDA(cudaStreamSynchronize(st));
+      float t_self = u2f_host(hs[0]);
+      *cap_hits = hs[1];
+      if (full || t_self * max_disp <= allowed) {
+        t = std::min(t, t_self);
+        break;
+      }
+      allowed = std::min(allowed * 4.0f, max_disp);
+    }
+  }
+  *t_out = std::min(std::max(t, 0.f), 1.f);
+  return MGUSO_OK;
+}
+
+}  // namespace mg

@@ -131,6 +131,25 @@ struct DotSink {
 
 constexpr int MAX_PARTIALS = 4096;
 
+// Device vectors, scalars and the cached CUDA graph of one PCG operator.
+struct PcgWork {
+  uint32_t n = 0;
+  DevBuf<float> b, x, r, z, p, ap;
+  DevBuf<PcgScalars> sc;
+  DevBuf<double> partials;
+  PcgScalars* h_sc = nullptr;  // pinned
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint64_t graph_key = 0;
+  bool graph_mixed = false;
+  int reserve(uint32_t n);
+  void drop_graph();
+  PcgWork() = default;
+  PcgWork(const PcgWork&) = delete;
+  PcgWork& operator=(const PcgWork&) = delete;
+  ~PcgWork();
+};
+
 }  // namespace mg
 
 struct mguso_linear_solver {
@@ -143,10 +162,8 @@ struct mguso_linear_solver {
   std::unique_ptr<mguso_bsr> bsr;
   std::unique_ptr<mguso_schwarz> schwarz;
   mg::DevBuf<float> bjinv;  // 9 per vertex (block Jacobi)
-  mg::DevBuf<float> b, x, r, z, p, ap;
-  mg::DevBuf<mg::PcgScalars> sc;
-  mg::DevBuf<double> partials;
-  mg::PcgScalars* h_sc = nullptr;  // pinned
+  mg::PcgWork work;
+  uint64_t generation = 0;         // bumped whenever the pattern is rebuilt
   std::vector<uint32_t> map_val;   // scalar CSR entry -> BSR value slot
   std::vector<float> h_val;
 };

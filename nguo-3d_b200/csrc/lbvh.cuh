@@ -49,3 +49,57 @@ struct mguso_lbvh {
   mg::DevBuf<float> hpos;
   mg::DevBuf<uint32_t> htris, hpairs;
 };
+
+namespace mg {
+
+// Visits every leaf whose box overlaps [qlo, qhi] (the predicate of
+// bvh_traverse.wgsl:64-92), calling f(leaf_primitive). 64-entry stack; returns false on
+// stack overflow.
+template <class F>
+__device__ __forceinline__ bool lbvh_visit(const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
+                                           const float4* __restrict__ node, const float4* __restrict__ leaf,
+                                           const uint32_t* __restrict__ prim, uint32_t nt, float4 qlo, float4 qhi,
+                                           F&& f) {
+  auto ov = [&](const float4& lo, const float4& hi) {
+    return qlo.x <= hi.x && qlo.y <= hi.y && qlo.z <= hi.z && lo.x <= qhi.x && lo.y <= qhi.y && lo.z <= qhi.z;
+  };
+  if (nt == 0) return true;
+  if (nt == 1) {
+    if (ov(leaf[0], leaf[1])) f(prim[0]);
+    return true;
+  }
+  if (!ov(__ldg(node), __ldg(node + 1))) return true;
+  uint32_t stack[64];
+  int sp = 0;
+  uint32_t cur = 0;
+  bool ok = true;
+  for (;;) {
+    uint32_t ch[2] = {__ldg(left + cur), __ldg(right + cur)};
+    uint32_t next = 0xffffffffu;
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      uint32_t x = ch[c];
+      const float4* b = (x & 0x80000000u) ? leaf + 2 * (x & 0x7fffffffu) : node + 2 * x;
+      if (!ov(__ldg(b), __ldg(b + 1))) continue;
+      if (x & 0x80000000u) {
+        f(prim[x & 0x7fffffffu]);
+      } else if (next == 0xffffffffu) {
+        next = x;
+      } else if (sp < 64) {
+        stack[sp++] = x;
+      } else {
+        ok = false;
+      }
+    }
+    if (next != 0xffffffffu) {
+      cur = next;
+    } else if (sp > 0) {
+      cur = stack[--sp];
+    } else {
+      break;
+    }
+  }
+  return ok;
+}
+
+}  // namespace mg

@@ -8,11 +8,12 @@
 // Every dot product is fused into the kernel producing its operand and reduced
 // deterministically (per-CTA partials summed in index order by the last CTA), which also
 // computes alpha/beta/residual on the device. Kernels after convergence exit at entry, so
-// the host launches CHECK iterations (captured once as a CUDA graph) between reads of the
-// done flag.
+// the host replays a CUDA graph of CHECK iterations between reads of the done flag; the
+// graph is captured once per operator and kept until its buffers change.
 #include <algorithm>
 #include <cstring>
 
+#include "pcg.cuh"
 #include "reduce.cuh"
 
 namespace mg {
@@ -86,124 +87,156 @@ __global__ void k_bj_apply(const float* __restrict__ inv, const float* __restric
   if (with_dot) grid_dot_commit<Acc>(d, acc);
 }
 
-static int vec_grid(uint32_t n, int threads, int sms) {
+int vec_grid(uint32_t n, int threads, int sms) {
   return (int)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div(n, threads), (uint64_t)sms * 8));
 }
 
-static int precond_apply(mguso_linear_solver* s, const float* r, float* z, cudaStream_t st, const DotSink* d) {
-  if (s->precond == MGUSO_PRECOND_SCHWARZ) return schwarz_apply(s->schwarz.get(), r, z, st, d);
-  uint32_t nb = s->bsr->nb;
-  int grid = vec_grid(nb, 256, s->ctx->sm_count);
+int bj_apply(const float* inv, const float* r, float* z, uint32_t nb, int sms, cudaStream_t st, const DotSink* d) {
+  int grid = vec_grid(nb, 256, sms);
   DotSink dd = d ? *d : DotSink{};
   if (d && d->mixed)
-    k_bj_apply<double><<<grid, 256, 0, st>>>(s->bjinv.p, r, z, nb, dd, d ? 1 : 0);
+    k_bj_apply<double><<<grid, 256, 0, st>>>(inv, r, z, nb, dd, d ? 1 : 0);
   else
-    k_bj_apply<float><<<grid, 256, 0, st>>>(s->bjinv.p, r, z, nb, dd, d ? 1 : 0);
+    k_bj_apply<float><<<grid, 256, 0, st>>>(inv, r, z, nb, dd, d ? 1 : 0);
   MG_CUDA(cudaGetLastError());
   return MGUSO_OK;
 }
 
-int pcg_solve(mguso_linear_solver* s, float tol, uint32_t max_iter, mguso_lin_stats* out) {
-  cudaStream_t st = s->ctx->stream;
-  mguso_bsr* a = s->bsr.get();
-  const uint32_t n = 3 * a->nb;
-  const bool mixed = s->precision == MGUSO_PRECISION_MIXED;
-  const int sms = s->ctx->sm_count;
-  if (!s->h_sc) MG_CUDA(cudaMallocHost((void**)&s->h_sc, sizeof(PcgScalars)));
-  MG_TRY(s->sc.reserve(1));
-  MG_TRY(s->partials.reserve(MAX_PARTIALS));
-  MG_TRY(s->x.reserve(n));
-  MG_TRY(s->r.reserve(n));
-  MG_TRY(s->z.reserve(n));
-  MG_TRY(s->p.reserve(n));
-  MG_TRY(s->ap.reserve(n));
+int PcgWork::reserve(uint32_t n_) {
+  n = n_;
+  if (!h_sc) MG_CUDA(cudaMallocHost((void**)&h_sc, sizeof(PcgScalars)));
+  size_t before = (size_t)b.p + (size_t)x.p + (size_t)r.p + (size_t)z.p + (size_t)p.p + (size_t)ap.p;
+  MG_TRY(sc.reserve(1));
+  MG_TRY(partials.reserve(MAX_PARTIALS));
+  MG_TRY(b.reserve(n));
+  MG_TRY(x.reserve(n));
+  MG_TRY(r.reserve(n));
+  MG_TRY(z.reserve(n));
+  MG_TRY(p.reserve(n));
+  MG_TRY(ap.reserve(n));
+  size_t after = (size_t)b.p + (size_t)x.p + (size_t)r.p + (size_t)z.p + (size_t)p.p + (size_t)ap.p;
+  if (before != after) drop_graph();
+  return MGUSO_OK;
+}
+
+void PcgWork::drop_graph() {
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  exec = nullptr;
+  graph = nullptr;
+}
+
+PcgWork::~PcgWork() {
+  drop_graph();
+  if (h_sc) cudaFreeHost(h_sc);
+}
+
+int pcg_run(const PcgOps& ops, PcgWork& w, float tol, uint32_t max_iter, mguso_lin_stats* out) {
+  cudaStream_t st = ops.stream;
+  const uint32_t n = w.n;
+  const bool mixed = ops.mixed;
+  const int sms = ops.sms;
   PcgScalars h{};
   h.tol = tol;
   h.max_iter = max_iter;
-  MG_CUDA(cudaMemcpyAsync(s->sc.p, &h, sizeof(h), cudaMemcpyHostToDevice, st));
-  auto sink = [&](int fin) { return DotSink{s->sc.p, s->partials.p, fin, mixed}; };
+  MG_CUDA(cudaMemcpyAsync(w.sc.p, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+  auto sink = [&](int fin) { return DotSink{w.sc.p, w.partials.p, fin, mixed}; };
   const int vg = vec_grid(n, 256, sms);
 
   DotSink d0 = sink(FIN_BNORM);
   if (mixed)
-    k_pcg_init<double><<<vg, 256, 0, st>>>(s->b.p, s->x.p, s->r.p, n, d0);
+    k_pcg_init<double><<<vg, 256, 0, st>>>(w.b.p, w.x.p, w.r.p, n, d0);
   else
-    k_pcg_init<float><<<vg, 256, 0, st>>>(s->b.p, s->x.p, s->r.p, n, d0);
+    k_pcg_init<float><<<vg, 256, 0, st>>>(w.b.p, w.x.p, w.r.p, n, d0);
   MG_CUDA(cudaGetLastError());
   DotSink d1 = sink(FIN_RZ0);
-  MG_TRY(precond_apply(s, s->r.p, s->z.p, st, &d1));
+  MG_TRY(ops.precond(w.r.p, w.z.p, st, &d1));
   DotSink d2 = sink(FIN_RR0);
   if (mixed)
-    k_copy_dot<double><<<vg, 256, 0, st>>>(s->z.p, s->p.p, s->r.p, n, d2);
+    k_copy_dot<double><<<vg, 256, 0, st>>>(w.z.p, w.p.p, w.r.p, n, d2);
   else
-    k_copy_dot<float><<<vg, 256, 0, st>>>(s->z.p, s->p.p, s->r.p, n, d2);
+    k_copy_dot<float><<<vg, 256, 0, st>>>(w.z.p, w.p.p, w.r.p, n, d2);
   MG_CUDA(cudaGetLastError());
 
   const uint32_t CHECK = 16;
   DotSink dp = sink(FIN_PAP), dr = sink(FIN_RR), dz = sink(FIN_RZ);
   auto one_iter = [&]() -> int {
-    MG_TRY(bsr_spmv(a, s->p.p, s->ap.p, st, &dp));
+    MG_TRY(ops.spmv(w.p.p, w.ap.p, st, &dp));
     if (mixed)
-      k_pcg_update<double><<<vg, 256, 0, st>>>(s->x.p, s->r.p, s->p.p, s->ap.p, n, dr);
+      k_pcg_update<double><<<vg, 256, 0, st>>>(w.x.p, w.r.p, w.p.p, w.ap.p, n, dr);
     else
-      k_pcg_update<float><<<vg, 256, 0, st>>>(s->x.p, s->r.p, s->p.p, s->ap.p, n, dr);
+      k_pcg_update<float><<<vg, 256, 0, st>>>(w.x.p, w.r.p, w.p.p, w.ap.p, n, dr);
     MG_CUDA(cudaGetLastError());
-    MG_TRY(precond_apply(s, s->r.p, s->z.p, st, &dz));
-    k_pcg_pupdate<<<vg, 256, 0, st>>>(s->p.p, s->z.p, n, s->sc.p);
+    MG_TRY(ops.precond(w.r.p, w.z.p, st, &dz));
+    k_pcg_pupdate<<<vg, 256, 0, st>>>(w.p.p, w.z.p, n, w.sc.p);
     MG_CUDA(cudaGetLastError());
     return MGUSO_OK;
   };
-  // Capture CHECK iterations once as a graph; replay until the done flag is set.
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  bool use_graph = max_iter > CHECK;
-  if (use_graph) {
+  bool use_graph = max_iter >= CHECK && ops.graphable;
+  if (use_graph && (!w.exec || w.graph_key != ops.key || w.graph_mixed != mixed)) {
+    w.drop_graph();
     MG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     int rc = MGUSO_OK;
     for (uint32_t i = 0; i < CHECK && rc == MGUSO_OK; ++i) rc = one_iter();
-    cudaError_t e = cudaStreamEndCapture(st, &graph);
-    if (rc != MGUSO_OK) return rc;
+    cudaError_t e = cudaStreamEndCapture(st, &w.graph);
+    if (rc != MGUSO_OK) {
+      if (w.graph) cudaGraphDestroy(w.graph);
+      w.graph = nullptr;
+      return rc;
+    }
     MG_CUDA(e);
-    MG_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+    MG_CUDA(cudaGraphInstantiate(&w.exec, w.graph, 0));
+    w.graph_key = ops.key;
+    w.graph_mixed = mixed;
   }
   uint32_t launched = 0;
-  int rc = MGUSO_OK;
   while (launched < max_iter) {
     if (use_graph && max_iter - launched >= CHECK) {
-      cudaError_t e = cudaGraphLaunch(exec, st);
-      if (e != cudaSuccess) {
-        set_error(std::string("cudaGraphLaunch: ") + cudaGetErrorString(e));
-        rc = MGUSO_ERR_CUDA;
-        break;
-      }
+      MG_CUDA(cudaGraphLaunch(w.exec, st));
       launched += CHECK;
     } else {
       uint32_t k = std::min<uint32_t>(CHECK, max_iter - launched);
-      for (uint32_t i = 0; i < k && rc == MGUSO_OK; ++i) rc = one_iter();
-      if (rc != MGUSO_OK) break;
+      for (uint32_t i = 0; i < k; ++i) MG_TRY(one_iter());
       launched += k;
     }
-    cudaError_t e = cudaMemcpyAsync(s->h_sc, s->sc.p, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) {
-      set_error(std::string("pcg sync: ") + cudaGetErrorString(e));
-      rc = MGUSO_ERR_CUDA;
-      break;
-    }
-    if (s->h_sc->done) break;
+    MG_CUDA(cudaMemcpyAsync(w.h_sc, w.sc.p, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+    MG_CUDA(cudaStreamSynchronize(st));
+    if (w.h_sc->done) break;
   }
-  if (exec) cudaGraphExecDestroy(exec);
-  if (graph) cudaGraphDestroy(graph);
-  if (rc != MGUSO_OK) return rc;
-  MG_CUDA(cudaMemcpyAsync(s->h_sc, s->sc.p, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
+  MG_CUDA(cudaMemcpyAsync(w.h_sc, w.sc.p, sizeof(PcgScalars), cudaMemcpyDeviceToHost, st));
   MG_CUDA(cudaStreamSynchronize(st));
   if (out) {
-    out->iters = s->h_sc->iters;
-    out->residual = s->h_sc->residual;
-    out->status = (s->h_sc->residual <= tol) ? MGUSO_OK : MGUSO_ERR_PCG_CAP;
-    if (s->h_sc->status & ST_PCG_BREAKDOWN) out->status = MGUSO_OK;
+    out->iters = w.h_sc->iters;
+    out->residual = w.h_sc->residual;
+    out->status = (w.h_sc->residual <= tol || (w.h_sc->status & ST_PCG_BREAKDOWN)) ? MGUSO_OK : MGUSO_ERR_PCG_CAP;
   }
   return MGUSO_OK;
+}
+
+// The LinearSolver entry point's system: the solver's own BSR and preconditioner.
+int pcg_solve(mguso_linear_solver* s, float tol, uint32_t max_iter, mguso_lin_stats* out) {
+  mguso_bsr* a = s->bsr.get();
+  MG_TRY(s->work.reserve(3 * a->nb));
+  PcgOps ops;
+  ops.stream = s->ctx->stream;
+  ops.mixed = s->precision == MGUSO_PRECISION_MIXED;
+  ops.sms = s->ctx->sm_count;
+  ops.key = (uint64_t)(uintptr_t)a ^ ((uint64_t)a->val.p << 1) ^ ((uint64_t)s->precond << 60) ^ s->generation;
+  ops.spmv = [a](const float* p, float* ap, cudaStream_t st, const DotSink* d) { return bsr_spmv(a, p, ap, st, d); };
+  if (s->precond == MGUSO_PRECOND_SCHWARZ) {
+    mguso_schwarz* sw = s->schwarz.get();
+    ops.precond = [sw](const float* r, float* z, cudaStream_t st, const DotSink* d) {
+      return schwarz_apply(sw, r, z, st, d);
+    };
+  } else {
+    const float* inv = s->bjinv.p;
+    uint32_t nb = a->nb;
+    int sms = ops.sms;
+    ops.precond = [inv, nb, sms](const float* r, float* z, cudaStream_t st, const DotSink* d) {
+      return bj_apply(inv, r, z, nb, sms, st, d);
+    };
+  }
+  return pcg_run(ops, s->work, tol, max_iter, out);
 }
 
 }  // namespace mg

@@ -1,0 +1,551 @@
+// Scene construction (host): topology, rest state, block patterns and push-order gather
+// lists for the implicit step, plus the scene half of the C ABI.
+//
+// Rest quantities are computed in f32 in the reference's operation order:
+//   ImplicitSolver::new (implicit.rs:530-601): hinges, 1-ring exclusion, unique edges,
+//     characteristic edge length;
+//   SimState::from_mesh (state.rs:37-61): stretch springs on the unique edges;
+//   build_shells (shell_model.rs:310-348): in-plane frame, Dm^-1, rest area;
+//   set_static_collider_verts (implicit.rs:1258-1320): winding check and angle-weighted
+//     pseudonormals (contact.rs:963-1001).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <unordered_map>
+
+#include "elements.cuh"
+#include "scene.cuh"
+
+namespace mg {
+
+namespace {
+
+using HV = V3<float>;
+
+HV hp(const float* p, uint32_t i) { return HV(p[3 * i], p[3 * i + 1], p[3 * i + 2]); }
+
+float host_dihedral(const HV p[4]) {
+  HV n1 = (p[1] - p[0]).cross(p[2] - p[0]);
+  HV n2 = (p[1] - p[2]).cross(p[3] - p[2]);
+  HV e = (p[2] - p[1]).normalize_or_zero();
+  HV n1n = n1.normalize_or_zero(), n2n = n2.normalize_or_zero();
+  float s = n1n.cross(n2n).dot(e);
+  float c = n1n.dot(n2n);
+  c = c < -1.f ? -1.f : (c > 1.f ? 1.f : c);
+  return std::atan2(s, c);
+}
+
+struct Contribution {
+  uint32_t row, col;
+};
+
+}  // namespace
+
+int scene_build(Scene& s, const mguso_scene_desc* d) {
+  MG_CHECK_ARG(d && d->positions && d->inv_mass && (d->nt == 0 || d->tris), "scene: null arrays");
+  MG_CHECK_ARG(d->nv > 0 && d->nv < (1u << 30), "scene: vertex count out of range");
+  const uint32_t nv = d->nv, nt = d->nt;
+  for (uint32_t t = 0; t < 3 * nt; ++t) MG_CHECK_ARG(d->tris[t] < nv, "scene: triangle index out of range");
+  for (uint32_t t = 0; t < 3 * d->nshell; ++t) MG_CHECK_ARG(d->shell_faces[t] < nv, "scene: shell face index out of range");
+  for (uint32_t i = 0; i < d->nstitch; ++i) {
+    for (int k = 0; k < 6; ++k) MG_CHECK_ARG(d->stitch_idx[6 * i + k] < nv, "scene: stitch references a missing vertex");
+    const float* kl = d->stitch_kl + 3 * i;
+    MG_CHECK_ARG(std::isfinite(kl[0]) && kl[0] >= 0, "scene: stitch stiffness must be finite and >= 0");
+    MG_CHECK_ARG(std::isfinite(kl[1]) && kl[1] > 0, "scene: stitch rest length must be > 0");
+    MG_CHECK_ARG(std::isfinite(kl[2]) && kl[2] >= kl[1], "scene: stitch cap below its rest length");
+    float ws = d->stitch_w[6 * i] + d->stitch_w[6 * i + 1] + d->stitch_w[6 * i + 2];
+    float wt = d->stitch_w[6 * i + 3] + d->stitch_w[6 * i + 4] + d->stitch_w[6 * i + 5];
+    MG_CHECK_ARG(std::fabs(ws - 1.f) <= 1e-3f && std::fabs(wt - 1.f) <= 1e-3f, "scene: stitch weights must sum to 1 per side");
+  }
+  MG_CHECK_ARG(d->params.dt > 0, "scene: dt must be > 0");
+  MG_CHECK_ARG(d->params.precond == MGUSO_PRECOND_BLOCK_JACOBI || d->params.precond == MGUSO_PRECOND_SCHWARZ,
+               "scene: unknown preconditioner");
+  s.p = d->params;
+  s.nv = nv;
+  s.nt = nt;
+  s.mixed = d->params.precision == MGUSO_PRECISION_MIXED;
+  s.st = s.ctx->stream;
+  cudaStream_t st = s.st;
+  const float* P = d->positions;
+
+  // ---- state -------------------------------------------------------------------------
+  s.h_inv_mass.assign(d->inv_mass, d->inv_mass + nv);
+  s.h_pinned.resize(nv);
+  std::vector<uint32_t> free_verts;
+  for (uint32_t i = 0; i < nv; ++i) {
+    s.h_pinned[i] = s.h_inv_mass[i] <= 0.f;
+    if (!s.h_pinned[i]) free_verts.push_back(i);
+  }
+  s.n_free = (uint32_t)free_verts.size();
+  MG_TRY(s.x.upload(P, 3 * (size_t)nv, st));
+  std::vector<float> vel(3 * (size_t)nv, 0.f);
+  if (d->velocities) std::memcpy(vel.data(), d->velocities, 4 * vel.size());
+  MG_TRY(s.v.upload(vel.data(), vel.size(), st));
+  MG_TRY(s.x0.reserve(3 * (size_t)nv));
+  MG_TRY(s.xt.reserve(3 * (size_t)nv));
+  MG_TRY(s.xstep.reserve(3 * (size_t)nv));
+  MG_TRY(s.dx.reserve(3 * (size_t)nv));
+  MG_TRY(s.inv_mass.upload(s.h_inv_mass.data(), nv, st));
+  MG_TRY(s.pinned.upload(s.h_pinned.data(), nv, st));
+  if (free_verts.empty())
+    MG_TRY(s.free_verts.reserve(1));
+  else
+    MG_TRY(s.free_verts.upload(free_verts.data(), free_verts.size(), st));
+  auto vfree = [&](uint32_t v) { return !s.h_pinned[v]; };
+
+  // ---- topology ------------------------------------------------------------------------
+  std::vector<std::array<uint32_t, 3>> tris(nt);
+  for (uint32_t t = 0; t < nt; ++t) tris[t] = {d->tris[3 * t], d->tris[3 * t + 1], d->tris[3 * t + 2]};
+  // unique edges (geometry.rs:38-47 / broadphase.rs:334-346): sorted (min, max)
+  std::vector<std::array<uint32_t, 2>> edges;
+  edges.reserve(3 * nt);
+  for (auto& t : tris)
+    for (int k = 0; k < 3; ++k) {
+      uint32_t a = t[k], b = t[(k + 1) % 3];
+      edges.push_back({std::min(a, b), std::max(a, b)});
+    }
+  std::sort(edges.begin(), edges.end());
+  edges.erase(std::unique(edges.begin(), edges.end()), edges.end());
+  s.n_edge = (uint32_t)edges.size();
+  // characteristic length: mean unique-edge length, summed in order (implicit.rs:533-542)
+  if (edges.empty()) {
+    s.char_len = 1.f;
+  } else {
+    float sum = 0.f;
+    for (auto& e : edges) sum += (hp(P, e[0]) - hp(P, e[1])).length();
+    s.char_len = std::max(sum / (float)edges.size(), 1e-6f);
+  }
+  // hinges (bending.rs:126-158): sorted edge key -> opposite vertices in triangle order
+  std::map<std::pair<uint32_t, uint32_t>, std::vector<uint32_t>> em;
+  for (auto& t : tris) {
+    uint32_t e3[3][3] = {{t[1], t[2], t[0]}, {t[0], t[2], t[1]}, {t[0], t[1], t[2]}};
+    for (auto& x : e3) em[{std::min(x[0], x[1]), std::max(x[0], x[1])}].push_back(x[2]);
+  }
+  std::vector<uint32_t> hinge_v;
+  std::vector<float> hinge_rest;
+  if (s.p.bend_stiffness > 0) {
+    for (auto& kv : em) {
+      if (kv.second.size() != 2) continue;
+      uint32_t hv[4] = {kv.second[0], kv.first.first, kv.first.second, kv.second[1]};
+      HV pp[4] = {hp(P, hv[0]), hp(P, hv[1]), hp(P, hv[2]), hp(P, hv[3])};
+      for (uint32_t q : hv) hinge_v.push_back(q);
+      hinge_rest.push_back(host_dihedral(pp));
+    }
+  }
+  s.n_hinge = (uint32_t)hinge_rest.size();
+  // shells (shell_model.rs:310-348), StVK, per-scene (mu, lambda)
+  std::vector<uint32_t> shell_v;
+  std::vector<float> shell_dm, shell_area, shell_mu, shell_lam;
+  if (s.p.shell_mu > 0 || s.p.shell_lambda > 0) {
+    for (uint32_t f = 0; f < d->nshell; ++f) {
+      const uint32_t* fv = d->shell_faces + 3 * f;
+      HV p0 = hp(P, fv[0]), p1 = hp(P, fv[1]), p2 = hp(P, fv[2]);
+      HV e1 = p1 - p0, e2 = p2 - p0;
+      float area = 0.5f * e1.cross(e2).length();
+      if (area <= 1e-12f) continue;
+      HV ax = e1.normalize();
+      HV ay = (e2 - ax * e2.dot(ax)).normalize();
+      float xx = e1.dot(ax), xy = e1.dot(ay), yx = e2.dot(ax), yy = e2.dot(ay);
+      float det = xx * yy - yx * xy;
+      if (std::fabs(det) < 1e-20f) continue;
+      float inv = 1.f / det;
+      shell_v.insert(shell_v.end(), {fv[0], fv[1], fv[2]});
+      shell_dm.insert(shell_dm.end(), {yy * inv, xy * -inv, yx * -inv, xx * inv});
+      shell_area.push_back(area);
+      shell_mu.push_back(s.p.shell_mu);
+      shell_lam.push_back(s.p.shell_lambda);
+    }
+  }
+  s.n_shell = (uint32_t)shell_area.size();
+  // stretch springs on the unique edges (state.rs:37-61), rest = initial length. At zero
+  // stiffness every spring block and gradient entry is exactly 0, so they are left out.
+  std::vector<uint32_t> spring_v;
+  std::vector<float> spring_rest;
+  for (auto& e : s.p.stiffness != 0.f ? edges : std::vector<std::array<uint32_t, 2>>()) {
+    spring_v.insert(spring_v.end(), {e[0], e[1]});
+    spring_rest.push_back((hp(P, e[0]) - hp(P, e[1])).length());
+  }
+  s.n_spring = (uint32_t)spring_rest.size();
+  // stitches with stiffness > 0 (implicit.rs:2456-2485 skips the rest)
+  std::vector<uint32_t> stitch_idx;
+  std::vector<float> stitch_w, stitch_kl;
+  for (uint32_t i = 0; i < d->nstitch; ++i) {
+    if (!(d->stitch_kl[3 * i] > 0)) continue;
+    stitch_idx.insert(stitch_idx.end(), d->stitch_idx + 6 * i, d->stitch_idx + 6 * i + 6);
+    stitch_w.insert(stitch_w.end(), d->stitch_w + 6 * i, d->stitch_w + 6 * i + 6);
+    stitch_kl.insert(stitch_kl.end(), d->stitch_kl + 3 * i, d->stitch_kl + 3 * i + 3);
+  }
+  s.n_stitch = (uint32_t)(stitch_kl.size() / 3);
+
+  auto up = [&](auto& buf, const auto& vec) -> int {
+    if (vec.empty()) return buf.reserve(1);
+    return buf.upload(vec.data(), vec.size(), st);
+  };
+  MG_TRY(up(s.shell_v, shell_v));
+  MG_TRY(up(s.shell_dm, shell_dm));
+  MG_TRY(up(s.shell_area, shell_area));
+  MG_TRY(up(s.shell_mu, shell_mu));
+  MG_TRY(up(s.shell_lam, shell_lam));
+  MG_TRY(up(s.hinge_v, hinge_v));
+  MG_TRY(up(s.hinge_rest, hinge_rest));
+  MG_TRY(up(s.spring_v, spring_v));
+  MG_TRY(up(s.spring_rest, spring_rest));
+  MG_TRY(up(s.stitch_idx, stitch_idx));
+  MG_TRY(up(s.stitch_w, stitch_w));
+  MG_TRY(up(s.stitch_kl, stitch_kl));
+
+  // active (>= 1 free vertex) element lists
+  auto active = [&](const std::vector<uint32_t>& vv, uint32_t k, uint32_t n, std::vector<uint32_t>& out) {
+    out.clear();
+    for (uint32_t e = 0; e < n; ++e) {
+      bool a = false;
+      for (uint32_t q = 0; q < k; ++q) a = a || vfree(vv[k * e + q]);
+      if (a) out.push_back(e);
+    }
+  };
+  std::vector<uint32_t> act;
+  active(shell_v, 3, s.n_shell, act);
+  s.n_act_shell = (uint32_t)act.size();
+  MG_TRY(up(s.act_shell, act));
+  active(hinge_v, 4, s.n_hinge, act);
+  s.n_act_hinge = (uint32_t)act.size();
+  MG_TRY(up(s.act_hinge, act));
+  active(spring_v, 2, s.n_spring, act);
+  s.n_act_spring = (uint32_t)act.size();
+  MG_TRY(up(s.act_spring, act));
+  active(stitch_idx, 6, s.n_stitch, act);
+  s.n_act_stitch = (uint32_t)act.size();
+  MG_TRY(up(s.act_stitch, act));
+
+  // ---- contributions in push order (implicit.rs:2394-2740) ----------------------------
+  std::vector<Contribution> cb;   // block contributions
+  std::vector<uint32_t> gvert;    // gradient entry -> vertex
+  s.cb_inertia = cb.size();
+  s.gb_inertia = gvert.size();
+  for (uint32_t v : free_verts) {
+    cb.push_back({v, v});
+    gvert.push_back(v);
+  }
+  s.cb_stitch = cb.size();
+  s.gb_stitch = gvert.size();
+  for (uint32_t e = 0; e < s.n_stitch; ++e) {
+    const uint32_t* ix = stitch_idx.data() + 6 * e;
+    for (int a = 0; a < 6; ++a) gvert.push_back(ix[a]);
+    for (int a = 0; a < 6; ++a)
+      for (int b = 0; b < 6; ++b) cb.push_back({ix[a], ix[b]});
+  }
+  s.cb_spring = cb.size();
+  s.gb_spring = gvert.size();
+  for (uint32_t e = 0; e < s.n_spring; ++e) {
+    uint32_t a = spring_v[2 * e], b = spring_v[2 * e + 1];
+    gvert.push_back(a);
+    gvert.push_back(b);
+    cb.push_back({a, a});
+    cb.push_back({b, b});
+    cb.push_back({a, b});
+    cb.push_back({b, a});
+  }
+  s.cb_shell = cb.size();
+  s.gb_shell = gvert.size();
+  for (uint32_t e = 0; e < s.n_shell; ++e) {
+    const uint32_t* sv = shell_v.data() + 3 * e;
+    for (int a = 0; a < 3; ++a) gvert.push_back(sv[a]);
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) cb.push_back({sv[a], sv[b]});
+  }
+  s.cb_hinge = cb.size();
+  s.gb_hinge = gvert.size();
+  for (uint32_t e = 0; e < s.n_hinge; ++e) {
+    const uint32_t* hv = hinge_v.data() + 4 * e;
+    for (int a = 0; a < 4; ++a) gvert.push_back(hv[a]);
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b) cb.push_back({hv[a], hv[b]});
+  }
+  s.n_cblocks = cb.size();
+  s.n_gentries = gvert.size();
+
+  // ---- patterns -------------------------------------------------------------------------
+  auto key = [](uint32_t r, uint32_t c) { return ((uint64_t)r << 32) | c; };
+  std::vector<uint64_t> ks, kp;
+  ks.reserve(cb.size() + nv);
+  for (auto& c : cb) {
+    if (vfree(c.row) && vfree(c.col))
+      ks.push_back(key(c.row, c.col));
+    else
+      kp.push_back(key(c.row, c.col));
+  }
+  for (uint32_t v = 0; v < nv; ++v) ks.push_back(key(v, v));  // every vertex owns a diagonal block
+  std::sort(ks.begin(), ks.end());
+  ks.erase(std::unique(ks.begin(), ks.end()), ks.end());
+  std::sort(kp.begin(), kp.end());
+  kp.erase(std::unique(kp.begin(), kp.end()), kp.end());
+  auto to_pattern = [&](const std::vector<uint64_t>& k, BlockPattern& pat) {
+    pat.nnz = (uint32_t)k.size();
+    pat.h_row_ptr.assign(nv + 1, 0);
+    pat.h_col.resize(k.size());
+    for (size_t i = 0; i < k.size(); ++i) {
+      pat.h_row_ptr[(k[i] >> 32) + 1]++;
+      pat.h_col[i] = (uint32_t)k[i];
+    }
+    for (uint32_t v = 0; v < nv; ++v) pat.h_row_ptr[v + 1] += pat.h_row_ptr[v];
+  };
+  to_pattern(ks, s.Ps);
+  to_pattern(kp, s.Pp);
+  MG_TRY(s.Ps.row_ptr.upload(s.Ps.h_row_ptr.data(), nv + 1, st));
+  MG_TRY(up(s.Ps.col, s.Ps.h_col));
+  MG_TRY(s.Pp.row_ptr.upload(s.Pp.h_row_ptr.data(), nv + 1, st));
+  MG_TRY(up(s.Pp.col, s.Pp.h_col));
+  auto slot_of = [&](uint32_t r, uint32_t c) -> uint32_t {
+    bool sys = vfree(r) && vfree(c);
+    const BlockPattern& pat = sys ? s.Ps : s.Pp;
+    auto b = pat.h_col.begin() + pat.h_row_ptr[r], e = pat.h_col.begin() + pat.h_row_ptr[r + 1];
+    auto it = std::lower_bound(b, e, c);
+    uint32_t local = (uint32_t)(it - pat.h_col.begin());
+    return sys ? local : s.Ps.nnz + local;
+  };
+  // per-slot contribution lists in push order (counting sort on the slot)
+  uint32_t nslots = s.Ps.nnz + s.Pp.nnz;
+  std::vector<uint32_t> slot_ptr(nslots + 1, 0), slot_of_c(cb.size());
+  for (size_t i = 0; i < cb.size(); ++i) {
+    slot_of_c[i] = slot_of(cb[i].row, cb[i].col);
+    slot_ptr[slot_of_c[i] + 1]++;
+  }
+  for (uint32_t k = 0; k < nslots; ++k) slot_ptr[k + 1] += slot_ptr[k];
+  std::vector<uint32_t> cursor(slot_ptr.begin(), slot_ptr.end() - 1), slot_list(cb.size());
+  for (size_t i = 0; i < cb.size(); ++i) slot_list[cursor[slot_of_c[i]]++] = (uint32_t)i;
+  MG_TRY(up(s.slot_ptr, slot_ptr));
+  MG_TRY(up(s.slot_list, slot_list));
+  std::vector<uint32_t> gv_ptr(nv + 1, 0), gv_list(gvert.size());
+  for (uint32_t v : gvert) gv_ptr[v + 1]++;
+  for (uint32_t k = 0; k < nv; ++k) gv_ptr[k + 1] += gv_ptr[k];
+  std::vector<uint32_t> gcur(gv_ptr.begin(), gv_ptr.end() - 1);
+  for (size_t i = 0; i < gvert.size(); ++i) gv_list[gcur[gvert[i]]++] = (uint32_t)i;
+  MG_TRY(up(s.gv_ptr, gv_ptr));
+  MG_TRY(up(s.gv_list, gv_list));
+  std::vector<uint32_t> diag(nv);
+  for (uint32_t v = 0; v < nv; ++v) {
+    if (vfree(v)) {
+      diag[v] = slot_of(v, v);
+    } else {
+      auto b = s.Pp.h_col.begin() + s.Pp.h_row_ptr[v], e = s.Pp.h_col.begin() + s.Pp.h_row_ptr[v + 1];
+      auto it = std::lower_bound(b, e, v);
+      diag[v] = (it != e && *it == v) ? s.Ps.nnz + (uint32_t)(it - s.Pp.h_col.begin()) : 0xffffffffu;
+    }
+  }
+  MG_TRY(up(s.diag_slot, diag));
+  MG_TRY(s.cblocks.reserve(9 * std::max<uint64_t>(s.n_cblocks, 1)));
+  MG_TRY(s.gentries.reserve(3 * std::max<uint64_t>(s.n_gentries, 1)));
+  MG_CUDA(cudaMemsetAsync(s.cblocks.p, 0, 36 * std::max<uint64_t>(s.n_cblocks, 1), st));
+  MG_CUDA(cudaMemsetAsync(s.gentries.p, 0, 12 * std::max<uint64_t>(s.n_gentries, 1), st));
+  MG_TRY(s.valp.reserve(9 * (size_t)std::max<uint32_t>(s.Pp.nnz, 1)));
+  MG_TRY(s.grad.reserve(3 * (size_t)nv));
+  MG_TRY(s.rhs.reserve(3 * (size_t)nv));
+  // the system operator over Ps
+  s.A = std::make_unique<mguso_bsr>();
+  s.A->ctx = s.ctx;
+  std::vector<float> zeros(9 * (size_t)s.Ps.nnz, 0.f);
+  MG_TRY(bsr_upload(s.A.get(), nv, s.Ps.h_row_ptr, s.Ps.h_col, zeros.data()));
+  s.A->variant = SPMV_DIRECT;
+
+  // ---- colliders -------------------------------------------------------------------------
+  s.n_col = d->ncollider;
+  s.h_colliders.assign(d->colliders, d->colliders + 8 * (size_t)d->ncollider);
+  MG_TRY(up(s.colliders, s.h_colliders));
+
+  // ---- collision topology -------------------------------------------------------------------
+  if (nt)
+    MG_TRY(s.tris.upload(d->tris, 3 * (size_t)nt, st));
+  else
+    MG_TRY(s.tris.reserve(3));
+  std::vector<uint32_t> ev, etris;
+  for (auto& e : edges) {
+    ev.insert(ev.end(), {e[0], e[1]});
+    etris.insert(etris.end(), {e[0], e[1], e[1]});
+  }
+  MG_TRY(up(s.edges, ev));
+  MG_TRY(up(s.edge_tris, etris));
+  // 1-ring exclusion: the vertex and its triangle neighbours, sorted
+  std::vector<std::vector<uint32_t>> ex(nv);
+  for (uint32_t i = 0; i < nv; ++i) ex[i].push_back(i);
+  for (auto& t : tris)
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b)
+        if (a != b) ex[t[a]].push_back(t[b]);
+  std::vector<uint32_t> ex_ptr(nv + 1, 0), ex_list;
+  for (uint32_t i = 0; i < nv; ++i) {
+    std::sort(ex[i].begin(), ex[i].end());
+    ex[i].erase(std::unique(ex[i].begin(), ex[i].end()), ex[i].end());
+    ex_list.insert(ex_list.end(), ex[i].begin(), ex[i].end());
+    ex_ptr[i + 1] = (uint32_t)ex_list.size();
+  }
+  MG_TRY(up(s.ex_ptr, ex_ptr));
+  MG_TRY(up(s.ex_list, ex_list));
+  // static mesh collider: winding check + pseudonormals (implicit.rs:1258-1320)
+  std::vector<uint8_t> svert(nv, 0), ctri(std::max<uint32_t>(nt, 1), 0);
+  std::vector<float> pn(3 * (size_t)nv, 0.f);
+  s.has_static = false;
+  if (d->static_mask) {
+    HV lo(INFINITY, INFINITY, INFINITY), hi(-INFINITY, -INFINITY, -INFINITY);
+    std::vector<uint32_t> marked;
+    for (uint32_t t = 0; t < nt; ++t) {
+      auto& tv = tris[t];
+      if (!(d->static_mask[tv[0]] && d->static_mask[tv[1]] && d->static_mask[tv[2]])) continue;
+      for (uint32_t i : tv) {
+        HV q = hp(P, i);
+        lo = HV(std::min(lo.x, q.x), std::min(lo.y, q.y), std::min(lo.z, q.z));
+        hi = HV(std::max(hi.x, q.x), std::max(hi.y, q.y), std::max(hi.z, q.z));
+      }
+      marked.push_back(t);
+    }
+    if (!marked.empty()) {
+      HV e = hi - lo;
+      double box_vol = (double)(e.x * e.y * e.z);
+      HV mid = (lo + hi) * 0.5f;
+      double vol = 0.0;
+      for (uint32_t t : marked) {
+        HV a = hp(P, tris[t][0]) - mid, b = hp(P, tris[t][1]) - mid, c = hp(P, tris[t][2]) - mid;
+        vol += (double)a.cross(b).dot(c) / 6.0;
+      }
+      if (!(vol < -0.05 * box_vol)) {
+        s.has_static = true;
+        for (uint32_t i = 0; i < nv; ++i) svert[i] = d->static_mask[i] ? 1 : 0;
+        for (uint32_t t : marked) ctri[t] = 1;
+        // angle-weighted pseudonormals, welded on exact position bits (-0 folded to +0)
+        std::unordered_map<uint64_t, uint32_t> weld;
+        std::vector<HV> acc;
+        std::vector<uint32_t> of(nv);
+        auto bits = [](float c) { if (c == 0.f) c = 0.f; uint32_t b; std::memcpy(&b, &c, 4); return (uint64_t)b; };
+        std::map<std::array<uint64_t, 3>, uint32_t> wmap;
+        for (uint32_t i = 0; i < nv; ++i) {
+          std::array<uint64_t, 3> kk = {bits(P[3 * i]), bits(P[3 * i + 1]), bits(P[3 * i + 2])};
+          auto it = wmap.find(kk);
+          if (it == wmap.end()) {
+            uint32_t id = (uint32_t)wmap.size();
+            wmap.emplace(kk, id);
+            of[i] = id;
+          } else {
+            of[i] = it->second;
+          }
+        }
+        acc.assign(wmap.size(), HV());
+        for (uint32_t t : marked) {
+          HV q[3] = {hp(P, tris[t][0]), hp(P, tris[t][1]), hp(P, tris[t][2])};
+          HV face = (q[1] - q[0]).cross(q[2] - q[0]).normalize_or_zero();
+          if (face.x == 0.f && face.y == 0.f && face.z == 0.f) continue;
+          for (int k = 0; k < 3; ++k) {
+            HV u = (q[(k + 1) % 3] - q[k]).normalize_or_zero();
+            HV w = (q[(k + 2) % 3] - q[k]).normalize_or_zero();
+            float dt = u.dot(w);
+            dt = dt < -1.f ? -1.f : (dt > 1.f ? 1.f : dt);
+            acc[of[tris[t][k]]] += face * std::acos(dt);
+          }
+        }
+        for (uint32_t i = 0; i < nv; ++i) {
+          HV n = acc[of[i]].normalize_or_zero();
+          pn[3 * i] = n.x;
+          pn[3 * i + 1] = n.y;
+          pn[3 * i + 2] = n.z;
+        }
+      }
+    }
+  }
+  MG_TRY(up(s.static_vert, svert));
+  MG_TRY(up(s.collider_tri, ctri));
+  MG_TRY(up(s.collider_pn, pn));
+  s.tri_bvh.ctx = s.ctx;
+  s.edge_bvh.ctx = s.ctx;
+
+  // ---- working set -------------------------------------------------------------------------
+  s.cap_pairs = std::max<uint32_t>(1u << 16, 8 * nv);
+  s.cap_stencils = std::max<uint32_t>(1u << 14, 2 * nv);
+  MG_TRY(s.pairs.reserve(2 * (size_t)s.cap_pairs));
+  MG_TRY(s.counters.reserve(8));
+  MG_TRY(s.side_best.reserve(nv));
+  MG_TRY(s.red.reserve(16));
+  MG_TRY(s.status.reserve(4));
+  MG_CUDA(cudaMemsetAsync(s.status.p, 0, 16, st));
+  s.cap_c = std::max<uint32_t>(1u << 14, 4 * nv);
+  MG_TRY(s.c_row_ptr.reserve(nv + 1));
+  MG_TRY(s.c_count.reserve(4));
+  MG_CUDA(cudaMemsetAsync(s.c_row_ptr.p, 0, 4 * ((size_t)nv + 1), st));
+
+  // ---- linear solver ---------------------------------------------------------------------
+  if (s.p.precond == MGUSO_PRECOND_SCHWARZ) {
+    MG_CHECK_ARG(s.p.schwarz_domain >= 1 && s.p.schwarz_domain <= 32, "Schwarz domain size must be in [1, 32]");
+    s.schwarz = std::make_unique<mguso_schwarz>();
+    s.schwarz->a = s.A.get();
+    s.schwarz->domain = s.p.schwarz_domain;
+    MG_TRY(schwarz_build(s.schwarz.get()));
+  } else {
+    MG_TRY(s.bjinv.reserve(9 * (size_t)nv));
+  }
+  MG_TRY(s.work.reserve(3 * nv));
+  MG_CUDA(cudaStreamSynchronize(st));
+  return MGUSO_OK;
+}
+
+}  // namespace mg
+
+using namespace mg;
+
+extern "C" {
+
+int mguso_scene_create(mguso_ctx* ctx, const mguso_scene_desc* desc, mguso_scene** out) {
+  MG_CHECK_ARG(ctx && desc && out, "null argument");
+  MG_CUDA(cudaSetDevice(ctx->device));
+  auto sc = std::make_unique<mguso_scene>();
+  sc->s.ctx = ctx;
+  MG_TRY(scene_build(sc->s, desc));
+  *out = sc.release();
+  return MGUSO_OK;
+}
+
+int mguso_scene_destroy(mguso_scene* s) {
+  if (s) cudaStreamSynchronize(s->s.st);
+  delete s;
+  return MGUSO_OK;
+}
+
+int mguso_step(mguso_scene* sc, int nsteps, mguso_step_stats* stats) {
+  MG_CHECK_ARG(sc && nsteps >= 0, "bad argument");
+  MG_CUDA(cudaSetDevice(sc->s.ctx->device));
+  for (int k = 0; k < nsteps; ++k) {
+    mguso_step_stats st{};
+    MG_TRY(scene_step(sc->s, &st));
+    if (stats) stats[k] = st;
+  }
+  return MGUSO_OK;
+}
+
+static int copy_state(mguso_scene* sc, DevBuf<float>& buf, float* out, const float* in) {
+  MG_CHECK_ARG(sc && (out || in), "null argument");
+  size_t bytes = 12 * (size_t)sc->s.nv;
+  if (out) MG_CUDA(cudaMemcpyAsync(out, buf.p, bytes, cudaMemcpyDeviceToHost, sc->s.st));
+  if (in) MG_CUDA(cudaMemcpyAsync(buf.p, in, bytes, cudaMemcpyHostToDevice, sc->s.st));
+  MG_CUDA(cudaStreamSynchronize(sc->s.st));
+  return MGUSO_OK;
+}
+
+int mguso_read_positions(mguso_scene* s, float* out) { return copy_state(s, s->s.x, out, nullptr); }
+int mguso_write_positions(mguso_scene* s, const float* in) { return copy_state(s, s->s.x, nullptr, in); }
+int mguso_read_velocities(mguso_scene* s, float* out) { return copy_state(s, s->s.v, out, nullptr); }
+int mguso_write_velocities(mguso_scene* s, const float* in) { return copy_state(s, s->s.v, nullptr, in); }
+
+int mguso_scene_info(mguso_scene* sc, uint32_t* out6) {
+  MG_CHECK_ARG(sc && out6, "null argument");
+  Scene& s = sc->s;
+  uint32_t nct = 0;
+  std::vector<uint8_t> ct(std::max<uint32_t>(s.nt, 1));
+  MG_CUDA(cudaMemcpy(ct.data(), s.collider_tri.p, ct.size(), cudaMemcpyDeviceToHost));
+  for (uint32_t t = 0; t < s.nt; ++t) nct += ct[t];
+  out6[0] = s.n_hinge;
+  out6[1] = s.n_shell;
+  out6[2] = s.n_edge;
+  out6[3] = nct;
+  out6[4] = s.Ps.nnz;
+  out6[5] = s.Pp.nnz;
+  return MGUSO_OK;
+}
+
+}  // extern "C"

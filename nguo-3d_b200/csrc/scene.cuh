@@ -1,0 +1,150 @@
+// Device layout of one implicit-step scene.
+//
+// Positions, velocities and the Newton iterate are AoS f32[3*nv]. Element data is SoA per
+// kind. The Hessian lives in two fixed 3x3 block patterns built once from the topology:
+//   Ps: the system pattern, every block whose row and column vertices are both free, plus
+//       an identity diagonal block per pinned vertex (the Dirichlet filter of
+//       csr.rs:385-415, applied structurally);
+//   Pp: every block that touches a pinned vertex. It is never solved with; it holds the
+//       unfiltered elastic blocks the contact Rayleigh stiffness gathers
+//       (implicit.rs:755-795 reads the Hessian before the Dirichlet filter).
+// Each element writes its local 3x3 blocks into a contribution buffer at positions fixed
+// by the reference's push order (implicit.rs:2394-2740); a gather kernel then sums every
+// slot's contributions in that order, so the assembly is deterministic and needs no
+// atomics. Self-contact blocks that land outside Ps form a per-iteration block matrix C.
+#pragma once
+#include "lbvh.cuh"
+#include "pcg.cuh"
+
+namespace mg {
+
+struct Stencil {  // one active self-contact stencil (implicit.rs:678-753)
+  uint32_t idx[4];
+  uint32_t kind;    // 0 vertex-triangle, 1 edge-edge
+  uint32_t pad;
+  double d;         // gap (signed for static-collider triangles)
+  double ghat;
+  double g[12];     // distance gradient per participant
+};
+
+struct BlockPattern {
+  uint32_t nnz = 0;
+  std::vector<uint32_t> h_row_ptr, h_col;
+  DevBuf<uint32_t> row_ptr, col;
+};
+
+struct Scene {
+  mguso_ctx* ctx = nullptr;
+  cudaStream_t st = nullptr;
+  mguso_params p{};
+  uint32_t nv = 0, nt = 0;
+  bool mixed = true;
+
+  // state
+  std::vector<float> h_inv_mass;
+  std::vector<uint8_t> h_pinned;
+  DevBuf<float> x, x0, xt, v, xstep, inv_mass, dx;
+  DevBuf<uint8_t> pinned;
+  double time = 0.0;
+
+  // elements (device, SoA)
+  uint32_t n_free = 0, n_shell = 0, n_hinge = 0, n_spring = 0, n_stitch = 0;
+  DevBuf<uint32_t> free_verts;
+  DevBuf<uint32_t> shell_v;      // 3 per shell
+  DevBuf<float> shell_dm;        // 4 per shell (dm_inv, glam column-major)
+  DevBuf<float> shell_area, shell_mu, shell_lam;
+  DevBuf<uint32_t> hinge_v;      // 4 per hinge
+  DevBuf<float> hinge_rest;
+  DevBuf<uint32_t> spring_v;     // 2 per spring
+  DevBuf<float> spring_rest;
+  DevBuf<uint32_t> stitch_idx;   // 6 per stitch
+  DevBuf<float> stitch_w, stitch_kl;
+  // elements with at least one free vertex (recomputed every Newton iteration); the
+  // contributions of all-pinned elements are constant and computed once
+  uint32_t n_act_shell = 0, n_act_hinge = 0, n_act_spring = 0, n_act_stitch = 0;
+  DevBuf<uint32_t> act_shell, act_hinge, act_spring, act_stitch;
+  bool static_done = false;
+
+  // contribution buffers: blocks (9 floats) and gradient entries (3 floats)
+  uint64_t cb_inertia = 0, cb_stitch = 0, cb_spring = 0, cb_shell = 0, cb_hinge = 0, n_cblocks = 0;
+  uint64_t gb_inertia = 0, gb_stitch = 0, gb_spring = 0, gb_shell = 0, gb_hinge = 0, n_gentries = 0;
+  DevBuf<float> cblocks, gentries;
+
+  // patterns + gather lists (slot < Ps.nnz: Ps; else Pp)
+  BlockPattern Ps, Pp;
+  DevBuf<uint32_t> slot_ptr, slot_list;     // contributions per slot, push order
+  DevBuf<uint32_t> gv_ptr, gv_list;         // gradient entries per vertex, push order
+  DevBuf<uint32_t> diag_slot;               // per vertex: its diagonal slot (Ps if free, Pp if pinned)
+  std::unique_ptr<mguso_bsr> A;             // Ps values live in A->val
+  DevBuf<float> valp;                       // Pp values
+  DevBuf<float> grad, rhs;
+
+  // colliders
+  uint32_t n_col = 0;
+  std::vector<float> h_colliders;
+  DevBuf<float> colliders;
+
+  // collision topology
+  uint32_t n_edge = 0;
+  DevBuf<uint32_t> tris, edge_tris;         // edges as degenerate triangles (a, b, b)
+  DevBuf<uint32_t> edges;                   // 2 per edge
+  DevBuf<uint32_t> ex_ptr, ex_list;         // 1-ring exclusion (broadphase.rs:756-775)
+  DevBuf<uint8_t> static_vert, collider_tri;
+  bool has_static = false;
+  DevBuf<float> collider_pn;                // 3 per vertex
+  float char_len = 1.f;
+  Lbvh tri_bvh, edge_bvh;
+
+  // self-contact working set
+  uint32_t cap_pairs = 0, cap_stencils = 0;
+  DevBuf<uint32_t> pairs;                   // 2 per candidate
+  DevBuf<unsigned long long> counters;      // [0] vt pairs, [1] stencils, [2] ee candidates, [3] unique keys
+  DevBuf<unsigned long long> side_best;     // per vertex (d2 bits << 32 | tri)
+  DevBuf<Stencil> stencils, stencils_sorted;
+  DevBuf<unsigned long long> st_keys;
+  DevBuf<uint32_t> st_ids;
+  // contact contributions (32 blocks + 4 gradient entries per stencil)
+  DevBuf<float> ccblocks, cgentries;
+  DevBuf<unsigned long long> ckeys;
+  DevBuf<uint32_t> cids;
+  DevBuf<unsigned long long> gkeys;
+  DevBuf<uint32_t> gids;
+  // C: contact blocks outside Ps (rows sorted), device row pointers over all vertices
+  uint32_t cap_c = 0;
+  DevBuf<uint32_t> c_row_ptr, c_col, c_row;
+  DevBuf<float> c_val;
+  DevBuf<uint32_t> c_count;
+  DevBuf<uint32_t> is_new, rank, scan_tmp;
+
+  // reductions / CCD
+  DevBuf<unsigned int> red;                 // misc per-iteration reductions (float bits)
+  DevBuf<uint32_t> status;
+
+  // linear solve
+  std::unique_ptr<mguso_schwarz> schwarz;
+  DevBuf<float> bjinv;
+  PcgWork work;
+
+  std::vector<mguso_step_stats> history;
+};
+
+int scene_build(Scene& s, const mguso_scene_desc* d);
+int scene_step(Scene& s, mguso_step_stats* out);
+
+// assembly (assemble.cu)
+int assemble_elastic(Scene& s);
+int assemble_colliders(Scene& s);
+int assemble_contacts(Scene& s, uint32_t nst);
+int finish_rhs(Scene& s);
+int system_spmv(Scene& s, const float* p, float* ap, cudaStream_t st, const DotSink* d);
+
+// contact (contact.cu)
+int build_bvhs(Scene& s, const float* x);
+int collect_stencils(Scene& s, uint32_t* nst);
+int ccd_step(Scene& s, float* t_out, uint32_t* cap_hits);
+
+}  // namespace mg
+
+struct mguso_scene {
+  mg::Scene s;
+};

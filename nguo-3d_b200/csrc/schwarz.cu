@@ -18,6 +18,8 @@
 namespace mg {
 
 int schwarz_configure();
+int schwarz_factor_with(mguso_schwarz* s, const uint32_t* c_rp, const uint32_t* c_col, const float* c_val,
+                        cudaStream_t st);
 
 // ---------------------------------------------------------------------------------------
 // Host: BFS domains over the block pattern (linsolve.rs:152-173).
@@ -100,7 +102,8 @@ __global__ void __launch_bounds__(FACTOR_THREADS) k_schwarz_factor(
     const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ col, const float* __restrict__ val,
     const uint32_t* __restrict__ dom_start, const uint32_t* __restrict__ dom_verts,
     const uint32_t* __restrict__ dom_of, const uint32_t* __restrict__ loc, const uint64_t* __restrict__ fac_off,
-    float* __restrict__ fac, uint32_t* status) {
+    float* __restrict__ fac, uint32_t* status, const uint32_t* __restrict__ c_rp, const uint32_t* __restrict__ c_col,
+    const float* __restrict__ c_val) {
   extern __shared__ __align__(16) double sA[];
   __shared__ double s_floor;
   __shared__ int s_fail;
@@ -128,6 +131,21 @@ __global__ void __launch_bounds__(FACTOR_THREADS) k_schwarz_factor(
     }
   }
   __syncthreads();
+  // contact blocks outside the fixed pattern (distinct (row, col) from the loop above)
+  if (c_rp) {
+    for (uint32_t p = w; p < nvd; p += nw) {
+      uint32_t v = dom_verts[vs + p];
+      for (uint32_t k = c_rp[v] + lane; k < c_rp[v + 1]; k += 32) {
+        uint32_t c = c_col[k];
+        if (dom_of[c] != d) continue;
+        uint32_t q = loc[c];
+        const float* b = c_val + 9 * (size_t)k;
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) A[(3 * p + i) * ld + 3 * q + j] = (double)b[3 * i + j];
+      }
+    }
+    __syncthreads();
+  }
   if (tid == 0) {
     double tr = 0.0;
     for (int k = 0; k < m; ++k) tr += A[k * ld + k];
@@ -190,11 +208,17 @@ __global__ void __launch_bounds__(FACTOR_THREADS) k_schwarz_factor(
 }
 
 int schwarz_factor(mguso_schwarz* s, cudaStream_t st) {
+  return schwarz_factor_with(s, nullptr, nullptr, nullptr, st);
+}
+
+int schwarz_factor_with(mguso_schwarz* s, const uint32_t* c_rp, const uint32_t* c_col, const float* c_val,
+                        cudaStream_t st) {
   if (s->ndom == 0) return MGUSO_OK;
   mguso_bsr* a = s->a;
   size_t smem = sizeof(double) * 2 * (size_t)s->max_m * (s->max_m + 1);
   k_schwarz_factor<<<s->ndom, FACTOR_THREADS, smem, st>>>(a->row_ptr.p, a->col.p, a->val.p, s->dom_start.p, s->dom_verts.p,
-                                               s->dom_of.p, s->loc.p, s->fac_off.p, s->fac.p, s->status.p);
+                                               s->dom_of.p, s->loc.p, s->fac_off.p, s->fac.p, s->status.p,
+                                                          c_col ? c_rp : nullptr, c_col, c_val);
   MG_CUDA(cudaGetLastError());
   return MGUSO_OK;
 }

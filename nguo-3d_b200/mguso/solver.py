@@ -1,0 +1,155 @@
+"""Host-side mirror of the reference's solver API (scene build -> step -> readback).
+
+``ImplicitSolver`` mirrors engine_core::ImplicitSolver (core-engine/crates/engine-core/src/
+implicit.rs:372-2191) as built by Scene::build_implicit plus its set_* calls: construct it
+from a scene (positions, triangles, masses, shell faces, stitches, colliders, parameters),
+call ``step()``, read ``positions``. Every step runs on the GPU through the C ABI.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, ptr
+
+_PARAM_FIELDS = [("dt", C.c_float), ("gravity", C.c_float * 3), ("newton_iters", C.c_uint32),
+                 ("stiffness", C.c_float), ("bend_stiffness", C.c_float), ("max_dx", C.c_float),
+                 ("target_toi", C.c_float), ("min_newton_steps", C.c_uint32), ("ccd_max_iter", C.c_uint32),
+                 ("eiganalysis_eps", C.c_float), ("contact_dhat", C.c_float), ("contact_kappa", C.c_float),
+                 ("contact_dynamic", C.c_float), ("shell_mu", C.c_float), ("shell_lambda", C.c_float),
+                 ("friction", C.c_float), ("friction_eps", C.c_float), ("barrier_kind", C.c_int),
+                 ("contact_rayleigh", C.c_int), ("self_collision", C.c_int), ("cg_tol", C.c_float),
+                 ("cg_max_iter", C.c_uint32), ("floor_y", C.c_float), ("newton_tol", C.c_float),
+                 ("precond", C.c_int), ("schwarz_domain", C.c_uint32), ("precision", C.c_int)]
+
+
+class Params(C.Structure):
+    _fields_ = _PARAM_FIELDS
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("nv", C.c_uint32), ("positions", C.c_void_p), ("velocities", C.c_void_p),
+                ("inv_mass", C.c_void_p), ("nt", C.c_uint32), ("tris", C.c_void_p), ("static_mask", C.c_void_p),
+                ("nshell", C.c_uint32), ("shell_faces", C.c_void_p), ("nstitch", C.c_uint32),
+                ("stitch_idx", C.c_void_p), ("stitch_w", C.c_void_p), ("stitch_kl", C.c_void_p),
+                ("ncollider", C.c_uint32), ("colliders", C.c_void_p), ("params", Params)]
+
+
+class StepStats(C.Structure):
+    _fields_ = [("newton_iters", C.c_uint32), ("max_cg_iters", C.c_uint32), ("num_contacts", C.c_uint32),
+                ("stencils", C.c_uint32), ("ccd_cap_hits", C.c_uint32), ("max_reresid", C.c_double),
+                ("t_min", C.c_double), ("penetration_free", C.c_int), ("all_finite", C.c_int), ("status", C.c_int)]
+
+
+def _sigs(lib):
+    vp, i32 = C.c_void_p, C.c_int
+    P = C.POINTER
+    for name, res, args in [
+        ("mguso_scene_create", i32, [vp, P(SceneDesc), P(vp)]),
+        ("mguso_scene_destroy", i32, [vp]),
+        ("mguso_step", i32, [vp, i32, vp]),
+        ("mguso_read_positions", i32, [vp, vp]),
+        ("mguso_write_positions", i32, [vp, vp]),
+        ("mguso_read_velocities", i32, [vp, vp]),
+        ("mguso_write_velocities", i32, [vp, vp]),
+        ("mguso_scene_info", i32, [vp, vp]),
+    ]:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+def make_params(p: dict, precision: str = "mixed") -> Params:
+    s = Params()
+    for k, v in p.items():
+        if k == "gravity":
+            s.gravity[:] = list(v)
+        elif any(k == f for f, _ in _PARAM_FIELDS):
+            setattr(s, k, v)
+    s.precision = {"fp32": _lib.PRECISION_FP32, "mixed": _lib.PRECISION_MIXED}[precision]
+    return s
+
+
+class ImplicitSolver:
+    """One drape on the GPU (scene from ``mguso.scenes``)."""
+
+    def __init__(self, ctx, scene: dict, precision: str = "mixed"):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        _sigs(self.lib)
+        keep = {k: np.ascontiguousarray(scene[k]) for k in ("positions", "velocities", "inv_mass", "tris",
+                                                           "shell_faces", "stitch_idx", "stitch_w", "stitch_kl",
+                                                           "colliders")}
+        pos = keep["positions"].astype(np.float32, copy=False)
+        self.nv = pos.shape[0]
+        mask = scene.get("static_mask")
+        mask = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+        d = SceneDesc()
+        d.nv = self.nv
+        d.positions = ptr(pos)
+        d.velocities = ptr(keep["velocities"].astype(np.float32, copy=False))
+        d.inv_mass = ptr(keep["inv_mass"].astype(np.float32, copy=False))
+        d.nt = keep["tris"].shape[0]
+        d.tris = ptr(keep["tris"].astype(np.uint32, copy=False)) if d.nt else None
+        d.static_mask = ptr(mask) if mask is not None else None
+        d.nshell = keep["shell_faces"].shape[0]
+        d.shell_faces = ptr(keep["shell_faces"].astype(np.uint32, copy=False)) if d.nshell else None
+        d.nstitch = keep["stitch_idx"].shape[0]
+        d.stitch_idx = ptr(keep["stitch_idx"]) if d.nstitch else None
+        d.stitch_w = ptr(keep["stitch_w"]) if d.nstitch else None
+        d.stitch_kl = ptr(keep["stitch_kl"]) if d.nstitch else None
+        d.ncollider = keep["colliders"].shape[0]
+        d.colliders = ptr(keep["colliders"]) if d.ncollider else None
+        d.params = make_params(scene["params"], precision)
+        self._keep = (keep, mask, pos)
+        h = C.c_void_p()
+        check(self.lib.mguso_scene_create(ctx.h, C.byref(d), C.byref(h)))
+        self.h = h
+        self.history: list[dict] = []
+
+    def step(self, n: int = 1) -> list[dict]:
+        out = (StepStats * n)()
+        check(self.lib.mguso_step(self.h, n, out))
+        st = [{f: getattr(o, f) for f, _ in StepStats._fields_} for o in out]
+        self.history += st
+        return st
+
+    @property
+    def positions(self) -> np.ndarray:
+        out = np.empty((self.nv, 3), np.float32)
+        check(self.lib.mguso_read_positions(self.h, ptr(out)))
+        return out
+
+    @positions.setter
+    def positions(self, p):
+        a = np.ascontiguousarray(p, np.float32)
+        check(self.lib.mguso_write_positions(self.h, ptr(a)))
+
+    @property
+    def velocities(self) -> np.ndarray:
+        out = np.empty((self.nv, 3), np.float32)
+        check(self.lib.mguso_read_velocities(self.h, ptr(out)))
+        return out
+
+    @velocities.setter
+    def velocities(self, v):
+        a = np.ascontiguousarray(v, np.float32)
+        check(self.lib.mguso_write_velocities(self.h, ptr(a)))
+
+    def info(self) -> dict:
+        out = np.zeros(6, np.uint32)
+        check(self.lib.mguso_scene_info(self.h, ptr(out)))
+        return dict(zip(["hinges", "shells", "edges", "collider_tris", "nnz_system", "nnz_pinned"], out.tolist()))
+
+    def close(self):
+        if self.h:
+            self.lib.mguso_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
