@@ -249,6 +249,10 @@ int mguso_write_velocities(mguso_scene* s, const float* in);
 /* Element counts: hinges, shells, unique edges, static collider triangles,
  * system blocks (free-free pattern), pinned-pattern blocks. */
 int mguso_scene_info(mguso_scene* s, uint32_t* out6);
+/* Times `reps` applications of the scene's current system operator y = (Ps + C) x on the
+ * context stream with CUDA events (the PCG's SpMV at the last Newton iterate): *us gets the
+ * mean time per apply, *bytes its algorithmic bytes (blocks, columns, row pointers, x, y). */
+int mguso_scene_spmv_time(mguso_scene* s, int reps, float* us, double* bytes);
 
 #ifdef __cplusplus
 }

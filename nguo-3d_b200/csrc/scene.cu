@@ -549,3 +549,31 @@ int mguso_scene_info(mguso_scene* sc, uint32_t* out6) {
 }
 
 }  // extern "C"
+
+extern "C" int mguso_scene_spmv_time(mguso_scene* sc, int reps, float* us, double* bytes) {
+  MG_CHECK_ARG(sc && us && bytes && reps > 0, "bad argument");
+  Scene& s = sc->s;
+  cudaStream_t st = s.st;
+  DevBuf<float> x, y;
+  MG_TRY(x.reserve(3 * (size_t)s.nv));
+  MG_TRY(y.reserve(3 * (size_t)s.nv));
+  MG_CUDA(cudaMemsetAsync(x.p, 0, 12 * (size_t)s.nv, st));
+  for (int i = 0; i < 3; ++i) MG_TRY(system_spmv(s, x.p, y.p, st, nullptr));
+  cudaEvent_t e0, e1;
+  MG_CUDA(cudaEventCreate(&e0));
+  MG_CUDA(cudaEventCreate(&e1));
+  cudaEventRecord(e0, st);
+  for (int i = 0; i < reps; ++i) MG_TRY(system_spmv(s, x.p, y.p, st, nullptr));
+  cudaEventRecord(e1, st);
+  MG_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  uint32_t nc = 0;
+  MG_CUDA(cudaMemcpy(&nc, s.c_count.p, 4, cudaMemcpyDeviceToHost));
+  *us = 1000.f * ms / reps;
+  double nnz = (double)s.Ps.nnz + nc;
+  *bytes = 40.0 * nnz + 4.0 * 2 * (s.nv + 1) + 24.0 * s.nv;
+  return MGUSO_OK;
+}

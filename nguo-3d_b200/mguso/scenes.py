@@ -194,3 +194,149 @@ def sheet_on_sphere(n: int = 64, side: float = 1.0, height: float = 0.5, jitter:
                 tris=tris, shell_faces=tris.copy(), static_mask=None, stitch_idx=si, stitch_w=sw, stitch_kl=skl,
                 colliders=np.array([[1, 0, 0, 0, 0, 0, 0, radius]], np.float32), params=params,
                 name=f"{n}x{n} sheet on r={radius} sphere")
+
+
+def _panel(width: float, height: float, edge: float, rng):
+    """Rectangular panel [0, width] x [0, height] triangulated by a seeded Delaunay of a
+    jittered lattice (mean edge ~ `edge`), with evenly spaced boundary points so the two
+    side seams of two panels sample identical heights. Returns (uv points, triangles,
+    left-seam vertex ids bottom->top, right-seam vertex ids bottom->top)."""
+    from scipy.spatial import Delaunay
+
+    nx = max(int(round(width / edge)), 2)
+    ny = max(int(round(height / edge)), 2)
+    xs = np.linspace(0.0, width, nx + 1)
+    ys = np.linspace(0.0, height, ny + 1)
+    # boundary
+    left = np.stack([np.zeros(ny + 1), ys], 1)
+    right = np.stack([np.full(ny + 1, width), ys], 1)
+    bottom = np.stack([xs[1:-1], np.zeros(nx - 1)], 1)
+    top = np.stack([xs[1:-1], np.full(nx - 1, height)], 1)
+    # interior: jittered lattice, offset every other row (near-equilateral triangles)
+    ix, iy = np.meshgrid(np.arange(1, nx), np.arange(1, ny))
+    px = (ix + 0.5 * (iy % 2) - 0.25).astype(np.float64) * (width / nx)
+    py = iy.astype(np.float64) * (height / ny)
+    jit = rng.uniform(-0.2, 0.2, (2,) + px.shape)
+    px = np.clip(px + jit[0] * width / nx, 0.3 * width / nx, width - 0.3 * width / nx)
+    py = np.clip(py + jit[1] * height / ny, 0.3 * height / ny, height - 0.3 * height / ny)
+    interior = np.stack([px.ravel(), py.ravel()], 1)
+    pts = np.concatenate([left, right, bottom, top, interior])
+    tri = Delaunay(pts).simplices.astype(np.int64)
+    # drop slivers along the convex hull (none expected on a rectangle) and fix winding
+    a, b, c = pts[tri[:, 0]], pts[tri[:, 1]], pts[tri[:, 2]]
+    cross = (b[:, 0] - a[:, 0]) * (c[:, 1] - a[:, 1]) - (b[:, 1] - a[:, 1]) * (c[:, 0] - a[:, 0])
+    tri = tri[np.abs(cross) > 1e-12]
+    flip = ((pts[tri[:, 1], 0] - pts[tri[:, 0], 0]) * (pts[tri[:, 2], 1] - pts[tri[:, 0], 1]) -
+            (pts[tri[:, 1], 1] - pts[tri[:, 0], 1]) * (pts[tri[:, 2], 0] - pts[tri[:, 0], 0])) < 0
+    tri[flip] = tri[flip][:, [0, 2, 1]]
+    return pts, tri, np.arange(ny + 1), np.arange(ny + 1, 2 * (ny + 1))
+
+
+def torso_mesh(seed: int = 0, scale: float = 1.0, n_phi: int = 100, n_y: int = 99):
+    """Closed, outward-wound torso: the union of three vertical-axis ellipsoids (chest,
+    waist, hip) with semi-axes drawn U[0.12, 0.20] m, meshed as a star-shaped surface
+    r(y, phi) = max over ellipsoids of their radial extent, with a pole vertex at each end.
+    n_phi * n_y * 2 + 2 * n_phi triangles (20 000 by default)."""
+    rng = np.random.default_rng(seed)
+    centers = np.array([1.30, 1.05, 0.85]) * scale
+    axes = rng.uniform(0.12, 0.20, (3, 3)) * scale  # (a_x, b_y, c_z) per ellipsoid
+    y_lo = float((centers - axes[:, 1]).min()) + 1e-4
+    y_hi = float((centers + axes[:, 1]).max()) - 1e-4
+    ys = np.linspace(y_lo, y_hi, n_y)
+    phi = np.linspace(0.0, 2 * np.pi, n_phi, endpoint=False)
+    Y, PH = np.meshgrid(ys, phi, indexing="ij")
+    r = np.zeros_like(Y)
+    for (cy, (a, b, c)) in zip(centers, axes):
+        s2 = 1.0 - ((Y - cy) / b) ** 2
+        ok = s2 > 0
+        s = np.sqrt(np.where(ok, s2, 0.0))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            rk = 1.0 / np.sqrt(np.cos(PH) ** 2 / (a * s) ** 2 + np.sin(PH) ** 2 / (c * s) ** 2)
+        r = np.maximum(r, np.where(ok, rk, 0.0))
+    r = np.maximum(r, 0.01 * scale)
+    ring = np.stack([r * np.cos(PH), Y, r * np.sin(PH)], -1).reshape(-1, 3)
+    bottom_pole = np.array([[0.0, y_lo - 0.005 * scale, 0.0]])
+    top_pole = np.array([[0.0, y_hi + 0.005 * scale, 0.0]])
+    pos = np.concatenate([ring, bottom_pole, top_pole])
+    ib, it = n_y * n_phi, n_y * n_phi + 1
+    tris = []
+    for j in range(n_y - 1):
+        for k in range(n_phi):
+            a = j * n_phi + k
+            b = j * n_phi + (k + 1) % n_phi
+            c = (j + 1) * n_phi + k
+            d = (j + 1) * n_phi + (k + 1) % n_phi
+            tris.append((a, c, b))
+            tris.append((b, c, d))
+    for k in range(n_phi):
+        tris.append((ib, k, (k + 1) % n_phi))
+        top = (n_y - 1) * n_phi
+        tris.append((it, top + (k + 1) % n_phi, top + k))
+    tris = np.array(tris, np.int64)
+    # outward winding check: signed volume must be positive
+    p = pos[tris]
+    vol = np.einsum("ij,ij->i", np.cross(p[:, 0], p[:, 1]), p[:, 2]).sum() / 6.0
+    if vol < 0:
+        tris = tris[:, [0, 2, 1]]
+    return pos.astype(np.float32), tris.astype(np.uint32), (centers, axes)
+
+
+def sheath_on_torso(width: float = 0.6, height: float = 1.1, edge: float = 8.0e-3, seed: int = 1,
+                    torso_seed: int = 11, torso_scale: float = 1.0, young: float = 1.0e5, poisson: float = 0.3,
+                    thickness: float = 5.0e-4, bend: float = 1.0e-5, density: float = 0.2, dhat: float = 1.0e-3,
+                    dt: float = 1.0 / 60.0, stitch_k: float = 1.0e3, seam_gap: float = 2.0e-3,
+                    newton_tol_mps: float = 1.0e-3, torso_res=(100, 99), **kw):
+    """Seamed sheath: two width x height panels (seeded Delaunay, mean edge `edge`) wrapped
+    into the two halves of a vertical tube of circumference 2 * width, the side seams held by
+    6-index stitches (stiffness `stitch_k`, rest length dhat, cap 10 * dhat, as the
+    in-process transport builds them), hanging just above a static three-ellipsoid torso
+    (20k triangles) it drapes onto. Materials as the sheet configuration."""
+    rng = np.random.default_rng(seed)
+    R = 2.0 * width / (2.0 * np.pi)
+    tpos, ttris, _ = torso_mesh(torso_seed, torso_scale, *torso_res)
+    y_top = float(tpos[:, 1].max())
+    base_y = y_top + 0.01  # the tube hangs 1 cm above the torso and falls onto it
+    panels, tris, seams = [], [], []
+    off = 0
+    for k in range(2):
+        uv, tr, left, right = _panel(width, height, edge, rng)
+        th = (uv[:, 0] / width) * np.pi + k * np.pi
+        p = np.stack([R * np.cos(th), base_y + uv[:, 1], R * np.sin(th)], 1)
+        if k == 1:
+            # back panel slightly larger so its seam edges sit seam_gap away from the front's
+            p[:, [0, 2]] *= (R + seam_gap) / R
+        panels.append(p)
+        tris.append(tr + off)
+        seams.append((left + off, right + off))
+        off += p.shape[0]
+    cloth = np.concatenate(panels)
+    ctris = np.concatenate(tris)
+    # seams: front left (theta=0) <-> back right (theta=2pi); front right (pi) <-> back left (pi)
+    l0 = dhat
+    sidx, sw, skl = [], [], []
+    for a_ids, b_ids in ((seams[0][0], seams[1][1]), (seams[0][1], seams[1][0])):
+        for a, b in zip(a_ids, b_ids):
+            sidx.append([a, a, a, b, b, b])
+            sw.append([1, 0, 0, 1, 0, 0])
+            skl.append([stitch_k, l0, 10.0 * l0])
+    nc = cloth.shape[0]
+    pos = np.concatenate([cloth, tpos]).astype(np.float32)
+    all_tris = np.concatenate([ctris, ttris.astype(np.int64) + nc]).astype(np.uint32)
+    static = np.concatenate([np.zeros(nc, np.uint8), np.ones(tpos.shape[0], np.uint8)])
+    m = uniform_mass(pos, all_tris, density)
+    inv_mass = np.where(static > 0, 0.0, 1.0 / m).astype(np.float32)
+    mu, lam = lame_from_young_poisson(young * thickness, poisson)
+    params = default_params(dt=dt, bend_stiffness=bend, contact_dhat=dhat, shell_mu=mu, shell_lambda=lam,
+                            newton_tol=newton_tol_mps * dt, **kw)
+    return dict(positions=pos, velocities=np.zeros_like(pos), inv_mass=inv_mass, tris=all_tris,
+                shell_faces=ctris.astype(np.uint32), static_mask=static,
+                stitch_idx=np.array(sidx, np.uint32), stitch_w=np.array(sw, np.float32),
+                stitch_kl=np.array(skl, np.float32), colliders=np.zeros((0, 8), np.float32), params=params,
+                name=f"sheath {ctris.shape[0]} tris on torso {ttris.shape[0]} tris")
+
+
+def graded_sheaths(n: int = 6, widths=(0.50, 0.55, 0.60, 0.65, 0.70, 0.75), torso_scales=(0.9, 0.96, 1.02, 1.08, 1.14, 1.2),
+                   **kw):
+    """One pattern graded into `n` sizes XS..XXL (panel widths 0.50-0.75 m, torsos scaled
+    0.9-1.2): the batched configuration."""
+    return [sheath_on_torso(width=widths[i], torso_scale=torso_scales[i], **kw) for i in range(n)]

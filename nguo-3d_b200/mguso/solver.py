@@ -55,6 +55,7 @@ def _sigs(lib):
         ("mguso_read_velocities", i32, [vp, vp]),
         ("mguso_write_velocities", i32, [vp, vp]),
         ("mguso_scene_info", i32, [vp, vp]),
+        ("mguso_scene_spmv_time", i32, [vp, i32, P(C.c_float), P(C.c_double)]),
     ]:
         fn = getattr(lib, name)
         fn.restype = res
@@ -142,6 +143,12 @@ class ImplicitSolver:
         out = np.zeros(6, np.uint32)
         check(self.lib.mguso_scene_info(self.h, ptr(out)))
         return dict(zip(["hinges", "shells", "edges", "collider_tris", "nnz_system", "nnz_pinned"], out.tolist()))
+
+    def spmv_time(self, reps: int = 50):
+        """(microseconds per system SpMV, algorithmic bytes per SpMV) at the last iterate."""
+        us, b = C.c_float(), C.c_double()
+        check(self.lib.mguso_scene_spmv_time(self.h, reps, C.byref(us), C.byref(b)))
+        return us.value, b.value
 
     def close(self):
         if self.h:
