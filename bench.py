@@ -367,7 +367,7 @@ def run_drape(args, dist: Dist):
     # live roofline of the dominant kernel class (the PCG's system SpMV) at this iterate
     us, nbytes = solver.spmv_time(200)
     # launches per step from a short traced pass (not timed)
-    nl = count_launches(lambda: solver.step(2))
+    nl = None if args.no_launch_count else count_launches(lambda: solver.step(2))
     launches = None if nl is None else int(round(nl / 2 * args.steps))
     # end to end through the C ABI: state in from pinned host, one step, positions out
     pin_p = torch.from_numpy(solver.positions).pin_memory()
@@ -461,6 +461,7 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-launch-count", action="store_true", help="skip the traced launch count (under ncu)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -254,6 +254,27 @@ int mguso_scene_info(mguso_scene* s, uint32_t* out6);
  * mean time per apply, *bytes its algorithmic bytes (blocks, columns, row pointers, x, y). */
 int mguso_scene_spmv_time(mguso_scene* s, int reps, float* us, double* bytes);
 
+/* Assemble the Newton system once at positions x (f32[3 nv]) with inertia target x_tilde
+   (f32[3 nv]; NULL means x), exactly as one Newton iteration of mguso_step does: contact
+   stencils, elastic elements, colliders, contacts, right-hand side. The scene's positions
+   are left at x. out3 = {blocks in the fixed pattern, contact-only blocks, stencils}.
+   Parity and diagnostics entry; the reference counterpart is the triplet assembly of
+   ImplicitSolver::step (core-engine/crates/engine-core/src/implicit.rs:2280-3155). */
+int mguso_scene_assemble(mguso_scene* scene, const float* x, const float* x_tilde, uint32_t out3[3]);
+
+/* Download the last assembled system: the fixed-pattern blocks (row_ptr u32[nv+1], col
+   u32[out3[0]], values f32[9*out3[0]] row-major 3x3), the contact-only blocks in the same
+   layout (out3[1] of them; col/val may be NULL when zero) and the right-hand side f32[3 nv].
+   The system matrix is their sum. */
+int mguso_scene_system(mguso_scene* scene, uint32_t* ps_row_ptr, uint32_t* ps_col, float* ps_val,
+                       uint32_t* c_row_ptr, uint32_t* c_col, float* c_val, float* rhs);
+
+/* The contact stencils of the last mguso_scene_assemble in assembly order: participants
+   u32[4 n], kind u32[n] (0 vertex-triangle, 1 edge-edge) and gap f64[n]; min(n, cap) are
+   written, *n_out = n. Counterpart: self_collision_stencils (implicit.rs:678-753). */
+int mguso_scene_stencils(mguso_scene* scene, uint32_t cap, uint32_t* idx4, uint32_t* kind, double* d,
+                         uint32_t* n_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -705,41 +705,55 @@ int finish_rhs(Scene& s) {
   return MGUSO_OK;
 }
 
-// y += C x over C's rows, then the fused dot(x, y) over every row.
+// y = (Ps + C) x over every block row in one pass, accumulated in Acc, then the fused
+// dot(x, y). In mixed precision Acc is FP64: products of FP32 values are exact there, so
+// the inertia term (m / h^2, ~0.04 for a 10 mg vertex) survives next to seam and barrier
+// blocks of ~1e6 whose contributions cancel between neighbours. Storage stays FP32.
+__device__ __forceinline__ float acc_fma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double acc_fma(double a, double b, double c) { return fma(a, b, c); }
+
 template <class Acc>
-__global__ void k_c_add_dot(const uint32_t* __restrict__ c_rp, const uint32_t* __restrict__ c_col,
-                            const float* __restrict__ c_val, uint32_t nv, const float* __restrict__ x,
-                            float* __restrict__ y, DotSink dot, int with_dot) {
+__global__ void k_system_spmv(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ col,
+                              const float* __restrict__ val, const uint32_t* __restrict__ c_rp,
+                              const uint32_t* __restrict__ c_col, const float* __restrict__ c_val, uint32_t nv,
+                              const float* __restrict__ x, float* __restrict__ y, DotSink dot, int with_dot) {
   if (with_dot && dot.sc->done) return;
   Acc acc = 0;
   for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < nv; r += gridDim.x * blockDim.x) {
-    float y0 = y[3 * r], y1 = y[3 * r + 1], y2 = y[3 * r + 2];
-    for (uint32_t k = c_rp[r]; k < c_rp[r + 1]; ++k) {
-      uint32_t c = c_col[k];
-      const float* a = c_val + 9 * (size_t)k;
-      float x0 = x[3 * c], x1 = x[3 * c + 1], x2 = x[3 * c + 2];
-      y0 += a[0] * x0 + a[1] * x1 + a[2] * x2;
-      y1 += a[3] * x0 + a[4] * x1 + a[5] * x2;
-      y2 += a[6] * x0 + a[7] * x1 + a[8] * x2;
-    }
-    y[3 * r] = y0;
-    y[3 * r + 1] = y1;
-    y[3 * r + 2] = y2;
-    acc += (Acc)x[3 * r] * (Acc)y0 + (Acc)x[3 * r + 1] * (Acc)y1 + (Acc)x[3 * r + 2] * (Acc)y2;
+    Acc y0 = 0, y1 = 0, y2 = 0;
+    auto block = [&](const float* __restrict__ a, uint32_t c) {
+      const Acc x0 = (Acc)__ldg(x + 3 * c), x1 = (Acc)__ldg(x + 3 * c + 1), x2 = (Acc)__ldg(x + 3 * c + 2);
+      y0 = acc_fma((Acc)a[0], x0, y0);
+      y0 = acc_fma((Acc)a[1], x1, y0);
+      y0 = acc_fma((Acc)a[2], x2, y0);
+      y1 = acc_fma((Acc)a[3], x0, y1);
+      y1 = acc_fma((Acc)a[4], x1, y1);
+      y1 = acc_fma((Acc)a[5], x2, y1);
+      y2 = acc_fma((Acc)a[6], x0, y2);
+      y2 = acc_fma((Acc)a[7], x1, y2);
+      y2 = acc_fma((Acc)a[8], x2, y2);
+    };
+    for (uint32_t k = rp[r]; k < rp[r + 1]; ++k) block(val + 9 * (size_t)k, col[k]);
+    for (uint32_t k = c_rp[r]; k < c_rp[r + 1]; ++k) block(c_val + 9 * (size_t)k, c_col[k]);
+    const float f0 = (float)y0, f1 = (float)y1, f2 = (float)y2;
+    y[3 * r] = f0;
+    y[3 * r + 1] = f1;
+    y[3 * r + 2] = f2;
+    acc += (Acc)x[3 * r] * (Acc)f0 + (Acc)x[3 * r + 1] * (Acc)f1 + (Acc)x[3 * r + 2] * (Acc)f2;
   }
   if (with_dot) grid_dot_commit<Acc>(dot, acc);
 }
 
 int system_spmv(Scene& s, const float* p, float* ap, cudaStream_t st, const DotSink* d) {
-  MG_TRY(bsr_spmv(s.A.get(), p, ap, st, nullptr));
-  int grid = vec_grid(s.nv, 256, s.ctx->sm_count);
+  int grid = vec_grid(s.nv, 128, s.ctx->sm_count);
   DotSink dd = d ? *d : DotSink{};
-  if (d && d->mixed)
-    k_c_add_dot<double><<<grid, 256, 0, st>>>(s.c_row_ptr.p, s.c_col.p ? s.c_col.p : s.c_row_ptr.p, s.c_val.p,
-                                              s.nv, p, ap, dd, d ? 1 : 0);
+  const uint32_t* c_col = s.c_col.p ? s.c_col.p : s.c_row_ptr.p;
+  if (s.mixed)
+    k_system_spmv<double><<<grid, 128, 0, st>>>(s.Ps.row_ptr.p, s.Ps.col.p, s.A->val.p, s.c_row_ptr.p, c_col,
+                                                s.c_val.p, s.nv, p, ap, dd, d ? 1 : 0);
   else
-    k_c_add_dot<float><<<grid, 256, 0, st>>>(s.c_row_ptr.p, s.c_col.p ? s.c_col.p : s.c_row_ptr.p, s.c_val.p, s.nv,
-                                             p, ap, dd, d ? 1 : 0);
+    k_system_spmv<float><<<grid, 128, 0, st>>>(s.Ps.row_ptr.p, s.Ps.col.p, s.A->val.p, s.c_row_ptr.p, c_col,
+                                               s.c_val.p, s.nv, p, ap, dd, d ? 1 : 0);
   MG_CUDA(cudaGetLastError());
   return MGUSO_OK;
 }

@@ -577,3 +577,76 @@ extern "C" int mguso_scene_spmv_time(mguso_scene* sc, int reps, float* us, doubl
   *bytes = 40.0 * nnz + 4.0 * 2 * (s.nv + 1) + 24.0 * s.nv;
   return MGUSO_OK;
 }
+
+// One Newton-system assembly at positions x (and inertia target x_tilde, x when null), as
+// one Newton iteration of mguso_step does it; the scene's positions are left at x.
+extern "C" int mguso_scene_assemble(mguso_scene* sc, const float* x, const float* x_tilde, uint32_t* out3) {
+  MG_CHECK_ARG(sc && x && out3, "bad argument");
+  Scene& s = sc->s;
+  cudaStream_t st = s.st;
+  const size_t bytes = 12 * (size_t)s.nv;
+  MG_CUDA(cudaMemcpyAsync(s.x.p, x, bytes, cudaMemcpyHostToDevice, st));
+  MG_CUDA(cudaMemcpyAsync(s.xt.p, x_tilde ? x_tilde : x, bytes, cudaMemcpyHostToDevice, st));
+  uint32_t nst = 0;
+  if (s.p.self_collision) {
+    MG_TRY(build_bvhs(s, s.x.p));
+    MG_TRY(collect_stencils(s, &nst));
+  }
+  MG_TRY(assemble_elastic(s));
+  MG_TRY(assemble_colliders(s));
+  MG_TRY(assemble_contacts(s, nst));
+  MG_TRY(finish_rhs(s));
+  uint32_t nc = 0;
+  MG_CUDA(cudaMemcpyAsync(&nc, s.c_count.p, 4, cudaMemcpyDeviceToHost, st));
+  MG_CUDA(cudaStreamSynchronize(st));
+  out3[0] = s.Ps.nnz;
+  out3[1] = nc;
+  out3[2] = nst;
+  s.last_nst = nst;
+  return MGUSO_OK;
+}
+
+// The contact stencils of the last mguso_scene_assemble, in assembly order: participants
+// u32[4 n], kind u32[n] (0 vertex-triangle, 1 edge-edge), gap f64[n]. Writes min(n, cap).
+extern "C" int mguso_scene_stencils(mguso_scene* sc, uint32_t cap, uint32_t* idx4, uint32_t* kind, double* d,
+                                    uint32_t* n_out) {
+  MG_CHECK_ARG(sc && n_out && (cap == 0 || (idx4 && kind && d)), "bad argument");
+  Scene& s = sc->s;
+  const uint32_t n = std::min(cap, s.last_nst);
+  *n_out = s.last_nst;
+  if (n == 0) return MGUSO_OK;
+  std::vector<Stencil> h(n);
+  MG_CUDA(cudaMemcpyAsync(h.data(), s.stencils_sorted.p, sizeof(Stencil) * n, cudaMemcpyDeviceToHost, s.st));
+  MG_CUDA(cudaStreamSynchronize(s.st));
+  for (uint32_t i = 0; i < n; ++i) {
+    for (int k = 0; k < 4; ++k) idx4[4 * i + k] = h[i].idx[k];
+    kind[i] = h[i].kind;
+    d[i] = h[i].d;
+  }
+  return MGUSO_OK;
+}
+
+// The last assembled system: fixed pattern Ps (row_ptr nv+1, col, 9 floats per block),
+// contact-only blocks C (same layout), right-hand side f32[3 nv].
+extern "C" int mguso_scene_system(mguso_scene* sc, uint32_t* ps_rp, uint32_t* ps_col, float* ps_val, uint32_t* c_rp,
+                                  uint32_t* c_col, float* c_val, float* rhs) {
+  MG_CHECK_ARG(sc && ps_rp && ps_col && ps_val && c_rp && rhs, "bad argument");
+  Scene& s = sc->s;
+  cudaStream_t st = s.st;
+  uint32_t nc = 0;
+  MG_CUDA(cudaMemcpyAsync(&nc, s.c_count.p, 4, cudaMemcpyDeviceToHost, st));
+  MG_CUDA(cudaStreamSynchronize(st));
+  MG_CHECK_ARG(nc == 0 || (c_col && c_val), "bad argument");
+  const size_t nv1 = (size_t)s.nv + 1;
+  MG_CUDA(cudaMemcpyAsync(ps_rp, s.Ps.row_ptr.p, 4 * nv1, cudaMemcpyDeviceToHost, st));
+  MG_CUDA(cudaMemcpyAsync(ps_col, s.Ps.col.p, 4 * (size_t)s.Ps.nnz, cudaMemcpyDeviceToHost, st));
+  MG_CUDA(cudaMemcpyAsync(ps_val, s.A->val.p, 36 * (size_t)s.Ps.nnz, cudaMemcpyDeviceToHost, st));
+  MG_CUDA(cudaMemcpyAsync(c_rp, s.c_row_ptr.p, 4 * nv1, cudaMemcpyDeviceToHost, st));
+  if (nc) {
+    MG_CUDA(cudaMemcpyAsync(c_col, s.c_col.p, 4 * (size_t)nc, cudaMemcpyDeviceToHost, st));
+    MG_CUDA(cudaMemcpyAsync(c_val, s.c_val.p, 36 * (size_t)nc, cudaMemcpyDeviceToHost, st));
+  }
+  MG_CUDA(cudaMemcpyAsync(rhs, s.work.b.p, 12 * (size_t)s.nv, cudaMemcpyDeviceToHost, st));
+  MG_CUDA(cudaStreamSynchronize(st));
+  return MGUSO_OK;
+}

@@ -101,6 +101,7 @@ struct Scene {
   DevBuf<unsigned long long> counters;      // [0] vt pairs, [1] stencils, [2] ee candidates, [3] unique keys
   DevBuf<unsigned long long> side_best;     // per vertex (d2 bits << 32 | tri)
   DevBuf<Stencil> stencils, stencils_sorted;
+  uint32_t last_nst = 0;  // stencils of the last mguso_scene_assemble
   DevBuf<unsigned long long> st_keys;
   DevBuf<uint32_t> st_ids;
   // contact contributions (32 blocks + 4 gradient entries per stencil)

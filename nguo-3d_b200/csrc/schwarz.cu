@@ -6,10 +6,10 @@
 // diagonal when a pivot is <= 1e-14), and z = (L L^T)^-1 r per domain.
 //
 // B200 layout: factorisation is one CTA per domain in FP64 shared memory (right-looking
-// Cholesky, then L^-1 and M^-1 = L^-T L^-1), and what is stored is M^-1 itself, packed
-// lower-triangular in FP32 (16-byte aligned per domain). The apply is then a dense
-// symmetric matvec per domain with no sequential triangular sweeps: one warp per domain
-// stages its packed inverse into shared memory with a single 1-D TMA bulk copy.
+// Cholesky, then W = L^-1), and what is stored is W, packed lower-triangular in FP32
+// (16-byte aligned per domain). The apply is then two dense triangular matvecs per domain,
+// z = W^T (W r), with no sequential triangular sweeps: one warp per domain stages its
+// packed factor into shared memory with a single 1-D TMA bulk copy.
 #include <algorithm>
 #include <deque>
 
@@ -88,13 +88,18 @@ int schwarz_build(mguso_schwarz* s) {
 }
 
 // ---------------------------------------------------------------------------------------
-// Factorisation: one CTA per domain, FP64 in shared memory. The dense block (with the
-// reference's diagonal floor) is inverted by Gauss-Jordan elimination without pivoting,
-// ping-ponging between two m x ld buffers so every step is one data-parallel pass and one
-// barrier. For an SPD block the k-th Gauss-Jordan pivot is the k-th Schur-complement
-// diagonal, i.e. exactly the value the reference's Cholesky tests against 1e-14 before
-// taking its square root (linsolve.rs:88-92), so the same blocks fall back to the
-// diagonal. ld = m + 1 keeps column accesses free of bank conflicts.
+// Factorisation: one CTA per domain, FP64 in shared memory, in place in one m x ld buffer
+// (ld = m + 1, so column walks are free of bank conflicts):
+//   1. gather the dense block and add the reference's diagonal floor;
+//   2. right-looking Cholesky on the lower triangle. The k-th pivot is the k-th Schur
+//      complement diagonal, the value the reference's row-by-row Cholesky tests against
+//      1e-14 (linsolve.rs:88-92), so the same blocks fall back to the diagonal;
+//   3. W = L^-1, one thread per column (forward substitution), written transposed into the
+//      upper triangle.
+// Stored: W packed row-major lower-triangular in FP32. The apply forms z = W^T (W r), so
+// the FP32 preconditioner W~^T W~ is symmetric positive definite for any rounding of W.
+// (An explicitly stored FP32 inverse is not: with stiff seams a domain block reaches a
+// condition number near 1e7 and rounding the inverse to FP32 can make it indefinite.)
 // ---------------------------------------------------------------------------------------
 constexpr int FACTOR_THREADS = 256;
 
@@ -112,7 +117,8 @@ __global__ void __launch_bounds__(FACTOR_THREADS) k_schwarz_factor(
   const int m = 3 * (int)nvd;
   const int ld = m + 1;
   double* A = sA;
-  double* B = sA + (size_t)m * ld;
+  double* dinv = sA + (size_t)m * ld;  // 1 / L_kk
+  double* diag0 = dinv + m;           // floored diagonal (fallback)
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int i = tid; i < m * ld; i += nt) A[i] = 0.0;
   __syncthreads();
@@ -153,10 +159,14 @@ __global__ void __launch_bounds__(FACTOR_THREADS) k_schwarz_factor(
     s_fail = 0;
   }
   __syncthreads();
-  for (int k = tid; k < m; k += nt) A[k * ld + k] += s_floor;
+  for (int k = tid; k < m; k += nt) {
+    A[k * ld + k] += s_floor;
+    diag0[k] = A[k * ld + k];
+  }
   __syncthreads();
-  float* out = fac + fac_off[d];
-  const int total = m * m;
+  // Cholesky: column k stays unscaled during its own trailing update (L_ik = A_ik / L_kk
+  // is applied after the loop), so one barrier per column suffices.
+  const int tx = tid & 31, ty = tid >> 5;
   for (int k = 0; k < m; ++k) {
     const double p = A[k * ld + k];
     if (!(p > 1e-14)) {  // uniform: every thread reads the same pivot
@@ -164,47 +174,53 @@ __global__ void __launch_bounds__(FACTOR_THREADS) k_schwarz_factor(
       break;
     }
     const double ip = 1.0 / p;
-    for (int e = tid; e < total; e += nt) {
-      int i = e / m, j = e - i * m;
-      double r;
-      if (i == k)
-        r = (j == k) ? ip : A[k * ld + j] * ip;
-      else if (j == k)
-        r = -A[i * ld + k] * ip;
-      else
-        r = A[i * ld + j] - A[i * ld + k] * (A[k * ld + j] * ip);
-      B[i * ld + j] = r;
+    for (int i = k + 1 + ty; i < m; i += 8) {
+      const double aik = A[i * ld + k] * ip;
+      for (int j = k + 1 + tx; j <= i; j += 32) A[i * ld + j] -= aik * A[j * ld + k];
+    }
+    if (tid == 0) {
+      const double l = sqrt(p);
+      dinv[k] = 1.0 / l;
     }
     __syncthreads();
-    double* t = A;
-    A = B;
-    B = t;
   }
   __syncthreads();
+  float* out = fac + fac_off[d];
   if (s_fail) {
-    // reference fallback: L = diag(sqrt(ad_pp)) (1 where ad_pp <= 1e-14), so
-    // M^-1 = diag(1 / ad_pp); the floored diagonal is re-gathered from the matrix.
+    // reference fallback: L = diag(sqrt(ad_pp)) (1 where ad_pp <= 1e-14), i.e.
+    // W = diag(1 / sqrt(ad_pp))
     for (int e = tid; e < m * (m + 1) / 2; e += nt) out[e] = 0.0f;
     __syncthreads();
-    for (uint32_t p = w; p < nvd; p += nw) {
-      uint32_t v = dom_verts[vs + p];
-      for (uint32_t k = row_ptr[v] + lane; k < row_ptr[v + 1]; k += 32) {
-        if (col[k] != v) continue;
-        const float* b = val + 9 * (size_t)k;
-        for (int i = 0; i < 3; ++i) {
-          double a = (double)b[4 * i] + s_floor;
-          int r = 3 * p + i;
-          out[r * (r + 1) / 2 + r] = (float)(a > 1e-14 ? 1.0 / a : 1.0);
-        }
-      }
+    for (int r = tid; r < m; r += nt) {
+      double a = diag0[r];
+      out[r * (r + 1) / 2 + r] = (float)(a > 1e-14 ? 1.0 / sqrt(a) : 1.0);
     }
     if (tid == 0) atomicOr(status, 1u << 8);
     return;
   }
-  // packed row-major lower triangle of the (symmetric) inverse; the two triangles are
-  // averaged so rounding asymmetry does not leak into the preconditioner
+  for (int i = ty; i < m; i += 8)
+    for (int k = tx; k < i; k += 32) A[i * ld + k] *= dinv[k];
+  __syncthreads();
+  // W = L^-1 by columns: thread j walks rows i > j; W_ij = -dinv_i * sum_{k=j}^{i-1} L_ik W_kj.
+  // W_kj (k >= j) lives at A[j * ld + k], the upper triangle and the diagonal.
+  for (int j = tid; j < m; j += nt) {
+    double* wj = A + (size_t)j * ld;
+    wj[j] = dinv[j];
+    for (int i = j + 1; i < m; ++i) {
+      const double* li = A + (size_t)i * ld;
+      double s0 = 0.0, s1 = 0.0;
+      int k = j;
+      for (; k + 1 < i; k += 2) {
+        s0 += li[k] * wj[k];
+        s1 += li[k + 1] * wj[k + 1];
+      }
+      if (k < i) s0 += li[k] * wj[k];
+      wj[i] = -(s0 + s1) * dinv[i];
+    }
+  }
+  __syncthreads();
   for (int i = w; i < m; i += nw)
-    for (int j = lane; j <= i; j += 32) out[i * (i + 1) / 2 + j] = (float)(0.5 * (A[i * ld + j] + A[j * ld + i]));
+    for (int j = lane; j <= i; j += 32) out[i * (i + 1) / 2 + j] = (float)A[j * ld + i];
 }
 
 int schwarz_factor(mguso_schwarz* s, cudaStream_t st) {
@@ -215,7 +231,7 @@ int schwarz_factor_with(mguso_schwarz* s, const uint32_t* c_rp, const uint32_t* 
                         cudaStream_t st) {
   if (s->ndom == 0) return MGUSO_OK;
   mguso_bsr* a = s->a;
-  size_t smem = sizeof(double) * 2 * (size_t)s->max_m * (s->max_m + 1);
+  size_t smem = sizeof(double) * ((size_t)s->max_m * (s->max_m + 1) + 2 * (size_t)s->max_m);
   k_schwarz_factor<<<s->ndom, FACTOR_THREADS, smem, st>>>(a->row_ptr.p, a->col.p, a->val.p, s->dom_start.p, s->dom_verts.p,
                                                s->dom_of.p, s->loc.p, s->fac_off.p, s->fac.p, s->status.p,
                                                           c_col ? c_rp : nullptr, c_col, c_val);
@@ -224,8 +240,8 @@ int schwarz_factor_with(mguso_schwarz* s, const uint32_t* c_rp, const uint32_t* 
 }
 
 // ---------------------------------------------------------------------------------------
-// Apply: one warp per domain. Per-warp shared slice: mbarrier, the packed inverse (bulk
-// copied), and the gathered residual.
+// Apply: one warp per domain. Per-warp shared slice: mbarrier, the packed factor W (bulk
+// copied), the gathered residual and W r.
 // ---------------------------------------------------------------------------------------
 template <int WARPS, class Acc>
 __global__ void __launch_bounds__(32 * WARPS) k_schwarz_apply(
@@ -237,7 +253,8 @@ __global__ void __launch_bounds__(32 * WARPS) k_schwarz_apply(
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   uint64_t* bar = (uint64_t*)(smem + 16 * w);
   float* buf = (float*)(smem + 128 + (size_t)w * slice_floats * 4);
-  float* rd = buf + (slice_floats - 96);
+  float* rd = buf + (slice_floats - 288);        // gathered residual
+  Acc* yd = (Acc*)(buf + (slice_floats - 192));  // W r
   const uint32_t d = blockIdx.x * WARPS + w;
   Acc acc = 0;
   bool ok = true;
@@ -263,13 +280,20 @@ __global__ void __launch_bounds__(32 * WARPS) k_schwarz_apply(
     __syncwarp();
     ok = mbar_wait(bar, 0);
     if (ok) {
-      for (int i = lane; i < m; i += 32) {
-        float s = 0.f;
+      // Acc = double (mixed precision) accumulates both matvecs in FP64: the entries of W
+      // span the square root of the domain's condition number and cancel in W r.
+      for (int i = lane; i < m; i += 32) {  // y = W r, rows of the packed lower triangle
+        Acc s = 0;
         const int ri = i * (i + 1) / 2;
-        for (int j = 0; j <= i; ++j) s = fmaf(buf[ri + j], rd[j], s);
-        for (int j = i + 1; j < m; ++j) s = fmaf(buf[j * (j + 1) / 2 + i], rd[j], s);
+        for (int j = 0; j <= i; ++j) s += (Acc)buf[ri + j] * (Acc)rd[j];
+        yd[i] = s;
+      }
+      __syncwarp();
+      for (int i = lane; i < m; i += 32) {  // z = W^T y, columns
+        Acc s = 0;
+        for (int j = i; j < m; ++j) s += (Acc)buf[j * (j + 1) / 2 + i] * yd[j];
         uint32_t v = dom_verts[vs + i / 3];
-        z[3 * v + i % 3] = s;
+        z[3 * v + i % 3] = (float)s;
         acc += (Acc)rd[i] * (Acc)s;
       }
     } else if (lane == 0) {
@@ -285,9 +309,9 @@ int schwarz_configure() {
   static bool done = false;
   if (done) return MGUSO_OK;
   constexpr int WARPS = 4;
-  size_t fsm = sizeof(double) * 2 * 96 * 97;
+  size_t fsm = sizeof(double) * (96 * 97 + 2 * 96);
   MG_CUDA(cudaFuncSetAttribute(k_schwarz_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
-  uint32_t slice = ((96 * 97 / 2 + 3) & ~3u) + 96;
+  uint32_t slice = ((96 * 97 / 2 + 3) & ~3u) + 288;
   slice = (slice + 31) & ~31u;
   size_t asmem = 128 + (size_t)WARPS * slice * 4;
   MG_CUDA(cudaFuncSetAttribute(k_schwarz_apply<WARPS, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -306,7 +330,7 @@ int schwarz_apply(mguso_schwarz* s, const float* r, float* z, cudaStream_t st, c
   bool mixed = dot && dot->mixed;
   uint32_t mm = std::max<uint32_t>(s->max_m, 3);
   uint32_t packed = (mm * (mm + 1) / 2 + 3) & ~3u;
-  uint32_t slice = packed + 96;  // factor + gathered residual (m <= 96 floats)
+  uint32_t slice = packed + 288;  // factor + gathered residual (96 floats) + W r (96 Acc)
   slice = (slice + 31) & ~31u;
   size_t smem = 128 + (size_t)WARPS * slice * 4;
   uint32_t grid = ceil_div(s->ndom, WARPS);

@@ -7,6 +7,8 @@
 // step length).
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 
 #include "elements.cuh"
 #include "reduce.cuh"
@@ -148,6 +150,8 @@ int scene_step(Scene& s, mguso_step_stats* out) {
   uint32_t taken = 0;
   const int sms = s.ctx->sm_count;
   const bool contacts = s.p.self_collision != 0;
+  // MGUSO_TRACE=1 prints one line per Newton iteration to stderr (diagnostics only)
+  static const bool trace = std::getenv("MGUSO_TRACE") != nullptr;
   for (uint32_t it = 0; it < cap; ++it) {
     ++taken;
     uint32_t nst = 0;
@@ -190,6 +194,9 @@ int scene_step(Scene& s, mguso_step_stats* out) {
     MG_CUDA(cudaMemcpyAsync(&msb, s.red.p + 9, 4, cudaMemcpyDeviceToHost, st));
     MG_CUDA(cudaStreamSynchronize(st));
     float max_step = u2f_host(msb);
+    if (trace)
+      std::fprintf(stderr, "[mguso] newton %u stencils %u cg %u res %.3e lin_status %d t %.4f max_step %.3e\n", it,
+                   nst, ls.iters, ls.residual, ls.status, t, max_step);
     if (max_step < 1.0e-7f) break;
     if (s.p.newton_tol > 0.f && max_step < s.p.newton_tol) break;
     if (final_step) break;

@@ -288,9 +288,14 @@ def sheath_on_torso(width: float = 0.6, height: float = 1.1, edge: float = 8.0e-
                     newton_tol_mps: float = 1.0e-3, torso_res=(100, 99), **kw):
     """Seamed sheath: two width x height panels (seeded Delaunay, mean edge `edge`) wrapped
     into the two halves of a vertical tube of circumference 2 * width, the side seams held by
-    6-index stitches (stiffness `stitch_k`, rest length dhat, cap 10 * dhat, as the
-    in-process transport builds them), hanging just above a static three-ellipsoid torso
-    (20k triangles) it drapes onto. Materials as the sheet configuration."""
+    6-index stitches (rest length dhat, cap 10 * dhat, as the in-process transport builds
+    them), hanging just above a static three-ellipsoid torso (20k triangles) it drapes onto.
+    Materials as the sheet configuration.
+
+    `stitch_k` is the seam's spring constant in N/m. The stitch energy
+    k_raw (|t| - l0)^2 / (2 l0) (stitch.rs:42-46) has spring constant k_raw / l0, so the
+    stitch carries k_raw = stitch_k * l0: 1.0 at 1e3 N/m and l0 = 1 mm, which is also the
+    reference's default stitch stiffness (golden.rs read_stitches)."""
     rng = np.random.default_rng(seed)
     R = 2.0 * width / (2.0 * np.pi)
     tpos, ttris, _ = torso_mesh(torso_seed, torso_scale, *torso_res)
@@ -318,7 +323,7 @@ def sheath_on_torso(width: float = 0.6, height: float = 1.1, edge: float = 8.0e-
         for a, b in zip(a_ids, b_ids):
             sidx.append([a, a, a, b, b, b])
             sw.append([1, 0, 0, 1, 0, 0])
-            skl.append([stitch_k, l0, 10.0 * l0])
+            skl.append([stitch_k * l0, l0, 10.0 * l0])
     nc = cloth.shape[0]
     pos = np.concatenate([cloth, tpos]).astype(np.float32)
     all_tris = np.concatenate([ctris, ttris.astype(np.int64) + nc]).astype(np.uint32)

@@ -56,6 +56,9 @@ def _sigs(lib):
         ("mguso_write_velocities", i32, [vp, vp]),
         ("mguso_scene_info", i32, [vp, vp]),
         ("mguso_scene_spmv_time", i32, [vp, i32, P(C.c_float), P(C.c_double)]),
+        ("mguso_scene_assemble", i32, [vp, vp, vp, vp]),
+        ("mguso_scene_system", i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
+        ("mguso_scene_stencils", i32, [vp, C.c_uint32, vp, vp, vp, vp]),
     ]:
         fn = getattr(lib, name)
         fn.restype = res
@@ -149,6 +152,37 @@ class ImplicitSolver:
         us, b = C.c_float(), C.c_double()
         check(self.lib.mguso_scene_spmv_time(self.h, reps, C.byref(us), C.byref(b)))
         return us.value, b.value
+
+    def assemble(self, x, x_tilde=None) -> dict:
+        """One Newton-system assembly at positions ``x`` (inertia target ``x_tilde``, ``x``
+        when None), downloaded as the fixed-pattern blocks ``ps`` and the contact-only
+        blocks ``c`` (each ``(row_ptr, col, val[nnz, 3, 3])``) plus ``rhs``; the scene's
+        positions are left at ``x``."""
+        xx = np.ascontiguousarray(x, np.float32)
+        xt = None if x_tilde is None else np.ascontiguousarray(x_tilde, np.float32)
+        n3 = np.zeros(3, np.uint32)
+        check(self.lib.mguso_scene_assemble(self.h, ptr(xx), ptr(xt) if xt is not None else None, ptr(n3)))
+        nps, nc, nst = (int(v) for v in n3)
+        ps_rp = np.empty(self.nv + 1, np.uint32)
+        ps_col = np.empty(nps, np.uint32)
+        ps_val = np.empty((nps, 3, 3), np.float32)
+        c_rp = np.empty(self.nv + 1, np.uint32)
+        c_col = np.empty(max(nc, 1), np.uint32)
+        c_val = np.empty((max(nc, 1), 3, 3), np.float32)
+        rhs = np.empty(3 * self.nv, np.float32)
+        check(self.lib.mguso_scene_system(self.h, ptr(ps_rp), ptr(ps_col), ptr(ps_val), ptr(c_rp), ptr(c_col),
+                                          ptr(c_val), ptr(rhs)))
+        return {"ps": (ps_rp, ps_col, ps_val), "c": (c_rp, c_col[:nc], c_val[:nc]), "rhs": rhs, "stencils": nst}
+
+    def stencils(self):
+        """Contact stencils of the last ``assemble``: (idx[n, 4], kind[n], gap[n])."""
+        n = C.c_uint32()
+        check(self.lib.mguso_scene_stencils(self.h, 0, None, None, None, C.byref(n)))
+        idx = np.empty((max(n.value, 1), 4), np.uint32)
+        kind = np.empty(max(n.value, 1), np.uint32)
+        d = np.empty(max(n.value, 1), np.float64)
+        check(self.lib.mguso_scene_stencils(self.h, n.value, ptr(idx), ptr(kind), ptr(d), C.byref(n)))
+        return idx[:n.value], kind[:n.value], d[:n.value]
 
     def close(self):
         if self.h:
