@@ -238,7 +238,11 @@ def run_spmv(args, dist: Dist):
     e1.record(stream)
     torch.cuda.synchronize()
     sch_us = 1000.0 * e0.elapsed_time(e1) / args.steps
-    sch_bytes = sch.factor_bytes + 24 * nb
+    # algorithmic bytes: each domain's triangular factor once (m (m + 1) / 2 floats), the
+    # gathered residual, the scattered result and the domain vertex lists
+    dsz = 3.0 * np.bincount(sch.domains().astype(np.int64))
+    sch_bytes = int(4 * (dsz * (dsz + 1) / 2).sum() + 28 * nb)
+    sch_stored = int(sch.factor_bytes + 28 * nb)
 
     # end to end through the C ABI with pinned host buffers
     xp, yp = x_h.numpy(), y_h.numpy()
@@ -275,11 +279,11 @@ def run_spmv(args, dist: Dist):
         "roofline": {
             "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": f"{peak_kind} (burst copy)",
-            "kernel": "k_spmv_tma / k_spmv_direct (autotuned)",
+            "kernel": "autotuned BSR SpMV: " + json.dumps(a.kernel()),
         },
         "schwarz_apply": {
             "us": round(sch_us, 2), "GB/s": round(sch_bytes / (sch_us * 1e-6) / 1e9, 1),
-            "domains": sch.ndomains, "bytes": sch_bytes,
+            "domains": sch.ndomains, "bytes": sch_bytes, "stored_bytes": sch_stored,
         },
         "e2e": {"value": round(nbytes / e2e_s / 1e9 * dist.world, 2), "unit": "GB/s",
                 "h2d_bytes_per_step": 12 * nb, "d2h_bytes_per_step": 12 * nb},
@@ -364,11 +368,11 @@ def run_drape(args, dist: Dist):
     clk = clocks.stop()
     ms = dist.max(e0.elapsed_time(e1))
     ms_step = ms / args.steps
-    # live roofline of the dominant kernel class (the PCG's system SpMV) at this iterate
-    us, nbytes = solver.spmv_time(200)
-    # launches per step from a short traced pass (not timed)
-    nl = None if args.no_launch_count else count_launches(lambda: solver.step(2))
-    launches = None if nl is None else int(round(nl / 2 * args.steps))
+    # live per-kernel times at the last assembled system (CUDA events, each kernel alone);
+    # the SpMV and the preconditioner apply each run once per PCG iteration
+    prof = solver.profile(100)
+    dom = max(("spmv", "precond_apply"), key=lambda k: prof[k][0])
+    us, nbytes = prof[dom]
     # end to end through the C ABI: state in from pinned host, one step, positions out
     pin_p = torch.from_numpy(solver.positions).pin_memory()
     pin_v = torch.from_numpy(solver.velocities).pin_memory()
@@ -383,6 +387,9 @@ def run_drape(args, dist: Dist):
         solver.step(1)
         mguso._lib.check(lib.mguso_read_positions(solver.h, out.data_ptr()))
     e2e_s = dist.max(time.perf_counter() - t0) / k2
+    # launches per step from a short traced pass (not timed)
+    nl = None if args.no_launch_count else count_launches(lambda: solver.step(2))
+    launches = None if nl is None else int(round(nl / 2 * args.steps))
     peak, peak_kind = load_peaks()
     achieved = nbytes / (us * 1e-6) / 1e9
     newton = [s_["newton_iters"] for s_ in stats]
@@ -409,8 +416,11 @@ def run_drape(args, dist: Dist):
         "roofline": {
             "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": f"{peak_kind} (burst copy)",
-            "kernel": "system SpMV (k_spmv_direct + k_c_add_dot) at the last Newton iterate",
+            "kernel": {"spmv": "k_system_spmv", "precond_apply": "k_schwarz_apply"}[dom]
+            + " (once per PCG iteration; timed alone at the last Newton system)",
             "us_per_launch": round(us, 2), "bytes_per_launch": int(nbytes),
+            "per_kernel": {k: {"us": round(v[0], 2), "bytes": int(v[1]),
+                               "GB/s": round(v[1] / (v[0] * 1e-6) / 1e9, 1)} for k, v in prof.items()},
         },
         "e2e": {"value": round(1.0 / e2e_s * dist.world, 3), "unit": "steps/s",
                 "h2d_bytes_per_step": 24 * int(nv), "d2h_bytes_per_step": 12 * int(nv)},

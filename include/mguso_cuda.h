@@ -112,12 +112,17 @@ int mguso_bsr_set_kernel(mguso_bsr* a, int variant, int* active);
 /* Runs the SpMV autotuner on this matrix (times every variant and tile shape with CUDA
  * events) and keeps the fastest. *best_us gets its time per apply. */
 int mguso_bsr_autotune(mguso_bsr* a, float* best_us);
+/* The variant in use (1 TMA, 2 direct, 3 sliced ELL; 0 before any choice) and, for TMA,
+ * its tile shape (block rows per tile, pipeline stages; 0 otherwise). */
+int mguso_bsr_kernel(const mguso_bsr* a, int* variant, int* tile_rows, int* stages);
 
 /* ---- One-level additive Schwarz preconditioner (linsolve.rs:126-258) --------------- */
 /* Domains are greedy BFS aggregates of <= `domain` vertices over the block graph of `a`
- * (linsolve.rs:152-173). Each domain's dense block (with the reference's diagonal floor)
- * is inverted in FP64 and the inverse stored packed in FP32; the apply is a dense
- * symmetric matvec per domain. */
+ * (linsolve.rs:152-173); vertices without off-diagonal blocks are packed `domain` at a
+ * time. Each domain's dense block (with the reference's diagonal floor) is
+ * Cholesky-factored in FP64 and W = L^-1 stored in FP32 (32 x 32 tiles of its lower
+ * block-triangle); the apply is z = W^T (W r) per domain, symmetric positive definite for
+ * any rounding of W. factor_bytes reports the stored tile bytes. */
 int mguso_schwarz_create(mguso_bsr* a, uint32_t domain, mguso_schwarz** out);
 int mguso_schwarz_destroy(mguso_schwarz* s);
 int mguso_schwarz_info(const mguso_schwarz* s, uint32_t* ndomains, uint64_t* factor_bytes);
@@ -253,6 +258,13 @@ int mguso_scene_info(mguso_scene* s, uint32_t* out6);
  * context stream with CUDA events (the PCG's SpMV at the last Newton iterate): *us gets the
  * mean time per apply, *bytes its algorithmic bytes (blocks, columns, row pointers, x, y). */
 int mguso_scene_spmv_time(mguso_scene* s, int reps, float* us, double* bytes);
+
+/* Mean device time in microseconds of the step's linear-solver kernels at the last
+ * assembled system, each timed alone over `reps` launches with CUDA events on the scene's
+ * stream: us4 = {system SpMV, preconditioner apply, preconditioner factorisation, PCG
+ * vector update}; bytes4 = their algorithmic bytes per launch (each stored block or factor
+ * entry and each vector read or written once). Clobbers the PCG scratch (not the state). */
+int mguso_scene_profile(mguso_scene* s, int reps, float* us4, double* bytes4);
 
 /* Assemble the Newton system once at positions x (f32[3 nv]) with inertia target x_tilde
    (f32[3 nv]; NULL means x), exactly as one Newton iteration of mguso_step does: contact

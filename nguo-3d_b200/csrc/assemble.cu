@@ -712,14 +712,22 @@ int finish_rhs(Scene& s) {
 __device__ __forceinline__ float acc_fma(float a, float b, float c) { return fmaf(a, b, c); }
 __device__ __forceinline__ double acc_fma(double a, double b, double c) { return fma(a, b, c); }
 
+// Eight lanes per block row: lane g takes blocks g, g + 8, ... of the row's fixed-pattern
+// and contact lists (coalesced 288-byte runs of values), then a fixed xor tree over the
+// eight lanes sums them, so the result is deterministic.
 template <class Acc>
-__global__ void k_system_spmv(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ col,
-                              const float* __restrict__ val, const uint32_t* __restrict__ c_rp,
-                              const uint32_t* __restrict__ c_col, const float* __restrict__ c_val, uint32_t nv,
-                              const float* __restrict__ x, float* __restrict__ y, DotSink dot, int with_dot) {
+__global__ void __launch_bounds__(256) k_system_spmv(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ col,
+                                                     const float* __restrict__ val, const uint32_t* __restrict__ c_rp,
+                                                     const uint32_t* __restrict__ c_col,
+                                                     const float* __restrict__ c_val, uint32_t nv,
+                                                     const float* __restrict__ x, float* __restrict__ y, DotSink dot,
+                                                     int with_dot) {
   if (with_dot && dot.sc->done) return;
+  const uint32_t g = threadIdx.x & 7u;
+  const unsigned gmask = 0xFFu << (threadIdx.x & 24u);
   Acc acc = 0;
-  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < nv; r += gridDim.x * blockDim.x) {
+  const uint32_t stride = (gridDim.x * blockDim.x) >> 3;
+  for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 3; r < nv; r += stride) {
     Acc y0 = 0, y1 = 0, y2 = 0;
     auto block = [&](const float* __restrict__ a, uint32_t c) {
       const Acc x0 = (Acc)__ldg(x + 3 * c), x1 = (Acc)__ldg(x + 3 * c + 1), x2 = (Acc)__ldg(x + 3 * c + 2);
@@ -733,26 +741,37 @@ __global__ void k_system_spmv(const uint32_t* __restrict__ rp, const uint32_t* _
       y2 = acc_fma((Acc)a[7], x1, y2);
       y2 = acc_fma((Acc)a[8], x2, y2);
     };
-    for (uint32_t k = rp[r]; k < rp[r + 1]; ++k) block(val + 9 * (size_t)k, col[k]);
-    for (uint32_t k = c_rp[r]; k < c_rp[r + 1]; ++k) block(c_val + 9 * (size_t)k, c_col[k]);
-    const float f0 = (float)y0, f1 = (float)y1, f2 = (float)y2;
-    y[3 * r] = f0;
-    y[3 * r + 1] = f1;
-    y[3 * r + 2] = f2;
-    acc += (Acc)x[3 * r] * (Acc)f0 + (Acc)x[3 * r + 1] * (Acc)f1 + (Acc)x[3 * r + 2] * (Acc)f2;
+    const uint32_t ke = rp[r + 1];
+    for (uint32_t k = rp[r] + g; k < ke; k += 8) block(val + 9 * (size_t)k, col[k]);
+    const uint32_t ce = c_rp[r + 1];
+    for (uint32_t k = c_rp[r] + g; k < ce; k += 8) block(c_val + 9 * (size_t)k, c_col[k]);
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) {
+      y0 += __shfl_xor_sync(gmask, y0, o, 8);
+      y1 += __shfl_xor_sync(gmask, y1, o, 8);
+      y2 += __shfl_xor_sync(gmask, y2, o, 8);
+    }
+    if (g == 0) {
+      const float f0 = (float)y0, f1 = (float)y1, f2 = (float)y2;
+      y[3 * r] = f0;
+      y[3 * r + 1] = f1;
+      y[3 * r + 2] = f2;
+      acc += (Acc)x[3 * r] * (Acc)f0 + (Acc)x[3 * r + 1] * (Acc)f1 + (Acc)x[3 * r + 2] * (Acc)f2;
+    }
   }
   if (with_dot) grid_dot_commit<Acc>(dot, acc);
 }
 
 int system_spmv(Scene& s, const float* p, float* ap, cudaStream_t st, const DotSink* d) {
-  int grid = vec_grid(s.nv, 128, s.ctx->sm_count);
+  const int grid = (int)std::max<uint64_t>(
+      1, std::min<uint64_t>(ceil_div(8ull * s.nv, 256), (uint64_t)s.ctx->sm_count * 8));
   DotSink dd = d ? *d : DotSink{};
   const uint32_t* c_col = s.c_col.p ? s.c_col.p : s.c_row_ptr.p;
   if (s.mixed)
-    k_system_spmv<double><<<grid, 128, 0, st>>>(s.Ps.row_ptr.p, s.Ps.col.p, s.A->val.p, s.c_row_ptr.p, c_col,
+    k_system_spmv<double><<<grid, 256, 0, st>>>(s.Ps.row_ptr.p, s.Ps.col.p, s.A->val.p, s.c_row_ptr.p, c_col,
                                                 s.c_val.p, s.nv, p, ap, dd, d ? 1 : 0);
   else
-    k_system_spmv<float><<<grid, 128, 0, st>>>(s.Ps.row_ptr.p, s.Ps.col.p, s.A->val.p, s.c_row_ptr.p, c_col,
+    k_system_spmv<float><<<grid, 256, 0, st>>>(s.Ps.row_ptr.p, s.Ps.col.p, s.A->val.p, s.c_row_ptr.p, c_col,
                                                s.c_val.p, s.nv, p, ap, dd, d ? 1 : 0);
   MG_CUDA(cudaGetLastError());
   return MGUSO_OK;

@@ -139,6 +139,15 @@ int mguso_bsr_set_kernel(mguso_bsr* a, int variant, int* active) {
   return MGUSO_OK;
 }
 
+int mguso_bsr_kernel(const mguso_bsr* a, int* variant, int* tile_rows, int* stages) {
+  MG_CHECK_ARG(a && variant, "bad argument");
+  *variant = a->variant;
+  const bool tma = a->variant == SPMV_TMA && a->tiling_choice >= 0 && a->tiling_choice < (int)a->tilings.size();
+  if (tile_rows) *tile_rows = tma ? a->tilings[a->tiling_choice]->rows : 0;
+  if (stages) *stages = tma ? a->tilings[a->tiling_choice]->stages : 0;
+  return MGUSO_OK;
+}
+
 int mguso_bsr_autotune(mguso_bsr* a, float* best_us) {
   MG_CHECK_ARG(a, "null bsr");
   return bsr_autotune(a, best_us);

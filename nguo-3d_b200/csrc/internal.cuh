@@ -77,7 +77,7 @@ struct mguso_schwarz {
   mg::DevBuf<uint32_t> dom_of;     // nb
   mg::DevBuf<uint32_t> loc;        // nb: local index of a vertex inside its domain
   mg::DevBuf<uint64_t> fac_off;    // ndom + 1 (float offsets, 4-float aligned)
-  mg::DevBuf<float> fac;           // packed lower-triangular FP32 inverse per domain
+  mg::DevBuf<float> fac;           // W = L^-1 per domain, swizzled 32x32 FP32 tiles
   uint64_t fac_floats = 0;
   mg::DevBuf<uint32_t> status;
 };

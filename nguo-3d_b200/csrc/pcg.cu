@@ -102,6 +102,19 @@ int bj_apply(const float* inv, const float* r, float* z, uint32_t nb, int sms, c
   return MGUSO_OK;
 }
 
+// One x/r update with its fused r.r into PcgScalars::out (used to time the kernel alone;
+// the scalar block must not be marked done).
+int pcg_vector_update(PcgWork& w, bool mixed, int sms, cudaStream_t st) {
+  DotSink d{w.sc.p, w.partials.p, FIN_STORE, mixed};
+  const int vg = vec_grid(w.n, 256, sms);
+  if (mixed)
+    k_pcg_update<double><<<vg, 256, 0, st>>>(w.x.p, w.r.p, w.p.p, w.ap.p, w.n, d);
+  else
+    k_pcg_update<float><<<vg, 256, 0, st>>>(w.x.p, w.r.p, w.p.p, w.ap.p, w.n, d);
+  MG_CUDA(cudaGetLastError());
+  return MGUSO_OK;
+}
+
 int PcgWork::reserve(uint32_t n_) {
   n = n_;
   if (!h_sc) MG_CUDA(cudaMallocHost((void**)&h_sc, sizeof(PcgScalars)));

@@ -20,6 +20,7 @@ struct PcgOps {
 
 int pcg_run(const PcgOps& ops, PcgWork& w, float tol, uint32_t max_iter, mguso_lin_stats* out);
 int vec_grid(uint32_t n, int threads, int sms);
+int pcg_vector_update(PcgWork& w, bool mixed, int sms, cudaStream_t st);
 int bj_apply(const float* inv, const float* r, float* z, uint32_t nb, int sms, cudaStream_t st, const DotSink* d);
 
 }  // namespace mg

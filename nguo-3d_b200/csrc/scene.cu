@@ -650,3 +650,71 @@ extern "C" int mguso_scene_system(mguso_scene* sc, uint32_t* ps_rp, uint32_t* ps
   MG_CUDA(cudaStreamSynchronize(st));
   return MGUSO_OK;
 }
+
+namespace mg {
+int schwarz_factor_with(mguso_schwarz* s, const uint32_t* c_rp, const uint32_t* c_col, const float* c_val,
+                        cudaStream_t st);
+}
+
+// Mean device time of the step's linear-solver kernels at the last assembled system, each
+// timed alone over `reps` launches with CUDA events on the scene's stream:
+// us4 = {system SpMV, preconditioner apply, preconditioner factorisation, PCG vector update}
+// and bytes4 their algorithmic bytes per launch (the minimum each must move: every stored
+// block or factor entry once, the vectors once).
+extern "C" int mguso_scene_profile(mguso_scene* sc, int reps, float* us4, double* bytes4) {
+  MG_CHECK_ARG(sc && us4 && bytes4 && reps > 0, "bad argument");
+  Scene& s = sc->s;
+  cudaStream_t st = s.st;
+  const size_t n3 = 3 * (size_t)s.nv;
+  DevBuf<float> x, y;
+  MG_TRY(x.reserve(n3));
+  MG_TRY(y.reserve(n3));
+  MG_CUDA(cudaMemsetAsync(x.p, 0, 4 * n3, st));
+  uint32_t nc = 0;
+  MG_CUDA(cudaMemcpyAsync(&nc, s.c_count.p, 4, cudaMemcpyDeviceToHost, st));
+  MG_CUDA(cudaStreamSynchronize(st));
+  cudaEvent_t e0, e1;
+  MG_CUDA(cudaEventCreate(&e0));
+  MG_CUDA(cudaEventCreate(&e1));
+  auto timed = [&](auto&& fn, float* out) -> int {
+    for (int i = 0; i < 3; ++i) MG_TRY(fn());
+    MG_CUDA(cudaEventRecord(e0, st));
+    for (int i = 0; i < reps; ++i) MG_TRY(fn());
+    MG_CUDA(cudaEventRecord(e1, st));
+    MG_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    MG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    *out = 1000.f * ms / reps;
+    return MGUSO_OK;
+  };
+  int rc = MGUSO_OK;
+  const double nnz = (double)s.Ps.nnz + nc;
+  bytes4[0] = 40.0 * nnz + 8.0 * (s.nv + 1) + 24.0 * s.nv;
+  if (rc == MGUSO_OK) rc = timed([&]() { return system_spmv(s, x.p, y.p, st, nullptr); }, &us4[0]);
+  if (s.schwarz) {
+    mguso_schwarz* sw = s.schwarz.get();
+    double packed = 0;
+    for (uint32_t d = 0; d < sw->ndom; ++d) {
+      double m = 3.0 * (sw->h_dom_start[d + 1] - sw->h_dom_start[d]);
+      packed += m * (m + 1) / 2;
+    }
+    bytes4[1] = 4.0 * packed + 4.0 * s.nv + 24.0 * s.nv + 8.0 * (sw->ndom + 1);
+    bytes4[2] = 36.0 * nnz + 4.0 * packed;
+    if (rc == MGUSO_OK) rc = timed([&]() { return schwarz_apply(sw, x.p, y.p, st, nullptr); }, &us4[1]);
+    if (rc == MGUSO_OK)
+      rc = timed([&]() { return schwarz_factor_with(sw, s.c_row_ptr.p, s.c_col.p, s.c_val.p, st); }, &us4[2]);
+  } else {
+    bytes4[1] = 36.0 * s.nv + 24.0 * s.nv;
+    bytes4[2] = 36.0 * s.Ps.nnz + 36.0 * s.nv;
+    if (rc == MGUSO_OK)
+      rc = timed([&]() { return bj_apply(s.bjinv.p, x.p, y.p, s.nv, s.ctx->sm_count, st, nullptr); }, &us4[1]);
+    if (rc == MGUSO_OK) rc = timed([&]() { return blockjacobi_factor(s.A.get(), s.bjinv.p, st); }, &us4[2]);
+  }
+  // the PCG update x += a p, r -= a Ap with its fused r.r: 4 vectors in, 2 out
+  bytes4[3] = 24.0 * n3;
+  if (rc == MGUSO_OK && cudaMemsetAsync(s.work.sc.p, 0, sizeof(PcgScalars), st) != cudaSuccess) rc = MGUSO_ERR_CUDA;
+  if (rc == MGUSO_OK) rc = timed([&]() { return pcg_vector_update(s.work, s.mixed, s.ctx->sm_count, st); }, &us4[3]);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}

@@ -6,16 +6,23 @@
 // diagonal when a pivot is <= 1e-14), and z = (L L^T)^-1 r per domain.
 //
 // B200 layout: factorisation is one CTA per domain in FP64 shared memory (right-looking
-// Cholesky, then W = L^-1), and what is stored is W, packed lower-triangular in FP32
-// (16-byte aligned per domain). The apply is then two dense triangular matvecs per domain,
-// z = W^T (W r), with no sequential triangular sweeps: one warp per domain stages its
-// packed factor into shared memory with a single 1-D TMA bulk copy.
+// Cholesky, then W = L^-1), and what is stored is W in FP32 as swizzled 32 x 32 tiles of
+// its lower block-triangle (4 KB aligned per tile). The apply is two dense triangular
+// matvecs per domain, z = W^T (W r), with no sequential triangular sweeps: one warp per
+// domain stages its tiles into shared memory with a single 1-D TMA bulk copy.
 #include <algorithm>
 #include <deque>
 
 #include "reduce.cuh"
 
 namespace mg {
+
+// W is stored per domain as its lower block-triangle of 32 x 32 tiles (I, J), J <= I, in
+// the order (0,0), (1,0), (1,1), (2,0), (2,1), (2,2); element (r, c) of a tile lives at
+// c * 32 + (r ^ c). Rows and columns past m are zero.
+constexpr int TILE_FLOATS = 1024;
+__host__ __device__ __forceinline__ int tile_index(int I, int J) { return I * (I + 1) / 2 + J; }
+__host__ __device__ __forceinline__ int tile_offset(int r, int c) { return c * 32 + (r ^ c); }
 
 int schwarz_configure();
 int schwarz_factor_with(mguso_schwarz* s, const uint32_t* c_rp, const uint32_t* c_col, const float* c_val,
@@ -37,6 +44,28 @@ int schwarz_build(mguso_schwarz* s) {
   std::vector<uint32_t> loc(nb, 0);
   uint32_t D = std::max<uint32_t>(s->domain, 1);
   uint32_t max_m = 0;
+  // Vertices with no off-diagonal block (pinned collider vertices, unconnected points)
+  // would each be a one-vertex domain; they are packed D at a time instead. Their blocks
+  // do not couple, so the packed domain's factor is block diagonal and the preconditioner
+  // is unchanged (only the diagonal floor averages over the packed vertices).
+  std::vector<uint32_t> singles;
+  for (uint32_t v = 0; v < nb; ++v) {
+    bool iso = true;
+    for (uint32_t k = rp[v]; k < rp[v + 1] && iso; ++k) iso = cl[k] == v;
+    if (iso) {
+      singles.push_back(v);
+      assigned[v] = 1;
+    }
+  }
+  auto close_domain = [&](size_t base) {
+    uint32_t d = (uint32_t)s->h_dom_start.size() - 1;
+    for (size_t i = base; i < s->h_dom_verts.size(); ++i) {
+      s->h_dom_of[s->h_dom_verts[i]] = d;
+      loc[s->h_dom_verts[i]] = (uint32_t)(i - base);
+    }
+    s->h_dom_start.push_back((uint32_t)s->h_dom_verts.size());
+    max_m = std::max<uint32_t>(max_m, 3 * (uint32_t)(s->h_dom_verts.size() - base));
+  };
   for (uint32_t seed = 0; seed < nb; ++seed) {
     if (assigned[seed]) continue;
     size_t base = s->h_dom_verts.size();
@@ -56,21 +85,20 @@ int schwarz_build(mguso_schwarz* s) {
         }
       }
     }
-    uint32_t d = (uint32_t)s->h_dom_start.size() - 1;
-    for (size_t i = base; i < s->h_dom_verts.size(); ++i) {
-      s->h_dom_of[s->h_dom_verts[i]] = d;
-      loc[s->h_dom_verts[i]] = (uint32_t)(i - base);
-    }
-    s->h_dom_start.push_back((uint32_t)s->h_dom_verts.size());
-    max_m = std::max<uint32_t>(max_m, 3 * (uint32_t)(s->h_dom_verts.size() - base));
+    close_domain(base);
+  }
+  for (size_t i = 0; i < singles.size(); i += D) {
+    size_t base = s->h_dom_verts.size();
+    for (size_t j = i; j < std::min(singles.size(), i + D); ++j) s->h_dom_verts.push_back(singles[j]);
+    close_domain(base);
   }
   s->ndom = (uint32_t)s->h_dom_start.size() - 1;
   s->max_m = max_m;
   std::vector<uint64_t> off(s->ndom + 1, 0);
   for (uint32_t d = 0; d < s->ndom; ++d) {
     uint64_t m = 3ull * (s->h_dom_start[d + 1] - s->h_dom_start[d]);
-    uint64_t packed = m * (m + 1) / 2;
-    off[d + 1] = off[d] + ((packed + 3) & ~3ull);
+    uint64_t t = (m + 31) / 32;
+    off[d + 1] = off[d] + t * (t + 1) / 2 * TILE_FLOATS;
   }
   s->fac_floats = off[s->ndom];
   cudaStream_t st = a->ctx->stream;
@@ -96,7 +124,7 @@ int schwarz_build(mguso_schwarz* s) {
 //      1e-14 (linsolve.rs:88-92), so the same blocks fall back to the diagonal;
 //   3. W = L^-1, one thread per column (forward substitution), written transposed into the
 //      upper triangle.
-// Stored: W packed row-major lower-triangular in FP32. The apply forms z = W^T (W r), so
+// Stored: W in FP32 as swizzled tiles (layout above). The apply forms z = W^T (W r), so
 // the FP32 preconditioner W~^T W~ is symmetric positive definite for any rounding of W.
 // (An explicitly stored FP32 inverse is not: with stiff seams a domain block reaches a
 // condition number near 1e7 and rounding the inverse to FP32 can make it indefinite.)
@@ -186,14 +214,16 @@ __global__ void __launch_bounds__(FACTOR_THREADS) k_schwarz_factor(
   }
   __syncthreads();
   float* out = fac + fac_off[d];
+  const int T = (m + 31) / 32, nfl = T * (T + 1) / 2 * TILE_FLOATS;
   if (s_fail) {
     // reference fallback: L = diag(sqrt(ad_pp)) (1 where ad_pp <= 1e-14), i.e.
     // W = diag(1 / sqrt(ad_pp))
-    for (int e = tid; e < m * (m + 1) / 2; e += nt) out[e] = 0.0f;
+    for (int e = tid; e < nfl; e += nt) out[e] = 0.0f;
     __syncthreads();
     for (int r = tid; r < m; r += nt) {
       double a = diag0[r];
-      out[r * (r + 1) / 2 + r] = (float)(a > 1e-14 ? 1.0 / sqrt(a) : 1.0);
+      const int I = r >> 5, lr = r & 31;
+      out[tile_index(I, I) * TILE_FLOATS + tile_offset(lr, lr)] = (float)(a > 1e-14 ? 1.0 / sqrt(a) : 1.0);
     }
     if (tid == 0) atomicOr(status, 1u << 8);
     return;
@@ -219,8 +249,14 @@ __global__ void __launch_bounds__(FACTOR_THREADS) k_schwarz_factor(
     }
   }
   __syncthreads();
-  for (int i = w; i < m; i += nw)
-    for (int j = lane; j <= i; j += 32) out[i * (i + 1) / 2 + j] = (float)A[j * ld + i];
+  // tiles in storage order; e walks each tile's swizzled offsets so the stores coalesce
+  for (int e = tid; e < nfl; e += nt) {
+    const int t = e / TILE_FLOATS, o = e - t * TILE_FLOATS;
+    const int I = t >= 3 ? 2 : (t >= 1 ? 1 : 0), J = t - I * (I + 1) / 2;
+    const int c = o >> 5, r = (o & 31) ^ c;
+    const int gi = 32 * I + r, gj = 32 * J + c;
+    out[e] = (gi < m && gj <= gi) ? (float)A[gj * ld + gi] : 0.0f;
+  }
 }
 
 int schwarz_factor(mguso_schwarz* s, cudaStream_t st) {
@@ -240,65 +276,127 @@ int schwarz_factor_with(mguso_schwarz* s, const uint32_t* c_rp, const uint32_t* 
 }
 
 // ---------------------------------------------------------------------------------------
-// Apply: one warp per domain. Per-warp shared slice: mbarrier, the packed factor W (bulk
-// copied), the gathered residual and W r.
+// Apply: one warp per domain (grid-stride over domains). The warp bulk-copies its domain's
+// W tiles into its shared slice, gathers r, then
+//   pass 1: y = W r    lane = row within a row tile, loop over columns c;
+//   pass 2: z = W^T y  lane = column within a column tile, loop over rows r.
+// The swizzled tile offset c*32 + (r ^ c) makes both passes free of bank conflicts. Every
+// lane carries one accumulator per tile row/column (<= 3), so there are no long serial
+// chains. Acc = double (mixed precision) accumulates in FP64.
 // ---------------------------------------------------------------------------------------
+template <int T, class Acc>
+__device__ __forceinline__ void tiles_apply(const float* __restrict__ w, const float* __restrict__ rd,
+                                            Acc* __restrict__ yd, Acc (&z)[3], int lane) {
+  const float* t00 = w;
+  const float* t10 = w + 1 * TILE_FLOATS;
+  const float* t11 = w + 2 * TILE_FLOATS;
+  const float* t20 = w + 3 * TILE_FLOATS;
+  const float* t21 = w + 4 * TILE_FLOATS;
+  const float* t22 = w + 5 * TILE_FLOATS;
+  Acc y0 = 0, y1 = 0, y2 = 0;
+#pragma unroll 8
+  for (int c = 0; c < 32; ++c) {
+    const int o = tile_offset(lane, c);
+    const Acc a0 = (Acc)rd[c];
+    y0 += (Acc)t00[o] * a0;
+    if (T > 1) {
+      const Acc a1 = (Acc)rd[32 + c];
+      y1 += (Acc)t10[o] * a0 + (Acc)t11[o] * a1;
+      if (T > 2) {
+        const Acc a2 = (Acc)rd[64 + c];
+        y2 += (Acc)t20[o] * a0 + (Acc)t21[o] * a1 + (Acc)t22[o] * a2;
+      }
+    }
+  }
+  yd[lane] = y0;
+  if (T > 1) yd[32 + lane] = y1;
+  if (T > 2) yd[64 + lane] = y2;
+  __syncwarp();
+  Acc z0 = 0, z1 = 0, z2 = 0;
+#pragma unroll 8
+  for (int r = 0; r < 32; ++r) {
+    const int o = tile_offset(r, lane);
+    const Acc b0 = yd[r];
+    z0 += (Acc)t00[o] * b0;
+    if (T > 1) {
+      const Acc b1 = yd[32 + r];
+      z0 += (Acc)t10[o] * b1;
+      z1 += (Acc)t11[o] * b1;
+      if (T > 2) {
+        const Acc b2 = yd[64 + r];
+        z0 += (Acc)t20[o] * b2;
+        z1 += (Acc)t21[o] * b2;
+        z2 += (Acc)t22[o] * b2;
+      }
+    }
+  }
+  z[0] = z0;
+  z[1] = z1;
+  z[2] = z2;
+}
+
+constexpr int APPLY_WARPS = 4;
+constexpr uint32_t APPLY_SLICE = 6 * TILE_FLOATS + 96 + 2 * 96;  // tiles, r, W r (Acc)
+
 template <int WARPS, class Acc>
 __global__ void __launch_bounds__(32 * WARPS) k_schwarz_apply(
     const uint32_t* __restrict__ dom_start, const uint32_t* __restrict__ dom_verts,
     const uint64_t* __restrict__ fac_off, const float* __restrict__ fac, const float* __restrict__ r,
-    float* __restrict__ z, uint32_t ndom, uint32_t slice_floats, uint32_t* status, DotSink dot, int with_dot) {
+    float* __restrict__ z, uint32_t ndom, uint32_t* status, DotSink dot, int with_dot) {
   extern __shared__ __align__(128) unsigned char smem[];
   if (with_dot && dot.sc->done) return;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   uint64_t* bar = (uint64_t*)(smem + 16 * w);
-  float* buf = (float*)(smem + 128 + (size_t)w * slice_floats * 4);
-  float* rd = buf + (slice_floats - 288);        // gathered residual
-  Acc* yd = (Acc*)(buf + (slice_floats - 192));  // W r
-  const uint32_t d = blockIdx.x * WARPS + w;
+  float* buf = (float*)(smem + 128 + (size_t)w * APPLY_SLICE * 4);
+  float* rd = buf + 6 * TILE_FLOATS;
+  Acc* yd = (Acc*)(rd + 96);
   Acc acc = 0;
-  bool ok = true;
-  if (d < ndom) {
+  if (lane == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+  }
+  __syncwarp();
+  uint32_t phase = 0;
+  for (uint32_t d = blockIdx.x * WARPS + w; d < ndom; d += gridDim.x * WARPS) {
     const uint32_t vs = dom_start[d], nvd = dom_start[d + 1] - vs;
     const int m = 3 * (int)nvd;
     const uint64_t off = fac_off[d];
     const uint32_t bytes = (uint32_t)((fac_off[d + 1] - off) * 4);
     if (lane == 0) {
-      mbar_init(bar, 1);
-      fence_mbar_init();
-    }
-    __syncwarp();
-    if (lane == 0) {
       fence_proxy_async();
       mbar_arrive_expect_tx(bar, bytes);
       bulk_g2s(buf, fac + off, bytes, bar);
     }
-    for (int i = lane; i < m; i += 32) {
-      uint32_t v = dom_verts[vs + i / 3];
-      rd[i] = r[3 * v + i % 3];
+    for (int i = lane; i < 96; i += 32) {
+      float v = 0.f;
+      if (i < m) v = r[3 * dom_verts[vs + i / 3] + i % 3];
+      rd[i] = v;
     }
     __syncwarp();
-    ok = mbar_wait(bar, 0);
-    if (ok) {
-      // Acc = double (mixed precision) accumulates both matvecs in FP64: the entries of W
-      // span the square root of the domain's condition number and cancel in W r.
-      for (int i = lane; i < m; i += 32) {  // y = W r, rows of the packed lower triangle
-        Acc s = 0;
-        const int ri = i * (i + 1) / 2;
-        for (int j = 0; j <= i; ++j) s += (Acc)buf[ri + j] * (Acc)rd[j];
-        yd[i] = s;
-      }
-      __syncwarp();
-      for (int i = lane; i < m; i += 32) {  // z = W^T y, columns
-        Acc s = 0;
-        for (int j = i; j < m; ++j) s += (Acc)buf[j * (j + 1) / 2 + i] * yd[j];
-        uint32_t v = dom_verts[vs + i / 3];
-        z[3 * v + i % 3] = (float)s;
-        acc += (Acc)rd[i] * (Acc)s;
-      }
-    } else if (lane == 0) {
-      atomicOr(status, ST_WAIT_TIMEOUT);
+    if (!mbar_wait(bar, phase)) {
+      if (lane == 0) atomicOr(status, ST_WAIT_TIMEOUT);
+      mbar_wait(bar, phase);  // the copy may still land: bounded second wait, then stop
+      break;
     }
+    phase ^= 1;
+    Acc zz[3];
+    const int T = (m + 31) >> 5;
+    if (T == 3)
+      tiles_apply<3, Acc>(buf, rd, yd, zz, lane);
+    else if (T == 2)
+      tiles_apply<2, Acc>(buf, rd, yd, zz, lane);
+    else
+      tiles_apply<1, Acc>(buf, rd, yd, zz, lane);
+#pragma unroll
+    for (int J = 0; J < 3; ++J) {
+      const int i = 32 * J + lane;
+      if (i < m) {
+        const float zi = (float)zz[J];
+        z[3 * dom_verts[vs + i / 3] + i % 3] = zi;
+        acc += (Acc)rd[i] * (Acc)zi;
+      }
+    }
+    __syncwarp();  // every lane is done with buf before the next copy overwrites it
   }
   if (with_dot) grid_dot_commit<Acc>(dot, acc);
 }
@@ -308,41 +406,30 @@ __global__ void __launch_bounds__(32 * WARPS) k_schwarz_apply(
 int schwarz_configure() {
   static bool done = false;
   if (done) return MGUSO_OK;
-  constexpr int WARPS = 4;
   size_t fsm = sizeof(double) * (96 * 97 + 2 * 96);
   MG_CUDA(cudaFuncSetAttribute(k_schwarz_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
-  uint32_t slice = ((96 * 97 / 2 + 3) & ~3u) + 288;
-  slice = (slice + 31) & ~31u;
-  size_t asmem = 128 + (size_t)WARPS * slice * 4;
-  MG_CUDA(cudaFuncSetAttribute(k_schwarz_apply<WARPS, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  size_t asmem = 128 + (size_t)APPLY_WARPS * APPLY_SLICE * 4;
+  MG_CUDA(cudaFuncSetAttribute(k_schwarz_apply<APPLY_WARPS, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)asmem));
-  MG_CUDA(cudaFuncSetAttribute(k_schwarz_apply<WARPS, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  MG_CUDA(cudaFuncSetAttribute(k_schwarz_apply<APPLY_WARPS, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)asmem));
   done = true;
   return MGUSO_OK;
 }
 
 int schwarz_apply(mguso_schwarz* s, const float* r, float* z, cudaStream_t st, const DotSink* dot) {
-  constexpr int WARPS = 4;
   DotSink d{};
   int with_dot = dot ? 1 : 0;
   if (dot) d = *dot;
   bool mixed = dot && dot->mixed;
-  uint32_t mm = std::max<uint32_t>(s->max_m, 3);
-  uint32_t packed = (mm * (mm + 1) / 2 + 3) & ~3u;
-  uint32_t slice = packed + 288;  // factor + gathered residual (96 floats) + W r (96 Acc)
-  slice = (slice + 31) & ~31u;
-  size_t smem = 128 + (size_t)WARPS * slice * 4;
-  uint32_t grid = ceil_div(s->ndom, WARPS);
-  if (with_dot && grid > (uint32_t)MAX_PARTIALS) {
-    set_error("Schwarz apply with fused dot: too many domains for one partial per CTA");
-    return MGUSO_ERR_UNSUPPORTED;
-  }
-  if (mm > 96) {
+  if (s->max_m > 96) {
     set_error("Schwarz domain larger than 32 vertices");
     return MGUSO_ERR_UNSUPPORTED;
   }
-  void* fn = mixed ? (void*)k_schwarz_apply<WARPS, double> : (void*)k_schwarz_apply<WARPS, float>;
+  size_t smem = 128 + (size_t)APPLY_WARPS * APPLY_SLICE * 4;
+  // two resident CTAs per SM, grid-stride over the domains
+  uint32_t grid = std::min<uint32_t>(ceil_div(s->ndom, APPLY_WARPS), 2u * (uint32_t)s->a->ctx->sm_count);
+  void* fn = mixed ? (void*)k_schwarz_apply<APPLY_WARPS, double> : (void*)k_schwarz_apply<APPLY_WARPS, float>;
   const uint32_t* a0 = s->dom_start.p;
   const uint32_t* a1 = s->dom_verts.p;
   const uint64_t* a2 = s->fac_off.p;
@@ -350,9 +437,9 @@ int schwarz_apply(mguso_schwarz* s, const float* r, float* z, cudaStream_t st, c
   uint32_t nd = s->ndom;
   uint32_t* stp = s->status.p;
   void* args[] = {(void*)&a0, (void*)&a1, (void*)&a2, (void*)&a3, (void*)&r, (void*)&z,
-                  (void*)&nd, (void*)&slice, (void*)&stp, (void*)&d, (void*)&with_dot};
+                  (void*)&nd, (void*)&stp, (void*)&d, (void*)&with_dot};
   if (grid == 0) return MGUSO_OK;
-  MG_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(32 * WARPS), args, smem, st));
+  MG_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(32 * APPLY_WARPS), args, smem, st));
   return MGUSO_OK;
 }
 

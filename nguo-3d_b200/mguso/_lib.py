@@ -79,6 +79,7 @@ def load() -> C.CDLL:
         "mguso_bsr_spmv_host": (i32, [vp, vp, vp]),
         "mguso_bsr_set_kernel": (i32, [vp, i32, P(i32)]),
         "mguso_bsr_autotune": (i32, [vp, P(f32)]),
+        "mguso_bsr_kernel": (i32, [vp, P(C.c_int), P(C.c_int), P(C.c_int)]),
         "mguso_schwarz_create": (i32, [vp, u32, P(vp)]),
         "mguso_schwarz_destroy": (i32, [vp]),
         "mguso_schwarz_info": (i32, [vp, P(u32), P(u64)]),

@@ -154,6 +154,13 @@ class Bsr:
         check(self.lib.mguso_bsr_set_kernel(self.h, variant, C.byref(act)))
         return act.value
 
+    def kernel(self) -> dict:
+        """The SpMV variant in use: {"variant": name, "tile_rows": r, "stages": s}."""
+        v, r, st = C.c_int(), C.c_int(), C.c_int()
+        check(self.lib.mguso_bsr_kernel(self.h, C.byref(v), C.byref(r), C.byref(st)))
+        name = {0: "auto", 1: "tma", 2: "direct", 3: "sliced_ell"}.get(v.value, str(v.value))
+        return {"variant": name, "tile_rows": r.value, "stages": st.value}
+
     def autotune(self) -> float:
         us = C.c_float()
         check(self.lib.mguso_bsr_autotune(self.h, C.byref(us)))

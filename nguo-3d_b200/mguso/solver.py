@@ -57,6 +57,7 @@ def _sigs(lib):
         ("mguso_scene_info", i32, [vp, vp]),
         ("mguso_scene_spmv_time", i32, [vp, i32, P(C.c_float), P(C.c_double)]),
         ("mguso_scene_assemble", i32, [vp, vp, vp, vp]),
+        ("mguso_scene_profile", i32, [vp, i32, vp, vp]),
         ("mguso_scene_system", i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
         ("mguso_scene_stencils", i32, [vp, C.c_uint32, vp, vp, vp, vp]),
     ]:
@@ -152,6 +153,15 @@ class ImplicitSolver:
         us, b = C.c_float(), C.c_double()
         check(self.lib.mguso_scene_spmv_time(self.h, reps, C.byref(us), C.byref(b)))
         return us.value, b.value
+
+    def profile(self, reps: int = 100) -> dict:
+        """Per-kernel device time (us) and algorithmic bytes of the linear solver at the last
+        assembled system: spmv, precond_apply, precond_factor, pcg_update."""
+        us = np.zeros(4, np.float32)
+        by = np.zeros(4, np.float64)
+        check(self.lib.mguso_scene_profile(self.h, reps, ptr(us), ptr(by)))
+        names = ["spmv", "precond_apply", "precond_factor", "pcg_update"]
+        return {k: (float(u), float(b)) for k, u, b in zip(names, us, by)}
 
     def assemble(self, x, x_tilde=None) -> dict:
         """One Newton-system assembly at positions ``x`` (inertia target ``x_tilde``, ``x``

@@ -141,3 +141,59 @@ def test_pcg_reports_cap_and_breakdown(ctx):
     assert s.last_stats().iters == 3 and s.last_stats().status == 4  # PCG_CAP
     x = s.solve(A, np.zeros(N, np.float32), 1e-6, 100)  # b = 0: pAp = 0 -> break, x = 0
     assert np.all(x == 0) and s.last_stats().iters == 0
+
+
+def grid_with_isolated(n=17, extra=70, seed=6):
+    """A cloth-grid matrix plus `extra` vertices that own only a diagonal block (pinned
+    collider vertices look like this), interleaved with the grid's vertices."""
+    nb0, rp0, col0, val0 = scenes.grid_bsr(n, seed)
+    nb = nb0 + extra
+    iso = np.sort(np.random.default_rng(seed).choice(nb, extra, replace=False))
+    is_iso = np.zeros(nb, bool)
+    is_iso[iso] = True
+    new_of_old = np.flatnonzero(~is_iso).astype(np.int64)  # grid vertex g -> new index
+    rows, cols, vals = [], [], []
+    for g in range(nb0):
+        for k in range(rp0[g], rp0[g + 1]):
+            rows.append(new_of_old[g])
+            cols.append(new_of_old[col0[k]])
+            vals.append(val0[k])
+    for v in iso:
+        rows.append(v)
+        cols.append(v)
+        vals.append(np.eye(3, dtype=np.float32) * np.float32(2.0 + v % 5))
+    order = np.lexsort((np.array(cols), np.array(rows)))
+    rows, cols = np.array(rows)[order], np.array(cols)[order]
+    vals = np.array(vals, np.float32).reshape(-1, 9)[order]
+    rp = np.zeros(nb + 1, np.uint32)
+    np.add.at(rp, rows + 1, 1)
+    rp = np.cumsum(rp).astype(np.uint32)
+    return nb, rp, cols.astype(np.uint32), vals.reshape(-1, 3, 3).astype(np.float32), iso
+
+
+def test_schwarz_packs_isolated_vertices(ctx):
+    """Vertices without off-diagonal blocks are packed D per domain instead of forming one
+    domain each; every other vertex keeps the oracle's BFS domain, and the apply still
+    matches the oracle's additive Schwarz (the packed blocks do not couple)."""
+    import torch
+    nb, rp, col, val, iso = grid_with_isolated()
+    N, srp, sci, svv = scenes.bsr_to_csr(nb, rp, col, val)
+    a = Bsr(ctx, nb, rp, col, val)
+    s = Schwarz(a, 32)
+    want, nd = O.schwarz_domains(N, srp, sci, 32)
+    got = s.domains()
+    assert s.ndomains == nd - len(iso) + (len(iso) + 31) // 32
+    conn = np.setdiff1d(np.arange(nb), iso)
+    # same partition of the connected vertices (domain ids may be renumbered)
+    pairs = set(zip(got[conn].tolist(), want[conn].tolist()))
+    assert len(pairs) == len(set(got[conn].tolist())) == len(set(want[conn].tolist()))
+    assert len(set(got[iso].tolist())) == (len(iso) + 31) // 32
+    st = torch.cuda.current_stream().cuda_stream
+    s.factor(st)
+    r = np.random.default_rng(9).standard_normal(N).astype(np.float32)
+    rd, zd = torch_dev(r), torch.zeros(N, device="cuda")
+    s.apply(rd.data_ptr(), zd.data_ptr(), st)
+    torch.cuda.synchronize()
+    z = zd.cpu().numpy()
+    ref = O.schwarz_apply(N, srp, sci, svv, 32, r.astype(np.float64))
+    assert np.abs(z - ref).max() <= 1e-4 * np.abs(ref).max()

@@ -103,3 +103,76 @@ def test_self_contact_stencils_and_step(ctx, precision):
         assert sg["stencils"] == so["stencils"], (k, sg["stencils"], so["stencils"])
         assert abs(sg["newton_iters"] - so["newton_iters"]) <= 1
         assert rel < 2e-2, (k, rel)
+
+
+def coarse_sheath(**kw):
+    """The garment configuration at a coarser resolution (30 mm edges, 1 740-triangle torso)."""
+    return scenes.sheath_on_torso(edge=0.03, torso_res=(30, 29), **kw)
+
+
+def _mid_step_state(sc):
+    """Positions after the oracle's first Newton iteration of step 0 (seams closing, cloth
+    near itself and the torso) and the step's inertia target."""
+    sc1 = dict(sc)
+    sc1["params"] = dict(sc["params"], newton_iters=1)
+    o = O.OracleSolver(sc1)
+    o.step(1, check_intersection=False)
+    x1 = o.positions().astype(np.float32)
+    x0 = sc["positions"].astype(np.float32)
+    dt = sc["params"]["dt"]
+    grav = np.array(sc["params"]["gravity"], np.float32)
+    free = sc["inv_mass"][:, None] > 0
+    xt = (x0 + np.where(free, dt * sc["velocities"] + dt * dt * grav[None, :], 0)).astype(np.float32)
+    return x1, xt
+
+
+def _bsr_sum(a, nv):
+    import scipy.sparse as sp
+
+    rp, col, val = a["ps"]
+    m = sp.bsr_matrix((val.astype(np.float64), col.astype(np.int64), rp.astype(np.int64)), shape=(3 * nv, 3 * nv))
+    crp, ccol, cval = a["c"]
+    if len(ccol):
+        m = m + sp.bsr_matrix((cval.astype(np.float64), ccol.astype(np.int64), crp.astype(np.int64)),
+                              shape=(3 * nv, 3 * nv))
+    return m.tocsr()
+
+
+def test_sheath_assembly_matches_oracle_fp32(ctx):
+    """One Newton system of the seamed sheath (stitches, StVK shells, hinges, static torso
+    collider and self contact): the FP32 stencil set equals the oracle's, and every matrix
+    and right-hand-side entry agrees to a few FP32 ulps (the contact sums are added to the
+    elastic slot as one term, the reference adds them one by one)."""
+    import scipy.sparse as sp
+
+    sc = coarse_sheath()
+    nv = sc["positions"].shape[0]
+    x1, xt = _mid_step_state(sc)
+    g = ImplicitSolver(ctx, sc, "fp32")
+    a = g.assemble(x1, xt)
+    gi, gk, gd = g.stencils()
+    o = O.OracleSolver(sc)
+    o.set_state(x1, sc["velocities"])
+    oi, od = o.stencils()
+    assert a["stencils"] > 100
+    assert set(map(tuple, gi.tolist())) == set(map(tuple, oi.tolist()))
+    (orp, oci, ovv), orhs = o.assemble(x1, xt)
+    ao = sp.csr_matrix((ovv.astype(np.float64), oci.astype(np.int64), orp.astype(np.int64)), shape=(3 * nv, 3 * nv))
+    ag = _bsr_sum(a, nv)
+    d = abs(ag - ao)
+    ulp = np.spacing(np.float32(abs(ao).max()))
+    assert d.max() <= 8 * ulp, (d.max(), ulp)
+    assert np.abs(a["rhs"] - orhs).max() <= 1e-5 * np.abs(orhs).max()
+
+
+def test_sheath_steps_match_oracle(ctx):
+    """Seamed sheath steps from identical states: Newton counts within +-1, positions within
+    1e-3 of the step's displacement (FP32 and mixed)."""
+    sc = coarse_sheath()
+    for prec in ("fp32", "mixed"):
+        g, o, out = run_pair(ctx, sc, 3, prec)
+        for k, sg, so, rel in out:
+            assert sg["status"] == 0 and sg["all_finite"] and sg["penetration_free"]
+            assert abs(sg["newton_iters"] - so["newton_iters"]) <= 1, (prec, k)
+            assert rel < 1e-3, (prec, k, rel)
+        assert max(sg["stencils"] for _, sg, _, _ in out) > 100
