@@ -168,6 +168,19 @@ int mguso_lbvh_build_query(mguso_ctx* ctx, const float* positions, uint32_t nv, 
  * u32 keys when key_bits <= 32, u64 keys otherwise. Replaces GpuRadixSort::sort_pairs
  * (radix.rs:112-352), which is limited to 65 536 keys. */
 int mguso_radix_sort_pairs(mguso_ctx* ctx, void* keys, uint32_t* vals, uint32_t n, int key_bits, void* stream);
+/* Allocation-free variant of mguso_radix_sort_pairs, with no counterpart in the reference.
+ * For callers that may not allocate device memory once they are running (a host engine
+ * that gives all of the GPU's memory to its own pool at start-up, or a per-frame path that
+ * cannot afford cudaMalloc's device-wide synchronisation): it allocates nothing and needs
+ * no context. Its temporaries live in one fixed 3.2 MiB device array inside this library
+ * (on every device that loads it, until the process exits), which limits n to 262 144
+ * pairs; larger n returns MGUSO_ERR_INVALID_ARG. Sorts the same (key, payload) pairs in
+ * place on the current device, stably, with the same result as mguso_radix_sort_pairs, and
+ * returns when the sort has finished on `stream`. The first call on each device looks up
+ * the array's device address once; make that first call before any stream capture. All
+ * calls share the one array, so calls that overlap on the GPU (other streams, other host
+ * threads) race and must be serialised by the caller. */
+int mguso_radix_sort_pairs_noalloc(void* keys, uint32_t* vals, uint32_t n, int key_bits, void* stream);
 
 /* ---- Implicit step: scene build -> step -> readback --------------------------------- */
 /* Solver knobs, named and defaulted as ImplicitParams (implicit.rs:30-229). Fields that

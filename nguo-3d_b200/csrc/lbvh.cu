@@ -12,6 +12,8 @@
 // boxes (bvh_traverse.wgsl:64-92).
 #include <algorithm>
 #include <cstring>
+#include <mutex>
+#include <string>
 
 #include "lbvh.cuh"
 
@@ -597,4 +599,114 @@ int lbvh_query_points(Lbvh* b, const float* pts, uint32_t np, float dhat, uint32
   return MGUSO_OK;
 }
 
+// ---------------------------------------------------------------------------------------
+// Allocation-free pair sort. Some callers may not allocate device memory after start-up:
+// a host engine that hands all of the GPU's memory to its own pool when it starts, or a
+// per-frame path where cudaMalloc's implicit device-wide synchronisation would stall the
+// other streams. mguso_radix_sort_pairs_noalloc runs the same onesweep passes as
+// radix_sort_pairs, with its temporaries in one fixed file-scope device array instead of
+// buffers that grow on demand.
+//
+// Differences from radix_sort_pairs: every digit pass runs (no host read-back of the
+// histogram to skip passes whose digit is constant; such a pass is the identity for a
+// stable sort, so the output is the same), and the call waits for the sort to finish so it
+// can report a look-back timeout from the scratch's error word.
+// ---------------------------------------------------------------------------------------
+constexpr uint32_t NOALLOC_MAX_PAIRS = 1u << 18;  // 262 144 pairs
+constexpr size_t NA_TMPK = 0;                                         // u64 keys, ping-pong
+constexpr size_t NA_TMPV = NA_TMPK + 8 * (size_t)NOALLOC_MAX_PAIRS;   // u32 payloads
+constexpr size_t NA_STATUS = NA_TMPV + 4 * (size_t)NOALLOC_MAX_PAIRS; // look-back flags
+constexpr size_t NA_HIST = NA_STATUS + 4 * 256 * (size_t)(NOALLOC_MAX_PAIRS / RS_TILE);
+constexpr size_t NA_OFS = NA_HIST + 4 * 8 * 256;
+constexpr size_t NA_MISC = NA_OFS + 4 * 8 * 256;  // [0] tile counter, [1] error word
+constexpr size_t NA_BYTES = NA_MISC + 256;         // 3.2 MiB per device
+static_assert(NOALLOC_MAX_PAIRS % RS_TILE == 0, "scratch holds whole tiles");
+
+// Every device that loads the library holds this array until the process exits. Host code
+// must not pass the symbol itself to a kernel: its device address comes from
+// cudaGetSymbolAddress, taken once per device below.
+static __device__ __align__(256) unsigned char g_noalloc_sort_scratch[NA_BYTES];
+
+constexpr int NA_MAX_DEVICES = 64;
+static std::mutex g_noalloc_mu;
+static unsigned char* g_noalloc_ptr[NA_MAX_DEVICES] = {};
+
+// Device address of the scratch array on the current device (looked up on first use).
+static int noalloc_scratch(unsigned char** out) {
+  int dev = 0;
+  MG_CUDA(cudaGetDevice(&dev));
+  MG_CHECK_ARG(dev >= 0 && dev < NA_MAX_DEVICES, "device index beyond the allocation-free sort's table");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_sort_scratch);
+    if (e != cudaSuccess || !p) {
+      set_error(std::string("cudaGetSymbolAddress(sort scratch): ") + cudaGetErrorString(e));
+      return MGUSO_ERR_CUDA;
+    }
+    g_noalloc_ptr[dev] = (unsigned char*)p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return MGUSO_OK;
+}
+
+template <class K>
+static int noalloc_sort(unsigned char* sc, K* keys, uint32_t* vals, uint32_t n, int key_bits, cudaStream_t s) {
+  const int passes = (key_bits + 7) / 8;
+  const uint32_t ntiles = ceil_div(n, RS_TILE);
+  uint32_t* hist = (uint32_t*)(sc + NA_HIST);
+  uint32_t* ofs = (uint32_t*)(sc + NA_OFS);
+  uint32_t* status = (uint32_t*)(sc + NA_STATUS);
+  uint32_t* counter = (uint32_t*)(sc + NA_MISC);
+  uint32_t* err = counter + 1;
+  // the array keeps the previous call's contents: clear what the passes accumulate into
+  MG_CUDA(cudaMemsetAsync(hist, 0, 4 * 8 * 256, s));
+  MG_CUDA(cudaMemsetAsync(err, 0, 4, s));
+  const int sms = device_sm_count();
+  k_rs_hist<K><<<std::min<uint32_t>(ceil_div(n, 256), sms * 8), 256, 0, s>>>(keys, n, passes, hist);
+  k_rs_scan<<<passes, 256, 0, s>>>(hist, ofs);
+  MG_CUDA(cudaGetLastError());
+  K* kA = keys;
+  uint32_t* vA = vals;
+  K* kB = (K*)(sc + NA_TMPK);
+  uint32_t* vB = (uint32_t*)(sc + NA_TMPV);
+  for (int p = 0; p < passes; ++p) {
+    MG_CUDA(cudaMemsetAsync(status, 0, 4 * (size_t)ntiles * 256, s));
+    MG_CUDA(cudaMemsetAsync(counter, 0, 4, s));
+    k_onesweep<K><<<ntiles, RS_THREADS, 0, s>>>(kA, vA, kB, vB, n, 8 * p, ofs + p * 256, status, counter, err);
+    MG_CUDA(cudaGetLastError());
+    std::swap(kA, kB);
+    std::swap(vA, vB);
+  }
+  if (kA != keys) {
+    MG_CUDA(cudaMemcpyAsync(keys, kA, sizeof(K) * (size_t)n, cudaMemcpyDeviceToDevice, s));
+    MG_CUDA(cudaMemcpyAsync(vals, vA, 4 * (size_t)n, cudaMemcpyDeviceToDevice, s));
+  }
+  uint32_t h_err = 0;
+  MG_CUDA(cudaMemcpyAsync(&h_err, err, 4, cudaMemcpyDeviceToHost, s));
+  MG_CUDA(cudaStreamSynchronize(s));
+  if (h_err & ST_WAIT_TIMEOUT) {
+    set_error("allocation-free sort: a decoupled look-back wait timed out");
+    return MGUSO_ERR_TIMEOUT;
+  }
+  return MGUSO_OK;
+}
+
 }  // namespace mg
+
+extern "C" int mguso_radix_sort_pairs_noalloc(void* keys, uint32_t* vals, uint32_t n, int key_bits, void* stream) {
+  using namespace mg;
+  MG_CHECK_ARG(key_bits >= 1 && key_bits <= 64, "key_bits must be in [1, 64]");
+  if (n > NOALLOC_MAX_PAIRS) {
+    set_error("mguso_radix_sort_pairs_noalloc: n = " + std::to_string(n) +
+              " exceeds its fixed scratch limit of 262144 pairs; use mguso_radix_sort_pairs");
+    return MGUSO_ERR_INVALID_ARG;
+  }
+  MG_CHECK_ARG(n == 0 || (keys && vals), "null argument");
+  unsigned char* sc = nullptr;
+  MG_TRY(noalloc_scratch(&sc));
+  if (n <= 1) return MGUSO_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (key_bits <= 32) return noalloc_sort<uint32_t>(sc, (uint32_t*)keys, vals, n, key_bits, s);
+  return noalloc_sort<uint64_t>(sc, (uint64_t*)keys, vals, n, key_bits, s);
+}

@@ -83,3 +83,15 @@ def build_query(ctx, positions: np.ndarray, tris: np.ndarray, key_bits: int, dha
 
 def radix_sort_pairs(ctx, keys_dev: int, vals_dev: int, n: int, key_bits: int, stream: int = 0):
     check(ctx.lib.mguso_radix_sort_pairs(ctx.h, keys_dev, vals_dev, n, key_bits, stream))
+
+
+# The allocation-free sort keeps its temporaries in a fixed device array of the library.
+NOALLOC_MAX_PAIRS = 1 << 18
+
+
+def radix_sort_pairs_noalloc(keys_dev: int, vals_dev: int, n: int, key_bits: int, stream: int = 0):
+    """Sorts (key, payload) pairs in place on the current device without allocating device
+    memory, for hosts that may not allocate once running (all memory handed to their own
+    pool, or no room for cudaMalloc's device-wide synchronisation in a per-frame path).
+    n <= NOALLOC_MAX_PAIRS; overlapping calls share the scratch array and race."""
+    check(_lib.load().mguso_radix_sort_pairs_noalloc(keys_dev, vals_dev, n, key_bits, stream))
