@@ -216,6 +216,8 @@ typedef struct {
   int precond;
   uint32_t schwarz_domain;
   int precision;
+  int pcg_mode;            /* 0: one cooperative persistent launch per linear solve (default);
+                              1: one launch per PCG kernel, replayed as CUDA graphs */
 } mguso_params;
 
 /* One scene (Scene::build_implicit + the set_* calls of implicit.rs). All pointers host;

@@ -131,10 +131,17 @@ struct DotSink {
 
 constexpr int MAX_PARTIALS = 4096;
 
+// Persistent PCG: instances per launch and each instance's result.
+constexpr int PCG_MAX_INST = 8;
+struct PcgInstResult {
+  double residual;
+  uint32_t iters, status, done, pad;
+};
+
 // Device vectors, scalars and the cached CUDA graph of one PCG operator.
 struct PcgWork {
   uint32_t n = 0;
-  DevBuf<float> b, x, r, z, p, ap;
+  DevBuf<float> b, x, r, z, p, ap, p2;  // p2: second direction buffer (persistent PCG)
   DevBuf<PcgScalars> sc;
   DevBuf<double> partials;
   PcgScalars* h_sc = nullptr;  // pinned

@@ -65,6 +65,7 @@ int scene_build(Scene& s, const mguso_scene_desc* d) {
   s.nv = nv;
   s.nt = nt;
   s.mixed = d->params.precision == MGUSO_PRECISION_MIXED;
+  MG_CHECK_ARG(d->params.pcg_mode == 0 || d->params.pcg_mode == 1, "scene: pcg_mode must be 0 or 1");
   s.st = s.ctx->stream;
   cudaStream_t st = s.st;
   const float* P = d->positions;

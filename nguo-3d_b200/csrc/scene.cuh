@@ -102,6 +102,14 @@ struct Scene {
   DevBuf<unsigned long long> side_best;     // per vertex (d2 bits << 32 | tri)
   DevBuf<Stencil> stencils, stencils_sorted;
   uint32_t last_nst = 0;  // stencils of the last mguso_scene_assemble
+  // persistent PCG: grid (-1 until configured, 0 when it cannot be resident), barrier words,
+  // per-instance results and the instance row offsets
+  int pp_grid = -1;
+  DevBuf<uint32_t> pp_bar, pp_inst;
+  DevBuf<PcgInstResult> pp_out;
+  DevBuf<uint64_t> pp_probe;
+  DevBuf<double> pp_part;
+  std::vector<uint32_t> pp_key;  // instance rows the uploaded layout was built for
   DevBuf<unsigned long long> st_keys;
   DevBuf<uint32_t> st_ids;
   // contact contributions (32 blocks + 4 gradient entries per stencil)
@@ -141,6 +149,7 @@ int system_spmv(Scene& s, const float* p, float* ap, cudaStream_t st, const DotS
 
 // contact (contact.cu)
 int build_bvhs(Scene& s, const float* x);
+int pcg_persistent(Scene& s, const uint32_t* h_inst_row, uint32_t ninst, PcgInstResult* out);
 int collect_stencils(Scene& s, uint32_t* nst);
 int ccd_step(Scene& s, float* t_out, uint32_t* cap_hits);
 

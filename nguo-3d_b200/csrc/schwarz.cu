@@ -14,15 +14,9 @@
 #include <deque>
 
 #include "reduce.cuh"
+#include "tiles.cuh"
 
 namespace mg {
-
-// W is stored per domain as its lower block-triangle of 32 x 32 tiles (I, J), J <= I, in
-// the order (0,0), (1,0), (1,1), (2,0), (2,1), (2,2); element (r, c) of a tile lives at
-// c * 32 + (r ^ c). Rows and columns past m are zero.
-constexpr int TILE_FLOATS = 1024;
-__host__ __device__ __forceinline__ int tile_index(int I, int J) { return I * (I + 1) / 2 + J; }
-__host__ __device__ __forceinline__ int tile_offset(int r, int c) { return c * 32 + (r ^ c); }
 
 int schwarz_configure();
 int schwarz_factor_with(mguso_schwarz* s, const uint32_t* c_rp, const uint32_t* c_col, const float* c_val,
@@ -284,59 +278,7 @@ int schwarz_factor_with(mguso_schwarz* s, const uint32_t* c_rp, const uint32_t* 
 // lane carries one accumulator per tile row/column (<= 3), so there are no long serial
 // chains. Acc = double (mixed precision) accumulates in FP64.
 // ---------------------------------------------------------------------------------------
-template <int T, class Acc>
-__device__ __forceinline__ void tiles_apply(const float* __restrict__ w, const float* __restrict__ rd,
-                                            Acc* __restrict__ yd, Acc (&z)[3], int lane) {
-  const float* t00 = w;
-  const float* t10 = w + 1 * TILE_FLOATS;
-  const float* t11 = w + 2 * TILE_FLOATS;
-  const float* t20 = w + 3 * TILE_FLOATS;
-  const float* t21 = w + 4 * TILE_FLOATS;
-  const float* t22 = w + 5 * TILE_FLOATS;
-  Acc y0 = 0, y1 = 0, y2 = 0;
-#pragma unroll 8
-  for (int c = 0; c < 32; ++c) {
-    const int o = tile_offset(lane, c);
-    const Acc a0 = (Acc)rd[c];
-    y0 += (Acc)t00[o] * a0;
-    if (T > 1) {
-      const Acc a1 = (Acc)rd[32 + c];
-      y1 += (Acc)t10[o] * a0 + (Acc)t11[o] * a1;
-      if (T > 2) {
-        const Acc a2 = (Acc)rd[64 + c];
-        y2 += (Acc)t20[o] * a0 + (Acc)t21[o] * a1 + (Acc)t22[o] * a2;
-      }
-    }
-  }
-  yd[lane] = y0;
-  if (T > 1) yd[32 + lane] = y1;
-  if (T > 2) yd[64 + lane] = y2;
-  __syncwarp();
-  Acc z0 = 0, z1 = 0, z2 = 0;
-#pragma unroll 8
-  for (int r = 0; r < 32; ++r) {
-    const int o = tile_offset(r, lane);
-    const Acc b0 = yd[r];
-    z0 += (Acc)t00[o] * b0;
-    if (T > 1) {
-      const Acc b1 = yd[32 + r];
-      z0 += (Acc)t10[o] * b1;
-      z1 += (Acc)t11[o] * b1;
-      if (T > 2) {
-        const Acc b2 = yd[64 + r];
-        z0 += (Acc)t20[o] * b2;
-        z1 += (Acc)t21[o] * b2;
-        z2 += (Acc)t22[o] * b2;
-      }
-    }
-  }
-  z[0] = z0;
-  z[1] = z1;
-  z[2] = z2;
-}
-
 constexpr int APPLY_WARPS = 4;
-constexpr uint32_t APPLY_SLICE = 6 * TILE_FLOATS + 96 + 2 * 96;  // tiles, r, W r (Acc)
 
 template <int WARPS, class Acc>
 __global__ void __launch_bounds__(32 * WARPS) k_schwarz_apply(

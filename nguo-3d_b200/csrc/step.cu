@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <chrono>
 
 #include "elements.cuh"
 #include "reduce.cuh"
@@ -110,6 +111,18 @@ static int linear_solve(Scene& s, mguso_lin_stats* ls) {
   } else {
     MG_TRY(blockjacobi_factor(s.A.get(), s.bjinv.p, st));
   }
+  if (s.p.pcg_mode == 0) {
+    const uint32_t rows[2] = {0, s.nv};
+    PcgInstResult r{};
+    int rc = pcg_persistent(s, rows, 1, &r);
+    if (rc == MGUSO_OK) {
+      ls->iters = r.iters;
+      ls->residual = r.residual;
+      ls->status = (r.residual <= s.p.cg_tol || (r.status & ST_PCG_BREAKDOWN)) ? MGUSO_OK : MGUSO_ERR_PCG_CAP;
+      return MGUSO_OK;
+    }
+    if (rc != MGUSO_ERR_UNSUPPORTED) return rc;
+  }
   PcgOps ops;
   ops.stream = st;
   ops.mixed = s.mixed;
@@ -152,20 +165,33 @@ int scene_step(Scene& s, mguso_step_stats* out) {
   const bool contacts = s.p.self_collision != 0;
   // MGUSO_TRACE=1 prints one line per Newton iteration to stderr (diagnostics only)
   static const bool trace = std::getenv("MGUSO_TRACE") != nullptr;
+  // with MGUSO_TRACE=2 the stream is drained at each phase boundary and the host time of
+  // the phases is printed too (stencils, assembly, linear solve, CCD + advance), in ms
+  static const bool trace_phases = trace && std::getenv("MGUSO_TRACE")[0] == '2';
+  double ph[5] = {0, 0, 0, 0, 0};
+  auto mark = [&]() -> double {
+    if (!trace_phases) return 0.0;
+    cudaStreamSynchronize(st);
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+  };
   for (uint32_t it = 0; it < cap; ++it) {
     ++taken;
     uint32_t nst = 0;
+    ph[0] = mark();
     if (contacts) {
       MG_TRY(build_bvhs(s, s.x.p));
       MG_TRY(collect_stencils(s, &nst));
     }
+    ph[1] = mark();
     stats.stencils = std::max(stats.stencils, nst);
     MG_TRY(assemble_elastic(s));
     MG_TRY(assemble_colliders(s));
     MG_TRY(assemble_contacts(s, nst));
     MG_TRY(finish_rhs(s));
+    ph[2] = mark();
     mguso_lin_stats ls{};
     MG_TRY(linear_solve(s, &ls));
+    ph[3] = mark();
     stats.max_reresid = std::max(stats.max_reresid, ls.residual);
     stats.max_cg_iters = std::max(stats.max_cg_iters, ls.iters);
     // uniform max_dx rescale (implicit.rs:1996-2004); INFINITY leaves dx unchanged
@@ -197,6 +223,11 @@ int scene_step(Scene& s, mguso_step_stats* out) {
     if (trace)
       std::fprintf(stderr, "[mguso] newton %u stencils %u cg %u res %.3e lin_status %d t %.4f max_step %.3e\n", it,
                    nst, ls.iters, ls.residual, ls.status, t, max_step);
+    if (trace_phases) {
+      ph[4] = mark();
+      std::fprintf(stderr, "[mguso]   ms: stencils %.3f assembly %.3f solve %.3f ccd+advance %.3f\n", ph[1] - ph[0],
+                   ph[2] - ph[1], ph[3] - ph[2], ph[4] - ph[3]);
+    }
     if (max_step < 1.0e-7f) break;
     if (s.p.newton_tol > 0.f && max_step < s.p.newton_tol) break;
     if (final_step) break;

@@ -22,7 +22,8 @@ _PARAM_FIELDS = [("dt", C.c_float), ("gravity", C.c_float * 3), ("newton_iters",
                  ("friction", C.c_float), ("friction_eps", C.c_float), ("barrier_kind", C.c_int),
                  ("contact_rayleigh", C.c_int), ("self_collision", C.c_int), ("cg_tol", C.c_float),
                  ("cg_max_iter", C.c_uint32), ("floor_y", C.c_float), ("newton_tol", C.c_float),
-                 ("precond", C.c_int), ("schwarz_domain", C.c_uint32), ("precision", C.c_int)]
+                 ("precond", C.c_int), ("schwarz_domain", C.c_uint32), ("precision", C.c_int),
+                 ("pcg_mode", C.c_int)]
 
 
 class Params(C.Structure):

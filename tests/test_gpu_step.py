@@ -176,3 +176,27 @@ def test_sheath_steps_match_oracle(ctx):
             assert abs(sg["newton_iters"] - so["newton_iters"]) <= 1, (prec, k)
             assert rel < 1e-3, (prec, k, rel)
         assert max(sg["stencils"] for _, sg, _, _ in out) > 100
+
+
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+@pytest.mark.parametrize("precond", [2, 1])
+def test_persistent_pcg_matches_per_kernel_pcg(ctx, precision, precond):
+    """The one-launch persistent PCG and the per-kernel PCG are the same iteration; they
+    differ only in the order of dot-product partial sums, so two drape steps agree to the
+    Newton tolerance and their PCG iteration counts stay close."""
+    sc = coarse_sheath()
+    sc["params"] = dict(sc["params"], precond=precond)
+    runs = []
+    for mode in (0, 1):
+        s2 = dict(sc)
+        s2["params"] = dict(sc["params"], pcg_mode=mode)
+        g = ImplicitSolver(ctx, s2, precision)
+        st = g.step(2)
+        runs.append((g.positions.astype(np.float64), st))
+    (p0, s0), (p1, s1) = runs
+    disp = np.abs(p1 - sc["positions"]).max()
+    assert np.abs(p0 - p1).max() <= 1e-3 * disp
+    for a, b in zip(s0, s1):
+        assert a["status"] == 0 and b["status"] == 0
+        assert abs(a["newton_iters"] - b["newton_iters"]) <= 1
+        assert abs(a["max_cg_iters"] - b["max_cg_iters"]) <= max(5, b["max_cg_iters"] // 10)
