@@ -259,9 +259,21 @@ typedef struct mguso_scene mguso_scene;
 int mguso_scene_create(mguso_ctx* ctx, const mguso_scene_desc* desc, mguso_scene** out);
 int mguso_scene_destroy(mguso_scene* s);
 /* Advances nsteps implicit steps (ImplicitSolver::step, implicit.rs:1951-2191). stats has
- * nsteps entries or is NULL. A non-finite step is rejected exactly as the reference does
+ * nsteps * (instances, 1 for a single scene) entries, step-major, or is NULL. A non-finite step is rejected exactly as the reference does
  * (positions kept, velocities zeroed) and reported as MGUSO_ERR_NONFINITE in its stats. */
 int mguso_step(mguso_scene* s, int nsteps, mguso_step_stats* stats);
+
+/* A batch of independent drapes (for example one pattern graded into sizes) as one scene:
+ * the n <= 8 descriptions are concatenated, so positions and velocities are read and
+ * written as one array with instance k at vertices [offsets[k], offsets[k+1]). Every
+ * instance runs its own Newton loop (its own termination, CCD step fraction and PCG
+ * convergence); the instances still iterating share each launch, and one persistent PCG
+ * launch solves all of them. All descriptions must share params and analytic colliders.
+ * mguso_step then writes nsteps * n stats, step-major. No counterpart in the reference,
+ * which steps one scene at a time. */
+int mguso_batch_create(mguso_ctx* ctx, const mguso_scene_desc* descs, uint32_t n, mguso_scene** out);
+/* Number of instances and their vertex offsets (u32[n + 1]; may be NULL). */
+int mguso_scene_instances(mguso_scene* s, uint32_t* n, uint32_t* vert_offsets);
 int mguso_read_positions(mguso_scene* s, float* out);   /* f32[3*nv] host */
 int mguso_write_positions(mguso_scene* s, const float* in);
 int mguso_read_velocities(mguso_scene* s, float* out);

@@ -663,7 +663,7 @@ int assemble_contacts(Scene& s, uint32_t nst) {
                                                 s.gkeys.p, s.gids.p);
   MG_CUDA(cudaGetLastError());
   // blocks: stable sort by (row, col); stencil order survives within equal keys
-  MG_TRY(radix_sort_pairs(&s.tri_bvh, s.ckeys.p, s.cids.p, mb, 64, st));
+  MG_TRY(radix_sort_pairs(&s.sorter, s.ckeys.p, s.cids.p, mb, 64, st));
   DevBuf<uint32_t>& is_new = s.is_new;
   DevBuf<uint32_t>& rank = s.rank;
   DevBuf<uint32_t>& tmp = s.scan_tmp;
@@ -686,7 +686,7 @@ int assemble_contacts(Scene& s, uint32_t nst) {
                                                   s.c_row.p, s.c_col.p, s.c_val.p);
   k_row_ptr_from_sorted<<<ceil_div(s.nv + 1, 256), 256, 0, st>>>(s.c_row.p, s.c_count.p, s.nv, s.c_row_ptr.p);
   // gradient entries: stable sort by vertex, then add in stencil order
-  MG_TRY(radix_sort_pairs(&s.tri_bvh, s.gkeys.p, s.gids.p, mg_, 64, st));
+  MG_TRY(radix_sort_pairs(&s.sorter, s.gkeys.p, s.gids.p, mg_, 64, st));
   k_contact_grad<<<ceil_div(mg_, 256), 256, 0, st>>>(s.gkeys.p, s.gids.p, mg_, s.cgentries.p, s.grad.p);
   MG_CUDA(cudaGetLastError());
   return MGUSO_OK;

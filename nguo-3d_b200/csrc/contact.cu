@@ -36,9 +36,28 @@ static BvhView view(const Lbvh& b) {
   return BvhView{b.left.p, b.right.p, b.perm.p, (const float4*)b.node.p, (const float4*)b.leaf.p, b.nt};
 }
 
+// One tree per instance over that instance's primitives (a query only meets its own
+// instance); base[k] turns a tree's local primitive index into the scene's.
+struct BvhSet {
+  BvhView t[PCG_MAX_INST];
+  uint32_t base[PCG_MAX_INST];
+};
+
+static BvhSet view_set(const std::vector<std::unique_ptr<Lbvh>>& b, const std::vector<uint32_t>& base) {
+  BvhSet s{};
+  for (size_t k = 0; k < b.size(); ++k) {
+    s.t[k] = view(*b[k]);
+    s.base[k] = base[k];
+  }
+  return s;
+}
+
 template <class F>
-__device__ __forceinline__ bool visit(const BvhView& bv, float4 lo, float4 hi, F&& f) {
-  return lbvh_visit(bv.left, bv.right, bv.node, bv.leaf, bv.prim, bv.n, lo, hi, f);
+__device__ __forceinline__ bool visit(const BvhSet& bs, uint32_t k, float4 lo, float4 hi, F&& f) {
+  const BvhView& bv = bs.t[k];
+  const uint32_t base = bs.base[k];
+  return lbvh_visit(bv.left, bv.right, bv.node, bv.leaf, bv.prim, bv.n, lo, hi,
+                    [&](uint32_t local) { f(base + local); });
 }
 
 __device__ __forceinline__ void point_box(const float* x, uint32_t v, float pad, float4& lo, float4& hi) {
@@ -59,8 +78,12 @@ __device__ __forceinline__ void edge_box(const float* x, uint32_t a, uint32_t b,
 }
 
 int build_bvhs(Scene& s, const float* x) {
-  MG_TRY(lbvh_build(&s.tri_bvh, x, s.nv, s.tris.p, s.nt, 30, s.st));
-  MG_TRY(lbvh_build(&s.edge_bvh, x, s.nv, s.edge_tris.p, s.n_edge, 30, s.st));
+  for (uint32_t k = 0; k < s.ninst; ++k) {
+    const uint32_t t0 = s.inst_tri[k], e0 = s.inst_edge[k];
+    MG_TRY(lbvh_build(s.tri_bvh[k].get(), x, s.nv, s.tris.p + 3 * (size_t)t0, s.inst_tri[k + 1] - t0, 30, s.st));
+    MG_TRY(lbvh_build(s.edge_bvh[k].get(), x, s.nv, s.edge_tris.p + 3 * (size_t)e0, s.inst_edge[k + 1] - e0, 30,
+                      s.st));
+  }
   return MGUSO_OK;
 }
 
@@ -68,7 +91,7 @@ int build_bvhs(Scene& s, const float* x) {
 // best (d2 bits, triangle) per non-static vertex over collider triangles within dhat; ties
 // go to the lowest triangle index, which is the first one the reference's triangle-major
 // visit reaches.
-__global__ void k_side_best(BvhView bv, const float* __restrict__ x, const uint32_t* __restrict__ tris,
+__global__ void k_side_best(BvhSet bv, const uint8_t* __restrict__ vinst, const float* __restrict__ x, const uint32_t* __restrict__ tris,
                             const uint8_t* __restrict__ ctri, const uint8_t* __restrict__ svert,
                             const float* __restrict__ im, const uint32_t* __restrict__ ex_ptr,
                             const uint32_t* __restrict__ ex_list, uint32_t nv, float dhat,
@@ -80,7 +103,7 @@ __global__ void k_side_best(BvhView bv, const float* __restrict__ x, const uint3
     float4 lo, hi;
     point_box(x, v, dhat, lo, hi);
     V3<float> p = ld3<float>(x, v);
-    bool ok = visit(bv, lo, hi, [&](uint32_t t) {
+    bool ok = visit(bv, vinst[v], lo, hi, [&](uint32_t t) {
       if (!ctri[t]) return;
       uint32_t a = tris[3 * t], bb = tris[3 * t + 1], c = tris[3 * t + 2];
       if (excluded(ex_ptr, ex_list, v, a, bb, c)) return;
@@ -153,7 +176,7 @@ __device__ __forceinline__ R ee_distance(const float* x, const uint32_t idx[4], 
   return d;
 }
 
-__global__ void k_vt_stencils(BvhView bv, const float* __restrict__ x, const uint32_t* __restrict__ tris,
+__global__ void k_vt_stencils(BvhSet bv, const uint8_t* __restrict__ vinst, const float* __restrict__ x, const uint32_t* __restrict__ tris,
                               const uint8_t* __restrict__ ctri, const float* __restrict__ im,
                               const uint32_t* __restrict__ ex_ptr, const uint32_t* __restrict__ ex_list,
                               const unsigned long long* __restrict__ best, const float* __restrict__ pn, int has_static,
@@ -165,7 +188,7 @@ __global__ void k_vt_stencils(BvhView bv, const float* __restrict__ x, const uin
   point_box(x, v, dhat, lo, hi);
   bool vmov = im[v] > 0.f;
   float side = 2.f;  // computed lazily
-  bool ok = visit(bv, lo, hi, [&](uint32_t t) {
+  bool ok = visit(bv, vinst[v], lo, hi, [&](uint32_t t) {
     uint32_t a = tris[3 * t], b = tris[3 * t + 1], c = tris[3 * t + 2];
     bool tmov = im[a] > 0.f || im[b] > 0.f || im[c] > 0.f;
     if (!tmov && !vmov) return;
@@ -186,7 +209,8 @@ __global__ void k_vt_stencils(BvhView bv, const float* __restrict__ x, const uin
   if (!ok) atomicOr(status, ST_STACK_OVERFLOW);
 }
 
-__global__ void k_ee_stencils(BvhView bv, const float* __restrict__ x, const uint32_t* __restrict__ edges,
+__global__ void k_ee_stencils(BvhSet bv, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
+                              const uint32_t* __restrict__ edges,
                               const float* __restrict__ im, uint32_t ne, float search, float dhat, int mixed,
                               Stencil* out, unsigned long long* keys, uint32_t* ids, unsigned long long* counter,
                               uint32_t cap, uint32_t* status) {
@@ -196,7 +220,7 @@ __global__ void k_ee_stencils(BvhView bv, const float* __restrict__ x, const uin
   float4 lo, hi;
   edge_box(x, b0, b1, search, lo, hi);
   bool jmov = im[b0] > 0.f || im[b1] > 0.f;
-  bool ok = visit(bv, lo, hi, [&](uint32_t i) {
+  bool ok = visit(bv, vinst[b0], lo, hi, [&](uint32_t i) {
     if (i >= j) return;
     uint32_t a0 = edges[2 * i], a1 = edges[2 * i + 1];
     if (!(jmov || im[a0] > 0.f || im[a1] > 0.f)) return;
@@ -224,9 +248,9 @@ __global__ void k_permute_stencils(const Stencil* __restrict__ in, const uint32_
 int collect_stencils(Scene& s, uint32_t* nst_out) {
   cudaStream_t st = s.st;
   const float dhat = s.p.contact_dhat;
-  BvhView tv = view(s.tri_bvh), ev = view(s.edge_bvh);
+  const BvhSet tv = view_set(s.tri_bvh, s.inst_tri), ev = view_set(s.edge_bvh, s.inst_edge);
   if (s.has_static) {
-    k_side_best<<<ceil_div(s.nv, 128), 128, 0, st>>>(tv, s.x.p, s.tris.p, s.collider_tri.p, s.static_vert.p,
+    k_side_best<<<ceil_div(s.nv, 128), 128, 0, st>>>(tv, s.vinst.p, s.x.p, s.tris.p, s.collider_tri.p, s.static_vert.p,
                                                    s.inv_mass.p, s.ex_ptr.p, s.ex_list.p, s.nv, dhat, s.side_best.p,
                                                    s.status.p);
   }
@@ -236,13 +260,13 @@ int collect_stencils(Scene& s, uint32_t* nst_out) {
     MG_TRY(s.st_keys.reserve(s.cap_stencils));
     MG_TRY(s.st_ids.reserve(s.cap_stencils));
     MG_CUDA(cudaMemsetAsync(s.counters.p, 0, 8 * 8, st));
-    k_vt_stencils<<<ceil_div(s.nv, 128), 128, 0, st>>>(tv, s.x.p, s.tris.p, s.collider_tri.p, s.inv_mass.p,
+    k_vt_stencils<<<ceil_div(s.nv, 128), 128, 0, st>>>(tv, s.vinst.p, s.x.p, s.tris.p, s.collider_tri.p, s.inv_mass.p,
                                                      s.ex_ptr.p, s.ex_list.p, s.side_best.p, s.collider_pn.p,
                                                      s.has_static ? 1 : 0, s.nv, dhat, s.mixed ? 1 : 0, s.stencils.p,
                                                      s.st_keys.p, s.st_ids.p, s.counters.p, s.cap_stencils,
                                                      s.status.p);
     if (s.n_edge)
-      k_ee_stencils<<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, s.x.p, s.edges.p, s.inv_mass.p, s.n_edge, dhat, dhat,
+      k_ee_stencils<<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, s.vinst.p, s.x.p, s.edges.p, s.inv_mass.p, s.n_edge, dhat, dhat,
                                                            s.mixed ? 1 : 0, s.stencils.p, s.st_keys.p, s.st_ids.p,
                                                            s.counters.p, s.cap_stencils, s.status.p);
     MG_CUDA(cudaGetLastError());
@@ -251,7 +275,7 @@ int collect_stencils(Scene& s, uint32_t* nst_out) {
     MG_CUDA(cudaStreamSynchronize(st));
     if (cnt <= s.cap_stencils) {
       uint32_t n = (uint32_t)cnt;
-      if (n > 1) MG_TRY(radix_sort_pairs(&s.tri_bvh, s.st_keys.p, s.st_ids.p, n, 64, st));
+      if (n > 1) MG_TRY(radix_sort_pairs(&s.sorter, s.st_keys.p, s.st_ids.p, n, 64, st));
       if (n) k_permute_stencils<<<ceil_div(n, 128), 128, 0, st>>>(s.stencils.p, s.st_ids.p, n, s.stencils_sorted.p);
       MG_CUDA(cudaGetLastError());
       *nst_out = n;
@@ -269,20 +293,19 @@ __device__ __forceinline__ void atomic_min_pos(unsigned int* addr, float v) {
   atomicMin(addr, __float_as_uint(fmaxf(v, 0.f)));
 }
 
-__global__ void k_max_norm(const float* __restrict__ dx, uint32_t nv, unsigned int* __restrict__ out) {
-  float m = 0.f;
+// per-instance maximum of |dx_v| into out[RED_STRIDE * instance]
+__global__ void k_max_norm(const float* __restrict__ dx, const uint8_t* __restrict__ vinst, uint32_t nv,
+                           unsigned int* __restrict__ out) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x) {
-    V3<float> d = ld3<float>(dx, i);
-    m = fmaxf(m, d.length());
+    const float m = ld3<float>(dx, i).length();
+    if (m > 0.f) atomicMax(out + RED_STRIDE * vinst[i], __float_as_uint(m));
   }
-  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
 }
 
 // analytic colliders: keep >= 20% of the current gap (implicit.rs:1795-1818)
-__global__ void k_ccd_colliders(const uint32_t* __restrict__ free_verts, uint32_t n_free, const float* __restrict__ x,
-                                const float* __restrict__ dx, const float* __restrict__ cols, uint32_t ncol,
-                                unsigned int* __restrict__ tmin) {
+__global__ void k_ccd_colliders(const uint32_t* __restrict__ free_verts, uint32_t n_free, const uint8_t* __restrict__ vinst,
+                                const float* __restrict__ x, const float* __restrict__ dx, const float* __restrict__ cols,
+                                uint32_t ncol, unsigned int* __restrict__ red) {
   uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= n_free) return;
   uint32_t i = free_verts[f];
@@ -316,26 +339,35 @@ __global__ void k_ccd_colliders(const uint32_t* __restrict__ free_verts, uint32_
       if (l > 1e-12f) t = fminf(t, (1.0f - GAP) * d0 / l);
     }
   }
-  if (t < 1.f) atomic_min_pos(tmin, t);
+  if (t < 1.f) atomic_min_pos(red + RED_STRIDE * vinst[i] + 1, t);
 }
 
+// Per-instance CCD pass parameters: search radius and whether the instance still needs a
+// pass (an instance whose step fraction was settled by an earlier pass is skipped).
+struct CcdPass {
+  float search[PCG_MAX_INST];
+  uint32_t todo;  // bit k: instance k
+};
+
 template <class R>
-__global__ void k_ccd_vt(BvhView bv, const float* __restrict__ x, const float* __restrict__ dx,
-                         const uint32_t* __restrict__ tris, const uint8_t* __restrict__ ctri,
-                         const float* __restrict__ im, const uint32_t* __restrict__ ex_ptr,
-                         const uint32_t* __restrict__ ex_list, const unsigned long long* __restrict__ best,
-                         const float* __restrict__ pn, int has_static, uint32_t nv, float search, float dhat,
-                         uint32_t max_iter, unsigned int* __restrict__ tmin, unsigned int* __restrict__ caps,
+__global__ void k_ccd_vt(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
+                         const float* __restrict__ dx, const uint32_t* __restrict__ tris,
+                         const uint8_t* __restrict__ ctri, const float* __restrict__ im,
+                         const uint32_t* __restrict__ ex_ptr, const uint32_t* __restrict__ ex_list,
+                         const unsigned long long* __restrict__ best, const float* __restrict__ pn, int has_static,
+                         uint32_t nv, float dhat, uint32_t max_iter, unsigned int* __restrict__ red,
                          uint32_t* __restrict__ status) {
   uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= nv) return;
+  const uint32_t k = vinst[v];
+  if (!((cp.todo >> k) & 1u)) return;
   float4 lo, hi;
-  point_box(x, v, search, lo, hi);
+  point_box(x, v, cp.search[k], lo, hi);
   bool vmov = im[v] > 0.f;
   float side = 2.f;
   float tloc = 1.f;
   uint32_t ncap = 0;
-  bool ok = visit(bv, lo, hi, [&](uint32_t t) {
+  bool ok = visit(bv, k, lo, hi, [&](uint32_t t) {
     uint32_t a = tris[3 * t], b = tris[3 * t + 1], c = tris[3 * t + 2];
     bool tmov = im[a] > 0.f || im[b] > 0.f || im[c] > 0.f;
     if (!tmov && !vmov) return;
@@ -346,9 +378,9 @@ __global__ void k_ccd_vt(BvhView bv, const float* __restrict__ x, const float* _
     }
     uint32_t idx[4] = {v, a, b, c};
     V3<R> x0[4], dd[4];
-    for (int k = 0; k < 4; ++k) {
-      x0[k] = ld3<R>(x, idx[k]);
-      dd[k] = ld3<R>(dx, idx[k]);
+    for (int q = 0; q < 4; ++q) {
+      x0[q] = ld3<R>(x, idx[q]);
+      dd[q] = ld3<R>(dx, idx[q]);
     }
     bool cap = false;
     R toi = accd_toi<R>(x0, dd, R(0), R(1.25), R(0.01), max_iter, 0, &cap);
@@ -356,33 +388,34 @@ __global__ void k_ccd_vt(BvhView bv, const float* __restrict__ x, const float* _
     tloc = fminf(tloc, (float)(toi / R(1.25)));
   });
   if (!ok) atomicOr(status, ST_STACK_OVERFLOW);
-  if (tloc < 1.f) atomic_min_pos(tmin, tloc);
-  if (ncap) atomicAdd(caps, ncap);
+  if (tloc < 1.f) atomic_min_pos(red + RED_STRIDE * k + 2, tloc);
+  if (ncap) atomicAdd(red + RED_STRIDE * k + 3, ncap);
 }
 
 template <class R>
-__global__ void k_ccd_ee(BvhView bv, const float* __restrict__ x, const float* __restrict__ dx,
-                         const uint32_t* __restrict__ edges, const float* __restrict__ im, uint32_t ne, float search,
-                         uint32_t max_iter, unsigned int* __restrict__ tmin, unsigned int* __restrict__ caps,
-                         uint32_t* __restrict__ status) {
+__global__ void k_ccd_ee(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
+                         const float* __restrict__ dx, const uint32_t* __restrict__ edges, const float* __restrict__ im,
+                         uint32_t ne, uint32_t max_iter, unsigned int* __restrict__ red, uint32_t* __restrict__ status) {
   uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ne) return;
   uint32_t b0 = edges[2 * j], b1 = edges[2 * j + 1];
+  const uint32_t k = vinst[b0];
+  if (!((cp.todo >> k) & 1u)) return;
   float4 lo, hi;
-  edge_box(x, b0, b1, search, lo, hi);
+  edge_box(x, b0, b1, cp.search[k], lo, hi);
   bool jmov = im[b0] > 0.f || im[b1] > 0.f;
   float tloc = 1.f;
   uint32_t ncap = 0;
-  bool ok = visit(bv, lo, hi, [&](uint32_t i) {
+  bool ok = visit(bv, k, lo, hi, [&](uint32_t i) {
     if (i >= j) return;
     uint32_t a0 = edges[2 * i], a1 = edges[2 * i + 1];
     if (!(jmov || im[a0] > 0.f || im[a1] > 0.f)) return;
     if (a0 == b0 || a0 == b1 || a1 == b0 || a1 == b1) return;
     uint32_t idx[4] = {a0, a1, b0, b1};
     V3<R> x0[4], dd[4];
-    for (int k = 0; k < 4; ++k) {
-      x0[k] = ld3<R>(x, idx[k]);
-      dd[k] = ld3<R>(dx, idx[k]);
+    for (int q = 0; q < 4; ++q) {
+      x0[q] = ld3<R>(x, idx[q]);
+      dd[q] = ld3<R>(dx, idx[q]);
     }
     bool cap = false;
     R toi = accd_toi<R>(x0, dd, R(0), R(1.25), R(0.01), max_iter, 1, &cap);
@@ -390,73 +423,90 @@ __global__ void k_ccd_ee(BvhView bv, const float* __restrict__ x, const float* _
     tloc = fminf(tloc, (float)(toi / R(1.25)));
   });
   if (!ok) atomicOr(status, ST_STACK_OVERFLOW);
-  if (tloc < 1.f) atomic_min_pos(tmin, tloc);
-  if (ncap) atomicAdd(caps, ncap);
+  if (tloc < 1.f) atomic_min_pos(red + RED_STRIDE * k + 2, tloc);
+  if (ncap) atomicAdd(red + RED_STRIDE * k + 3, ncap);
 }
 
-// ccd_max_step (implicit.rs:1690-1947) without strain limiting or pins. The search
-// direction is s.dx; red[0] = max |dx|, red[1] = collider t, red[2] = self t, red[3] = caps.
-int ccd_step(Scene& s, float* t_out, uint32_t* cap_hits) {
+// ccd_max_step (implicit.rs:1690-1947) without strain limiting or pins, per instance. The
+// search direction is s.dx; per instance k, red[RED_STRIDE k + 0] = max |dx|, + 1 collider t,
+// + 2 self t, + 3 caps. Instances outside `active` get t = 1 and no work. Each instance runs
+// the reference's widening-radius schedule on its own displacement and edge length; a pass
+// covers every instance that still needs one.
+int ccd_step(Scene& s, uint32_t active, float* t_out, uint32_t* cap_hits) {
   cudaStream_t st = s.st;
-  if (s.n_col == 0 && !s.p.self_collision) {
-    *t_out = 1.f;
-    return MGUSO_OK;
+  const uint32_t K = s.ninst;
+  for (uint32_t k = 0; k < K; ++k) {
+    t_out[k] = 1.f;
+    cap_hits[k] = 0;
   }
-  unsigned int init[4] = {0u, f2u_host(1.f), 0u, 0u};
-  MG_CUDA(cudaMemcpyAsync(s.red.p, init, sizeof(init), cudaMemcpyHostToDevice, st));
+  if (s.n_col == 0 && !s.p.self_collision) return MGUSO_OK;
+  std::vector<unsigned int> init(RED_STRIDE * K, 0u);
+  for (uint32_t k = 0; k < K; ++k) {
+    init[RED_STRIDE * k + 1] = f2u_host(1.f);
+    init[RED_STRIDE * k + 2] = f2u_host(1.f);
+  }
+  MG_CUDA(cudaMemcpyAsync(s.red.p, init.data(), 4 * init.size(), cudaMemcpyHostToDevice, st));
   int sms = s.ctx->sm_count;
-  k_max_norm<<<std::min<uint32_t>(ceil_div(s.nv, 256), sms * 4), 256, 0, st>>>(s.dx.p, s.nv, s.red.p);
+  k_max_norm<<<std::min<uint32_t>(ceil_div(s.nv, 256), sms * 4), 256, 0, st>>>(s.dx.p, s.vinst.p, s.nv, s.red.p);
   if (s.n_col && s.n_free)
-    k_ccd_colliders<<<ceil_div(s.n_free, 128), 128, 0, st>>>(s.free_verts.p, s.n_free, s.x.p, s.dx.p, s.colliders.p,
-                                                           s.n_col, s.red.p + 1);
+    k_ccd_colliders<<<ceil_div(s.n_free, 128), 128, 0, st>>>(s.free_verts.p, s.n_free, s.vinst.p, s.x.p, s.dx.p,
+                                                           s.colliders.p, s.n_col, s.red.p);
   MG_CUDA(cudaGetLastError());
-  unsigned int h[4];
-  MG_CUDA(cudaMemcpyAsync(h, s.red.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+  std::vector<unsigned int> h(RED_STRIDE * K);
+  MG_CUDA(cudaMemcpyAsync(h.data(), s.red.p, 4 * h.size(), cudaMemcpyDeviceToHost, st));
   MG_CUDA(cudaStreamSynchronize(st));
-  float max_disp = u2f_host(h[0]);
-  float t = u2f_host(h[1]);
+  float max_disp[PCG_MAX_INST], allowed[PCG_MAX_INST];
+  for (uint32_t k = 0; k < K; ++k) {
+    max_disp[k] = u2f_host(h[RED_STRIDE * k]);
+    if ((active >> k) & 1u) t_out[k] = u2f_host(h[RED_STRIDE * k + 1]);
+  }
   if (s.p.self_collision) {
     const float dhat = s.p.contact_dhat;
     const float fixed = dhat;  // max_edge_gap() + 2 * max_edge_offset() for face edges
-    float allowed = std::max(std::min(0.5f * s.char_len, max_disp), 1.0e-9f);
+    uint32_t todo = active;
+    for (uint32_t k = 0; k < K; ++k) allowed[k] = std::max(std::min(0.5f * s.char_len[k], max_disp[k]), 1.0e-9f);
     uint32_t iters = std::max<uint32_t>(s.p.ccd_max_iter, 1);
-    BvhView tv = view(s.tri_bvh), ev = view(s.edge_bvh);
-    for (int pass = 0; pass < 64; ++pass) {
-      bool full = allowed >= max_disp;
-      float search = fixed + 2.0f * allowed;
-      unsigned int one = f2u_host(1.f);
-      MG_CUDA(cudaMemcpyAsync(s.red.p + 2, &one, 4, cudaMemcpyHostToDevice, st));
+    const BvhSet tv = view_set(s.tri_bvh, s.inst_tri), ev = view_set(s.edge_bvh, s.inst_edge);
+    for (int pass = 0; pass < 64 && todo; ++pass) {
+      CcdPass cp{};
+      cp.todo = todo;
+      for (uint32_t k = 0; k < K; ++k) {
+        cp.search[k] = fixed + 2.0f * allowed[k];
+        MG_CUDA(cudaMemcpyAsync(s.red.p + RED_STRIDE * k + 2, &init[RED_STRIDE * k + 2], 8, cudaMemcpyHostToDevice, st));
+      }
       if (s.mixed) {
         k_ccd_vt<double><<<ceil_div(s.nv, 128), 128, 0, st>>>(
-            tv, s.x.p, s.dx.p, s.tris.p, s.collider_tri.p, s.inv_mass.p, s.ex_ptr.p, s.ex_list.p, s.side_best.p,
-            s.collider_pn.p, s.has_static ? 1 : 0, s.nv, search, dhat, iters, s.red.p + 2, s.red.p + 3, s.status.p);
+            tv, cp, s.vinst.p, s.x.p, s.dx.p, s.tris.p, s.collider_tri.p, s.inv_mass.p, s.ex_ptr.p, s.ex_list.p,
+            s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.red.p, s.status.p);
         if (s.n_edge)
-          k_ccd_ee<double><<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, s.x.p, s.dx.p, s.edges.p, s.inv_mass.p,
-                                                                   s.n_edge, search, iters, s.red.p + 2, s.red.p + 3,
-                                                                   s.status.p);
+          k_ccd_ee<double><<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, cp, s.vinst.p, s.x.p, s.dx.p, s.edges.p,
+                                                                   s.inv_mass.p, s.n_edge, iters, s.red.p, s.status.p);
       } else {
         k_ccd_vt<float><<<ceil_div(s.nv, 128), 128, 0, st>>>(
-            tv, s.x.p, s.dx.p, s.tris.p, s.collider_tri.p, s.inv_mass.p, s.ex_ptr.p, s.ex_list.p, s.side_best.p,
-            s.collider_pn.p, s.has_static ? 1 : 0, s.nv, search, dhat, iters, s.red.p + 2, s.red.p + 3, s.status.p);
+            tv, cp, s.vinst.p, s.x.p, s.dx.p, s.tris.p, s.collider_tri.p, s.inv_mass.p, s.ex_ptr.p, s.ex_list.p,
+            s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.red.p, s.status.p);
         if (s.n_edge)
-          k_ccd_ee<float><<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, s.x.p, s.dx.p, s.edges.p, s.inv_mass.p,
-                                                                  s.n_edge, search, iters, s.red.p + 2, s.red.p + 3,
-                                                                  s.status.p);
+          k_ccd_ee<float><<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, cp, s.vinst.p, s.x.p, s.dx.p, s.edges.p,
+                                                                  s.inv_mass.p, s.n_edge, iters, s.red.p, s.status.p);
       }
       MG_CUDA(cudaGetLastError());
-      unsigned int hs[2];
-      MG_CUDA(cudaMemcpyAsync(hs, s.red.p + 2, 8, cudaMemcpyDeviceToHost, st));
+      MG_CUDA(cudaMemcpyAsync(h.data(), s.red.p, 4 * h.size(), cudaMemcpyDeviceToHost, st));
       MG_CUDA(cudaStreamSynchronize(st));
-      float t_self = u2f_host(hs[0]);
-      *cap_hits = hs[1];
-      if (full || t_self * max_disp <= allowed) {
-        t = std::min(t, t_self);
-        break;
+      for (uint32_t k = 0; k < K; ++k) {
+        if (!((todo >> k) & 1u)) continue;
+        const bool full = allowed[k] >= max_disp[k];
+        const float t_self = u2f_host(h[RED_STRIDE * k + 2]);
+        cap_hits[k] = h[RED_STRIDE * k + 3];
+        if (full || t_self * max_disp[k] <= allowed[k]) {
+          t_out[k] = std::min(t_out[k], t_self);
+          todo &= ~(1u << k);
+        } else {
+          allowed[k] = std::min(allowed[k] * 4.0f, max_disp[k]);
+        }
       }
-      allowed = std::min(allowed * 4.0f, max_disp);
     }
   }
-  *t_out = std::min(std::max(t, 0.f), 1.f);
+  for (uint32_t k = 0; k < K; ++k) t_out[k] = std::min(std::max(t_out[k], 0.f), 1.f);
   return MGUSO_OK;
 }
 

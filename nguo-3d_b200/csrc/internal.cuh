@@ -71,6 +71,7 @@ struct mguso_schwarz {
   uint32_t domain = 32;
   uint32_t ndom = 0;
   uint32_t max_m = 0;
+  std::vector<uint32_t> inst_vert;  // optional instance vertex ranges (domains stay inside one)
   std::vector<uint32_t> h_dom_start, h_dom_verts, h_dom_of;
   mg::DevBuf<uint32_t> dom_start;  // ndom + 1 (vertex offsets)
   mg::DevBuf<uint32_t> dom_verts;  // nb

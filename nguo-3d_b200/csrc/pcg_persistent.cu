@@ -52,6 +52,7 @@ struct PersistentArgs {
   float *x, *r, *z, *p, *p2, *ap;
   float tol;
   uint32_t max_iter;
+  uint32_t active;  // bit k: instance k is solved; the others keep x = 0
   PcgInstResult* out;
   void* partials;     // gridDim.x * PCG_MAX_INST accumulators
   uint32_t* bar;      // [0] arrivals, [1] generation, [2] error bits
@@ -160,7 +161,7 @@ __global__ void __launch_bounds__(PP_THREADS, 1) k_pcg_persistent(PersistentArgs
   uint32_t target = 0;
   if (tid < K) {
     s_iters[tid] = 0;
-    s_done[tid] = 0;
+    s_done[tid] = ((a.active >> tid) & 1u) ? 0u : 1u;
     s_status[tid] = 0;
     s_beta[tid] = 0.0;
     s_alpha[tid] = 0.0;
@@ -419,7 +420,7 @@ int pcg_persistent_configure(Scene& s, int* grid_out) {
 // h_inst_row (host, ninst + 1 block-row offsets) splits the rows into instances; results go
 // to out[0 .. ninst). Returns MGUSO_ERR_UNSUPPORTED when the kernel cannot be resident on
 // every SM or a Schwarz domain spans two instances (the caller then uses the per-kernel PCG).
-int pcg_persistent(Scene& s, const uint32_t* h_inst_row, uint32_t ninst, PcgInstResult* out) {
+int pcg_persistent(Scene& s, const uint32_t* h_inst_row, uint32_t ninst, uint32_t active, PcgInstResult* out) {
   MG_CHECK_ARG(ninst >= 1 && ninst <= PCG_MAX_INST, "persistent PCG: 1..8 instances");
   if (s.pp_grid < 0) MG_TRY(pcg_persistent_configure(s, &s.pp_grid));
   if (s.pp_grid == 0 || (int)ninst > s.pp_grid) return MGUSO_ERR_UNSUPPORTED;
@@ -493,6 +494,7 @@ int pcg_persistent(Scene& s, const uint32_t* h_inst_row, uint32_t ninst, PcgInst
   a.p2 = w.p2.p;
   a.ap = w.ap.p;
   a.tol = s.p.cg_tol;
+  a.active = active;
   a.max_iter = s.p.cg_max_iter;
   a.out = s.pp_out.p;
   // two alternating buffers x grid x (r.r, r.z)

@@ -42,7 +42,7 @@ struct Contribution {
 
 }  // namespace
 
-int scene_build(Scene& s, const mguso_scene_desc* d) {
+int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>& inst_vert) {
   MG_CHECK_ARG(d && d->positions && d->inv_mass && (d->nt == 0 || d->tris), "scene: null arrays");
   MG_CHECK_ARG(d->nv > 0 && d->nv < (1u << 30), "scene: vertex count out of range");
   const uint32_t nv = d->nv, nt = d->nt;
@@ -69,6 +69,37 @@ int scene_build(Scene& s, const mguso_scene_desc* d) {
   s.st = s.ctx->stream;
   cudaStream_t st = s.st;
   const float* P = d->positions;
+  MG_CHECK_ARG(inst_vert.size() >= 2 && inst_vert.size() <= PCG_MAX_INST + 1 && inst_vert.front() == 0 &&
+                   inst_vert.back() == nv,
+               "scene: instance vertex ranges");
+  s.ninst = (uint32_t)inst_vert.size() - 1;
+  s.inst_vert = inst_vert;
+  std::vector<uint8_t> vinst(nv);
+  for (uint32_t k = 0; k < s.ninst; ++k) {
+    MG_CHECK_ARG(inst_vert[k] < inst_vert[k + 1], "scene: empty instance");
+    for (uint32_t v = inst_vert[k]; v < inst_vert[k + 1]; ++v) vinst[v] = (uint8_t)k;
+  }
+  MG_TRY(s.vinst.upload(vinst.data(), nv, st));
+  // every triangle, stitch and shell face lies in one instance, triangles in instance order
+  s.inst_tri.assign(s.ninst + 1, nt);
+  s.inst_tri[0] = 0;
+  {
+    uint32_t k = 0;
+    for (uint32_t t = 0; t < nt; ++t) {
+      const uint32_t a = vinst[d->tris[3 * t]];
+      MG_CHECK_ARG(a == vinst[d->tris[3 * t + 1]] && a == vinst[d->tris[3 * t + 2]] && a >= k,
+                   "scene: triangles must be grouped by instance");
+      while (k < a) s.inst_tri[++k] = t;
+    }
+    while (k < s.ninst) s.inst_tri[++k] = nt;
+  }
+  for (uint32_t f = 0; f < d->nshell; ++f)
+    MG_CHECK_ARG(vinst[d->shell_faces[3 * f]] == vinst[d->shell_faces[3 * f + 1]] &&
+                     vinst[d->shell_faces[3 * f]] == vinst[d->shell_faces[3 * f + 2]],
+                 "scene: a shell face spans two instances");
+  for (uint32_t i = 0; i < d->nstitch; ++i)
+    for (int k = 1; k < 6; ++k)
+      MG_CHECK_ARG(vinst[d->stitch_idx[6 * i + k]] == vinst[d->stitch_idx[6 * i]], "scene: a stitch spans two instances");
 
   // ---- state -------------------------------------------------------------------------
   s.h_inv_mass.assign(d->inv_mass, d->inv_mass + nv);
@@ -109,13 +140,23 @@ int scene_build(Scene& s, const mguso_scene_desc* d) {
   std::sort(edges.begin(), edges.end());
   edges.erase(std::unique(edges.begin(), edges.end()), edges.end());
   s.n_edge = (uint32_t)edges.size();
-  // characteristic length: mean unique-edge length, summed in order (implicit.rs:533-542)
-  if (edges.empty()) {
-    s.char_len = 1.f;
-  } else {
+  // sorted (min, max) edges are grouped by instance
+  s.inst_edge.assign(s.ninst + 1, s.n_edge);
+  s.inst_edge[0] = 0;
+  {
+    uint32_t k = 0;
+    for (uint32_t e = 0; e < s.n_edge; ++e)
+      while (k < vinst[edges[e][0]]) s.inst_edge[++k] = e;
+  }
+  // characteristic length per instance: mean unique-edge length, summed in order
+  // (implicit.rs:533-542)
+  s.char_len.assign(s.ninst, 1.f);
+  for (uint32_t k = 0; k < s.ninst; ++k) {
+    if (s.inst_edge[k + 1] == s.inst_edge[k]) continue;
     float sum = 0.f;
-    for (auto& e : edges) sum += (hp(P, e[0]) - hp(P, e[1])).length();
-    s.char_len = std::max(sum / (float)edges.size(), 1e-6f);
+    for (uint32_t e = s.inst_edge[k]; e < s.inst_edge[k + 1]; ++e)
+      sum += (hp(P, edges[e][0]) - hp(P, edges[e][1])).length();
+    s.char_len[k] = std::max(sum / (float)(s.inst_edge[k + 1] - s.inst_edge[k]), 1e-6f);
   }
   // hinges (bending.rs:126-158): sorted edge key -> opposite vertices in triangle order
   std::map<std::pair<uint32_t, uint32_t>, std::vector<uint32_t>> em;
@@ -419,7 +460,8 @@ int scene_build(Scene& s, const mguso_scene_desc* d) {
         auto bits = [](float c) { if (c == 0.f) c = 0.f; uint32_t b; std::memcpy(&b, &c, 4); return (uint64_t)b; };
         std::map<std::array<uint64_t, 3>, uint32_t> wmap;
         for (uint32_t i = 0; i < nv; ++i) {
-          std::array<uint64_t, 3> kk = {bits(P[3 * i]), bits(P[3 * i + 1]), bits(P[3 * i + 2])};
+          std::array<uint64_t, 3> kk = {bits(P[3 * i]) | ((uint64_t)vinst[i] << 32), bits(P[3 * i + 1]),
+                                        bits(P[3 * i + 2])};
           auto it = wmap.find(kk);
           if (it == wmap.end()) {
             uint32_t id = (uint32_t)wmap.size();
@@ -454,8 +496,13 @@ int scene_build(Scene& s, const mguso_scene_desc* d) {
   MG_TRY(up(s.static_vert, svert));
   MG_TRY(up(s.collider_tri, ctri));
   MG_TRY(up(s.collider_pn, pn));
-  s.tri_bvh.ctx = s.ctx;
-  s.edge_bvh.ctx = s.ctx;
+  s.sorter.ctx = s.ctx;
+  for (uint32_t k = 0; k < s.ninst; ++k) {
+    s.tri_bvh.push_back(std::make_unique<Lbvh>());
+    s.edge_bvh.push_back(std::make_unique<Lbvh>());
+    s.tri_bvh.back()->ctx = s.ctx;
+    s.edge_bvh.back()->ctx = s.ctx;
+  }
 
   // ---- working set -------------------------------------------------------------------------
   s.cap_pairs = std::max<uint32_t>(1u << 16, 8 * nv);
@@ -463,7 +510,7 @@ int scene_build(Scene& s, const mguso_scene_desc* d) {
   MG_TRY(s.pairs.reserve(2 * (size_t)s.cap_pairs));
   MG_TRY(s.counters.reserve(8));
   MG_TRY(s.side_best.reserve(nv));
-  MG_TRY(s.red.reserve(16));
+  MG_TRY(s.red.reserve(RED_STRIDE * s.ninst));
   MG_TRY(s.status.reserve(4));
   MG_CUDA(cudaMemsetAsync(s.status.p, 0, 16, st));
   s.cap_c = std::max<uint32_t>(1u << 14, 4 * nv);
@@ -477,6 +524,7 @@ int scene_build(Scene& s, const mguso_scene_desc* d) {
     s.schwarz = std::make_unique<mguso_schwarz>();
     s.schwarz->a = s.A.get();
     s.schwarz->domain = s.p.schwarz_domain;
+    s.schwarz->inst_vert = s.inst_vert;
     MG_TRY(schwarz_build(s.schwarz.get()));
   } else {
     MG_TRY(s.bjinv.reserve(9 * (size_t)nv));
@@ -497,7 +545,7 @@ int mguso_scene_create(mguso_ctx* ctx, const mguso_scene_desc* desc, mguso_scene
   MG_CUDA(cudaSetDevice(ctx->device));
   auto sc = std::make_unique<mguso_scene>();
   sc->s.ctx = ctx;
-  MG_TRY(scene_build(sc->s, desc));
+  MG_TRY(scene_build(sc->s, desc, {0, desc->nv}));
   *out = sc.release();
   return MGUSO_OK;
 }
@@ -508,13 +556,105 @@ int mguso_scene_destroy(mguso_scene* s) {
   return MGUSO_OK;
 }
 
+// Several independent drapes as one scene: the descriptions are concatenated (vertex,
+// triangle, shell-face and stitch indices offset), every instance keeps its own Newton
+// loop, and the launches of a step are shared. All instances share one mguso_params and one
+// set of analytic colliders.
+int mguso_batch_create(mguso_ctx* ctx, const mguso_scene_desc* descs, uint32_t n, mguso_scene** out) {
+  MG_CHECK_ARG(ctx && descs && out && n >= 1, "null argument");
+  MG_CHECK_ARG(n <= PCG_MAX_INST, "batch: at most 8 instances");
+  const mguso_scene_desc& d0 = descs[0];
+  uint64_t nv = 0, nt = 0, nsh = 0, nst = 0;
+  bool any_mask = false;
+  for (uint32_t k = 0; k < n; ++k) {
+    const mguso_scene_desc& d = descs[k];
+    MG_CHECK_ARG(d.positions && d.inv_mass && d.nv > 0 && (d.nt == 0 || d.tris), "batch: null arrays");
+    MG_CHECK_ARG(std::memcmp(&d.params, &d0.params, sizeof(mguso_params)) == 0, "batch: instances must share params");
+    MG_CHECK_ARG(d.ncollider == d0.ncollider &&
+                     (d.ncollider == 0 || std::memcmp(d.colliders, d0.colliders, 32 * (size_t)d.ncollider) == 0),
+                 "batch: instances must share their analytic colliders");
+    nv += d.nv;
+    nt += d.nt;
+    nsh += d.nshell;
+    nst += d.nstitch;
+    any_mask = any_mask || d.static_mask;
+  }
+  MG_CHECK_ARG(nv < (1u << 30), "batch: too many vertices");
+  std::vector<float> pos, vel, im, skl, sw;
+  std::vector<uint32_t> tri, shf, sidx, inst{0};
+  std::vector<uint8_t> mask;
+  pos.reserve(3 * nv);
+  for (uint32_t k = 0; k < n; ++k) {
+    const mguso_scene_desc& d = descs[k];
+    const uint32_t o = (uint32_t)(pos.size() / 3);
+    pos.insert(pos.end(), d.positions, d.positions + 3 * (size_t)d.nv);
+    if (d.velocities)
+      vel.insert(vel.end(), d.velocities, d.velocities + 3 * (size_t)d.nv);
+    else
+      vel.insert(vel.end(), 3 * (size_t)d.nv, 0.f);
+    im.insert(im.end(), d.inv_mass, d.inv_mass + d.nv);
+    if (any_mask) {
+      if (d.static_mask)
+        mask.insert(mask.end(), d.static_mask, d.static_mask + d.nv);
+      else
+        mask.insert(mask.end(), d.nv, 0);
+    }
+    for (uint64_t i = 0; i < 3ull * d.nt; ++i) {
+      MG_CHECK_ARG(d.tris[i] < d.nv, "batch: triangle index out of range");
+      tri.push_back(d.tris[i] + o);
+    }
+    for (uint64_t i = 0; i < 3ull * d.nshell; ++i) {
+      MG_CHECK_ARG(d.shell_faces[i] < d.nv, "batch: shell face index out of range");
+      shf.push_back(d.shell_faces[i] + o);
+    }
+    for (uint64_t i = 0; i < 6ull * d.nstitch; ++i) {
+      MG_CHECK_ARG(d.stitch_idx[i] < d.nv, "batch: stitch index out of range");
+      sidx.push_back(d.stitch_idx[i] + o);
+    }
+    if (d.nstitch) {
+      sw.insert(sw.end(), d.stitch_w, d.stitch_w + 6 * (size_t)d.nstitch);
+      skl.insert(skl.end(), d.stitch_kl, d.stitch_kl + 3 * (size_t)d.nstitch);
+    }
+    inst.push_back(o + d.nv);
+  }
+  mguso_scene_desc u = d0;
+  u.nv = (uint32_t)nv;
+  u.positions = pos.data();
+  u.velocities = vel.data();
+  u.inv_mass = im.data();
+  u.nt = (uint32_t)nt;
+  u.tris = tri.empty() ? nullptr : tri.data();
+  u.static_mask = any_mask ? mask.data() : nullptr;
+  u.nshell = (uint32_t)nsh;
+  u.shell_faces = shf.empty() ? nullptr : shf.data();
+  u.nstitch = (uint32_t)nst;
+  u.stitch_idx = sidx.empty() ? nullptr : sidx.data();
+  u.stitch_w = sw.empty() ? nullptr : sw.data();
+  u.stitch_kl = skl.empty() ? nullptr : skl.data();
+  MG_CUDA(cudaSetDevice(ctx->device));
+  auto sc = std::make_unique<mguso_scene>();
+  sc->s.ctx = ctx;
+  MG_TRY(scene_build(sc->s, &u, inst));
+  *out = sc.release();
+  return MGUSO_OK;
+}
+
+int mguso_scene_instances(mguso_scene* sc, uint32_t* n, uint32_t* vert_offsets) {
+  MG_CHECK_ARG(sc && n, "bad argument");
+  *n = sc->s.ninst;
+  if (vert_offsets) std::memcpy(vert_offsets, sc->s.inst_vert.data(), 4 * sc->s.inst_vert.size());
+  return MGUSO_OK;
+}
+
 int mguso_step(mguso_scene* sc, int nsteps, mguso_step_stats* stats) {
   MG_CHECK_ARG(sc && nsteps >= 0, "bad argument");
   MG_CUDA(cudaSetDevice(sc->s.ctx->device));
+  const uint32_t K = sc->s.ninst;
   for (int k = 0; k < nsteps; ++k) {
-    mguso_step_stats st{};
-    MG_TRY(scene_step(sc->s, &st));
-    if (stats) stats[k] = st;
+    mguso_step_stats st[PCG_MAX_INST];
+    MG_TRY(scene_step(sc->s, st));
+    if (stats)
+      for (uint32_t i = 0; i < K; ++i) stats[(size_t)k * K + i] = st[i];
   }
   return MGUSO_OK;
 }

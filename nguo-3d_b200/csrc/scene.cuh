@@ -33,6 +33,8 @@ struct BlockPattern {
   DevBuf<uint32_t> row_ptr, col;
 };
 
+constexpr uint32_t RED_STRIDE = 16;
+
 struct Scene {
   mguso_ctx* ctx = nullptr;
   cudaStream_t st = nullptr;
@@ -92,8 +94,14 @@ struct Scene {
   DevBuf<uint8_t> static_vert, collider_tri;
   bool has_static = false;
   DevBuf<float> collider_pn;                // 3 per vertex
-  float char_len = 1.f;
-  Lbvh tri_bvh, edge_bvh;
+  // instances: a batch of independent drapes in one scene (one for a single scene), as
+  // contiguous vertex, triangle and edge ranges; every element and stencil lies in one
+  uint32_t ninst = 1;
+  std::vector<uint32_t> inst_vert, inst_tri, inst_edge;  // ninst + 1 each
+  DevBuf<uint8_t> vinst;                                 // per vertex
+  std::vector<float> char_len;                           // per instance
+  std::vector<std::unique_ptr<Lbvh>> tri_bvh, edge_bvh;  // per instance
+  Lbvh sorter;                                           // radix-sort scratch
 
   // self-contact working set
   uint32_t cap_pairs = 0, cap_stencils = 0;
@@ -126,7 +134,7 @@ struct Scene {
   DevBuf<uint32_t> is_new, rank, scan_tmp;
 
   // reductions / CCD
-  DevBuf<unsigned int> red;                 // misc per-iteration reductions (float bits)
+  DevBuf<unsigned int> red;                 // per-iteration reductions (float bits), RED_STRIDE per instance
   DevBuf<uint32_t> status;
 
   // linear solve
@@ -137,7 +145,7 @@ struct Scene {
   std::vector<mguso_step_stats> history;
 };
 
-int scene_build(Scene& s, const mguso_scene_desc* d);
+int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>& inst_vert);
 int scene_step(Scene& s, mguso_step_stats* out);
 
 // assembly (assemble.cu)
@@ -149,9 +157,9 @@ int system_spmv(Scene& s, const float* p, float* ap, cudaStream_t st, const DotS
 
 // contact (contact.cu)
 int build_bvhs(Scene& s, const float* x);
-int pcg_persistent(Scene& s, const uint32_t* h_inst_row, uint32_t ninst, PcgInstResult* out);
+int pcg_persistent(Scene& s, const uint32_t* h_inst_row, uint32_t ninst, uint32_t active, PcgInstResult* out);
 int collect_stencils(Scene& s, uint32_t* nst);
-int ccd_step(Scene& s, float* t_out, uint32_t* cap_hits);
+int ccd_step(Scene& s, uint32_t active, float* t_out, uint32_t* cap_hits);
 
 }  // namespace mg
 

@@ -60,7 +60,13 @@ int schwarz_build(mguso_schwarz* s) {
     s->h_dom_start.push_back((uint32_t)s->h_dom_verts.size());
     max_m = std::max<uint32_t>(max_m, 3 * (uint32_t)(s->h_dom_verts.size() - base));
   };
-  for (uint32_t seed = 0; seed < nb; ++seed) {
+  // instance by instance (vertex ranges; one range for a single scene), so that each
+  // domain lies in one instance and the domains of an instance are contiguous
+  std::vector<uint32_t> ranges = s->inst_vert;
+  if (ranges.size() < 2) ranges = {0, nb};
+  size_t si = 0;
+  for (size_t r = 0; r + 1 < ranges.size(); ++r) {
+  for (uint32_t seed = ranges[r]; seed < ranges[r + 1]; ++seed) {
     if (assigned[seed]) continue;
     size_t base = s->h_dom_verts.size();
     s->h_dom_verts.push_back(seed);
@@ -81,10 +87,15 @@ int schwarz_build(mguso_schwarz* s) {
     }
     close_domain(base);
   }
-  for (size_t i = 0; i < singles.size(); i += D) {
+  // this instance's isolated vertices, D per domain
+  size_t se = si;
+  while (se < singles.size() && singles[se] < ranges[r + 1]) ++se;
+  for (size_t i = si; i < se; i += D) {
     size_t base = s->h_dom_verts.size();
-    for (size_t j = i; j < std::min(singles.size(), i + D); ++j) s->h_dom_verts.push_back(singles[j]);
+    for (size_t j = i; j < std::min(se, i + D); ++j) s->h_dom_verts.push_back(singles[j]);
     close_domain(base);
+  }
+  si = se;
   }
   s->ndom = (uint32_t)s->h_dom_start.size() - 1;
   s->max_m = max_m;

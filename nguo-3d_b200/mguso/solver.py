@@ -59,12 +59,45 @@ def _sigs(lib):
         ("mguso_scene_spmv_time", i32, [vp, i32, P(C.c_float), P(C.c_double)]),
         ("mguso_scene_assemble", i32, [vp, vp, vp, vp]),
         ("mguso_scene_profile", i32, [vp, i32, vp, vp]),
+        ("mguso_batch_create", i32, [vp, vp, C.c_uint32, P(vp)]),
+        ("mguso_scene_instances", i32, [vp, P(C.c_uint32), vp]),
         ("mguso_scene_system", i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
         ("mguso_scene_stencils", i32, [vp, C.c_uint32, vp, vp, vp, vp]),
     ]:
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
+
+
+def _desc(scene: dict, precision: str):
+    """SceneDesc for one scene dict and the arrays it points into (kept alive by the caller)."""
+    keep = {k: np.ascontiguousarray(scene[k]) for k in ("positions", "velocities", "inv_mass", "tris", "shell_faces",
+                                                       "stitch_idx", "stitch_w", "stitch_kl", "colliders")}
+    keep["positions"] = keep["positions"].astype(np.float32, copy=False)
+    keep["velocities"] = keep["velocities"].astype(np.float32, copy=False)
+    keep["inv_mass"] = keep["inv_mass"].astype(np.float32, copy=False)
+    keep["tris"] = keep["tris"].astype(np.uint32, copy=False)
+    keep["shell_faces"] = keep["shell_faces"].astype(np.uint32, copy=False)
+    mask = scene.get("static_mask")
+    keep["mask"] = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+    d = SceneDesc()
+    d.nv = keep["positions"].shape[0]
+    d.positions = ptr(keep["positions"])
+    d.velocities = ptr(keep["velocities"])
+    d.inv_mass = ptr(keep["inv_mass"])
+    d.nt = keep["tris"].shape[0]
+    d.tris = ptr(keep["tris"]) if d.nt else None
+    d.static_mask = ptr(keep["mask"]) if keep["mask"] is not None else None
+    d.nshell = keep["shell_faces"].shape[0]
+    d.shell_faces = ptr(keep["shell_faces"]) if d.nshell else None
+    d.nstitch = keep["stitch_idx"].shape[0]
+    d.stitch_idx = ptr(keep["stitch_idx"]) if d.nstitch else None
+    d.stitch_w = ptr(keep["stitch_w"]) if d.nstitch else None
+    d.stitch_kl = ptr(keep["stitch_kl"]) if d.nstitch else None
+    d.ncollider = keep["colliders"].shape[0]
+    d.colliders = ptr(keep["colliders"]) if d.ncollider else None
+    d.params = make_params(scene["params"], precision)
+    return d, keep
 
 
 def make_params(p: dict, precision: str = "mixed") -> Params:
@@ -85,40 +118,23 @@ class ImplicitSolver:
         self.ctx = ctx
         self.lib = ctx.lib
         _sigs(self.lib)
-        keep = {k: np.ascontiguousarray(scene[k]) for k in ("positions", "velocities", "inv_mass", "tris",
-                                                           "shell_faces", "stitch_idx", "stitch_w", "stitch_kl",
-                                                           "colliders")}
-        pos = keep["positions"].astype(np.float32, copy=False)
-        self.nv = pos.shape[0]
-        mask = scene.get("static_mask")
-        mask = None if mask is None else np.ascontiguousarray(mask, np.uint8)
-        d = SceneDesc()
-        d.nv = self.nv
-        d.positions = ptr(pos)
-        d.velocities = ptr(keep["velocities"].astype(np.float32, copy=False))
-        d.inv_mass = ptr(keep["inv_mass"].astype(np.float32, copy=False))
-        d.nt = keep["tris"].shape[0]
-        d.tris = ptr(keep["tris"].astype(np.uint32, copy=False)) if d.nt else None
-        d.static_mask = ptr(mask) if mask is not None else None
-        d.nshell = keep["shell_faces"].shape[0]
-        d.shell_faces = ptr(keep["shell_faces"].astype(np.uint32, copy=False)) if d.nshell else None
-        d.nstitch = keep["stitch_idx"].shape[0]
-        d.stitch_idx = ptr(keep["stitch_idx"]) if d.nstitch else None
-        d.stitch_w = ptr(keep["stitch_w"]) if d.nstitch else None
-        d.stitch_kl = ptr(keep["stitch_kl"]) if d.nstitch else None
-        d.ncollider = keep["colliders"].shape[0]
-        d.colliders = ptr(keep["colliders"]) if d.ncollider else None
-        d.params = make_params(scene["params"], precision)
-        self._keep = (keep, mask, pos)
+        d, keep = _desc(scene, precision)
+        self.nv = d.nv
+        self._keep = keep
         h = C.c_void_p()
         check(self.lib.mguso_scene_create(ctx.h, C.byref(d), C.byref(h)))
         self.h = h
+        self.ninst = 1
         self.history: list[dict] = []
 
-    def step(self, n: int = 1) -> list[dict]:
-        out = (StepStats * n)()
+    def step(self, n: int = 1) -> list:
+        """Advances n steps. Returns one stats dict per step (a single scene) or, for a
+        batch, one list of per-instance stats dicts per step."""
+        out = (StepStats * (n * self.ninst))()
         check(self.lib.mguso_step(self.h, n, out))
         st = [{f: getattr(o, f) for f, _ in StepStats._fields_} for o in out]
+        if self.ninst > 1:
+            st = [st[i * self.ninst:(i + 1) * self.ninst] for i in range(n)]
         self.history += st
         return st
 
@@ -205,3 +221,29 @@ class ImplicitSolver:
             self.close()
         except Exception:
             pass
+
+
+class ImplicitBatch(ImplicitSolver):
+    """Independent drapes stepped together (mguso_batch_create): one scene whose vertices are
+    the instances' vertices concatenated; each instance keeps its own Newton loop."""
+
+    def __init__(self, ctx, scenes_: list, precision: str = "mixed"):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        _sigs(self.lib)
+        pairs = [_desc(sc, precision) for sc in scenes_]
+        arr = (SceneDesc * len(pairs))(*[d for d, _ in pairs])
+        self._keep = (pairs, arr)
+        h = C.c_void_p()
+        check(self.lib.mguso_batch_create(ctx.h, arr, len(pairs), C.byref(h)))
+        self.h = h
+        n = C.c_uint32()
+        offs = np.zeros(len(pairs) + 1, np.uint32)
+        check(self.lib.mguso_scene_instances(h, C.byref(n), ptr(offs)))
+        self.ninst = n.value
+        self.offsets = offs
+        self.nv = int(offs[-1])
+        self.history = []
+
+    def instance_positions(self, k: int) -> np.ndarray:
+        return self.positions[self.offsets[k]:self.offsets[k + 1]]

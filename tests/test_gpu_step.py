@@ -200,3 +200,49 @@ def test_persistent_pcg_matches_per_kernel_pcg(ctx, precision, precond):
         assert a["status"] == 0 and b["status"] == 0
         assert abs(a["newton_iters"] - b["newton_iters"]) <= 1
         assert abs(a["max_cg_iters"] - b["max_cg_iters"]) <= max(5, b["max_cg_iters"] // 10)
+
+
+def graded_coarse(n=3):
+    widths = (0.50, 0.60, 0.70, 0.55, 0.65, 0.75)[:n]
+    scales = (0.9, 1.02, 1.14, 0.96, 1.08, 1.2)[:n]
+    return [scenes.sheath_on_torso(edge=0.03, torso_res=(30, 29), width=w, torso_scale=t) for w, t in zip(widths, scales)]
+
+
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_batch_matches_instances_run_alone(ctx, precision):
+    """Three graded sheaths stepped as one batch give each instance the trajectory it has when
+    stepped alone: the element, stencil and CCD work is per instance, and only the order of
+    the PCG's dot-product partial sums differs."""
+    from mguso import ImplicitBatch
+
+    scs = graded_coarse(3)
+    b = ImplicitBatch(ctx, scs, precision)
+    assert b.ninst == 3
+    bst = b.step(3)
+    for k, sc in enumerate(scs):
+        g = ImplicitSolver(ctx, sc, precision)
+        gst = g.step(3)
+        pa, pb = g.positions.astype(np.float64), b.instance_positions(k).astype(np.float64)
+        disp = np.abs(pa - sc["positions"]).max()
+        assert np.abs(pa - pb).max() <= 1e-3 * disp, (k, np.abs(pa - pb).max(), disp)
+        for i in range(3):
+            assert bst[i][k]["status"] == 0 and bst[i][k]["penetration_free"]
+            assert abs(bst[i][k]["newton_iters"] - gst[i]["newton_iters"]) <= 1
+        g.close()
+
+
+def test_batch_instance_matches_oracle(ctx):
+    """The second instance of a batch against the oracle of that instance alone."""
+    from mguso import ImplicitBatch
+
+    scs = graded_coarse(2)
+    b = ImplicitBatch(ctx, scs, "mixed")
+    o = O.OracleSolver(scs[1])
+    for i in range(2):
+        st = b.step(1)[0][1]
+        so = o.step(1, check_intersection=False)[0]
+        assert abs(st["newton_iters"] - so["newton_iters"]) <= 1
+    pb = b.instance_positions(1).astype(np.float64)
+    po = o.positions()
+    disp = np.abs(po - scs[1]["positions"]).max()
+    assert np.abs(pb - po).max() <= 2e-2 * disp
