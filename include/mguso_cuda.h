@@ -216,8 +216,11 @@ typedef struct {
   int precond;
   uint32_t schwarz_domain;
   int precision;
-  int pcg_mode;            /* 0: one cooperative persistent launch per linear solve (default);
-                              1: one launch per PCG kernel, replayed as CUDA graphs */
+  int pcg_mode;            /* 0: two fused kernels per iteration (rows, domains) at full
+                                 occupancy, replayed as CUDA graphs (default);
+                              1: one launch per PCG kernel, replayed as CUDA graphs (single
+                                 scenes only);
+                              2: one cooperative persistent launch per linear solve */
 } mguso_params;
 
 /* One scene (Scene::build_implicit + the set_* calls of implicit.rs). All pointers host;

@@ -134,6 +134,17 @@ constexpr int MAX_PARTIALS = 4096;
 
 // Persistent PCG: instances per launch and each instance's result.
 constexpr int PCG_MAX_INST = 8;
+// Fused (two-kernel) PCG: device-resident per-instance state and control words.
+struct FusedInst {
+  double rz, alpha, beta, bnorm, residual;
+  uint32_t iters, done, upd, status;
+};
+struct FusedCtl {
+  uint32_t counter[2];
+  uint32_t all_done;
+  uint32_t pad;
+};
+
 struct PcgInstResult {
   double residual;
   uint32_t iters, status, done, pad;

@@ -1,0 +1,513 @@
+// Fused two-kernel PCG for the Newton systems (linsolve.rs:350-411), replayed as CUDA
+// graphs of 16 iterations, for systems large enough to fill the GPU (batches of drapes).
+//
+// Each iteration is two full-occupancy kernels:
+//   rows:    p = z + beta p_old for the CTA's block rows (into the other p buffer), Ap with
+//            every gathered p_j formed the same way, p.Ap; the last CTA to finish sums the
+//            per-CTA partials of each instance in CTA order and sets alpha (or flags a
+//            breakdown, pAp <= 0 or NaN, where the reference breaks out);
+//   domains: one warp per Schwarz domain (block Jacobi: one thread per vertex) updates
+//            x += alpha p, r -= alpha Ap on its rows, applies the preconditioner to them,
+//            and accumulates r.r and r.z; the last CTA sets the residual, the convergence
+//            flag, beta and rz.
+// CTAs are partitioned by instance, so a CTA's partials belong to one instance and each
+// instance's sums are deterministic. Kernels of converged instances skip their work, and a
+// kernel launched after every instance converged returns at entry.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "reduce.cuh"
+#include "scene.cuh"
+#include "tiles.cuh"
+
+namespace mg {
+
+constexpr int FR_THREADS = 256;
+constexpr int FR_LPR = 2;          // lanes per block row
+constexpr int FD_WARPS = 4;        // Schwarz: warps (domains) per CTA
+constexpr int FD_THREADS = 256;    // block Jacobi: vertices per CTA
+constexpr uint32_t FUSED_CHECK = 16;
+
+struct FusedArgs {
+  uint32_t ninst;
+  const uint32_t* lay;  // [0, K] rows, [9 ..] row-kernel CTAs, [18 ..] domain-kernel CTAs, [27 ..] domains
+  const uint32_t *rp, *col;
+  const float* val;
+  const uint32_t *crp, *ccol;
+  const float* cval;
+  const float* bjinv;
+  const uint32_t *dom_start, *dom_verts;
+  const uint64_t* fac_off;
+  const float* fac;
+  const float* b;
+  float *x, *r, *z, *ap;
+  float tol;
+  uint32_t max_iter;
+  FusedInst* inst;
+  FusedCtl* ctl;
+  double* part;  // row kernel: [cta]; domain kernel: [2 * cta + j]
+};
+
+constexpr int LAY = PCG_MAX_INST + 1;
+
+__device__ __forceinline__ float fr_fma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fr_fma(double a, double b, double c) { return fma(a, b, c); }
+
+__device__ __forceinline__ int cta_instance(const uint32_t* cta, uint32_t K) {
+  int k = 0;
+  while (k + 1 < (int)K && blockIdx.x >= __ldg(cta + k + 1)) ++k;
+  return k;
+}
+
+// The last CTA of the grid to arrive returns true (after a fence, so all partials are visible).
+__device__ __forceinline__ bool last_cta(uint32_t* counter) {
+  __shared__ bool s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_last) __threadfence();
+  return s_last;
+}
+
+template <class Acc>
+__global__ void __launch_bounds__(FR_THREADS) k_fr_rows(FusedArgs a, const float* __restrict__ po,
+                                                        float* __restrict__ pn) {
+  if (a.ctl->all_done) return;
+  const uint32_t K = a.ninst;
+  const int k = cta_instance(a.lay + LAY, K);
+  const uint32_t c0 = __ldg(a.lay + LAY + k), nc = __ldg(a.lay + LAY + k + 1) - c0, lc = blockIdx.x - c0;
+  const uint32_t row0 = __ldg(a.lay + k), row1 = __ldg(a.lay + k + 1);
+  const bool done = a.inst[k].done != 0;
+  const float be = (float)a.inst[k].beta;
+  const int tid = threadIdx.x, lane = tid & 31;
+  const uint32_t sub = tid % FR_LPR;
+  const unsigned gmask = ((1u << FR_LPR) - 1u) << (lane & ~(FR_LPR - 1));
+  Acc acc = 0;
+  if (!done) {
+    for (uint32_t row = row0 + (lc * FR_THREADS + tid) / FR_LPR; row < row1; row += nc * FR_THREADS / FR_LPR) {
+      Acc y0 = 0, y1 = 0, y2 = 0;
+      auto block = [&](const float* __restrict__ m9, uint32_t c) {
+        const Acc x0 = (Acc)fmaf(be, po[3 * c], a.z[3 * c]);
+        const Acc x1 = (Acc)fmaf(be, po[3 * c + 1], a.z[3 * c + 1]);
+        const Acc x2 = (Acc)fmaf(be, po[3 * c + 2], a.z[3 * c + 2]);
+        y0 = fr_fma((Acc)__ldg(m9 + 0), x0, y0);
+        y0 = fr_fma((Acc)__ldg(m9 + 1), x1, y0);
+        y0 = fr_fma((Acc)__ldg(m9 + 2), x2, y0);
+        y1 = fr_fma((Acc)__ldg(m9 + 3), x0, y1);
+        y1 = fr_fma((Acc)__ldg(m9 + 4), x1, y1);
+        y1 = fr_fma((Acc)__ldg(m9 + 5), x2, y1);
+        y2 = fr_fma((Acc)__ldg(m9 + 6), x0, y2);
+        y2 = fr_fma((Acc)__ldg(m9 + 7), x1, y2);
+        y2 = fr_fma((Acc)__ldg(m9 + 8), x2, y2);
+      };
+      const uint32_t ke = __ldg(a.rp + row + 1);
+#pragma unroll 4
+      for (uint32_t kk = __ldg(a.rp + row) + sub; kk < ke; kk += FR_LPR) block(a.val + 9 * (size_t)kk, __ldg(a.col + kk));
+      const uint32_t ce = __ldg(a.crp + row + 1);
+      for (uint32_t kk = __ldg(a.crp + row) + sub; kk < ce; kk += FR_LPR) block(a.cval + 9 * (size_t)kk, __ldg(a.ccol + kk));
+#pragma unroll
+      for (int o = FR_LPR / 2; o > 0; o >>= 1) {
+        y0 += __shfl_xor_sync(gmask, y0, o, FR_LPR);
+        y1 += __shfl_xor_sync(gmask, y1, o, FR_LPR);
+        y2 += __shfl_xor_sync(gmask, y2, o, FR_LPR);
+      }
+      if (sub == 0) {
+        const float f0 = (float)y0, f1 = (float)y1, f2 = (float)y2;
+        const float q0 = fmaf(be, po[3 * row], a.z[3 * row]);
+        const float q1 = fmaf(be, po[3 * row + 1], a.z[3 * row + 1]);
+        const float q2 = fmaf(be, po[3 * row + 2], a.z[3 * row + 2]);
+        pn[3 * row] = q0;
+        pn[3 * row + 1] = q1;
+        pn[3 * row + 2] = q2;
+        a.ap[3 * row] = f0;
+        a.ap[3 * row + 1] = f1;
+        a.ap[3 * row + 2] = f2;
+        acc += (Acc)q0 * (Acc)f0 + (Acc)q1 * (Acc)f1 + (Acc)q2 * (Acc)f2;
+      }
+    }
+  }
+  const Acc s = block_sum<Acc>(acc);
+  if (tid == 0) a.part[blockIdx.x] = (double)s;
+  if (!last_cta(&a.ctl->counter[0])) return;
+  // alpha per instance, partials summed in CTA order
+  const int w = tid >> 5;
+  for (uint32_t q = w; q < K; q += FR_THREADS / 32) {
+    const uint32_t cb = a.lay[LAY + q], ce = a.lay[LAY + q + 1];
+    double t = 0;
+    for (uint32_t c = cb + lane; c < ce; c += 32) t += ((volatile double*)a.part)[c];
+    t = warp_sum(t);
+    if (lane == 0) {
+      FusedInst& I = a.inst[q];
+      I.upd = 0;
+      if (!I.done) {
+        if (!(t > 0.0)) {
+          I.done = 1;
+          I.status |= ST_PCG_BREAKDOWN;
+        } else {
+          I.alpha = I.rz / t;
+          I.upd = 1;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    a.ctl->counter[0] = 0;
+    __threadfence();
+  }
+}
+
+// finish of the domain kernel (and of the initialisation): instance sums of r.r and r.z
+__device__ __forceinline__ void fd_finish(const FusedArgs& a, bool init) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const uint32_t K = a.ninst;
+  for (uint32_t q = w; q < K; q += nw) {
+    const uint32_t cb = a.lay[2 * LAY + q], ce = a.lay[2 * LAY + q + 1];
+    double rr = 0, rz = 0;
+    for (uint32_t c = cb + lane; c < ce; c += 32) {
+      rr += ((volatile double*)a.part)[2 * c];
+      rz += ((volatile double*)a.part)[2 * c + 1];
+    }
+    rr = warp_sum(rr);
+    rz = warp_sum(rz);
+    if (lane == 0) {
+      FusedInst& I = a.inst[q];
+      if (init) {
+        I.bnorm = fmax(sqrt(rr), 1e-30);
+        I.residual = sqrt(rr) / I.bnorm;
+        I.rz = rz;
+        I.beta = 0.0;
+      } else if (I.upd) {
+        I.iters += 1;
+        I.residual = sqrt(rr) / I.bnorm;
+        if (I.residual <= (double)a.tol || I.iters >= a.max_iter) {
+          I.done = 1;
+        } else {
+          I.beta = rz / I.rz;
+          I.rz = rz;
+        }
+        I.upd = 0;
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t all = 1;
+    for (uint32_t q = 0; q < K; ++q) all &= a.inst[q].done ? 1u : 0u;
+    a.ctl->all_done = all;
+    a.ctl->counter[1] = 0;
+    __threadfence();
+  }
+}
+
+// Schwarz domains: one warp per domain. init: x = 0, r = b, p_init = 0.
+template <class Acc>
+__global__ void __launch_bounds__(32 * FD_WARPS) k_fr_schwarz(FusedArgs a, const float* __restrict__ pc,
+                                                             float* __restrict__ p_init, int init) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  if (!init && a.ctl->all_done) return;
+  const uint32_t K = a.ninst;
+  const int k = cta_instance(a.lay + 2 * LAY, K);
+  const uint32_t c0 = __ldg(a.lay + 2 * LAY + k);
+  const uint32_t d = __ldg(a.lay + 3 * LAY + k) + (blockIdx.x - c0) * FD_WARPS + (threadIdx.x >> 5);
+  const uint32_t dend = __ldg(a.lay + 3 * LAY + k + 1);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const bool upd = !init && a.inst[k].upd != 0;
+  const float al = (float)a.inst[k].alpha;
+  const bool skip = !init && a.inst[k].done != 0 && !upd;
+  uint64_t* bar = (uint64_t*)(smem + 16 * w);
+  float* buf = (float*)(smem + 128 + (size_t)w * APPLY_SLICE * 4);
+  float* rd = buf + 6 * TILE_FLOATS;
+  Acc* yd = (Acc*)(rd + 96);
+  Acc rr = 0, rz = 0;
+  if (d < dend && !skip) {
+    const uint32_t vs = a.dom_start[d], nvd = a.dom_start[d + 1] - vs;
+    const int m = 3 * (int)nvd;
+    const uint64_t off = a.fac_off[d];
+    const uint32_t bytes = (uint32_t)((a.fac_off[d + 1] - off) * 4);
+    if (lane == 0) {
+      mbar_init(bar, 1);
+      fence_mbar_init();
+      fence_proxy_async();
+      mbar_arrive_expect_tx(bar, bytes);
+      bulk_g2s(buf, a.fac + off, bytes, bar);
+    }
+    for (int i = lane; i < 96; i += 32) {
+      float v = 0.f;
+      if (i < m) {
+        const uint32_t e = 3 * a.dom_verts[vs + i / 3] + i % 3;
+        if (init) {
+          v = a.b[e];
+          a.x[e] = 0.f;
+          a.r[e] = v;
+          p_init[e] = 0.f;
+        } else if (upd) {
+          a.x[e] = fmaf(al, pc[e], a.x[e]);
+          v = fmaf(-al, a.ap[e], a.r[e]);
+          a.r[e] = v;
+        } else {
+          v = a.r[e];
+        }
+      }
+      rd[i] = v;
+    }
+    __syncwarp();
+    if (!mbar_wait(bar, 0)) {
+      if (lane == 0) atomicOr(&a.inst[k].status, ST_WAIT_TIMEOUT);
+      mbar_wait(bar, 0);  // bounded again: the copy may still land
+    } else {
+      Acc zz[3];
+      const int T = (m + 31) >> 5;
+      if (T == 3)
+        tiles_apply<3, Acc>(buf, rd, yd, zz, lane);
+      else if (T == 2)
+        tiles_apply<2, Acc>(buf, rd, yd, zz, lane);
+      else
+        tiles_apply<1, Acc>(buf, rd, yd, zz, lane);
+#pragma unroll
+      for (int J = 0; J < 3; ++J) {
+        const int i = 32 * J + lane;
+        if (i < m) {
+          const float zi = (float)zz[J];
+          a.z[3 * a.dom_verts[vs + i / 3] + i % 3] = zi;
+          rr += (Acc)rd[i] * (Acc)rd[i];
+          rz += (Acc)rd[i] * (Acc)zi;
+        }
+      }
+    }
+  }
+  const Acc s0 = block_sum<Acc>(rr);
+  const Acc s1 = block_sum<Acc>(rz);
+  if (threadIdx.x == 0) {
+    a.part[2 * blockIdx.x] = (double)s0;
+    a.part[2 * blockIdx.x + 1] = (double)s1;
+  }
+  if (!last_cta(&a.ctl->counter[1])) return;
+  fd_finish(a, init != 0);
+}
+
+// Block Jacobi: one thread per vertex. init: x = 0, r = b, p_init = 0.
+template <class Acc>
+__global__ void __launch_bounds__(FD_THREADS) k_fr_bj(FusedArgs a, const float* __restrict__ pc,
+                                                     float* __restrict__ p_init, int init) {
+  if (!init && a.ctl->all_done) return;
+  const uint32_t K = a.ninst;
+  const int k = cta_instance(a.lay + 2 * LAY, K);
+  const uint32_t c0 = __ldg(a.lay + 2 * LAY + k);
+  const uint32_t v = __ldg(a.lay + k) + (blockIdx.x - c0) * FD_THREADS + threadIdx.x;
+  const uint32_t vend = __ldg(a.lay + k + 1);
+  const bool upd = !init && a.inst[k].upd != 0;
+  const float al = (float)a.inst[k].alpha;
+  const bool skip = !init && a.inst[k].done != 0 && !upd;
+  Acc rr = 0, rz = 0;
+  if (v < vend && !skip) {
+    float q[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const uint32_t e = 3 * v + c;
+      if (init) {
+        q[c] = a.b[e];
+        a.x[e] = 0.f;
+        a.r[e] = q[c];
+        p_init[e] = 0.f;
+      } else if (upd) {
+        a.x[e] = fmaf(al, pc[e], a.x[e]);
+        q[c] = fmaf(-al, a.ap[e], a.r[e]);
+        a.r[e] = q[c];
+      } else {
+        q[c] = a.r[e];
+      }
+    }
+    const float* m9 = a.bjinv + 9 * (size_t)v;
+    const float z0 = m9[0] * q[0] + m9[1] * q[1] + m9[2] * q[2];
+    const float z1 = m9[3] * q[0] + m9[4] * q[1] + m9[5] * q[2];
+    const float z2 = m9[6] * q[0] + m9[7] * q[1] + m9[8] * q[2];
+    a.z[3 * v] = z0;
+    a.z[3 * v + 1] = z1;
+    a.z[3 * v + 2] = z2;
+    rr = (Acc)q[0] * (Acc)q[0] + (Acc)q[1] * (Acc)q[1] + (Acc)q[2] * (Acc)q[2];
+    rz = (Acc)q[0] * (Acc)z0 + (Acc)q[1] * (Acc)z1 + (Acc)q[2] * (Acc)z2;
+  }
+  const Acc s0 = block_sum<Acc>(rr);
+  const Acc s1 = block_sum<Acc>(rz);
+  if (threadIdx.x == 0) {
+    a.part[2 * blockIdx.x] = (double)s0;
+    a.part[2 * blockIdx.x + 1] = (double)s1;
+  }
+  if (!last_cta(&a.ctl->counter[1])) return;
+  fd_finish(a, init != 0);
+}
+
+namespace {
+struct Launch {
+  void* rows;
+  void* dom;
+  size_t dom_smem;
+  uint32_t grid_rows, grid_dom;
+};
+
+Launch fused_kernels(const Scene& s) {
+  Launch L{};
+  const bool sch = s.schwarz != nullptr;
+  L.rows = s.mixed ? (void*)k_fr_rows<double> : (void*)k_fr_rows<float>;
+  if (sch) {
+    L.dom = s.mixed ? (void*)k_fr_schwarz<double> : (void*)k_fr_schwarz<float>;
+    L.dom_smem = 128 + (size_t)FD_WARPS * APPLY_SLICE * 4;
+  } else {
+    L.dom = s.mixed ? (void*)k_fr_bj<double> : (void*)k_fr_bj<float>;
+    L.dom_smem = 0;
+  }
+  return L;
+}
+}  // namespace
+
+// Solves the scene's current system (work.b) into work.x; instance k covers block rows
+// [h_inst_row[k], h_inst_row[k+1]); instances outside `active` keep x = 0. out[k] gets each
+// instance's result. Schwarz domains must be grouped by instance.
+int pcg_fused(Scene& s, const uint32_t* h_inst_row, uint32_t K, uint32_t active, PcgInstResult* out) {
+  MG_CHECK_ARG(K >= 1 && K <= PCG_MAX_INST, "fused PCG: 1..8 instances");
+  cudaStream_t st = s.st;
+  PcgWork& w = s.work;
+  Launch L = fused_kernels(s);
+  // layout: rows, row-kernel CTAs, domain-kernel CTAs, domains (per instance)
+  std::vector<uint32_t> key(h_inst_row, h_inst_row + K + 1);
+  if (key != s.fr_key) {
+    std::vector<uint32_t> lay(4 * LAY, 0);
+    for (uint32_t k = 0; k <= K; ++k) lay[k] = h_inst_row[k];
+    uint32_t* dom = lay.data() + 3 * LAY;
+    if (s.schwarz) {
+      mguso_schwarz* sw = s.schwarz.get();
+      uint32_t kk = 0;
+      for (uint32_t d = 0; d < sw->ndom; ++d) {
+        const uint32_t v0 = sw->h_dom_verts[sw->h_dom_start[d]];
+        while (kk < K && v0 >= h_inst_row[kk + 1]) dom[++kk] = d;
+        MG_CHECK_ARG(kk < K, "fused PCG: Schwarz domains are not grouped by instance");
+      }
+      while (kk < K) dom[++kk] = sw->ndom;
+    }
+    for (uint32_t k = 0; k < K; ++k) {
+      const uint32_t rows = h_inst_row[k + 1] - h_inst_row[k];
+      const uint32_t cr = std::max<uint32_t>(1, ceil_div(rows * FR_LPR, FR_THREADS));
+      const uint32_t cd = s.schwarz ? std::max<uint32_t>(1, ceil_div(dom[k + 1] - dom[k], FD_WARPS))
+                                    : std::max<uint32_t>(1, ceil_div(rows, FD_THREADS));
+      lay[LAY + k + 1] = lay[LAY + k] + cr;
+      lay[2 * LAY + k + 1] = lay[2 * LAY + k] + cd;
+    }
+    MG_TRY(s.fr_lay.upload(lay.data(), lay.size(), st));
+    s.fr_grid_rows = lay[LAY + K];
+    s.fr_grid_dom = lay[2 * LAY + K];
+    s.fr_key = key;
+    s.fr_graph_key.clear();
+  }
+  L.grid_rows = s.fr_grid_rows;
+  L.grid_dom = s.fr_grid_dom;
+  MG_TRY(w.p2.reserve(w.n));
+  MG_TRY(s.fr_inst.reserve(PCG_MAX_INST));
+  MG_TRY(s.fr_ctl.reserve(1));
+  MG_TRY(s.fr_part.reserve(2ull * std::max(L.grid_rows, L.grid_dom)));
+  FusedInst hi[PCG_MAX_INST] = {};
+  for (uint32_t k = 0; k < K; ++k) hi[k].done = ((active >> k) & 1u) ? 0u : 1u;
+  FusedCtl hc{};
+  MG_CUDA(cudaMemcpyAsync(s.fr_inst.p, hi, sizeof(FusedInst) * K, cudaMemcpyHostToDevice, st));
+  MG_CUDA(cudaMemcpyAsync(s.fr_ctl.p, &hc, sizeof(FusedCtl), cudaMemcpyHostToDevice, st));
+
+  FusedArgs a{};
+  a.ninst = K;
+  a.lay = s.fr_lay.p;
+  a.rp = s.Ps.row_ptr.p;
+  a.col = s.Ps.col.p;
+  a.val = s.A->val.p;
+  a.crp = s.c_row_ptr.p;
+  a.ccol = s.c_col.p ? s.c_col.p : s.c_row_ptr.p;
+  a.cval = s.c_val.p;
+  a.bjinv = s.bjinv.p;
+  if (s.schwarz) {
+    mguso_schwarz* sw = s.schwarz.get();
+    a.dom_start = sw->dom_start.p;
+    a.dom_verts = sw->dom_verts.p;
+    a.fac_off = sw->fac_off.p;
+    a.fac = sw->fac.p;
+  }
+  a.b = w.b.p;
+  a.x = w.x.p;
+  a.r = w.r.p;
+  a.z = w.z.p;
+  a.ap = w.ap.p;
+  a.tol = s.p.cg_tol;
+  a.max_iter = s.p.cg_max_iter;
+  a.inst = s.fr_inst.p;
+  a.ctl = s.fr_ctl.p;
+  a.part = s.fr_part.p;
+  float* p0 = w.p.p;
+  float* p1 = w.p2.p;
+  auto launch_dom = [&](const float* pc, float* pinit, int init) -> int {
+    void* args[] = {(void*)&a, (void*)&pc, (void*)&pinit, (void*)&init};
+    MG_CUDA(cudaLaunchKernel(L.dom, dim3(L.grid_dom), dim3(s.schwarz ? 32 * FD_WARPS : FD_THREADS), args,
+                             L.dom_smem, st));
+    return MGUSO_OK;
+  };
+  auto launch_rows = [&](const float* po, float* pn) -> int {
+    void* args[] = {(void*)&a, (void*)&po, (void*)&pn};
+    MG_CUDA(cudaLaunchKernel(L.rows, dim3(L.grid_rows), dim3(FR_THREADS), args, 0, st));
+    return MGUSO_OK;
+  };
+  if (L.dom_smem) MG_CUDA(cudaFuncSetAttribute(L.dom, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.dom_smem));
+  // x = 0, r = b, p0 = 0, z = M^-1 r, norms
+  MG_TRY(launch_dom(p0, p0, 1));
+  // one graph of FUSED_CHECK iterations (p alternates between the two buffers)
+  std::vector<unsigned char> gk(sizeof(FusedArgs) + 2 * sizeof(void*) + 2 * sizeof(uint32_t));
+  std::memcpy(gk.data(), &a, sizeof(FusedArgs));
+  std::memcpy(gk.data() + sizeof(FusedArgs), &p0, sizeof(void*));
+  std::memcpy(gk.data() + sizeof(FusedArgs) + sizeof(void*), &p1, sizeof(void*));
+  std::memcpy(gk.data() + sizeof(FusedArgs) + 2 * sizeof(void*), &L.grid_rows, 4);
+  std::memcpy(gk.data() + sizeof(FusedArgs) + 2 * sizeof(void*) + 4, &L.grid_dom, 4);
+  if (gk != s.fr_graph_key || !s.fr_exec) {
+    if (s.fr_exec) cudaGraphExecDestroy(s.fr_exec);
+    s.fr_exec = nullptr;
+    cudaGraph_t g = nullptr;
+    MG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int rc = MGUSO_OK;
+    for (uint32_t i = 0; i < FUSED_CHECK && rc == MGUSO_OK; ++i) {
+      const float* po = (i & 1) ? p1 : p0;
+      float* pn = (i & 1) ? p0 : p1;
+      rc = launch_rows(po, pn);
+      if (rc == MGUSO_OK) rc = launch_dom(pn, pn, 0);
+    }
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (rc != MGUSO_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    MG_CUDA(e);
+    cudaError_t ie = cudaGraphInstantiate(&s.fr_exec, g, 0);
+    cudaGraphDestroy(g);
+    MG_CUDA(ie);
+    s.fr_graph_key = gk;
+  }
+  FusedCtl h{};
+  for (uint32_t launched = 0; launched < s.p.cg_max_iter + FUSED_CHECK; launched += FUSED_CHECK) {
+    MG_CUDA(cudaGraphLaunch(s.fr_exec, st));
+    MG_CUDA(cudaMemcpyAsync(&h, s.fr_ctl.p, sizeof(FusedCtl), cudaMemcpyDeviceToHost, st));
+    MG_CUDA(cudaStreamSynchronize(st));
+    if (h.all_done) break;
+  }
+  MG_CUDA(cudaMemcpyAsync(hi, s.fr_inst.p, sizeof(FusedInst) * K, cudaMemcpyDeviceToHost, st));
+  MG_CUDA(cudaStreamSynchronize(st));
+  for (uint32_t k = 0; k < K; ++k) {
+    out[k].iters = hi[k].iters;
+    out[k].residual = hi[k].residual;
+    out[k].status = hi[k].status;
+    out[k].done = hi[k].done;
+    if (hi[k].status & ST_WAIT_TIMEOUT) {
+      set_error("fused PCG: a bounded bulk-copy wait timed out");
+      return MGUSO_ERR_TIMEOUT;
+    }
+  }
+  return MGUSO_OK;
+}
+
+}  // namespace mg

@@ -65,7 +65,7 @@ int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>
   s.nv = nv;
   s.nt = nt;
   s.mixed = d->params.precision == MGUSO_PRECISION_MIXED;
-  MG_CHECK_ARG(d->params.pcg_mode == 0 || d->params.pcg_mode == 1, "scene: pcg_mode must be 0 or 1");
+  MG_CHECK_ARG(d->params.pcg_mode >= 0 && d->params.pcg_mode <= 2, "scene: pcg_mode must be 0, 1 or 2");
   s.st = s.ctx->stream;
   cudaStream_t st = s.st;
   const float* P = d->positions;

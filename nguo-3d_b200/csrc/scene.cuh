@@ -118,6 +118,18 @@ struct Scene {
   DevBuf<uint64_t> pp_probe;
   DevBuf<double> pp_part;
   std::vector<uint32_t> pp_key;  // instance rows the uploaded layout was built for
+  // fused two-kernel PCG: layout, per-instance state, partials and the cached graph
+  std::vector<uint32_t> fr_key;
+  std::vector<unsigned char> fr_graph_key;
+  DevBuf<uint32_t> fr_lay;
+  uint32_t fr_grid_rows = 0, fr_grid_dom = 0;
+  DevBuf<FusedInst> fr_inst;
+  DevBuf<FusedCtl> fr_ctl;
+  DevBuf<double> fr_part;
+  cudaGraphExec_t fr_exec = nullptr;
+  ~Scene() {
+    if (fr_exec) cudaGraphExecDestroy(fr_exec);
+  }
   DevBuf<unsigned long long> st_keys;
   DevBuf<uint32_t> st_ids;
   // contact contributions (32 blocks + 4 gradient entries per stencil)
@@ -158,6 +170,7 @@ int system_spmv(Scene& s, const float* p, float* ap, cudaStream_t st, const DotS
 // contact (contact.cu)
 int build_bvhs(Scene& s, const float* x);
 int pcg_persistent(Scene& s, const uint32_t* h_inst_row, uint32_t ninst, uint32_t active, PcgInstResult* out);
+int pcg_fused(Scene& s, const uint32_t* h_inst_row, uint32_t ninst, uint32_t active, PcgInstResult* out);
 int collect_stencils(Scene& s, uint32_t* nst);
 int ccd_step(Scene& s, uint32_t active, float* t_out, uint32_t* cap_hits);
 

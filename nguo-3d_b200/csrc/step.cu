@@ -126,9 +126,10 @@ static int linear_solve(Scene& s, uint32_t active, mguso_lin_stats* ls) {
   } else {
     MG_TRY(blockjacobi_factor(s.A.get(), s.bjinv.p, st));
   }
-  if (s.p.pcg_mode == 0 || s.ninst > 1) {
+  if (s.p.pcg_mode == 0 || s.p.pcg_mode == 2 || s.ninst > 1) {
     PcgInstResult r[PCG_MAX_INST] = {};
-    int rc = pcg_persistent(s, s.inst_vert.data(), s.ninst, active, r);
+    int rc = s.p.pcg_mode == 2 ? pcg_persistent(s, s.inst_vert.data(), s.ninst, active, r)
+                               : pcg_fused(s, s.inst_vert.data(), s.ninst, active, r);
     if (rc == MGUSO_OK) {
       for (uint32_t k = 0; k < s.ninst; ++k) {
         ls[k].iters = r[k].iters;

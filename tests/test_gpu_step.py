@@ -181,25 +181,27 @@ def test_sheath_steps_match_oracle(ctx):
 @pytest.mark.parametrize("precision", ["fp32", "mixed"])
 @pytest.mark.parametrize("precond", [2, 1])
 def test_persistent_pcg_matches_per_kernel_pcg(ctx, precision, precond):
-    """The one-launch persistent PCG and the per-kernel PCG are the same iteration; they
-    differ only in the order of dot-product partial sums, so two drape steps agree to the
-    Newton tolerance and their PCG iteration counts stay close."""
+    """The fused two-kernel PCG (mode 0), the per-kernel PCG (mode 1) and the one-launch
+    persistent PCG (mode 2) are the same iteration; they differ only in the order of
+    dot-product partial sums, so two drape steps agree to the Newton tolerance and their PCG
+    iteration counts stay close."""
     sc = coarse_sheath()
     sc["params"] = dict(sc["params"], precond=precond)
     runs = []
-    for mode in (0, 1):
+    for mode in (0, 1, 2):
         s2 = dict(sc)
         s2["params"] = dict(sc["params"], pcg_mode=mode)
         g = ImplicitSolver(ctx, s2, precision)
         st = g.step(2)
         runs.append((g.positions.astype(np.float64), st))
-    (p0, s0), (p1, s1) = runs
+    (p1, s1) = runs[1]
     disp = np.abs(p1 - sc["positions"]).max()
-    assert np.abs(p0 - p1).max() <= 1e-3 * disp
-    for a, b in zip(s0, s1):
-        assert a["status"] == 0 and b["status"] == 0
-        assert abs(a["newton_iters"] - b["newton_iters"]) <= 1
-        assert abs(a["max_cg_iters"] - b["max_cg_iters"]) <= max(5, b["max_cg_iters"] // 10)
+    for p0, s0 in (runs[0], runs[2]):
+        assert np.abs(p0 - p1).max() <= 1e-3 * disp
+        for a, b in zip(s0, s1):
+            assert a["status"] == 0 and b["status"] == 0
+            assert abs(a["newton_iters"] - b["newton_iters"]) <= 1
+            assert abs(a["max_cg_iters"] - b["max_cg_iters"]) <= max(5, b["max_cg_iters"] // 10)
 
 
 def graded_coarse(n=3):
@@ -208,14 +210,17 @@ def graded_coarse(n=3):
     return [scenes.sheath_on_torso(edge=0.03, torso_res=(30, 29), width=w, torso_scale=t) for w, t in zip(widths, scales)]
 
 
+@pytest.mark.parametrize("pcg_mode", [0, 2])
 @pytest.mark.parametrize("precision", ["fp32", "mixed"])
-def test_batch_matches_instances_run_alone(ctx, precision):
+def test_batch_matches_instances_run_alone(ctx, precision, pcg_mode):
     """Three graded sheaths stepped as one batch give each instance the trajectory it has when
     stepped alone: the element, stencil and CCD work is per instance, and only the order of
     the PCG's dot-product partial sums differs."""
     from mguso import ImplicitBatch
 
     scs = graded_coarse(3)
+    for sc in scs:
+        sc["params"] = dict(sc["params"], pcg_mode=pcg_mode)
     b = ImplicitBatch(ctx, scs, precision)
     assert b.ninst == 3
     bst = b.step(3)
