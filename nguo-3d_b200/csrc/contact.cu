@@ -30,10 +30,12 @@ struct BvhView {
   const uint32_t *left, *right, *prim;
   const float4 *node, *leaf;
   uint32_t n;
+  const float4 *cnode, *cleaf;  // CCD-inflated boxes of the same tree (CCD only)
 };
 
 static BvhView view(const Lbvh& b) {
-  return BvhView{b.left.p, b.right.p, b.perm.p, (const float4*)b.node.p, (const float4*)b.leaf.p, b.nt};
+  return BvhView{b.left.p, b.right.p, b.perm.p, (const float4*)b.node.p, (const float4*)b.leaf.p, b.nt,
+                 (const float4*)b.cnode.p, (const float4*)b.cleaf.p};
 }
 
 // One tree per instance over that instance's primitives (a query only meets its own
@@ -50,6 +52,16 @@ static BvhSet view_set(const std::vector<std::unique_ptr<Lbvh>>& b, const std::v
     s.base[k] = base[k];
   }
   return s;
+}
+
+// search box against the exact boxes and pruning box against the inflated ones
+template <class F>
+__device__ __forceinline__ bool visit_ccd(const BvhSet& bs, uint32_t k, float4 lo, float4 hi, float4 plo, float4 phi,
+                                          F&& f) {
+  const BvhView& bv = bs.t[k];
+  const uint32_t base = bs.base[k];
+  return lbvh_visit2(bv.left, bv.right, bv.node, bv.leaf, bv.cnode, bv.cleaf, bv.prim, bv.n, lo, hi, plo, phi,
+                     [&](uint32_t local) { f(base + local); });
 }
 
 template <class F>
@@ -342,6 +354,37 @@ __global__ void k_ccd_colliders(const uint32_t* __restrict__ free_verts, uint32_
   if (t < 1.f) atomic_min_pos(red + RED_STRIDE * vinst[i] + 1, t);
 }
 
+// CCD candidate pruning. accd_toi (contact.rs:378-437) returns max_t at its first test
+// whenever max_t * u_max < 0.98 d0, where u_max is the largest relative displacement of the
+// four points and d0 their distance: such a pair cannot lower the step fraction. For any
+// common vector c, u_max <= 2 max_i |dx_i - c|, so with per-vertex radii r_v = 2.6 |dx_v - c|
+// (2% above 1.25 / 0.98 x 2) a pair whose query box (radius r_v) misses its primitive's box
+// grown by the primitive's largest radius is exactly such a pair, and is skipped. c is the
+// instance's mean displacement of free vertices, so a cloth falling as a whole prunes almost
+// everything. Traversal enters a subtree only if the reference's search box overlaps its exact
+// box and the pruning box overlaps its inflated box.
+__global__ void k_ccd_mean(const float* __restrict__ dx, const float* __restrict__ im,
+                           const uint8_t* __restrict__ vinst, uint32_t nv, float* __restrict__ acc) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv || !(im[i] > 0.f)) return;
+  float* a = acc + 4 * vinst[i];
+  atomicAdd(a, dx[3 * i]);
+  atomicAdd(a + 1, dx[3 * i + 1]);
+  atomicAdd(a + 2, dx[3 * i + 2]);
+  atomicAdd(a + 3, 1.f);
+}
+
+__global__ void k_ccd_radius(const float* __restrict__ dx, const uint8_t* __restrict__ vinst, uint32_t nv,
+                             const float* __restrict__ acc, float* __restrict__ rv) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  const float* a = acc + 4 * vinst[i];
+  const float n = fmaxf(a[3], 1.f);
+  const float cx = a[0] / n, cy = a[1] / n, cz = a[2] / n;
+  const float ex = dx[3 * i] - cx, ey = dx[3 * i + 1] - cy, ez = dx[3 * i + 2] - cz;
+  rv[i] = 2.6f * sqrtf(ex * ex + ey * ey + ez * ez) + 1.0e-9f;
+}
+
 // Per-instance CCD pass parameters: search radius and whether the instance still needs a
 // pass (an instance whose step fraction was settled by an earlier pass is skipped).
 struct CcdPass {
@@ -355,19 +398,20 @@ __global__ void k_ccd_vt(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vins
                          const uint8_t* __restrict__ ctri, const float* __restrict__ im,
                          const uint32_t* __restrict__ ex_ptr, const uint32_t* __restrict__ ex_list,
                          const unsigned long long* __restrict__ best, const float* __restrict__ pn, int has_static,
-                         uint32_t nv, float dhat, uint32_t max_iter, unsigned int* __restrict__ red,
-                         uint32_t* __restrict__ status) {
+                         uint32_t nv, float dhat, uint32_t max_iter, const float* __restrict__ rv,
+                         unsigned int* __restrict__ red, uint32_t* __restrict__ status) {
   uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= nv) return;
   const uint32_t k = vinst[v];
   if (!((cp.todo >> k) & 1u)) return;
-  float4 lo, hi;
+  float4 lo, hi, plo, phi;
   point_box(x, v, cp.search[k], lo, hi);
+  point_box(x, v, rv[v], plo, phi);
   bool vmov = im[v] > 0.f;
   float side = 2.f;
   float tloc = 1.f;
   uint32_t ncap = 0;
-  bool ok = visit(bv, k, lo, hi, [&](uint32_t t) {
+  bool ok = visit_ccd(bv, k, lo, hi, plo, phi, [&](uint32_t t) {
     uint32_t a = tris[3 * t], b = tris[3 * t + 1], c = tris[3 * t + 2];
     bool tmov = im[a] > 0.f || im[b] > 0.f || im[c] > 0.f;
     if (!tmov && !vmov) return;
@@ -395,18 +439,20 @@ __global__ void k_ccd_vt(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vins
 template <class R>
 __global__ void k_ccd_ee(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
                          const float* __restrict__ dx, const uint32_t* __restrict__ edges, const float* __restrict__ im,
-                         uint32_t ne, uint32_t max_iter, unsigned int* __restrict__ red, uint32_t* __restrict__ status) {
+                         uint32_t ne, uint32_t max_iter, const float* __restrict__ rv, unsigned int* __restrict__ red,
+                         uint32_t* __restrict__ status) {
   uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ne) return;
   uint32_t b0 = edges[2 * j], b1 = edges[2 * j + 1];
   const uint32_t k = vinst[b0];
   if (!((cp.todo >> k) & 1u)) return;
-  float4 lo, hi;
+  float4 lo, hi, plo, phi;
   edge_box(x, b0, b1, cp.search[k], lo, hi);
+  edge_box(x, b0, b1, fmaxf(rv[b0], rv[b1]), plo, phi);
   bool jmov = im[b0] > 0.f || im[b1] > 0.f;
   float tloc = 1.f;
   uint32_t ncap = 0;
-  bool ok = visit(bv, k, lo, hi, [&](uint32_t i) {
+  bool ok = visit_ccd(bv, k, lo, hi, plo, phi, [&](uint32_t i) {
     if (i >= j) return;
     uint32_t a0 = edges[2 * i], a1 = edges[2 * i + 1];
     if (!(jmov || im[a0] > 0.f || im[a1] > 0.f)) return;
@@ -466,6 +512,18 @@ int ccd_step(Scene& s, uint32_t active, float* t_out, uint32_t* cap_hits) {
     uint32_t todo = active;
     for (uint32_t k = 0; k < K; ++k) allowed[k] = std::max(std::min(0.5f * s.char_len[k], max_disp[k]), 1.0e-9f);
     uint32_t iters = std::max<uint32_t>(s.p.ccd_max_iter, 1);
+    // pruning radii and the trees' inflated boxes (the trees were built at this iterate)
+    MG_TRY(s.ccd_rv.reserve(s.nv));
+    MG_TRY(s.ccd_c.reserve(4 * PCG_MAX_INST));
+    MG_CUDA(cudaMemsetAsync(s.ccd_c.p, 0, 16 * PCG_MAX_INST, st));
+    k_ccd_mean<<<ceil_div(s.nv, 256), 256, 0, st>>>(s.dx.p, s.inv_mass.p, s.vinst.p, s.nv, s.ccd_c.p);
+    k_ccd_radius<<<ceil_div(s.nv, 256), 256, 0, st>>>(s.dx.p, s.vinst.p, s.nv, s.ccd_c.p, s.ccd_rv.p);
+    MG_CUDA(cudaGetLastError());
+    for (uint32_t k = 0; k < K; ++k) {
+      MG_TRY(lbvh_refit_inflated(s.tri_bvh[k].get(), s.x.p, s.tris.p + 3 * (size_t)s.inst_tri[k], s.ccd_rv.p, st));
+      MG_TRY(lbvh_refit_inflated(s.edge_bvh[k].get(), s.x.p, s.edge_tris.p + 3 * (size_t)s.inst_edge[k], s.ccd_rv.p,
+                                 st));
+    }
     const BvhSet tv = view_set(s.tri_bvh, s.inst_tri), ev = view_set(s.edge_bvh, s.inst_edge);
     for (int pass = 0; pass < 64 && todo; ++pass) {
       CcdPass cp{};
@@ -477,17 +535,19 @@ int ccd_step(Scene& s, uint32_t active, float* t_out, uint32_t* cap_hits) {
       if (s.mixed) {
         k_ccd_vt<double><<<ceil_div(s.nv, 128), 128, 0, st>>>(
             tv, cp, s.vinst.p, s.x.p, s.dx.p, s.tris.p, s.collider_tri.p, s.inv_mass.p, s.ex_ptr.p, s.ex_list.p,
-            s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.red.p, s.status.p);
+            s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.ccd_rv.p, s.red.p, s.status.p);
         if (s.n_edge)
           k_ccd_ee<double><<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, cp, s.vinst.p, s.x.p, s.dx.p, s.edges.p,
-                                                                   s.inv_mass.p, s.n_edge, iters, s.red.p, s.status.p);
+                                                                   s.inv_mass.p, s.n_edge, iters, s.ccd_rv.p, s.red.p,
+                                                                   s.status.p);
       } else {
         k_ccd_vt<float><<<ceil_div(s.nv, 128), 128, 0, st>>>(
             tv, cp, s.vinst.p, s.x.p, s.dx.p, s.tris.p, s.collider_tri.p, s.inv_mass.p, s.ex_ptr.p, s.ex_list.p,
-            s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.red.p, s.status.p);
+            s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.ccd_rv.p, s.red.p, s.status.p);
         if (s.n_edge)
           k_ccd_ee<float><<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, cp, s.vinst.p, s.x.p, s.dx.p, s.edges.p,
-                                                                  s.inv_mass.p, s.n_edge, iters, s.red.p, s.status.p);
+                                                                  s.inv_mass.p, s.n_edge, iters, s.ccd_rv.p, s.red.p,
+                                                                  s.status.p);
       }
       MG_CUDA(cudaGetLastError());
       MG_CUDA(cudaMemcpyAsync(h.data(), s.red.p, 4 * h.size(), cudaMemcpyDeviceToHost, st));
