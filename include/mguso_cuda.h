@@ -243,6 +243,13 @@ typedef struct {
   const float* colliders;      /* f32[8*ncollider]: kind (0 half-space, 1 sphere), point/center xyz,
                                   normal xyz, radius (Collider, contact.rs:21-31) */
   mguso_params params;
+  /* Optional per-shell-face overrides (NULL: rest shape from the initial positions and the
+   * scene's (shell_mu, shell_lambda), as Scene::build_implicit does). shell_rest: 5 floats per
+   * face, the inverse rest shape (column-major 2x2) and the rest area; shell_stiff: a factor
+   * on (shell_mu, shell_lambda) per face. Used for sewing-pattern rest shapes and for the
+   * parameters of the adjoint. */
+  const float* shell_rest;
+  const float* shell_stiff;
 } mguso_scene_desc;
 
 typedef struct {
@@ -277,6 +284,39 @@ int mguso_step(mguso_scene* s, int nsteps, mguso_step_stats* stats);
 int mguso_batch_create(mguso_ctx* ctx, const mguso_scene_desc* descs, uint32_t n, mguso_scene** out);
 /* Number of instances and their vertex offsets (u32[n + 1]; may be NULL). */
 int mguso_scene_instances(mguso_scene* s, uint32_t* n, uint32_t* vert_offsets);
+
+/* ---- Adjoint of an N-step drape (configuration 4) ------------------------------------- */
+/* Gradients of a loss on the final positions with respect to sewing-pattern parameters, as a
+ * forward/backward pair mirroring torch.autograd.Function (forward(theta) -> x_N,
+ * backward(dL/dx_N) -> dL/dtheta). No counterpart in the reference, which has no
+ * differentiation. theta has 3 npanel + nseam entries:
+ *   [stiff_0 .. stiff_{P-1}, warp_0, weft_0, .., warp_{P-1}, weft_{P-1}, seam_0 .. seam_{S-1}]
+ * stiff_p multiplies (shell_mu, shell_lambda) of panel p's shell faces; a face rests at its
+ * pattern triangle (shell_uv) scaled by weft_p along u and warp_p along v; seam_q multiplies
+ * the stiffness of seam q's stitches. The backward pass solves, per step and in reverse,
+ * H w = a_x + a_v / h with H the exact Hessian of the step at its converged positions
+ * (symmetric, possibly indefinite: no eigenvalue clamps, with the second-derivative terms of
+ * hinges and barriers) by MINRES to a relative residual of 1e-7, preconditioned by the
+ * step's own preconditioner factored from its projected matrix, recomputing the states
+ * between checkpoints taken every `checkpoint_every` steps. A contact stiffness's dependence
+ * on the gap enters H, its dependence on the elastic blocks does not; friction must be 0.
+ * MGUSO_ERR_PCG_CAP when MINRES reaches max(cg_max_iter, 4000) iterations. */
+typedef struct {
+  uint32_t npanel, nseam;
+  const float* shell_uv;       /* 6 per shell face: u0 v0 u1 v1 u2 v2 (pattern coordinates) */
+  const uint8_t* shell_panel;  /* per shell face */
+  const uint8_t* stitch_seam;  /* per stitch */
+} mguso_adjoint_spec;
+typedef struct mguso_adjoint mguso_adjoint;
+int mguso_adjoint_create(mguso_ctx* ctx, const mguso_scene_desc* desc, const mguso_adjoint_spec* spec,
+                         mguso_adjoint** out);
+int mguso_adjoint_destroy(mguso_adjoint* a);
+/* Runs nsteps steps at theta from the description's initial state; x_out f32[3 nv] gets the
+ * final positions, stats (optional) nsteps entries. */
+int mguso_adjoint_forward(mguso_adjoint* a, const double* theta, uint32_t nsteps, uint32_t checkpoint_every,
+                          float* x_out, mguso_step_stats* stats);
+/* dl_dx f32[3 nv] (dL/dx_N) -> dl_dtheta f64[3 npanel + nseam], for the last forward. */
+int mguso_adjoint_backward(mguso_adjoint* a, const float* dl_dx, double* dl_dtheta);
 int mguso_read_positions(mguso_scene* s, float* out);   /* f32[3*nv] host */
 int mguso_write_positions(mguso_scene* s, const float* in);
 int mguso_read_velocities(mguso_scene* s, float* out);

@@ -48,7 +48,7 @@ __global__ void k_inertia(const uint32_t* __restrict__ free_verts, uint32_t n_fr
 // ---- stitches (stitch.rs:57-107 at the stitch's stiffness) ------------------------------
 __global__ void k_stitch(const uint32_t* __restrict__ act, uint32_t n, const uint32_t* __restrict__ sidx,
                          const float* __restrict__ sw, const float* __restrict__ skl, const float* __restrict__ x,
-                         float* __restrict__ cb, float* __restrict__ ge) {
+                         float* __restrict__ cb, float* __restrict__ ge, int exact) {
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   uint32_t e = act[k];
@@ -81,6 +81,12 @@ __global__ void k_stitch(const uint32_t* __restrict__ act, uint32_t n, const uin
   float r = (l - l0) / l;
   float c0 = fmaxf(1.0f - r, 0.f) / l0;
   float c1 = fmaxf(r / l0, 0.f);
+  if (exact) {
+    // the Jacobian of the gradient: no clamp below rest length; past the cap the gradient
+    // is linear in t
+    c1 = r / l0;
+    if (tn > lcap) c0 = 0.f;
+  }
   for (int a = 0; a < 6; ++a) {
     V3<float> ga = nn * swt[a];
     for (int b = 0; b < 6; ++b) {
@@ -100,7 +106,7 @@ __global__ void k_stitch(const uint32_t* __restrict__ act, uint32_t n, const uin
 // ---- stretch springs (spring_block, implicit.rs:3240-3263) --------------------------------
 __global__ void k_spring(const uint32_t* __restrict__ act, uint32_t n, const uint32_t* __restrict__ sv,
                          const float* __restrict__ rest, float k, const float* __restrict__ x, float* __restrict__ cb,
-                         float* __restrict__ ge) {
+                         float* __restrict__ ge, int exact) {
   uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
   uint32_t e = act[q];
@@ -113,7 +119,7 @@ __global__ void k_spring(const uint32_t* __restrict__ act, uint32_t n, const uin
     for (int i = 0; i < 9; ++i) h[i] = (i % 4 == 0) ? k : 0.f;
   } else {
     V3<float> nrm = d / l;
-    float ct = fmaxf(1.0f - rest[e] / l, 0.f);
+    float ct = exact ? 1.0f - rest[e] / l : fmaxf(1.0f - rest[e] / l, 0.f);
     for (int i = 0; i < 3; ++i)
       for (int j = 0; j < 3; ++j) {
         float nnt = nrm[i] * nrm[j];
@@ -138,7 +144,7 @@ __global__ void __launch_bounds__(128) k_shell(const uint32_t* __restrict__ act,
                                                const uint32_t* __restrict__ sv, const float* __restrict__ dm,
                                                const float* __restrict__ area, const float* __restrict__ mu,
                                                const float* __restrict__ lam, float eps, const float* __restrict__ x,
-                                               float* __restrict__ cb, float* __restrict__ ge) {
+                                               float* __restrict__ cb, float* __restrict__ ge, int exact) {
   uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
   uint32_t e = act[q];
@@ -146,7 +152,17 @@ __global__ void __launch_bounds__(128) k_shell(const uint32_t* __restrict__ act,
   M2<float> D{dm[4 * e], dm[4 * e + 1], dm[4 * e + 2], dm[4 * e + 3]};
   V3<float> g[3];
   float h[81];
-  shell_grad_hess<float>(p, D, area[e], mu[e], lam[e], eps, g, h);
+  shell_grad_hess<float>(p, D, area[e], mu[e], lam[e], eps, g, h, !exact);
+  if (exact) {
+    // the exact Hessian in FP64 (its eigenvalue quotients cancel in FP32 when the two
+    // singular values are close)
+    V3<double> pd[3] = {p[0].cast<double>(), p[1].cast<double>(), p[2].cast<double>()};
+    M2<double> Dd{D.xx, D.xy, D.yx, D.yy};
+    V3<double> gd[3];
+    double hd[81];
+    shell_grad_hess<double>(pd, Dd, (double)area[e], (double)mu[e], (double)lam[e], (double)eps, gd, hd, false);
+    for (int k = 0; k < 81; ++k) h[k] = (float)hd[k];
+  }
   float* blk = cb + 81 * (size_t)e;
   for (int a = 0; a < 3; ++a)
     for (int b = 0; b < 3; ++b) put_block(blk + 9 * (3 * a + b), h, 9, 3 * a, 3 * b, 1.0f);
@@ -161,7 +177,7 @@ __global__ void __launch_bounds__(128) k_shell(const uint32_t* __restrict__ act,
 // ---- hinges ----------------------------------------------------------------------------------
 __global__ void k_hinge(const uint32_t* __restrict__ act, uint32_t n, const uint32_t* __restrict__ hv,
                         const float* __restrict__ rest, float kb, const float* __restrict__ x, float* __restrict__ cb,
-                        float* __restrict__ ge) {
+                        float* __restrict__ ge, int exact) {
   uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
   uint32_t e = act[q];
@@ -176,6 +192,35 @@ __global__ void k_hinge(const uint32_t* __restrict__ act, uint32_t n, const uint
   for (int a = 0; a < 4; ++a)
     for (int c = 0; c < 3; ++c) gg[3 * a + c] = kwt * gval * g[a][c];
   float* blk = cb + 144 * (size_t)e;
+  if (exact) {
+    // k (grad theta grad theta^T + (theta - theta0) hess theta), hess theta from FP64
+    // central differences of the angle's gradient
+    V3<double> pd[4], gd[4];
+    for (int a = 0; a < 4; ++a) pd[a] = ld3<double>(x, hv[4 * e + a]);
+    dihedral_grad<double>(pd, gd);
+    const double gv = dihedral_angle<double>(pd) - (double)rest[e];
+    const double eps = 1e-6 * fmax((pd[2] - pd[1]).length(), 1e-3);
+    double H[144];
+    for (int i = 0; i < 12; ++i)
+      for (int j = 0; j < 12; ++j) H[12 * i + j] = gd[i / 3][i % 3] * gd[j / 3][j % 3];
+    for (int i = 0; i < 12; ++i) {
+      V3<double> q[4] = {pd[0], pd[1], pd[2], pd[3]}, gp[4], gm[4];
+      q[i / 3][i % 3] = pd[i / 3][i % 3] + eps;
+      dihedral_grad<double>(q, gp);
+      q[i / 3][i % 3] = pd[i / 3][i % 3] - eps;
+      dihedral_grad<double>(q, gm);
+      for (int j = 0; j < 12; ++j) {
+        const double hij = 0.5 * gv * (gp[j / 3][j % 3] - gm[j / 3][j % 3]) / (2 * eps);
+        H[12 * i + j] += hij;
+        H[12 * j + i] += hij;
+      }
+    }
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b)
+        for (int r = 0; r < 3; ++r)
+          for (int c = 0; c < 3; ++c) blk[9 * (4 * a + b) + 3 * r + c] = (float)(kwt * H[12 * (3 * a + r) + 3 * b + c]);
+    return;
+  }
   for (int a = 0; a < 4; ++a)
     for (int b = 0; b < 4; ++b)
       for (int r = 0; r < 3; ++r)
@@ -232,6 +277,9 @@ int assemble_elastic(Scene& s) {
   auto grid = [](uint32_t n) { return std::max<uint32_t>(ceil_div(n, 128), 1u); };
   float* cb = s.cblocks.p;
   float* ge = s.gentries.p;
+  const int exact_all = s.hess_mode == 2;
+  const int ex_shell = exact_all && (s.exact_terms & EXACT_SHELLS), ex_stitch = exact_all && (s.exact_terms & EXACT_STITCHES);
+  const int ex_hinge = exact_all && (s.exact_terms & EXACT_HINGES), ex_spring = exact_all && (s.exact_terms & EXACT_SPRINGS);
   if (s.n_free)
     k_inertia<<<grid(s.n_free), 128, 0, st>>>(s.free_verts.p, s.n_free, s.inv_mass.p, s.x.p, s.xt.p, inv_h2,
                                             cb + 9 * s.cb_inertia, ge + 3 * s.gb_inertia);
@@ -244,34 +292,34 @@ int assemble_elastic(Scene& s) {
     MG_TRY(all.upload(ids.data(), ids.size(), st));
     if (s.n_stitch)
       k_stitch<<<grid(s.n_stitch), 128, 0, st>>>(all.p, s.n_stitch, s.stitch_idx.p, s.stitch_w.p, s.stitch_kl.p,
-                                                 s.x.p, cb + 9 * s.cb_stitch, ge + 3 * s.gb_stitch);
+                                                 s.x.p, cb + 9 * s.cb_stitch, ge + 3 * s.gb_stitch, ex_stitch);
     if (s.n_spring)
       k_spring<<<grid(s.n_spring), 128, 0, st>>>(all.p, s.n_spring, s.spring_v.p, s.spring_rest.p, s.p.stiffness,
-                                                 s.x.p, cb + 9 * s.cb_spring, ge + 3 * s.gb_spring);
+                                                 s.x.p, cb + 9 * s.cb_spring, ge + 3 * s.gb_spring, ex_spring);
     if (s.n_shell)
       k_shell<<<grid(s.n_shell), 128, 0, st>>>(all.p, s.n_shell, s.shell_v.p, s.shell_dm.p, s.shell_area.p,
                                                s.shell_mu.p, s.shell_lam.p, s.p.eiganalysis_eps, s.x.p,
-                                               cb + 9 * s.cb_shell, ge + 3 * s.gb_shell);
+                                               cb + 9 * s.cb_shell, ge + 3 * s.gb_shell, ex_shell);
     if (s.n_hinge)
       k_hinge<<<grid(s.n_hinge), 128, 0, st>>>(all.p, s.n_hinge, s.hinge_v.p, s.hinge_rest.p, s.p.bend_stiffness,
-                                               s.x.p, cb + 9 * s.cb_hinge, ge + 3 * s.gb_hinge);
+                                               s.x.p, cb + 9 * s.cb_hinge, ge + 3 * s.gb_hinge, ex_hinge);
     MG_CUDA(cudaGetLastError());
     MG_CUDA(cudaStreamSynchronize(st));
     s.static_done = true;
   } else {
     if (s.n_act_stitch)
       k_stitch<<<grid(s.n_act_stitch), 128, 0, st>>>(s.act_stitch.p, s.n_act_stitch, s.stitch_idx.p, s.stitch_w.p,
-                                                     s.stitch_kl.p, s.x.p, cb + 9 * s.cb_stitch, ge + 3 * s.gb_stitch);
+                                                     s.stitch_kl.p, s.x.p, cb + 9 * s.cb_stitch, ge + 3 * s.gb_stitch, ex_stitch);
     if (s.n_act_spring)
       k_spring<<<grid(s.n_act_spring), 128, 0, st>>>(s.act_spring.p, s.n_act_spring, s.spring_v.p, s.spring_rest.p,
-                                                     s.p.stiffness, s.x.p, cb + 9 * s.cb_spring, ge + 3 * s.gb_spring);
+                                                     s.p.stiffness, s.x.p, cb + 9 * s.cb_spring, ge + 3 * s.gb_spring, ex_spring);
     if (s.n_act_shell)
       k_shell<<<grid(s.n_act_shell), 128, 0, st>>>(s.act_shell.p, s.n_act_shell, s.shell_v.p, s.shell_dm.p,
                                                    s.shell_area.p, s.shell_mu.p, s.shell_lam.p, s.p.eiganalysis_eps,
-                                                   s.x.p, cb + 9 * s.cb_shell, ge + 3 * s.gb_shell);
+                                                   s.x.p, cb + 9 * s.cb_shell, ge + 3 * s.gb_shell, ex_shell);
     if (s.n_act_hinge)
       k_hinge<<<grid(s.n_act_hinge), 128, 0, st>>>(s.act_hinge.p, s.n_act_hinge, s.hinge_v.p, s.hinge_rest.p,
-                                                   s.p.bend_stiffness, s.x.p, cb + 9 * s.cb_hinge, ge + 3 * s.gb_hinge);
+                                                   s.p.bend_stiffness, s.x.p, cb + 9 * s.cb_hinge, ge + 3 * s.gb_hinge, ex_hinge);
   }
   MG_CUDA(cudaGetLastError());
   uint32_t nslots = s.Ps.nnz + s.Pp.nnz;
@@ -394,6 +442,47 @@ __device__ __forceinline__ const float* find_block(uint32_t va, uint32_t vb, con
 
 constexpr unsigned long long INVALID_KEY = ~0ull;
 
+// self_contact_rayleigh (implicit.rs:755-795): a stencil's barrier stiffness from the
+// gathered blocks of its participants and their masses (kappa when the normal degenerates).
+// km, when given, receives the masses' part of it, sum m w^2 / d^2 (its only part that
+// depends on the gap d).
+template <class R>
+__device__ inline R stencil_stiffness(const Stencil& S, const V3<R> g[4], const float* __restrict__ im,
+                                      const uint8_t* __restrict__ pinned, const uint32_t* __restrict__ ps_rp,
+                                      const uint32_t* __restrict__ ps_col, const float* __restrict__ vals,
+                                      const uint32_t* __restrict__ pp_rp, const uint32_t* __restrict__ pp_col,
+                                      const float* __restrict__ valp, float kappa, R* km) {
+  const R d = (R)S.d;
+  if (km) *km = R(0);
+  const R nlen = g[0].length();
+  if (nlen < R(1.0e-12)) return (R)kappa;
+  V3<R> nrm = g[0] / nlen;
+  R wts[4], mass[4];
+  R el[16][9];
+  for (int a = 0; a < 4; ++a) {
+    wts[a] = g[a].dot(nrm);
+    R imv = (R)im[S.idx[a]];
+    mass[a] = imv > 0 ? R(1) / imv : R(0);
+  }
+  for (int ia = 0; ia < 4; ++ia)
+    for (int ib = 0; ib < 4; ++ib) {
+      const float* b = find_block(S.idx[ia], S.idx[ib], pinned, ps_rp, ps_col, vals, pp_rp, pp_col, valp);
+      for (int q = 0; q < 9; ++q) el[ia * 4 + ib][q] = b ? (R)b[q] : R(0);
+    }
+  R k = rayleigh_stiffness<R>(el, mass, wts, 4, nrm * d);
+  if (!(k > 0)) return (R)kappa;
+  if (km) {
+    R m_max = 0, ws = 0, acc = 0;
+    for (int a = 0; a < 4; ++a) m_max = rmax(m_max, mass[a]);
+    for (int a = 0; a < 4; ++a) {
+      ws += wts[a] * wts[a];
+      acc += (mass[a] > 0 ? mass[a] : m_max) * wts[a] * wts[a];
+    }
+    *km = ws > 0 ? acc / ws / (d * d) : R(0);
+  }
+  return k;
+}
+
 template <class R>
 __global__ void k_contact_assemble(const Stencil* __restrict__ sts, uint32_t nst, const float* __restrict__ im,
                                    const uint8_t* __restrict__ pinned, const float* __restrict__ x,
@@ -410,28 +499,8 @@ __global__ void k_contact_assemble(const Stencil* __restrict__ sts, uint32_t nst
   V3<R> g[4];
   for (int a = 0; a < 4; ++a) g[a] = V3<R>((R)S.g[3 * a], (R)S.g[3 * a + 1], (R)S.g[3 * a + 2]);
   R d = (R)S.d;
-  // self_contact_rayleigh (implicit.rs:755-795)
-  R k;
+  const R k = stencil_stiffness<R>(S, g, im, pinned, ps_rp, ps_col, vals, pp_rp, pp_col, valp, kappa, (R*)nullptr);
   R nlen = g[0].length();
-  if (nlen < R(1.0e-12)) {
-    k = (R)kappa;
-  } else {
-    V3<R> nrm = g[0] / nlen;
-    R wts[4], mass[4];
-    R el[16][9];
-    for (int a = 0; a < 4; ++a) {
-      wts[a] = g[a].dot(nrm);
-      R imv = (R)im[S.idx[a]];
-      mass[a] = imv > 0 ? R(1) / imv : R(0);
-    }
-    for (int ia = 0; ia < 4; ++ia)
-      for (int ib = 0; ib < 4; ++ib) {
-        const float* b = find_block(S.idx[ia], S.idx[ib], pinned, ps_rp, ps_col, vals, pp_rp, pp_col, valp);
-        for (int q = 0; q < 9; ++q) el[ia * 4 + ib][q] = b ? (R)b[q] : R(0);
-      }
-    k = rayleigh_stiffness<R>(el, mass, wts, 4, nrm * d);
-    if (!(k > 0)) k = (R)kappa;
-  }
   int kind = d < 0 ? 1 : barrier_kind;
   R bg = 0, bh = 0;
   bool active = barrier_of<R>(kind, d, (R)S.ghat, k, bg, bh);
@@ -495,6 +564,126 @@ __global__ void k_contact_assemble(const Stencil* __restrict__ sts, uint32_t nst
     gkeys[id2] = fr ? S.idx[a] : INVALID_KEY;
     gids[id2] = (uint32_t)id2;
   }
+}
+
+// The stencils' stiffnesses and their mass parts, 2 per stencil, as the step's assembly
+// computes them from the gathered (projected) blocks.
+template <class R>
+__global__ void k_contact_stiffness(const Stencil* __restrict__ sts, uint32_t nst, const float* __restrict__ im,
+                                    const uint8_t* __restrict__ pinned, const uint32_t* __restrict__ ps_rp,
+                                    const uint32_t* __restrict__ ps_col, const float* __restrict__ vals,
+                                    const uint32_t* __restrict__ pp_rp, const uint32_t* __restrict__ pp_col,
+                                    const float* __restrict__ valp, float kappa, double* __restrict__ out) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nst) return;
+  const Stencil& S = sts[s];
+  V3<R> g[4];
+  for (int a = 0; a < 4; ++a) g[a] = V3<R>((R)S.g[3 * a], (R)S.g[3 * a + 1], (R)S.g[3 * a + 2]);
+  R km;
+  R k = stencil_stiffness<R>(S, g, im, pinned, ps_rp, ps_col, vals, pp_rp, pp_col, valp, kappa, &km);
+  out[2 * (size_t)s] = (double)k;
+  out[2 * (size_t)s + 1] = (double)km;
+}
+
+// the stencil's gap and its gradient in FP64 at positions p (the signed vertex-triangle
+// gap of a static collider triangle keeps the sign it had, `inside`)
+__device__ inline double stencil_gap(uint32_t kind, bool inside, const V3<double> p[4], double g[12]) {
+  V3<double> gg[4];
+  double d = kind == 0 ? point_tri_distance_grad<double>(p[0], p[1], p[2], p[3], inside, gg)
+                       : segment_segment_distance_grad<double>(p[0], p[1], p[2], p[3], gg);
+  for (int a = 0; a < 4; ++a)
+    for (int c = 0; c < 3; ++c) g[3 * a + c] = gg[a][c];
+  return d;
+}
+
+// The exact Hessian of a stencil's barrier term b'(d; k(d)) grad d with the stiffness
+// recorded by k_contact_stiffness: (b'' + b'/k dk/dd) grad d grad d^T + b' hess d, where
+// dk/dd = -2 km / d (the stiffness's mass part goes as 1/d^2; its elastic part is held
+// fixed) and hess d comes from FP64 central differences of the gap's gradient. Outputs as
+// k_contact_assemble (no friction: the adjoint takes frictionless scenes).
+__global__ void k_contact_exact(const Stencil* __restrict__ sts, uint32_t nst, const uint8_t* __restrict__ pinned,
+                                const float* __restrict__ x, const double* __restrict__ kst, int barrier_kind,
+                                float* __restrict__ ccb, unsigned long long* __restrict__ ckeys,
+                                uint32_t* __restrict__ cids, float* __restrict__ cge,
+                                unsigned long long* __restrict__ gkeys, uint32_t* __restrict__ gids) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nst) return;
+  const Stencil& S = sts[s];
+  const double d = S.d, k = kst[2 * (size_t)s], km = kst[2 * (size_t)s + 1];
+  int kind = d < 0 ? 1 : barrier_kind;
+  double bg = 0, bh = 0;
+  bool active = barrier_of<double>(kind, d, S.ghat, k, bg, bh);
+  double H[144];
+  for (int q = 0; q < 144; ++q) H[q] = 0;
+  if (active) {
+    const double dkdd = d != 0 ? -2.0 * km / d : 0.0;
+    const double coef = bh + bg / k * dkdd;
+    for (int i = 0; i < 12; ++i)
+      for (int j = 0; j < 12; ++j) H[12 * i + j] = coef * S.g[i] * S.g[j];
+    V3<double> p[4];
+    for (int a = 0; a < 4; ++a) p[a] = ld3<double>(x, S.idx[a]);
+    const double eps = fmax(1e-4 * fabs(d), 1e-9);
+    const bool inside = d < 0;
+    for (int i = 0; i < 12; ++i) {
+      double gp[12], gm[12];
+      V3<double> q[4] = {p[0], p[1], p[2], p[3]};
+      q[i / 3][i % 3] = p[i / 3][i % 3] + eps;
+      stencil_gap(S.kind, inside, q, gp);
+      q[i / 3][i % 3] = p[i / 3][i % 3] - eps;
+      stencil_gap(S.kind, inside, q, gm);
+      for (int j = 0; j < 12; ++j) {
+        const double hij = 0.5 * bg * (gp[j] - gm[j]) / (2 * eps);
+        H[12 * i + j] += hij;
+        H[12 * j + i] += hij;
+      }
+    }
+  }
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b) {
+      uint32_t ra = S.idx[a], cbv = S.idx[b];
+      bool keep = !pinned[ra] && !pinned[cbv];
+      size_t id = 32 * (size_t)s + 4 * a + b;
+      float* o = ccb + 9 * id;
+      bool any = false;
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+          float vh = (float)H[12 * (3 * a + r) + 3 * b + c];
+          o[3 * r + c] = vh;
+          any = any || vh != 0.f;
+        }
+      ckeys[id] = (keep && any) ? (((unsigned long long)ra << 32) | cbv) : INVALID_KEY;
+      cids[id] = (uint32_t)id;
+      size_t id2 = id + 16;
+      for (int q = 0; q < 9; ++q) ccb[9 * id2 + q] = 0.f;
+      ckeys[id2] = INVALID_KEY;
+      cids[id2] = (uint32_t)id2;
+    }
+  for (int a = 0; a < 4; ++a) {
+    size_t id = 8 * (size_t)s + a;
+    for (int c = 0; c < 3; ++c) cge[3 * id + c] = active ? (float)(S.g[3 * a + c] * bg) : 0.f;
+    gkeys[id] = active ? S.idx[a] : INVALID_KEY;
+    gids[id] = (uint32_t)id;
+    size_t id2 = id + 4;
+    for (int c = 0; c < 3; ++c) cge[3 * id2 + c] = 0.f;
+    gkeys[id2] = INVALID_KEY;
+    gids[id2] = (uint32_t)id2;
+  }
+}
+
+int contact_stiffness(Scene& s, uint32_t nst) {
+  if (nst == 0) return MGUSO_OK;
+  MG_TRY(s.contact_k.reserve(2 * (size_t)nst));
+  unsigned g = ceil_div(nst, 64);
+  if (s.mixed)
+    k_contact_stiffness<double><<<g, 64, 0, s.st>>>(s.stencils_sorted.p, nst, s.inv_mass.p, s.pinned.p,
+                                                    s.Ps.row_ptr.p, s.Ps.col.p, s.A->val.p, s.Pp.row_ptr.p,
+                                                    s.Pp.col.p, s.valp.p, s.p.contact_kappa, s.contact_k.p);
+  else
+    k_contact_stiffness<float><<<g, 64, 0, s.st>>>(s.stencils_sorted.p, nst, s.inv_mass.p, s.pinned.p,
+                                                   s.Ps.row_ptr.p, s.Ps.col.p, s.A->val.p, s.Pp.row_ptr.p,
+                                                   s.Pp.col.p, s.valp.p, s.p.contact_kappa, s.contact_k.p);
+  MG_CUDA(cudaGetLastError());
+  return MGUSO_OK;
 }
 
 // Segment heads of the sorted block keys: add onto Ps when the block exists there, else
@@ -649,7 +838,10 @@ int assemble_contacts(Scene& s, uint32_t nst) {
   MG_TRY(s.gkeys.reserve(mg_));
   MG_TRY(s.gids.reserve(mg_));
   unsigned g = ceil_div(nst, 64);
-  if (s.mixed)
+  if (s.hess_mode == 2 && (s.exact_terms & EXACT_CONTACTS))
+    k_contact_exact<<<g, 64, 0, st>>>(s.stencils_sorted.p, nst, s.pinned.p, s.x.p, s.contact_k.p, s.p.barrier_kind,
+                                      s.ccblocks.p, s.ckeys.p, s.cids.p, s.cgentries.p, s.gkeys.p, s.gids.p);
+  else if (s.mixed)
     k_contact_assemble<double><<<g, 64, 0, st>>>(s.stencils_sorted.p, nst, s.inv_mass.p, s.pinned.p, s.x.p, s.x0.p,
                                                  s.Ps.row_ptr.p, s.Ps.col.p, s.A->val.p, s.Pp.row_ptr.p, s.Pp.col.p,
                                                  s.valp.p, s.p.contact_kappa, s.p.barrier_kind, s.p.friction,

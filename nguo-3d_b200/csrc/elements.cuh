@@ -432,11 +432,33 @@ __device__ inline void svd3x2(const M32<R>& f, M32<R>& u, R s[2], M2<R>& v) {
   u.c1 = (u1_raw - u0 * u1_raw.dot(u0)).normalize_or(Y);
 }
 
+// StVK shell element gradient alone (shell_model.rs:366-380), as in shell_grad_hess.
+template <class R>
+__device__ inline void shell_grad(const V3<R> p[3], const M2<R>& dm, R area, R mu, R lambda, V3<R> grad[3]) {
+  M32<R> f = M32<R>{p[1] - p[0], p[2] - p[0]}.mul(dm);
+  M32<R> u;
+  R s[2];
+  M2<R> v;
+  svd3x2(f, u, s, v);
+  R j = s[0] * s[1];
+  R s0m = s[0] - R(1), s1m = s[1] - R(1);
+  R deda[2] = {mu * (s0m * (s0m * s0m)) + lambda * s[1] * (j - R(1)),
+               mu * (s1m * (s1m * s1m)) + lambda * s[0] * (j - R(1))};
+  M32<R> pk1 = M32<R>{u.c0 * deda[0], u.c1 * deda[1]}.mul(v.transpose());
+  M32<R> hh = pk1.mul(dm.transpose());
+  V3<R> g1 = hh.c0 * area, g2 = hh.c1 * area;
+  grad[0] = -(g1 + g2);
+  grad[1] = g1;
+  grad[2] = g2;
+}
+
 // StVK shell element: gradient (shell_model.rs:366-380) and eigen-projected Hessian
 // (shell_model.rs:178-290 + :403-438). dm = inverse rest shape (column-major 2x2).
+// project = false keeps the negative eigenvalues: the exact Hessian (the six eigenpairs
+// span the 3x2 deformation gradients).
 template <class R>
 __device__ inline void shell_grad_hess(const V3<R> p[3], const M2<R>& dm, R area, R mu, R lambda, R eps, V3<R> grad[3],
-                                       R* h /*81*/) {
+                                       R* h /*81*/, bool project = true) {
   M32<R> f = M32<R>{p[1] - p[0], p[2] - p[0]}.mul(dm);
   M32<R> u;
   R s[2];
@@ -474,7 +496,7 @@ __device__ inline void shell_grad_hess(const V3<R> p[3], const M2<R>& dm, R area
   for (int k = 0; k < 36; ++k) a6[k] = 0;
   M2<R> vt = v.transpose();
   for (int k = 0; k < 6; ++k) {
-    R l = rmax(lam[k], R(0));
+    R l = project ? rmax(lam[k], R(0)) : lam[k];
     if (l == 0) continue;
     M32<R> uq{u.c0 * qc0[k].x + u.c1 * qc0[k].y + u2 * qc0[k].z, u.c0 * qc1[k].x + u.c1 * qc1[k].y + u2 * qc1[k].z};
     M32<R> m = uq.mul(vt);

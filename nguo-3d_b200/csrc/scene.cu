@@ -182,6 +182,16 @@ int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>
   if (s.p.shell_mu > 0 || s.p.shell_lambda > 0) {
     for (uint32_t f = 0; f < d->nshell; ++f) {
       const uint32_t* fv = d->shell_faces + 3 * f;
+      const float k = d->shell_stiff ? d->shell_stiff[f] : 1.f;
+      if (d->shell_rest) {
+        const float* r = d->shell_rest + 5 * f;
+        shell_v.insert(shell_v.end(), {fv[0], fv[1], fv[2]});
+        shell_dm.insert(shell_dm.end(), {r[0], r[1], r[2], r[3]});
+        shell_area.push_back(r[4]);
+        shell_mu.push_back(s.p.shell_mu * k);
+        shell_lam.push_back(s.p.shell_lambda * k);
+        continue;
+      }
       HV p0 = hp(P, fv[0]), p1 = hp(P, fv[1]), p2 = hp(P, fv[2]);
       HV e1 = p1 - p0, e2 = p2 - p0;
       float area = 0.5f * e1.cross(e2).length();
@@ -195,8 +205,8 @@ int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>
       shell_v.insert(shell_v.end(), {fv[0], fv[1], fv[2]});
       shell_dm.insert(shell_dm.end(), {yy * inv, xy * -inv, yx * -inv, xx * inv});
       shell_area.push_back(area);
-      shell_mu.push_back(s.p.shell_mu);
-      shell_lam.push_back(s.p.shell_lambda);
+      shell_mu.push_back(s.p.shell_mu * k);
+      shell_lam.push_back(s.p.shell_lambda * k);
     }
   }
   s.n_shell = (uint32_t)shell_area.size();
@@ -578,6 +588,7 @@ int mguso_batch_create(mguso_ctx* ctx, const mguso_scene_desc* descs, uint32_t n
     nsh += d.nshell;
     nst += d.nstitch;
     any_mask = any_mask || d.static_mask;
+    MG_CHECK_ARG(!d.shell_rest && !d.shell_stiff, "batch: per-shell overrides are not supported");
   }
   MG_CHECK_ARG(nv < (1u << 30), "batch: too many vertices");
   std::vector<float> pos, vel, im, skl, sw;

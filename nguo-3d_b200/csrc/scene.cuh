@@ -35,6 +35,15 @@ struct BlockPattern {
 
 constexpr uint32_t RED_STRIDE = 16;
 
+enum : uint32_t {
+  EXACT_SHELLS = 1,
+  EXACT_STITCHES = 2,
+  EXACT_HINGES = 4,
+  EXACT_CONTACTS = 8,
+  EXACT_SPRINGS = 16,
+  EXACT_ALL = 31
+};
+
 struct Scene {
   mguso_ctx* ctx = nullptr;
   cudaStream_t st = nullptr;
@@ -66,6 +75,13 @@ struct Scene {
   uint32_t n_act_shell = 0, n_act_hinge = 0, n_act_spring = 0, n_act_stitch = 0;
   DevBuf<uint32_t> act_shell, act_hinge, act_spring, act_stitch;
   bool static_done = false;
+  // Hessians the assembly writes: 0 the step's PSD-projected ones; 2 the exact ones (shells
+  // without the eigenvalue clamp, stitches below rest length, hinges and barriers with their
+  // second-derivative terms), the contact stiffness held at `contact_k` (2 per stencil:
+  // stiffness and its mass part) recorded by contact_stiffness()
+  int hess_mode = 0;
+  uint32_t exact_terms = EXACT_ALL;  // which element kinds mode 2 writes exactly
+  DevBuf<double> contact_k;
 
   // contribution buffers: blocks (9 floats) and gradient entries (3 floats)
   uint64_t cb_inertia = 0, cb_stitch = 0, cb_spring = 0, cb_shell = 0, cb_hinge = 0, n_cblocks = 0;
@@ -165,6 +181,7 @@ int scene_step(Scene& s, mguso_step_stats* out);
 int assemble_elastic(Scene& s);
 int assemble_colliders(Scene& s);
 int assemble_contacts(Scene& s, uint32_t nst);
+int contact_stiffness(Scene& s, uint32_t nst);  // records s.contact_k from the gathered blocks
 int finish_rhs(Scene& s);
 int system_spmv(Scene& s, const float* p, float* ap, cudaStream_t st, const DotSink* d);
 

@@ -8,3 +8,4 @@ operator entry points (BSR SpMV, Schwarz, LBVH). Everything computes on the GPU 
 from ._lib import MgusoError, load  # noqa: F401
 from .linsolve import Bsr, Context, CsrMatrix, CudaLinearSolver, LinearStats, Schwarz  # noqa: F401
 from .solver import ImplicitBatch, ImplicitSolver  # noqa: F401,E402
+from .adjoint import AdjointDrape  # noqa: F401,E402

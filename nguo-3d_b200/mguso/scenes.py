@@ -301,10 +301,12 @@ def sheath_on_torso(width: float = 0.6, height: float = 1.1, edge: float = 8.0e-
     tpos, ttris, _ = torso_mesh(torso_seed, torso_scale, *torso_res)
     y_top = float(tpos[:, 1].max())
     base_y = y_top + 0.01  # the tube hangs 1 cm above the torso and falls onto it
-    panels, tris, seams = [], [], []
+    panels, tris, seams, uvs, panel_of = [], [], [], [], []
     off = 0
     for k in range(2):
         uv, tr, left, right = _panel(width, height, edge, rng)
+        uvs.append(uv)
+        panel_of.append(np.full(tr.shape[0], k, np.uint8))
         th = (uv[:, 0] / width) * np.pi + k * np.pi
         p = np.stack([R * np.cos(th), base_y + uv[:, 1], R * np.sin(th)], 1)
         if k == 1:
@@ -318,12 +320,13 @@ def sheath_on_torso(width: float = 0.6, height: float = 1.1, edge: float = 8.0e-
     ctris = np.concatenate(tris)
     # seams: front left (theta=0) <-> back right (theta=2pi); front right (pi) <-> back left (pi)
     l0 = dhat
-    sidx, sw, skl = [], [], []
-    for a_ids, b_ids in ((seams[0][0], seams[1][1]), (seams[0][1], seams[1][0])):
+    sidx, sw, skl, seam_of = [], [], [], []
+    for si_, (a_ids, b_ids) in enumerate(((seams[0][0], seams[1][1]), (seams[0][1], seams[1][0]))):
         for a, b in zip(a_ids, b_ids):
             sidx.append([a, a, a, b, b, b])
             sw.append([1, 0, 0, 1, 0, 0])
             skl.append([stitch_k * l0, l0, 10.0 * l0])
+            seam_of.append(si_)
     nc = cloth.shape[0]
     pos = np.concatenate([cloth, tpos]).astype(np.float32)
     all_tris = np.concatenate([ctris, ttris.astype(np.int64) + nc]).astype(np.uint32)
@@ -337,6 +340,11 @@ def sheath_on_torso(width: float = 0.6, height: float = 1.1, edge: float = 8.0e-
                 shell_faces=ctris.astype(np.uint32), static_mask=static,
                 stitch_idx=np.array(sidx, np.uint32), stitch_w=np.array(sw, np.float32),
                 stitch_kl=np.array(skl, np.float32), colliders=np.zeros((0, 8), np.float32), params=params,
+                # sewing pattern: panel coordinates of every shell face's corners (u along the
+                # weft / circumference, v along the warp / height), its panel, and each
+                # stitch's seam (0: front-left to back-right, 1: front-right to back-left)
+                shell_uv=np.concatenate(uvs)[ctris].astype(np.float32), shell_panel=np.concatenate(panel_of),
+                stitch_seam=np.array(seam_of, np.uint8),
                 name=f"sheath {ctris.shape[0]} tris on torso {ttris.shape[0]} tris")
 
 

@@ -35,7 +35,8 @@ class SceneDesc(C.Structure):
                 ("inv_mass", C.c_void_p), ("nt", C.c_uint32), ("tris", C.c_void_p), ("static_mask", C.c_void_p),
                 ("nshell", C.c_uint32), ("shell_faces", C.c_void_p), ("nstitch", C.c_uint32),
                 ("stitch_idx", C.c_void_p), ("stitch_w", C.c_void_p), ("stitch_kl", C.c_void_p),
-                ("ncollider", C.c_uint32), ("colliders", C.c_void_p), ("params", Params)]
+                ("ncollider", C.c_uint32), ("colliders", C.c_void_p), ("params", Params),
+                ("shell_rest", C.c_void_p), ("shell_stiff", C.c_void_p)]
 
 
 class StepStats(C.Structure):
@@ -97,6 +98,10 @@ def _desc(scene: dict, precision: str):
     d.ncollider = keep["colliders"].shape[0]
     d.colliders = ptr(keep["colliders"]) if d.ncollider else None
     d.params = make_params(scene["params"], precision)
+    for name in ("shell_rest", "shell_stiff"):
+        if scene.get(name) is not None:
+            keep[name] = np.ascontiguousarray(scene[name], np.float32)
+            setattr(d, name, ptr(keep[name]))
     return d, keep
 
 

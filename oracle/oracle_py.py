@@ -225,6 +225,8 @@ def _step_sigs(lib):
         "oracle_shell": (i32, [i32, vp, vp, C.c_double, C.c_double, C.c_double, vp, vp, vp]),
         "oracle_hinge": (C.c_double, [i32, vp, vp, vp]),
         "oracle_stitch": (None, [vp, vp, C.c_double, C.c_double, vp, vp]),
+        "oracle_solver_set_shells": (None, [vp, C.c_uint32, vp, vp, vp, vp]),
+        "oracle_solver_scale_stitches": (None, [vp, vp]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -310,6 +312,19 @@ class OracleSolver:
     def ccd(self, dx):
         d = np.ascontiguousarray(dx, np.float32)
         return float(self.lib.oracle_solver_ccd(self.h, _p(d)))
+
+    def set_shells(self, faces, rest, mu, lam):
+        """Replace the shells with explicit rest data (inverse rest shape column-major and
+        area per face) and per-face (mu, lambda)."""
+        f = np.ascontiguousarray(faces, np.uint32)
+        r = np.ascontiguousarray(rest, np.float64)
+        m = np.ascontiguousarray(mu, np.float64)
+        l_ = np.ascontiguousarray(lam, np.float64)
+        self.lib.oracle_solver_set_shells(self.h, f.shape[0], _p(f), _p(r), _p(m), _p(l_))
+
+    def scale_stitches(self, factor):
+        f = np.ascontiguousarray(factor, np.float64)
+        self.lib.oracle_solver_scale_stitches(self.h, _p(f))
 
     def close(self):
         if self.h:

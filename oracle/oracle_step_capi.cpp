@@ -154,6 +154,26 @@ int shell_eval(const double* rest9, const double* p9, double mu, double lambda, 
 
 }  // namespace
 
+namespace {
+// Replaces the shell elements with explicit rest data: per face its vertices, the inverse
+// rest shape (column-major 2x2) and area (5 values), and its (mu, lambda).
+template <class R>
+static void set_shells(ImplicitSolver<R>& s, uint32_t n, const uint32_t* faces, const double* rest, const double* mu,
+                       const double* lam) {
+  s.shells.clear();
+  s.shell_k.clear();
+  for (uint32_t f = 0; f < n; ++f) {
+    ShellEl<R> el;
+    for (int k = 0; k < 3; ++k) el.v[k] = faces[3 * f + k];
+    el.dm_inv = Mat2<R>{(R)rest[5 * f], (R)rest[5 * f + 1], (R)rest[5 * f + 2], (R)rest[5 * f + 3]};
+    el.area = (R)rest[5 * f + 4];
+    s.shells.push_back(el);
+    s.shell_k.push_back({(R)mu[f], (R)lam[f]});
+  }
+}
+
+}  // namespace
+
 extern "C" {
 
 void* oracle_solver_new(int precision, uint32_t nv, const float* pos, const float* vel, const float* inv_mass,
@@ -201,6 +221,25 @@ void oracle_solver_state(void* h, double* pos, double* vel) {
         if (vel) vel[3 * i + c] = a->d->velocities[i][c];
       }
     }
+}
+
+// Multiplies every stitch's stiffness by factor[i] (in the solver's precision).
+void oracle_solver_scale_stitches(void* h, const double* factor) {
+  auto* a = (AnySolver*)h;
+  if (a->prec == 0) {
+    for (size_t i = 0; i < a->f->stitches.size(); ++i) a->f->stitches[i].stiffness *= (float)factor[i];
+  } else {
+    for (size_t i = 0; i < a->d->stitches.size(); ++i) a->d->stitches[i].stiffness *= factor[i];
+  }
+}
+
+void oracle_solver_set_shells(void* h, uint32_t n, const uint32_t* faces, const double* rest, const double* mu,
+                              const double* lam) {
+  auto* a = (AnySolver*)h;
+  if (a->prec == 0)
+    set_shells(*a->f, n, faces, rest, mu, lam);
+  else
+    set_shells(*a->d, n, faces, rest, mu, lam);
 }
 
 void oracle_solver_set_state(void* h, const double* pos, const double* vel) {
