@@ -277,8 +277,9 @@ int mguso_step(mguso_scene* s, int nsteps, mguso_step_stats* stats);
  * the n <= 8 descriptions are concatenated, so positions and velocities are read and
  * written as one array with instance k at vertices [offsets[k], offsets[k+1]). Every
  * instance runs its own Newton loop (its own termination, CCD step fraction and PCG
- * convergence); the instances still iterating share each launch, and one persistent PCG
- * launch solves all of them. All descriptions must share params and analytic colliders.
+ * convergence); the instances still iterating share each launch, and each PCG iteration's
+ * kernels cover all of them (pcg_mode 0 or 2). All descriptions must share params and
+ * analytic colliders.
  * mguso_step then writes nsteps * n stats, step-major. No counterpart in the reference,
  * which steps one scene at a time. */
 int mguso_batch_create(mguso_ctx* ctx, const mguso_scene_desc* descs, uint32_t n, mguso_scene** out);
