@@ -11,6 +11,8 @@
 // same 1-ring exclusion, movability filter and shared-vertex rule. Stencils are sorted by
 // (kind, primitive, primitive) to reproduce the reference's sorted, deduplicated order.
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 
 #include "elements.cuh"
 #include "scene.cuh"
@@ -30,12 +32,12 @@ struct BvhView {
   const uint32_t *left, *right, *prim;
   const float4 *node, *leaf;
   uint32_t n;
-  const float4 *cnode, *cleaf;  // CCD-inflated boxes of the same tree (CCD only)
+  const float4 *dnode, *dleaf;  // displacement boxes of the same tree (CCD only)
 };
 
 static BvhView view(const Lbvh& b) {
   return BvhView{b.left.p, b.right.p, b.perm.p, (const float4*)b.node.p, (const float4*)b.leaf.p, b.nt,
-                 (const float4*)b.cnode.p, (const float4*)b.cleaf.p};
+                 (const float4*)b.dnode.p, (const float4*)b.dleaf.p};
 }
 
 // One tree per instance over that instance's primitives (a query only meets its own
@@ -54,14 +56,15 @@ static BvhSet view_set(const std::vector<std::unique_ptr<Lbvh>>& b, const std::v
   return s;
 }
 
-// search box against the exact boxes and pruning box against the inflated ones
+// search box (lo, hi) against the position boxes, the pruning test with the query's own box
+// (qlo, qhi) and displacement ball (cq, rq) against the displacement boxes
 template <class F>
-__device__ __forceinline__ bool visit_ccd(const BvhSet& bs, uint32_t k, float4 lo, float4 hi, float4 plo, float4 phi,
-                                          F&& f) {
+__device__ __forceinline__ bool visit_ccd(const BvhSet& bs, uint32_t k, float4 lo, float4 hi, float4 qlo, float4 qhi,
+                                          float3 cq, float rq, F&& f) {
   const BvhView& bv = bs.t[k];
   const uint32_t base = bs.base[k];
-  return lbvh_visit2(bv.left, bv.right, bv.node, bv.leaf, bv.cnode, bv.cleaf, bv.prim, bv.n, lo, hi, plo, phi,
-                     [&](uint32_t local) { f(base + local); });
+  return lbvh_visit_ccd(bv.left, bv.right, bv.node, bv.leaf, bv.dnode, bv.dleaf, bv.prim, bv.n, lo, hi, qlo, qhi, cq,
+                        rq, [&](uint32_t local) { f(base + local); });
 }
 
 template <class F>
@@ -354,36 +357,9 @@ __global__ void k_ccd_colliders(const uint32_t* __restrict__ free_verts, uint32_
   if (t < 1.f) atomic_min_pos(red + RED_STRIDE * vinst[i] + 1, t);
 }
 
-// CCD candidate pruning. accd_toi (contact.rs:378-437) returns max_t at its first test
-// whenever max_t * u_max < 0.98 d0, where u_max is the largest relative displacement of the
-// four points and d0 their distance: such a pair cannot lower the step fraction. For any
-// common vector c, u_max <= 2 max_i |dx_i - c|, so with per-vertex radii r_v = 2.6 |dx_v - c|
-// (2% above 1.25 / 0.98 x 2) a pair whose query box (radius r_v) misses its primitive's box
-// grown by the primitive's largest radius is exactly such a pair, and is skipped. c is the
-// instance's mean displacement of free vertices, so a cloth falling as a whole prunes almost
-// everything. Traversal enters a subtree only if the reference's search box overlaps its exact
-// box and the pruning box overlaps its inflated box.
-__global__ void k_ccd_mean(const float* __restrict__ dx, const float* __restrict__ im,
-                           const uint8_t* __restrict__ vinst, uint32_t nv, float* __restrict__ acc) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nv || !(im[i] > 0.f)) return;
-  float* a = acc + 4 * vinst[i];
-  atomicAdd(a, dx[3 * i]);
-  atomicAdd(a + 1, dx[3 * i + 1]);
-  atomicAdd(a + 2, dx[3 * i + 2]);
-  atomicAdd(a + 3, 1.f);
-}
-
-__global__ void k_ccd_radius(const float* __restrict__ dx, const uint8_t* __restrict__ vinst, uint32_t nv,
-                             const float* __restrict__ acc, float* __restrict__ rv) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nv) return;
-  const float* a = acc + 4 * vinst[i];
-  const float n = fmaxf(a[3], 1.f);
-  const float cx = a[0] / n, cy = a[1] / n, cz = a[2] / n;
-  const float ex = dx[3 * i] - cx, ey = dx[3 * i + 1] - cy, ez = dx[3 * i + 2] - cz;
-  rv[i] = 2.6f * sqrtf(ex * ex + ey * ey + ez * ez) + 1.0e-9f;
-}
+// CCD candidate pruning: a pair whose accd_toi (contact.rs:378-437) would return max_t at
+// its first test cannot lower the step fraction, and traversal skips whole subtrees of such
+// pairs (lbvh_visit_ccd) from the primitives' displacement boxes, refitted per CCD call.
 
 // Per-instance CCD pass parameters: search radius and whether the instance still needs a
 // pass (an instance whose step fraction was settled by an earlier pass is skipped).
@@ -398,20 +374,22 @@ __global__ void k_ccd_vt(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vins
                          const uint8_t* __restrict__ ctri, const float* __restrict__ im,
                          const uint32_t* __restrict__ ex_ptr, const uint32_t* __restrict__ ex_list,
                          const unsigned long long* __restrict__ best, const float* __restrict__ pn, int has_static,
-                         uint32_t nv, float dhat, uint32_t max_iter, const float* __restrict__ rv,
-                         unsigned int* __restrict__ red, uint32_t* __restrict__ status) {
+                         uint32_t nv, float dhat, uint32_t max_iter, unsigned int* __restrict__ red,
+                         uint32_t* __restrict__ status) {
   uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= nv) return;
   const uint32_t k = vinst[v];
   if (!((cp.todo >> k) & 1u)) return;
-  float4 lo, hi, plo, phi;
+  float4 lo, hi, qlo, qhi;
   point_box(x, v, cp.search[k], lo, hi);
-  point_box(x, v, rv[v], plo, phi);
+  point_box(x, v, 0.f, qlo, qhi);
+  const float3 cq = make_float3(dx[3 * v], dx[3 * v + 1], dx[3 * v + 2]);
   bool vmov = im[v] > 0.f;
   float side = 2.f;
   float tloc = 1.f;
-  uint32_t ncap = 0;
-  bool ok = visit_ccd(bv, k, lo, hi, plo, phi, [&](uint32_t t) {
+  uint32_t ncap = 0, nleaf = 0, nacc = 0;
+  bool ok = visit_ccd(bv, k, lo, hi, qlo, qhi, cq, 0.f, [&](uint32_t t) {
+    ++nleaf;
     uint32_t a = tris[3 * t], b = tris[3 * t + 1], c = tris[3 * t + 2];
     bool tmov = im[a] > 0.f || im[b] > 0.f || im[c] > 0.f;
     if (!tmov && !vmov) return;
@@ -427,6 +405,7 @@ __global__ void k_ccd_vt(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vins
       dd[q] = ld3<R>(dx, idx[q]);
     }
     bool cap = false;
+    ++nacc;
     R toi = accd_toi<R>(x0, dd, R(0), R(1.25), R(0.01), max_iter, 0, &cap);
     ncap += cap ? 1u : 0u;
     tloc = fminf(tloc, (float)(toi / R(1.25)));
@@ -434,25 +413,34 @@ __global__ void k_ccd_vt(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vins
   if (!ok) atomicOr(status, ST_STACK_OVERFLOW);
   if (tloc < 1.f) atomic_min_pos(red + RED_STRIDE * k + 2, tloc);
   if (ncap) atomicAdd(red + RED_STRIDE * k + 3, ncap);
+  if (nleaf) atomicAdd(red + RED_STRIDE * k + 5, nleaf);
+  if (nacc) atomicAdd(red + RED_STRIDE * k + 6, nacc);
 }
 
 template <class R>
 __global__ void k_ccd_ee(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
                          const float* __restrict__ dx, const uint32_t* __restrict__ edges, const float* __restrict__ im,
-                         uint32_t ne, uint32_t max_iter, const float* __restrict__ rv, unsigned int* __restrict__ red,
+                         uint32_t ne, uint32_t max_iter, unsigned int* __restrict__ red,
                          uint32_t* __restrict__ status) {
   uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ne) return;
   uint32_t b0 = edges[2 * j], b1 = edges[2 * j + 1];
   const uint32_t k = vinst[b0];
   if (!((cp.todo >> k) & 1u)) return;
-  float4 lo, hi, plo, phi;
+  float4 lo, hi, qlo, qhi;
   edge_box(x, b0, b1, cp.search[k], lo, hi);
-  edge_box(x, b0, b1, fmaxf(rv[b0], rv[b1]), plo, phi);
+  edge_box(x, b0, b1, 0.f, qlo, qhi);
+  // the query edge's displacements lie in the ball around their midpoint
+  const float3 d0 = make_float3(dx[3 * b0], dx[3 * b0 + 1], dx[3 * b0 + 2]);
+  const float3 d1 = make_float3(dx[3 * b1], dx[3 * b1 + 1], dx[3 * b1 + 2]);
+  const float3 cq = make_float3(0.5f * (d0.x + d1.x), 0.5f * (d0.y + d1.y), 0.5f * (d0.z + d1.z));
+  const float ex = d1.x - d0.x, ey = d1.y - d0.y, ez = d1.z - d0.z;
+  const float rq = 0.5f * sqrtf(ex * ex + ey * ey + ez * ez) * 1.0001f;
   bool jmov = im[b0] > 0.f || im[b1] > 0.f;
   float tloc = 1.f;
-  uint32_t ncap = 0;
-  bool ok = visit_ccd(bv, k, lo, hi, plo, phi, [&](uint32_t i) {
+  uint32_t ncap = 0, nleaf = 0, nacc = 0;
+  bool ok = visit_ccd(bv, k, lo, hi, qlo, qhi, cq, rq, [&](uint32_t i) {
+    ++nleaf;
     if (i >= j) return;
     uint32_t a0 = edges[2 * i], a1 = edges[2 * i + 1];
     if (!(jmov || im[a0] > 0.f || im[a1] > 0.f)) return;
@@ -464,6 +452,7 @@ __global__ void k_ccd_ee(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vins
       dd[q] = ld3<R>(dx, idx[q]);
     }
     bool cap = false;
+    ++nacc;
     R toi = accd_toi<R>(x0, dd, R(0), R(1.25), R(0.01), max_iter, 1, &cap);
     ncap += cap ? 1u : 0u;
     tloc = fminf(tloc, (float)(toi / R(1.25)));
@@ -471,6 +460,8 @@ __global__ void k_ccd_ee(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vins
   if (!ok) atomicOr(status, ST_STACK_OVERFLOW);
   if (tloc < 1.f) atomic_min_pos(red + RED_STRIDE * k + 2, tloc);
   if (ncap) atomicAdd(red + RED_STRIDE * k + 3, ncap);
+  if (nleaf) atomicAdd(red + RED_STRIDE * k + 7, nleaf);
+  if (nacc) atomicAdd(red + RED_STRIDE * k + 8, nacc);
 }
 
 // ccd_max_step (implicit.rs:1690-1947) without strain limiting or pins, per instance. The
@@ -512,20 +503,18 @@ int ccd_step(Scene& s, uint32_t active, float* t_out, uint32_t* cap_hits) {
     uint32_t todo = active;
     for (uint32_t k = 0; k < K; ++k) allowed[k] = std::max(std::min(0.5f * s.char_len[k], max_disp[k]), 1.0e-9f);
     uint32_t iters = std::max<uint32_t>(s.p.ccd_max_iter, 1);
-    // pruning radii and the trees' inflated boxes (the trees were built at this iterate)
-    MG_TRY(s.ccd_rv.reserve(s.nv));
-    MG_TRY(s.ccd_c.reserve(4 * PCG_MAX_INST));
-    MG_CUDA(cudaMemsetAsync(s.ccd_c.p, 0, 16 * PCG_MAX_INST, st));
-    k_ccd_mean<<<ceil_div(s.nv, 256), 256, 0, st>>>(s.dx.p, s.inv_mass.p, s.vinst.p, s.nv, s.ccd_c.p);
-    k_ccd_radius<<<ceil_div(s.nv, 256), 256, 0, st>>>(s.dx.p, s.vinst.p, s.nv, s.ccd_c.p, s.ccd_rv.p);
-    MG_CUDA(cudaGetLastError());
+    // the trees' displacement boxes (the trees were built at this iterate)
     for (uint32_t k = 0; k < K; ++k) {
-      MG_TRY(lbvh_refit_inflated(s.tri_bvh[k].get(), s.x.p, s.tris.p + 3 * (size_t)s.inst_tri[k], s.ccd_rv.p, st));
-      MG_TRY(lbvh_refit_inflated(s.edge_bvh[k].get(), s.x.p, s.edge_tris.p + 3 * (size_t)s.inst_edge[k], s.ccd_rv.p,
-                                 st));
+      MG_TRY(lbvh_refit_disp(s.tri_bvh[k].get(), s.dx.p, s.tris.p + 3 * (size_t)s.inst_tri[k], st));
+      MG_TRY(lbvh_refit_disp(s.edge_bvh[k].get(), s.dx.p, s.edge_tris.p + 3 * (size_t)s.inst_edge[k], st));
     }
     const BvhSet tv = view_set(s.tri_bvh, s.inst_tri), ev = view_set(s.edge_bvh, s.inst_edge);
+    static const bool trace = std::getenv("MGUSO_TRACE") && std::getenv("MGUSO_TRACE")[0] == '2';
+    cudaEvent_t ev3[3];
+    if (trace)
+      for (auto& e : ev3) MG_CUDA(cudaEventCreate(&e));
     for (int pass = 0; pass < 64 && todo; ++pass) {
+      if (trace) MG_CUDA(cudaEventRecord(ev3[0], st));
       CcdPass cp{};
       cp.todo = todo;
       for (uint32_t k = 0; k < K; ++k) {
@@ -535,23 +524,40 @@ int ccd_step(Scene& s, uint32_t active, float* t_out, uint32_t* cap_hits) {
       if (s.mixed) {
         k_ccd_vt<double><<<ceil_div(s.nv, 128), 128, 0, st>>>(
             tv, cp, s.vinst.p, s.x.p, s.dx.p, s.tris.p, s.collider_tri.p, s.inv_mass.p, s.ex_ptr.p, s.ex_list.p,
-            s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.ccd_rv.p, s.red.p, s.status.p);
+            s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.red.p, s.status.p);
+        if (trace) MG_CUDA(cudaEventRecord(ev3[1], st));
         if (s.n_edge)
           k_ccd_ee<double><<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, cp, s.vinst.p, s.x.p, s.dx.p, s.edges.p,
-                                                                   s.inv_mass.p, s.n_edge, iters, s.ccd_rv.p, s.red.p,
+                                                                   s.inv_mass.p, s.n_edge, iters, s.red.p,
                                                                    s.status.p);
       } else {
         k_ccd_vt<float><<<ceil_div(s.nv, 128), 128, 0, st>>>(
             tv, cp, s.vinst.p, s.x.p, s.dx.p, s.tris.p, s.collider_tri.p, s.inv_mass.p, s.ex_ptr.p, s.ex_list.p,
-            s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.ccd_rv.p, s.red.p, s.status.p);
+            s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.red.p, s.status.p);
+        if (trace) MG_CUDA(cudaEventRecord(ev3[1], st));
         if (s.n_edge)
           k_ccd_ee<float><<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, cp, s.vinst.p, s.x.p, s.dx.p, s.edges.p,
-                                                                  s.inv_mass.p, s.n_edge, iters, s.ccd_rv.p, s.red.p,
+                                                                  s.inv_mass.p, s.n_edge, iters, s.red.p,
                                                                   s.status.p);
       }
       MG_CUDA(cudaGetLastError());
+      if (trace) MG_CUDA(cudaEventRecord(ev3[2], st));
       MG_CUDA(cudaMemcpyAsync(h.data(), s.red.p, 4 * h.size(), cudaMemcpyDeviceToHost, st));
       MG_CUDA(cudaStreamSynchronize(st));
+      if (trace) {
+        float ms_all = 0, ms_vt = 0;
+        MG_CUDA(cudaEventElapsedTime(&ms_all, ev3[0], ev3[2]));
+        MG_CUDA(cudaEventElapsedTime(&ms_vt, ev3[0], ev3[1]));
+        unsigned long long lv = 0, av = 0, le = 0, ae = 0;
+        for (uint32_t k = 0; k < K; ++k) {
+          lv += h[RED_STRIDE * k + 5];
+          av += h[RED_STRIDE * k + 6];
+          le += h[RED_STRIDE * k + 7];
+          ae += h[RED_STRIDE * k + 8];
+        }
+        fprintf(stderr, "[mguso]   ccd pass %d todo %x: vt %.3f ms (leaves %llu, accd %llu), ee %.3f ms (leaves %llu, accd %llu)\n",
+                pass, todo, ms_vt, lv, av, ms_all - ms_vt, le, ae);
+      }
       for (uint32_t k = 0; k < K; ++k) {
         if (!((todo >> k) & 1u)) continue;
         const bool full = allowed[k] >= max_disp[k];
@@ -565,6 +571,8 @@ int ccd_step(Scene& s, uint32_t active, float* t_out, uint32_t* cap_hits) {
         }
       }
     }
+    if (trace)
+      for (auto& e : ev3) cudaEventDestroy(e);
   }
   for (uint32_t k = 0; k < K; ++k) t_out[k] = std::min(std::max(t_out[k], 0.f), 1.f);
   return MGUSO_OK;

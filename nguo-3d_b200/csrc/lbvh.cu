@@ -359,19 +359,18 @@ __global__ void k_leaf_boxes(const float* __restrict__ pos, const uint32_t* __re
   leaf[2 * i + 1] = make_float4(hi[0], hi[1], hi[2], 0.f);
 }
 
-__global__ void k_leaf_boxes_inflated(const float* __restrict__ pos, const uint32_t* __restrict__ tris,
-                                      const uint32_t* __restrict__ perm, uint32_t nt, const float* __restrict__ rv,
-                                      float4* __restrict__ leaf) {
+// Displacement boxes: per leaf, the AABB of the primitive's vertices' displacements dx.
+__global__ void k_leaf_disp_boxes(const float* __restrict__ dx, const uint32_t* __restrict__ tris,
+                                  const uint32_t* __restrict__ perm, uint32_t nt, float4* __restrict__ leaf) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nt) return;
   uint32_t t = perm[i];
   const uint32_t v0 = tris[3 * t], v1 = tris[3 * t + 1], v2 = tris[3 * t + 2];
-  const float r = fmaxf(fmaxf(rv[v0], rv[v1]), rv[v2]);
   float lo[3], hi[3];
   for (int c = 0; c < 3; ++c) {
-    float a = pos[3 * v0 + c], b = pos[3 * v1 + c], d = pos[3 * v2 + c];
-    lo[c] = fminf(fminf(a, b), d) - r;
-    hi[c] = fmaxf(fmaxf(a, b), d) + r;
+    float a = dx[3 * v0 + c], b = dx[3 * v1 + c], d = dx[3 * v2 + c];
+    lo[c] = fminf(fminf(a, b), d);
+    hi[c] = fmaxf(fmaxf(a, b), d);
   }
   leaf[2 * i] = make_float4(lo[0], lo[1], lo[2], 0.f);
   leaf[2 * i + 1] = make_float4(hi[0], hi[1], hi[2], 0.f);
@@ -577,16 +576,16 @@ static int build_impl(Lbvh* b, const float* pos, const uint32_t* tris, uint32_t 
   return MGUSO_OK;
 }
 
-int lbvh_refit_inflated(Lbvh* b, const float* pos, const uint32_t* tris, const float* rv, cudaStream_t s) {
+int lbvh_refit_disp(Lbvh* b, const float* dx, const uint32_t* tris, cudaStream_t s) {
   const uint32_t nt = b->nt;
-  MG_TRY(b->cleaf.reserve(2 * (size_t)std::max<uint32_t>(nt, 1)));
-  MG_TRY(b->cnode.reserve(2 * (size_t)std::max<uint32_t>(nt, 2)));
+  MG_TRY(b->dleaf.reserve(2 * (size_t)std::max<uint32_t>(nt, 1)));
+  MG_TRY(b->dnode.reserve(2 * (size_t)std::max<uint32_t>(nt, 2)));
   if (nt == 0) return MGUSO_OK;
-  k_leaf_boxes_inflated<<<ceil_div(nt, 256), 256, 0, s>>>(pos, tris, b->perm.p, nt, rv, b->cleaf.p);
+  k_leaf_disp_boxes<<<ceil_div(nt, 256), 256, 0, s>>>(dx, tris, b->perm.p, nt, b->dleaf.p);
   if (nt > 1) {
     MG_CUDA(cudaMemsetAsync(b->flags.p, 0, 4 * (size_t)(nt - 1), s));
-    k_refit<<<ceil_div(nt, 256), 256, 0, s>>>(b->parent_leaf.p, b->parent_int.p, b->left.p, b->right.p, b->cleaf.p,
-                                             b->cnode.p, b->flags.p, nt);
+    k_refit<<<ceil_div(nt, 256), 256, 0, s>>>(b->parent_leaf.p, b->parent_int.p, b->left.p, b->right.p, b->dleaf.p,
+                                             b->dnode.p, b->flags.p, nt);
   }
   MG_CUDA(cudaGetLastError());
   return MGUSO_OK;

@@ -16,7 +16,7 @@ struct Lbvh {
   DevBuf<uint32_t> left, right;     // nt - 1 internal nodes
   DevBuf<uint32_t> parent_int, parent_leaf;
   DevBuf<float4> leaf, node;        // 2 float4 per box (lo, hi)
-  DevBuf<float4> cleaf, cnode;      // boxes inflated per primitive (CCD pruning), same tree
+  DevBuf<float4> dleaf, dnode;      // displacement boxes of the same tree (CCD pruning)
   DevBuf<uint32_t> flags;
   DevBuf<float> params;             // centroid lo.xyz, inv.xyz
   DevBuf<uint32_t> ord;
@@ -37,9 +37,9 @@ struct Lbvh {
 int radix_sort_pairs(Lbvh* b, void* keys, uint32_t* vals, uint32_t n, int key_bits, cudaStream_t s);
 int lbvh_build(Lbvh* b, const float* pos, uint32_t nv, const uint32_t* tris, uint32_t nt, int key_bits,
                cudaStream_t s);
-// Refits the built tree with every leaf box grown by the largest radius rv[] of its
-// primitive's vertices (tris as passed to lbvh_build), into cleaf/cnode.
-int lbvh_refit_inflated(Lbvh* b, const float* pos, const uint32_t* tris, const float* rv, cudaStream_t s);
+// Displacement boxes (AABB of dx over each primitive's vertices, refitted up the tree) into
+// dleaf/dnode, for the CCD's pruning test.
+int lbvh_refit_disp(Lbvh* b, const float* dx, const uint32_t* tris, cudaStream_t s);
 int lbvh_query_boxes(Lbvh* b, const float4* qbox, const uint32_t* qorder, uint32_t nq, uint32_t* pairs, uint64_t cap,
                      unsigned long long* count, cudaStream_t s);
 int lbvh_query_points(Lbvh* b, const float* pts, uint32_t np, float dhat, uint32_t* pairs, uint64_t cap,
@@ -106,27 +106,43 @@ __device__ __forceinline__ bool lbvh_visit(const uint32_t* __restrict__ left, co
   return ok;
 }
 
-// As lbvh_visit, but a subtree is entered only if query box 1 overlaps its box in (node,
-// leaf) AND query box 2 overlaps its box in (node2, leaf2): two conservative tests over the
-// same tree, intersected.
+// CCD traversal (ccd_max_step's broad phase, implicit.rs:1690-1947, with exact pruning).
+// A subtree is entered when the search box overlaps its position box (node, leaf) and its
+// pairs with the query are not all settled by accd_toi's first test (contact.rs:378-437),
+// which returns max_t = 1.25 whenever 1.25 u_max < 0.98 d0 (u_max: the largest relative
+// displacement of the pair's four points; d0: their distance). Over a subtree, with the
+// query's displacements inside the ball (cq, rq) and the subtree's inside its displacement
+// box D (dnode, dleaf): u_max <= 2 max(rq, farthest(cq, D)), and d0 >= the distance between
+// the query's box (qlo, qhi) and the subtree's position box. The subtree is skipped when
+// 2.6 max(rq, farthest) < 0.98 distance (4% margin over 2 x 1.25 for rounding).
 template <class F>
-__device__ __forceinline__ bool lbvh_visit2(const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
-                                            const float4* __restrict__ node, const float4* __restrict__ leaf,
-                                            const float4* __restrict__ node2, const float4* __restrict__ leaf2,
-                                            const uint32_t* __restrict__ prim, uint32_t nt, float4 q1lo, float4 q1hi,
-                                            float4 q2lo, float4 q2hi, F&& f) {
-  auto ov = [](const float4& qlo, const float4& qhi, const float4& lo, const float4& hi) {
-    return qlo.x <= hi.x && qlo.y <= hi.y && qlo.z <= hi.z && lo.x <= qhi.x && lo.y <= qhi.y && lo.z <= qhi.z;
-  };
-  auto both = [&](const float4* b1, const float4* b2) {
-    return ov(q1lo, q1hi, __ldg(b1), __ldg(b1 + 1)) && ov(q2lo, q2hi, __ldg(b2), __ldg(b2 + 1));
+__device__ __forceinline__ bool lbvh_visit_ccd(const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
+                                               const float4* __restrict__ node, const float4* __restrict__ leaf,
+                                               const float4* __restrict__ dnode, const float4* __restrict__ dleaf,
+                                               const uint32_t* __restrict__ prim, uint32_t nt, float4 slo, float4 shi,
+                                               float4 qlo, float4 qhi, float3 cq, float rq, F&& f) {
+  auto enter = [&](const float4* pb, const float4* db) {
+    const float4 lo = __ldg(pb), hi = __ldg(pb + 1);
+    if (!(slo.x <= hi.x && slo.y <= hi.y && slo.z <= hi.z && lo.x <= shi.x && lo.y <= shi.y && lo.z <= shi.z))
+      return false;
+    const float gx = fmaxf(fmaxf(qlo.x - hi.x, lo.x - qhi.x), 0.f);
+    const float gy = fmaxf(fmaxf(qlo.y - hi.y, lo.y - qhi.y), 0.f);
+    const float gz = fmaxf(fmaxf(qlo.z - hi.z, lo.z - qhi.z), 0.f);
+    const float gap2 = gx * gx + gy * gy + gz * gz;
+    if (gap2 == 0.f) return true;
+    const float4 dlo = __ldg(db), dhi = __ldg(db + 1);
+    const float fx = fmaxf(fabsf(cq.x - dlo.x), fabsf(cq.x - dhi.x));
+    const float fy = fmaxf(fabsf(cq.y - dlo.y), fabsf(cq.y - dhi.y));
+    const float fz = fmaxf(fabsf(cq.z - dlo.z), fabsf(cq.z - dhi.z));
+    const float far = fmaxf(sqrtf(fx * fx + fy * fy + fz * fz), rq);
+    return !(2.6f * far < 0.98f * sqrtf(gap2));
   };
   if (nt == 0) return true;
   if (nt == 1) {
-    if (both(leaf, leaf2)) f(prim[0]);
+    if (enter(leaf, dleaf)) f(prim[0]);
     return true;
   }
-  if (!both(node, node2)) return true;
+  if (!enter(node, dnode)) return true;
   uint32_t stack[64];
   int sp = 0;
   uint32_t cur = 0;
@@ -139,7 +155,7 @@ __device__ __forceinline__ bool lbvh_visit2(const uint32_t* __restrict__ left, c
       uint32_t x = ch[c];
       const bool lf = (x & 0x80000000u) != 0;
       const uint32_t i = x & 0x7fffffffu;
-      if (!(lf ? both(leaf + 2 * i, leaf2 + 2 * i) : both(node + 2 * i, node2 + 2 * i))) continue;
+      if (!(lf ? enter(leaf + 2 * i, dleaf + 2 * i) : enter(node + 2 * i, dnode + 2 * i))) continue;
       if (lf) {
         f(prim[i]);
       } else if (next == 0xffffffffu) {

@@ -118,7 +118,6 @@ struct Scene {
   std::vector<float> char_len;                           // per instance
   std::vector<std::unique_ptr<Lbvh>> tri_bvh, edge_bvh;  // per instance
   Lbvh sorter;                                           // radix-sort scratch
-  DevBuf<float> ccd_rv, ccd_c;                           // CCD pruning radii, mean displacements
 
   // self-contact working set
   uint32_t cap_pairs = 0, cap_stencils = 0;
