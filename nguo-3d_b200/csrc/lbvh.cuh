@@ -112,9 +112,11 @@ __device__ __forceinline__ bool lbvh_visit(const uint32_t* __restrict__ left, co
 // which returns max_t = 1.25 whenever 1.25 u_max < 0.98 d0 (u_max: the largest relative
 // displacement of the pair's four points; d0: their distance). Over a subtree, with the
 // query's displacements inside the ball (cq, rq) and the subtree's inside its displacement
-// box D (dnode, dleaf): u_max <= 2 max(rq, farthest(cq, D)), and d0 >= the distance between
-// the query's box (qlo, qhi) and the subtree's position box. The subtree is skipped when
-// 2.6 max(rq, farthest) < 0.98 distance (4% margin over 2 x 1.25 for rounding).
+// box D (dnode, dleaf), the pairs' relative displacements are bounded by 2 rq (within the
+// query), the diagonal of D (within a primitive) and rq + farthest(cq, D) (across), so
+// u_max <= max(2 rq, diag D, rq + farthest(cq, D)); and d0 >= the distance between the
+// query's box (qlo, qhi) and the subtree's position box. The subtree is skipped when
+// 1.3 u_bound < 0.98 distance (4% margin over 1.25 for rounding).
 template <class F>
 __device__ __forceinline__ bool lbvh_visit_ccd(const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
                                                const float4* __restrict__ node, const float4* __restrict__ leaf,
@@ -134,8 +136,9 @@ __device__ __forceinline__ bool lbvh_visit_ccd(const uint32_t* __restrict__ left
     const float fx = fmaxf(fabsf(cq.x - dlo.x), fabsf(cq.x - dhi.x));
     const float fy = fmaxf(fabsf(cq.y - dlo.y), fabsf(cq.y - dhi.y));
     const float fz = fmaxf(fabsf(cq.z - dlo.z), fabsf(cq.z - dhi.z));
-    const float far = fmaxf(sqrtf(fx * fx + fy * fy + fz * fz), rq);
-    return !(2.6f * far < 0.98f * sqrtf(gap2));
+    const float ex = dhi.x - dlo.x, ey = dhi.y - dlo.y, ez = dhi.z - dlo.z;
+    const float u = fmaxf(fmaxf(2.f * rq, sqrtf(ex * ex + ey * ey + ez * ez)), rq + sqrtf(fx * fx + fy * fy + fz * fz));
+    return !(1.3f * u < 0.98f * sqrtf(gap2));
   };
   if (nt == 0) return true;
   if (nt == 1) {
