@@ -173,7 +173,7 @@ int mguso_schwarz_destroy(mguso_schwarz* s) {
 int mguso_schwarz_info(const mguso_schwarz* s, uint32_t* ndomains, uint64_t* factor_bytes) {
   MG_CHECK_ARG(s, "null schwarz");
   if (ndomains) *ndomains = s->ndom;
-  if (factor_bytes) *factor_bytes = 4 * s->fac_floats;
+  if (factor_bytes) *factor_bytes = (s->half ? 2 : 4) * s->fac_floats;
   return MGUSO_OK;
 }
 

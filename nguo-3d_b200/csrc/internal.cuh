@@ -3,6 +3,8 @@
 #include <memory>
 #include <vector>
 
+#include <cuda_fp16.h>
+
 #include "common.cuh"
 
 namespace mg {
@@ -79,7 +81,12 @@ struct mguso_schwarz {
   mg::DevBuf<uint32_t> loc;        // nb: local index of a vertex inside its domain
   mg::DevBuf<uint64_t> fac_off;    // ndom + 1 (float offsets, 4-float aligned)
   mg::DevBuf<float> fac;           // W = L^-1 per domain, swizzled 32x32 FP32 tiles
-  uint64_t fac_floats = 0;
+  uint64_t fac_floats = 0;         // elements of the tile storage
+  // FP16 storage instead (the step's preconditioner): W = fac_scale[d] * fac_h (the largest
+  // |W| of the domain), which halves the apply's traffic and shared-memory slice
+  bool half = false;
+  mg::DevBuf<__half> fac_h;
+  mg::DevBuf<float> fac_scale;
   mg::DevBuf<uint32_t> status;
 };
 

@@ -24,7 +24,7 @@
 namespace mg {
 
 constexpr int FR_THREADS = 256;
-constexpr int FR_LPR = 2;          // lanes per block row
+constexpr int FR_LPR = 2;          // lanes per block row (4 and 8 measured slower on the batch)
 constexpr int FD_WARPS = 4;        // Schwarz: warps (domains) per CTA
 constexpr int FD_THREADS = 256;    // block Jacobi: vertices per CTA
 constexpr uint32_t FUSED_CHECK = 16;
@@ -39,7 +39,8 @@ struct FusedArgs {
   const float* bjinv;
   const uint32_t *dom_start, *dom_verts;
   const uint64_t* fac_off;
-  const float* fac;
+  const void* fac;         // float or __half tiles
+  const float* fac_scale;  // per domain (FP16 tiles), else null
   const float* b;
   float *x, *r, *z, *ap;
   float tol;
@@ -205,7 +206,7 @@ __device__ __forceinline__ void fd_finish(const FusedArgs& a, bool init) {
 }
 
 // Schwarz domains: one warp per domain. init: x = 0, r = b, p_init = 0.
-template <class Acc>
+template <class Acc, class TS>
 __global__ void __launch_bounds__(32 * FD_WARPS) k_fr_schwarz(FusedArgs a, const float* __restrict__ pc,
                                                              float* __restrict__ p_init, int init) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -220,21 +221,21 @@ __global__ void __launch_bounds__(32 * FD_WARPS) k_fr_schwarz(FusedArgs a, const
   const float al = (float)a.inst[k].alpha;
   const bool skip = !init && a.inst[k].done != 0 && !upd;
   uint64_t* bar = (uint64_t*)(smem + 16 * w);
-  float* buf = (float*)(smem + 128 + (size_t)w * APPLY_SLICE * 4);
-  float* rd = buf + 6 * TILE_FLOATS;
+  TS* buf = (TS*)(smem + 128 + (size_t)w * apply_slice_bytes<TS>());
+  float* rd = (float*)(buf + 6 * TILE_FLOATS);
   Acc* yd = (Acc*)(rd + 96);
   Acc rr = 0, rz = 0;
   if (d < dend && !skip) {
     const uint32_t vs = a.dom_start[d], nvd = a.dom_start[d + 1] - vs;
     const int m = 3 * (int)nvd;
     const uint64_t off = a.fac_off[d];
-    const uint32_t bytes = (uint32_t)((a.fac_off[d + 1] - off) * 4);
+    const uint32_t bytes = (uint32_t)((a.fac_off[d + 1] - off) * sizeof(TS));
     if (lane == 0) {
       mbar_init(bar, 1);
       fence_mbar_init();
       fence_proxy_async();
       mbar_arrive_expect_tx(bar, bytes);
-      bulk_g2s(buf, a.fac + off, bytes, bar);
+      bulk_g2s(buf, (const TS*)a.fac + off, bytes, bar);
     }
     for (int i = lane; i < 96; i += 32) {
       float v = 0.f;
@@ -263,16 +264,17 @@ __global__ void __launch_bounds__(32 * FD_WARPS) k_fr_schwarz(FusedArgs a, const
       Acc zz[3];
       const int T = (m + 31) >> 5;
       if (T == 3)
-        tiles_apply<3, Acc>(buf, rd, yd, zz, lane);
+        tiles_apply<3, Acc, TS>(buf, rd, yd, zz, lane);
       else if (T == 2)
-        tiles_apply<2, Acc>(buf, rd, yd, zz, lane);
+        tiles_apply<2, Acc, TS>(buf, rd, yd, zz, lane);
       else
-        tiles_apply<1, Acc>(buf, rd, yd, zz, lane);
+        tiles_apply<1, Acc, TS>(buf, rd, yd, zz, lane);
+      const Acc sc = a.fac_scale ? (Acc)a.fac_scale[d] : (Acc)1;
 #pragma unroll
       for (int J = 0; J < 3; ++J) {
         const int i = 32 * J + lane;
         if (i < m) {
-          const float zi = (float)zz[J];
+          const float zi = (float)(zz[J] * sc * sc);
           a.z[3 * a.dom_verts[vs + i / 3] + i % 3] = zi;
           rr += (Acc)rd[i] * (Acc)rd[i];
           rz += (Acc)rd[i] * (Acc)zi;
@@ -354,9 +356,12 @@ Launch fused_kernels(const Scene& s) {
   Launch L{};
   const bool sch = s.schwarz != nullptr;
   L.rows = s.mixed ? (void*)k_fr_rows<double> : (void*)k_fr_rows<float>;
-  if (sch) {
-    L.dom = s.mixed ? (void*)k_fr_schwarz<double> : (void*)k_fr_schwarz<float>;
-    L.dom_smem = 128 + (size_t)FD_WARPS * APPLY_SLICE * 4;
+  if (sch && s.schwarz->half) {
+    L.dom = s.mixed ? (void*)k_fr_schwarz<double, __half> : (void*)k_fr_schwarz<float, __half>;
+    L.dom_smem = 128 + (size_t)FD_WARPS * apply_slice_bytes<__half>();
+  } else if (sch) {
+    L.dom = s.mixed ? (void*)k_fr_schwarz<double, float> : (void*)k_fr_schwarz<float, float>;
+    L.dom_smem = 128 + (size_t)FD_WARPS * apply_slice_bytes<float>();
   } else {
     L.dom = s.mixed ? (void*)k_fr_bj<double> : (void*)k_fr_bj<float>;
     L.dom_smem = 0;
@@ -430,7 +435,8 @@ int pcg_fused(Scene& s, const uint32_t* h_inst_row, uint32_t K, uint32_t active,
     a.dom_start = sw->dom_start.p;
     a.dom_verts = sw->dom_verts.p;
     a.fac_off = sw->fac_off.p;
-    a.fac = sw->fac.p;
+    a.fac = sw->half ? (const void*)sw->fac_h.p : (const void*)sw->fac.p;
+    a.fac_scale = sw->half ? sw->fac_scale.p : nullptr;
   }
   a.b = w.b.p;
   a.x = w.x.p;

@@ -46,7 +46,8 @@ struct PersistentArgs {
   const float* bjinv;
   const uint32_t *dom_start, *dom_verts;
   const uint64_t* fac_off;
-  const float* fac;
+  const void* fac;         // float or __half tiles
+  const float* fac_scale;  // per domain (FP16 tiles), else null
   uint32_t ndom;
   const float* b;
   float *x, *r, *z, *p, *p2, *ap;
@@ -139,7 +140,7 @@ constexpr int PP_LPR = 2;  // lanes per block row in the SpMV phase
 //                      between; r.r and r.z together.
 // This is the reference's iteration with its arithmetic unchanged; only the scheduling and
 // the order of the partial sums of the dot products differ.
-template <int PRE, class Acc>
+template <int PRE, class Acc, class TS>
 __global__ void __launch_bounds__(PP_THREADS, 1) k_pcg_persistent(PersistentArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint32_t s_row[PCG_MAX_INST + 1], s_cta[PCG_MAX_INST + 1], s_dom[PCG_MAX_INST + 1];
@@ -175,7 +176,7 @@ __global__ void __launch_bounds__(PP_THREADS, 1) k_pcg_persistent(PersistentArgs
   const uint32_t lthreads = nc * PP_THREADS, ltid = lc * PP_THREADS + tid;
 
   uint64_t* mbar = (uint64_t*)(smem + 16 * w);
-  float* buf = (float*)(smem + 128 + (size_t)w * APPLY_SLICE * 4);
+  TS* buf = (TS*)(smem + 128 + (size_t)w * apply_slice_bytes<TS>());
   uint32_t mphase = 0;
   if (PRE == MGUSO_PRECOND_SCHWARZ && lane == 0) {
     mbar_init(mbar, 1);
@@ -193,17 +194,17 @@ __global__ void __launch_bounds__(PP_THREADS, 1) k_pcg_persistent(PersistentArgs
     acc[0] = 0;
     acc[1] = 0;
     if (PRE == MGUSO_PRECOND_SCHWARZ) {
-      float* rd = buf + 6 * TILE_FLOATS;
+      float* rd = (float*)(buf + 6 * TILE_FLOATS);
       Acc* yd = (Acc*)(rd + 96);
       for (uint32_t d = s_dom[k] + lc * PP_WARPS + w; d < s_dom[k + 1]; d += nc * PP_WARPS) {
         const uint32_t vs = a.dom_start[d], nvd = a.dom_start[d + 1] - vs;
         const int m = 3 * (int)nvd;
         const uint64_t off = a.fac_off[d];
-        const uint32_t bytes = (uint32_t)((a.fac_off[d + 1] - off) * 4);
+        const uint32_t bytes = (uint32_t)((a.fac_off[d + 1] - off) * sizeof(TS));
         if (lane == 0) {
           fence_proxy_async();
           mbar_arrive_expect_tx(mbar, bytes);
-          bulk_g2s(buf, a.fac + off, bytes, mbar);
+          bulk_g2s(buf, (const TS*)a.fac + off, bytes, mbar);
         }
         for (int i = lane; i < 96; i += 32) {
           float v = 0.f;
@@ -237,16 +238,17 @@ __global__ void __launch_bounds__(PP_THREADS, 1) k_pcg_persistent(PersistentArgs
         Acc zz[3];
         const int T = (m + 31) >> 5;
         if (T == 3)
-          tiles_apply<3, Acc>(buf, rd, yd, zz, lane);
+          tiles_apply<3, Acc, TS>(buf, rd, yd, zz, lane);
         else if (T == 2)
-          tiles_apply<2, Acc>(buf, rd, yd, zz, lane);
+          tiles_apply<2, Acc, TS>(buf, rd, yd, zz, lane);
         else
-          tiles_apply<1, Acc>(buf, rd, yd, zz, lane);
+          tiles_apply<1, Acc, TS>(buf, rd, yd, zz, lane);
+        const Acc sc = a.fac_scale ? (Acc)a.fac_scale[d] : (Acc)1;
 #pragma unroll
         for (int J = 0; J < 3; ++J) {
           const int i = 32 * J + lane;
           if (i < m) {
-            const float zi = (float)zz[J];
+            const float zi = (float)(zz[J] * sc * sc);
             a.z[3 * a.dom_verts[vs + i / 3] + i % 3] = zi;
             acc[0] += (Acc)rd[i] * (Acc)rd[i];
             acc[1] += (Acc)rd[i] * (Acc)zi;
@@ -402,13 +404,22 @@ __global__ void __launch_bounds__(PP_THREADS, 1) k_pcg_persistent(PersistentArgs
   }
 }
 
+static void* persistent_kernel(const Scene& s) {
+  if (!s.schwarz)
+    return s.mixed ? (void*)k_pcg_persistent<MGUSO_PRECOND_BLOCK_JACOBI, double, float>
+                   : (void*)k_pcg_persistent<MGUSO_PRECOND_BLOCK_JACOBI, float, float>;
+  if (s.schwarz->half)
+    return s.mixed ? (void*)k_pcg_persistent<MGUSO_PRECOND_SCHWARZ, double, __half>
+                   : (void*)k_pcg_persistent<MGUSO_PRECOND_SCHWARZ, float, __half>;
+  return s.mixed ? (void*)k_pcg_persistent<MGUSO_PRECOND_SCHWARZ, double, float>
+                 : (void*)k_pcg_persistent<MGUSO_PRECOND_SCHWARZ, float, float>;
+}
+
 int pcg_persistent_configure(Scene& s, int* grid_out) {
   const bool sch = s.schwarz != nullptr;
-  const size_t smem = sch ? 128 + (size_t)PP_WARPS * APPLY_SLICE * 4 : 0;
-  void* fn = sch ? (s.mixed ? (void*)k_pcg_persistent<MGUSO_PRECOND_SCHWARZ, double>
-                            : (void*)k_pcg_persistent<MGUSO_PRECOND_SCHWARZ, float>)
-                 : (s.mixed ? (void*)k_pcg_persistent<MGUSO_PRECOND_BLOCK_JACOBI, double>
-                            : (void*)k_pcg_persistent<MGUSO_PRECOND_BLOCK_JACOBI, float>);
+  const size_t smem = !sch ? 0
+                     : 128 + (size_t)PP_WARPS * (s.schwarz->half ? apply_slice_bytes<__half>() : apply_slice_bytes<float>());
+  void* fn = persistent_kernel(s);
   if (smem) MG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   MG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, PP_THREADS, smem));
@@ -482,7 +493,8 @@ int pcg_persistent(Scene& s, const uint32_t* h_inst_row, uint32_t ninst, uint32_
     a.dom_start = sw->dom_start.p;
     a.dom_verts = sw->dom_verts.p;
     a.fac_off = sw->fac_off.p;
-    a.fac = sw->fac.p;
+    a.fac = sw->half ? (const void*)sw->fac_h.p : (const void*)sw->fac.p;
+    a.fac_scale = sw->half ? sw->fac_scale.p : nullptr;
     a.ndom = sw->ndom;
   }
   a.b = w.b.p;
@@ -508,11 +520,9 @@ int pcg_persistent(Scene& s, const uint32_t* h_inst_row, uint32_t ninst, uint32_
     a.probe = (unsigned long long*)s.pp_probe.p;
   }
   const bool sch = s.schwarz != nullptr;
-  const size_t smem = sch ? 128 + (size_t)PP_WARPS * APPLY_SLICE * 4 : 0;
-  void* fn = sch ? (s.mixed ? (void*)k_pcg_persistent<MGUSO_PRECOND_SCHWARZ, double>
-                            : (void*)k_pcg_persistent<MGUSO_PRECOND_SCHWARZ, float>)
-                 : (s.mixed ? (void*)k_pcg_persistent<MGUSO_PRECOND_BLOCK_JACOBI, double>
-                            : (void*)k_pcg_persistent<MGUSO_PRECOND_BLOCK_JACOBI, float>);
+  const size_t smem = !sch ? 0
+                     : 128 + (size_t)PP_WARPS * (s.schwarz->half ? apply_slice_bytes<__half>() : apply_slice_bytes<float>());
+  void* fn = persistent_kernel(s);
   void* args[] = {(void*)&a};
   MG_CUDA(cudaLaunchCooperativeKernel(fn, dim3(s.pp_grid), dim3(PP_THREADS), args, smem, st));
   uint32_t err[4] = {0, 0, 0, 0};

@@ -9,6 +9,7 @@
 //   set_static_collider_verts (implicit.rs:1258-1320): winding check and angle-weighted
 //     pseudonormals (contact.rs:963-1001).
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -534,6 +535,7 @@ int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>
     s.schwarz = std::make_unique<mguso_schwarz>();
     s.schwarz->a = s.A.get();
     s.schwarz->domain = s.p.schwarz_domain;
+    s.schwarz->half = true;  // FP16 factor tiles: the apply moves half the bytes
     s.schwarz->inst_vert = s.inst_vert;
     MG_TRY(schwarz_build(s.schwarz.get()));
   } else {
@@ -850,8 +852,10 @@ extern "C" int mguso_scene_profile(mguso_scene* sc, int reps, float* us4, double
       double m = 3.0 * (sw->h_dom_start[d + 1] - sw->h_dom_start[d]);
       packed += m * (m + 1) / 2;
     }
-    bytes4[1] = 4.0 * packed + 4.0 * s.nv + 24.0 * s.nv + 8.0 * (sw->ndom + 1);
-    bytes4[2] = 36.0 * nnz + 4.0 * packed;
+    // factor entries at their stored width (2 bytes in FP16 plus a scale per domain)
+    const double fe = sw->half ? 2.0 : 4.0, fs = sw->half ? 4.0 * sw->ndom : 0.0;
+    bytes4[1] = fe * packed + fs + 4.0 * s.nv + 24.0 * s.nv + 8.0 * (sw->ndom + 1);
+    bytes4[2] = 36.0 * nnz + fe * packed + fs;
     if (rc == MGUSO_OK) rc = timed([&]() { return schwarz_apply(sw, x.p, y.p, st, nullptr); }, &us4[1]);
     if (rc == MGUSO_OK)
       rc = timed([&]() { return schwarz_factor_with(sw, s.c_row_ptr.p, s.c_col.p, s.c_val.p, st); }, &us4[2]);

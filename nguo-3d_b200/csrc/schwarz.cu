@@ -112,7 +112,12 @@ int schwarz_build(mguso_schwarz* s) {
   MG_TRY(s->dom_of.upload(s->h_dom_of.data(), nb, st));
   MG_TRY(s->loc.upload(loc.data(), nb, st));
   MG_TRY(s->fac_off.upload(off.data(), off.size(), st));
-  MG_TRY(s->fac.reserve(std::max<uint64_t>(s->fac_floats, 4)));
+  if (s->half) {
+    MG_TRY(s->fac_h.reserve(std::max<uint64_t>(s->fac_floats, 8)));
+    MG_TRY(s->fac_scale.reserve(std::max<uint32_t>(s->ndom, 1)));
+  } else {
+    MG_TRY(s->fac.reserve(std::max<uint64_t>(s->fac_floats, 4)));
+  }
   MG_TRY(s->status.reserve(4));
   MG_CUDA(cudaMemsetAsync(s->status.p, 0, 16, st));
   MG_CUDA(cudaStreamSynchronize(st));
@@ -136,12 +141,47 @@ int schwarz_build(mguso_schwarz* s) {
 // ---------------------------------------------------------------------------------------
 constexpr int FACTOR_THREADS = 256;
 
+template <class TS>
+__device__ __forceinline__ TS to_tile(double v) {
+  return (TS)v;
+}
+template <>
+__device__ __forceinline__ __half to_tile<__half>(double v) {
+  return __float2half_rn((float)v);
+}
+
+// Largest |W_ij| over the domain's lower triangle (W_ij at A[j * ld + i], j <= i < m), or
+// over diag when the factorisation failed; every thread gets it.
+__device__ double factor_amax(const double* A, int ld, int m, const double* diag, bool failed) {
+  __shared__ double s_w[FACTOR_THREADS / 32];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  double mx = 0.0;
+  if (failed) {
+    for (int r = tid; r < m; r += nt) mx = fmax(mx, diag[r] > 1e-14 ? 1.0 / sqrt(diag[r]) : 1.0);
+  } else {
+    for (int e = tid; e < m * m; e += nt) {
+      const int i = e / m, j = e - i * m;
+      if (j <= i) mx = fmax(mx, fabs(A[j * ld + i]));
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((tid & 31) == 0) s_w[tid >> 5] = mx;
+  __syncthreads();
+  double r = 0.0;
+  for (int q = 0; q < nt / 32; ++q) r = fmax(r, s_w[q]);
+  __syncthreads();
+  return r > 0.0 ? r : 1.0;
+}
+
+template <class TS>
 __global__ void __launch_bounds__(FACTOR_THREADS) k_schwarz_factor(
     const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ col, const float* __restrict__ val,
     const uint32_t* __restrict__ dom_start, const uint32_t* __restrict__ dom_verts,
     const uint32_t* __restrict__ dom_of, const uint32_t* __restrict__ loc, const uint64_t* __restrict__ fac_off,
-    float* __restrict__ fac, uint32_t* status, const uint32_t* __restrict__ c_rp, const uint32_t* __restrict__ c_col,
-    const float* __restrict__ c_val) {
+    TS* __restrict__ fac, float* __restrict__ fac_scale, uint32_t* status, const uint32_t* __restrict__ c_rp,
+    const uint32_t* __restrict__ c_col, const float* __restrict__ c_val) {
+  // FP16 tiles hold W / scale (scale: the domain's largest |W|); FP32 tiles hold W
+  constexpr bool scaled = sizeof(TS) == 2;
   extern __shared__ __align__(16) double sA[];
   __shared__ double s_floor;
   __shared__ int s_fail;
@@ -218,17 +258,19 @@ __global__ void __launch_bounds__(FACTOR_THREADS) k_schwarz_factor(
     __syncthreads();
   }
   __syncthreads();
-  float* out = fac + fac_off[d];
+  TS* out = fac + fac_off[d];
   const int T = (m + 31) / 32, nfl = T * (T + 1) / 2 * TILE_FLOATS;
   if (s_fail) {
     // reference fallback: L = diag(sqrt(ad_pp)) (1 where ad_pp <= 1e-14), i.e.
     // W = diag(1 / sqrt(ad_pp))
-    for (int e = tid; e < nfl; e += nt) out[e] = 0.0f;
+    const double sc = scaled ? factor_amax(A, ld, m, diag0, true) : 1.0;
+    if (scaled && tid == 0) fac_scale[d] = (float)sc;
+    for (int e = tid; e < nfl; e += nt) out[e] = to_tile<TS>(0.0);
     __syncthreads();
     for (int r = tid; r < m; r += nt) {
       double a = diag0[r];
       const int I = r >> 5, lr = r & 31;
-      out[tile_index(I, I) * TILE_FLOATS + tile_offset(lr, lr)] = (float)(a > 1e-14 ? 1.0 / sqrt(a) : 1.0);
+      out[tile_index(I, I) * TILE_FLOATS + tile_offset(lr, lr)] = to_tile<TS>((a > 1e-14 ? 1.0 / sqrt(a) : 1.0) / sc);
     }
     if (tid == 0) atomicOr(status, 1u << 8);
     return;
@@ -254,13 +296,15 @@ __global__ void __launch_bounds__(FACTOR_THREADS) k_schwarz_factor(
     }
   }
   __syncthreads();
+  const double inv_sc = scaled ? 1.0 / factor_amax(A, ld, m, diag0, false) : 1.0;
+  if (scaled && tid == 0) fac_scale[d] = (float)(1.0 / inv_sc);
   // tiles in storage order; e walks each tile's swizzled offsets so the stores coalesce
   for (int e = tid; e < nfl; e += nt) {
     const int t = e / TILE_FLOATS, o = e - t * TILE_FLOATS;
     const int I = t >= 3 ? 2 : (t >= 1 ? 1 : 0), J = t - I * (I + 1) / 2;
     const int c = o >> 5, r = (o & 31) ^ c;
     const int gi = 32 * I + r, gj = 32 * J + c;
-    out[e] = (gi < m && gj <= gi) ? (float)A[gj * ld + gi] : 0.0f;
+    out[e] = to_tile<TS>((gi < m && gj <= gi) ? A[gj * ld + gi] * inv_sc : 0.0);
   }
 }
 
@@ -273,9 +317,14 @@ int schwarz_factor_with(mguso_schwarz* s, const uint32_t* c_rp, const uint32_t* 
   if (s->ndom == 0) return MGUSO_OK;
   mguso_bsr* a = s->a;
   size_t smem = sizeof(double) * ((size_t)s->max_m * (s->max_m + 1) + 2 * (size_t)s->max_m);
-  k_schwarz_factor<<<s->ndom, FACTOR_THREADS, smem, st>>>(a->row_ptr.p, a->col.p, a->val.p, s->dom_start.p, s->dom_verts.p,
-                                               s->dom_of.p, s->loc.p, s->fac_off.p, s->fac.p, s->status.p,
-                                                          c_col ? c_rp : nullptr, c_col, c_val);
+  if (s->half)
+    k_schwarz_factor<__half><<<s->ndom, FACTOR_THREADS, smem, st>>>(
+        a->row_ptr.p, a->col.p, a->val.p, s->dom_start.p, s->dom_verts.p, s->dom_of.p, s->loc.p, s->fac_off.p,
+        s->fac_h.p, s->fac_scale.p, s->status.p, c_col ? c_rp : nullptr, c_col, c_val);
+  else
+    k_schwarz_factor<float><<<s->ndom, FACTOR_THREADS, smem, st>>>(
+        a->row_ptr.p, a->col.p, a->val.p, s->dom_start.p, s->dom_verts.p, s->dom_of.p, s->loc.p, s->fac_off.p,
+        s->fac.p, nullptr, s->status.p, c_col ? c_rp : nullptr, c_col, c_val);
   MG_CUDA(cudaGetLastError());
   return MGUSO_OK;
 }
@@ -291,17 +340,17 @@ int schwarz_factor_with(mguso_schwarz* s, const uint32_t* c_rp, const uint32_t* 
 // ---------------------------------------------------------------------------------------
 constexpr int APPLY_WARPS = 4;
 
-template <int WARPS, class Acc>
+template <int WARPS, class Acc, class TS>
 __global__ void __launch_bounds__(32 * WARPS) k_schwarz_apply(
     const uint32_t* __restrict__ dom_start, const uint32_t* __restrict__ dom_verts,
-    const uint64_t* __restrict__ fac_off, const float* __restrict__ fac, const float* __restrict__ r,
-    float* __restrict__ z, uint32_t ndom, uint32_t* status, DotSink dot, int with_dot) {
+    const uint64_t* __restrict__ fac_off, const TS* __restrict__ fac, const float* __restrict__ fac_scale,
+    const float* __restrict__ r, float* __restrict__ z, uint32_t ndom, uint32_t* status, DotSink dot, int with_dot) {
   extern __shared__ __align__(128) unsigned char smem[];
   if (with_dot && dot.sc->done) return;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   uint64_t* bar = (uint64_t*)(smem + 16 * w);
-  float* buf = (float*)(smem + 128 + (size_t)w * APPLY_SLICE * 4);
-  float* rd = buf + 6 * TILE_FLOATS;
+  TS* buf = (TS*)(smem + 128 + (size_t)w * apply_slice_bytes<TS>());
+  float* rd = (float*)(buf + 6 * TILE_FLOATS);
   Acc* yd = (Acc*)(rd + 96);
   Acc acc = 0;
   if (lane == 0) {
@@ -314,7 +363,7 @@ __global__ void __launch_bounds__(32 * WARPS) k_schwarz_apply(
     const uint32_t vs = dom_start[d], nvd = dom_start[d + 1] - vs;
     const int m = 3 * (int)nvd;
     const uint64_t off = fac_off[d];
-    const uint32_t bytes = (uint32_t)((fac_off[d + 1] - off) * 4);
+    const uint32_t bytes = (uint32_t)((fac_off[d + 1] - off) * sizeof(TS));
     if (lane == 0) {
       fence_proxy_async();
       mbar_arrive_expect_tx(bar, bytes);
@@ -335,16 +384,17 @@ __global__ void __launch_bounds__(32 * WARPS) k_schwarz_apply(
     Acc zz[3];
     const int T = (m + 31) >> 5;
     if (T == 3)
-      tiles_apply<3, Acc>(buf, rd, yd, zz, lane);
+      tiles_apply<3, Acc, TS>(buf, rd, yd, zz, lane);
     else if (T == 2)
-      tiles_apply<2, Acc>(buf, rd, yd, zz, lane);
+      tiles_apply<2, Acc, TS>(buf, rd, yd, zz, lane);
     else
-      tiles_apply<1, Acc>(buf, rd, yd, zz, lane);
+      tiles_apply<1, Acc, TS>(buf, rd, yd, zz, lane);
+    const Acc sc = fac_scale ? (Acc)fac_scale[d] : (Acc)1;
 #pragma unroll
     for (int J = 0; J < 3; ++J) {
       const int i = 32 * J + lane;
       if (i < m) {
-        const float zi = (float)zz[J];
+        const float zi = (float)(zz[J] * sc * sc);
         z[3 * dom_verts[vs + i / 3] + i % 3] = zi;
         acc += (Acc)rd[i] * (Acc)zi;
       }
@@ -360,12 +410,18 @@ int schwarz_configure() {
   static bool done = false;
   if (done) return MGUSO_OK;
   size_t fsm = sizeof(double) * (96 * 97 + 2 * 96);
-  MG_CUDA(cudaFuncSetAttribute(k_schwarz_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
-  size_t asmem = 128 + (size_t)APPLY_WARPS * APPLY_SLICE * 4;
-  MG_CUDA(cudaFuncSetAttribute(k_schwarz_apply<APPLY_WARPS, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)asmem));
-  MG_CUDA(cudaFuncSetAttribute(k_schwarz_apply<APPLY_WARPS, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)asmem));
+  MG_CUDA(cudaFuncSetAttribute(k_schwarz_factor<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
+  MG_CUDA(cudaFuncSetAttribute(k_schwarz_factor<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
+  const int asm32 = (int)(128 + (size_t)APPLY_WARPS * apply_slice_bytes<float>());
+  const int asm16 = (int)(128 + (size_t)APPLY_WARPS * apply_slice_bytes<__half>());
+  MG_CUDA(cudaFuncSetAttribute(k_schwarz_apply<APPLY_WARPS, double, float>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, asm32));
+  MG_CUDA(cudaFuncSetAttribute(k_schwarz_apply<APPLY_WARPS, float, float>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, asm32));
+  MG_CUDA(cudaFuncSetAttribute(k_schwarz_apply<APPLY_WARPS, double, __half>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, asm16));
+  MG_CUDA(cudaFuncSetAttribute(k_schwarz_apply<APPLY_WARPS, float, __half>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, asm16));
   done = true;
   return MGUSO_OK;
 }
@@ -379,17 +435,22 @@ int schwarz_apply(mguso_schwarz* s, const float* r, float* z, cudaStream_t st, c
     set_error("Schwarz domain larger than 32 vertices");
     return MGUSO_ERR_UNSUPPORTED;
   }
-  size_t smem = 128 + (size_t)APPLY_WARPS * APPLY_SLICE * 4;
-  // two resident CTAs per SM, grid-stride over the domains
-  uint32_t grid = std::min<uint32_t>(ceil_div(s->ndom, APPLY_WARPS), 2u * (uint32_t)s->a->ctx->sm_count);
-  void* fn = mixed ? (void*)k_schwarz_apply<APPLY_WARPS, double> : (void*)k_schwarz_apply<APPLY_WARPS, float>;
+  const bool h = s->half;
+  size_t smem = 128 + (size_t)APPLY_WARPS * (h ? apply_slice_bytes<__half>() : apply_slice_bytes<float>());
+  // resident CTAs per SM as shared memory allows (2 with FP32 tiles, 4 with FP16), grid-stride
+  uint32_t grid = std::min<uint32_t>(ceil_div(s->ndom, APPLY_WARPS), (h ? 4u : 2u) * (uint32_t)s->a->ctx->sm_count);
+  void* fn = h ? (mixed ? (void*)k_schwarz_apply<APPLY_WARPS, double, __half>
+                        : (void*)k_schwarz_apply<APPLY_WARPS, float, __half>)
+               : (mixed ? (void*)k_schwarz_apply<APPLY_WARPS, double, float>
+                        : (void*)k_schwarz_apply<APPLY_WARPS, float, float>);
   const uint32_t* a0 = s->dom_start.p;
   const uint32_t* a1 = s->dom_verts.p;
   const uint64_t* a2 = s->fac_off.p;
-  const float* a3 = s->fac.p;
+  const void* a3 = h ? (const void*)s->fac_h.p : (const void*)s->fac.p;
+  const float* a4 = h ? s->fac_scale.p : nullptr;
   uint32_t nd = s->ndom;
   uint32_t* stp = s->status.p;
-  void* args[] = {(void*)&a0, (void*)&a1, (void*)&a2, (void*)&a3, (void*)&r, (void*)&z,
+  void* args[] = {(void*)&a0, (void*)&a1, (void*)&a2, (void*)&a3, (void*)&a4, (void*)&r, (void*)&z,
                   (void*)&nd, (void*)&stp, (void*)&d, (void*)&with_dot};
   if (grid == 0) return MGUSO_OK;
   MG_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(32 * APPLY_WARPS), args, smem, st));

@@ -11,32 +11,44 @@ constexpr int TILE_FLOATS = 1024;
 __host__ __device__ __forceinline__ int tile_index(int I, int J) { return I * (I + 1) / 2 + J; }
 __host__ __device__ __forceinline__ int tile_offset(int r, int c) { return c * 32 + (r ^ c); }
 
-// Per-warp shared slice of an apply: the domain's tiles, the gathered residual (96 floats)
-// and W r (96 values of the accumulation type, 192 floats' room).
-constexpr uint32_t APPLY_SLICE = 6 * TILE_FLOATS + 96 + 2 * 96;
+// Per-warp shared slice of an apply: the domain's tiles (6 tiles of elements TS), the
+// gathered residual (96 floats) and W r (96 values of the accumulation type, 768 bytes).
+template <class TS>
+__host__ __device__ constexpr uint32_t apply_slice_bytes() {
+  return 6 * TILE_FLOATS * (uint32_t)sizeof(TS) + 96 * 4 + 96 * 8;
+}
+template <class TS>
+__device__ __forceinline__ float tile_ld(const TS* t, int o) {
+  return (float)t[o];
+}
+template <>
+__device__ __forceinline__ float tile_ld<__half>(const __half* t, int o) {
+  return __half2float(t[o]);
+}
 
-// One domain's z = W^T (W r) by one warp (see the apply kernel in schwarz.cu).
-template <int T, class Acc>
-__device__ __forceinline__ void tiles_apply(const float* __restrict__ w, const float* __restrict__ rd,
+// One domain's z = W^T (W r) by one warp (see the apply kernel in schwarz.cu); tiles of
+// element type TS (FP16 tiles give W / scale, so z comes out divided by scale^2).
+template <int T, class Acc, class TS = float>
+__device__ __forceinline__ void tiles_apply(const TS* __restrict__ w, const float* __restrict__ rd,
                                             Acc* __restrict__ yd, Acc (&z)[3], int lane) {
-  const float* t00 = w;
-  const float* t10 = w + 1 * TILE_FLOATS;
-  const float* t11 = w + 2 * TILE_FLOATS;
-  const float* t20 = w + 3 * TILE_FLOATS;
-  const float* t21 = w + 4 * TILE_FLOATS;
-  const float* t22 = w + 5 * TILE_FLOATS;
+  const TS* t00 = w;
+  const TS* t10 = w + 1 * TILE_FLOATS;
+  const TS* t11 = w + 2 * TILE_FLOATS;
+  const TS* t20 = w + 3 * TILE_FLOATS;
+  const TS* t21 = w + 4 * TILE_FLOATS;
+  const TS* t22 = w + 5 * TILE_FLOATS;
   Acc y0 = 0, y1 = 0, y2 = 0;
 #pragma unroll 8
   for (int c = 0; c < 32; ++c) {
     const int o = tile_offset(lane, c);
     const Acc a0 = (Acc)rd[c];
-    y0 += (Acc)t00[o] * a0;
+    y0 += (Acc)tile_ld(t00, o) * a0;
     if (T > 1) {
       const Acc a1 = (Acc)rd[32 + c];
-      y1 += (Acc)t10[o] * a0 + (Acc)t11[o] * a1;
+      y1 += (Acc)tile_ld(t10, o) * a0 + (Acc)tile_ld(t11, o) * a1;
       if (T > 2) {
         const Acc a2 = (Acc)rd[64 + c];
-        y2 += (Acc)t20[o] * a0 + (Acc)t21[o] * a1 + (Acc)t22[o] * a2;
+        y2 += (Acc)tile_ld(t20, o) * a0 + (Acc)tile_ld(t21, o) * a1 + (Acc)tile_ld(t22, o) * a2;
       }
     }
   }
@@ -49,16 +61,16 @@ __device__ __forceinline__ void tiles_apply(const float* __restrict__ w, const f
   for (int r = 0; r < 32; ++r) {
     const int o = tile_offset(r, lane);
     const Acc b0 = yd[r];
-    z0 += (Acc)t00[o] * b0;
+    z0 += (Acc)tile_ld(t00, o) * b0;
     if (T > 1) {
       const Acc b1 = yd[32 + r];
-      z0 += (Acc)t10[o] * b1;
-      z1 += (Acc)t11[o] * b1;
+      z0 += (Acc)tile_ld(t10, o) * b1;
+      z1 += (Acc)tile_ld(t11, o) * b1;
       if (T > 2) {
         const Acc b2 = yd[64 + r];
-        z0 += (Acc)t20[o] * b2;
-        z1 += (Acc)t21[o] * b2;
-        z2 += (Acc)t22[o] * b2;
+        z0 += (Acc)tile_ld(t20, o) * b2;
+        z1 += (Acc)tile_ld(t21, o) * b2;
+        z2 += (Acc)tile_ld(t22, o) * b2;
       }
     }
   }
