@@ -361,12 +361,47 @@ __global__ void k_ccd_colliders(const uint32_t* __restrict__ free_verts, uint32_
 // its first test cannot lower the step fraction, and traversal skips whole subtrees of such
 // pairs (lbvh_visit_ccd) from the primitives' displacement boxes, refitted per CCD call.
 
-// Per-instance CCD pass parameters: search radius and whether the instance still needs a
-// pass (an instance whose step fraction was settled by an earlier pass is skipped).
+// Per-instance CCD passes of one launch: up to CCD_CHUNK consecutive search radii of the
+// widening schedule (ascending). The traversal uses the largest; each candidate pair's ACCD
+// result then counts for every pass whose search box reaches it (the box test of that pass
+// alone), so one launch yields each pass's step fraction and cap count exactly as separate
+// passes would. Instances whose fraction an earlier launch settled are skipped.
+constexpr int CCD_CHUNK = 6;
 struct CcdPass {
-  float search[PCG_MAX_INST];
+  float search[PCG_MAX_INST][CCD_CHUNK];
+  uint32_t npass[PCG_MAX_INST];
   uint32_t todo;  // bit k: instance k
 };
+
+// per (instance, pass) accumulators: [0] step fraction (float bits, atomic min), [1] caps
+__device__ __forceinline__ unsigned int* ccd_slot(unsigned int* acc, uint32_t k, int i) {
+  return acc + 2 * (CCD_CHUNK * k + i);
+}
+
+// The first pass (index into the chunk) whose query box overlaps the primitive's box
+// [plo, phi]; the query box of pass i is built as the traversal builds its own.
+__device__ __forceinline__ int first_pass_point(const CcdPass& cp, uint32_t k, const float* x, uint32_t v,
+                                                const float plo[3], const float phi[3]) {
+  const int n = (int)cp.npass[k];
+  for (int i = 0; i < n; ++i) {
+    float4 lo, hi;
+    point_box(x, v, cp.search[k][i], lo, hi);
+    if (lo.x <= phi[0] && lo.y <= phi[1] && lo.z <= phi[2] && plo[0] <= hi.x && plo[1] <= hi.y && plo[2] <= hi.z)
+      return i;
+  }
+  return n;
+}
+__device__ __forceinline__ int first_pass_edge(const CcdPass& cp, uint32_t k, const float* x, uint32_t a,
+                                               uint32_t b, const float plo[3], const float phi[3]) {
+  const int n = (int)cp.npass[k];
+  for (int i = 0; i < n; ++i) {
+    float4 lo, hi;
+    edge_box(x, a, b, cp.search[k][i], lo, hi);
+    if (lo.x <= phi[0] && lo.y <= phi[1] && lo.z <= phi[2] && plo[0] <= hi.x && plo[1] <= hi.y && plo[2] <= hi.z)
+      return i;
+  }
+  return n;
+}
 
 template <class R>
 __global__ void k_ccd_vt(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
@@ -375,19 +410,26 @@ __global__ void k_ccd_vt(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vins
                          const uint32_t* __restrict__ ex_ptr, const uint32_t* __restrict__ ex_list,
                          const unsigned long long* __restrict__ best, const float* __restrict__ pn, int has_static,
                          uint32_t nv, float dhat, uint32_t max_iter, unsigned int* __restrict__ red,
-                         uint32_t* __restrict__ status) {
+                         unsigned int* __restrict__ acc, uint32_t* __restrict__ status) {
   uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= nv) return;
   const uint32_t k = vinst[v];
   if (!((cp.todo >> k) & 1u)) return;
+  const int np = (int)cp.npass[k];
   float4 lo, hi, qlo, qhi;
-  point_box(x, v, cp.search[k], lo, hi);
+  point_box(x, v, cp.search[k][np - 1], lo, hi);
   point_box(x, v, 0.f, qlo, qhi);
   const float3 cq = make_float3(dx[3 * v], dx[3 * v + 1], dx[3 * v + 2]);
   bool vmov = im[v] > 0.f;
   float side = 2.f;
-  float tloc = 1.f;
-  uint32_t ncap = 0, nleaf = 0, nacc = 0;
+  float tloc[CCD_CHUNK];
+  uint32_t ncap[CCD_CHUNK];
+#pragma unroll
+  for (int i = 0; i < CCD_CHUNK; ++i) {
+    tloc[i] = 1.f;
+    ncap[i] = 0;
+  }
+  uint32_t nleaf = 0, nacc = 0;
   bool ok = visit_ccd(bv, k, lo, hi, qlo, qhi, cq, 0.f, [&](uint32_t t) {
     ++nleaf;
     uint32_t a = tris[3 * t], b = tris[3 * t + 1], c = tris[3 * t + 2];
@@ -398,6 +440,14 @@ __global__ void k_ccd_vt(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vins
       if (side == 2.f) side = side_of(v, best, x, tris, pn, dhat);
       if (side < 0.f) return;
     }
+    float plo[3], phi[3];
+    for (int q = 0; q < 3; ++q) {
+      const float pa = x[3 * a + q], pb = x[3 * b + q], pc = x[3 * c + q];
+      plo[q] = fminf(fminf(pa, pb), pc);
+      phi[q] = fmaxf(fmaxf(pa, pb), pc);
+    }
+    const int i0 = first_pass_point(cp, k, x, v, plo, phi);
+    if (i0 >= np) return;
     uint32_t idx[4] = {v, a, b, c};
     V3<R> x0[4], dd[4];
     for (int q = 0; q < 4; ++q) {
@@ -407,12 +457,20 @@ __global__ void k_ccd_vt(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vins
     bool cap = false;
     ++nacc;
     R toi = accd_toi<R>(x0, dd, R(0), R(1.25), R(0.01), max_iter, 0, &cap);
-    ncap += cap ? 1u : 0u;
-    tloc = fminf(tloc, (float)(toi / R(1.25)));
+    const float tt = (float)(toi / R(1.25));
+#pragma unroll
+    for (int i = 0; i < CCD_CHUNK; ++i)
+      if (i >= i0) {
+        tloc[i] = fminf(tloc[i], tt);
+        ncap[i] += cap ? 1u : 0u;
+      }
   });
   if (!ok) atomicOr(status, ST_STACK_OVERFLOW);
-  if (tloc < 1.f) atomic_min_pos(red + RED_STRIDE * k + 2, tloc);
-  if (ncap) atomicAdd(red + RED_STRIDE * k + 3, ncap);
+#pragma unroll
+  for (int i = 0; i < CCD_CHUNK; ++i) {
+    if (i < np && tloc[i] < 1.f) atomic_min_pos(ccd_slot(acc, k, i), tloc[i]);
+    if (i < np && ncap[i]) atomicAdd(ccd_slot(acc, k, i) + 1, ncap[i]);
+  }
   if (nleaf) atomicAdd(red + RED_STRIDE * k + 5, nleaf);
   if (nacc) atomicAdd(red + RED_STRIDE * k + 6, nacc);
 }
@@ -421,14 +479,15 @@ template <class R>
 __global__ void k_ccd_ee(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
                          const float* __restrict__ dx, const uint32_t* __restrict__ edges, const float* __restrict__ im,
                          uint32_t ne, uint32_t max_iter, unsigned int* __restrict__ red,
-                         uint32_t* __restrict__ status) {
+                         unsigned int* __restrict__ acc, uint32_t* __restrict__ status) {
   uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ne) return;
   uint32_t b0 = edges[2 * j], b1 = edges[2 * j + 1];
   const uint32_t k = vinst[b0];
   if (!((cp.todo >> k) & 1u)) return;
+  const int np = (int)cp.npass[k];
   float4 lo, hi, qlo, qhi;
-  edge_box(x, b0, b1, cp.search[k], lo, hi);
+  edge_box(x, b0, b1, cp.search[k][np - 1], lo, hi);
   edge_box(x, b0, b1, 0.f, qlo, qhi);
   // the query edge's displacements lie in the ball around their midpoint
   const float3 d0 = make_float3(dx[3 * b0], dx[3 * b0 + 1], dx[3 * b0 + 2]);
@@ -437,14 +496,28 @@ __global__ void k_ccd_ee(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vins
   const float ex = d1.x - d0.x, ey = d1.y - d0.y, ez = d1.z - d0.z;
   const float rq = 0.5f * sqrtf(ex * ex + ey * ey + ez * ez) * 1.0001f;
   bool jmov = im[b0] > 0.f || im[b1] > 0.f;
-  float tloc = 1.f;
-  uint32_t ncap = 0, nleaf = 0, nacc = 0;
+  float tloc[CCD_CHUNK];
+  uint32_t ncap[CCD_CHUNK];
+#pragma unroll
+  for (int i = 0; i < CCD_CHUNK; ++i) {
+    tloc[i] = 1.f;
+    ncap[i] = 0;
+  }
+  uint32_t nleaf = 0, nacc = 0;
   bool ok = visit_ccd(bv, k, lo, hi, qlo, qhi, cq, rq, [&](uint32_t i) {
     ++nleaf;
     if (i >= j) return;
     uint32_t a0 = edges[2 * i], a1 = edges[2 * i + 1];
     if (!(jmov || im[a0] > 0.f || im[a1] > 0.f)) return;
     if (a0 == b0 || a0 == b1 || a1 == b0 || a1 == b1) return;
+    float plo[3], phi[3];
+    for (int q = 0; q < 3; ++q) {
+      const float pa = x[3 * a0 + q], pb = x[3 * a1 + q];
+      plo[q] = fminf(pa, pb);
+      phi[q] = fmaxf(pa, pb);
+    }
+    const int i0 = first_pass_edge(cp, k, x, b0, b1, plo, phi);
+    if (i0 >= np) return;
     uint32_t idx[4] = {a0, a1, b0, b1};
     V3<R> x0[4], dd[4];
     for (int q = 0; q < 4; ++q) {
@@ -454,12 +527,20 @@ __global__ void k_ccd_ee(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vins
     bool cap = false;
     ++nacc;
     R toi = accd_toi<R>(x0, dd, R(0), R(1.25), R(0.01), max_iter, 1, &cap);
-    ncap += cap ? 1u : 0u;
-    tloc = fminf(tloc, (float)(toi / R(1.25)));
+    const float tt = (float)(toi / R(1.25));
+#pragma unroll
+    for (int q = 0; q < CCD_CHUNK; ++q)
+      if (q >= i0) {
+        tloc[q] = fminf(tloc[q], tt);
+        ncap[q] += cap ? 1u : 0u;
+      }
   });
   if (!ok) atomicOr(status, ST_STACK_OVERFLOW);
-  if (tloc < 1.f) atomic_min_pos(red + RED_STRIDE * k + 2, tloc);
-  if (ncap) atomicAdd(red + RED_STRIDE * k + 3, ncap);
+#pragma unroll
+  for (int i = 0; i < CCD_CHUNK; ++i) {
+    if (i < np && tloc[i] < 1.f) atomic_min_pos(ccd_slot(acc, k, i), tloc[i]);
+    if (i < np && ncap[i]) atomicAdd(ccd_slot(acc, k, i) + 1, ncap[i]);
+  }
   if (nleaf) atomicAdd(red + RED_STRIDE * k + 7, nleaf);
   if (nacc) atomicAdd(red + RED_STRIDE * k + 8, nacc);
 }
@@ -513,35 +594,57 @@ int ccd_step(Scene& s, uint32_t active, float* t_out, uint32_t* cap_hits) {
     cudaEvent_t ev3[3];
     if (trace)
       for (auto& e : ev3) MG_CUDA(cudaEventCreate(&e));
-    for (int pass = 0; pass < 64 && todo; ++pass) {
+    MG_TRY(s.ccd_acc.reserve(2 * CCD_CHUNK * PCG_MAX_INST));
+    std::vector<unsigned int> acc0(2 * CCD_CHUNK * PCG_MAX_INST), acc(2 * CCD_CHUNK * PCG_MAX_INST);
+    for (int i = 0; i < CCD_CHUNK * PCG_MAX_INST; ++i) {
+      acc0[2 * i] = f2u_host(1.f);
+      acc0[2 * i + 1] = 0u;
+    }
+    // launch 0 runs the schedule's first pass alone (often decisive, and cheap); each later
+    // launch runs up to CCD_CHUNK further passes of every undecided instance in one traversal
+    float sched[PCG_MAX_INST][CCD_CHUNK];
+    for (int launch = 0; launch < 64 && todo; ++launch) {
       if (trace) MG_CUDA(cudaEventRecord(ev3[0], st));
       CcdPass cp{};
       cp.todo = todo;
       for (uint32_t k = 0; k < K; ++k) {
-        cp.search[k] = fixed + 2.0f * allowed[k];
-        MG_CUDA(cudaMemcpyAsync(s.red.p + RED_STRIDE * k + 2, &init[RED_STRIDE * k + 2], 8, cudaMemcpyHostToDevice, st));
+        if (!((todo >> k) & 1u)) continue;
+        float a_ = allowed[k];
+        uint32_t n = 0;
+        for (;;) {
+          sched[k][n] = a_;
+          cp.search[k][n] = fixed + 2.0f * a_;
+          ++n;
+          if (launch == 0 || n == (uint32_t)CCD_CHUNK || a_ >= max_disp[k]) break;
+          a_ = std::min(a_ * 4.0f, max_disp[k]);
+        }
+        cp.npass[k] = n;
       }
+      MG_CUDA(cudaMemcpyAsync(s.ccd_acc.p, acc0.data(), 4 * acc0.size(), cudaMemcpyHostToDevice, st));
       if (s.mixed) {
         k_ccd_vt<double><<<ceil_div(s.nv, 128), 128, 0, st>>>(
             tv, cp, s.vinst.p, s.x.p, s.dx.p, s.tris.p, s.collider_tri.p, s.inv_mass.p, s.ex_ptr.p, s.ex_list.p,
-            s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.red.p, s.status.p);
+            s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.red.p, s.ccd_acc.p,
+            s.status.p);
         if (trace) MG_CUDA(cudaEventRecord(ev3[1], st));
         if (s.n_edge)
           k_ccd_ee<double><<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, cp, s.vinst.p, s.x.p, s.dx.p, s.edges.p,
                                                                    s.inv_mass.p, s.n_edge, iters, s.red.p,
-                                                                   s.status.p);
+                                                                   s.ccd_acc.p, s.status.p);
       } else {
         k_ccd_vt<float><<<ceil_div(s.nv, 128), 128, 0, st>>>(
             tv, cp, s.vinst.p, s.x.p, s.dx.p, s.tris.p, s.collider_tri.p, s.inv_mass.p, s.ex_ptr.p, s.ex_list.p,
-            s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.red.p, s.status.p);
+            s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.red.p, s.ccd_acc.p,
+            s.status.p);
         if (trace) MG_CUDA(cudaEventRecord(ev3[1], st));
         if (s.n_edge)
           k_ccd_ee<float><<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, cp, s.vinst.p, s.x.p, s.dx.p, s.edges.p,
                                                                   s.inv_mass.p, s.n_edge, iters, s.red.p,
-                                                                  s.status.p);
+                                                                  s.ccd_acc.p, s.status.p);
       }
       MG_CUDA(cudaGetLastError());
       if (trace) MG_CUDA(cudaEventRecord(ev3[2], st));
+      MG_CUDA(cudaMemcpyAsync(acc.data(), s.ccd_acc.p, 4 * acc.size(), cudaMemcpyDeviceToHost, st));
       MG_CUDA(cudaMemcpyAsync(h.data(), s.red.p, 4 * h.size(), cudaMemcpyDeviceToHost, st));
       MG_CUDA(cudaStreamSynchronize(st));
       if (trace) {
@@ -555,20 +658,23 @@ int ccd_step(Scene& s, uint32_t active, float* t_out, uint32_t* cap_hits) {
           le += h[RED_STRIDE * k + 7];
           ae += h[RED_STRIDE * k + 8];
         }
-        fprintf(stderr, "[mguso]   ccd pass %d todo %x: vt %.3f ms (leaves %llu, accd %llu), ee %.3f ms (leaves %llu, accd %llu)\n",
-                pass, todo, ms_vt, lv, av, ms_all - ms_vt, le, ae);
+        fprintf(stderr, "[mguso]   ccd launch %d todo %x passes %u: vt %.3f ms (leaves %llu, accd %llu), ee %.3f ms "
+                "(leaves %llu, accd %llu)\n", launch, todo, cp.npass[0], ms_vt, lv, av, ms_all - ms_vt, le, ae);
       }
       for (uint32_t k = 0; k < K; ++k) {
         if (!((todo >> k) & 1u)) continue;
-        const bool full = allowed[k] >= max_disp[k];
-        const float t_self = u2f_host(h[RED_STRIDE * k + 2]);
-        cap_hits[k] = h[RED_STRIDE * k + 3];
-        if (full || t_self * max_disp[k] <= allowed[k]) {
-          t_out[k] = std::min(t_out[k], t_self);
-          todo &= ~(1u << k);
-        } else {
-          allowed[k] = std::min(allowed[k] * 4.0f, max_disp[k]);
+        bool settled = false;
+        for (uint32_t i = 0; i < cp.npass[k] && !settled; ++i) {
+          const bool full = sched[k][i] >= max_disp[k];
+          const float t_self = u2f_host(acc[2 * (CCD_CHUNK * k + i)]);
+          if (full || t_self * max_disp[k] <= sched[k][i]) {
+            cap_hits[k] = acc[2 * (CCD_CHUNK * k + i) + 1];
+            t_out[k] = std::min(t_out[k], t_self);
+            todo &= ~(1u << k);
+            settled = true;
+          }
         }
+        if (!settled) allowed[k] = std::min(sched[k][cp.npass[k] - 1] * 4.0f, max_disp[k]);
       }
     }
     if (trace)

@@ -163,6 +163,7 @@ struct Scene {
 
   // reductions / CCD
   DevBuf<unsigned int> red;                 // per-iteration reductions (float bits), RED_STRIDE per instance
+  DevBuf<unsigned int> ccd_acc;             // CCD per (instance, pass): step fraction bits, caps
   DevBuf<uint32_t> status;
 
   // linear solve
