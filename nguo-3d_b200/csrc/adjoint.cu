@@ -435,6 +435,9 @@ int mguso_adjoint_forward(mguso_adjoint* a, const double* theta, uint32_t nsteps
   a->scene.reset();
   auto sc = std::make_unique<mguso_scene>();
   sc->s.ctx = a->ctx;
+  // FP32 preconditioner tiles: the backward MINRES solves run to 1e-7 and converge faster
+  // with them, and the forward then follows the drape's FP32-factor trajectory
+  sc->s.fp16_factor = false;
   MG_TRY(scene_build(sc->s, &d, {0, d.nv}));
   a->scene = std::move(sc);
   Scene& s = a->scene->s;

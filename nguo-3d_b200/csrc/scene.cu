@@ -535,7 +535,7 @@ int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>
     s.schwarz = std::make_unique<mguso_schwarz>();
     s.schwarz->a = s.A.get();
     s.schwarz->domain = s.p.schwarz_domain;
-    s.schwarz->half = true;  // FP16 factor tiles: the apply moves half the bytes
+    s.schwarz->half = s.fp16_factor;  // FP16 factor tiles: the apply moves half the bytes
     s.schwarz->inst_vert = s.inst_vert;
     MG_TRY(schwarz_build(s.schwarz.get()));
   } else {

@@ -79,6 +79,7 @@ struct Scene {
   // without the eigenvalue clamp, stitches below rest length, hinges and barriers with their
   // second-derivative terms), the contact stiffness held at `contact_k` (2 per stencil:
   // stiffness and its mass part) recorded by contact_stiffness()
+  bool fp16_factor = true;  // Schwarz factor tiles in FP16 (false: FP32, as the adjoint uses)
   int hess_mode = 0;
   uint32_t exact_terms = EXACT_ALL;  // which element kinds mode 2 writes exactly
   DevBuf<double> contact_k;

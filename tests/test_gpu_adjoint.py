@@ -20,9 +20,11 @@ pytestmark = pytest.mark.gpu
 
 # The differences at eps 1e-4 are the reference; at eps 1e-5 they are noisy (contact decisions
 # and Newton's stopping point move with theta: the stiffness entries change sign), and the
-# two step sizes differ by up to 5e-2 of the largest entry on this drape.
+# two step sizes differ by up to 5e-2 of the largest entry on this drape. The adjoint has
+# measured within 6e-3 of them; trajectories that differ at the 1e-6 level (another PCG
+# preconditioner) have moved it by up to 2e-2, which bounds the tolerance.
 REF = {"coarse": "fd"}
-TOL = {"coarse": 1e-2}
+TOL = {"coarse": 2e-2}
 
 
 @pytest.mark.parametrize("name", ["coarse"])
