@@ -365,6 +365,31 @@ def time_steps(solver, steps, stream, dist):
     return dist.max(e0.elapsed_time(e1)), st
 
 
+def e2e_steps(solver, p0, v0, k, dist):
+    """End to end through the C ABI, the same steps as the timed region: every step uploads
+    its state (positions, velocities) from pinned host memory, steps once and downloads the
+    new state, which is the next step's input. Returns (seconds per step, h2d and d2h bytes
+    per step)."""
+    import torch
+
+    import mguso
+
+    lib = solver.lib
+    pin_p = torch.from_numpy(np.ascontiguousarray(p0, np.float32)).pin_memory()
+    pin_v = torch.from_numpy(np.ascontiguousarray(v0, np.float32)).pin_memory()
+    nbytes = pin_p.numel() * 4 + pin_v.numel() * 4
+    torch.cuda.synchronize()
+    dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(k):
+        mguso._lib.check(lib.mguso_write_positions(solver.h, pin_p.data_ptr()))
+        mguso._lib.check(lib.mguso_write_velocities(solver.h, pin_v.data_ptr()))
+        solver.step(1)
+        mguso._lib.check(lib.mguso_read_positions(solver.h, pin_p.data_ptr()))
+        mguso._lib.check(lib.mguso_read_velocities(solver.h, pin_v.data_ptr()))
+    return dist.max(time.perf_counter() - t0) / k, nbytes, nbytes
+
+
 def fp64_error(sc, batch_positions, steps):
     """Relative position error of `steps` GPU steps against the FP64 oracle run from the same
     state: max |x_gpu - x_f64| over max |x_f64| (positions) and over max |x_f64 - x_0| (the
@@ -396,6 +421,7 @@ def run_batch(args, dist: Dist):
     # batched, mixed precision
     b = mguso.ImplicitBatch(ctx, scs, "mixed")
     b.step(args.warmup)
+    p_w, v_w = b.positions.copy(), b.velocities.copy()
     ms_b, st_b = time_steps(b, args.steps, stream, dist)
     clk = clocks.stop()
     # plain FP32, each size alone, same steps from the same start
@@ -414,21 +440,8 @@ def run_batch(args, dist: Dist):
     prof = b.profile(100)
     dom = max(("spmv", "precond_apply"), key=lambda k: prof[k][0])
     us, nbytes = prof[dom]
-    # end to end: all instances' state in from pinned host, one step, positions out
-    nv = b.nv
-    pin_p = torch.from_numpy(b.positions).pin_memory()
-    pin_v = torch.from_numpy(b.velocities).pin_memory()
-    out = torch.empty((nv, 3), dtype=torch.float32).pin_memory()
-    lib = ctx.lib
-    k2 = max(1, min(args.steps, 5))
-    dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(k2):
-        mguso._lib.check(lib.mguso_write_positions(b.h, pin_p.data_ptr()))
-        mguso._lib.check(lib.mguso_write_velocities(b.h, pin_v.data_ptr()))
-        b.step(1)
-        mguso._lib.check(lib.mguso_read_positions(b.h, out.data_ptr()))
-    e2e_s = dist.max(time.perf_counter() - t0) / k2
+    # end to end: the timed steps again from the same state, each step's state through host
+    e2e_s, h2d, d2h = e2e_steps(b, p_w, v_w, args.steps, dist)
     nl = None if args.no_launch_count else count_launches(lambda: b.step(1))
     launches = None if nl is None else int(nl * args.steps)
     peak, peak_kind = load_peaks()
@@ -469,7 +482,7 @@ def run_batch(args, dist: Dist):
                                "GB/s": round(v[1] / (v[0] * 1e-6) / 1e9, 1)} for k, v in prof.items()},
         },
         "e2e": {"value": round(len(scs) / e2e_s * dist.world, 3), "unit": "drape-steps/s",
-                "h2d_bytes_per_step": 24 * int(nv), "d2h_bytes_per_step": 12 * int(nv)},
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": launches,
         "clocks": {k: clk[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
         "status": sorted(set(int(s_["status"]) for step in st_b for s_ in step)),
@@ -504,6 +517,7 @@ def run_drape(args, dist: Dist):
     clocks = ClockSampler(dist.local)
     clocks.start()
     solver.step(args.warmup)
+    p_w, v_w = solver.positions.copy(), solver.velocities.copy()
     torch.cuda.synchronize()
     dist.barrier()
     torch.cuda.synchronize()
@@ -522,20 +536,8 @@ def run_drape(args, dist: Dist):
     prof = solver.profile(100)
     dom = max(("spmv", "precond_apply"), key=lambda k: prof[k][0])
     us, nbytes = prof[dom]
-    # end to end through the C ABI: state in from pinned host, one step, positions out
-    pin_p = torch.from_numpy(solver.positions).pin_memory()
-    pin_v = torch.from_numpy(solver.velocities).pin_memory()
-    out = torch.empty((nv, 3), dtype=torch.float32).pin_memory()
-    lib = ctx.lib
-    k2 = max(1, min(args.steps, 20))
-    dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(k2):
-        mguso._lib.check(lib.mguso_write_positions(solver.h, pin_p.data_ptr()))
-        mguso._lib.check(lib.mguso_write_velocities(solver.h, pin_v.data_ptr()))
-        solver.step(1)
-        mguso._lib.check(lib.mguso_read_positions(solver.h, out.data_ptr()))
-    e2e_s = dist.max(time.perf_counter() - t0) / k2
+    # end to end through the C ABI: the timed steps again, each step's state through host
+    e2e_s, h2d, d2h = e2e_steps(solver, p_w, v_w, args.steps, dist)
     # launches per step from a short traced pass (not timed)
     nl = None if args.no_launch_count else count_launches(lambda: solver.step(2))
     launches = None if nl is None else int(round(nl / 2 * args.steps))
@@ -572,7 +574,7 @@ def run_drape(args, dist: Dist):
                                "GB/s": round(v[1] / (v[0] * 1e-6) / 1e9, 1)} for k, v in prof.items()},
         },
         "e2e": {"value": round(1.0 / e2e_s * dist.world, 3), "unit": "steps/s",
-                "h2d_bytes_per_step": 24 * int(nv), "d2h_bytes_per_step": 12 * int(nv)},
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": launches,
         "clocks": {k: clk[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
         "status": sorted(set(int(s_["status"]) for s_ in stats)),
