@@ -463,7 +463,7 @@ def run_batch(args, dist: Dist):
         "config": {
             "workload": "config 3: sheath graded XS..XXL (panel widths 0.50-0.75 m) on 6 torsos scaled 0.9-1.2, "
                         "one batch, per-instance Newton/CCD/PCG convergence",
-            "triangles_per_size": ntri, "vertices_total": int(nv),
+            "triangles_per_size": ntri, "vertices_total": int(b.nv),
             "drapes_per_s": round(value / 120.0, 4),
             "plain_fp32_per_size_drape_steps_per_s": round(plain, 3),
             "batched_mixed_over_plain_fp32": round(value / plain, 3),
