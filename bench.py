@@ -153,7 +153,7 @@ class Dist:
 
 
 # ---------------------------------------------------------------------------------------
-# workload: BSR SpMV (config 2a)
+# workload: BSR SpMV + Schwarz apply on the 1024x1024 cloth grid
 # ---------------------------------------------------------------------------------------
 def spmv_bytes(nb: int, nnzb: int) -> int:
     """Algorithmic bytes of one FP32 BSR SpMV: values 36/block, column 4/block, row_ptr,
@@ -275,7 +275,7 @@ def run_spmv(args, dist: Dist):
         "dtype": "f32",
         "data": "synthetic (seeded N(0,1) SPD blocks on the 1024^2 cloth-grid pattern)",
         "config": {
-            "workload": "BSR SpMV, 1024x1024 cloth grid stiffness pattern (config 2a)",
+            "workload": "BSR SpMV, 1024x1024 cloth grid stiffness pattern",
             "block_rows": nb, "nnzb": a.nnzb, "bytes_per_apply": nbytes,
             "l2": "inputs larger than L2 (293 MB of blocks+columns streamed per step; x gathered from L2)",
             "parallelism": f"replicas x{dist.world}",
@@ -309,11 +309,11 @@ def drape_scene(which: str):
     from mguso import scenes
 
     if which == "batch":
-        return scenes.graded_sheaths()[0], "XS size of the graded sheath (config 3), 1 of 6 instances"
+        return scenes.graded_sheaths()[0], "XS size of the graded sheath (0.50 m panels, torso scaled 0.9), 1 of 6 instances"
     if which == "sheet":
-        return scenes.sheet_on_sphere(64), "64x64 sheet (7938 tris) on r=0.3 m sphere, 36-step drape (config 0)"
+        return scenes.sheet_on_sphere(64), "64x64 sheet (7938 tris) on r=0.3 m sphere, 36-step drape"
     sc = scenes.sheath_on_torso()
-    return sc, "seamed sheath 41400 tris + 278 stitches on 19800-tri torso, 120-step drape (config 1)"
+    return sc, "seamed sheath 41400 tris + 278 stitches on 19800-tri torso, 120-step drape"
 
 
 def cpu_drape_sample(which: str, seconds: float):
@@ -404,7 +404,7 @@ def fp64_error(sc, batch_positions, steps):
 
 
 def run_batch(args, dist: Dist):
-    """Configuration 3: the sheath graded into 6 sizes on 6 scaled torsos, stepped as one
+    """The sheath graded into 6 sizes on 6 scaled torsos, stepped as one
     mixed-precision batch, against the plain FP32 path stepping each size alone."""
     import torch
 
@@ -461,7 +461,7 @@ def run_batch(args, dist: Dist):
         "dtype": "f32+f64(dots,norms,spmv/precond accumulation,barrier,ccd)",
         "data": "synthetic (seeded meshes; no dataset)",
         "config": {
-            "workload": "config 3: sheath graded XS..XXL (panel widths 0.50-0.75 m) on 6 torsos scaled 0.9-1.2, "
+            "workload": "sheath graded XS..XXL (panel widths 0.50-0.75 m) on 6 torsos scaled 0.9-1.2, "
                         "one batch, per-instance Newton/CCD/PCG convergence",
             "triangles_per_size": ntri, "vertices_total": int(b.nv),
             "drapes_per_s": round(value / 120.0, 4),
@@ -597,7 +597,7 @@ def run_reference(args, dist: Dist):
             "impl": "reference", "metric": METRIC, "value": round(gbs, 3), "unit": "GB/s",
             "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": {"workload": "BSR SpMV, 1024x1024 cloth grid stiffness pattern (config 2a)"},
+            "data": "synthetic", "config": {"workload": "BSR SpMV, 1024x1024 cloth grid stiffness pattern"},
             "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": 1, "kind": "port", "sample": sample},
             "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }

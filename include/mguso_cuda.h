@@ -286,7 +286,7 @@ int mguso_batch_create(mguso_ctx* ctx, const mguso_scene_desc* descs, uint32_t n
 /* Number of instances and their vertex offsets (u32[n + 1]; may be NULL). */
 int mguso_scene_instances(mguso_scene* s, uint32_t* n, uint32_t* vert_offsets);
 
-/* ---- Adjoint of an N-step drape (configuration 4) ------------------------------------- */
+/* ---- Adjoint of an N-step drape ------------------------------------------------------- */
 /* Gradients of a loss on the final positions with respect to sewing-pattern parameters, as a
  * forward/backward pair mirroring torch.autograd.Function (forward(theta) -> x_N,
  * backward(dL/dx_N) -> dL/dtheta). No counterpart in the reference, which has no

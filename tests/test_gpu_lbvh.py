@@ -107,7 +107,7 @@ def test_onesweep_sort_stable(ctx, bits):
 
 
 def test_lbvh_full_size_4m(ctx):
-    """Config 2b size: 4 194 304 triangles. Keys, permutation, tree and boxes bit-exact
+    """4 194 304 triangles (uniform in the unit cube, 2 mm edges). Keys, permutation, tree and boxes bit-exact
     against the oracle; the pair count and a hash of the sorted pair set equal too."""
     pos, tris = scenes.triangle_soup(4 << 20, seed=3)
     for bits in (30, 63):

@@ -63,7 +63,7 @@ def test_spmv_edge_cases(ctx):
 
 
 def test_spmv_full_size_property(ctx):
-    """Config 2a at full size (1024^2 grid, 7 331 842 blocks): GPU y vs float64, and
+    """The 1024^2 cloth grid at full size (7 331 842 blocks): GPU y vs float64, and
     linearity A(x1 + x2) = A x1 + A x2 within FP32 rounding."""
     import torch
     nb, rp, col, val = scenes.grid_bsr(1024, seed=2)

@@ -1,6 +1,6 @@
 """GPU implicit step vs the CPU oracle of the reference's step, through the C ABI.
 
-Per-step parity is judged from identical states: both solvers start every compared step
+Per-step parity is compared from identical states: both solvers start every compared step
 from the same positions and velocities, and the resulting positions must agree within a
 relative tolerance of the step's displacement. Newton iteration counts must agree within
 +-1 over the run."""
