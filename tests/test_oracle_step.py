@@ -251,3 +251,91 @@ def test_self_contact_stencils_are_exact_predicate():
     got_vt = {g for g in got if any(g == w for w in want_vt) or (g[0], g[1], g[2], g[3]) in want_vt}
     assert want_vt <= got
     assert len(got) > len(want_vt)  # edge-edge stencils too
+
+
+def test_stepping_along_the_gradient_changes_the_distance_as_predicted():  # contact.rs:1560-1582
+    pts = [(0.25, 0.25, 0.4), (0, 0, 0), (1, 0, 0), (0, 1, 0)]
+    d0, g, _ = O.point_tri(pts)
+    eps = 1e-3
+    moved = [tuple(np.asarray(pts[0]) + eps * g[0])] + pts[1:]
+    d1, _, _ = O.point_tri(moved)
+    assert abs(d1 - (d0 + eps * float(g[0] @ g[0]))) < 1e-5
+
+
+def test_cubic_barrier_is_finite_and_repulsive_including_penetration():  # contact.rs:1632-1662
+    ghat = 0.1
+    assert O.barrier(0.1, ghat, 1.0, kind="cubic") is None
+    assert O.barrier(0.5, ghat, 1.0, kind="cubic") is None
+    for gap in (0.09, 0.05, 0.01, 0.0, -0.05, -0.5):
+        e, g, c = O.barrier(gap, ghat, 1.0, kind="cubic")
+        assert e > 0 and np.isfinite(e), gap
+        assert g < 0 and np.isfinite(g), gap
+        assert c > 0 and np.isfinite(c), gap
+    e0, _, c0 = O.barrier(1e-9, ghat, 1.0, kind="cubic")
+    assert e0 < 1.0 and c0 <= 4.0 + 1e-5
+    assert O.barrier(-0.2, ghat, 1.0, kind="cubic")[1] < O.barrier(0.01, ghat, 1.0, kind="cubic")[1]
+
+
+def _two_point_stitch(stiffness):
+    pos = np.array([[0, 0, 0], [0.05, 0, 0]], np.float32)
+    return dict(positions=pos, velocities=np.zeros_like(pos), inv_mass=np.array([0.0, 1.0], np.float32),
+                tris=np.zeros((0, 3), np.uint32), shell_faces=np.zeros((0, 3), np.uint32), static_mask=None,
+                stitch_idx=np.array([[0, 0, 0, 1, 1, 1]], np.uint32),
+                stitch_w=np.array([[1, 0, 0, 1, 0, 0]], np.float32),
+                stitch_kl=np.array([[stiffness, 0.001, 0.01]], np.float32),
+                colliders=np.zeros((0, 8), np.float32), params=scenes.default_params(gravity=(0.0, 0.0, 0.0)))
+
+
+def test_a_stitch_closes_the_seam_it_sews():  # implicit.rs:3426-3490
+    o = O.OracleSolver(_two_point_stitch(1.0))
+    st = o.step(400, check_intersection=False)
+    p = o.positions().astype(np.float64)
+    assert np.all(np.isfinite(p)) and len(st) == 400
+    assert abs(np.linalg.norm(p[1] - p[0]) - 0.001) <= 1e-4 * 0.001
+    assert np.linalg.norm(p[0]) < 1e-6
+    # zero stiffness sews nothing
+    o = O.OracleSolver(_two_point_stitch(0.0))
+    o.step(400, check_intersection=False)
+    p = o.positions().astype(np.float64)
+    assert abs(np.linalg.norm(p[1] - p[0]) - 0.05) < 1e-6
+
+
+def _two_layers(n, y_upper, mass, **params):
+    pos, tris = [], []
+    for li, y in ((0, 0.0), (1, y_upper)):
+        base = len(pos)
+        pos += [(i * 0.1, y, j * 0.1) for j in range(n) for i in range(n)]
+        for j in range(n - 1):
+            for i in range(n - 1):
+                v = base + j * n + i
+                r = v + n
+                tris += [(v, v + 1, r), (r, v + 1, r + 1)]
+    pos = np.array(pos, np.float32)
+    im = np.full(len(pos), 1.0 / mass, np.float32)
+    im[: n * n] = 0.0  # the lower layer is pinned
+    si, sw, skl = scenes._empty_stitches()
+    return dict(positions=pos, velocities=np.zeros_like(pos), inv_mass=im, tris=np.array(tris, np.uint32),
+                shell_faces=np.zeros((0, 3), np.uint32), static_mask=None, stitch_idx=si, stitch_w=sw,
+                stitch_kl=skl, colliders=np.zeros((0, 8), np.float32),
+                params=scenes.default_params(self_collision=1, **params)), n * n
+
+
+def test_self_collision_holds_resting_contact():  # implicit.rs:4294-4345
+    sc, lower = _two_layers(5, 0.018, 0.02, dt=1.0 / 480.0, stiffness=500.0, gravity=(0.0, -4.0, 0.0),
+                            contact_dhat=0.02, contact_kappa=2.0e3)
+    o = O.OracleSolver(sc)
+    o.step(300)
+    p = o.positions()
+    assert np.all(np.isfinite(p))
+    assert p[lower:, 1].min() > -0.005
+
+
+def test_self_collision_rayleigh_stiffness_holds_a_heavy_resting_contact():  # implicit.rs:4359-4412
+    sc, lower = _two_layers(4, 0.02, 0.1, dt=1.0 / 240.0, stiffness=500.0, gravity=(0.0, -9.8, 0.0),
+                            contact_dhat=0.02, contact_kappa=1.0e2)
+    o = O.OracleSolver(sc)
+    st = o.step(200)
+    p = o.positions()
+    assert np.all(np.isfinite(p))
+    assert all(s["penetration_free"] for s in st)  # no self-intersection develops
+    assert p[lower:, 1].min() > -0.01
