@@ -276,6 +276,13 @@ def test_cubic_barrier_is_finite_and_repulsive_including_penetration():  # conta
     assert O.barrier(-0.2, ghat, 1.0, kind="cubic")[1] < O.barrier(0.01, ghat, 1.0, kind="cubic")[1]
 
 
+def reference_defaults(**kw):
+    """ImplicitParams::default() (implicit.rs:176-229) in this library's parameter names."""
+    return scenes.default_params(**dict(dict(newton_iters=4, stiffness=1.0e3, bend_stiffness=0.0,
+                                             contact_dhat=1.0e-2, contact_kappa=1.0e2, contact_rayleigh=0,
+                                             self_collision=0), **kw))
+
+
 def _two_point_stitch(stiffness):
     pos = np.array([[0, 0, 0], [0.05, 0, 0]], np.float32)
     return dict(positions=pos, velocities=np.zeros_like(pos), inv_mass=np.array([0.0, 1.0], np.float32),
@@ -283,7 +290,7 @@ def _two_point_stitch(stiffness):
                 stitch_idx=np.array([[0, 0, 0, 1, 1, 1]], np.uint32),
                 stitch_w=np.array([[1, 0, 0, 1, 0, 0]], np.float32),
                 stitch_kl=np.array([[stiffness, 0.001, 0.01]], np.float32),
-                colliders=np.zeros((0, 8), np.float32), params=scenes.default_params(gravity=(0.0, 0.0, 0.0)))
+                colliders=np.zeros((0, 8), np.float32), params=reference_defaults(gravity=(0.0, 0.0, 0.0)))
 
 
 def test_a_stitch_closes_the_seam_it_sews():  # implicit.rs:3426-3490
@@ -317,7 +324,7 @@ def _two_layers(n, y_upper, mass, **params):
     return dict(positions=pos, velocities=np.zeros_like(pos), inv_mass=im, tris=np.array(tris, np.uint32),
                 shell_faces=np.zeros((0, 3), np.uint32), static_mask=None, stitch_idx=si, stitch_w=sw,
                 stitch_kl=skl, colliders=np.zeros((0, 8), np.float32),
-                params=scenes.default_params(self_collision=1, **params)), n * n
+                params=reference_defaults(self_collision=1, **params)), n * n
 
 
 def test_self_collision_holds_resting_contact():  # implicit.rs:4294-4345
@@ -339,3 +346,43 @@ def test_self_collision_rayleigh_stiffness_holds_a_heavy_resting_contact():  # i
     assert np.all(np.isfinite(p))
     assert all(s["penetration_free"] for s in st)  # no self-intersection develops
     assert p[lower:, 1].min() > -0.01
+
+
+def _vertex_over_triangle(z):
+    pos = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0.3, 0.3, z]], np.float32)
+    si, sw, skl = scenes._empty_stitches()
+    return dict(positions=pos, velocities=np.zeros_like(pos), inv_mass=np.array([0, 0, 0, 1], np.float32),
+                tris=np.array([[0, 1, 2]], np.uint32), shell_faces=np.zeros((0, 3), np.uint32), static_mask=None,
+                stitch_idx=si, stitch_w=sw, stitch_kl=skl, colliders=np.zeros((0, 8), np.float32),
+                params=reference_defaults(self_collision=1, contact_dhat=0.02))
+
+
+@pytest.mark.parametrize("z, step", [(0.05, -0.2), (4.0, -8.0)])
+def test_ccd_clamps_a_step_toward_a_triangle(z, step):  # implicit.rs:4634-4668, 4722-4760
+    o = O.OracleSolver(_vertex_over_triangle(z))
+    dx = np.zeros((4, 3), np.float32)
+    dx[3, 2] = step
+    t = o.ccd(dx)
+    assert t < 1.0
+    assert z + t * step > 0.0
+
+
+def test_implicit_hanging_cloth_is_stable():  # implicit.rs:4806-4834
+    n = 6
+    pos = np.array([(i * 0.1, 1.0, j * 0.1) for j in range(n) for i in range(n)], np.float32)
+    tris = []
+    for j in range(n - 1):
+        for i in range(n - 1):
+            v = j * n + i
+            tris += [(v, v + 1, v + n), (v + n, v + 1, v + n + 1)]
+    im = np.full(n * n, 1.0 / 0.05, np.float32)
+    im[0] = im[n - 1] = 0.0
+    si, sw, skl = scenes._empty_stitches()
+    sc = dict(positions=pos, velocities=np.zeros_like(pos), inv_mass=im, tris=np.array(tris, np.uint32),
+              shell_faces=np.zeros((0, 3), np.uint32), static_mask=None, stitch_idx=si, stitch_w=sw,
+              stitch_kl=skl, colliders=np.zeros((0, 8), np.float32), params=reference_defaults())
+    o = O.OracleSolver(sc)
+    o.step(120)
+    p = o.positions()
+    assert np.all(np.isfinite(p))
+    assert p[n // 2 * n + n // 2, 1] < 1.0  # it hangs: the middle has fallen
