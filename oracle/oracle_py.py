@@ -222,6 +222,7 @@ def _step_sigs(lib):
         "oracle_accd": (f32, [vp, vp, f32, f32, f32, u32, i32]),
         "oracle_barrier": (i32, [i32, C.c_double, C.c_double, C.c_double, i32, vp]),
         "oracle_rayleigh": (f32, [i32, vp, vp, vp, vp, f32]),
+        "oracle_friction": (i32, [vp, vp, vp, f32, f32, vp, vp]),
         "oracle_shell": (i32, [i32, vp, vp, C.c_double, C.c_double, C.c_double, vp, vp, vp]),
         "oracle_hinge": (C.c_double, [i32, vp, vp, vp]),
         "oracle_stitch": (None, [vp, vp, C.c_double, C.c_double, vp, vp]),
@@ -375,6 +376,18 @@ def barrier(d, dhat, kappa, kind="log", f64=False):
     out = np.zeros(3, np.float64)
     on = lib.oracle_barrier(0 if kind == "log" else 1, d, dhat, kappa, 1 if f64 else 0, _p(out))
     return (tuple(out.tolist()) if on else None)
+
+
+def friction(force_contact, dx, normal, mu, eps):
+    """contact.rs friction: (gradient 3, Hessian 3x3), zeros when it does not apply."""
+    lib = _lib_elem()
+    f = np.ascontiguousarray(force_contact, np.float32)
+    d = np.ascontiguousarray(dx, np.float32)
+    n = np.ascontiguousarray(normal, np.float32)
+    g = np.zeros(3, np.float32)
+    h = np.zeros(9, np.float32)
+    lib.oracle_friction(_p(f), _p(d), _p(n), mu, eps, _p(g), _p(h))
+    return g, h.reshape(3, 3)
 
 
 def rayleigh(elastic, mass, weights, e, offset=0.0):

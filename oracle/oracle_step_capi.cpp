@@ -371,6 +371,19 @@ int oracle_barrier(int kind, double d, double dhat, double kappa, int f64, doubl
   return on;
 }
 
+// friction (contact.rs:613-644) in f32: gradient g3 and Hessian h9 (row-major); 0 when
+// nothing applies (mu <= 0 or a separating contact), with g3/h9 zeroed.
+int oracle_friction(const float* fc3, const float* dx3, const float* n3, float mu, float eps, float* g3, float* h9) {
+  Vt<float> g;
+  float h[3][3] = {};
+  bool on = friction<float>(Vt<float>(fc3[0], fc3[1], fc3[2]), Vt<float>(dx3[0], dx3[1], dx3[2]),
+                            Vt<float>(n3[0], n3[1], n3[2]), mu, eps, g, h);
+  for (int c = 0; c < 3; ++c) g3[c] = on ? g[c] : 0.f;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) h9[3 * r + c] = on ? h[r][c] : 0.f;
+  return on;
+}
+
 float oracle_rayleigh(int n, const float* elastic, const float* mass, const float* weights, const float* e3,
                       float offset) {
   float el[16][9];

@@ -386,3 +386,44 @@ def test_implicit_hanging_cloth_is_stable():  # implicit.rs:4806-4834
     p = o.positions()
     assert np.all(np.isfinite(p))
     assert p[n // 2 * n + n // 2, 1] < 1.0  # it hangs: the middle has fallen
+
+
+def test_friction_is_tangential_opposes_slip_and_respects_coulomb():  # contact.rs:2112-2172
+    n = np.array([0, 1, 0], np.float32)
+    f_c = -10.0 * n
+    mu, eps = 0.4, 1e-3
+    contact = -float(n @ f_c)
+    slip = np.array([0.05, 0.02, -0.03], np.float32)
+    g, h = O.friction(f_c, slip, n, mu, eps)
+    assert abs(float(g @ n)) < 1e-5
+    pdx = slip - float(n @ slip) * n
+    assert float(g @ pdx) > 0
+    assert abs(np.linalg.norm(g) - mu * contact) < 1e-3 * mu * contact
+    assert np.abs(h - h.T).max() < 1e-6
+    for t in range(8):
+        x = np.array([(t * 7919 % 100) / 50 - 1, (t * 104729 % 100) / 50 - 1, (t * 1299709 % 100) / 50 - 1])
+        assert x @ h @ x >= -1e-5
+    g0, h0 = O.friction(f_c, slip, n, 0.0, eps)
+    assert not g0.any() and not h0.any()
+
+
+def test_friction_regularization_caps_tiny_slip():  # contact.rs:2174-2204
+    n = np.array([0, 1, 0], np.float32)
+    f_c = -10.0 * n
+    mu, eps = 0.5, 1e-3
+    bound = mu * -float(n @ f_c)
+    prev = 0.0
+    for k in range(6):
+        s = 1e-6 * 10.0 ** k
+        g, _ = O.friction(f_c, np.array([s, 0, 0], np.float32), n, mu, eps)
+        m = float(np.linalg.norm(g))
+        assert np.isfinite(m) and m <= bound + 1e-4 and m >= prev - 1e-6
+        prev = m
+        if s < eps:
+            assert abs(m - bound * s / eps) < 1e-3 * max(bound, 1.0)
+
+
+def test_friction_vanishes_without_normal_force():  # contact.rs:2206-2214
+    n = np.array([0, 1, 0], np.float32)
+    g, h = O.friction(5.0 * n, np.array([0.1, 0, 0], np.float32), n, 0.5, 1e-3)
+    assert not g.any() and not h.any()
