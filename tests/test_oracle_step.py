@@ -427,3 +427,47 @@ def test_friction_vanishes_without_normal_force():  # contact.rs:2206-2214
     n = np.array([0, 1, 0], np.float32)
     g, h = O.friction(5.0 * n, np.array([0.1, 0, 0], np.float32), n, 0.5, 1e-3)
     assert not g.any() and not h.any()
+
+
+def test_a_degenerate_stitch_source_reduces_to_a_single_vertex():  # stitch.rs:256-282
+    p = np.zeros(3)
+    t1, t2 = np.array([0.003, 0.001, 0.0]), np.array([0.013, 0.001, 0.0])
+    x = np.array([p, p, p, t1, t2, t2])
+    w = np.array([1.0, 0.0, 0.0, 0.75, 0.25, 0.0])
+    g, _ = O.stitch(x, w, 0.001, 0.01)
+    t = p - (0.75 * t1 + 0.25 * t2)
+    l = min(np.linalg.norm(t), 0.01)
+    dedt = (l / 0.001 - 1.0) * (t / l)
+    n = np.linalg.norm(dedt)
+    assert np.linalg.norm(g[0] - dedt) <= 1e-4 * n
+    assert np.linalg.norm(g[1]) < 1e-9 and np.linalg.norm(g[2]) < 1e-9
+    assert np.linalg.norm(g[3] + 0.75 * dedt) <= 1e-4 * n
+    assert np.linalg.norm(g[4] + 0.25 * dedt) <= 1e-4 * n
+    assert np.linalg.norm(g[5]) < 1e-9
+
+
+def test_beyond_the_stitch_cap_the_pull_grows_linearly():  # stitch.rs:284-305
+    w = np.array([1.0, 0, 0, 1.0, 0, 0])
+
+    def mag(sep):
+        x = np.array([[0, 0, 0]] * 3 + [[sep, 0, 0]] * 3, np.float64)
+        return np.linalg.norm(O.stitch(x, w, 0.001, 0.01)[0][0])
+
+    assert abs(mag(0.08) / mag(0.04) - 2.0) < 1e-3
+
+
+def _flap(fold_deg):
+    a = np.radians(fold_deg)
+    return np.array([[0.5, -1.0, 0.0], [0, 0, 0], [1, 0, 0], [0.5, np.cos(a), np.sin(a)]])
+
+
+def test_folding_changes_the_hinge_angle_monotonically():  # bending.rs:267-272
+    assert abs(O.hinge(_flap(90.0))[0]) > abs(O.hinge(_flap(45.0))[0])
+
+
+def test_the_hinge_gradient_reduces_energy_toward_rest():  # bending.rs:274-290
+    p = _flap(120.0)
+    th0, g, _ = O.hinge(p)
+    step = 1e-3 * np.sign(th0)
+    th1 = O.hinge(p - g * step * 50.0)[0]
+    assert abs(th1) < abs(th0)
