@@ -1,0 +1,201 @@
+"""The capture reader and OBJ writer (mguso.capture) on synthetic captures, with the
+reference reader's own parsing tests (engine-io/src/golden.rs:1926-2062) restated."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle_py as O
+from mguso import capture as cap
+
+
+def _f64(vals):
+    return np.asarray(vals, "<f8").tobytes()
+
+
+def _f32(vals):
+    return np.asarray(vals, "<f4").tobytes()
+
+
+def _u64(vals):
+    return np.asarray(vals, "<u8").tobytes()
+
+
+def test_decodes_synthetic_buffers():  # golden.rs:1926-1949
+    assert cap.decode_vec3_f64(_f64([1, 2, 3, -4, 5.5, 6.25])).tolist() == [[1, 2, 3], [-4, 5.5, 6.25]]
+    assert cap.decode_vec3_f32(_f32([0.5, -0.25, 10.0])).tolist() == [[0.5, -0.25, 10.0]]
+    assert cap.decode_tris_u64(_u64([0, 1, 2, 2, 1, 3])).tolist() == [[0, 1, 2], [2, 1, 3]]
+
+
+def test_rejects_misaligned_and_oversized():  # golden.rs:2053-2061
+    with pytest.raises(cap.CaptureError):
+        cap.decode_vec3_f64(bytes(23))
+    with pytest.raises(cap.CaptureError):
+        cap.decode_vec3_f32(bytes(10))
+    with pytest.raises(cap.CaptureError):
+        cap.decode_tris_u64(_u64([2 ** 32]) + bytes(16))
+
+
+def test_compare_identical_is_zero_and_passes():  # golden.rs:1951-1959
+    f = [[0, 0, 0], [1, 0, 0], [0, 1, 0]]
+    r = cap.compare_frames(f, f)
+    assert r.max_rel == 0 and r.rms == 0 and r.centroid_rel == 0 and r.passes()
+
+
+def test_compare_known_offset():  # golden.rs:1961-1977
+    ref = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32)
+    g = cap.compare_frames(ref + [0.1, 0, 0], ref)
+    d = np.sqrt(2.0)
+    assert abs(g.diagonal - d) < 1e-5
+    for v in (g.max_rel, g.rms, g.centroid_rel):
+        assert abs(v - 0.1 / d) < 1e-5
+    assert not g.passes()  # rms 0.0707 exceeds the 2e-2 gate
+
+
+def test_compare_length_mismatch_errors():  # golden.rs:1979-1982
+    with pytest.raises(cap.CaptureError):
+        cap.compare_frames([[0, 0, 0]], [[0, 0, 0], [1, 1, 1]])
+
+
+def test_parses_param_toml_from_text(tmp_path):  # golden.rs:1984-2001
+    (tmp_path / "param.toml").write_text('[param]\ndt = 0.001\nfps = 60.0\nframes = 200\n'
+                                         'gravity = [0.0, -9.8, 0.0]\nworld_scaling = 2.0\nbarrier = "cubic"\n'
+                                         'friction_mode = "max"\ncg_tol = oops\n')
+    p = cap.read_param_toml(str(tmp_path))
+    assert p["dt"] == 0.001 and p["fps"] == 60.0 and p["frames"] == 200
+    assert p["gravity"] == (0.0, -9.8, 0.0) and p["world_scaling"] == 2.0
+    assert p["cubic_barrier"] and p["friction_mode"] == "max"
+    assert p["cg_tol"] == 1.0e-3  # unparsable: the default stays
+
+
+def test_reads_material_means_from_synthetic(tmp_path):  # golden.rs:2003-2028
+    d = tmp_path / "input_bin" / "param"
+    d.mkdir(parents=True)
+    (d / "tri-young-mod.bin").write_bytes(_f32([100, 100, 100]))
+    (d / "tri-bend.bin").write_bytes(_f32([1, 3]))
+    (d / "tri-density.bin").write_bytes(_f32([1]))
+    (d / "tri-strain-limit.bin").write_bytes(_f32([0.01, 0.03]))
+    m = cap.read_material(str(tmp_path))
+    assert m["young_mod"] == 100 and abs(m["bend"] - 2) < 1e-6 and m["density"] == 1
+    assert abs(m["strain_limit"] - 0.02) < 1e-6
+    (d / "tri-young-mod.bin").unlink()
+    assert cap.read_material(str(tmp_path)) is None
+
+
+def test_reads_pin_list_from_synthetic(tmp_path):  # golden.rs:2030-2051
+    ib = tmp_path / "input_bin"
+    ib.mkdir()
+    (ib / "pin-ind-0.bin").write_bytes(_u64([10, 13]))
+    (ib / "pin-ind-1.bin").write_bytes(_u64([7]))
+    assert cap.read_pin_indices(str(tmp_path)).tolist() == [10, 13, 7]
+    (ib / "pin-ind-2.bin").write_bytes(bytes(12))
+    with pytest.raises(cap.CaptureError):
+        cap.read_pin_indices(str(tmp_path))
+
+
+def _sheet_capture(root, n=6, with_disp=True, stitches=True):
+    """A small captured sheet: n x n grid at y = 0 in the template, lifted by displacement
+    group 1 (all but the first row), two pinned corners, two stitches."""
+    ib = root / "input_bin"
+    (ib / "param").mkdir(parents=True)
+    v = np.array([(i * 0.1, 0.0, j * 0.1) for j in range(n) for i in range(n)], np.float64)
+    tris = []
+    for j in range(n - 1):
+        for i in range(n - 1):
+            a = j * n + i
+            tris += [(a, a + 1, a + n), (a + n, a + 1, a + n + 1)]
+    (ib / "vert.bin").write_bytes(_f64(v.ravel()))
+    (ib / "tri.bin").write_bytes(_u64(np.ravel(tris)))
+    (ib / "vel.bin").write_bytes(_f32(np.zeros(3 * n * n)))
+    if with_disp:
+        dmap = np.ones(n * n, np.uint32)
+        dmap[:n] = 0
+        (ib / "vert_dmap.bin").write_bytes(dmap.astype("<u4").tobytes())
+        (ib / "displacement.bin").write_bytes(_f64([0, 0, 0, 0, 0.5, 0]))
+    (ib / "pin-ind-0.bin").write_bytes(_u64([n * n - n, n * n - 1]))
+    if stitches:
+        (ib / "stitch_ind.bin").write_bytes(_u64([0, 0, 0, 2, 3, 3, 1, 1, 1, 4, 4, 4]))
+        (ib / "stitch_w.bin").write_bytes(_f32([1, 0, 0, 0.5, 0.5, 0, 1, 0, 0, 1, 0, 0]))
+    (ib / "param" / "tri-young-mod.bin").write_bytes(_f32(np.full(len(tris), 1e5)))
+    (ib / "param" / "tri-density.bin").write_bytes(_f32(np.full(len(tris), 0.2)))
+    (root / "param.toml").write_text("[param]\ndt = 0.004\ngravity = [0.0, -9.8, 0.0]\ncg_tol = 1e-4\n")
+    ck = root / "checkpoints"
+    ck.mkdir()
+    return v, np.array(tris, np.uint32)
+
+
+def test_capture_input_applies_the_displacement_groups(tmp_path):  # golden.rs:313-380, 600-640
+    v, tris = _sheet_capture(tmp_path)
+    inp = cap.load_capture_input(str(tmp_path))
+    want = v.astype(np.float32)
+    want[6:, 1] += np.float32(0.5)
+    assert np.array_equal(inp["positions"], want)
+    assert np.array_equal(inp["tris"], tris)
+    assert inp["velocities"].shape == want.shape
+    # without both displacement files the template is the initial state
+    (tmp_path / "input_bin" / "displacement.bin").unlink()
+    assert np.array_equal(cap.load_capture_input(str(tmp_path))["positions"], v.astype(np.float32))
+
+
+def test_capture_input_rejects_inconsistent_files(tmp_path):
+    _sheet_capture(tmp_path)
+    ib = tmp_path / "input_bin"
+    (ib / "vert_dmap.bin").write_bytes(np.full(36, 5, "<u4").tobytes())  # group 5 does not exist
+    with pytest.raises(cap.CaptureError):
+        cap.load_capture_input(str(tmp_path))
+    (ib / "vert_dmap.bin").unlink()
+    (ib / "tri.bin").write_bytes(_u64([0, 1, 99]))
+    with pytest.raises(cap.CaptureError):
+        cap.load_capture_input(str(tmp_path))
+    (ib / "tri.bin").unlink()  # rod-only scenes ship no tri.bin
+    assert cap.load_capture_input(str(tmp_path))["tris"].shape == (0, 3)
+    (ib / "vel.bin").write_bytes(_f32(np.zeros(3 * 35)))
+    with pytest.raises(cap.CaptureError):
+        cap.load_capture_input(str(tmp_path))
+
+
+def test_reads_stitches_with_default_stiffness(tmp_path):  # golden.rs:839-888
+    _sheet_capture(tmp_path)
+    idx, w, k = cap.read_stitches(str(tmp_path))
+    assert idx.tolist() == [[0, 0, 0, 2, 3, 3], [1, 1, 1, 4, 4, 4]]
+    assert w[0].tolist() == [1, 0, 0, 0.5, 0.5, 0] and k.tolist() == [1.0, 1.0]
+    ib = tmp_path / "input_bin"
+    (ib / "stitch_stiffness.bin").write_bytes(_f32([2.0, 3.0]))
+    assert cap.read_stitches(str(tmp_path))[2].tolist() == [2.0, 3.0]
+    (ib / "stitch_w.bin").write_bytes(_f32(np.zeros(6)))
+    with pytest.raises(cap.CaptureError):
+        cap.read_stitches(str(tmp_path))
+
+
+def test_obj_round_trip_is_exact(tmp_path):
+    rng = np.random.default_rng(0)
+    p = rng.normal(size=(50, 3)).astype(np.float32)
+    t = rng.integers(0, 50, size=(30, 3)).astype(np.uint32)
+    path = str(tmp_path / "frame.obj")
+    cap.write_obj(path, p, t)
+    q, u = cap.read_obj(path)
+    assert np.array_equal(p, q) and np.array_equal(t, u)
+
+
+def test_a_capture_drives_the_step_and_compares_to_its_checkpoint(tmp_path):
+    """scene_from_capture gives a description the solver interface takes: the oracle steps
+    it, the pins hold, and compare_frames measures the result against a checkpoint written
+    in the capture's own format."""
+    _sheet_capture(tmp_path)
+    sc = cap.scene_from_capture(str(tmp_path), contact_dhat=1e-3)
+    assert sc["params"]["dt"] == 0.004 and sc["shell_faces"].shape[0] == 50
+    assert np.allclose(sc["stitch_kl"], [[1.0, 1e-3, 1e-2]] * 2)
+    assert (sc["inv_mass"] == 0).sum() == 2
+    o = O.OracleSolver(sc)
+    o.step(3, check_intersection=False)
+    x = o.positions()
+    assert np.all(np.isfinite(x))
+    assert np.array_equal(x[[30, 35]], sc["positions"][[30, 35]])  # pinned corners
+    (tmp_path / "checkpoints" / "vert_3.bin").write_bytes(x.astype("<f4").tobytes())
+    ref = cap.load_checkpoint(str(tmp_path), 3)
+    g = cap.compare_frames(x, ref)
+    assert g.max_rel == 0 and g.passes()
+    assert cap.compare_frames(sc["positions"], ref).max_rel > 0
+    cap.write_obj(str(tmp_path / "frame_3.obj"), x, sc["tris"])
+    q, _ = cap.read_obj(str(tmp_path / "frame_3.obj"))
+    assert np.array_equal(q, x.astype(np.float32))
