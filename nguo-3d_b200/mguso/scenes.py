@@ -348,8 +348,16 @@ def sheath_on_torso(width: float = 0.6, height: float = 1.1, edge: float = 8.0e-
                 name=f"sheath {ctris.shape[0]} tris on torso {ttris.shape[0]} tris")
 
 
-def graded_sheaths(n: int = 6, widths=(0.50, 0.55, 0.60, 0.65, 0.70, 0.75), torso_scales=(0.9, 0.96, 1.02, 1.08, 1.14, 1.2),
-                   **kw):
+GRADE_WIDTHS = (0.50, 0.55, 0.60, 0.65, 0.70, 0.75)
+GRADE_TORSO_SCALES = (0.9, 0.96, 1.02, 1.08, 1.14, 1.2)
+
+
+def graded_sheath(i: int, widths=GRADE_WIDTHS, torso_scales=GRADE_TORSO_SCALES, **kw):
+    """Size `i` (0 = XS) of the graded sheath."""
+    return sheath_on_torso(width=widths[i], torso_scale=torso_scales[i], **kw)
+
+
+def graded_sheaths(n: int = 6, widths=GRADE_WIDTHS, torso_scales=GRADE_TORSO_SCALES, **kw):
     """One pattern graded into `n` sizes XS..XXL (panel widths 0.50-0.75 m, torsos scaled
     0.9-1.2): the batched configuration."""
-    return [sheath_on_torso(width=widths[i], torso_scale=torso_scales[i], **kw) for i in range(n)]
+    return [graded_sheath(i, widths, torso_scales, **kw) for i in range(n)]
