@@ -322,6 +322,14 @@ int mguso_read_positions(mguso_scene* s, float* out);   /* f32[3*nv] host */
 int mguso_write_positions(mguso_scene* s, const float* in);
 int mguso_read_velocities(mguso_scene* s, float* out);
 int mguso_write_velocities(mguso_scene* s, const float* in);
+/* Move the scene's static mesh collider (its vertices of static_mask) to x (f32[3 nv]; other
+ * rows are ignored) between steps: those vertices take x and the velocity of that move over
+ * one step, and the collider's pseudonormals are recomputed. MGUSO_ERR_INVALID_ARG, with
+ * nothing written, when the scene has no static collider or a collider row of x is not
+ * finite. The next step's CCD sees the collider already at x (the body teleports, as in the
+ * reference). Counterpart: ImplicitSolver::set_kinematic_collider_positions
+ * (core-engine/crates/engine-core/src/implicit.rs:1368-1398). */
+int mguso_set_kinematic_collider_positions(mguso_scene* s, const float* x);
 /* Element counts: hinges, shells, unique edges, static collider triangles,
  * system blocks (free-free pattern), pinned-pattern blocks. */
 int mguso_scene_info(mguso_scene* s, uint32_t* out6);

@@ -26,6 +26,49 @@ using HV = V3<float>;
 
 HV hp(const float* p, uint32_t i) { return HV(p[3 * i], p[3 * i + 1], p[3 * i + 2]); }
 
+// Angle-weighted pseudonormals of the static collider's triangles `ctris` at positions P
+// (contact.rs:963-1001), welded on exact position bits within an instance (-0 folded to
+// +0); pn gets 3 per vertex (zero off the collider).
+static void collider_pseudonormals(const float* P, uint32_t nv, const std::vector<std::array<uint32_t, 3>>& ctris,
+                                   const std::vector<uint8_t>& vinst, std::vector<float>& pn) {
+  std::vector<HV> acc;
+  std::vector<uint32_t> of(nv);
+  auto bits = [](float c) { if (c == 0.f) c = 0.f; uint32_t b; std::memcpy(&b, &c, 4); return (uint64_t)b; };
+  std::map<std::array<uint64_t, 3>, uint32_t> wmap;
+  for (uint32_t i = 0; i < nv; ++i) {
+    std::array<uint64_t, 3> kk = {bits(P[3 * i]) | ((uint64_t)vinst[i] << 32), bits(P[3 * i + 1]),
+                                  bits(P[3 * i + 2])};
+    auto it = wmap.find(kk);
+    if (it == wmap.end()) {
+      uint32_t id = (uint32_t)wmap.size();
+      wmap.emplace(kk, id);
+      of[i] = id;
+    } else {
+      of[i] = it->second;
+    }
+  }
+  acc.assign(wmap.size(), HV());
+  for (const auto& tv : ctris) {
+    HV q[3] = {hp(P, tv[0]), hp(P, tv[1]), hp(P, tv[2])};
+    HV face = (q[1] - q[0]).cross(q[2] - q[0]).normalize_or_zero();
+    if (face.x == 0.f && face.y == 0.f && face.z == 0.f) continue;
+    for (int k = 0; k < 3; ++k) {
+      HV u = (q[(k + 1) % 3] - q[k]).normalize_or_zero();
+      HV w = (q[(k + 2) % 3] - q[k]).normalize_or_zero();
+      float dt = u.dot(w);
+      dt = dt < -1.f ? -1.f : (dt > 1.f ? 1.f : dt);
+      acc[of[tv[k]]] += face * std::acos(dt);
+    }
+  }
+  pn.assign(3 * (size_t)nv, 0.f);
+  for (uint32_t i = 0; i < nv; ++i) {
+    HV n = acc[of[i]].normalize_or_zero();
+    pn[3 * i] = n.x;
+    pn[3 * i + 1] = n.y;
+    pn[3 * i + 2] = n.z;
+  }
+}
+
 float host_dihedral(const HV p[4]) {
   HV n1 = (p[1] - p[0]).cross(p[2] - p[0]);
   HV n2 = (p[1] - p[2]).cross(p[3] - p[2]);
@@ -464,43 +507,12 @@ int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>
         s.has_static = true;
         for (uint32_t i = 0; i < nv; ++i) svert[i] = d->static_mask[i] ? 1 : 0;
         for (uint32_t t : marked) ctri[t] = 1;
-        // angle-weighted pseudonormals, welded on exact position bits (-0 folded to +0)
-        std::unordered_map<uint64_t, uint32_t> weld;
-        std::vector<HV> acc;
-        std::vector<uint32_t> of(nv);
-        auto bits = [](float c) { if (c == 0.f) c = 0.f; uint32_t b; std::memcpy(&b, &c, 4); return (uint64_t)b; };
-        std::map<std::array<uint64_t, 3>, uint32_t> wmap;
-        for (uint32_t i = 0; i < nv; ++i) {
-          std::array<uint64_t, 3> kk = {bits(P[3 * i]) | ((uint64_t)vinst[i] << 32), bits(P[3 * i + 1]),
-                                        bits(P[3 * i + 2])};
-          auto it = wmap.find(kk);
-          if (it == wmap.end()) {
-            uint32_t id = (uint32_t)wmap.size();
-            wmap.emplace(kk, id);
-            of[i] = id;
-          } else {
-            of[i] = it->second;
-          }
-        }
-        acc.assign(wmap.size(), HV());
-        for (uint32_t t : marked) {
-          HV q[3] = {hp(P, tris[t][0]), hp(P, tris[t][1]), hp(P, tris[t][2])};
-          HV face = (q[1] - q[0]).cross(q[2] - q[0]).normalize_or_zero();
-          if (face.x == 0.f && face.y == 0.f && face.z == 0.f) continue;
-          for (int k = 0; k < 3; ++k) {
-            HV u = (q[(k + 1) % 3] - q[k]).normalize_or_zero();
-            HV w = (q[(k + 2) % 3] - q[k]).normalize_or_zero();
-            float dt = u.dot(w);
-            dt = dt < -1.f ? -1.f : (dt > 1.f ? 1.f : dt);
-            acc[of[tris[t][k]]] += face * std::acos(dt);
-          }
-        }
-        for (uint32_t i = 0; i < nv; ++i) {
-          HV n = acc[of[i]].normalize_or_zero();
-          pn[3 * i] = n.x;
-          pn[3 * i + 1] = n.y;
-          pn[3 * i + 2] = n.z;
-        }
+        std::vector<std::array<uint32_t, 3>> ctris;
+        for (uint32_t t : marked) ctris.push_back(tris[t]);
+        collider_pseudonormals(P, nv, ctris, vinst, pn);
+        s.h_static = svert;
+        s.h_ctris = ctris;
+        s.h_vinst = vinst;
       }
     }
   }
@@ -678,6 +690,40 @@ static int copy_state(mguso_scene* sc, DevBuf<float>& buf, float* out, const flo
   if (out) MG_CUDA(cudaMemcpyAsync(out, buf.p, bytes, cudaMemcpyDeviceToHost, sc->s.st));
   if (in) MG_CUDA(cudaMemcpyAsync(buf.p, in, bytes, cudaMemcpyHostToDevice, sc->s.st));
   MG_CUDA(cudaStreamSynchronize(sc->s.st));
+  return MGUSO_OK;
+}
+
+// set_kinematic_collider_positions (implicit.rs:1368-1398).
+int mguso_set_kinematic_collider_positions(mguso_scene* sc, const float* x) {
+  MG_CHECK_ARG(sc && x, "null argument");
+  Scene& s = sc->s;
+  MG_CHECK_ARG(s.has_static && !s.h_static.empty(), "kinematic collider: the scene has no static collider");
+  const uint32_t nv = s.nv;
+  for (uint32_t i = 0; i < nv; ++i)
+    if (s.h_static[i])
+      MG_CHECK_ARG(std::isfinite(x[3 * i]) && std::isfinite(x[3 * i + 1]) && std::isfinite(x[3 * i + 2]),
+                   "kinematic collider: a collider position is not finite");
+  MG_CUDA(cudaSetDevice(s.ctx->device));
+  std::vector<float> pos(3 * (size_t)nv), vel(3 * (size_t)nv);
+  MG_CUDA(cudaMemcpyAsync(pos.data(), s.x.p, 12 * (size_t)nv, cudaMemcpyDeviceToHost, s.st));
+  MG_CUDA(cudaMemcpyAsync(vel.data(), s.v.p, 12 * (size_t)nv, cudaMemcpyDeviceToHost, s.st));
+  MG_CUDA(cudaStreamSynchronize(s.st));
+  const float inv_h = 1.0f / s.p.dt;
+  for (uint32_t i = 0; i < nv; ++i) {
+    if (!s.h_static[i]) continue;
+    for (int c = 0; c < 3; ++c) {
+      const float dd = x[3 * i + c] - pos[3 * i + c];
+      pos[3 * i + c] = x[3 * i + c];
+      vel[3 * i + c] = dd * inv_h;
+    }
+  }
+  std::vector<float> pn;
+  collider_pseudonormals(pos.data(), nv, s.h_ctris, s.h_vinst, pn);
+  MG_CUDA(cudaMemcpyAsync(s.x.p, pos.data(), 12 * (size_t)nv, cudaMemcpyHostToDevice, s.st));
+  MG_CUDA(cudaMemcpyAsync(s.v.p, vel.data(), 12 * (size_t)nv, cudaMemcpyHostToDevice, s.st));
+  MG_CUDA(cudaMemcpyAsync(s.collider_pn.p, pn.data(), 4 * pn.size(), cudaMemcpyHostToDevice, s.st));
+  MG_CUDA(cudaStreamSynchronize(s.st));
+  s.static_done = false;  // contributions of all-pinned elements move with the collider
   return MGUSO_OK;
 }
 

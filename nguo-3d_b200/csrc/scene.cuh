@@ -13,6 +13,7 @@
 // slot's contributions in that order, so the assembly is deterministic and needs no
 // atomics. Self-contact blocks that land outside Ps form a per-iteration block matrix C.
 #pragma once
+#include <array>
 #include "lbvh.cuh"
 #include "pcg.cuh"
 
@@ -75,6 +76,10 @@ struct Scene {
   uint32_t n_act_shell = 0, n_act_hinge = 0, n_act_spring = 0, n_act_stitch = 0;
   DevBuf<uint32_t> act_shell, act_hinge, act_spring, act_stitch;
   bool static_done = false;
+  // the static collider on the host (for re-posing it): its vertex mask, its triangles and
+  // every vertex's instance (empty without a static collider)
+  std::vector<uint8_t> h_static, h_vinst;
+  std::vector<std::array<uint32_t, 3>> h_ctris;
   // Hessians the assembly writes: 0 the step's PSD-projected ones; 2 the exact ones (shells
   // without the eigenvalue clamp, stitches below rest length, hinges and barriers with their
   // second-derivative terms), the contact stiffness held at `contact_k` (2 per stencil:

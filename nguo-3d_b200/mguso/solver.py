@@ -56,6 +56,7 @@ def _sigs(lib):
         ("mguso_write_positions", i32, [vp, vp]),
         ("mguso_read_velocities", i32, [vp, vp]),
         ("mguso_write_velocities", i32, [vp, vp]),
+        ("mguso_set_kinematic_collider_positions", i32, [vp, vp]),
         ("mguso_scene_info", i32, [vp, vp]),
         ("mguso_scene_spmv_time", i32, [vp, i32, P(C.c_float), P(C.c_double)]),
         ("mguso_scene_assemble", i32, [vp, vp, vp, vp]),
@@ -164,6 +165,14 @@ class ImplicitSolver:
     def velocities(self, v):
         a = np.ascontiguousarray(v, np.float32)
         check(self.lib.mguso_write_velocities(self.h, ptr(a)))
+
+    def set_kinematic_collider_positions(self, x) -> None:
+        """Move the static mesh collider to ``x`` (rows of the static mask; the others are
+        ignored) between steps, with the velocity of that move
+        (ImplicitSolver::set_kinematic_collider_positions, implicit.rs:1368-1398). Raises
+        MgusoError, changing nothing, without a static collider or with a non-finite row."""
+        a = np.ascontiguousarray(x, np.float32).reshape(self.nv, 3)
+        check(self.lib.mguso_set_kinematic_collider_positions(self.h, ptr(a)))
 
     def info(self) -> dict:
         out = np.zeros(6, np.uint32)

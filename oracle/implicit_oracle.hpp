@@ -1256,6 +1256,26 @@ struct ImplicitSolver {
     collider_pn = pseudonormals(positions, collider_tris);
   }
 
+  // set_kinematic_collider_positions (implicit.rs:1368-1398): move the static collider's
+  // vertices to x (its rows only), give them the velocity of that move over one step and
+  // recompute the pseudonormals. False, with nothing written, when there is no static
+  // collider, x has the wrong length or a collider row of x is not finite.
+  bool set_kinematic_collider_positions(const std::vector<V>& x) {
+    if (static_collider_vert.empty() || x.size() != positions.size()) return false;
+    for (size_t i = 0; i < x.size(); ++i)
+      if (static_collider_vert[i] && !(std::isfinite(x[i].x) && std::isfinite(x[i].y) && std::isfinite(x[i].z)))
+        return false;
+    const R inv_h = R(1) / params.dt;
+    for (size_t i = 0; i < x.size(); ++i) {
+      if (!static_collider_vert[i]) continue;
+      V d = x[i] - positions[i];
+      positions[i] = x[i];
+      velocities[i] = d * inv_h;
+    }
+    collider_pn = pseudonormals(positions, collider_tris);
+    return true;
+  }
+
   std::vector<uint8_t> movable_mask() const {
     std::vector<uint8_t> m(inv_mass.size());
     for (size_t i = 0; i < m.size(); ++i) m[i] = inv_mass[i] > 0;

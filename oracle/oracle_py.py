@@ -213,6 +213,7 @@ def _step_sigs(lib):
         "oracle_solver_step": (i32, [vp, i32, i32, vp]),
         "oracle_solver_state": (None, [vp, vp, vp]),
         "oracle_solver_set_state": (None, [vp, vp, vp]),
+        "oracle_solver_set_kinematic": (i32, [vp, vp]),
         "oracle_solver_counts": (None, [vp, vp]),
         "oracle_solver_stencils": (u32, [vp, vp, vp, u32]),
         "oracle_solver_assemble": (vp, [vp, vp, vp, vp]),
@@ -279,6 +280,11 @@ class OracleSolver:
         v = np.empty((self.nv, 3), np.float64)
         self.lib.oracle_solver_state(self.h, None, _p(v))
         return v
+
+    def set_kinematic_collider_positions(self, x) -> bool:
+        """Move the static collider to x (its rows; implicit.rs:1368-1398)."""
+        p = np.ascontiguousarray(x, np.float64)
+        return bool(self.lib.oracle_solver_set_kinematic(self.h, _p(p)))
 
     def set_state(self, pos, vel):
         p = np.ascontiguousarray(pos, np.float64)

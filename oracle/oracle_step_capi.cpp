@@ -242,6 +242,18 @@ void oracle_solver_set_shells(void* h, uint32_t n, const uint32_t* faces, const 
     set_shells(*a->d, n, faces, rest, mu, lam);
 }
 
+int oracle_solver_set_kinematic(void* h, const double* pos) {
+  auto* a = (AnySolver*)h;
+  if (a->prec == 0) {
+    std::vector<Vt<float>> x(a->f->positions.size());
+    for (size_t i = 0; i < x.size(); ++i) x[i] = Vt<float>((float)pos[3 * i], (float)pos[3 * i + 1], (float)pos[3 * i + 2]);
+    return a->f->set_kinematic_collider_positions(x);
+  }
+  std::vector<Vt<double>> x(a->d->positions.size());
+  for (size_t i = 0; i < x.size(); ++i) x[i] = Vt<double>(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+  return a->d->set_kinematic_collider_positions(x);
+}
+
 void oracle_solver_set_state(void* h, const double* pos, const double* vel) {
   auto* a = (AnySolver*)h;
   size_t n = a->prec == 0 ? a->f->positions.size() : a->d->positions.size();

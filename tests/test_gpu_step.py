@@ -251,3 +251,43 @@ def test_batch_instance_matches_oracle(ctx):
     po = o.positions()
     disp = np.abs(po - scs[1]["positions"]).max()
     assert np.abs(pb - po).max() <= 2e-2 * disp
+
+
+def test_kinematic_collider_repose_matches_oracle(ctx):
+    """The torso moved between steps (0.3 mm sideways, 0.2 mm up) on both solvers: its
+    vertices take the new positions, the following steps agree with the oracle's from identical
+    states, and a non-finite collider row is refused with nothing written
+    (implicit.rs:1368-1398)."""
+    from mguso import MgusoError
+
+    sc = coarse_sheath()
+    body = np.asarray(sc["static_mask"], bool)
+    g = ImplicitSolver(ctx, sc, "mixed")
+    o = O.OracleSolver(sc)
+    g.step(1)
+    o.step(1, check_intersection=False)
+    x = o.positions().astype(np.float32)
+    x[body] += np.float32([3e-4, 2e-4, 0.0])
+    bad = x.copy()
+    bad[np.flatnonzero(body)[0], 0] = np.nan
+    before = g.positions.copy()
+    with pytest.raises(MgusoError):
+        g.set_kinematic_collider_positions(bad)
+    assert np.array_equal(g.positions, before)
+    g.positions = o.positions().astype(np.float32)
+    g.velocities = o.velocities().astype(np.float32)
+    g.set_kinematic_collider_positions(x)
+    assert o.set_kinematic_collider_positions(x.astype(np.float64))
+    assert np.array_equal(g.positions[body], x[body])
+    assert np.array_equal(g.positions[~body], o.positions()[~body].astype(np.float32))
+    for k in range(2):
+        p0, v0 = o.positions().copy(), o.velocities().copy()
+        g.positions = p0.astype(np.float32)
+        g.velocities = v0.astype(np.float32)
+        sg = g.step(1)[0]
+        so = o.step(1, check_intersection=False)[0]
+        pg, po = g.positions.astype(np.float64), o.positions()
+        rel = np.abs(pg - po).max() / (np.abs(po - p0).max() + 1e-12)
+        assert sg["status"] == 0 and sg["penetration_free"]
+        assert abs(sg["newton_iters"] - so["newton_iters"]) <= 1
+        assert rel < 1e-3, (k, rel)

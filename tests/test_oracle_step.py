@@ -471,3 +471,26 @@ def test_the_hinge_gradient_reduces_energy_toward_rest():  # bending.rs:274-290
     step = 1e-3 * np.sign(th0)
     th1 = O.hinge(p - g * step * 50.0)[0]
     assert abs(th1) < abs(th0)
+
+
+def test_kinematic_collider_repose_moves_only_the_collider_and_sets_its_velocity():  # implicit.rs:1368-1398
+    sc = scenes.sheath_on_torso(edge=0.05, torso_res=(24, 23), width=0.5, torso_scale=0.9)
+    o = O.OracleSolver(sc, "f64")
+    o.step(1, check_intersection=False)
+    x0, v0 = o.positions().copy(), o.velocities().copy()
+    body = np.asarray(sc["static_mask"], bool)
+    x = x0.copy()
+    x[body, 1] += 0.002
+    x[~body] = 123.0  # rows that are not the collider's are ignored
+    bad = x.copy()
+    bad[np.flatnonzero(body)[0], 0] = np.nan
+    assert not o.set_kinematic_collider_positions(bad)
+    assert np.array_equal(o.positions(), x0)  # nothing written
+    assert o.set_kinematic_collider_positions(x)
+    x1, v1 = o.positions(), o.velocities()
+    assert np.allclose(x1[body], x0[body] + [0, 0.002, 0]) and np.array_equal(x1[~body], x0[~body])
+    assert np.allclose(v1[body], [0, 0.002 / sc["params"]["dt"], 0]) and np.array_equal(v1[~body], v0[~body])
+    st = o.step(1)
+    assert st[0]["penetration_free"] and np.all(np.isfinite(o.positions()))
+    free = dict(sc, static_mask=None)
+    assert not O.OracleSolver(free, "f64").set_kinematic_collider_positions(x)
