@@ -353,6 +353,13 @@ int mguso_scene_profile(mguso_scene* s, int reps, float* us4, double* bytes4);
    ImplicitSolver::step (core-engine/crates/engine-core/src/implicit.rs:2280-3155). */
 int mguso_scene_assemble(mguso_scene* scene, const float* x, const float* x_tilde, uint32_t out3[3]);
 
+/* The step fraction the CCD filter allows for search direction dx (f32[3 nv]) from positions
+   x (f32[3 nv]; the scene's positions are left at x): t_out f32[instances] (one per instance
+   of a batch), cap_hits (optional) u32[instances] root solves that reached ccd_max_iter.
+   Parity and diagnostics entry; counterpart: ImplicitSolver::ccd_max_step
+   (core-engine/crates/engine-core/src/implicit.rs:1690-1947). */
+int mguso_scene_ccd(mguso_scene* scene, const float* x, const float* dx, float* t_out, uint32_t* cap_hits);
+
 /* Download the last assembled system: the fixed-pattern blocks (row_ptr u32[nv+1], col
    u32[out3[0]], values f32[9*out3[0]] row-major 3x3), the contact-only blocks in the same
    layout (out3[1] of them; col/val may be NULL when zero) and the right-hand side f32[3 nv].

@@ -780,6 +780,29 @@ extern "C" int mguso_scene_spmv_time(mguso_scene* sc, int reps, float* us, doubl
 
 // One Newton-system assembly at positions x (and inertia target x_tilde, x when null), as
 // one Newton iteration of mguso_step does it; the scene's positions are left at x.
+extern "C" int mguso_scene_ccd(mguso_scene* sc, const float* x, const float* dx, float* t_out, uint32_t* cap_hits) {
+  MG_CHECK_ARG(sc && x && dx && t_out, "bad argument");
+  Scene& s = sc->s;
+  cudaStream_t st = s.st;
+  const size_t bytes = 12 * (size_t)s.nv;
+  MG_CUDA(cudaMemcpyAsync(s.x.p, x, bytes, cudaMemcpyHostToDevice, st));
+  MG_CUDA(cudaMemcpyAsync(s.dx.p, dx, bytes, cudaMemcpyHostToDevice, st));
+  if (s.p.self_collision) {
+    uint32_t nst = 0;
+    MG_TRY(build_bvhs(s, s.x.p));
+    MG_TRY(collect_stencils(s, &nst));  // also decides each vertex's side of a static collider
+  }
+  std::vector<float> t(s.ninst, 1.f);
+  std::vector<uint32_t> caps(s.ninst, 0u);
+  MG_TRY(ccd_step(s, (s.ninst >= 32 ? ~0u : ((1u << s.ninst) - 1u)), t.data(), caps.data()));
+  MG_CUDA(cudaStreamSynchronize(st));
+  for (uint32_t k = 0; k < s.ninst; ++k) {
+    t_out[k] = t[k];
+    if (cap_hits) cap_hits[k] = caps[k];
+  }
+  return MGUSO_OK;
+}
+
 extern "C" int mguso_scene_assemble(mguso_scene* sc, const float* x, const float* x_tilde, uint32_t* out3) {
   MG_CHECK_ARG(sc && x && out3, "bad argument");
   Scene& s = sc->s;

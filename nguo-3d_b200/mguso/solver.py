@@ -60,6 +60,7 @@ def _sigs(lib):
         ("mguso_scene_info", i32, [vp, vp]),
         ("mguso_scene_spmv_time", i32, [vp, i32, P(C.c_float), P(C.c_double)]),
         ("mguso_scene_assemble", i32, [vp, vp, vp, vp]),
+        ("mguso_scene_ccd", i32, [vp, vp, vp, vp, vp]),
         ("mguso_scene_profile", i32, [vp, i32, vp, vp]),
         ("mguso_batch_create", i32, [vp, vp, C.c_uint32, P(vp)]),
         ("mguso_scene_instances", i32, [vp, P(C.c_uint32), vp]),
@@ -193,6 +194,17 @@ class ImplicitSolver:
         check(self.lib.mguso_scene_profile(self.h, reps, ptr(us), ptr(by)))
         names = ["spmv", "precond_apply", "precond_factor", "pcg_update"]
         return {k: (float(u), float(b)) for k, u, b in zip(names, us, by)}
+
+    def ccd(self, x, dx):
+        """Step fraction the CCD filter allows along ``dx`` from ``x`` (one per instance) and
+        its ACCD cap hits (implicit.rs:1690-1947); the scene's positions are left at ``x``."""
+        xx = np.ascontiguousarray(x, np.float32).reshape(self.nv, 3)
+        dd = np.ascontiguousarray(dx, np.float32).reshape(self.nv, 3)
+        k = getattr(self, "ninst", 1)
+        t = np.zeros(k, np.float32)
+        caps = np.zeros(k, np.uint32)
+        check(self.lib.mguso_scene_ccd(self.h, ptr(xx), ptr(dd), ptr(t), ptr(caps)))
+        return t, caps
 
     def assemble(self, x, x_tilde=None) -> dict:
         """One Newton-system assembly at positions ``x`` (inertia target ``x_tilde``, ``x``

@@ -287,8 +287,9 @@ class OracleSolver:
         return bool(self.lib.oracle_solver_set_kinematic(self.h, _p(p)))
 
     def set_state(self, pos, vel):
-        p = np.ascontiguousarray(pos, np.float64)
-        v = np.ascontiguousarray(vel, np.float64)
+        """Overwrite positions and/or velocities (f64 (nv, 3)); None leaves that one as is."""
+        p = None if pos is None else np.ascontiguousarray(pos, np.float64).reshape(self.nv, 3)
+        v = None if vel is None else np.ascontiguousarray(vel, np.float64).reshape(self.nv, 3)
         self.lib.oracle_solver_set_state(self.h, _p(p), _p(v))
 
     def counts(self):

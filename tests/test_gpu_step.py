@@ -291,3 +291,28 @@ def test_kinematic_collider_repose_matches_oracle(ctx):
         assert sg["status"] == 0 and sg["penetration_free"]
         assert abs(sg["newton_iters"] - so["newton_iters"]) <= 1
         assert rel < 1e-3, (k, rel)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_ccd_step_fraction_matches_oracle(ctx, precision):
+    """The CCD filter alone (pruned traversal, widening passes merged after the first) against
+    the oracle's ccd_max_step on the coarse sheath, for directions from well inside the first
+    pass's radius to several passes beyond it, with collisions and without."""
+    sc = coarse_sheath()
+    g = ImplicitSolver(ctx, sc, precision)
+    o = O.OracleSolver(sc)
+    o.step(1, check_intersection=False)
+    x = o.positions().astype(np.float32)
+    free = np.asarray(sc["inv_mass"]) > 0
+    rng = np.random.default_rng(7)
+    ts = []
+    for mag in (5e-4, 5e-3, 3e-2, 0.2, 0.6):
+        dx = np.zeros_like(x)
+        dx[free] = rng.normal(0, 0.3 * mag, (free.sum(), 3)) + np.float32([0.0, -mag, 0.0])
+        t_gpu, _ = g.ccd(x, dx)
+        o.set_state(x.astype(np.float64), None)
+        t_o = o.ccd(dx)
+        ts.append((mag, float(t_gpu[0]), t_o))
+        assert abs(float(t_gpu[0]) - t_o) <= 1e-4 * max(t_o, 1e-3), (mag, t_gpu, t_o)
+    print(ts)
+    assert min(t for _, _, t in ts) < 1.0  # some direction collides
