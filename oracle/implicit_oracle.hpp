@@ -731,7 +731,24 @@ inline R shell_energy(const Vt<R> p[3], const ShellEl<R>& el, R mu, R lambda) {
   return el.area * stvk_density(sigma, mu, lambda);
 }
 
-// shell_dfdx (shell_model.rs:384-400) and shell_hessian_analytic (:403-438)
+// shell_dfdx (shell_model.rs:384-400): dvec(F)/dx as a 6 x 9 row-major matrix.
+template <class R>
+inline void shell_dfdx(const Mat2<R>& dm_inv, R b[54]) {
+  for (int k = 0; k < 54; ++k) b[k] = 0;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 2; ++j) {
+      int row = 2 * i + j;
+      R sum = 0;
+      for (int k = 0; k < 2; ++k) {
+        R d = dm_inv.at(k, j);
+        b[row * 9 + 3 * (k + 1) + i] = d;
+        sum += d;
+      }
+      b[row * 9 + i] = -sum;
+    }
+}
+
+// shell_hessian_analytic (shell_model.rs:403-438)
 template <class R>
 inline void shell_hessian(const Vt<R> p[3], const ShellEl<R>& el, R mu, R lambda, R eps, R h[81]) {
   Mat3x2<R> f = shell_F(p, el.dm_inv);
@@ -745,18 +762,7 @@ inline void shell_hessian(const Vt<R> p[3], const ShellEl<R>& el, R mu, R lambda
   R a6[36];
   shell_d2psi_df2(u, sigma, v, deda, d2, eps, a6);
   R b[54];
-  for (int k = 0; k < 54; ++k) b[k] = 0;
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 2; ++j) {
-      int row = 2 * i + j;
-      R sum = 0;
-      for (int k = 0; k < 2; ++k) {
-        R d = el.dm_inv.at(k, j);
-        b[row * 9 + 3 * (k + 1) + i] = d;
-        sum += d;
-      }
-      b[row * 9 + i] = -sum;
-    }
+  shell_dfdx(el.dm_inv, b);
   R ab[54];
   for (int r = 0; r < 6; ++r)
     for (int c = 0; c < 9; ++c) {
@@ -770,6 +776,111 @@ inline void shell_hessian(const Vt<R> p[3], const ShellEl<R>& el, R mu, R lambda
       for (int k = 0; k < 6; ++k) acc += b[k * 9 + r] * ab[k * 9 + c];
       h[r * 9 + c] = el.area * acc;
     }
+}
+
+// ---------------------------------------------------------------------------------------
+// Strain limiting: the per-face barrier on the principal-stretch excess
+// (shell_model.rs:438-640) and the one-sided per-edge spring (strain_limit.rs:24-63).
+// ---------------------------------------------------------------------------------------
+// SL_GAP_FLOOR (shell_model.rs:444): the barrier argument never drops below this fraction
+// of the limit.
+template <class R>
+inline R sl_gap_floor() { return R(1.0e-3); }
+
+// strain_limit_derivs (shell_model.rs:456-484): (E, dE/da, d2E/da2) over the two principal
+// stretch excesses a = sigma - 1; false when neither exceeds rest.
+template <class R>
+inline bool strain_limit_derivs(const R sigma[2], R limit, BarrierKind kind, R& energy, R deda[2], R d2[4]) {
+  if (limit <= 0) return false;
+  energy = 0;
+  deda[0] = deda[1] = 0;
+  d2[0] = d2[1] = d2[2] = d2[3] = 0;
+  bool active = false;
+  for (int i = 0; i < 2; ++i) {
+    R a = sigma[i] - R(1);
+    if (a <= 0) continue;
+    R y = rmax(limit - a, sl_gap_floor<R>() * limit);
+    R e, g, h;
+    if (barrier_of(kind, y, limit, R(1), e, g, h)) {
+      energy += e;
+      deda[i] = -g;
+      d2[i * 2 + i] = h;
+      active = true;
+    }
+  }
+  return active;
+}
+
+// strain_limit_energy (shell_model.rs:493-502), no area factor.
+template <class R>
+inline R strain_limit_energy(const Vt<R> p[3], const ShellEl<R>& el, R limit, BarrierKind kind) {
+  Mat3x2<R> f = shell_F(p, el.dm_inv);
+  Mat3x2<R> u;
+  R sigma[2];
+  Mat2<R> v;
+  svd3x2(f, u, sigma, v);
+  R e, deda[2], d2[4];
+  return strain_limit_derivs(sigma, limit, kind, e, deda, d2) ? e : R(0);
+}
+
+// The barrier's 9-vector gradient and 9x9 Hessian at unit stiffness (shell_model.rs:508-561)
+// when `stiffness` is 1 and `elastic_k`/`face_mass` are unused; strain_limit_assembly
+// (:582-640) otherwise: stiffness = max(elastic_k, 0) + face_mass / d^2 with d the headroom
+// limit - max(sigma - 1), floored. Returns false when the term is inactive.
+template <class R>
+inline bool strain_limit_eval(const Vt<R> p[3], const ShellEl<R>& el, R limit, R face_mass, R elastic_k,
+                              BarrierKind kind, R eps, bool dynamic_stiffness, Vt<R> grad[3], R hess[81]) {
+  Mat3x2<R> f = shell_F(p, el.dm_inv);
+  Mat3x2<R> u;
+  R sigma[2];
+  Mat2<R> v;
+  svd3x2(f, u, sigma, v);
+  R energy, deda[2], d2[4];
+  if (!strain_limit_derivs(sigma, limit, kind, energy, deda, d2)) return false;
+  R stiffness = R(1);
+  if (dynamic_stiffness) {
+    R max_a = rmax(sigma[0] - R(1), sigma[1] - R(1));
+    R d = rmax(limit - max_a, sl_gap_floor<R>() * limit);
+    stiffness = rmax(elastic_k, R(0)) + face_mass / (d * d);
+    if (stiffness <= 0) return false;
+  }
+  Mat3x2<R> pk1 = Mat3x2<R>{u.c0 * deda[0], u.c1 * deda[1]}.mul_mat2(v.transpose());
+  Mat3x2<R> hg = pk1.mul_mat2(el.dm_inv.transpose());
+  Vt<R> g1 = dynamic_stiffness ? hg.c0 * stiffness : hg.c0;
+  Vt<R> g2 = dynamic_stiffness ? hg.c1 * stiffness : hg.c1;
+  grad[0] = -(g1 + g2);
+  grad[1] = g1;
+  grad[2] = g2;
+  R a6[36];
+  shell_d2psi_df2(u, sigma, v, deda, d2, eps, a6);
+  R b[54];
+  shell_dfdx(el.dm_inv, b);
+  R ab[54];
+  for (int r = 0; r < 6; ++r)
+    for (int c = 0; c < 9; ++c) {
+      R acc = 0;
+      for (int k = 0; k < 6; ++k) acc += a6[r * 6 + k] * b[k * 9 + c];
+      ab[r * 9 + c] = acc;
+    }
+  for (int r = 0; r < 9; ++r)
+    for (int c = 0; c < 9; ++c) {
+      R acc = 0;
+      for (int k = 0; k < 6; ++k) acc += b[k * 9 + r] * ab[k * 9 + c];
+      hess[r * 9 + c] = dynamic_stiffness ? stiffness * acc : acc;
+    }
+  return true;
+}
+
+// The largest principal-stretch excess max(sigma - 1) of a face at positions p
+// (the quantity the strain-limit line search bisects on, implicit.rs:1719-1729).
+template <class R>
+inline R max_stretch_excess(const Vt<R> p[3], const Mat2<R>& dm_inv) {
+  Mat3x2<R> f = shell_F(p, dm_inv);
+  Mat3x2<R> u;
+  R sigma[2];
+  Mat2<R> v;
+  svd3x2(f, u, sigma, v);
+  return rmax(sigma[0] - R(1), sigma[1] - R(1));
 }
 
 // ---------------------------------------------------------------------------------------
@@ -920,6 +1031,28 @@ inline void spring_block(const Vt<R>& d, R rest, R k, R h[3][3], Vt<R>& g) {
       h[i][j] = k * (nnt + coeff_t * (iden - nnt));
     }
   g = nrm * (k * (l - rest));
+}
+
+// strain_energy / strain_block (strain_limit.rs:31-63): a spring of rest length
+// max_ratio * rest acting only while the edge is longer than that. Returns grad_i and h_ii
+// (grad_j = -grad_i, h_jj = h_ii, h_ij = h_ji = -h_ii).
+template <class R>
+inline R edge_strain_energy(const Vt<R>& xi, const Vt<R>& xj, R rest, R max_ratio, R k) {
+  R l = (xi - xj).length();
+  R r = rest * max_ratio;
+  return l > r ? R(0.5) * k * (l - r) * (l - r) : R(0);
+}
+template <class R>
+inline void edge_strain_block(const Vt<R>& xi, const Vt<R>& xj, R rest, R max_ratio, R k, Vt<R>& g, R h[3][3]) {
+  Vt<R> d = xi - xj;
+  R r = rest * max_ratio;
+  if (d.length() <= r) {
+    g = Vt<R>();
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) h[i][j] = 0;
+    return;
+  }
+  spring_block(d, r, k, h, g);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1131,9 +1264,37 @@ struct Params {
   R cg_tol = R(1.0e-4);
   uint32_t cg_max_iter = 2000;
   R floor_y = -std::numeric_limits<R>::infinity();
+  R constraint_tol = R(1.0e-2);  // pin gap floor as a fraction of ghat
+  R strain_limit_ratio = 0, strain_limit_k = 0, strain_limit_ratio_weft = 0;
   R newton_tol = 0;          // added termination (0 disables)
   int precond = 2;           // 1 block Jacobi (CgCpu), 2 Schwarz
   uint32_t schwarz_domain = 32;
+};
+
+// Pin (implicit.rs:230-262, the reference's FixPair): the vertex is confined to a ball of
+// radius ghat around target and pulled by k |x - target|^2 / 2 with a dynamic k.
+template <class R>
+struct Pin {
+  uint32_t index;
+  Vt<R> target;
+  R ghat;
+  bool kinematic;
+  R stiffness;
+};
+
+// Pull (implicit.rs:264-282, the reference's PullPair): w |x - target|^2 / 2.
+template <class R>
+struct Pull {
+  uint32_t index;
+  Vt<R> target;
+  R weight;
+};
+
+// A face under the strain-limit barrier: its element, allowed stretch fraction and mass.
+template <class R>
+struct SlFace {
+  ShellEl<R> el;
+  R limit, mass;
 };
 
 struct StepStats {
@@ -1178,6 +1339,10 @@ struct ImplicitSolver {
   std::vector<Edge> edges;
   R char_len = 1;
   std::vector<R> vertex_area;
+  std::vector<Pin<R>> pins;
+  std::vector<Pull<R>> pulls;
+  std::vector<SlFace<R>> sl_faces;
+  std::vector<std::array<R, 2>> uvs;
   LinearSolver linear;
   std::vector<StepStats> history;
 
@@ -1274,6 +1439,54 @@ struct ImplicitSolver {
     }
     collider_pn = pseudonormals(positions, collider_tris);
     return true;
+  }
+
+  // set_pins (implicit.rs:826-838): all or nothing; false for a vertex out of range or a
+  // ghat that is not positive.
+  bool set_pins(const std::vector<Pin<R>>& p) {
+    for (auto& q : p)
+      if (q.index >= positions.size() || std::isnan(q.ghat) || q.ghat <= 0) return false;
+    pins = p;
+    return true;
+  }
+
+  // set_pulls (implicit.rs:852-864): false for a vertex out of range or a weight that is not
+  // positive.
+  bool set_pulls(const std::vector<Pull<R>>& p) {
+    for (auto& q : p)
+      if (q.index >= positions.size() || std::isnan(q.weight) || q.weight <= 0) return false;
+    pulls = p;
+    return true;
+  }
+
+  // set_strain_limit_faces (implicit.rs:1088-1121): faces with a positive limit (allowed
+  // stretch fraction) and mass, rest shape from the current positions, degenerate faces
+  // skipped. False when the arrays' lengths disagree.
+  bool set_strain_limit_faces(const std::vector<Tri>& faces, const std::vector<R>& limits,
+                              const std::vector<R>& masses) {
+    if (limits.size() != faces.size() || masses.size() != faces.size()) return false;
+    std::vector<SlFace<R>> out;
+    for (size_t i = 0; i < faces.size(); ++i) {
+      if (limits[i] <= 0 || masses[i] <= 0) continue;
+      const Tri& f = faces[i];
+      SlFace<R> sf;
+      sf.el.v[0] = f[0]; sf.el.v[1] = f[1]; sf.el.v[2] = f[2];
+      if (!build_shell(positions[f[0]], positions[f[1]], positions[f[2]], R(1.0e-12), sf.el)) continue;
+      sf.limit = limits[i];
+      sf.mass = masses[i];
+      out.push_back(sf);
+    }
+    sl_faces = out;
+    return true;
+  }
+
+  // edge_strain_ratio (implicit.rs:798-817): the warp ratio, or with a weft ratio set and
+  // per-vertex UVs present, warp for an edge more U-aligned in UV space, else weft.
+  R edge_strain_ratio(uint32_t a, uint32_t b) const {
+    R warp = params.strain_limit_ratio, weft = params.strain_limit_ratio_weft;
+    if (weft <= 0 || uvs.size() != positions.size()) return warp;
+    R du = std::fabs(uvs[a][0] - uvs[b][0]), dv = std::fabs(uvs[a][1] - uvs[b][1]);
+    return du >= dv ? warp : weft;
   }
 
   std::vector<uint8_t> movable_mask() const {
@@ -1409,8 +1622,17 @@ struct ImplicitSolver {
     for (size_t i = 0; i < n; ++i) pinned[i] = inv_mass[i] <= 0;
     std::vector<Stencil<R>> sc = params.self_collision ? self_collision_stencils(x) : std::vector<Stencil<R>>();
     if (nstencils) *nstencils = (uint32_t)sc.size();
-    bool want_diag = !colliders.empty() && params.contact_rayleigh;
+    bool want_diag = !pins.empty() || !pulls.empty() || (!colliders.empty() && params.contact_rayleigh);
     std::unordered_map<uint64_t, size_t> slots;
+    for (auto& f : sl_faces)
+      for (uint32_t a : f.el.v)
+        for (uint32_t b : f.el.v) {
+          uint64_t key = ((uint64_t)a << 32) | b;
+          if (!slots.count(key)) {
+            size_t kk = slots.size();
+            slots[key] = kk;
+          }
+        }
     for (auto& s : sc)
       for (int a = 0; a < 4; ++a)
         for (int b = 0; b < 4; ++b) {
@@ -1474,6 +1696,25 @@ struct ImplicitSolver {
           trips.push(3 * a + r, 3 * b + cc, -v);
           trips.push(3 * b + r, 3 * a + cc, -v);
         }
+      // one-sided strain limit on the same edge (implicit.rs:2508-2530)
+      R slk = params.strain_limit_k, slr = edge_strain_ratio(a, b);
+      if (slr > 0 && slk > 0) {
+        V sg;
+        R sh[3][3];
+        edge_strain_block(x[a], x[b], stretch_rest[e], slr, slk, sg, sh);
+        for (int c = 0; c < 3; ++c) {
+          grad[3 * a + c] += sg[c];
+          grad[3 * b + c] -= sg[c];
+        }
+        for (int r = 0; r < 3; ++r)
+          for (int cc = 0; cc < 3; ++cc) {
+            R v = sh[r][cc];
+            trips.push(3 * a + r, 3 * a + cc, v);
+            trips.push(3 * b + r, 3 * b + cc, v);
+            trips.push(3 * a + r, 3 * b + cc, -v);
+            trips.push(3 * b + r, 3 * a + cc, -v);
+          }
+      }
     }
     // shells
     if (!shells.empty() && (params.shell_mu > 0 || params.shell_lambda > 0 || !shell_k.empty())) {
@@ -1523,6 +1764,84 @@ struct ImplicitSolver {
               }
           }
         }
+      }
+    }
+    // strain-limit barrier (implicit.rs:2743-2807): every elastic term is in, so the
+    // gathered blocks give each face the elastic half of its stiffness, w.(H_elastic w) with
+    // w the face's positions about their centroid, unnormalised.
+    if (!sl_faces.empty()) {
+      auto blocks = trips.blocks;
+      for (auto& f : sl_faces) {
+        const uint32_t* vs = f.el.v;
+        V p[3] = {x[vs[0]], x[vs[1]], x[vs[2]]};
+        V centroid = (p[0] + p[1] + p[2]) / R(3);
+        V w[3] = {p[0] - centroid, p[1] - centroid, p[2] - centroid};
+        R elastic_k = 0;
+        for (int ia = 0; ia < 3; ++ia)
+          for (int ib = 0; ib < 3; ++ib) {
+            auto it = slots.find(((uint64_t)vs[ia] << 32) | vs[ib]);
+            if (it == slots.end()) continue;
+            const auto& blk = blocks[it->second];
+            for (int r = 0; r < 3; ++r)
+              for (int c = 0; c < 3; ++c) elastic_k += w[ia][r] * blk[3 * r + c] * w[ib][c];
+          }
+        V eg[3];
+        R eh[81];
+        if (!strain_limit_eval(p, f.el, f.limit, f.mass, elastic_k, params.barrier_kind, params.eiganalysis_eps, true,
+                               eg, eh))
+          continue;
+        for (int a = 0; a < 3; ++a) {
+          uint32_t va = vs[a];
+          for (int c = 0; c < 3; ++c) grad[3 * va + c] += eg[a][c];
+          for (int b = 0; b < 3; ++b) {
+            uint32_t vb = vs[b];
+            for (int r = 0; r < 3; ++r)
+              for (int cc = 0; cc < 3; ++cc) {
+                R v = eh[(3 * a + r) * 9 + (3 * b + cc)];
+                if (v != 0) trips.push(3 * va + r, 3 * vb + cc, v);
+              }
+          }
+        }
+      }
+    }
+    // pins (implicit.rs:2809-2856): k = (H w).w / |w|^2 + m / gap^2 from the vertex's own
+    // elastic diagonal block, gap = max(ghat - |w|, constraint_tol ghat); kinematic pins
+    // scale k by their stiffness.
+    if (!pins.empty()) {
+      auto diag = trips.diag;
+      for (auto& pin : pins) {
+        size_t i = pin.index;
+        if (inv_mass[i] <= 0) continue;
+        R m = R(1) / inv_mass[i];
+        V w = x[i] - pin.target;
+        R d = w.length();
+        R floor = params.constraint_tol * pin.ghat;
+        R gap = rmax(pin.ghat - d, floor);
+        R d2 = w.length_squared();
+        R tmp = 0;
+        if (d2 > 0) {
+          const auto& hb = diag[i];
+          V hw(hb[0] * w.x + hb[1] * w.y + hb[2] * w.z, hb[3] * w.x + hb[4] * w.y + hb[5] * w.z,
+               hb[6] * w.x + hb[7] * w.y + hb[8] * w.z);
+          tmp = hw.dot(w) / d2;
+        }
+        R kp = tmp + m / (gap * gap);
+        if (pin.kinematic) kp *= pin.stiffness;
+        V gp = w * kp;
+        for (int c = 0; c < 3; ++c) {
+          grad[3 * i + c] += gp[c];
+          trips.push((uint32_t)(3 * i + c), (uint32_t)(3 * i + c), kp);
+        }
+      }
+    }
+    // pulls (implicit.rs:2858-2872)
+    for (auto& pl : pulls) {
+      size_t i = pl.index;
+      if (inv_mass[i] <= 0) continue;
+      V d = (x[i] - pl.target) * pl.weight;
+      for (int c = 0; c < 3; ++c) {
+        grad[3 * i + c] += d[c];
+        trips.push((uint32_t)(3 * i + c), (uint32_t)(3 * i + c), pl.weight);
       }
     }
     // analytic colliders (implicit.rs:2954-3021)
@@ -1593,13 +1912,59 @@ struct ImplicitSolver {
     return sink.finish(pinned);
   }
 
-  // ccd_max_step (implicit.rs:1690-1947) without strain limiting and pins
+  // ccd_max_step (implicit.rs:1690-1947)
   R ccd_max_step(const std::vector<V>& x, const std::vector<V>& dx, uint32_t* cap_hits) const {
     bool has_self = params.self_collision;
-    if (colliders.empty() && !has_self) return 1;
+    bool has_static_pins = false;
+    for (auto& p : pins)
+      if (!p.kinematic) has_static_pins = true;
+    if (colliders.empty() && !has_self && !has_static_pins && sl_faces.empty()) return 1;
     const R GAP = R(0.2), T_MIN = 0;
     size_t n = x.size();
     R t = 1;
+    // strain-limit line search (implicit.rs:1709-1753): per face, bisect the step fraction
+    // on max(sigma(x + t dx) - 1) < limit over [0, 1.25] until the window stops shrinking.
+    if (!sl_faces.empty()) {
+      const R LS_MAX_T = R(1.25);
+      for (auto& f : sl_faces) {
+        const uint32_t* vs = f.el.v;
+        auto at = [&](R frac) {
+          V p[3] = {x[vs[0]] + dx[vs[0]] * frac, x[vs[1]] + dx[vs[1]] * frac, x[vs[2]] + dx[vs[2]] * frac};
+          return max_stretch_excess(p, f.el.dm_inv);
+        };
+        if (at(LS_MAX_T) < f.limit) continue;
+        R lo = 0, hi = LS_MAX_T;
+        R window = hi - lo;
+        for (int it = 0; it < 64; ++it) {
+          R mid = R(0.5) * (lo + hi);
+          if (at(mid) - f.limit < 0)
+            lo = mid;
+          else
+            hi = mid;
+          R w = hi - lo;
+          if (w == window) break;
+          window = w;
+        }
+        t = rmin(t, lo);
+      }
+    }
+    // static-pin confinement (implicit.rs:1755-1789): radius interpolated linearly over the
+    // extended horizon 1.25 dx, clamped to land on the ghat sphere.
+    if (has_static_pins) {
+      const R LS_MAX_T = R(1.25);
+      for (auto& pin : pins) {
+        if (pin.kinematic) continue;
+        size_t i = pin.index;
+        if (inv_mass[i] <= 0) continue;
+        R r0 = (x[i] - pin.target).length();
+        if (r0 >= pin.ghat) continue;
+        R r1 = (x[i] + dx[i] * LS_MAX_T - pin.target).length();
+        if (r1 > pin.ghat) {
+          R denom = r1 - r0;
+          if (denom != 0) t = rmin(t, LS_MAX_T * (pin.ghat - r0) / denom);
+        }
+      }
+    }
     for (size_t i = 0; i < n; ++i) {
       if (inv_mass[i] <= 0) continue;
       for (auto& c : colliders) {

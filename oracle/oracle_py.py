@@ -229,6 +229,14 @@ def _step_sigs(lib):
         "oracle_stitch": (None, [vp, vp, C.c_double, C.c_double, vp, vp]),
         "oracle_solver_set_shells": (None, [vp, C.c_uint32, vp, vp, vp, vp]),
         "oracle_solver_scale_stitches": (None, [vp, vp]),
+        "oracle_solver_set_pins": (i32, [vp, u32, vp, vp, vp, vp, vp]),
+        "oracle_solver_set_pulls": (i32, [vp, u32, vp, vp, vp]),
+        "oracle_solver_set_strain_limit_faces": (i32, [vp, u32, vp, vp, vp, u32, u32]),
+        "oracle_solver_set_limits": (None, [vp, C.c_double, C.c_double, C.c_double, C.c_double, u32, vp]),
+        "oracle_solver_set_stretch_edges": (None, [vp, u32, vp]),
+        "oracle_strain_limit_face": (i32, [i32, i32, vp, vp, C.c_double, C.c_double, C.c_double, C.c_double, i32,
+                                           vp, vp, vp]),
+        "oracle_edge_strain": (f32, [vp, vp, f32, f32, f32, vp, vp]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -329,6 +337,51 @@ class OracleSolver:
         m = np.ascontiguousarray(mu, np.float64)
         l_ = np.ascontiguousarray(lam, np.float64)
         self.lib.oracle_solver_set_shells(self.h, f.shape[0], _p(f), _p(r), _p(m), _p(l_))
+
+    def set_pins(self, pins) -> bool:
+        """Pins (implicit.rs:826-838), each (index, target xyz, ghat, kinematic, stiffness);
+        all or nothing: False, with the previous pins kept, when one is out of range or has
+        ghat <= 0."""
+        n = len(pins)
+        idx = np.array([p[0] for p in pins], np.uint32)
+        tgt = np.array([p[1] for p in pins], np.float64).reshape(n, 3)
+        gh = np.array([p[2] for p in pins], np.float64)
+        kin = np.array([1 if p[3] else 0 for p in pins], np.int32)
+        st = np.array([p[4] for p in pins], np.float64)
+        return bool(self.lib.oracle_solver_set_pins(self.h, n, _p(idx), _p(tgt), _p(gh), _p(kin), _p(st)))
+
+    def set_pulls(self, pulls) -> bool:
+        """Pulls (implicit.rs:852-864), each (index, target xyz, weight)."""
+        n = len(pulls)
+        idx = np.array([p[0] for p in pulls], np.uint32)
+        tgt = np.array([p[1] for p in pulls], np.float64).reshape(n, 3)
+        w = np.array([p[2] for p in pulls], np.float64)
+        return bool(self.lib.oracle_solver_set_pulls(self.h, n, _p(idx), _p(tgt), _p(w)))
+
+    def set_strain_limit_faces(self, faces, limits, masses) -> int:
+        """Strain-limit barrier faces (implicit.rs:1088-1121), rest shape from the current
+        positions; returns the number kept. Raises ValueError when the lengths disagree."""
+        f = np.ascontiguousarray(faces, np.uint32).reshape(-1, 3)
+        lim = np.ascontiguousarray(limits, np.float64).reshape(-1)
+        m = np.ascontiguousarray(masses, np.float64).reshape(-1)
+        k = self.lib.oracle_solver_set_strain_limit_faces(self.h, f.shape[0], _p(f), _p(lim), _p(m), lim.size, m.size)
+        if k < 0:
+            raise ValueError(f"strain-limit arrays must match the face count: {f.shape[0]} faces, "
+                             f"{lim.size} limits, {m.size} masses")
+        return int(k)
+
+    def set_limits(self, constraint_tol=1e-2, strain_limit_ratio=0.0, strain_limit_k=0.0,
+                   strain_limit_ratio_weft=0.0, uvs=None):
+        """Pin gap floor, per-edge strain limit and per-vertex UVs (the ImplicitParams fields
+        of the same names; uvs None clears them)."""
+        uv = None if uvs is None else np.ascontiguousarray(uvs, np.float64).reshape(-1, 2)
+        self.lib.oracle_solver_set_limits(self.h, constraint_tol, strain_limit_ratio, strain_limit_k,
+                                          strain_limit_ratio_weft, 0 if uv is None else uv.shape[0], _p(uv))
+
+    def set_stretch_edges(self, edges):
+        """Replace the stretch edges (rest lengths from the current positions)."""
+        e = np.ascontiguousarray(edges, np.uint32).reshape(-1, 2)
+        self.lib.oracle_solver_set_stretch_edges(self.h, e.shape[0], _p(e))
 
     def scale_stitches(self, factor):
         f = np.ascontiguousarray(factor, np.float64)
@@ -435,3 +488,30 @@ def stitch(x6, w6, l0, lcap):
     h = np.zeros(324, np.float64)
     lib.oracle_stitch(_p(x), _p(w), l0, lcap, _p(g), _p(h))
     return g.reshape(6, 3), h.reshape(18, 18)
+
+
+def strain_limit_face(rest, p, limit, kind="cubic", mass=0.0, elastic_k=0.0, eps=1e-6, dynamic=False, f64=False):
+    """Strain-limit barrier of one face (shell_model.rs:438-640): (energy, gradient 3x3,
+    Hessian 9x9, active); None for a degenerate rest face."""
+    lib = _lib_elem()
+    r = np.ascontiguousarray(rest, np.float64).reshape(9)
+    q = np.ascontiguousarray(p, np.float64).reshape(9)
+    e = np.zeros(1, np.float64)
+    g = np.zeros(9, np.float64)
+    h = np.zeros(81, np.float64)
+    on = lib.oracle_strain_limit_face(1 if f64 else 0, 0 if kind == "log" else 1, _p(r), _p(q), limit, mass,
+                                      elastic_k, eps, 1 if dynamic else 0, _p(e), _p(g), _p(h))
+    if on < 0:
+        return None
+    return float(e[0]), g.reshape(3, 3), h.reshape(9, 9), bool(on)
+
+
+def edge_strain(xi, xj, rest, ratio, k):
+    """One-sided edge strain limit (strain_limit.rs:31-63) in f32: (energy, grad_i, h_ii)."""
+    lib = _lib_elem()
+    a = np.ascontiguousarray(xi, np.float32)
+    b = np.ascontiguousarray(xj, np.float32)
+    g = np.zeros(3, np.float32)
+    h = np.zeros(9, np.float32)
+    e = lib.oracle_edge_strain(_p(a), _p(b), rest, ratio, k, _p(g), _p(h))
+    return float(e), g, h.reshape(3, 3)

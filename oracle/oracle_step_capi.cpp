@@ -172,6 +172,84 @@ static void set_shells(ImplicitSolver<R>& s, uint32_t n, const uint32_t* faces, 
   }
 }
 
+template <class R>
+static int set_pins_t(ImplicitSolver<R>& s, uint32_t n, const uint32_t* idx, const double* target, const double* ghat,
+                      const int* kinematic, const double* stiffness) {
+  std::vector<Pin<R>> p(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    p[i].index = idx[i];
+    p[i].target = Vt<R>((R)target[3 * i], (R)target[3 * i + 1], (R)target[3 * i + 2]);
+    p[i].ghat = (R)ghat[i];
+    p[i].kinematic = kinematic[i] != 0;
+    p[i].stiffness = (R)stiffness[i];
+  }
+  return s.set_pins(p);
+}
+
+template <class R>
+static int set_pulls_t(ImplicitSolver<R>& s, uint32_t n, const uint32_t* idx, const double* target,
+                       const double* weight) {
+  std::vector<Pull<R>> p(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    p[i].index = idx[i];
+    p[i].target = Vt<R>((R)target[3 * i], (R)target[3 * i + 1], (R)target[3 * i + 2]);
+    p[i].weight = (R)weight[i];
+  }
+  return s.set_pulls(p);
+}
+
+template <class R>
+static int set_sl_faces_t(ImplicitSolver<R>& s, uint32_t n, const uint32_t* faces, const double* limits,
+                          const double* masses, uint32_t nl, uint32_t nm) {
+  std::vector<std::array<uint32_t, 3>> f(n);
+  for (uint32_t i = 0; i < n; ++i) f[i] = {faces[3 * i], faces[3 * i + 1], faces[3 * i + 2]};
+  std::vector<R> l(limits, limits + nl), m(masses, masses + nm);
+  if (!s.set_strain_limit_faces(f, l, m)) return -1;
+  return (int)s.sl_faces.size();
+}
+
+template <class R>
+static void set_limits_t(ImplicitSolver<R>& s, double constraint_tol, double ratio, double k, double ratio_weft,
+                         uint32_t nuv, const double* uv) {
+  s.params.constraint_tol = (R)constraint_tol;
+  s.params.strain_limit_ratio = (R)ratio;
+  s.params.strain_limit_k = (R)k;
+  s.params.strain_limit_ratio_weft = (R)ratio_weft;
+  s.uvs.assign(nuv, {});
+  for (uint32_t i = 0; i < nuv; ++i) s.uvs[i] = {(R)uv[2 * i], (R)uv[2 * i + 1]};
+}
+
+template <class R>
+static void set_stretch_edges_t(ImplicitSolver<R>& s, uint32_t n, const uint32_t* edges) {
+  s.stretch_edges.assign(n, {});
+  s.stretch_rest.assign(n, R(0));
+  for (uint32_t i = 0; i < n; ++i) {
+    s.stretch_edges[i] = {edges[2 * i], edges[2 * i + 1]};
+    s.stretch_rest[i] = (s.positions[edges[2 * i]] - s.positions[edges[2 * i + 1]]).length();
+  }
+}
+
+template <class R>
+static int strain_limit_face_t(int kind, const double* rest9, const double* p9, double limit, double mass,
+                               double elastic_k, double eps, int dynamic, double* energy, double* grad9,
+                               double* hess81) {
+  ShellEl<R> el;
+  Vt<R> r[3], p[3];
+  for (int k = 0; k < 3; ++k) {
+    r[k] = Vt<R>((R)rest9[3 * k], (R)rest9[3 * k + 1], (R)rest9[3 * k + 2]);
+    p[k] = Vt<R>((R)p9[3 * k], (R)p9[3 * k + 1], (R)p9[3 * k + 2]);
+  }
+  if (!build_shell(r[0], r[1], r[2], R(1.0e-12), el)) return -1;
+  *energy = strain_limit_energy(p, el, (R)limit, (BarrierKind)kind);
+  Vt<R> g[3];
+  R h[81];
+  bool on = strain_limit_eval(p, el, (R)limit, (R)mass, (R)elastic_k, (BarrierKind)kind, (R)eps, dynamic != 0, g, h);
+  for (int k = 0; k < 3; ++k)
+    for (int c = 0; c < 3; ++c) grad9[3 * k + c] = on ? (double)g[k][c] : 0.0;
+  for (int k = 0; k < 81; ++k) hess81[k] = on ? (double)h[k] : 0.0;
+  return on ? 1 : 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -252,6 +330,49 @@ int oracle_solver_set_kinematic(void* h, const double* pos) {
   std::vector<Vt<double>> x(a->d->positions.size());
   for (size_t i = 0; i < x.size(); ++i) x[i] = Vt<double>(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
   return a->d->set_kinematic_collider_positions(x);
+}
+
+// Pins (FixPair): 1 when accepted, 0 when rejected (nothing changed).
+int oracle_solver_set_pins(void* h, uint32_t n, const uint32_t* idx, const double* target, const double* ghat,
+                           const int* kinematic, const double* stiffness) {
+  auto* a = (AnySolver*)h;
+  return a->prec == 0 ? set_pins_t(*a->f, n, idx, target, ghat, kinematic, stiffness)
+                      : set_pins_t(*a->d, n, idx, target, ghat, kinematic, stiffness);
+}
+
+// Pulls (PullPair): 1 when accepted, 0 when rejected.
+int oracle_solver_set_pulls(void* h, uint32_t n, const uint32_t* idx, const double* target, const double* weight) {
+  auto* a = (AnySolver*)h;
+  return a->prec == 0 ? set_pulls_t(*a->f, n, idx, target, weight) : set_pulls_t(*a->d, n, idx, target, weight);
+}
+
+// Strain-limit barrier faces: the number of faces kept, or -1 when the lengths disagree.
+int oracle_solver_set_strain_limit_faces(void* h, uint32_t n, const uint32_t* faces, const double* limits,
+                                         const double* masses, uint32_t nl, uint32_t nm) {
+  auto* a = (AnySolver*)h;
+  return a->prec == 0 ? set_sl_faces_t(*a->f, n, faces, limits, masses, nl, nm)
+                      : set_sl_faces_t(*a->d, n, faces, limits, masses, nl, nm);
+}
+
+// Pin gap floor, per-edge strain limit (warp ratio, stiffness, weft ratio) and per-vertex
+// UVs (nuv pairs; 0 clears them).
+void oracle_solver_set_limits(void* h, double constraint_tol, double ratio, double k, double ratio_weft, uint32_t nuv,
+                              const double* uv) {
+  auto* a = (AnySolver*)h;
+  if (a->prec == 0)
+    set_limits_t(*a->f, constraint_tol, ratio, k, ratio_weft, nuv, uv);
+  else
+    set_limits_t(*a->d, constraint_tol, ratio, k, ratio_weft, nuv, uv);
+}
+
+// Replaces the stretch edges (a mesh with explicit edges, as the reference's Mesh carries);
+// rest lengths from the current positions.
+void oracle_solver_set_stretch_edges(void* h, uint32_t n, const uint32_t* edges) {
+  auto* a = (AnySolver*)h;
+  if (a->prec == 0)
+    set_stretch_edges_t(*a->f, n, edges);
+  else
+    set_stretch_edges_t(*a->d, n, edges);
 }
 
 void oracle_solver_set_state(void* h, const double* pos, const double* vel) {
@@ -372,12 +493,12 @@ float oracle_accd(const float* x12, const float* dx12, float offset, float max_t
 
 int oracle_barrier(int kind, double d, double dhat, double kappa, int f64, double* egh) {
   if (f64) {
-    double e, g, h;
+    double e = 0, g = 0, h = 0;
     bool on = barrier_of<double>((BarrierKind)kind, d, dhat, kappa, e, g, h);
     egh[0] = e; egh[1] = g; egh[2] = h;
     return on;
   }
-  float e, g, h;
+  float e = 0, g = 0, h = 0;
   bool on = barrier_of<float>((BarrierKind)kind, (float)d, (float)dhat, (float)kappa, e, g, h);
   egh[0] = e; egh[1] = g; egh[2] = h;
   return on;
@@ -394,6 +515,27 @@ int oracle_friction(const float* fc3, const float* dx3, const float* n3, float m
   for (int r = 0; r < 3; ++r)
     for (int c = 0; c < 3; ++c) h9[3 * r + c] = on ? h[r][c] : 0.f;
   return on;
+}
+
+// Strain-limit barrier of one face (rest shape rest9): energy, and the gradient and Hessian
+// at unit stiffness (dynamic = 0) or as assembled (dynamic = 1: elastic_k + mass / d^2).
+// Returns 1 active, 0 inactive, -1 degenerate rest face.
+int oracle_strain_limit_face(int f64, int kind, const double* rest9, const double* p9, double limit, double mass,
+                             double elastic_k, double eps, int dynamic, double* energy, double* grad9,
+                             double* hess81) {
+  return f64 ? strain_limit_face_t<double>(kind, rest9, p9, limit, mass, elastic_k, eps, dynamic, energy, grad9, hess81)
+             : strain_limit_face_t<float>(kind, rest9, p9, limit, mass, elastic_k, eps, dynamic, energy, grad9, hess81);
+}
+
+// One-sided edge strain limit in f32: energy, grad_i g3 and h_ii h9 (row-major).
+float oracle_edge_strain(const float* xi3, const float* xj3, float rest, float ratio, float k, float* g3, float* h9) {
+  Vt<float> xi(xi3[0], xi3[1], xi3[2]), xj(xj3[0], xj3[1], xj3[2]), g;
+  float h[3][3];
+  edge_strain_block(xi, xj, rest, ratio, k, g, h);
+  for (int c = 0; c < 3; ++c) g3[c] = g[c];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) h9[3 * r + c] = h[r][c];
+  return edge_strain_energy(xi, xj, rest, ratio, k);
 }
 
 float oracle_rayleigh(int n, const float* elastic, const float* mass, const float* weights, const float* e3,
