@@ -237,6 +237,11 @@ def _step_sigs(lib):
         "oracle_strain_limit_face": (i32, [i32, i32, vp, vp, C.c_double, C.c_double, C.c_double, C.c_double, i32,
                                            vp, vp, vp]),
         "oracle_edge_strain": (f32, [vp, vp, f32, f32, f32, vp, vp]),
+        "oracle_vt_pairs": (C.c_uint64, [u32, vp, u32, vp, f32, i32, vp, vp, C.c_uint64]),
+        "oracle_ee_pairs": (C.c_uint64, [u32, vp, u32, vp, f32, vp, vp, C.c_uint64]),
+        "oracle_unique_edges": (u32, [u32, vp, vp]),
+        "oracle_grid_cell": (f32, [f32, f32]),
+        "oracle_edge_triangle_intersect": (i32, [vp]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -515,3 +520,46 @@ def edge_strain(xi, xj, rest, ratio, k):
     h = np.zeros(9, np.float32)
     e = lib.oracle_edge_strain(_p(a), _p(b), rest, ratio, k, _p(g), _p(h))
     return float(e), g, h.reshape(3, 3)
+
+
+def _pairs(fn, *args):
+    n = fn(*args, None, 0)
+    out = np.empty((max(n, 1), 2), np.uint32)
+    fn(*args, _p(out), n)
+    return [tuple(r) for r in out[:n].tolist()]
+
+
+def vt_pairs(pos, tris, search, exclude_one_ring=True, movable=None):
+    """vertex_triangle_pairs (broadphase.rs:250-264): sorted unique (vertex, triangle)."""
+    lib = _lib_elem()
+    p = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+    t = np.ascontiguousarray(tris, np.uint32).reshape(-1, 3)
+    m = None if movable is None or len(movable) == 0 else np.ascontiguousarray(movable, np.uint8)
+    return _pairs(lib.oracle_vt_pairs, p.shape[0], _p(p), t.shape[0], _p(t), search, 1 if exclude_one_ring else 0,
+                  _p(m))
+
+
+def ee_pairs(pos, edges, search, movable=None):
+    """edge_edge_pairs (broadphase.rs:356-367): sorted unique (ei, ej), ei < ej."""
+    lib = _lib_elem()
+    p = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+    e = np.ascontiguousarray(edges, np.uint32).reshape(-1, 2)
+    m = None if movable is None or len(movable) == 0 else np.ascontiguousarray(movable, np.uint8)
+    return _pairs(lib.oracle_ee_pairs, p.shape[0], _p(p), e.shape[0], _p(e), search, _p(m))
+
+
+def unique_edges(tris):
+    """unique_edges (broadphase.rs:332-343): sorted (min, max) vertex pairs."""
+    lib = _lib_elem()
+    t = np.ascontiguousarray(tris, np.uint32).reshape(-1, 3)
+    out = np.empty((3 * max(t.shape[0], 1), 2), np.uint32)
+    n = lib.oracle_unique_edges(t.shape[0], _p(t), _p(out))
+    return out[:n].copy()
+
+
+def grid_cell(search, extent):
+    return _lib_elem().oracle_grid_cell(search, extent)
+
+
+def edge_triangle_intersect(p0, p1, a, b, c):
+    return bool(_lib_elem().oracle_edge_triangle_intersect(_p(np.ascontiguousarray([p0, p1, a, b, c], np.float32))))

@@ -538,6 +538,68 @@ float oracle_edge_strain(const float* xi3, const float* xj3, float rest, float r
   return edge_strain_energy(xi, xj, rest, ratio, k);
 }
 
+// vertex_triangle_pairs / edge_edge_pairs (broadphase.rs:250-264, 356-367) in f32: the
+// candidate pairs sorted and deduplicated into out (2 u32 each, up to cap); returns the count.
+// exclude_one_ring applies one_ring_exclusion over tris; movable (u8 per vertex) may be null.
+uint64_t oracle_vt_pairs(uint32_t nv, const float* pos, uint32_t nt, const uint32_t* tris, float search,
+                         int exclude_one_ring, const uint8_t* movable, uint32_t* out, uint64_t cap) {
+  std::vector<Vt<float>> P(nv);
+  for (uint32_t i = 0; i < nv; ++i) P[i] = Vt<float>(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+  std::vector<std::array<uint32_t, 3>> T(nt);
+  for (uint32_t t = 0; t < nt; ++t) T[t] = {tris[3 * t], tris[3 * t + 1], tris[3 * t + 2]};
+  std::vector<std::vector<uint32_t>> ex = exclude_one_ring ? one_ring_exclusion(nv, T)
+                                                           : std::vector<std::vector<uint32_t>>(nv);
+  std::vector<uint8_t> mov = movable ? std::vector<uint8_t>(movable, movable + nv) : std::vector<uint8_t>();
+  std::vector<std::pair<uint32_t, uint32_t>> pr;
+  for_each_vertex_triangle_pair<float>(P, T, search, ex, mov, [&](uint32_t v, uint32_t t) { pr.push_back({v, t}); });
+  std::sort(pr.begin(), pr.end());
+  pr.erase(std::unique(pr.begin(), pr.end()), pr.end());
+  for (size_t i = 0; i < pr.size() && i < cap; ++i) {
+    out[2 * i] = pr[i].first;
+    out[2 * i + 1] = pr[i].second;
+  }
+  return pr.size();
+}
+
+uint64_t oracle_ee_pairs(uint32_t nv, const float* pos, uint32_t ne, const uint32_t* edges, float search,
+                         const uint8_t* movable, uint32_t* out, uint64_t cap) {
+  std::vector<Vt<float>> P(nv);
+  for (uint32_t i = 0; i < nv; ++i) P[i] = Vt<float>(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+  std::vector<std::array<uint32_t, 2>> E(ne);
+  for (uint32_t e = 0; e < ne; ++e) E[e] = {edges[2 * e], edges[2 * e + 1]};
+  std::vector<uint8_t> mov = movable ? std::vector<uint8_t>(movable, movable + nv) : std::vector<uint8_t>();
+  std::vector<std::pair<uint32_t, uint32_t>> pr;
+  for_each_edge_edge_pair<float>(P, E, search, mov, [&](uint32_t a, uint32_t b) { pr.push_back({a, b}); });
+  std::sort(pr.begin(), pr.end());
+  pr.erase(std::unique(pr.begin(), pr.end()), pr.end());
+  for (size_t i = 0; i < pr.size() && i < cap; ++i) {
+    out[2 * i] = pr[i].first;
+    out[2 * i + 1] = pr[i].second;
+  }
+  return pr.size();
+}
+
+// unique_edges (broadphase.rs:332-343) into out (2 u32 each, room for 3 nt); returns the count.
+uint32_t oracle_unique_edges(uint32_t nt, const uint32_t* tris, uint32_t* out) {
+  std::vector<std::array<uint32_t, 3>> T(nt);
+  for (uint32_t t = 0; t < nt; ++t) T[t] = {tris[3 * t], tris[3 * t + 1], tris[3 * t + 2]};
+  auto e = unique_edges(T);
+  for (size_t i = 0; i < e.size(); ++i) {
+    out[2 * i] = e[i][0];
+    out[2 * i + 1] = e[i][1];
+  }
+  return (uint32_t)e.size();
+}
+
+float oracle_grid_cell(float search, float extent) { return grid_cell(search, extent); }
+
+// edge_triangle_intersect (contact.rs:324-352) for the segment p0p1 against triangle abc.
+int oracle_edge_triangle_intersect(const float* p15) {
+  Vt<float> v[5];
+  for (int k = 0; k < 5; ++k) v[k] = Vt<float>(p15[3 * k], p15[3 * k + 1], p15[3 * k + 2]);
+  return edge_triangle_intersect(v[0], v[1], v[2], v[3], v[4]) ? 1 : 0;
+}
+
 float oracle_rayleigh(int n, const float* elastic, const float* mass, const float* weights, const float* e3,
                       float offset) {
   float el[16][9];
