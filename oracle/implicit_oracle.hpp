@@ -8,12 +8,15 @@
 //   engine-core/src/shell_model.rs (svd3x2, StVK derivatives, eigen-projected Hessian)
 //   engine-core/src/bending.rs   (hinges, dihedral angle, analytic gradient)
 //   engine-core/src/stitch.rs    (six-participant seam spring)
+//   engine-core/src/strain_limit.rs (one-sided edge strain limit)
 //   engine-core/src/broadphase.rs (uniform hash grid V-T / E-E, 1-ring exclusion)
 //   engine-core/src/implicit.rs  (new, stencils, Rayleigh gather, assemble + Asm push order,
-//                                 ccd_max_step, step)
-// Only the element kinds the synthetic configurations use are restated: inertia, stretch
-// springs, StVK shells, hinges, stitches, analytic colliders, static-mesh colliders with a
-// signed gap, and vertex-triangle / edge-edge self contact (+ friction when mu > 0).
+//                                 ccd_max_step with the strain-limit and static-pin clamps,
+//                                 pins, pulls, step)
+// Restated element kinds: inertia, stretch springs (+ the one-sided edge strain limit),
+// StVK shells, hinges, stitches, the per-face strain-limit barrier, pins and pulls, analytic
+// colliders, static-mesh colliders with a signed gap, and vertex-triangle / edge-edge self
+// contact (+ friction when mu > 0).
 // Added to both this oracle and the CUDA path: a Newton termination on the step actually
 // taken, max_i |t dx_i| < newton_tol (0 disables it).
 #pragma once

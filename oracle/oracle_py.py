@@ -242,6 +242,13 @@ def _step_sigs(lib):
         "oracle_unique_edges": (u32, [u32, vp, vp]),
         "oracle_grid_cell": (f32, [f32, f32]),
         "oracle_edge_triangle_intersect": (i32, [vp]),
+        "oracle_closest_point": (None, [vp, vp, vp]),
+        "oracle_ee_witness": (None, [vp, vp]),
+        "oracle_signed_point_tri": (f32, [vp, vp, vp]),
+        "oracle_collider_distance": (f32, [vp, vp, vp]),
+        "oracle_vertex_contact": (None, [vp, u32, vp, f32, f32, f32, f32, vp, vp]),
+        "oracle_dynamic_stiffness": (f32, [f32, f32, f32, f32, f32]),
+        "oracle_stencil_friction": (i32, [vp, vp, f32, f32, f32, vp, vp]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -563,3 +570,67 @@ def grid_cell(search, extent):
 
 def edge_triangle_intersect(p0, p1, a, b, c):
     return bool(_lib_elem().oracle_edge_triangle_intersect(_p(np.ascontiguousarray([p0, p1, a, b, c], np.float32))))
+
+
+def closest_point(p, a, b, c):
+    """closest_point_on_triangle_bary (contact.rs:84-124): (q, weights)."""
+    lib = _lib_elem()
+    x = np.ascontiguousarray([p, a, b, c], np.float32)
+    q = np.zeros(3, np.float32)
+    w = np.zeros(3, np.float32)
+    lib.oracle_closest_point(_p(x), _p(q), _p(w))
+    return q, w
+
+
+def ee_witness(p4):
+    """edge_edge_witness (contact.rs:238-311): weights (a0, a1, b0, b1)."""
+    lib = _lib_elem()
+    x = np.ascontiguousarray(p4, np.float32).reshape(12)
+    w = np.zeros(4, np.float32)
+    lib.oracle_ee_witness(_p(x), _p(w))
+    return w
+
+
+def signed_point_tri(p, a, b, c):
+    """The signed point-triangle gap of a one-triangle collider: (gap, gradient 4x3, inside)."""
+    lib = _lib_elem()
+    x = np.ascontiguousarray([p, a, b, c], np.float32)
+    g = np.zeros(12, np.float32)
+    inside = np.zeros(1, np.int32)
+    d = lib.oracle_signed_point_tri(_p(x), _p(g), _p(inside))
+    return d, g.reshape(4, 3), bool(inside[0])
+
+
+def collider_distance(col8, x):
+    lib = _lib_elem()
+    c = np.ascontiguousarray(col8, np.float32)
+    xx = np.ascontiguousarray(x, np.float32)
+    n = np.zeros(3, np.float32)
+    d = lib.oracle_collider_distance(_p(c), _p(xx), _p(n))
+    return d, n
+
+
+def vertex_contact(x, colliders, dhat, kappa, coupling, mass):
+    """vertex_contact (contact.rs:1029-1050): (gradient, Hessian 3x3)."""
+    lib = _lib_elem()
+    xx = np.ascontiguousarray(x, np.float32)
+    cs = np.ascontiguousarray(colliders, np.float32).reshape(-1, 8)
+    g = np.zeros(3, np.float32)
+    h = np.zeros(9, np.float32)
+    lib.oracle_vertex_contact(_p(xx), cs.shape[0], _p(cs), dhat, kappa, coupling, mass, _p(g), _p(h))
+    return g, h.reshape(3, 3)
+
+
+def dynamic_stiffness(base, coupling, mass, gap, dhat):
+    return _lib_elem().oracle_dynamic_stiffness(base, coupling, mass, gap, dhat)
+
+
+def stencil_friction(g4, dx4, barrier_grad, mu, eps):
+    """stencil_friction (contact.rs:659-705): (gradient 4x3, Hessian 12x12), zeros when off."""
+    lib = _lib_elem()
+    g = np.ascontiguousarray(g4, np.float32).reshape(12)
+    d = np.ascontiguousarray(dx4, np.float32).reshape(12)
+    fg = np.zeros(12, np.float32)
+    fh = np.zeros(144, np.float32)
+    lib.oracle_stencil_friction(_p(g), _p(d), barrier_grad, mu, eps, _p(fg), _p(fh))
+    return fg.reshape(4, 3), fh.reshape(12, 12)

@@ -600,6 +600,97 @@ int oracle_edge_triangle_intersect(const float* p15) {
   return edge_triangle_intersect(v[0], v[1], v[2], v[3], v[4]) ? 1 : 0;
 }
 
+// closest_point_on_triangle_bary (contact.rs:84-124): q3 and weights w3 for p12 = p, a, b, c.
+void oracle_closest_point(const float* p12, float* q3, float* w3) {
+  Vt<float> v[4];
+  for (int k = 0; k < 4; ++k) v[k] = Vt<float>(p12[3 * k], p12[3 * k + 1], p12[3 * k + 2]);
+  Vt<float> q = closest_point_bary(v[0], v[1], v[2], v[3], w3);
+  for (int c = 0; c < 3; ++c) q3[c] = q[c];
+}
+
+// edge_edge_witness (contact.rs:238-311): the four witness weights for p12 = ea0, ea1, eb0, eb1.
+void oracle_ee_witness(const float* p12, float* w4) {
+  Vt<float> v[4];
+  for (int k = 0; k < 4; ++k) v[k] = Vt<float>(p12[3 * k], p12[3 * k + 1], p12[3 * k + 2]);
+  edge_edge_witness(v[0], v[1], v[2], v[3], w4);
+}
+
+// signed_point_tri_distance_grad (contact.rs:889-915) with the side taken the way the
+// stencil collection takes it for a one-triangle mesh: pseudonormals of that triangle,
+// surface_normal_at the closest point, inside when (p - q).n < 0. Returns the signed gap,
+// gradient in g12 and the side in *inside.
+float oracle_signed_point_tri(const float* p12, float* g12, int* inside) {
+  Vt<float> v[4];
+  for (int k = 0; k < 4; ++k) v[k] = Vt<float>(p12[3 * k], p12[3 * k + 1], p12[3 * k + 2]);
+  auto pn = pseudonormals<float>({v[1], v[2], v[3]}, {{0u, 1u, 2u}});
+  float w[3];
+  Vt<float> q = closest_point_bary(v[0], v[1], v[2], v[3], w);
+  Vt<float> pnv[3] = {pn[0], pn[1], pn[2]};
+  Vt<float> n = surface_normal_at(w, (v[2] - v[1]).cross(v[3] - v[1]).normalize_or_zero(), pnv);
+  bool in = (v[0] - q).dot(n) < 0;
+  Vt<float> g[4];
+  float d = signed_point_tri_distance_grad(v[0], v[1], v[2], v[3], in, g);
+  for (int k = 0; k < 4; ++k)
+    for (int c = 0; c < 3; ++c) g12[3 * k + c] = g[k][c];
+  *inside = in ? 1 : 0;
+  return d;
+}
+
+// Collider::distance (contact.rs:33-51) of col8 = (kind, a xyz, n xyz, radius) at x3.
+float oracle_collider_distance(const float* col8, const float* x3, float* n3) {
+  Collider<float> c;
+  c.kind = (int)col8[0];
+  c.a = Vt<float>(col8[1], col8[2], col8[3]);
+  c.n = Vt<float>(col8[4], col8[5], col8[6]);
+  c.radius = col8[7];
+  float d;
+  Vt<float> n;
+  c.distance(Vt<float>(x3[0], x3[1], x3[2]), d, n);
+  for (int k = 0; k < 3; ++k) n3[k] = n[k];
+  return d;
+}
+
+// vertex_contact (contact.rs:1029-1050): log barrier, dynamic stiffness, no friction.
+void oracle_vertex_contact(const float* x3, uint32_t ncol, const float* cols, float dhat, float kappa, float coupling,
+                           float mass, float* g3, float* h9) {
+  std::vector<Collider<float>> cs(ncol);
+  for (uint32_t i = 0; i < ncol; ++i) {
+    const float* c = cols + 8 * i;
+    cs[i].kind = (int)c[0];
+    cs[i].a = Vt<float>(c[1], c[2], c[3]);
+    cs[i].n = Vt<float>(c[4], c[5], c[6]);
+    cs[i].radius = c[7];
+  }
+  Vt<float> g;
+  float h[3][3];
+  vertex_contact_full<float>(Vt<float>(x3[0], x3[1], x3[2]), cs, dhat, kappa, coupling, mass, BarrierKind::Log,
+                             nullptr, false, Vt<float>(), 0.f, 0.f, g, h);
+  for (int c = 0; c < 3; ++c) g3[c] = g[c];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) h9[3 * r + c] = h[r][c];
+}
+
+float oracle_dynamic_stiffness(float base, float coupling, float mass, float gap, float dhat) {
+  return dynamic_stiffness(base, coupling, mass, gap, dhat);
+}
+
+// stencil_friction (contact.rs:659-705): gradient fg12 and Hessian fh144 (row-major);
+// 0 with both zeroed when nothing applies.
+int oracle_stencil_friction(const float* g12, const float* dx12, float barrier_grad, float mu, float eps, float* fg12,
+                            float* fh144) {
+  Vt<float> g[4], dx[4], fg[4];
+  for (int k = 0; k < 4; ++k) {
+    g[k] = Vt<float>(g12[3 * k], g12[3 * k + 1], g12[3 * k + 2]);
+    dx[k] = Vt<float>(dx12[3 * k], dx12[3 * k + 1], dx12[3 * k + 2]);
+  }
+  bool on = stencil_friction(g, dx, barrier_grad, mu, eps, fg, fh144);
+  for (int k = 0; k < 4; ++k)
+    for (int c = 0; c < 3; ++c) fg12[3 * k + c] = on ? fg[k][c] : 0.f;
+  if (!on)
+    for (int k = 0; k < 144; ++k) fh144[k] = 0.f;
+  return on ? 1 : 0;
+}
+
 float oracle_rayleigh(int n, const float* elastic, const float* mass, const float* weights, const float* e3,
                       float offset) {
   float el[16][9];
