@@ -153,7 +153,7 @@ class ImplicitSolver:
 
     @positions.setter
     def positions(self, p):
-        a = np.ascontiguousarray(p, np.float32)
+        a = np.ascontiguousarray(p, np.float32).reshape(self.nv, 3)
         check(self.lib.mguso_write_positions(self.h, ptr(a)))
 
     @property
@@ -164,7 +164,7 @@ class ImplicitSolver:
 
     @velocities.setter
     def velocities(self, v):
-        a = np.ascontiguousarray(v, np.float32)
+        a = np.ascontiguousarray(v, np.float32).reshape(self.nv, 3)
         check(self.lib.mguso_write_velocities(self.h, ptr(a)))
 
     def set_kinematic_collider_positions(self, x) -> None:

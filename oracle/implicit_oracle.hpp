@@ -1346,6 +1346,7 @@ struct ImplicitSolver {
   std::vector<Pull<R>> pulls;
   std::vector<SlFace<R>> sl_faces;
   std::vector<std::array<R, 2>> uvs;
+  std::vector<V> kinematic_dx;  // the static collider's move since the last step
   LinearSolver linear;
   std::vector<StepStats> history;
 
@@ -1425,18 +1426,21 @@ struct ImplicitSolver {
   }
 
   // set_kinematic_collider_positions (implicit.rs:1368-1398): move the static collider's
-  // vertices to x (its rows only), give them the velocity of that move over one step and
-  // recompute the pseudonormals. False, with nothing written, when there is no static
-  // collider, x has the wrong length or a collider row of x is not finite.
+  // vertices to x (its rows only), give them the velocity of that move over one step,
+  // accumulate the move into kinematic_dx (the friction slip of the next step) and recompute
+  // the pseudonormals. False, with nothing written, when there is no static collider, x has
+  // the wrong length or a collider row of x is not finite.
   bool set_kinematic_collider_positions(const std::vector<V>& x) {
     if (static_collider_vert.empty() || x.size() != positions.size()) return false;
     for (size_t i = 0; i < x.size(); ++i)
       if (static_collider_vert[i] && !(std::isfinite(x[i].x) && std::isfinite(x[i].y) && std::isfinite(x[i].z)))
         return false;
+    if (kinematic_dx.empty()) kinematic_dx.assign(x.size(), V());
     const R inv_h = R(1) / params.dt;
     for (size_t i = 0; i < x.size(); ++i) {
       if (!static_collider_vert[i]) continue;
       V d = x[i] - positions[i];
+      kinematic_dx[i] += d;
       positions[i] = x[i];
       velocities[i] = d * inv_h;
     }
@@ -1890,7 +1894,12 @@ struct ImplicitSolver {
         R mu_s = params.friction;
         if (mu_s > 0) {
           V dxs[4];
-          for (int a = 0; a < 4; ++a) dxs[a] = x[s.idx[a]] - positions[s.idx[a]];
+          // the slip is relative (fdx_override, implicit.rs:3068-3078): a re-posed collider
+          // vertex contributes the displacement it was moved by before this step
+          for (int a = 0; a < 4; ++a) {
+            uint32_t i = s.idx[a];
+            dxs[a] = x[i] - positions[i] + (kinematic_dx.empty() ? V() : kinematic_dx[i]);
+          }
           V fg[4];
           R fh[144];
           if (stencil_friction(s.g, dxs, bg, mu_s, params.friction_eps, fg, fh)) {
@@ -2138,6 +2147,8 @@ struct ImplicitSolver {
       }
     }
     time += (double)h;
+    // the collider move described this step only (implicit.rs:2065-2070)
+    for (auto& d : kinematic_dx) d = V();
     st.newton_iters = taken;
     st.all_finite = finite ? 1 : 0;
     // count_active_contacts (implicit.rs:2213-2232)

@@ -229,6 +229,7 @@ def _step_sigs(lib):
         "oracle_stitch": (None, [vp, vp, C.c_double, C.c_double, vp, vp]),
         "oracle_solver_set_shells": (None, [vp, C.c_uint32, vp, vp, vp, vp]),
         "oracle_solver_scale_stitches": (None, [vp, vp]),
+        "oracle_solver_collider_sides": (i32, [vp, vp]),
         "oracle_solver_set_pins": (i32, [vp, u32, vp, vp, vp, vp, vp]),
         "oracle_solver_set_pulls": (i32, [vp, u32, vp, vp, vp]),
         "oracle_solver_set_strain_limit_faces": (i32, [vp, u32, vp, vp, vp, u32, u32]),
@@ -304,6 +305,8 @@ class OracleSolver:
     def set_kinematic_collider_positions(self, x) -> bool:
         """Move the static collider to x (its rows; implicit.rs:1368-1398)."""
         p = np.ascontiguousarray(x, np.float64)
+        if p.size != 3 * self.nv:
+            return False  # a wrong-length array is refused, as the reference's setter does
         return bool(self.lib.oracle_solver_set_kinematic(self.h, _p(p)))
 
     def set_state(self, pos, vel):
@@ -349,6 +352,12 @@ class OracleSolver:
         m = np.ascontiguousarray(mu, np.float64)
         l_ = np.ascontiguousarray(lam, np.float64)
         self.lib.oracle_solver_set_shells(self.h, f.shape[0], _p(f), _p(r), _p(m), _p(l_))
+
+    def collider_sides(self):
+        """Per-vertex side of the static collider at the current positions (+1 outside, -1
+        inside; implicit.rs:1431-1480), or None without a static collider."""
+        out = np.ones(self.nv, np.float32)
+        return out if self.lib.oracle_solver_collider_sides(self.h, _p(out)) else None
 
     def set_pins(self, pins) -> bool:
         """Pins (implicit.rs:826-838), each (index, target xyz, ghat, kinematic, stiffness);

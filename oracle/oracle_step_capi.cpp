@@ -332,6 +332,16 @@ int oracle_solver_set_kinematic(void* h, const double* pos) {
   return a->d->set_kinematic_collider_positions(x);
 }
 
+// collider_sides (implicit.rs:1431-1475) at the current positions: +1 outside, -1 inside,
+// per vertex (f32[nv]); returns 0 when there is no static collider (nothing written).
+int oracle_solver_collider_sides(void* h, float* out) {
+  auto* a = (AnySolver*)h;
+  if (a->prec != 0) return 0;
+  auto side = a->f->collider_sides(a->f->positions);
+  for (size_t i = 0; i < side.size(); ++i) out[i] = side[i];
+  return side.empty() ? 0 : 1;
+}
+
 // Pins (FixPair): 1 when accepted, 0 when rejected (nothing changed).
 int oracle_solver_set_pins(void* h, uint32_t n, const uint32_t* idx, const double* target, const double* ghat,
                            const int* kinematic, const double* stiffness) {
