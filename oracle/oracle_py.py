@@ -230,6 +230,7 @@ def _step_sigs(lib):
         "oracle_solver_set_shells": (None, [vp, C.c_uint32, vp, vp, vp, vp]),
         "oracle_solver_scale_stitches": (None, [vp, vp]),
         "oracle_solver_collider_sides": (i32, [vp, vp]),
+        "oracle_solver_self_intersect": (i32, [vp, vp]),
         "oracle_solver_set_pins": (i32, [vp, u32, vp, vp, vp, vp, vp]),
         "oracle_solver_set_pulls": (i32, [vp, u32, vp, vp, vp]),
         "oracle_solver_set_strain_limit_faces": (i32, [vp, u32, vp, vp, vp, u32, u32]),
@@ -352,6 +353,11 @@ class OracleSolver:
         m = np.ascontiguousarray(mu, np.float64)
         l_ = np.ascontiguousarray(lam, np.float64)
         self.lib.oracle_solver_set_shells(self.h, f.shape[0], _p(f), _p(r), _p(m), _p(l_))
+
+    def self_intersects(self, pos) -> bool:
+        """positions_self_intersect (implicit.rs:618-650) at pos."""
+        p = np.ascontiguousarray(pos, np.float32).reshape(self.nv, 3)
+        return bool(self.lib.oracle_solver_self_intersect(self.h, _p(p)))
 
     def collider_sides(self):
         """Per-vertex side of the static collider at the current positions (+1 outside, -1

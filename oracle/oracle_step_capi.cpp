@@ -332,6 +332,15 @@ int oracle_solver_set_kinematic(void* h, const double* pos) {
   return a->d->set_kinematic_collider_positions(x);
 }
 
+// positions_self_intersect (implicit.rs:618-650) at positions pos (f32[3 nv]).
+int oracle_solver_self_intersect(void* h, const float* pos) {
+  auto* a = (AnySolver*)h;
+  if (a->prec != 0) return -1;
+  std::vector<Vt<float>> x(a->f->positions.size());
+  for (size_t i = 0; i < x.size(); ++i) x[i] = Vt<float>(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+  return a->f->positions_self_intersect(x) ? 1 : 0;
+}
+
 // collider_sides (implicit.rs:1431-1475) at the current positions: +1 outside, -1 inside,
 // per vertex (f32[nv]); returns 0 when there is no static collider (nothing written).
 int oracle_solver_collider_sides(void* h, float* out) {
