@@ -266,6 +266,13 @@ typedef struct {
 } mguso_step_stats;
 
 typedef struct mguso_scene mguso_scene;
+/* Checks a description without building anything (host only: needs no device or context):
+ * index ranges, the stitch rules of ImplicitSolver::set_stitches (implicit.rs:939-966: every
+ * index in range, stiffness finite and >= 0, l0 finite and > 0, l_cap finite and >= l0, each
+ * side's weights summing to 1 within 1e-3) and the parameters. MGUSO_OK, or
+ * MGUSO_ERR_INVALID_ARG with the reason in mguso_last_error, as mguso_scene_create would
+ * return for it; the reference's setters return the same rules as Result<(), String>. */
+int mguso_scene_validate(const mguso_scene_desc* desc);
 int mguso_scene_create(mguso_ctx* ctx, const mguso_scene_desc* desc, mguso_scene** out);
 int mguso_scene_destroy(mguso_scene* s);
 /* Advances nsteps implicit steps (ImplicitSolver::step, implicit.rs:1951-2191). stats has

@@ -86,9 +86,13 @@ struct Contribution {
 
 }  // namespace
 
-int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>& inst_vert) {
+// The checks a description must pass before anything is built: index ranges, the stitch
+// rules of ImplicitSolver::set_stitches (implicit.rs:939-966) and the parameters. Host only.
+static int validate_desc(const mguso_scene_desc* d) {
   MG_CHECK_ARG(d && d->positions && d->inv_mass && (d->nt == 0 || d->tris), "scene: null arrays");
   MG_CHECK_ARG(d->nv > 0 && d->nv < (1u << 30), "scene: vertex count out of range");
+  MG_CHECK_ARG(d->nshell == 0 || d->shell_faces, "scene: null arrays");
+  MG_CHECK_ARG(d->nstitch == 0 || (d->stitch_idx && d->stitch_w && d->stitch_kl), "scene: null arrays");
   const uint32_t nv = d->nv, nt = d->nt;
   for (uint32_t t = 0; t < 3 * nt; ++t) MG_CHECK_ARG(d->tris[t] < nv, "scene: triangle index out of range");
   for (uint32_t t = 0; t < 3 * d->nshell; ++t) MG_CHECK_ARG(d->shell_faces[t] < nv, "scene: shell face index out of range");
@@ -105,11 +109,17 @@ int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>
   MG_CHECK_ARG(d->params.dt > 0, "scene: dt must be > 0");
   MG_CHECK_ARG(d->params.precond == MGUSO_PRECOND_BLOCK_JACOBI || d->params.precond == MGUSO_PRECOND_SCHWARZ,
                "scene: unknown preconditioner");
+  MG_CHECK_ARG(d->params.pcg_mode >= 0 && d->params.pcg_mode <= 2, "scene: pcg_mode must be 0, 1 or 2");
+  return MGUSO_OK;
+}
+
+int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>& inst_vert) {
+  MG_TRY(validate_desc(d));
+  const uint32_t nv = d->nv, nt = d->nt;
   s.p = d->params;
   s.nv = nv;
   s.nt = nt;
   s.mixed = d->params.precision == MGUSO_PRECISION_MIXED;
-  MG_CHECK_ARG(d->params.pcg_mode >= 0 && d->params.pcg_mode <= 2, "scene: pcg_mode must be 0, 1 or 2");
   s.st = s.ctx->stream;
   cudaStream_t st = s.st;
   const float* P = d->positions;
@@ -563,6 +573,8 @@ int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>
 using namespace mg;
 
 extern "C" {
+
+int mguso_scene_validate(const mguso_scene_desc* desc) { return validate_desc(desc); }
 
 int mguso_scene_create(mguso_ctx* ctx, const mguso_scene_desc* desc, mguso_scene** out) {
   MG_CHECK_ARG(ctx && desc && out, "null argument");

@@ -66,6 +66,7 @@ def _sigs(lib):
         ("mguso_scene_instances", i32, [vp, P(C.c_uint32), vp]),
         ("mguso_scene_system", i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
         ("mguso_scene_stencils", i32, [vp, C.c_uint32, vp, vp, vp, vp]),
+        ("mguso_scene_validate", i32, [vp]),
     ]:
         fn = getattr(lib, name)
         fn.restype = res
@@ -81,6 +82,10 @@ def _desc(scene: dict, precision: str):
     keep["inv_mass"] = keep["inv_mass"].astype(np.float32, copy=False)
     keep["tris"] = keep["tris"].astype(np.uint32, copy=False)
     keep["shell_faces"] = keep["shell_faces"].astype(np.uint32, copy=False)
+    keep["stitch_idx"] = keep["stitch_idx"].astype(np.uint32, copy=False)
+    keep["stitch_w"] = keep["stitch_w"].astype(np.float32, copy=False)
+    keep["stitch_kl"] = keep["stitch_kl"].astype(np.float32, copy=False)
+    keep["colliders"] = keep["colliders"].astype(np.float32, copy=False)
     mask = scene.get("static_mask")
     keep["mask"] = None if mask is None else np.ascontiguousarray(mask, np.uint8)
     d = SceneDesc()
@@ -105,6 +110,18 @@ def _desc(scene: dict, precision: str):
             keep[name] = np.ascontiguousarray(scene[name], np.float32)
             setattr(d, name, ptr(keep[name]))
     return d, keep
+
+
+def validate_scene(scene: dict, precision: str = "mixed") -> None:
+    """Checks a scene description on the host, with no device (mguso_scene_validate): the
+    index ranges, the stitch rules of ImplicitSolver::set_stitches (implicit.rs:939-966) and
+    the parameters. Raises MgusoError (MGUSO_ERR_INVALID_ARG) with the reason, as building
+    the scene would."""
+    lib = _lib.load()
+    _sigs(lib)
+    d, keep = _desc(scene, precision)
+    check(lib.mguso_scene_validate(C.byref(d)))
+    del keep
 
 
 def make_params(p: dict, precision: str = "mixed") -> Params:

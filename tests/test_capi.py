@@ -28,3 +28,44 @@ def test_invalid_arguments_are_rejected_without_gpu():
     lib = _lib.load()
     assert lib.mguso_linear_solver_create(None, 1, 32, 1, None) == 1  # INVALID_ARG
     assert "null" in _lib.last_error()
+
+
+def _triangle_scene(**stitch):
+    import numpy as np
+
+    from mguso import scenes
+
+    pos = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32)
+    st = dict(index=[0, 0, 0, 1, 1, 1], weight=[1.0, 0.0, 0.0, 1.0, 0.0, 0.0], stiffness=1.0, l0=0.001, l_cap=0.01)
+    st.update(stitch)
+    return dict(positions=pos, velocities=np.zeros_like(pos), inv_mass=np.ones(3, np.float32),
+                tris=np.array([[0, 1, 2]], np.uint32), shell_faces=np.zeros((0, 3), np.uint32), static_mask=None,
+                stitch_idx=np.array([st["index"]], np.uint32), stitch_w=np.array([st["weight"]], np.float32),
+                stitch_kl=np.array([[st["stiffness"], st["l0"], st["l_cap"]]], np.float32),
+                colliders=np.zeros((0, 8), np.float32), params=scenes.default_params())
+
+
+def test_scene_validation_rejects_nonsense_stitches_without_gpu():  # implicit.rs:3494-3535
+    import math
+
+    import numpy as np
+    import pytest
+
+    from mguso import MgusoError
+    from mguso.solver import validate_scene
+
+    validate_scene(_triangle_scene())
+    bad = [dict(index=[0, 0, 0, 9, 9, 9]), dict(stiffness=-1.0), dict(l0=0.0), dict(l_cap=0.0005),
+           dict(weight=[0.5, 0, 0, 1.0, 0, 0]), dict(weight=[1.0, 0, 0, 0.5, 0, 0]), dict(l0=math.nan)]
+    for b in bad:
+        with pytest.raises(MgusoError) as e:
+            validate_scene(_triangle_scene(**b))
+        assert e.value.code == 1 and "stitch" in str(e.value), b
+    sc = _triangle_scene()
+    sc["tris"] = np.array([[0, 1, 7]], np.uint32)
+    with pytest.raises(MgusoError, match="triangle index"):
+        validate_scene(sc)
+    sc = _triangle_scene()
+    sc["params"] = dict(sc["params"], dt=0.0)
+    with pytest.raises(MgusoError, match="dt"):
+        validate_scene(sc)
