@@ -231,6 +231,8 @@ def _step_sigs(lib):
         "oracle_solver_scale_stitches": (None, [vp, vp]),
         "oracle_solver_collider_sides": (i32, [vp, vp]),
         "oracle_solver_self_intersect": (i32, [vp, vp]),
+        "oracle_solver_set_shell_stiffness": (i32, [vp, u32, vp]),
+        "oracle_solver_hinges": (u32, [vp, vp, vp, u32]),
         "oracle_solver_set_pins": (i32, [vp, u32, vp, vp, vp, vp, vp]),
         "oracle_solver_set_pulls": (i32, [vp, u32, vp, vp, vp]),
         "oracle_solver_set_strain_limit_faces": (i32, [vp, u32, vp, vp, vp, u32, u32]),
@@ -353,6 +355,19 @@ class OracleSolver:
         m = np.ascontiguousarray(mu, np.float64)
         l_ = np.ascontiguousarray(lam, np.float64)
         self.lib.oracle_solver_set_shells(self.h, f.shape[0], _p(f), _p(r), _p(m), _p(l_))
+
+    def set_shell_stiffness(self, mu_lam) -> bool:
+        """Per-face (mu, lambda) for the shells in order; False when the count differs."""
+        a = np.ascontiguousarray(mu_lam, np.float64).reshape(-1, 2)
+        return bool(self.lib.oracle_solver_set_shell_stiffness(self.h, a.shape[0], _p(a)))
+
+    def hinges(self):
+        """(vertices (n, 4) u32, rest angles (n,) f64) of build_hinges."""
+        n = self.lib.oracle_solver_hinges(self.h, None, None, 0)
+        idx = np.zeros((max(n, 1), 4), np.uint32)
+        rest = np.zeros(max(n, 1), np.float64)
+        self.lib.oracle_solver_hinges(self.h, _p(idx), _p(rest), n)
+        return idx[:n], rest[:n]
 
     def self_intersects(self, pos) -> bool:
         """positions_self_intersect (implicit.rs:618-650) at pos."""

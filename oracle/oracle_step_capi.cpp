@@ -332,6 +332,34 @@ int oracle_solver_set_kinematic(void* h, const double* pos) {
   return a->d->set_kinematic_collider_positions(x);
 }
 
+// set_shell_stiffness (per-face (mu, lambda) for the current shells, in their order):
+// 1 when accepted, 0 when n is not the shell count (nothing changed).
+int oracle_solver_set_shell_stiffness(void* h, uint32_t n, const double* mu_lam) {
+  auto* a = (AnySolver*)h;
+  auto apply = [&](auto& s) {
+    using R = typename std::decay_t<decltype(s.shell_k)>::value_type::value_type;
+    if (n != s.shells.size()) return 0;
+    s.shell_k.assign(n, {});
+    for (uint32_t i = 0; i < n; ++i) s.shell_k[i] = {(R)mu_lam[2 * i], (R)mu_lam[2 * i + 1]};
+    return 1;
+  };
+  return a->prec == 0 ? apply(*a->f) : apply(*a->d);
+}
+
+// The hinges (build_hinges, bending.rs:126-158): vertices u32[4 n] and rest angles f64[n],
+// up to cap; returns the count.
+uint32_t oracle_solver_hinges(void* h, uint32_t* idx, double* rest, uint32_t cap) {
+  auto* a = (AnySolver*)h;
+  auto copy = [&](auto& s) {
+    for (size_t i = 0; i < s.hinges.size() && i < cap; ++i) {
+      for (int k = 0; k < 4; ++k) idx[4 * i + k] = s.hinges[i].v[k];
+      rest[i] = (double)s.hinges[i].rest;
+    }
+    return (uint32_t)s.hinges.size();
+  };
+  return a->prec == 0 ? copy(*a->f) : copy(*a->d);
+}
+
 // positions_self_intersect (implicit.rs:618-650) at positions pos (f32[3 nv]).
 int oracle_solver_self_intersect(void* h, const float* pos) {
   auto* a = (AnySolver*)h;

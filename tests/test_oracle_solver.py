@@ -198,3 +198,58 @@ def test_max_dx_rescales_the_search_direction_without_changing_it():  # implicit
     moving = fl > 1e-6
     scales = np.linalg.norm(capped, axis=1)[moving] / fl[moving]
     assert scales.size and scales.max() - scales.min() < 1e-3 * max(scales.max(), 1e-6)
+
+
+def _shell_sheet(y, pinned_row, **kw):
+    pos, tris = grid(5, y)
+    sc = scene(pos, tris, 0.1, dt=1.0 / 240.0, **kw)
+    sc["shell_faces"] = tris.copy()
+    if pinned_row:
+        sc["inv_mass"][:5] = 0.0
+    return sc
+
+
+def test_shell_faces_with_zero_stiffness_are_bit_identical():  # implicit.rs:5719-5749
+    a, _ = run(_shell_sheet(0.3, False, stiffness=500.0), 40)
+    sc = _shell_sheet(0.3, False, stiffness=500.0)
+    sc["shell_faces"] = np.zeros((0, 3), np.uint32)
+    b, _ = run(sc, 40)
+    assert a.counts()["shells"] > 0 and b.counts()["shells"] == 0
+    assert np.array_equal(a.positions(), b.positions())
+
+
+def test_shell_only_sheet_is_elastic():  # implicit.rs:5755-5776 (StVK, the model this path runs)
+    def sag(mu):
+        o, _ = run(_shell_sheet(0.0, True, stiffness=0.0, shell_mu=mu, shell_lambda=0.5 * mu), 200)
+        p = o.positions()
+        assert np.all(np.isfinite(p))
+        return float(p[-1, 1])
+
+    soft, stiff = sag(50.0), sag(5000.0)
+    assert soft < -0.001 and stiff > soft, (soft, stiff)
+
+
+def test_per_face_shell_stiffness_works_without_the_scalars():  # implicit.rs:5783-5820
+    mu, lam = 800.0, 400.0
+    a, _ = run(_shell_sheet(0.0, True, stiffness=0.0, shell_mu=mu, shell_lambda=lam), 120)
+    o = O.OracleSolver(_shell_sheet(0.0, True, stiffness=0.0))
+    assert not o.set_shell_stiffness([[mu, lam]] * 3)
+    assert o.set_shell_stiffness([[mu, lam]] * o.counts()["shells"])
+    o.step(120, check_intersection=False)
+    assert np.all(np.isfinite(o.positions()))
+    assert o.positions()[-1, 1] == a.positions()[-1, 1]
+
+
+def test_build_hinges_finds_shared_edge():  # bending.rs:292-306
+    pos = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [1, 1, 0]], f32)
+    idx, rest = O.OracleSolver(scene(pos, [[0, 1, 2], [2, 1, 3]], 1.0)).hinges()
+    assert len(idx) == 1 and abs(rest[0]) < 1e-3
+    assert sorted(idx[0][1:3].tolist()) == [1, 2]  # the shared edge is the hinge's axis
+
+
+def test_the_stitch_energy_is_translation_invariant():  # stitch.rs:239-255 (the cog terms cancel)
+    x = np.array([[0, 0, 0], [0.01, 0, 0], [0, 0.01, 0], [0.03, 0.002, 0], [0.04, 0.002, 0], [0.03, 0.012, 0]])
+    w = np.array([0.2, 0.3, 0.5, 0.25, 0.25, 0.5])
+    g0, h0 = O.stitch(x, w, 0.001, 0.01)
+    g1, h1 = O.stitch(x + [1.5, -2.0, 0.25], w, 0.001, 0.01)
+    assert np.allclose(g0, g1, rtol=1e-9, atol=1e-12) and np.allclose(h0, h1, rtol=1e-9, atol=1e-9)
