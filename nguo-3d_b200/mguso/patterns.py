@@ -139,6 +139,20 @@ def mesh_panel(outline_mm: Sequence[Sequence[float]], target_edge_mm: float, see
     return PanelMesh(pts_out, tri.astype(np.uint32), chains)
 
 
+def panel_from_triangulation(mesh, edges: Sequence[int]) -> PanelMesh:
+    """A piece meshed by ``triangulate.triangulate`` as a PanelMesh: the chains of the pattern
+    edges ``edges`` (ids, in the order the panel's seams will name them: panel edge k is
+    pattern edge edges[k]) become the panel's chains, each from its edge's start to its end."""
+    chains = []
+    for e in edges:
+        c = mesh.chain(e)
+        if c is None:
+            raise PatternError(f"pattern edge {e} has no chain in the mesh (a grain marker, or outside the fabric)")
+        vs = [v for v, _ in c.points]
+        chains.append(sewing.EdgeChain(vs, mesh.pattern_mm[vs]))
+    return PanelMesh(np.asarray(mesh.pattern_mm, np.float64), mesh.indices.astype(np.uint32), chains)
+
+
 @dataclass
 class _Placed:
     mesh: PanelMesh

@@ -94,3 +94,39 @@ def test_a_sewn_tube_closes_its_seams_in_the_step():
     x = o.positions().astype(np.float64)
     assert np.all(np.isfinite(x))
     assert gap(x) < 0.2 * gap(sc["positions"].astype(np.float64))
+
+
+def _curved_panel(size, bulge, target):
+    """A square piece whose right side bulges out as a cubic, meshed by mguso.triangulate."""
+    from mguso import triangulate as T
+
+    n = T.Network()
+    v = [n.add_vertex(x, y) for x, y in [(0, 0), (size, 0), (size, size), (0, size)]]
+    e = [n.add_edge(v[0], v[1], T.CUT),
+         n.add_edge(v[1], v[2], T.SEAM, c1=(size + bulge, size / 3), c2=(size + bulge, 2 * size / 3)),
+         n.add_edge(v[2], v[3], T.CUT),
+         n.add_edge(v[3], v[0], T.SEAM)]
+    m = T.triangulate(n, (), T.Options().with_target_edge_mm(target))
+    return patterns.panel_from_triangulation(m, e)
+
+
+def test_triangulated_panels_with_a_curved_seam_sew_and_close():
+    g = patterns.Garment()
+    front, back = _curved_panel(300.0, 40.0, 40.0), _curved_panel(300.0, 40.0, 55.0)
+    f = g.add_panel(front, origin_m=(0.0, 0.0, 0.02))
+    b = g.add_panel(back, origin_m=(0.3, 0.0, -0.02), x_axis=(-1.0, 0.0, 0.0))
+    g.sew(f, [(1, False)], b, [(1, False)])  # the two bulging sides face each other
+    idx, w, info = g.stitches()
+    assert idx.shape[0] == len(front.chains[1].vertices)  # the denser side sews every vertex
+    assert abs(info[0][0] - 1.0) < 1e-3  # equal arc lengths: no ease
+    sc = g.scene(gravity=(0.0, 0.0, 0.0), self_collision=0, bend_stiffness=0.0)
+
+    def gap(x):
+        t = x[idx[:, 3]] * (1 - w[:, 4:5]) + x[idx[:, 4]] * w[:, 4:5]
+        return np.linalg.norm(x[idx[:, 0]] - t, axis=1).max()
+
+    o = O.OracleSolver(sc)
+    o.step(40, check_intersection=False)
+    x = o.positions().astype(np.float64)
+    assert np.all(np.isfinite(x))
+    assert gap(x) < 0.2 * gap(sc["positions"].astype(np.float64))
