@@ -402,6 +402,11 @@ def _samples(net: Network, e: int, notches: Sequence[float], opts: Options) -> L
     return out
 
 
+def _round_half_away(v: float) -> int:
+    """Nearest integer, ties away from zero (the snap-rounding key, lib.rs:541-543)."""
+    return int(math.copysign(math.floor(abs(v) + 0.5), v))
+
+
 def _segments_cross(p, q, r, s) -> np.ndarray:
     """Proper crossings of segments p_i q_i and r_j s_j (broadcast): strictly opposite sides
     both ways (touching at an endpoint or collinear overlap is not a crossing)."""
@@ -595,7 +600,7 @@ def triangulate(net: Network, notches: Sequence[Tuple[int, float]] = (), opts: O
     for eid, e in live:
         points = []
         for t, p in _samples(net, eid, by_edge.get(eid, ()), opts):
-            k = (int(round(p[0] / w)), int(round(p[1] / w)))
+            k = (_round_half_away(p[0] / w), _round_half_away(p[1] / w))
             src = ("vertex", e.start) if t == 0.0 else (("vertex", e.end) if t == 1.0 else ("edge", eid))
             if k not in index:
                 index[k] = len(pts)
