@@ -16,12 +16,12 @@ The pipeline:
    every link is then split evenly in t so none is longer than ``target_edge_mm``. Each
    sample keeps its exact t.
 2. Snap-round every sample to a ``weld_mm`` grid and deduplicate (lib.rs:630-668).
-3. Triangulate: the Delaunay triangulation of the samples, with every pattern link
-   recovered as a mesh edge. A link that the Delaunay triangulation does not contain is split
-   at its parameter midpoint, on the curve, until it does (the reference inserts constraints
-   into a constrained Delaunay triangulation instead and never splits them; here a split
-   point is still exactly on its edge with an exact t, so the chains stay facts). Pattern
-   links that cross away from a shared vertex are refused (``CrossingConstraint``).
+3. Triangulate: the constrained Delaunay triangulation of the samples with every pattern
+   link as an edge (the Delaunay triangulation, each missing link inserted by edge flips,
+   Lawson flips around it). A link that runs exactly through another sample is split there,
+   at its parameter midpoint on the curve, so a split point is still exactly on its edge
+   with an exact t and the chains stay facts. Pattern links that cross away from a shared
+   vertex are refused (``CrossingConstraint``).
 4. Refine (``refine=True``): a hexagonal lattice at ``target_edge_mm`` spacing seeds the
    fabric away from the pattern links, then triangles over the area bound (the equilateral
    triangle of side ``target_edge_mm``, lib.rs:681) or under ``min_angle_deg`` get their
@@ -476,21 +476,23 @@ class _Mesher:
         return _delaunay(P), P
 
     def recover(self, net, net_edges: List[int], rounds: int = 30):
-        """Split every pattern link missing from the Delaunay triangulation at its parameter
-        midpoint (on the curve) until all are mesh edges."""
+        """The constrained Delaunay triangulation of the points with every pattern link as an
+        edge: the Delaunay triangulation, then each missing link inserted by edge flips
+        (Sloan's algorithm) and the Delaunay property restored around it by Lawson flips. A
+        link that runs exactly through another point is split there instead, at its
+        parameter midpoint on the curve, and the triangulation is rebuilt."""
         for _ in range(rounds):
             tri, P = self.triangulate()
             if tri is None:
                 return None
-            have = _edge_keys(tri.simplices, len(P))
+            cdt = _Cdt(P, tri.simplices, tri.neighbors)
             ab, _, _ = self.link_array()
-            lk = np.minimum(ab[:, 0], ab[:, 1]) * len(P) + np.maximum(ab[:, 0], ab[:, 1])
-            pos = np.minimum(np.searchsorted(have, lk), len(have) - 1)
-            gone = have[pos] != lk
-            if not gone.any():
-                return tri
             links = [(ci, k) for ci, k, *_ in self.links()]
-            for i in sorted(np.flatnonzero(gone).tolist(), reverse=True):
+            constraints = {(min(a, b), max(a, b)) for a, b in ab.tolist()}
+            failed = [i for i, (a, b) in enumerate(ab.tolist()) if not cdt.insert(a, b, constraints)]
+            if not failed:
+                return cdt
+            for i in sorted(failed, reverse=True):
                 ci, k = links[i]
                 e, _, _, pts = self.chains[ci]
                 (_, t0), (_, t1) = pts[k], pts[k + 1]
@@ -498,6 +500,234 @@ class _Mesher:
                 self.pts.append(net.eval(net_edges[ci], tm))
                 pts.insert(k + 1, (len(self.pts) - 1, tm))
         raise Invalid("pattern edges could not be recovered as mesh edges")
+
+
+def _orient(a, b, c) -> float:
+    return (b[0] - a[0]) * (c[1] - a[1]) - (b[1] - a[1]) * (c[0] - a[0])
+
+
+def _incircle(a, b, c, d) -> float:
+    """> 0 when d lies inside the circumcircle of the counter-clockwise triangle abc."""
+    adx, ady, bdx, bdy, cdx, cdy = a[0] - d[0], a[1] - d[1], b[0] - d[0], b[1] - d[1], c[0] - d[0], c[1] - d[1]
+    return ((adx * adx + ady * ady) * (bdx * cdy - cdx * bdy) - (bdx * bdx + bdy * bdy) * (adx * cdy - cdx * ady)
+            + (cdx * cdx + cdy * cdy) * (adx * bdy - bdx * ady))
+
+
+class _Cdt:
+    """A mutable triangulation (counter-clockwise triangles, neighbour opposite each vertex)
+    that takes constraint edges by flips."""
+
+    def __init__(self, P: np.ndarray, simplices: np.ndarray, neighbors: np.ndarray):
+        self.P = P
+        self.T = [list(map(int, t)) for t in simplices]
+        self.N = [list(map(int, n)) for n in neighbors]
+        for f, t in enumerate(self.T):
+            if _orient(P[t[0]], P[t[1]], P[t[2]]) < 0:
+                t[1], t[2] = t[2], t[1]
+                self.N[f][1], self.N[f][2] = self.N[f][2], self.N[f][1]
+        self._S = self._Nb = None
+        self.V: Dict[int, set] = {}
+        for f, t in enumerate(self.T):
+            for v in t:
+                self.V.setdefault(v, set()).add(f)
+
+    # -- queries (arrays cached until the next flip)
+    @property
+    def simplices(self) -> np.ndarray:
+        if self._S is None:
+            self._S = np.asarray(self.T, np.int64).reshape(-1, 3)
+        return self._S
+
+    @property
+    def neighbors(self) -> np.ndarray:
+        if self._Nb is None:
+            self._Nb = np.asarray(self.N, np.int64).reshape(-1, 3)
+        return self._Nb
+
+    @property
+    def vertex_neighbor_vertices(self):
+        t = self.simplices
+        e = np.concatenate([t[:, [0, 1]], t[:, [1, 2]], t[:, [2, 0]], t[:, [1, 0]], t[:, [2, 1]], t[:, [0, 2]]])
+        e = np.unique(e, axis=0)
+        ind = np.searchsorted(e[:, 0], np.arange(len(self.P) + 1))
+        return ind, e[:, 1]
+
+    def find_simplex(self, q: np.ndarray) -> np.ndarray:
+        """The face containing each query point (-1 when none of the nearest faces does)."""
+        from scipy.spatial import cKDTree
+
+        t = self.simplices
+        tp = self.P[t]
+        out = np.full(len(q), -1, np.int64)
+        if not len(t) or not len(q):
+            return out
+        k = min(12, len(t))
+        _, cand = cKDTree(tp.mean(1)).query(q, k=k)
+        cand = cand.reshape(len(q), k)
+        for j in range(k):
+            f = cand[:, j]
+            a, b, c = tp[f, 0], tp[f, 1], tp[f, 2]
+            inside = ((_orient_v(a, b, q) >= 0) & (_orient_v(b, c, q) >= 0) & (_orient_v(c, a, q) >= 0))
+            take = inside & (out < 0)
+            out[take] = f[take]
+        return out
+
+    def _face_with_edge(self, a: int, b: int) -> Optional[Tuple[int, int]]:
+        """(face, index of its vertex opposite the directed edge a->b) or None."""
+        for f in self.V.get(a, ()):
+            t = self.T[f]
+            i = t.index(a)
+            if t[(i + 1) % 3] == b:
+                return f, (i + 2) % 3
+        return None
+
+    def has_edge(self, a: int, b: int) -> bool:
+        return self._face_with_edge(a, b) is not None or self._face_with_edge(b, a) is not None
+
+    # -- flips
+    def _flip(self, f: int, i: int) -> Tuple[int, int]:
+        """Flip the edge of face f opposite its vertex i; returns the new diagonal (p, s)."""
+        T, N = self.T, self.N
+        self._S = self._Nb = None
+        p, q, r = T[f][i], T[f][(i + 1) % 3], T[f][(i + 2) % 3]
+        g = N[f][i]
+        j = [k for k in range(3) if T[g][k] not in (q, r)][0]
+        s = T[g][j]
+        # neighbours: A across r-p (opposite q in f), B across p-q (opposite r in f),
+        # C across q-s (opposite r in g), D across s-r (opposite q in g)
+        A, B = N[f][(i + 1) % 3], N[f][(i + 2) % 3]
+        gq, gr = T[g].index(q), T[g].index(r)
+        C, D = N[g][gr], N[g][gq]
+        for v in (r,):
+            self.V[v].discard(f)
+        for v in (q,):
+            self.V[v].discard(g)
+        T[f], N[f] = [p, q, s], [C, g, B]
+        T[g], N[g] = [p, s, r], [D, A, f]
+        self.V[s].add(f)
+        self.V[p].add(g)
+        if A >= 0:
+            N[A][N[A].index(f)] = g
+        if C >= 0:
+            N[C][N[C].index(g)] = f
+        return p, s
+
+    def _legalise(self, edges, constraints) -> None:
+        """Lawson flips of the given edges (and those they expose) that are not constraints."""
+        stack = list(edges)
+        guard = 0
+        while stack and guard < 200000:
+            guard += 1
+            a, b = stack.pop()
+            if (min(a, b), max(a, b)) in constraints:
+                continue
+            fe = self._face_with_edge(a, b)
+            if fe is None:
+                continue
+            f, i = fe
+            g = self.N[f][i]
+            if g < 0:
+                continue
+            t = self.T[f]
+            s = [v for v in self.T[g] if v not in (a, b)][0]
+            P = self.P
+            if _incircle(P[t[0]], P[t[1]], P[t[2]], P[s]) > 0:
+                p = t[i]
+                # the quad is convex when s is inside the circumcircle of a Delaunay-adjacent pair
+                if _orient(P[p], P[a], P[s]) * _orient(P[p], P[b], P[s]) < 0:
+                    self._flip(f, i)
+                    stack += [(p, a), (a, s), (s, b), (b, p)]
+
+    def insert(self, a: int, b: int, constraints: set) -> bool:
+        """Make a-b an edge; False when the segment runs through another vertex."""
+        if self.has_edge(a, b):
+            return True
+        P = self.P
+        pa, pb = P[a], P[b]
+        crossing = self._crossed_edges(a, b)
+        if crossing is None:
+            return False
+        queue = deque(crossing)
+        new_edges = []
+        guard = 0
+        while queue:
+            guard += 1
+            if guard > 100000:
+                return False
+            u, v = queue.popleft()
+            fe = self._face_with_edge(u, v) or self._face_with_edge(v, u)
+            if fe is None:
+                return False
+            f, i = fe
+            g = self.N[f][i]
+            if g < 0:
+                return False
+            p = self.T[f][i]
+            s = [w for w in self.T[g] if w not in (u, v)][0]
+            # convex quad p, u, s, v: the diagonals cross properly
+            if not _segments_cross(P[p], P[s], P[u], P[v]):
+                queue.append((u, v))
+                if len(queue) > 1 and guard > 50 * (len(crossing) + 1) ** 2:
+                    return False
+                continue
+            x, y = self._flip(f, i)
+            if {x, y} == {a, b}:
+                continue
+            if _segments_cross(P[x], P[y], pa, pb):
+                queue.append((x, y))
+            else:
+                new_edges.append((x, y))
+        self._legalise(new_edges, constraints | {(min(a, b), max(a, b))})
+        return self.has_edge(a, b)
+
+    def _crossed_edges(self, a: int, b: int):
+        """Edges crossed by the open segment a-b, walking from a; None when the segment meets
+        another vertex."""
+        P = self.P
+        pa, pb = P[a], P[b]
+        start = None
+        for f in self.V.get(a, ()):
+            t = self.T[f]
+            i = t.index(a)
+            u, v = t[(i + 1) % 3], t[(i + 2) % 3]
+            ou, ov = _orient(pa, pb, P[u]), _orient(pa, pb, P[v])
+            if (ou == 0 and _between(pa, pb, P[u])) or (ov == 0 and _between(pa, pb, P[v])):
+                return None
+            if ou < 0 < ov:  # b lies strictly inside the wedge u-a-v, beyond edge u-v
+                start = (f, u, v)
+                break
+        if start is None:
+            return None
+        out = []
+        f, u, v = start
+        for _ in range(len(self.T) + 1):
+            out.append((u, v))
+            fe = self._face_with_edge(v, u)
+            if fe is None:
+                return None
+            g, k = fe
+            w = self.T[g][k]
+            if w == b:
+                return out
+            ow = _orient(pa, pb, P[w])
+            if ow == 0:
+                return None
+            if ow < 0:
+                u = w
+            else:
+                v = w
+        return None
+
+
+def _orient_v(a, b, c):
+    return (b[:, 0] - a[:, 0]) * (c[:, 1] - a[:, 1]) - (b[:, 1] - a[:, 1]) * (c[:, 0] - a[:, 0])
+
+
+def _between(a, b, c) -> bool:
+    """c (collinear with a-b) lies strictly between a and b."""
+    d = b - a
+    t = float(np.dot(c - a, d)) / max(float(np.dot(d, d)), 1e-300)
+    return 0.0 < t < 1.0
 
 
 def _edge_keys(simplices: np.ndarray, n: int) -> np.ndarray:

@@ -327,3 +327,128 @@ def test_notches_add_vertices_without_changing_the_area(seed):  # tests/mesh.rs:
     assert abs(notched.area_mm2() - plain.area_mm2()) < area_tolerance(poly)
     for k, t in enumerate(ts):
         assert any(tt == float(t) for _, tt in notched.chain(e[k]).points)
+
+
+def bodice():
+    """The reference's half bodice front (tests/mesh.rs:33-111): straight waist in three pieces
+    around a dart, cubic side seam, armhole and neckline, a centre-front fold, a grain marker
+    and four notches."""
+    n = T.Network()
+    cf_waist, dart_l, dart_r, side_waist = (n.add_vertex(x, 0.0) for x in (0.0, 45.0, 65.0, 110.0))
+    underarm, shoulder_out = n.add_vertex(118.0, 180.0), n.add_vertex(78.0, 330.0)
+    shoulder_in, cf_neck = n.add_vertex(28.0, 356.0), n.add_vertex(0.0, 300.0)
+    waist_a = n.add_edge(cf_waist, dart_l, T.SEAM)
+    n.add_edge(dart_l, dart_r, T.SEAM)
+    waist_c = n.add_edge(dart_r, side_waist, T.SEAM)
+    side = n.add_edge(side_waist, underarm, T.SEAM, c1=(106.0, 60.0), c2=(108.0, 120.0))
+    armhole = n.add_edge(underarm, shoulder_out, T.SEAM, c1=(128.0, 250.0), c2=(108.0, 320.0))
+    n.add_edge(shoulder_out, shoulder_in, T.SEAM)
+    n.add_edge(shoulder_in, cf_neck, T.SEAM, c1=(14.0, 348.0), c2=(0.0, 330.0))
+    n.add_edge(cf_neck, cf_waist, T.FOLD)
+    apex = n.add_vertex(55.0, 150.0)
+    n.add_edge(dart_l, apex, T.DART_LEG)
+    n.add_edge(apex, dart_r, T.DART_LEG)
+    g0, g1 = n.add_vertex(60.0, 40.0), n.add_vertex(60.0, 260.0)
+    n.add_edge(g0, g1, T.GRAIN)
+    return n, [(armhole, 0.5), (side, 0.5), (waist_a, 0.5), (waist_c, 0.25)]
+
+
+def test_the_bodice_triangulates_and_maps_back_to_the_pattern():  # tests/mesh.rs:213-280
+    import copy
+
+    net, notches = bodice()
+    m = T.triangulate(net, notches)
+    assert m.check() is None
+    for e, t in notches:
+        i = next(i for i, ct in m.chain(e).points if abs(ct - t) < 1e-12)
+        assert np.linalg.norm(m.pattern_mm[i] - net.eval(e, t)) < 1e-3
+    no_dart = copy.deepcopy(net)
+    for ed in no_dart.edges:
+        if ed is not None and ed.semantic == T.DART_LEG:
+            ed.semantic = T.INTERNAL
+    whole = T.triangulate(no_dart, notches)
+    assert abs((whole.area_mm2() - m.area_mm2()) - 1_500.0) < 1e-3  # the 20 x 150 / 2 wedge
+    assert all(c.semantic != T.GRAIN for c in m.chains)
+    assert len(m.outline_vertices()) > 80
+    assert m.angle_quantile_deg(0.01) > 20.0
+    assert (m.min_angles_deg() < 15.0).sum() < 0.02 * m.triangle_count()
+
+
+def golden_panel():
+    """tests/mesh.rs:144-201: a 200 x 300 panel with a waist dart, a pocket line T-junction to
+    T-junction, a triangular cut-out and three notches."""
+    n = T.Network()
+    o = [n.add_vertex(x, y) for x, y in [(0, 0), (70, 0), (110, 0), (200, 0), (200, 300), (0, 300)]]
+    e = [n.add_edge(o[i], o[(i + 1) % 6], T.SEAM) for i in range(6)]
+    apex = n.add_vertex(90.0, 160.0)
+    n.add_edge(o[1], apex, T.DART_LEG)
+    n.add_edge(apex, o[2], T.DART_LEG)
+    n.add_edge(n.add_vertex(40.0, 220.0), n.add_vertex(160.0, 220.0), T.INTERNAL)
+    h = [n.add_vertex(x, y) for x, y in [(150, 60), (180, 60), (180, 100)]]
+    for i in range(3):
+        n.add_edge(h[i], h[(i + 1) % 3], T.CUT)
+    return n, [(e[0], 0.5), (e[3], 0.25), (e[3], 0.75)]
+
+
+def test_the_panel_mesh_has_the_golden_panels_shape():  # tests/mesh.rs:286-307
+    net, notches = golden_panel()
+    m = T.triangulate(net, notches, T.Options().with_target_edge_mm(40.0))
+    assert m.check() is None
+    assert 80 < m.triangle_count() < 400
+    assert abs(m.area_mm2() - (60_000.0 - 3_200.0 - 600.0)) < 1e-6
+
+
+def ref_star(seed):
+    """tests/mesh.rs:350-368: 3..39 vertices at jittered even angles, radii 5..400 mm."""
+    rng = np.random.default_rng(seed)
+    k = int(rng.integers(3, 40))
+    step = 2 * np.pi / k
+    ang = (np.arange(k) + rng.uniform(-0.2, 0.2, k)) * step
+    r = rng.uniform(5.0, 400.0, k)
+    return np.stack([r * np.cos(ang), r * np.sin(ang)], 1)
+
+
+def _star_net(poly):
+    n = T.Network()
+    v = [n.add_vertex(*p) for p in poly]
+    for i in range(len(v)):
+        n.add_edge(v[i], v[(i + 1) % len(v)], T.CUT)
+    return n
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_duplicate_vertices_produce_an_identical_mesh(seed):  # tests/mesh.rs:438-466
+    poly = ref_star(100 + seed)
+
+    def build(duplicate):
+        net = _star_net(poly)
+        hub = net.add_vertex(0.0, 0.0)
+        for c in range(len(poly)):
+            start = net.add_vertex(*net.vertices[c]) if duplicate else c
+            net.add_edge(start, hub, T.INTERNAL)
+        return net
+
+    opts = T.Options().with_target_edge_mm(25.0)
+    want, got = T.triangulate(build(False), (), opts), T.triangulate(build(True), (), opts)
+    assert got.check() is None
+    assert np.array_equal(got.pattern_mm, want.pattern_mm) and np.array_equal(got.indices, want.indices)
+    assert got.chains == want.chains
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_nothing_degenerate_ever_panics_or_lies(seed):  # tests/mesh.rs:476-499
+    rng = np.random.default_rng(200 + seed)
+    poly = ref_star(200 + seed)
+    jitter, t = float(rng.uniform(0.0, 1e-3)), float(rng.uniform(0.0, 1.0))
+    net = _star_net(poly)
+    hub = net.add_vertex(0.0, 0.0)
+    for p in poly:
+        ghost = net.add_vertex(p[0] + jitter, p[1] - jitter)
+        net.add_edge(ghost, hub, T.DART_LEG)
+    notches = [(e, tt) for e in range(len(net.edges)) for tt in (t, 1.0 - t)]
+    try:
+        m = T.triangulate(net, notches, T.Options().with_target_edge_mm(15.0))
+    except T.TriangulateError as err:
+        assert str(err)
+    else:
+        assert m.check() is None
