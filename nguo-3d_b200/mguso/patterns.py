@@ -159,6 +159,7 @@ class _Placed:
     origin_m: np.ndarray
     axes: np.ndarray  # 3x2: pattern x and y axes in world space
     base: int
+    placement: object = None  # an arrange.Wrap / arrange.Rigid instead of origin and axes
 
 
 @dataclass
@@ -175,6 +176,13 @@ class Garment:
         self.panels.append(_Placed(mesh, np.asarray(origin_m, np.float64), axes, base))
         return len(self.panels) - 1
 
+    def add_arranged_panel(self, mesh: PanelMesh, placement) -> int:
+        """Place a panel by an ``arrange`` placement (a cylinder wrap or a rigid transform of
+        the pattern plane); its triangles are re-wound when the placement mirrors the plane."""
+        base = sum(p.mesh.points_mm.shape[0] for p in self.panels)
+        self.panels.append(_Placed(mesh, np.zeros(3), np.zeros((3, 2)), base, placement))
+        return len(self.panels) - 1
+
     def sew(self, panel_a: int, edges_a, panel_b: int, edges_b, flip=None):
         """Sew panel_a's edge chain (a list of (edge, reversed)) to panel_b's; ``flip`` None
         picks the direction that closes with less travel in the current placement."""
@@ -183,7 +191,10 @@ class Garment:
     def positions(self) -> np.ndarray:
         out = []
         for p in self.panels:
-            out.append(p.origin_m[None, :] + (p.mesh.points_mm * 1e-3) @ p.axes.T)
+            if p.placement is not None:
+                out.append(np.asarray(p.placement.apply(p.mesh.points_mm), np.float64))
+            else:
+                out.append(p.origin_m[None, :] + (p.mesh.points_mm * 1e-3) @ p.axes.T)
         return np.concatenate(out).astype(np.float32)
 
     def _side(self, pi, edges):
@@ -217,11 +228,12 @@ class Garment:
         from . import scenes
 
         pos = self.positions()
-        tris = np.concatenate([p.mesh.tris.astype(np.int64) + p.base for p in self.panels]).astype(np.uint32)
+        tris = np.concatenate([(p.mesh.tris[:, [0, 2, 1]] if p.placement is not None and p.placement.flips_winding()
+                                else p.mesh.tris).astype(np.int64) + p.base for p in self.panels]).astype(np.uint32)
         idx, w, _ = self.stitches()
         mu, lam = scenes.lame_from_young_poisson(young * thickness, poisson)
         m = scenes.uniform_mass(pos, tris, density)
-        # rest shapes from the pattern (the placement is rigid per panel, so they agree)
+        # rest shapes from the pattern (rigid placements and cylinder wraps are isometric, so they agree)
         rest = np.concatenate([p.mesh.points_mm * 1e-3 for p in self.panels])
         kl = np.tile(np.float32([[stitch_k, stitch_l0, stitch_cap]]), (idx.shape[0], 1))
         return {"positions": pos, "velocities": np.zeros_like(pos), "inv_mass": np.full(len(pos), 1.0 / m, np.float32),
