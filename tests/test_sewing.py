@@ -28,7 +28,7 @@ def rect(w, h, target):
     return pts, chains
 
 
-def test_a_full_side_is_sampled_end_to_end_in_normalised_arc_length():  # correspond.rs:401-418
+def test_a_full_side_is_sampled_end_to_end_in_normalised_arc_length():  # correspond.rs:416-431
     _, e = rect(100, 200, 20)
     s = sewing.side_samples([(e[1], False)])
     assert abs(s.len_mm - 200) < 1e-6 and len(s.vertices) >= 3
@@ -36,7 +36,7 @@ def test_a_full_side_is_sampled_end_to_end_in_normalised_arc_length():  # corres
     assert all(a[1] <= b[1] for a, b in zip(s.vertices, s.vertices[1:]))
 
 
-def test_a_two_edge_side_is_one_parameter_space_with_no_duplicate_join():  # correspond.rs:420-447
+def test_a_two_edge_side_is_one_parameter_space_with_no_duplicate_join():  # correspond.rs:435-458
     _, e = rect(100, 200, 25)
     s = sewing.side_samples([(e[0], False), (e[1], False)])
     assert abs(s.len_mm - 300) < 1e-6
@@ -45,7 +45,7 @@ def test_a_two_edge_side_is_one_parameter_space_with_no_duplicate_join():  # cor
     assert abs(dict(s.vertices)[corner] - 1 / 3) < 1e-6
 
 
-def test_reversing_an_edge_reverses_its_parameter():  # correspond.rs:449-461
+def test_reversing_an_edge_reverses_its_parameter():  # correspond.rs:460-472
     _, e = rect(100, 200, 20)
     fwd = sewing.side_samples([(e[1], False)])
     rev = sewing.side_samples([(e[1], True)])
@@ -54,7 +54,7 @@ def test_reversing_an_edge_reverses_its_parameter():  # correspond.rs:449-461
         assert vf == vr and abs(uf - (1 - ur)) < 1e-9
 
 
-def test_a_partial_span_keeps_only_its_own_vertices_and_renormalises():  # correspond.rs:463-479
+def test_a_partial_span_keeps_only_its_own_vertices_and_renormalises():  # correspond.rs:474-490
     _, e = rect(100, 200, 10)
     s = sewing.side_samples([(e[1], False)], span=(0.5, 1.0))
     assert abs(s.len_mm - 100) < 1e-6
@@ -63,20 +63,20 @@ def test_a_partial_span_keeps_only_its_own_vertices_and_renormalises():  # corre
     assert sewing.side_samples([(e[1], False)], span=(1.0, 0.5)).len_mm == s.len_mm
 
 
-def test_a_discontinuous_side_is_an_error_naming_the_edge():  # correspond.rs:481-491
+def test_a_discontinuous_side_is_an_error_naming_the_edge():  # correspond.rs:492-503
     _, e = rect(100, 200, 25)
     with pytest.raises(sewing.BrokenChain) as err:
         sewing.side_samples([(e[0], False), (e[1], True)])
     assert err.value.edge == 1
 
 
-def test_a_zero_length_span_is_an_error_not_a_division_by_zero():  # correspond.rs:493-502
+def test_a_zero_length_span_is_an_error_not_a_division_by_zero():  # correspond.rs:505-515
     _, e = rect(100, 200, 25)
     with pytest.raises(sewing.DegenerateSpan):
         sewing.side_samples([(e[1], False)], span=(0.4, 0.4))
 
 
-def test_unequal_resolutions_pair_by_parameter_not_by_vertex_count():  # correspond.rs:504-533
+def test_unequal_resolutions_pair_by_parameter_not_by_vertex_count():  # correspond.rs:520-547
     fine_p, fe = rect(100, 200, 8)
     coarse_p, ce = rect(100, 200, 40)
     a = sewing.side_samples([(fe[1], False)])
@@ -90,7 +90,7 @@ def test_unequal_resolutions_pair_by_parameter_not_by_vertex_count():  # corresp
         assert abs(sum(w[:3]) - 1) < 1e-6 and abs(sum(w[3:]) - 1) < 1e-6
 
 
-def test_unequal_lengths_become_ease_and_pair_proportionally():  # correspond.rs:535-570
+def test_unequal_lengths_become_ease_and_pair_proportionally():  # correspond.rs:551-586
     long_p, le = rect(100, 250, 10)
     short_p, se = rect(100, 200, 10)
     a = sewing.side_samples([(se[1], False)])
@@ -104,7 +104,7 @@ def test_unequal_lengths_become_ease_and_pair_proportionally():  # correspond.rs
     assert abs(target / 200 - long_p[v][1] / 250) < 1e-6
 
 
-def test_a_flipped_pairing_measures_shorter_when_the_seam_is_twisted():  # correspond.rs:572-617
+def test_a_flipped_pairing_measures_shorter_when_the_seam_is_twisted():  # correspond.rs:590-617
     p, e = rect(100, 200, 20)
     a = sewing.side_samples([(e[1], False)])
     b0 = sewing.side_samples([(e[1], False)])
