@@ -730,13 +730,6 @@ def _between(a, b, c) -> bool:
     return 0.0 < t < 1.0
 
 
-def _edge_keys(simplices: np.ndarray, n: int) -> np.ndarray:
-    """Sorted unique keys min * n + max of the triangulation's edges."""
-    t = simplices.astype(np.int64)
-    e = np.concatenate([t[:, [0, 1]], t[:, [1, 2]], t[:, [2, 0]]])
-    return np.unique(e.min(1) * n + e.max(1))
-
-
 def _classify(simplices: np.ndarray, neighbors: np.ndarray, edge_kind: Dict[Tuple[int, int], int],
               areas: np.ndarray) -> np.ndarray:
     """Fabric faces: odd outline-crossing depth from the hull (0-1 BFS), then the largest
