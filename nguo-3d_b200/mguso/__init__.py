@@ -9,4 +9,4 @@ from ._lib import MgusoError, load  # noqa: F401
 from .linsolve import Bsr, Context, CsrMatrix, CudaLinearSolver, LinearStats, Schwarz  # noqa: F401
 from .solver import ImplicitBatch, ImplicitSolver  # noqa: F401,E402
 from .adjoint import AdjointDrape  # noqa: F401,E402
-from . import arrange, bridge, capture, metrics, patterns, seams, sewing, triangulate  # noqa: F401,E402
+from . import arrange, bridge, capture, garment, metrics, patterns, seams, sewing, triangulate  # noqa: F401,E402

@@ -41,12 +41,17 @@ class Seam:
 
 @dataclass
 class Document:
+    """Pieces (networks by id) and seams by id. ``features`` per piece may hold ``notches``
+    ([(edge, t)], registration marks that become mesh vertices), ``placement`` (an authored
+    ((x, y, z) mm, quaternion)), ``support_edge`` (the edge the piece hangs by) and ``name``."""
     pieces: Dict[int, Network] = field(default_factory=dict)
     seams: Dict[int, Seam] = field(default_factory=dict)
+    features: Dict[int, dict] = field(default_factory=dict)
 
-    def add_piece(self, net: Network) -> int:
+    def add_piece(self, net: Network, **features) -> int:
         i = max(self.pieces, default=-1) + 1
         self.pieces[i] = net
+        self.features[i] = dict(features)
         return i
 
     def add_seam(self, seam: Seam) -> int:
@@ -58,8 +63,8 @@ class Document:
 @dataclass
 class Diagnostic:
     severity: str
-    kind: str        # unsewn, dangling_piece, dangling_edge, bad_direction, ease, ease_too_large,
-    #                  ease_not_as_declared, unmeasurable
+    kind: str        # unsewn, dangling_piece, dangling_edge, bad_direction, flipped, ease,
+    #                  ease_too_large, ease_not_as_declared, unmeasurable
     seam: Optional[int] = None
     piece: Optional[int] = None
     edge: Optional[int] = None
@@ -80,6 +85,9 @@ class Diagnostic:
         if self.kind == "bad_direction":
             return (f"the seam's side on piece {self.piece} runs in two directions at once: its edges do not "
                     f"join end to start — flip the mis-ordered edge")
+        if self.kind == "flipped":
+            return ("the seam's two sides run in opposite directions, so it was sewn reversed to close it — check "
+                    "which way round the pieces go if the drape looks twisted")
         if self.kind == "ease":
             return f"the two sides differ by {(self.ratio - 1.0) * 100:+.1f} % of their length; the seam absorbs it as ease"
         if self.kind == "ease_too_large":

@@ -163,7 +163,8 @@ def pairing_distance_m(a: SideSamples, b: SideSamples, positions, flip: bool = F
 
 
 def sew(a: SideSamples, b: SideSamples, positions) -> Tuple[Correspondence, bool]:
-    """Correspond two sides in whichever direction the current arrangement closes with less
-    travel; returns the correspondence and whether side b was flipped."""
-    flip = pairing_distance_m(a, b, positions, True) < pairing_distance_m(a, b, positions, False)
+    """Correspond two sides straight, or reversed when the reversed pairing closes with less
+    than half the travel of the straight one (garment.rs:349-353); returns the correspondence
+    and whether side b was flipped."""
+    flip = pairing_distance_m(a, b, positions, True) < 0.5 * pairing_distance_m(a, b, positions, False)
     return correspond(a, b, flip), flip
