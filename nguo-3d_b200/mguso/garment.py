@@ -106,6 +106,10 @@ class SewnGarment:
             return f"a stitch indexes past {n} vertices"
         return None
 
+    def stitch_pairs(self) -> list:
+        """The stitches as the bridge's drape loop takes them: (index[6], weight[6]) each."""
+        return [(i.tolist(), w.tolist()) for i, w in zip(self.stitch_idx, self.stitch_w)]
+
     def scene(self, density=0.2, young=1e5, poisson=0.3, thickness=5e-4, stitch_k=1.0, stitch_l0=1e-3,
               stitch_cap=1e-2, **params) -> dict:
         """The garment as a scene description for ImplicitSolver / the oracle: StVK membranes

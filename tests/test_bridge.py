@@ -137,3 +137,27 @@ def test_a_sewn_drape_through_the_loop_closes_its_seam():
     d0 = np.linalg.norm(sc["positions"][3] - sc["positions"][12])
     assert np.linalg.norm(last[3] - last[12]) < 0.5 * d0
     assert np.all(np.isfinite(last)) and np.array_equal(last[0], sc["positions"][0])
+
+
+def test_a_sewn_garment_document_drapes_through_the_loop():
+    """A garment document sewn by mguso.garment and submitted as the app does: the placed
+    scene with its stitches handed to the loop, which attaches them at the bridge's
+    constants and steps."""
+    from mguso import garment as G
+
+    g = G.build(G.sample_bodice_block(), G.SewOptions(triangulate=G.T.Options(target_edge_mm=90.0)))
+    sc = g.scene(gravity=(0.0, -9.8, 0.0), self_collision=0, bend_stiffness=0.0, contact_dhat=1e-3)
+    sc["stitch_idx"], sc["stitch_w"], sc["stitch_kl"] = scenes._empty_stitches()
+    top = np.flatnonzero(np.abs(sc["positions"][:, 1] - sc["positions"][:, 1].max()) < 1e-6)
+    sc["inv_mass"][top] = 0.0  # held by its waist
+    sink = Sink()
+    rep = bridge.drape(None, sc, 12, stitches=g.stitch_pairs(), frame_stride=4, sink=sink,
+                       solver_factory=OracleStepper)
+    assert rep["stitches"] == len(g.stitch_idx) > 0 and rep["frames_emitted"] == 4
+    last = sink.frames[-1][1]
+    assert np.all(np.isfinite(last))
+    idx, w = g.stitch_idx, g.stitch_w
+    a = (last[idx[:, :3]] * w[:, :3, None]).sum(1)
+    b = (last[idx[:, 3:]] * w[:, 3:, None]).sum(1)
+    assert np.linalg.norm(a - b, axis=1).max() < 0.01  # the seams hold while it hangs
+    assert last[:, 1].min() < sc["positions"][:, 1].min()  # and it hangs
