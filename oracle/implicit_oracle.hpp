@@ -9,14 +9,15 @@
 //   engine-core/src/bending.rs   (hinges, dihedral angle, analytic gradient)
 //   engine-core/src/stitch.rs    (six-participant seam spring)
 //   engine-core/src/strain_limit.rs (one-sided edge strain limit)
+//   engine-core/src/membrane.rs  (Baraff-Witkin warp / weft / shear membrane)
 //   engine-core/src/broadphase.rs (uniform hash grid V-T / E-E, 1-ring exclusion)
 //   engine-core/src/implicit.rs  (new, stencils, Rayleigh gather, assemble + Asm push order,
 //                                 ccd_max_step with the strain-limit and static-pin clamps,
 //                                 pins, pulls, step)
-// Restated element kinds: inertia, stretch springs (+ the one-sided edge strain limit),
-// StVK shells, hinges, stitches, the per-face strain-limit barrier, pins and pulls, analytic
-// colliders, static-mesh colliders with a signed gap, and vertex-triangle / edge-edge self
-// contact (+ friction when mu > 0).
+// Restated element kinds: inertia, stretch springs (+ the one-sided edge strain limit), the
+// Baraff-Witkin membrane, StVK shells, hinges, stitches, the per-face strain-limit barrier,
+// pins and pulls, analytic colliders, static-mesh colliders with a signed gap, and
+// vertex-triangle / edge-edge self contact (+ friction when mu > 0).
 // Added to both this oracle and the CUDA path: a Newton termination on the step actually
 // taken, max_i |t dx_i| < newton_tol (0 disables it).
 #pragma once
@@ -1059,6 +1060,189 @@ inline void edge_strain_block(const Vt<R>& xi, const Vt<R>& xj, R rest, R max_ra
 }
 
 // ---------------------------------------------------------------------------------------
+// membrane.rs: Baraff-Witkin membrane (warp / weft stretch and shear conditions)
+// ---------------------------------------------------------------------------------------
+template <class R>
+struct MembraneEl {
+  uint32_t tri[3];
+  R dm_inv[2][2];  // row-major
+  R area;
+};
+
+// deformation (membrane.rs:43-51): the columns wu, wv of F = Ds Dm^-1.
+template <class R>
+inline void bw_deformation(const Vt<R> p[3], const R dm[2][2], Vt<R>& wu, Vt<R>& wv) {
+  Vt<R> ds0 = p[1] - p[0], ds1 = p[2] - p[0];
+  wu = ds0 * dm[0][0] + ds1 * dm[1][0];
+  wv = ds0 * dm[0][1] + ds1 * dm[1][1];
+}
+
+// conditions (membrane.rs:53-57): Cu = |wu| - 1, Cv = |wv| - 1, Csh = wu.wv.
+template <class R>
+inline void bw_conditions(const Vt<R> p[3], const R dm[2][2], R c[3]) {
+  Vt<R> wu, wv;
+  bw_deformation(p, dm, wu, wv);
+  c[0] = wu.length() - R(1);
+  c[1] = wv.length() - R(1);
+  c[2] = wu.dot(wv);
+}
+
+// stretch_coeffs (membrane.rs:86-91): wu = sum cu_j x_j, wv = sum cv_j x_j.
+template <class R>
+inline void bw_coeffs(const R dm[2][2], R cu[3], R cv[3]) {
+  R a0 = dm[0][0], a1 = dm[1][0], b0 = dm[0][1], b1 = dm[1][1];
+  cu[0] = -(a0 + a1); cu[1] = a0; cu[2] = a1;
+  cv[0] = -(b0 + b1); cv[1] = b0; cv[2] = b1;
+}
+
+// condition_grads (membrane.rs:65-84): g[condition][vertex].
+template <class R>
+inline void bw_condition_grads(const Vt<R> p[3], const R dm[2][2], Vt<R> g[3][3]) {
+  Vt<R> wu, wv;
+  bw_deformation(p, dm, wu, wv);
+  R cu[3], cv[3];
+  bw_coeffs(dm, cu, cv);
+  Vt<R> nu = wu.normalize_or_zero(), nv = wv.normalize_or_zero();
+  for (int j = 0; j < 3; ++j) {
+    g[0][j] = nu * cu[j];
+    g[1][j] = nv * cv[j];
+    g[2][j] = wv * cu[j] + wu * cv[j];
+  }
+}
+
+// stretch_eigen_material (membrane.rs:100-120): n n^T + max(0, 1 - 1/|w|) (I - n n^T).
+template <class R>
+inline void bw_stretch_material(const Vt<R>& w, R m[3][3]) {
+  R s = w.length();
+  Vt<R> n = w.normalize_or_zero();
+  R perp = s > R(1.0e-6) ? rmax(R(1) - R(1) / s, R(0)) : R(0);
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      R nnt = n[r] * n[c];
+      R iden = r == c ? R(1) : R(0);
+      m[r][c] = nnt + perp * (iden - nnt);
+    }
+}
+
+template <class R>
+inline void bw_add_outer(R m[3][3], const Vt<R>& u, const Vt<R>& v, R s) {
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) m[r][c] += s * u[r] * v[c];
+}
+
+template <class R>
+inline void bw_proj_perp(const Vt<R>& w, R q[3][3]) {
+  Vt<R> n = w.normalize_or_zero();
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) q[r][c] = (r == c ? R(1) : R(0)) - n[r] * n[c];
+}
+
+// shear_material (membrane.rs:164-205): the blocks [uu, uv, vu, vv] of the eigen-projected
+// (clamp) or exact (no clamp) 6x6 shear Hessian in (wu; wv).
+template <class R>
+inline void bw_shear_material(const Vt<R>& wu, const Vt<R>& wv, bool clamp, R m[4][3][3]) {
+  R f = wu.dot(wv);
+  R a = wu.length_squared() + wv.length_squared();
+  R disc = std::sqrt(rmax(a * a + R(12) * f * f, R(0)));
+  R mu[2] = {R(0.5) * (a + disc), R(0.5) * (a - disc)};
+  auto ev = [&](R x) { return clamp ? rmax(x, R(0)) : x; };
+  for (int b = 0; b < 4; ++b)
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) m[b][r][c] = 0;
+  for (R mui : mu) {
+    Vt<R> top = wv * mui + wu * f, bot = wu * mui + wv * f;
+    R n = top.length_squared() + bot.length_squared();
+    if (n > R(1e-20)) {
+      R sc = ev(mui) / n;
+      bw_add_outer(m[0], top, top, sc);
+      bw_add_outer(m[1], top, bot, sc);
+      bw_add_outer(m[2], bot, top, sc);
+      bw_add_outer(m[3], bot, bot, sc);
+    }
+  }
+  R fp = R(0.5) * ev(f);
+  if (fp != 0) {
+    R qp[3][3];
+    bw_proj_perp(wu + wv, qp);
+    for (int b = 0; b < 4; ++b)
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) m[b][r][c] += fp * qp[r][c];
+  }
+  R fm = R(0.5) * ev(-f);
+  if (fm != 0) {
+    R qm[3][3];
+    bw_proj_perp(wv - wu, qm);
+    const R sgn[4] = {R(1), R(-1), R(-1), R(1)};
+    for (int b = 0; b < 4; ++b)
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) m[b][r][c] += (sgn[b] * fm) * qm[r][c];
+  }
+}
+
+// build_membrane (membrane.rs:272-312) for one triangle; false when degenerate.
+template <class R>
+inline bool build_membrane_el(const Vt<R>& x0, const Vt<R>& x1, const Vt<R>& x2, MembraneEl<R>& el) {
+  Vt<R> e1 = x1 - x0, e2 = x2 - x0;
+  R a = e1.length();
+  Vt<R> n = e1.cross(e2);
+  R area = R(0.5) * n.length();
+  if (a < R(1.0e-9) || area < R(1.0e-12)) return false;
+  Vt<R> t1 = e1 / a;
+  Vt<R> t2 = n.cross(e1).normalize_or_zero();
+  R b = e2.dot(t1), d = e2.dot(t2);
+  R det = a * d;
+  if (std::fabs(det) < R(1.0e-12)) return false;
+  el.dm_inv[0][0] = R(1) / a;
+  el.dm_inv[0][1] = -b / (a * d);
+  el.dm_inv[1][0] = 0;
+  el.dm_inv[1][1] = R(1) / d;
+  el.area = area;
+  return true;
+}
+
+// element_assembly (membrane.rs:225-270): gradient (vertex-major) and 9x9 Hessian of one
+// element for stiffnesses (kw, kf, ks).
+template <class R>
+inline void bw_element(const Vt<R> p[3], const MembraneEl<R>& el, R kw, R kf, R ks, R grad[9], R hess[81]) {
+  R c[3];
+  bw_conditions(p, el.dm_inv, c);
+  Vt<R> g[3][3];
+  bw_condition_grads(p, el.dm_inv, g);
+  R cu[3], cv[3];
+  bw_coeffs(el.dm_inv, cu, cv);
+  Vt<R> wu, wv;
+  bw_deformation(p, el.dm_inv, wu, wv);
+  R mu_[3][3], mv_[3][3], sm[4][3][3];
+  bw_stretch_material(wu, mu_);
+  bw_stretch_material(wv, mv_);
+  bw_shear_material(wu, wv, true, sm);
+  for (int k = 0; k < 9; ++k) grad[k] = 0;
+  for (int k = 0; k < 81; ++k) hess[k] = 0;
+  const R kc[3] = {kw, kf, ks};
+  for (int ci = 0; ci < 3; ++ci) {
+    R ka = kc[ci] * el.area;
+    if (ka <= 0) continue;
+    for (int a = 0; a < 3; ++a) {
+      for (int cc = 0; cc < 3; ++cc) grad[3 * a + cc] += ka * c[ci] * g[ci][a][cc];
+      for (int b = 0; b < 3; ++b)
+        for (int r = 0; r < 3; ++r)
+          for (int cc = 0; cc < 3; ++cc) {
+            R v;
+            if (ci < 2) {
+              const R* co = ci == 0 ? cu : cv;
+              R(*m)[3] = ci == 0 ? mu_ : mv_;
+              v = ka * co[a] * co[b] * m[r][cc];
+            } else {
+              v = ka * (cu[a] * cu[b] * sm[0][r][cc] + cu[a] * cv[b] * sm[1][r][cc] + cv[a] * cu[b] * sm[2][r][cc] +
+                        cv[a] * cv[b] * sm[3][r][cc]);
+            }
+            hess[(3 * a + r) * 9 + (3 * b + cc)] += v;
+          }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
 // broadphase.rs: uniform hash grid
 // ---------------------------------------------------------------------------------------
 struct CellKey {
@@ -1268,6 +1452,7 @@ struct Params {
   uint32_t cg_max_iter = 2000;
   R floor_y = -std::numeric_limits<R>::infinity();
   R constraint_tol = R(1.0e-2);  // pin gap floor as a fraction of ghat
+  R membrane_warp = 0, membrane_weft = 0, membrane_shear = 0;  // Baraff-Witkin stiffnesses
   R strain_limit_ratio = 0, strain_limit_k = 0, strain_limit_ratio_weft = 0;
   R newton_tol = 0;          // added termination (0 disables)
   int precond = 2;           // 1 block Jacobi (CgCpu), 2 Schwarz
@@ -1347,6 +1532,8 @@ struct ImplicitSolver {
   std::vector<SlFace<R>> sl_faces;
   std::vector<std::array<R, 2>> uvs;
   std::vector<V> kinematic_dx;  // the static collider's move since the last step
+  std::vector<MembraneEl<R>> membrane;               // built from every triangle at init
+  std::vector<std::array<R, 3>> membrane_k;          // per-element (kw, kf, ks), or empty
   LinearSolver linear;
   std::vector<StepStats> history;
 
@@ -1364,6 +1551,12 @@ struct ImplicitSolver {
     for (size_t i = 0; i < stretch_edges.size(); ++i)
       stretch_rest[i] = (pos[stretch_edges[i][0]] - pos[stretch_edges[i][1]]).length();
     hinges = build_hinges<R>(tris, positions);
+    membrane.clear();
+    for (auto& f : tris) {
+      MembraneEl<R> el;
+      el.tri[0] = f[0]; el.tri[1] = f[1]; el.tri[2] = f[2];
+      if (build_membrane_el(positions[f[0]], positions[f[1]], positions[f[2]], el)) membrane.push_back(el);
+    }
     exclusion = one_ring_exclusion(positions.size(), tris);
     edges = unique_edges(tris);
     if (edges.empty()) {
@@ -1721,6 +1914,54 @@ struct ImplicitSolver {
             trips.push(3 * a + r, 3 * b + cc, -v);
             trips.push(3 * b + r, 3 * a + cc, -v);
           }
+      }
+    }
+    // Baraff-Witkin membrane (implicit.rs:2532-2596)
+    if (params.membrane_warp > 0 || params.membrane_weft > 0 || params.membrane_shear > 0 || !membrane_k.empty()) {
+      for (size_t ei = 0; ei < membrane.size(); ++ei) {
+        const auto& el = membrane[ei];
+        R kw = membrane_k.empty() ? params.membrane_warp : membrane_k[ei][0];
+        R kf = membrane_k.empty() ? params.membrane_weft : membrane_k[ei][1];
+        R ks = membrane_k.empty() ? params.membrane_shear : membrane_k[ei][2];
+        V p[3] = {x[el.tri[0]], x[el.tri[1]], x[el.tri[2]]};
+        R cnd[3];
+        bw_conditions(p, el.dm_inv, cnd);
+        V g[3][3];
+        bw_condition_grads(p, el.dm_inv, g);
+        R cu[3], cv[3];
+        bw_coeffs(el.dm_inv, cu, cv);
+        V wu, wv;
+        bw_deformation(p, el.dm_inv, wu, wv);
+        R mu_[3][3], mv_[3][3], sm[4][3][3];
+        bw_stretch_material(wu, mu_);
+        bw_stretch_material(wv, mv_);
+        bw_shear_material(wu, wv, true, sm);
+        const R kc[3] = {kw, kf, ks};
+        // pushed per condition, vertex pair and entry, in the reference's order
+        for (int ci = 0; ci < 3; ++ci) {
+          R ka = kc[ci] * el.area;
+          if (ka <= 0) continue;
+          for (int a = 0; a < 3; ++a) {
+            uint32_t va = el.tri[a];
+            for (int c = 0; c < 3; ++c) grad[3 * va + c] += ka * cnd[ci] * g[ci][a][c];
+            for (int b = 0; b < 3; ++b) {
+              uint32_t vb = el.tri[b];
+              for (int r = 0; r < 3; ++r)
+                for (int cc = 0; cc < 3; ++cc) {
+                  R v;
+                  if (ci < 2) {
+                    const R* co = ci == 0 ? cu : cv;
+                    R(*m)[3] = ci == 0 ? mu_ : mv_;
+                    v = ka * co[a] * co[b] * m[r][cc];
+                  } else {
+                    v = ka * (cu[a] * cu[b] * sm[0][r][cc] + cu[a] * cv[b] * sm[1][r][cc] +
+                              cv[a] * cu[b] * sm[2][r][cc] + cv[a] * cv[b] * sm[3][r][cc]);
+                  }
+                  if (v != 0) trips.push(3 * va + r, 3 * vb + cc, v);
+                }
+            }
+          }
+        }
       }
     }
     // shells

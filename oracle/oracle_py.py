@@ -232,6 +232,9 @@ def _step_sigs(lib):
         "oracle_solver_collider_sides": (i32, [vp, vp]),
         "oracle_solver_self_intersect": (i32, [vp, vp]),
         "oracle_solver_set_shell_stiffness": (i32, [vp, u32, vp]),
+        "oracle_solver_set_membrane": (i32, [vp, C.c_double, C.c_double, C.c_double, u32, vp]),
+        "oracle_membrane_element": (i32, [vp, vp, f32, f32, f32, vp, vp, vp, vp]),
+        "oracle_membrane_materials": (None, [vp, vp, vp, i32, vp, vp]),
         "oracle_solver_hinges": (u32, [vp, vp, vp, u32]),
         "oracle_solver_set_pins": (i32, [vp, u32, vp, vp, vp, vp, vp]),
         "oracle_solver_set_pulls": (i32, [vp, u32, vp, vp, vp]),
@@ -355,6 +358,13 @@ class OracleSolver:
         m = np.ascontiguousarray(mu, np.float64)
         l_ = np.ascontiguousarray(lam, np.float64)
         self.lib.oracle_solver_set_shells(self.h, f.shape[0], _p(f), _p(r), _p(m), _p(l_))
+
+    def set_membrane(self, warp=0.0, weft=0.0, shear=0.0, per_element=None) -> bool:
+        """Baraff-Witkin membrane stiffnesses (ImplicitParams::membrane_*), or per element
+        (n, 3) for the membrane built from every triangle; False on a count mismatch."""
+        k = None if per_element is None else np.ascontiguousarray(per_element, np.float64).reshape(-1, 3)
+        return bool(self.lib.oracle_solver_set_membrane(self.h, warp, weft, shear, 0 if k is None else k.shape[0],
+                                                        _p(k)))
 
     def set_shell_stiffness(self, mu_lam) -> bool:
         """Per-face (mu, lambda) for the shells in order; False when the count differs."""
@@ -664,3 +674,24 @@ def stencil_friction(g4, dx4, barrier_grad, mu, eps):
     fh = np.zeros(144, np.float32)
     lib.oracle_stencil_friction(_p(g), _p(d), barrier_grad, mu, eps, _p(fg), _p(fh))
     return fg.reshape(4, 3), fh.reshape(12, 12)
+
+
+def membrane_element(rest, p, kw=1.0, kf=1.0, ks=1.0):
+    """Baraff-Witkin element (membrane.rs:225-270) in f32: (conditions, gradient 3x3,
+    Hessian 9x9, (wu, wv)), or None for a degenerate rest triangle."""
+    lib = _lib_elem()
+    r = np.ascontiguousarray(rest, np.float32).reshape(9)
+    q = np.ascontiguousarray(p, np.float32).reshape(9)
+    c, g, h, w = np.zeros(3, np.float32), np.zeros(9, np.float32), np.zeros(81, np.float32), np.zeros(6, np.float32)
+    if not lib.oracle_membrane_element(_p(r), _p(q), kw, kf, ks, _p(c), _p(g), _p(h), _p(w)):
+        return None
+    return c, g.reshape(3, 3), h.reshape(9, 9), (w[:3].copy(), w[3:].copy())
+
+
+def membrane_materials(w, wu, wv, clamp=True):
+    """(stretch material of w 3x3, shear blocks [uu, uv, vu, vv] 4x3x3) (membrane.rs:100-205)."""
+    lib = _lib_elem()
+    a, b, c = (np.ascontiguousarray(v, np.float32) for v in (w, wu, wv))
+    m9, m36 = np.zeros(9, np.float32), np.zeros(36, np.float32)
+    lib.oracle_membrane_materials(_p(a), _p(b), _p(c), 1 if clamp else 0, _p(m9), _p(m36))
+    return m9.reshape(3, 3), m36.reshape(4, 3, 3)

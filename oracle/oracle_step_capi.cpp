@@ -332,6 +332,23 @@ int oracle_solver_set_kinematic(void* h, const double* pos) {
   return a->d->set_kinematic_collider_positions(x);
 }
 
+// Baraff-Witkin membrane stiffnesses (warp, weft, shear) and optional per-element values
+// (n = 0 clears them; otherwise n must be the element count): 1 accepted, 0 not.
+int oracle_solver_set_membrane(void* h, double kw, double kf, double ks, uint32_t n, const double* k3) {
+  auto* a = (AnySolver*)h;
+  auto apply = [&](auto& s) {
+    using R = typename std::decay_t<decltype(s.membrane_k)>::value_type::value_type;
+    if (n && n != s.membrane.size()) return 0;
+    s.params.membrane_warp = (R)kw;
+    s.params.membrane_weft = (R)kf;
+    s.params.membrane_shear = (R)ks;
+    s.membrane_k.assign(n, {});
+    for (uint32_t i = 0; i < n; ++i) s.membrane_k[i] = {(R)k3[3 * i], (R)k3[3 * i + 1], (R)k3[3 * i + 2]};
+    return 1;
+  };
+  return a->prec == 0 ? apply(*a->f) : apply(*a->d);
+}
+
 // set_shell_stiffness (per-face (mu, lambda) for the current shells, in their order):
 // 1 when accepted, 0 when n is not the shell count (nothing changed).
 int oracle_solver_set_shell_stiffness(void* h, uint32_t n, const double* mu_lam) {
@@ -572,6 +589,45 @@ int oracle_strain_limit_face(int f64, int kind, const double* rest9, const doubl
                              double* hess81) {
   return f64 ? strain_limit_face_t<double>(kind, rest9, p9, limit, mass, elastic_k, eps, dynamic, energy, grad9, hess81)
              : strain_limit_face_t<float>(kind, rest9, p9, limit, mass, elastic_k, eps, dynamic, energy, grad9, hess81);
+}
+
+// Baraff-Witkin element (f32) from a rest triangle rest9 at positions p9: conditions c3,
+// element gradient g9 and Hessian h81 (element_assembly); returns 0 for a degenerate rest
+// triangle. wuv6, when given, receives the deformation columns wu, wv.
+int oracle_membrane_element(const float* rest9, const float* p9, float kw, float kf, float ks, float* c3, float* g9,
+                            float* h81, float* wuv6) {
+  Vt<float> r[3], p[3];
+  for (int k = 0; k < 3; ++k) {
+    r[k] = Vt<float>(rest9[3 * k], rest9[3 * k + 1], rest9[3 * k + 2]);
+    p[k] = Vt<float>(p9[3 * k], p9[3 * k + 1], p9[3 * k + 2]);
+  }
+  MembraneEl<float> el;
+  if (!build_membrane_el(r[0], r[1], r[2], el)) return 0;
+  bw_conditions(p, el.dm_inv, c3);
+  bw_element(p, el, kw, kf, ks, g9, h81);
+  if (wuv6) {
+    Vt<float> wu, wv;
+    bw_deformation(p, el.dm_inv, wu, wv);
+    for (int c = 0; c < 3; ++c) {
+      wuv6[c] = wu[c];
+      wuv6[3 + c] = wv[c];
+    }
+  }
+  return 1;
+}
+
+// Baraff-Witkin materials (f32): stretch material of w3 into m9, shear blocks of (wu, wv)
+// into m36 ([uu, uv, vu, vv], each row-major), clamped or exact.
+void oracle_membrane_materials(const float* w3, const float* wu3, const float* wv3, int clamp, float* m9,
+                               float* m36) {
+  float m[3][3], sm[4][3][3];
+  bw_stretch_material(Vt<float>(w3[0], w3[1], w3[2]), m);
+  bw_shear_material(Vt<float>(wu3[0], wu3[1], wu3[2]), Vt<float>(wv3[0], wv3[1], wv3[2]), clamp != 0, sm);
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) m9[3 * r + c] = m[r][c];
+  for (int b = 0; b < 4; ++b)
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) m36[9 * b + 3 * r + c] = sm[b][r][c];
 }
 
 // One-sided edge strain limit in f32: energy, grad_i g3 and h_ii h9 (row-major).
