@@ -24,8 +24,10 @@ with the reference's three scale-free gates; ``write_obj`` writes one frame as O
 """
 from __future__ import annotations
 
+import math
 import os
-from dataclasses import dataclass
+from dataclasses import dataclass, field
+from typing import Optional
 
 import numpy as np
 
@@ -179,6 +181,152 @@ def read_pin_indices(scene_dir: str) -> np.ndarray:
         out.append(decode_u64_list(_read(os.path.join(ib, f"pin-ind-{i}.bin")), f"pin-ind-{i}.bin"))
         i += 1
     return np.concatenate(out) if out else np.zeros(0, np.uint32)
+
+
+def read_pin_blocks(scene_dir: str) -> list:
+    """Each pin block's vertex list, in block order (golden.rs:880-913)."""
+    ib = os.path.join(scene_dir, "input_bin")
+    out, i = [], 0
+    while os.path.exists(os.path.join(ib, f"pin-ind-{i}.bin")):
+        out.append(decode_u64_list(_read(os.path.join(ib, f"pin-ind-{i}.bin")), f"pin-ind-{i}.bin"))
+        i += 1
+    return out
+
+
+def _toml_section(text: str, want: str) -> dict:
+    """key = value pairs of one [section] of a flat TOML text, quotes stripped
+    (golden.rs:1205-1225)."""
+    out, inside = {}, False
+    for line in text.splitlines():
+        t = line.strip()
+        if t.startswith("[") and t.endswith("]"):
+            inside = t[1:-1] == want
+            continue
+        if inside and "=" in t:
+            k, v = (x.strip() for x in t.split("=", 1))
+            out[k] = v.strip('"')
+    return out
+
+
+@dataclass
+class PinOp:
+    """One scheduled pin operation (golden.rs:930-1018): kind (move_by, move_to, spin, scale
+    or an unsupported name), its window and easing, the spin / scale parameters and the
+    per-vertex payload (a delta for move_by, a target for move_to)."""
+    kind: str
+    t_start: float
+    t_end: float
+    transition: str = "linear"   # linear, smooth, bezier (bezier eases linearly)
+    center: tuple = (0.0, 0.0, 0.0)
+    axis: tuple = (0.0, 0.0, 0.0)
+    angular_velocity: float = 0.0  # degrees per second
+    factor: float = 1.0
+    data: Optional[np.ndarray] = None
+
+    def progress_at(self, time: float) -> Optional[float]:
+        """The eased ramp in [0, 1]; None before t_start (golden.rs:974-993)."""
+        if time < self.t_start:
+            return None
+        if time >= self.t_end:
+            return 1.0
+        denom = self.t_end - self.t_start
+        raw = (time - self.t_start) / denom if denom != 0.0 else 0.0
+        return raw * raw * (3.0 - 2.0 * raw) if self.transition == "smooth" else raw
+
+
+def _rodrigues(p, center, axis, angle):
+    """p rotated by angle about the normalised axis through center, in f64, returned in f32
+    (golden.rs:1088-1116); a zero axis does not rotate."""
+    a = np.asarray(axis, np.float32).astype(np.float64)
+    n = float(np.sqrt((np.float32(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]))))
+    a = a * (1.0 / n if n > 0.0 else 0.0)
+    c = np.asarray(center, np.float32)
+    d = (np.asarray(p, np.float32) - c).astype(np.float64)
+    ct, st = math.cos(angle), math.sin(angle)
+    out = d * ct + np.cross(a, d) * st + a * float(d @ a) * (1.0 - ct)
+    return out.astype(np.float32) + c
+
+
+@dataclass
+class PinBlockSchedule:
+    """A pin block: its vertices, the FixPair stiffness and pull scalars, and its ordered
+    operations (golden.rs:995-1083)."""
+    indices: np.ndarray
+    stiffness: float = 1.0
+    pull: float = 0.0
+    ops: list = field(default_factory=list)
+
+    def target_at(self, slot: int, base, time: float):
+        """(target, kinematic) of the block's slot-th vertex at time, composing every
+        operation in order from its displaced initial position (golden.rs:1022-1082)."""
+        p = np.asarray(base, np.float32).copy()
+        kinematic = False
+        for op in self.ops:
+            if op.kind in ("move_by", "move_to"):
+                prog = op.progress_at(time)
+                if prog is None or op.data is None or slot >= len(op.data):
+                    continue
+                row = np.asarray(op.data[slot], np.float32)
+                pr = np.float32(prog)
+                p = p + row * pr if op.kind == "move_by" else p + (row - p) * pr
+                kinematic = True
+            elif op.kind == "spin":
+                angle = math.radians(float(np.float32(op.angular_velocity))) * (min(time, op.t_end) - op.t_start)
+                if angle <= 0.0:
+                    continue
+                p = _rodrigues(p, op.center, op.axis, angle)
+                kinematic = True
+            elif op.kind == "scale":
+                if time < op.t_start:
+                    continue
+                if time >= op.t_end:
+                    f = np.float32(op.factor)
+                else:
+                    f = np.float32(1.0 + (float(np.float32(op.factor)) - 1.0) * (op.progress_at(time) or 0.0))
+                c = np.asarray(op.center, np.float32)
+                p = (p - c) * f + c
+                kinematic = True
+        return p.astype(np.float32), kinematic
+
+
+def read_pin_schedule(scene_dir: str) -> list:
+    """Every pin block's schedule from info.toml's [pin-<i>] / [pin-<i>-op-<j>] tables and
+    the op payloads pin-<i>-op-<j>.bin (golden.rs:1122-1200)."""
+    blocks = read_pin_blocks(scene_dir)
+    ip = os.path.join(scene_dir, "info.toml")
+    info = open(ip, encoding="utf-8", errors="replace").read() if os.path.exists(ip) else ""
+    ib = os.path.join(scene_dir, "input_bin")
+
+    def num(sec, k, d):
+        try:
+            return float(sec[k])
+        except (KeyError, ValueError):
+            return d
+
+    out = []
+    for i, idx in enumerate(blocks):
+        head = _toml_section(info, f"pin-{i}")
+        ops = []
+        for j in range(int(num(head, "operation_count", 0))):
+            sec = _toml_section(info, f"pin-{i}-op-{j}")
+            ty = sec.get("type", "")
+            vec = tuple(float(np.float32(num(sec, f"center_{a}", 0.0))) for a in "xyz")
+            axis = tuple(float(np.float32(num(sec, f"axis_{a}", 0.0))) for a in "xyz")
+            path = os.path.join(ib, f"pin-{i}-op-{j}.bin")
+            data = None
+            if os.path.exists(path):
+                data = decode_vec3_f64(_read(path)).astype(np.float32)
+                if len(data) != len(idx):
+                    raise CaptureError(f"pin-{i}-op-{j}.bin has {len(data)} rows but block {i} holds {len(idx)} vertices")
+            tr = sec.get("transition")
+            ops.append(PinOp(ty if ty in ("move_by", "move_to", "spin", "scale") else (ty or "unsupported"),
+                             num(sec, "t_start", 0.0), num(sec, "t_end", 0.0),
+                             tr if tr in ("smooth", "bezier") else "linear", vec, axis,
+                             float(np.float32(num(sec, "angular_velocity", 0.0))),
+                             float(np.float32(num(sec, "factor", 1.0))), data))
+        out.append(PinBlockSchedule(idx, float(np.float32(num(head, "stiffness", 1.0))),
+                                    float(np.float32(num(head, "pull", 0.0))), ops))
+    return out
 
 
 def read_stitches(scene_dir: str):

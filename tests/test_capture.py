@@ -7,6 +7,7 @@ import pytest
 
 import oracle_py as O
 from mguso import capture as cap
+from mguso import scenes
 
 
 def _f64(vals):
@@ -199,3 +200,82 @@ def test_a_capture_drives_the_step_and_compares_to_its_checkpoint(tmp_path):
     cap.write_obj(str(tmp_path / "frame_3.obj"), x, sc["tris"])
     q, _ = cap.read_obj(str(tmp_path / "frame_3.obj"))
     assert np.array_equal(q, x.astype(np.float32))
+
+
+def _sched(kind, t0, t1, **kw):
+    from mguso.capture import PinBlockSchedule, PinOp
+
+    return PinBlockSchedule(np.array([0], np.uint32), 1.0, 0.0, [PinOp(kind, t0, t1, **kw)])
+
+
+def test_spin_and_scale_ops_match_the_reference_laws():  # golden.rs:1544-1635
+    def near(a, b):
+        return np.abs(np.asarray(a, np.float64) - np.asarray(b, np.float64)).max() < 1e-5
+
+    spin = _sched("spin", 0.0, 2.0, center=(0.0, 0.0, 0.0), axis=(0.0, 0.0, 1.0), angular_velocity=90.0)
+    x = [1.0, 0.0, 0.0]
+    q, kin = spin.target_at(0, x, 1.0)
+    assert near(q, [0, 1, 0]) and kin
+    h, _ = spin.target_at(0, x, 0.5)
+    r = np.float32(np.sqrt(0.5))
+    assert near(h, [r, r, 0]) and abs(np.hypot(h[0], h[1]) - 1.0) < 1e-5
+    e1, e2 = spin.target_at(0, x, 2.0)[0], spin.target_at(0, x, 50.0)[0]
+    assert near(e1, [-1, 0, 0]) and near(e1, e2)
+    later = _sched("spin", 5.0, 6.0, center=(0.0, 0.0, 0.0), axis=(0.0, 0.0, 1.0), angular_velocity=90.0)
+    pre, pre_kin = later.target_at(0, x, 0.0)
+    assert near(pre, x) and not pre_kin
+    sc = _sched("scale", 0.0, 1.0, center=(1.0, 1.0, 1.0), factor=3.0)
+    p = [2.0, 1.0, 1.0]
+    assert near(sc.target_at(0, p, 0.0)[0], [2, 1, 1]) and near(sc.target_at(0, p, 0.5)[0], [3, 1, 1])
+    assert near(sc.target_at(0, p, 1.0)[0], [4, 1, 1]) and near(sc.target_at(0, p, 9.0)[0], [4, 1, 1])
+    assert near(sc.target_at(0, [1, 1, 1], 1.0)[0], [1, 1, 1])
+
+
+def test_a_pin_schedule_decodes_from_info_toml_and_composes(tmp_path):  # golden.rs:1122-1200
+    from mguso import capture
+
+    d = tmp_path / "scene"
+    ib = d / "input_bin"
+    ib.mkdir(parents=True)
+    (ib / "pin-ind-0.bin").write_bytes(np.array([3, 7], "<u8").tobytes())
+    (ib / "pin-0-op-0.bin").write_bytes(np.array([[0.0, 0.1, 0.0], [0.0, 0.1, 0.0]], "<f8").tobytes())
+    (d / "info.toml").write_text('[pin-0]\noperation_count = 2\nstiffness = 2.5\n\n'
+                                 '[pin-0-op-0]\ntype = "move_by"\nt_start = 0.0\nt_end = 1.0\ntransition = "smooth"\n\n'
+                                 '[pin-0-op-1]\ntype = "torque"\nt_start = 0.0\nt_end = 1.0\n')
+    (s,) = capture.read_pin_schedule(str(d))
+    assert s.indices.tolist() == [3, 7] and s.stiffness == 2.5
+    assert [o.kind for o in s.ops] == ["move_by", "torque"]
+    # smoothstep at a quarter of the window: 0.25^2 (3 - 0.5) = 0.15625 of the 0.1 delta
+    q, kin = s.target_at(1, [1.0, 0.0, 0.0], 0.25)
+    assert kin and abs(q[1] - 0.015625) < 1e-7 and q[0] == 1.0
+    assert s.target_at(1, [1.0, 0.0, 0.0], 5.0)[0].tolist() == [1.0, np.float32(0.1), 0.0]
+    (ib / "pin-0-op-0.bin").write_bytes(np.zeros((3, 3), "<f8").tobytes())
+    with pytest.raises(capture.CaptureError):
+        capture.read_pin_schedule(str(d))
+
+
+def test_a_scheduled_pin_drags_its_vertex_in_the_oracle_step(tmp_path):
+    """A move_by schedule driving kinematic pins between steps, as a capture replay does."""
+    from mguso.capture import PinBlockSchedule, PinOp
+
+    n = 4
+    pos = np.array([(i * 0.1, 0.0, j * 0.1) for j in range(n) for i in range(n)], np.float32)
+    tris = np.array([(j * n + i, j * n + i + 1, j * n + i + n) for j in range(n - 1) for i in range(n - 1)] +
+                    [(j * n + i + n, j * n + i + 1, j * n + i + n + 1) for j in range(n - 1) for i in range(n - 1)],
+                    np.uint32)
+    si, sw, skl = scenes._empty_stitches()
+    sc = dict(positions=pos, velocities=np.zeros_like(pos), inv_mass=np.full(n * n, 10.0, np.float32), tris=tris,
+              shell_faces=np.zeros((0, 3), np.uint32), static_mask=None, stitch_idx=si, stitch_w=sw, stitch_kl=skl,
+              colliders=np.zeros((0, 8), np.float32),
+              params=scenes.default_params(self_collision=0, stiffness=500.0, gravity=(0.0, 0.0, 0.0),
+                                           bend_stiffness=0.0, newton_iters=4, precond=1))
+    sched = PinBlockSchedule(np.array([0], np.uint32), 1.0, 0.0,
+                             [PinOp("move_by", 0.0, 0.5, data=np.array([[0.0, 0.3, 0.0]], np.float32))])
+    o = O.OracleSolver(sc)
+    dt = sc["params"]["dt"]
+    for k in range(1, 41):
+        t, _ = sched.target_at(0, pos[0], k * dt)
+        assert o.set_pins([(0, t.astype(np.float64), 0.02, True, sched.stiffness)])
+        o.step(1, check_intersection=False)
+    x = o.positions()
+    assert np.all(np.isfinite(x)) and abs(x[0, 1] - 0.3) < 0.04 and x[0, 1] > 0.2
