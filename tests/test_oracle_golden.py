@@ -1,7 +1,7 @@
 """The oracle reproduces its committed golden trajectories bit for bit (FP32 and FP64
 positions and per-step Newton counts of three small drapes, made by
 tests/golden/make_oracle_trajectories.py), so any change to the restatement that moves a
-trajectory is seen here before it can move a GPU parity verdict."""
+trajectory is seen here before it can change a GPU parity result."""
 import os
 import sys
 
