@@ -477,19 +477,57 @@ def write_obj(path: str, positions, tris=None) -> None:
             np.savetxt(f, t, fmt="f %d %d %d")
 
 
+def parse_obj(text: str, with_uvs: bool = False):
+    """(positions float32 (n, 3), triangles uint32 (m, 3)[, per-vertex uvs float32 (n, 2) or
+    empty]) from Wavefront OBJ text (engine-io obj.rs): polygons are fan-triangulated,
+    ``f a/b/c`` forms read the vertex (and texture) index, negative indices count back from
+    the records read so far, and an index out of range is a CaptureError. UVs are kept only
+    when every face corner names one (parallel or empty), a missing ``vt`` v reads as 0."""
+    v, vt, fcs, fuv = [], [], [], []
+    all_uv = True
+    for line in text.splitlines():
+        s = line.split()
+        if not s:
+            continue
+        if s[0] == "v":
+            v.append([float(x) for x in s[1:4]])
+        elif s[0] == "vt":
+            vt.append([float(s[1]), float(s[2]) if len(s) > 2 else 0.0])
+        elif s[0] == "f":
+            ids, uvs = [], []
+            for tok in s[1:]:
+                parts = tok.split("/")
+                i = int(parts[0])
+                i = i - 1 if i > 0 else len(v) + i
+                if not 0 <= i < len(v):
+                    raise CaptureError(f"face index {parts[0]} is outside the {len(v)} vertices")
+                ids.append(i)
+                if len(parts) > 1 and parts[1]:
+                    j = int(parts[1])
+                    j = j - 1 if j > 0 else len(vt) + j
+                    if not 0 <= j < len(vt):
+                        raise CaptureError(f"texture index {parts[1]} is outside the {len(vt)} uvs")
+                    uvs.append(j)
+                else:
+                    all_uv = False
+            for k in range(1, len(ids) - 1):  # fan-triangulate polygons
+                fcs.append([ids[0], ids[k], ids[k + 1]])
+                if len(uvs) == len(ids):
+                    fuv.append([uvs[0], uvs[k], uvs[k + 1]])
+    pos = np.asarray(v, np.float32).reshape(-1, 3)
+    tris = np.asarray(fcs, np.uint32).reshape(-1, 3)
+    if not with_uvs:
+        return pos, tris
+    uv = np.zeros((0, 2), np.float32)
+    if all_uv and fcs and vt:
+        uv = np.zeros((len(v), 2), np.float32)
+        for t, tu in zip(fcs, fuv):
+            for a, b in zip(t, tu):
+                uv[a] = vt[b]
+    return pos, tris, uv
+
+
 def read_obj(path: str):
-    """(positions float32 (n, 3), triangles uint32 (m, 3)) from an OBJ holding ``v`` and
-    triangular ``f`` records (``f a/b/c`` forms keep the vertex index)."""
-    v, fcs = [], []
+    """(positions float32 (n, 3), triangles uint32 (m, 3)) of an OBJ file (see parse_obj)."""
     with open(path) as f:
-        for line in f:
-            s = line.split()
-            if not s:
-                continue
-            if s[0] == "v":
-                v.append([float(x) for x in s[1:4]])
-            elif s[0] == "f":
-                ids = [int(x.split("/")[0]) for x in s[1:]]
-                for k in range(1, len(ids) - 1):  # fan-triangulate polygons
-                    fcs.append([ids[0] - 1, ids[k] - 1, ids[k + 1] - 1])
-    return np.asarray(v, np.float32).reshape(-1, 3), np.asarray(fcs, np.uint32).reshape(-1, 3)
+        return parse_obj(f.read())

@@ -279,3 +279,33 @@ def test_a_scheduled_pin_drags_its_vertex_in_the_oracle_step(tmp_path):
         o.step(1, check_intersection=False)
     x = o.positions()
     assert np.all(np.isfinite(x)) and abs(x[0, 1] - 0.3) < 0.04 and x[0, 1] > 0.2
+
+
+def test_obj_round_trip_quad(tmp_path):  # engine-io obj.rs:429-440
+    pos, tris = cap.parse_obj("v 0 0 0\nv 1 0 0\nv 0 1 0\nv 1 1 0\nf 1 2 3\nf 3 2 4\n")
+    assert pos.shape == (4, 3) and tris.shape == (2, 3)
+    cap.write_obj(str(tmp_path / "q.obj"), pos, tris)
+    p2, t2 = cap.read_obj(str(tmp_path / "q.obj"))
+    assert np.array_equal(p2, pos) and np.array_equal(t2, tris)
+
+
+def test_obj_triangulates_quad_face():  # obj.rs:442-446
+    assert cap.parse_obj("v 0 0 0\nv 1 0 0\nv 1 1 0\nv 0 1 0\nf 1 2 3 4\n")[1].shape == (2, 3)
+
+
+def test_obj_handles_slashed_and_negative_indices():  # obj.rs:448-458
+    _, tris, uv = cap.parse_obj("v 0 0 0\nv 1 0 0\nv 0 1 0\nvt 0 0\nvt 1 0\nvt 0 1\nvn 0 0 1\nvn 0 0 1\nvn 0 0 1\n"
+                                "f -3/-3/-3 -2/-2/-2 -1/-1/-1\n", with_uvs=True)
+    assert tris.tolist() == [[0, 1, 2]] and uv.tolist() == [[0, 0], [1, 0], [0, 1]]
+
+
+def test_obj_rejects_out_of_range_index():  # obj.rs:459-464
+    with pytest.raises(cap.CaptureError):
+        cap.parse_obj("v 0 0 0\nf 1 2 3\n")
+    with pytest.raises(cap.CaptureError):
+        cap.parse_obj("v 0 0 0\nv 1 0 0\nv 0 1 0\nvt 0 0\nf 1/1 2/2 3/1\n")
+
+
+def test_obj_face_without_uv_index_drops_the_uv_array():  # obj.rs:477-484
+    _, _, uv = cap.parse_obj("v 0 0 0\nv 1 0 0\nv 0 1 0\nvt 0 0\nvt 1 0\nvt 0 1\nf 1/1 2/2 3\n", with_uvs=True)
+    assert uv.shape == (0, 2)
