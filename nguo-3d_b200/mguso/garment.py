@@ -160,9 +160,7 @@ def build(doc: Document, opts: SewOptions = SewOptions()) -> SewnGarment:
     extents = []
     for pid, mesh in meshes:
         f = doc.features.get(pid, {})
-        support = f.get("support_edge")
-        extents.append(A.PieceExtent(pid, tuple(mesh.pattern_bounds()), f.get("placement"),
-                                     None if support is None else doc.pieces[pid].arc_length(support)))
+        extents.append(A.PieceExtent(pid, tuple(mesh.pattern_bounds()), f.get("placement"), support_arc_mm(doc, pid)))
     arrangement = A.arrange(extents, opts.arrange)
     timings["arrange"] = (time.perf_counter() - t) * 1e3
 
@@ -207,7 +205,34 @@ def build(doc: Document, opts: SewOptions = SewOptions()) -> SewnGarment:
     return g
 
 
+@dataclass
+class Hang:
+    """Where a garment hangs, read off the document before any mesh exists (arrange.rs:253-294):
+    the first piece's support landmark and the tallest piece's height in pattern mm."""
+    landmark: Optional[str] = None
+    drop_mm: float = 0.0
+
+
+def hang(doc: Document) -> Hang:
+    out = Hang()
+    for pid in sorted(doc.pieces):
+        net = doc.pieces[pid]
+        if net.vertices:
+            x0, y0, x1, y1 = net.bounds()
+            out.drop_mm = max(out.drop_mm, y1 - y0)
+        if out.landmark is None:
+            out.landmark = doc.features.get(pid, {}).get("landmark")
+    return out
+
+
+def support_arc_mm(doc: Document, pid: int) -> Optional[float]:
+    """Arc length of the piece's support edge in pattern mm (arrange.rs:296-303)."""
+    e = doc.features.get(pid, {}).get("support_edge")
+    return None if e is None else doc.pieces[pid].arc_length(e)
+
+
 PANEL_W_MM = PANEL_H_MM = 560.0
+SUPPORT_LANDMARK = "hip"
 PANEL_GAP_MM = 80.0
 E_WAIST, E_RIGHT, E_HEM, E_LEFT = 0, 1, 2, 3
 
@@ -226,7 +251,7 @@ def sample_bodice_block() -> Document:
     added = []
     for name, x in (("Front bodice", 0.0), ("Back bodice", PANEL_W_MM + PANEL_GAP_MM)):
         net, e = _rect_panel(x, PANEL_W_MM, PANEL_H_MM)
-        added.append((doc.add_piece(net, name=name, support_edge=e[E_WAIST]), e))
+        added.append((doc.add_piece(net, name=name, support_edge=e[E_WAIST], landmark=SUPPORT_LANDMARK), e))
     (front, fe), (back, be) = added
     doc.add_seam(Seam(SeamSide(front, [(fe[E_RIGHT], False)]), SeamSide(back, [(be[E_LEFT], True)])))
     doc.add_seam(Seam(SeamSide(front, [(fe[E_LEFT], True)]), SeamSide(back, [(be[E_RIGHT], False)])))

@@ -43,7 +43,8 @@ class Seam:
 class Document:
     """Pieces (networks by id) and seams by id. ``features`` per piece may hold ``notches``
     ([(edge, t)], registration marks that become mesh vertices), ``placement`` (an authored
-    ((x, y, z) mm, quaternion)), ``support_edge`` (the edge the piece hangs by) and ``name``."""
+    ((x, y, z) mm, quaternion)), ``support_edge`` (the edge the piece hangs by), ``landmark`` (the
+    body landmark it hangs from) and ``name``."""
     pieces: Dict[int, Network] = field(default_factory=dict)
     seams: Dict[int, Seam] = field(default_factory=dict)
     features: Dict[int, dict] = field(default_factory=dict)

@@ -120,3 +120,24 @@ def test_the_sewn_sample_holds_its_seams_in_the_step():
     o.step(10, check_intersection=False)
     x = o.positions()
     assert np.all(np.isfinite(x)) and gap(x) < 5e-3  # the closed tube stays closed
+
+
+def test_the_sample_hangs_from_the_girth_it_was_sized_for():  # sample.rs:379-395
+    doc = G.sample_bodice_block()
+    h = G.hang(doc)
+    assert h.landmark == G.SUPPORT_LANDMARK and abs(h.drop_mm - G.PANEL_H_MM) < 1e-9
+    arcs = [G.support_arc_mm(doc, p) for p in sorted(doc.pieces)]
+    assert arcs == [G.PANEL_W_MM, G.PANEL_W_MM]
+    assert 0.025 < sum(arcs) / 1087.3 - 1.0 < 0.035  # 3 % ease over the hip girth it was sized for
+
+
+def test_hang_reads_the_support_annotation_and_the_garment_drop():  # arrange.rs:694-734
+    assert G.hang(S.Document()) == G.Hang()
+    n = G.T.Network()
+    v = [n.add_vertex(x, y) for x, y in [(0, 0), (400, 0), (400, 700), (0, 700)]]
+    e = [n.add_edge(v[k], v[(k + 1) % 4], G.T.CUT) for k in range(4)]
+    doc = S.Document()
+    pid = doc.add_piece(n, support_edge=e[0], landmark="waist")
+    assert G.support_arc_mm(doc, pid) == 400.0
+    h = G.hang(doc)
+    assert h.landmark == "waist" and abs(h.drop_mm - 700.0) < 1e-9
