@@ -1445,6 +1445,7 @@ struct Params {
   R shell_mu = 0, shell_lambda = 0;
   R friction = 0, friction_eps = R(1.0e-3);
   R collider_friction = std::numeric_limits<R>::infinity();
+  int friction_mode = 0;  // how two coefficients combine: 0 min, 1 max, 2 mean (contact.rs:141-205)
   BarrierKind barrier_kind = BarrierKind::Log;
   bool contact_rayleigh = false;
   bool self_collision = false;
@@ -2101,7 +2102,11 @@ struct ImplicitSolver {
         if (inv_mass[i] <= 0) continue;
         R m = R(1) / inv_mass[i];
         R mu_i = params.friction;
-        if (std::isfinite(params.collider_friction)) mu_i = rmin(mu_i, params.collider_friction);
+        // combined with the collider's own coefficient only when it is set (implicit.rs:2975-2990)
+        if (std::isfinite(params.collider_friction)) {
+          R cf = params.collider_friction;
+          mu_i = params.friction_mode == 1 ? rmax(mu_i, cf) : params.friction_mode == 2 ? R(0.5) * (mu_i + cf) : rmin(mu_i, cf);
+        }
         bool has_slip = mu_i > 0;
         V cg;
         R ch[3][3];

@@ -241,6 +241,7 @@ def _step_sigs(lib):
         "oracle_solver_set_strain_limit_faces": (i32, [vp, u32, vp, vp, vp, u32, u32]),
         "oracle_solver_set_limits": (None, [vp, C.c_double, C.c_double, C.c_double, C.c_double, u32, vp]),
         "oracle_solver_set_stretch_edges": (None, [vp, u32, vp]),
+        "oracle_solver_set_friction": (None, [vp, C.c_double, i32]),
         "oracle_strain_limit_face": (i32, [i32, i32, vp, vp, C.c_double, C.c_double, C.c_double, C.c_double, i32,
                                            vp, vp, vp]),
         "oracle_edge_strain": (f32, [vp, vp, f32, f32, f32, vp, vp]),
@@ -429,6 +430,11 @@ class OracleSolver:
         uv = None if uvs is None else np.ascontiguousarray(uvs, np.float64).reshape(-1, 2)
         self.lib.oracle_solver_set_limits(self.h, constraint_tol, strain_limit_ratio, strain_limit_k,
                                           strain_limit_ratio_weft, 0 if uv is None else uv.shape[0], _p(uv))
+
+    def set_collider_friction(self, collider_friction=float("inf"), mode="min"):
+        """The collider's coefficient (inf: unset) and the mode it combines with the cloth's
+        under (ImplicitParams::collider_friction, friction_mode)."""
+        self.lib.oracle_solver_set_friction(self.h, collider_friction, {"min": 0, "max": 1, "mean": 2}[mode])
 
     def set_stretch_edges(self, edges):
         """Replace the stretch edges (rest lengths from the current positions)."""

@@ -429,6 +429,19 @@ void oracle_solver_set_limits(void* h, double constraint_tol, double ratio, doub
     set_limits_t(*a->d, constraint_tol, ratio, k, ratio_weft, nuv, uv);
 }
 
+// The collider's friction coefficient (infinity: unset) and the friction mode (0 min, 1 max,
+// 2 mean) it combines with the cloth's under.
+void oracle_solver_set_friction(void* h, double collider_friction, int mode) {
+  auto* a = (AnySolver*)h;
+  if (a->prec == 0) {
+    a->f->params.collider_friction = (float)collider_friction;
+    a->f->params.friction_mode = mode;
+  } else {
+    a->d->params.collider_friction = collider_friction;
+    a->d->params.friction_mode = mode;
+  }
+}
+
 // Replaces the stretch edges (a mesh with explicit edges, as the reference's Mesh carries);
 // rest lengths from the current positions.
 void oracle_solver_set_stretch_edges(void* h, uint32_t n, const uint32_t* edges) {

@@ -253,3 +253,26 @@ def test_the_stitch_energy_is_translation_invariant():  # stitch.rs:239-255 (the
     g0, h0 = O.stitch(x, w, 0.001, 0.01)
     g1, h1 = O.stitch(x + [1.5, -2.0, 0.25], w, 0.001, 0.01)
     assert np.allclose(g0, g1, rtol=1e-9, atol=1e-12) and np.allclose(h0, h1, rtol=1e-9, atol=1e-9)
+
+
+def _slide_on_floor(collider_friction, mode):
+    pos, tris = grid(4, 0.25)
+    o = O.OracleSolver(scene(pos, tris, 0.1, FLOOR, stiffness=5.0e2, gravity=(2.0, -9.8, 0.0), contact_dhat=0.02,
+                             contact_kappa=1.0e3, friction=0.9))
+    o.set_collider_friction(collider_friction, mode)
+    o.step(80, check_intersection=False)
+    p = o.positions()
+    assert np.all(np.isfinite(p))
+    return float((p[:, 0] - pos[:, 0]).astype(f32).mean())
+
+
+def test_collider_friction_combines_as_min_with_the_vertex_value():  # implicit.rs:6877-6928
+    rough, slick = _slide_on_floor(0.9, "min"), _slide_on_floor(0.0, "min")
+    assert slick > rough * 1.5 and slick > 1e-3, (slick, rough)
+    assert abs(_slide_on_floor(float("inf"), "min") - rough) < 1e-6
+
+
+def test_unset_collider_friction_is_inert_under_every_friction_mode():  # implicit.rs:6938-6991
+    for mode in ("min", "max", "mean"):
+        unset, explicit = _slide_on_floor(float("inf"), mode), _slide_on_floor(0.9, mode)
+        assert abs(unset - explicit) < 1e-4 and np.isfinite(unset), mode
