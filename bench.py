@@ -307,6 +307,7 @@ def run_spmv(args, dist: Dist):
 
 BATCH_WORKLOAD = ("sheath graded XS..XXL (panel widths 0.50-0.75 m) on 6 torsos scaled 0.9-1.2, one batch, "
                   "per-instance Newton/CCD/PCG convergence")
+BATCH_UNIT = "drape-steps/s"
 
 
 def drape_scene(which: str):
@@ -320,43 +321,69 @@ def drape_scene(which: str):
     return sc, "seamed sheath 41400 tris + 278 stitches on 19800-tri torso, 120-step drape"
 
 
-def _oracle_drape_worker(job):
-    """One drape on the oracle's f32 implicit step for at least `seconds` (one step at least):
-    (steps, seconds)."""
-    which, i, seconds = job
-    import oracle_py as O
+def _instance_scene(which: str, i: int):
     from mguso import scenes
 
-    sc = scenes.graded_sheath(i) if which == "batch" else drape_scene(which)[0]
-    o = O.OracleSolver(sc, "f32")
+    return scenes.graded_sheath(i) if which == "batch" else drape_scene(which)[0]
+
+
+def _oracle_window_worker(job):
+    """One drape on the oracle's implicit step: `warmup` untimed steps from the scene's start
+    (or the given state), then at least one timed step and more while `seconds` last.
+    Returns (timed steps, seconds, Newton iterations per timed step, positions after the
+    first timed step)."""
+    which, i, precision, warmup, seconds, state = job
+    import oracle_py as O
+
+    sc = _instance_scene(which, i)
+    o = O.OracleSolver(sc, precision)
+    if state is not None:
+        o.set_state(state[0], state[1])
+    if warmup:
+        o.step(warmup, check_intersection=False)
     t0 = time.perf_counter()
-    n = 0
+    n, newton, first = 0, [], None
     while n == 0 or time.perf_counter() - t0 < seconds:
-        o.step(1, check_intersection=False)
+        st = o.step(1, check_intersection=False)[0]
+        newton.append(int(st["newton_iters"]))
+        if first is None:
+            first = o.positions()
         n += 1
-    return n, time.perf_counter() - t0
+    return n, time.perf_counter() - t0, newton, first
 
 
-def cpu_drape_sample(which: str, seconds: float):
-    """The oracle's f32 implicit step (implicit.rs:1951-2191 restated; one drape is one
-    thread, as in the reference) on the first steps of the workload's drapes, for at least
-    `seconds`: the six graded sizes of the batch run concurrently, one process each (as many
-    at a time as the host has cores). Returns (drape steps per second, sample description,
-    cores used)."""
-    if which != "batch":
-        n, dt = _oracle_drape_worker((which, 0, seconds))
-        return n / dt, f"oracle f32 implicit step, first {n} steps of the same drape ({dt:.1f} s)", 1
+def _pool_map(jobs, workers):
     import multiprocessing as mp
 
-    k = 6
+    with mp.get_context("spawn").Pool(max(1, workers)) as pool:
+        return pool.map(_oracle_window_worker, jobs)
+
+
+def cpu_drape_window(which: str, warmup: int, seconds: float, states=None):
+    """The oracle's f32 implicit step (implicit.rs:1951-2191 restated; one drape is one
+    thread, as in the reference) on the same drape steps the GPU arm times: each drape runs
+    `warmup` untimed steps (or starts from `states`, the GPU's state after its warm-up),
+    then steps warmup+1, ... for at least `seconds`. The six graded sizes of the batch run
+    concurrently, one process each. Returns (drape steps per second, sample description,
+    cores, Newton iterations per timed step, positions after the first timed step)."""
+    k = 6 if which == "batch" else 1
     workers = max(1, min(k, os.cpu_count() or 1))
+    jobs = [(which, i, "f32", 0 if states is not None else warmup, seconds,
+             None if states is None else states[i]) for i in range(k)]
     t0 = time.perf_counter()
-    with mp.get_context("spawn").Pool(workers) as pool:
-        res = pool.map(_oracle_drape_worker, [(which, i, seconds) for i in range(k)])
+    res = _pool_map(jobs, workers)
     wall = time.perf_counter() - t0
-    steps = sum(n for n, _ in res)
-    return steps / wall, (f"oracle f32 implicit step, the 6 graded sizes in {workers} concurrent processes, "
-                          f"first {min(n for n, _ in res)}-{max(n for n, _ in res)} steps each ({wall:.1f} s wall)"), workers
+    steps = sum(n for n, _, _, _ in res)
+    busy = max(dt for _, dt, _, _ in res)
+    newton = [nw for _, _, nw, _ in res]
+    start = "from the GPU's post-warm-up states" if states is not None else f"after {warmup} untimed oracle steps"
+    desc = (f"oracle f32 implicit step, {'the 6 graded sizes' if k == 6 else 'the drape'} in {workers} concurrent "
+            f"process{'es' if workers > 1 else ''}, steps {warmup + 1}..{warmup + max(n for n, _, _, _ in res)} "
+            f"{start} ({busy:.1f} s timed, {wall:.1f} s wall); Newton iterations per timed step "
+            f"{[x for nw in newton for x in nw]}")
+    # each process times its own steps; the drapes run concurrently, so the rate is the
+    # steps of all drapes over the longest timed span
+    return steps / busy, desc, workers, newton, [f for _, _, _, f in res]
 
 
 def count_launches(fn):
@@ -417,17 +444,30 @@ def e2e_steps(solver, p0, v0, k, dist):
     return dist.max(time.perf_counter() - t0) / k, nbytes, nbytes
 
 
-def fp64_error(sc, batch_positions, steps):
-    """Relative position error of `steps` GPU steps against the FP64 oracle run from the same
-    state: max |x_gpu - x_f64| over max |x_f64| (positions) and over max |x_f64 - x_0| (the
-    displacement)."""
-    import oracle_py as O
+def step_errors(x_start, x_test, x_ref):
+    """Relative position error of one step against a reference result from the same start:
+    max and RMS |x_test - x_ref| over max and RMS of the reference's step displacement, and
+    the max over max |x_ref| (the positions)."""
+    d = np.linalg.norm(x_test.astype(np.float64) - x_ref, axis=1)
+    disp = np.linalg.norm(x_ref - x_start.astype(np.float64), axis=1)
+    return {"max_rel_to_step_displacement": float(f"{d.max() / max(disp.max(), 1e-30):.3e}"),
+            "rms_rel_to_step_displacement": float(f"{np.sqrt((d ** 2).mean() / max((disp ** 2).mean(), 1e-60)):.3e}"),
+            "max_rel_to_positions": float(f"{d.max() / np.abs(x_ref).max():.3e}")}
 
-    o = O.OracleSolver(sc, "f64")
-    o.step(steps, check_intersection=False)
-    po = o.positions()
-    d = np.abs(batch_positions.astype(np.float64) - po).max()
-    return d / np.abs(po).max(), d / max(np.abs(po - sc["positions"]).max(), 1e-30)
+
+def traffic_from_profiles(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summaries: a line
+    `traffic_bytes_per_launch <kernel> = <bytes>` in profiles/*.md (None when absent)."""
+    import glob
+    import re
+
+    pat = re.compile(r"traffic_bytes_per_launch\s+(\S+)\s*=\s*([0-9.eE+]+)")
+    for f in sorted(glob.glob(os.path.join(REPO, "profiles", "*.md"))):
+        for line in open(f):
+            m = pat.search(line)
+            if m and m.group(1) == kernel:
+                return float(m.group(2)), os.path.basename(f)
+    return None, None
 
 
 def run_batch(args, dist: Dist):
@@ -445,13 +485,19 @@ def run_batch(args, dist: Dist):
     ntri = [int(sc["shell_faces"].shape[0]) for sc in scs]
     clocks = ClockSampler(dist.local)
     clocks.start()
-    # batched, mixed precision
+    # batched, mixed precision (FP16 Schwarz factor tiles): the headline
     b = mguso.ImplicitBatch(ctx, scs, "mixed")
     b.step(args.warmup)
     p_w, v_w = b.positions.copy(), b.velocities.copy()
     ms_b, st_b = time_steps(b, args.steps, stream, dist)
     clk = clocks.stop()
-    # plain FP32, each size alone, same steps from the same start
+    # batched, mixed precision with FP32 factor tiles (the apply in FP32 storage), same steps
+    scs32 = [dict(sc, params=dict(sc["params"], factor_storage=1)) for sc in scs]
+    b32 = mguso.ImplicitBatch(ctx, scs32, "mixed")
+    b32.step(args.warmup)
+    ms_b32, st_b32 = time_steps(b32, args.steps, stream, dist)
+    b32.close()
+    # plain FP32 (FP32 storage everywhere, FP32 factor tiles), each size alone, same steps
     ms_p = 0.0
     newton_p = []
     for sc in scs:
@@ -463,10 +509,16 @@ def run_batch(args, dist: Dist):
         g.close()
     inst_steps = len(scs) * args.steps
     value = inst_steps / (ms_b * 1e-3) * dist.world
+    value32 = inst_steps / (ms_b32 * 1e-3) * dist.world
     plain = inst_steps / (ms_p * 1e-3) * dist.world
+    # the fused PCG kernels timed inside a solve of the last Newton system (CUDA events per
+    # launch), and the other solver kernels timed alone
+    fused = b.profile_pcg(64)
     prof = b.profile(100)
-    dom = max(("spmv", "precond_apply"), key=lambda k: prof[k][0])
-    us, nbytes = prof[dom]
+    dom = max(fused, key=lambda k: fused[k][0])
+    us, nbytes = fused[dom]
+    kname = {"rows": "k_fr_rows<double>", "domains": "k_fr_schwarz<double, __half>"}[dom]
+    traffic, tsrc = traffic_from_profiles(kname)
     # end to end: the timed steps again from the same state, each step's state through host
     e2e_s, h2d, d2h = e2e_steps(b, p_w, v_w, args.steps, dist)
     nl = None if args.no_launch_count else count_launches(lambda: b.step(1))
@@ -477,7 +529,7 @@ def run_batch(args, dist: Dist):
     res = {
         "metric": METRIC,
         "value": round(value, 3),
-        "unit": "drape-steps/s (instance steps per second, 6 graded sizes batched, mixed precision)",
+        "unit": BATCH_UNIT,
         "n_gpus": dist.world,
         "steps": args.steps,
         "warmup": args.warmup,
@@ -485,45 +537,71 @@ def run_batch(args, dist: Dist):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32+f64(dots,norms,spmv/precond accumulation,barrier,ccd)",
+        "dtype": "f32 storage + f64 (dots, norms, SpMV/apply accumulation, barrier, CCD root); "
+                 "Schwarz factor tiles f16 scaled per domain",
         "data": "synthetic (seeded meshes; no dataset)",
         "config": {
             "workload": BATCH_WORKLOAD,
+            "unit_note": "instance steps per second: 6 graded sizes batched, mixed precision, steps "
+                         f"{args.warmup + 1}..{args.warmup + args.steps} of each drape",
             "triangles_per_size": ntri, "vertices_total": int(b.nv),
             "drapes_per_s": round(value / 120.0, 4),
+            "batched_mixed_fp32_tiles_drape_steps_per_s": round(value32, 3),
             "plain_fp32_per_size_drape_steps_per_s": round(plain, 3),
             "batched_mixed_over_plain_fp32": round(value / plain, 3),
+            "batched_mixed_fp32_tiles_over_plain_fp32": round(value32 / plain, 3),
             "newton_iters_mean_batched": round(float(np.mean(newton_b)), 2),
             "newton_iters_mean_plain": round(float(np.mean(newton_p)), 2),
+            "newton_iters_mean_batched_fp32_tiles": round(float(np.mean([s_["newton_iters"] for step in st_b32
+                                                                          for s_ in step])), 2),
+            "pcg_iters_max_batched": int(max(s_["max_cg_iters"] for step in st_b for s_ in step)),
             "l2": "working set L2-resident (latency-bound step); per-kernel GB/s reported, not graded",
             "parallelism": f"replicas x{dist.world}",
         },
         "roofline": {
             "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-            "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": f"{peak_kind} (burst copy)",
-            "kernel": {"spmv": "k_system_spmv", "precond_apply": "k_schwarz_apply"}[dom]
-            + " (batch system, timed alone at the last Newton system)",
+            "frac": round(achieved / peak, 4),
+            "traffic": None if traffic is None else int(traffic),
+            "traffic_source": tsrc, "peak_kind": f"{peak_kind} (burst copy)",
+            "kernel": kname + " (fused PCG, timed inside a solve of the last Newton system)",
             "us_per_launch": round(us, 2), "bytes_per_launch": int(nbytes),
-            "per_kernel": {k: {"us": round(v[0], 2), "bytes": int(v[1]),
-                               "GB/s": round(v[1] / (v[0] * 1e-6) / 1e9, 1)} for k, v in prof.items()},
+            "fused": {k: {"us": round(v[0], 2), "bytes": int(v[1]), "GB/s": round(v[1] / (v[0] * 1e-6) / 1e9, 1)}
+                      for k, v in fused.items()},
+            "per_kernel_alone": {k: {"us": round(v[0], 2), "bytes": int(v[1]),
+                                     "GB/s": round(v[1] / (v[0] * 1e-6) / 1e9, 1)} for k, v in prof.items()},
         },
-        "e2e": {"value": round(len(scs) / e2e_s * dist.world, 3), "unit": "drape-steps/s",
+        "e2e": {"value": round(len(scs) / e2e_s * dist.world, 3), "unit": BATCH_UNIT,
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": launches,
         "clocks": {k: clk[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
         "status": sorted(set(int(s_["status"]) for step in st_b for s_ in step)),
     }
     if dist.rank == 0 and not args.no_cpu_baseline:
-        # error of the batched mixed path against the FP64 oracle: XS instance, first step
+        # first timed step (warmup + 1) of every size from the GPU's post-warm-up state: the
+        # batch's result, the FP32 oracle's (timed: the CPU baseline) and the FP64 oracle's
         b1 = mguso.ImplicitBatch(ctx, scs, "mixed")
+        b1.positions, b1.velocities = p_w, v_w
         b1.step(1)
-        e_pos, e_disp = fp64_error(scs[0], b1.instance_positions(0), 1)
-        res["config"]["fp64_oracle_error_xs_step1"] = {"rel_to_positions": float(f"{e_pos:.3e}"),
-                                                      "rel_to_step_displacement": float(f"{e_disp:.3e}")}
+        x_gpu = b1.positions
         b1.close()
-        sps, sample, cores = cpu_drape_sample("batch", args.cpu_seconds)
-        res["cpu_baseline"] = {"value": round(sps, 4), "unit": "drape-steps/s", "cores": cores, "kind": "port",
+        off = b.offsets
+        states = [(p_w[off[i]:off[i + 1]], v_w[off[i]:off[i + 1]]) for i in range(len(scs))]
+        sps, sample, cores, newton_cpu, x32 = cpu_drape_window("batch", args.warmup, args.cpu_seconds, states)
+        res["cpu_baseline"] = {"value": round(sps, 4), "unit": BATCH_UNIT, "cores": cores, "kind": "port",
                                "sample": sample}
+        if not args.no_fp64_check:
+            jobs = [("batch", i, "f64", 0, 0.0, states[i]) for i in range(len(scs))]
+            r64 = _pool_map(jobs, min(len(scs), os.cpu_count() or 1))
+            table = []
+            for i in range(len(scs)):
+                x64 = r64[i][3]
+                xs = p_w[off[i]:off[i + 1]]
+                table.append({"size": i, "step": args.warmup + 1,
+                              "batch_mixed_vs_fp64": step_errors(xs, x_gpu[off[i]:off[i + 1]], x64),
+                              "oracle_fp32_vs_fp64": step_errors(xs, x32[i], x64),
+                              "newton_batch_fp64_fp32": [int(st_b[0][i]["newton_iters"]), r64[i][2][0],
+                                                         newton_cpu[i][0]]})
+            res["config"]["fp64_oracle_error_first_timed_step"] = table
     b.close()
     ctx.close()
     return res
@@ -606,7 +684,7 @@ def run_drape(args, dist: Dist):
         "status": sorted(set(int(s_["status"]) for s_ in stats)),
     }
     if dist.rank == 0 and not args.no_cpu_baseline:
-        sps, sample, cores = cpu_drape_sample(args.workload, args.cpu_seconds)
+        sps, sample, cores, _, _ = cpu_drape_window(args.workload, args.warmup, args.cpu_seconds, [(p_w, v_w)])
         res["cpu_baseline"] = {"value": round(sps, 4), "unit": "steps/s", "cores": cores, "kind": "port",
                                "sample": sample}
     solver.close()
@@ -627,9 +705,9 @@ def run_reference(args, dist: Dist):
             "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": 1, "kind": "port", "sample": sample},
             "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }
-    sps, sample, cores = cpu_drape_sample(args.workload, max(5.0, min(args.cpu_seconds, 30.0)))
+    sps, sample, cores, _, _ = cpu_drape_window(args.workload, args.warmup, max(1.0, min(args.cpu_seconds, 30.0)))
     _, desc = drape_scene(args.workload)
-    unit = "drape-steps/s" if args.workload == "batch" else "steps/s"
+    unit = BATCH_UNIT if args.workload == "batch" else "steps/s"
     return {
         "impl": "reference", "metric": METRIC, "value": round(sps, 4), "unit": unit, "n_gpus": dist.world,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
@@ -649,6 +727,7 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-check", action="store_true", help="skip the FP64-oracle error of the first timed step")
     ap.add_argument("--no-launch-count", action="store_true", help="skip the traced launch count (under ncu)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -177,7 +177,9 @@ int mguso_radix_sort_pairs(mguso_ctx* ctx, void* keys, uint32_t* vals, uint32_t 
  * pairs; larger n returns MGUSO_ERR_INVALID_ARG. Sorts the same (key, payload) pairs in
  * place on the current device, stably, with the same result as mguso_radix_sort_pairs, and
  * returns when the sort has finished on `stream`. The first call on each device looks up
- * the array's device address once; make that first call before any stream capture. All
+ * the array's device address once; make that first call before any stream capture. That
+ * address is kept for the life of the process: after cudaDeviceReset on a device it is
+ * stale, so a process that resets a device must not call this function on it again. All
  * calls share the one array, so calls that overlap on the GPU (other streams, other host
  * threads) race and must be serialised by the caller. */
 int mguso_radix_sort_pairs_noalloc(void* keys, uint32_t* vals, uint32_t n, int key_bits, void* stream);
@@ -221,6 +223,13 @@ typedef struct {
                               1: one launch per PCG kernel, replayed as CUDA graphs (single
                                  scenes only);
                               2: one cooperative persistent launch per linear solve */
+  int factor_storage;      /* Schwarz factor tiles: 0 = by precision (FP32 tiles with
+                              MGUSO_PRECISION_FP32, FP16 tiles scaled per domain with MIXED),
+                              1 = FP32 tiles, 2 = FP16 tiles */
+  uint32_t schwarz_levels; /* 1 (or 0): one-level Schwarz (SchwarzCpu, linsolve.rs:463-520);
+                              2: two-level Galerkin Schwarz (SchwarzMlCpu, linsolve.rs:534-836) */
+  float schwarz_weight;    /* coarse-correction weight w of the two-level form
+                              z = S0 r + w C1^T S1 (C1 r) (the CLI default 0.7, main.rs:761-763) */
 } mguso_params;
 
 /* One scene (Scene::build_implicit + the set_* calls of implicit.rs). All pointers host;
@@ -351,6 +360,14 @@ int mguso_scene_spmv_time(mguso_scene* s, int reps, float* us, double* bytes);
  * vector update}; bytes4 = their algorithmic bytes per launch (each stored block or factor
  * entry and each vector read or written once). Clobbers the PCG scratch (not the state). */
 int mguso_scene_profile(mguso_scene* s, int reps, float* us4, double* bytes4);
+
+/* Mean device time in microseconds of the two fused PCG kernels (pcg_mode 0 and batches)
+ * inside a solve of the last assembled system: `iters` iterations of every instance at
+ * tolerance 0, each launch bracketed by its own CUDA events on the scene's stream, so the
+ * kernels see the cache state of a real solve. us2 = {rows kernel (direction update, system
+ * SpMV, p.Ap), domain kernel (x/r update, preconditioner apply, r.r and r.z)}; bytes2 =
+ * their algorithmic bytes per launch. Clobbers the PCG scratch (not the state). */
+int mguso_scene_profile_pcg(mguso_scene* s, int iters, float* us2, double* bytes2);
 
 /* Assemble the Newton system once at positions x (f32[3 nv]) with inertia target x_tilde
    (f32[3 nv]; NULL means x), exactly as one Newton iteration of mguso_step does: contact

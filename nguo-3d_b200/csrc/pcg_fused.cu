@@ -370,14 +370,13 @@ Launch fused_kernels(const Scene& s) {
 }
 }  // namespace
 
-// Solves the scene's current system (work.b) into work.x; instance k covers block rows
-// [h_inst_row[k], h_inst_row[k+1]); instances outside `active` keep x = 0. out[k] gets each
-// instance's result. Schwarz domains must be grouped by instance.
-int pcg_fused(Scene& s, const uint32_t* h_inst_row, uint32_t K, uint32_t active, PcgInstResult* out) {
+// Layout of the fused kernels over the scene's instances and the arguments of both; resets
+// the per-instance state (instances outside `active` start done) on the scene's stream.
+static int fused_prepare(Scene& s, const uint32_t* h_inst_row, uint32_t K, uint32_t active, FusedArgs& a, Launch& L) {
   MG_CHECK_ARG(K >= 1 && K <= PCG_MAX_INST, "fused PCG: 1..8 instances");
   cudaStream_t st = s.st;
   PcgWork& w = s.work;
-  Launch L = fused_kernels(s);
+  L = fused_kernels(s);
   // layout: rows, row-kernel CTAs, domain-kernel CTAs, domains (per instance)
   std::vector<uint32_t> key(h_inst_row, h_inst_row + K + 1);
   if (key != s.fr_key) {
@@ -418,9 +417,10 @@ int pcg_fused(Scene& s, const uint32_t* h_inst_row, uint32_t K, uint32_t active,
   for (uint32_t k = 0; k < K; ++k) hi[k].done = ((active >> k) & 1u) ? 0u : 1u;
   FusedCtl hc{};
   MG_CUDA(cudaMemcpyAsync(s.fr_inst.p, hi, sizeof(FusedInst) * K, cudaMemcpyHostToDevice, st));
+  // pageable sources: the copies are staged before cudaMemcpyAsync returns
   MG_CUDA(cudaMemcpyAsync(s.fr_ctl.p, &hc, sizeof(FusedCtl), cudaMemcpyHostToDevice, st));
 
-  FusedArgs a{};
+  a = FusedArgs{};
   a.ninst = K;
   a.lay = s.fr_lay.p;
   a.rp = s.Ps.row_ptr.p;
@@ -448,22 +448,35 @@ int pcg_fused(Scene& s, const uint32_t* h_inst_row, uint32_t K, uint32_t active,
   a.inst = s.fr_inst.p;
   a.ctl = s.fr_ctl.p;
   a.part = s.fr_part.p;
-  float* p0 = w.p.p;
-  float* p1 = w.p2.p;
-  auto launch_dom = [&](const float* pc, float* pinit, int init) -> int {
-    void* args[] = {(void*)&a, (void*)&pc, (void*)&pinit, (void*)&init};
-    MG_CUDA(cudaLaunchKernel(L.dom, dim3(L.grid_dom), dim3(s.schwarz ? 32 * FD_WARPS : FD_THREADS), args,
-                             L.dom_smem, st));
-    return MGUSO_OK;
-  };
-  auto launch_rows = [&](const float* po, float* pn) -> int {
-    void* args[] = {(void*)&a, (void*)&po, (void*)&pn};
-    MG_CUDA(cudaLaunchKernel(L.rows, dim3(L.grid_rows), dim3(FR_THREADS), args, 0, st));
-    return MGUSO_OK;
-  };
   if (L.dom_smem) MG_CUDA(cudaFuncSetAttribute(L.dom, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.dom_smem));
+  return MGUSO_OK;
+}
+
+static int launch_dom(const Scene& s, const Launch& L, FusedArgs& a, const float* pc, float* pinit, int init) {
+  void* args[] = {(void*)&a, (void*)&pc, (void*)&pinit, (void*)&init};
+  MG_CUDA(cudaLaunchKernel(L.dom, dim3(L.grid_dom), dim3(s.schwarz ? 32 * FD_WARPS : FD_THREADS), args, L.dom_smem,
+                           s.st));
+  return MGUSO_OK;
+}
+
+static int launch_rows(const Scene& s, const Launch& L, FusedArgs& a, const float* po, float* pn) {
+  void* args[] = {(void*)&a, (void*)&po, (void*)&pn};
+  MG_CUDA(cudaLaunchKernel(L.rows, dim3(L.grid_rows), dim3(FR_THREADS), args, 0, s.st));
+  return MGUSO_OK;
+}
+
+// Solves the scene's current system (work.b) into work.x; instance k covers block rows
+// [h_inst_row[k], h_inst_row[k+1]); instances outside `active` keep x = 0. out[k] gets each
+// instance's result. Schwarz domains must be grouped by instance.
+int pcg_fused(Scene& s, const uint32_t* h_inst_row, uint32_t K, uint32_t active, PcgInstResult* out) {
+  cudaStream_t st = s.st;
+  FusedArgs a;
+  Launch L;
+  MG_TRY(fused_prepare(s, h_inst_row, K, active, a, L));
+  float* p0 = s.work.p.p;
+  float* p1 = s.work.p2.p;
   // x = 0, r = b, p0 = 0, z = M^-1 r, norms
-  MG_TRY(launch_dom(p0, p0, 1));
+  MG_TRY(launch_dom(s, L, a, p0, p0, 1));
   // one graph of FUSED_CHECK iterations (p alternates between the two buffers)
   std::vector<unsigned char> gk(sizeof(FusedArgs) + 2 * sizeof(void*) + 2 * sizeof(uint32_t));
   std::memcpy(gk.data(), &a, sizeof(FusedArgs));
@@ -480,8 +493,8 @@ int pcg_fused(Scene& s, const uint32_t* h_inst_row, uint32_t K, uint32_t active,
     for (uint32_t i = 0; i < FUSED_CHECK && rc == MGUSO_OK; ++i) {
       const float* po = (i & 1) ? p1 : p0;
       float* pn = (i & 1) ? p0 : p1;
-      rc = launch_rows(po, pn);
-      if (rc == MGUSO_OK) rc = launch_dom(pn, pn, 0);
+      rc = launch_rows(s, L, a, po, pn);
+      if (rc == MGUSO_OK) rc = launch_dom(s, L, a, pn, pn, 0);
     }
     cudaError_t e = cudaStreamEndCapture(st, &g);
     if (rc != MGUSO_OK) {
@@ -501,6 +514,7 @@ int pcg_fused(Scene& s, const uint32_t* h_inst_row, uint32_t K, uint32_t active,
     MG_CUDA(cudaStreamSynchronize(st));
     if (h.all_done) break;
   }
+  FusedInst hi[PCG_MAX_INST] = {};
   MG_CUDA(cudaMemcpyAsync(hi, s.fr_inst.p, sizeof(FusedInst) * K, cudaMemcpyDeviceToHost, st));
   MG_CUDA(cudaStreamSynchronize(st));
   for (uint32_t k = 0; k < K; ++k) {
@@ -513,6 +527,60 @@ int pcg_fused(Scene& s, const uint32_t* h_inst_row, uint32_t K, uint32_t active,
       return MGUSO_ERR_TIMEOUT;
     }
   }
+  return MGUSO_OK;
+}
+
+// Device time of the two fused kernels inside a PCG solve of the scene's current system:
+// `iters` iterations of every instance (tolerance 0, so none stops early unless it breaks
+// down), each kernel launch bracketed by its own CUDA events on the scene's stream, in the
+// order and with the cache state of the solve. us2 = mean microseconds per launch of
+// {rows kernel, domain kernel}; the solution left in work.x is not the system's.
+int pcg_fused_profile(Scene& s, uint32_t iters, float* us2) {
+  MG_CHECK_ARG(iters >= 1 && iters <= 4096, "profile: 1..4096 iterations");
+  const uint32_t K = s.ninst;
+  const uint32_t all = (K >= 32) ? ~0u : ((1u << K) - 1u);
+  const float tol = s.p.cg_tol;
+  const uint32_t mx = s.p.cg_max_iter;
+  s.p.cg_tol = 0.f;
+  s.p.cg_max_iter = iters + 1;
+  FusedArgs a;
+  Launch L;
+  int rc = fused_prepare(s, s.inst_vert.data(), K, all, a, L);
+  s.p.cg_tol = tol;
+  s.p.cg_max_iter = mx;
+  MG_TRY(rc);
+  std::vector<cudaEvent_t> ev(4 * iters, nullptr);
+  for (auto& e : ev)
+    if (cudaEventCreate(&e) != cudaSuccess) rc = MGUSO_ERR_CUDA;
+  float* p0 = s.work.p.p;
+  float* p1 = s.work.p2.p;
+  if (rc == MGUSO_OK) rc = launch_dom(s, L, a, p0, p0, 1);
+  for (uint32_t i = 0; i < iters && rc == MGUSO_OK; ++i) {
+    const float* po = (i & 1) ? p1 : p0;
+    float* pn = (i & 1) ? p0 : p1;
+    if (cudaEventRecord(ev[4 * i], s.st) != cudaSuccess) rc = MGUSO_ERR_CUDA;
+    if (rc == MGUSO_OK) rc = launch_rows(s, L, a, po, pn);
+    if (rc == MGUSO_OK && cudaEventRecord(ev[4 * i + 1], s.st) != cudaSuccess) rc = MGUSO_ERR_CUDA;
+    if (rc == MGUSO_OK && cudaEventRecord(ev[4 * i + 2], s.st) != cudaSuccess) rc = MGUSO_ERR_CUDA;
+    if (rc == MGUSO_OK) rc = launch_dom(s, L, a, pn, pn, 0);
+    if (rc == MGUSO_OK && cudaEventRecord(ev[4 * i + 3], s.st) != cudaSuccess) rc = MGUSO_ERR_CUDA;
+  }
+  if (rc == MGUSO_OK && cudaStreamSynchronize(s.st) != cudaSuccess) rc = MGUSO_ERR_CUDA;
+  double t_rows = 0, t_dom = 0;
+  for (uint32_t i = 0; i < iters && rc == MGUSO_OK; ++i) {
+    float m0 = 0, m1 = 0;
+    if (cudaEventElapsedTime(&m0, ev[4 * i], ev[4 * i + 1]) != cudaSuccess ||
+        cudaEventElapsedTime(&m1, ev[4 * i + 2], ev[4 * i + 3]) != cudaSuccess)
+      rc = MGUSO_ERR_CUDA;
+    t_rows += m0;
+    t_dom += m1;
+  }
+  for (auto& e : ev)
+    if (e) cudaEventDestroy(e);
+  if (rc == MGUSO_ERR_CUDA) set_error("fused PCG profile: a CUDA event call failed");
+  MG_TRY(rc);
+  us2[0] = (float)(1000.0 * t_rows / iters);
+  us2[1] = (float)(1000.0 * t_dom / iters);
   return MGUSO_OK;
 }
 

@@ -110,6 +110,10 @@ static int validate_desc(const mguso_scene_desc* d) {
   MG_CHECK_ARG(d->params.precond == MGUSO_PRECOND_BLOCK_JACOBI || d->params.precond == MGUSO_PRECOND_SCHWARZ,
                "scene: unknown preconditioner");
   MG_CHECK_ARG(d->params.pcg_mode >= 0 && d->params.pcg_mode <= 2, "scene: pcg_mode must be 0, 1 or 2");
+  MG_CHECK_ARG(d->params.factor_storage >= 0 && d->params.factor_storage <= 2, "scene: factor_storage must be 0, 1 or 2");
+  MG_CHECK_ARG(d->params.schwarz_levels <= 2, "scene: schwarz_levels must be 1 or 2");
+  MG_CHECK_ARG(std::isfinite(d->params.schwarz_weight) && d->params.schwarz_weight >= 0.f,
+               "scene: schwarz_weight must be finite and >= 0");
   return MGUSO_OK;
 }
 
@@ -120,6 +124,10 @@ int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>
   s.nv = nv;
   s.nt = nt;
   s.mixed = d->params.precision == MGUSO_PRECISION_MIXED;
+  // Schwarz factor storage: FP32 tiles for plain FP32 (and whenever asked), FP16 tiles
+  // scaled per domain for mixed precision unless the caller (or the adjoint) chose FP32
+  if (d->params.factor_storage == 1 || (d->params.factor_storage == 0 && !s.mixed)) s.fp16_factor = false;
+  if (d->params.factor_storage == 2) s.fp16_factor = true;
   s.st = s.ctx->stream;
   cudaStream_t st = s.st;
   const float* P = d->positions;
@@ -955,3 +963,34 @@ extern "C" int mguso_scene_profile(mguso_scene* sc, int reps, float* us4, double
   cudaEventDestroy(e1);
   return rc;
 }
+
+// Device time of the two fused PCG kernels inside a solve of the last assembled system
+// (pcg_fused_profile: `iters` iterations, every launch bracketed by its own events), with
+// their algorithmic bytes per launch: rows = every block and column index of Ps and C once,
+// both row-pointer arrays, z and the old direction read, the new direction and Ap written;
+// domains = the factor's packed lower triangle at its stored width (FP16 plus a scale per
+// domain, or FP32), x and r read and written, the direction and Ap read, z written, the
+// domain vertex lists and offsets (block Jacobi: the 3x3 inverses instead of the factor).
+extern "C" int mguso_scene_profile_pcg(mguso_scene* sc, int iters, float* us2, double* bytes2) {
+  MG_CHECK_ARG(sc && us2 && bytes2 && iters > 0, "bad argument");
+  Scene& s = sc->s;
+  uint32_t nc = 0;
+  MG_CUDA(cudaMemcpyAsync(&nc, s.c_count.p, 4, cudaMemcpyDeviceToHost, s.st));
+  MG_CUDA(cudaStreamSynchronize(s.st));
+  const double nv = s.nv;
+  bytes2[0] = 40.0 * ((double)s.Ps.nnz + nc) + 8.0 * (nv + 1) + 48.0 * nv;
+  if (s.schwarz) {
+    mguso_schwarz* sw = s.schwarz.get();
+    double packed = 0;
+    for (uint32_t d = 0; d < sw->ndom; ++d) {
+      const double m = 3.0 * (sw->h_dom_start[d + 1] - sw->h_dom_start[d]);
+      packed += m * (m + 1) / 2;
+    }
+    const double fe = sw->half ? 2.0 : 4.0, fs = sw->half ? 4.0 * sw->ndom : 0.0;
+    bytes2[1] = fe * packed + fs + 88.0 * nv + 12.0 * sw->ndom;
+  } else {
+    bytes2[1] = 36.0 * nv + 84.0 * nv;
+  }
+  return pcg_fused_profile(s, (uint32_t)iters, us2);
+}
+

@@ -195,6 +195,7 @@ int system_spmv(Scene& s, const float* p, float* ap, cudaStream_t st, const DotS
 int build_bvhs(Scene& s, const float* x);
 int pcg_persistent(Scene& s, const uint32_t* h_inst_row, uint32_t ninst, uint32_t active, PcgInstResult* out);
 int pcg_fused(Scene& s, const uint32_t* h_inst_row, uint32_t ninst, uint32_t active, PcgInstResult* out);
+int pcg_fused_profile(Scene& s, uint32_t iters, float* us2);
 int collect_stencils(Scene& s, uint32_t* nst);
 int ccd_step(Scene& s, uint32_t active, float* t_out, uint32_t* cap_hits);
 

@@ -485,25 +485,45 @@ def parse_obj(text: str, with_uvs: bool = False):
     when every face corner names one (parallel or empty), a missing ``vt`` v reads as 0."""
     v, vt, fcs, fuv = [], [], [], []
     all_uv = True
-    for line in text.splitlines():
-        s = line.split()
+
+    def num(tok, what, lineno):
+        try:
+            return float(tok)
+        except ValueError:
+            raise CaptureError(f"bad {what} on line {lineno}") from None
+
+    def index(tok, what, lineno):
+        try:
+            return int(tok)
+        except ValueError:
+            raise CaptureError(f"bad {what} index {tok!r} on line {lineno}") from None
+
+    for lineno, line in enumerate(text.splitlines(), 1):
+        # '#' starts a comment anywhere on the line (obj.rs:103-107)
+        s = line.split("#", 1)[0].split()
         if not s:
             continue
         if s[0] == "v":
-            v.append([float(x) for x in s[1:4]])
+            if len(s) < 4:
+                raise CaptureError(f"vertex needs 3 coords on line {lineno}")
+            v.append([num(x, "vertex", lineno) for x in s[1:4]])
         elif s[0] == "vt":
-            vt.append([float(s[1]), float(s[2]) if len(s) > 2 else 0.0])
+            if len(s) < 2:
+                raise CaptureError(f"vt needs >=1 coord on line {lineno}")
+            vt.append([num(s[1], "texcoord", lineno), num(s[2], "texcoord", lineno) if len(s) > 2 else 0.0])
         elif s[0] == "f":
+            if len(s) < 4:
+                raise CaptureError(f"face needs >=3 verts on line {lineno}")
             ids, uvs = [], []
             for tok in s[1:]:
                 parts = tok.split("/")
-                i = int(parts[0])
+                i = index(parts[0], "vertex", lineno)
                 i = i - 1 if i > 0 else len(v) + i
                 if not 0 <= i < len(v):
                     raise CaptureError(f"face index {parts[0]} is outside the {len(v)} vertices")
                 ids.append(i)
                 if len(parts) > 1 and parts[1]:
-                    j = int(parts[1])
+                    j = index(parts[1], "texture", lineno)
                     j = j - 1 if j > 0 else len(vt) + j
                     if not 0 <= j < len(vt):
                         raise CaptureError(f"texture index {parts[1]} is outside the {len(vt)} uvs")
@@ -514,6 +534,8 @@ def parse_obj(text: str, with_uvs: bool = False):
                 fcs.append([ids[0], ids[k], ids[k + 1]])
                 if len(uvs) == len(ids):
                     fuv.append([uvs[0], uvs[k], uvs[k + 1]])
+    if not v:
+        raise CaptureError("OBJ contained no vertices")
     pos = np.asarray(v, np.float32).reshape(-1, 3)
     tris = np.asarray(fcs, np.uint32).reshape(-1, 3)
     if not with_uvs:

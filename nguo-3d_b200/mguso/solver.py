@@ -23,7 +23,8 @@ _PARAM_FIELDS = [("dt", C.c_float), ("gravity", C.c_float * 3), ("newton_iters",
                  ("contact_rayleigh", C.c_int), ("self_collision", C.c_int), ("cg_tol", C.c_float),
                  ("cg_max_iter", C.c_uint32), ("floor_y", C.c_float), ("newton_tol", C.c_float),
                  ("precond", C.c_int), ("schwarz_domain", C.c_uint32), ("precision", C.c_int),
-                 ("pcg_mode", C.c_int)]
+                 ("pcg_mode", C.c_int), ("factor_storage", C.c_int), ("schwarz_levels", C.c_uint32),
+                 ("schwarz_weight", C.c_float)]
 
 
 class Params(C.Structure):
@@ -62,6 +63,7 @@ def _sigs(lib):
         ("mguso_scene_assemble", i32, [vp, vp, vp, vp]),
         ("mguso_scene_ccd", i32, [vp, vp, vp, vp, vp]),
         ("mguso_scene_profile", i32, [vp, i32, vp, vp]),
+        ("mguso_scene_profile_pcg", i32, [vp, i32, vp, vp]),
         ("mguso_batch_create", i32, [vp, vp, C.c_uint32, P(vp)]),
         ("mguso_scene_instances", i32, [vp, P(C.c_uint32), vp]),
         ("mguso_scene_system", i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
@@ -211,6 +213,15 @@ class ImplicitSolver:
         check(self.lib.mguso_scene_profile(self.h, reps, ptr(us), ptr(by)))
         names = ["spmv", "precond_apply", "precond_factor", "pcg_update"]
         return {k: (float(u), float(b)) for k, u, b in zip(names, us, by)}
+
+    def profile_pcg(self, iters: int = 64) -> dict:
+        """Device time (us per launch, CUDA events around each launch) and algorithmic bytes
+        of the two fused PCG kernels inside a solve of the last assembled system:
+        {"rows": (us, bytes), "domains": (us, bytes)}."""
+        us = np.zeros(2, np.float32)
+        by = np.zeros(2, np.float64)
+        check(self.lib.mguso_scene_profile_pcg(self.h, iters, ptr(us), ptr(by)))
+        return {"rows": (float(us[0]), float(by[0])), "domains": (float(us[1]), float(by[1]))}
 
     def ccd(self, x, dx):
         """Step fraction the CCD filter allows along ``dx`` from ``x`` (one per instance) and

@@ -261,7 +261,7 @@ inline std::vector<R> csr_diagonal(const CsrT<R>& a) {
 // ---------------------------------------------------------------------------------------
 // linsolve.rs
 // ---------------------------------------------------------------------------------------
-enum class Precond { Diagonal = 0, Block = 1, Schwarz = 2 };
+enum class Precond { Diagonal = 0, Block = 1, Schwarz = 2, SchwarzMl = 3 };
 
 struct LinearStats {
   uint32_t iters = 0;
@@ -433,6 +433,93 @@ struct SchwarzTopology {
   }
 };
 
+// Two-level Galerkin additive Schwarz (MultilevelSchwarz, linsolve.rs:534-655):
+//   z = S0 r + w C1^T S1 (C1 r)
+// S0: the one-level domain solves; C1: restriction of a fine vertex to its level-0 domain
+// (one coarse node per domain, three dofs), by summation; A1 = C1 A0 C1^T, the Galerkin
+// coarse operator, aggregated in fine value order in the matrix's own precision
+// (coarse_matrix, linsolve.rs:618-630); S1: a one-level Schwarz over A1 with the same domain
+// size (its coarse domains are BFS groups of coarse nodes).
+struct MultilevelSchwarz {
+  SchwarzTopology l0;
+  std::vector<uint32_t> agg0;  // fine vertex -> coarse node (its level-0 domain)
+  size_t n_coarse = 0;
+  CsrT<float> coarse_structure;        // values unused (structure only)
+  std::vector<size_t> coarse_gather;   // fine value index -> coarse value index
+  SchwarzTopology l1;
+  double weight = 1.0;
+
+  // build (linsolve.rs:555-608)
+  template <class R>
+  static MultilevelSchwarz build(const CsrT<R>& a, size_t domain, double weight) {
+    MultilevelSchwarz ml;
+    ml.l0 = SchwarzTopology::build(a, domain);
+    const size_t nv = a.n / 3;
+    ml.agg0.assign(nv, 0);
+    for (size_t d = 0; d < ml.l0.domains.size(); ++d)
+      for (uint32_t v : ml.l0.domains[d]) ml.agg0[v] = (uint32_t)d;
+    ml.n_coarse = ml.l0.domains.size();
+    auto coarse_dof = [&](size_t row) -> uint32_t { return (uint32_t)(3 * (size_t)ml.agg0[row / 3] + row % 3); };
+    std::vector<TripletT<float>> trips;
+    trips.reserve(a.nnz());
+    for (size_t row = 0; row < a.n; ++row) {
+      const uint32_t cr = coarse_dof(row);
+      for (size_t k = a.row_ptr[row]; k < a.row_ptr[row + 1]; ++k)
+        trips.push_back({cr, coarse_dof(a.col_idx[k]), 0.0f});
+    }
+    ml.coarse_structure = csr_from_triplets(3 * ml.n_coarse, trips.data(), trips.size());
+    // (coarse row, coarse col) -> flat index: columns are sorted and unique per row
+    const CsrT<float>& cs = ml.coarse_structure;
+    ml.coarse_gather.assign(a.nnz(), 0);
+    for (size_t row = 0; row < a.n; ++row) {
+      const uint32_t cr = coarse_dof(row);
+      const uint32_t* b = cs.col_idx.data() + cs.row_ptr[cr];
+      const uint32_t* e = cs.col_idx.data() + cs.row_ptr[cr + 1];
+      for (size_t k = a.row_ptr[row]; k < a.row_ptr[row + 1]; ++k) {
+        const uint32_t cc = coarse_dof(a.col_idx[k]);
+        ml.coarse_gather[k] = (size_t)(std::lower_bound(b, e, cc) - cs.col_idx.data());
+      }
+    }
+    ml.l1 = SchwarzTopology::build(ml.coarse_structure, domain);
+    ml.weight = weight;
+    return ml;
+  }
+
+  // coarse_matrix (linsolve.rs:618-630): values summed in fine value order
+  template <class R>
+  CsrT<R> coarse_matrix(const CsrT<R>& a) const {
+    CsrT<R> c;
+    c.n = coarse_structure.n;
+    c.row_ptr = coarse_structure.row_ptr;
+    c.col_idx = coarse_structure.col_idx;
+    c.values.assign(coarse_structure.nnz(), R(0));
+    for (size_t k = 0; k < coarse_gather.size(); ++k) c.values[coarse_gather[k]] += a.values[k];
+    return c;
+  }
+
+  // apply (linsolve.rs:641-666): level 0, restriction by sums in vertex order, coarse
+  // smoother, weighted prolongation added to z
+  void apply(const std::vector<std::vector<double>>& f0, const std::vector<std::vector<double>>& f1, const double* r,
+             double* z) const {
+    l0.apply(f0, r, z);
+    const size_t nv = agg0.size();
+    std::vector<double> rc(3 * n_coarse, 0.0), ec(3 * n_coarse, 0.0);
+    for (size_t i = 0; i < nv; ++i) {
+      const size_t g = agg0[i];
+      rc[3 * g] += r[3 * i];
+      rc[3 * g + 1] += r[3 * i + 1];
+      rc[3 * g + 2] += r[3 * i + 2];
+    }
+    l1.apply(f1, rc.data(), ec.data());
+    for (size_t i = 0; i < nv; ++i) {
+      const size_t g = agg0[i];
+      z[3 * i] += weight * ec[3 * g];
+      z[3 * i + 1] += weight * ec[3 * g + 1];
+      z[3 * i + 2] += weight * ec[3 * g + 2];
+    }
+  }
+};
+
 // cg_run (linsolve.rs:350-411): f64 PCG, x0 = 0, relative residual stop, pAp <= 0 break.
 template <class R, class PrecondFn>
 inline LinearStats cg_run(const CsrT<R>& a, const R* b, R tol, uint32_t max_iter, PrecondFn precond,
@@ -553,15 +640,37 @@ inline double relative_residual(const CsrT<R>& a, const R* x, const R* b) {
   return std::sqrt(num) / std::max(std::sqrt(den), 1e-30);
 }
 
+// SchwarzMlCpu::solve (linsolve.rs:803-836): two-level Schwarz CG, stats from cg_run.
+template <class R>
+inline LinearStats cg_schwarz_ml(const CsrT<R>& a, const R* b, R tol, uint32_t max_iter, size_t domain,
+                                 double weight, R* x_out) {
+  MultilevelSchwarz ml = MultilevelSchwarz::build(a, std::max<size_t>(domain, 1), weight);
+  CsrT<R> coarse = ml.coarse_matrix(a);
+  auto f0 = ml.l0.factorize(a);
+  auto f1 = ml.l1.factorize(coarse);
+  auto precond = [&](const std::vector<double>& r, std::vector<double>& z) { ml.apply(f0, f1, r.data(), z.data()); };
+  return cg_run(a, b, tol, max_iter, precond, x_out);
+}
+
 // A LinearSolver in the reference's sense (linsolve.rs:21-28): CgCpu (block Jacobi,
-// stats residual recomputed by relative_residual) or SchwarzCpu(domain).
+// stats residual recomputed by relative_residual), SchwarzCpu(domain) or
+// SchwarzMlCpu(domain, weight).
 struct LinearSolver {
   Precond kind = Precond::Block;
   size_t domain = 32;
+  double weight = 0.7;
   LinearStats last;
   template <class R>
   void solve(const CsrT<R>& a, const R* b, R tol, uint32_t max_iter, R* x) {
-    if (kind == Precond::Schwarz && a.n % 3 == 0) {
+    if (kind == Precond::SchwarzMl && a.n % 3 == 0) {
+      last = cg_schwarz_ml(a, b, tol, max_iter, domain, weight, x);
+    } else if (kind == Precond::SchwarzMl) {
+      // SchwarzMlCpu on a non-3-block system: plain CG (solve_cg_cpu), iterations 0
+      LinearStats s = cg_precond(a, b, tol, max_iter, Precond::Diagonal, domain, x);
+      (void)s;
+      last.iters = 0;
+      last.residual = relative_residual(a, x, b);
+    } else if (kind == Precond::Schwarz && a.n % 3 == 0) {
       last = cg_precond(a, b, tol, max_iter, Precond::Schwarz, domain, x);
     } else {
       Precond k = (a.n % 3 == 0) ? Precond::Block : Precond::Diagonal;

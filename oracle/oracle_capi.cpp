@@ -104,6 +104,53 @@ void oracle_schwarz_apply(uint32_t n, const uint32_t* rp, const uint32_t* ci, co
   t.apply(f, r, z);
 }
 
+// The reference's SchwarzMlCpu(domain, weight) LinearSolver (two-level Schwarz CG).
+int oracle_linear_solve_ml(uint32_t n, const uint32_t* rp, const uint32_t* ci, const float* v, const float* b,
+                           float tol, uint32_t max_iter, uint32_t domain, double weight, float* x, uint32_t* iters,
+                           double* residual) {
+  Csr a = view_csr(n, rp, ci, v);
+  LinearSolver s;
+  s.kind = Precond::SchwarzMl;
+  s.domain = domain;
+  s.weight = weight;
+  s.solve(a, b, tol, max_iter, x);
+  *iters = s.last.iters;
+  *residual = s.last.residual;
+  return 0;
+}
+
+// z = M^-1 r for the two-level Schwarz preconditioner (SchwarzGpuBuilder::apply_cpu's
+// arithmetic, linsolve.rs:767-775, in f64 throughout).
+void oracle_schwarz_ml_apply(uint32_t n, const uint32_t* rp, const uint32_t* ci, const float* v, uint32_t domain,
+                             double weight, const double* r, double* z) {
+  Csr a = view_csr(n, rp, ci, v);
+  MultilevelSchwarz ml = MultilevelSchwarz::build(a, domain, weight);
+  Csr coarse = ml.coarse_matrix(a);
+  auto f0 = ml.l0.factorize(a);
+  auto f1 = ml.l1.factorize(coarse);
+  ml.apply(f0, f1, r, z);
+}
+
+// The two-level plan: coarse node of every fine vertex (agg0), coarse domain of every
+// coarse node, and the Galerkin coarse operator (scalar CSR, values aggregated in f32).
+// Returns the coarse node count; coarse arrays are written only when the pointers are set
+// and hold nnz entries (*nnz is set first).
+uint32_t oracle_schwarz_ml_plan(uint32_t n, const uint32_t* rp, const uint32_t* ci, const float* v, uint32_t domain,
+                                uint32_t* agg0, uint32_t* coarse_dom, uint64_t* nnz, uint32_t* c_rp, uint32_t* c_ci,
+                                float* c_v) {
+  Csr a = view_csr(n, rp, ci, v);
+  MultilevelSchwarz ml = MultilevelSchwarz::build(a, domain, 1.0);
+  std::memcpy(agg0, ml.agg0.data(), 4 * ml.agg0.size());
+  for (size_t d = 0; d < ml.l1.domains.size(); ++d)
+    for (uint32_t g : ml.l1.domains[d]) coarse_dom[g] = (uint32_t)d;
+  Csr c = ml.coarse_matrix(a);
+  *nnz = c.nnz();
+  if (c_rp) std::memcpy(c_rp, c.row_ptr.data(), 4 * (c.n + 1));
+  if (c_ci) std::memcpy(c_ci, c.col_idx.data(), 4 * c.nnz());
+  if (c_v) std::memcpy(c_v, c.values.data(), 4 * c.nnz());
+  return (uint32_t)ml.n_coarse;
+}
+
 // ---- LBVH ------------------------------------------------------------------------------
 void oracle_morton(const float* pos, const uint32_t* tris, uint64_t nt, int bits, uint64_t* out) {
   if (bits == 30) {

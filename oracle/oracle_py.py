@@ -40,6 +40,9 @@ def load() -> C.CDLL:
         "oracle_linear_solve": (i32, [u32, vp, vp, vp, vp, f32, u32, i32, u32, vp, P(u32), P(f64)]),
         "oracle_schwarz_domains": (u32, [u32, vp, vp, u32, vp]),
         "oracle_schwarz_apply": (None, [u32, vp, vp, vp, u32, vp, vp]),
+        "oracle_linear_solve_ml": (i32, [u32, vp, vp, vp, vp, f32, u32, u32, f64, vp, P(u32), P(f64)]),
+        "oracle_schwarz_ml_apply": (None, [u32, vp, vp, vp, u32, f64, vp, vp]),
+        "oracle_schwarz_ml_plan": (u32, [u32, vp, vp, vp, u32, vp, vp, P(u64), vp, vp, vp]),
         "oracle_morton": (None, [vp, vp, u64, i32, vp]),
         "oracle_centroid_bounds": (None, [vp, vp, u64, vp, vp]),
         "oracle_sort_pairs": (None, [vp, vp, u64]),
@@ -111,6 +114,42 @@ def linear_solve(n, rp, ci, vv, b, tol, max_iter, kind="schwarz", domain=32):
     lib.oracle_linear_solve(n, _p(rp), _p(ci), _p(vv), _p(bb), tol, max_iter, k, domain, _p(x), C.byref(it),
                             C.byref(res))
     return x, it.value, res.value
+
+
+def linear_solve_ml(n, rp, ci, vv, b, tol, max_iter, domain=16, weight=0.7):
+    """SchwarzMlCpu(domain, weight) LinearSolver::solve + last_stats (linsolve.rs:779-836)."""
+    lib = load()
+    x = np.empty(n, np.float32)
+    it, res = C.c_uint32(), C.c_double()
+    bb = np.ascontiguousarray(b, np.float32)
+    lib.oracle_linear_solve_ml(n, _p(rp), _p(ci), _p(vv), _p(bb), C.c_float(tol), max_iter, domain,
+                               C.c_double(weight), _p(x), C.byref(it), C.byref(res))
+    return x, it.value, res.value
+
+
+def schwarz_ml_apply(n, rp, ci, vv, domain, weight, r):
+    """z = S0 r + w C1^T S1 (C1 r), the two-level Schwarz apply in f64 (linsolve.rs:641-666)."""
+    lib = load()
+    rr = np.ascontiguousarray(r, np.float64)
+    z = np.empty(n, np.float64)
+    lib.oracle_schwarz_ml_apply(n, _p(rp), _p(ci), _p(vv), domain, C.c_double(weight), _p(rr), _p(z))
+    return z
+
+
+def schwarz_ml_plan(n, rp, ci, vv, domain):
+    """(agg0[nv], coarse_dom[n_coarse], coarse CSR (rp, ci, v)) of the two-level Schwarz."""
+    lib = load()
+    agg = np.empty(n // 3, np.uint32)
+    cdom = np.empty(n // 3, np.uint32)
+    nnz = C.c_uint64()
+    nc = lib.oracle_schwarz_ml_plan(n, _p(rp), _p(ci), _p(vv), domain, _p(agg), _p(cdom), C.byref(nnz), None, None,
+                                    None)
+    crp = np.empty(3 * nc + 1, np.uint32)
+    cci = np.empty(nnz.value, np.uint32)
+    cv = np.empty(nnz.value, np.float32)
+    lib.oracle_schwarz_ml_plan(n, _p(rp), _p(ci), _p(vv), domain, _p(agg), _p(cdom), C.byref(nnz), _p(crp), _p(cci),
+                               _p(cv))
+    return agg, cdom[:nc], (crp, cci, cv)
 
 
 def schwarz_domains(n, rp, ci, domain):

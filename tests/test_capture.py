@@ -309,3 +309,21 @@ def test_obj_rejects_out_of_range_index():  # obj.rs:459-464
 def test_obj_face_without_uv_index_drops_the_uv_array():  # obj.rs:477-484
     _, _, uv = cap.parse_obj("v 0 0 0\nv 1 0 0\nv 0 1 0\nvt 0 0\nvt 1 0\nvt 0 1\nf 1/1 2/2 3\n", with_uvs=True)
     assert uv.shape == (0, 2)
+
+
+def test_obj_comment_anywhere_on_the_line():  # obj.rs:103-107: '#' starts a comment anywhere
+    pos, tris = cap.parse_obj("# header\nv 0 0 0 # a\nv 1 0 0\nv 0 1 0\nf 1 2 3 # trailing comment\n")
+    assert pos.shape == (3, 3) and tris.tolist() == [[0, 1, 2]]
+
+
+def test_obj_rejects_short_faces_empty_files_and_malformed_records():  # obj.rs:136-138, 195-197, 249-262
+    with pytest.raises(cap.CaptureError):
+        cap.parse_obj("v 0 0 0\nv 1 0 0\nf 1 2\n")
+    with pytest.raises(cap.CaptureError):
+        cap.parse_obj("# nothing here\n")
+    with pytest.raises(cap.CaptureError):
+        cap.parse_obj("v 0 0\n")
+    with pytest.raises(cap.CaptureError):
+        cap.parse_obj("v 0 0 0\nvt\n")
+    with pytest.raises(cap.CaptureError):
+        cap.parse_obj("v 0 0 x\n")

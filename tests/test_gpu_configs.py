@@ -1,0 +1,73 @@
+"""GPU implicit step vs the oracle at the benchmark configurations' full sizes.
+
+Configuration 0 (64 x 64 sheet, 7 938 triangles, dropped onto an r = 0.3 m sphere, 36 steps)
+and configuration 1 (two 0.6 x 1.1 m panels at 8 mm edges, 41 400 triangles, 278 side-seam
+stitches, on a 19 800-triangle torso). The GPU drapes the whole run; at sampled steps the
+oracle's step (implicit.rs:1951-2191 restated) starts from the GPU's state before that step,
+so both sides take the same step from identical states: positions must agree within a
+fraction of the step's displacement and Newton iteration counts within +-1. The oracle steps
+run in parallel processes (tests/oracle_pool.py)."""
+import numpy as np
+import pytest
+
+from mguso import ImplicitSolver, scenes
+from oracle_pool import oracle_steps_from
+
+pytestmark = pytest.mark.gpu
+
+
+def _drape(ctx, sc, precision, steps, sample):
+    g = ImplicitSolver(ctx, sc, precision)
+    states, outs, all_stats = [], [], []
+    for k in range(steps):
+        p0, v0 = g.positions.copy(), g.velocities.copy()
+        st = g.step(1)[0]
+        all_stats.append(st)
+        if k in sample:
+            states.append((p0.astype(np.float64), v0.astype(np.float64)))
+            outs.append((g.positions.astype(np.float64), st))
+    g.close()
+    return states, outs, all_stats
+
+
+def _compare(sc, states, outs, precision_oracle="f32", params=None):
+    res = oracle_steps_from(sc, states, precision_oracle, params)
+    rows = []
+    for (p0, _), (pg, sg), (po, so) in zip(states, outs, res):
+        d = np.linalg.norm(pg - po, axis=1)
+        disp = np.linalg.norm(po - p0, axis=1)
+        rows.append({"rel": d.max() / max(disp.max(), 1e-30), "rms": np.sqrt((d ** 2).mean() / max((disp ** 2).mean(), 1e-60)),
+                     "newton": (int(sg["newton_iters"]), int(so["newton_iters"])),
+                     "stencils": (int(sg["stencils"]), int(so["stencils"])), "contacts": int(so["num_contacts"])})
+    for r in rows:
+        print(r)
+    return rows
+
+
+SHEET_SAMPLE = (0, 6, 12, 18, 24, 30, 35)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_config0_full_sheet_drape_matches_oracle(ctx, precision):
+    sc = scenes.sheet_on_sphere(64)
+    states, outs, stats = _drape(ctx, sc, precision, 36, SHEET_SAMPLE)
+    assert all(s["status"] == 0 and s["all_finite"] and s["penetration_free"] for s in stats)
+    rows = _compare(sc, states, outs)
+    assert any(r["contacts"] > 0 for r in rows)
+    for k, r in zip(SHEET_SAMPLE, rows):
+        assert abs(r["newton"][0] - r["newton"][1]) <= 1, (k, r)
+        assert r["rel"] < 1e-3, (k, r)
+
+
+SHEATH_SAMPLE = (0, 1, 2, 8)
+
+
+def test_config1_full_sheath_matches_oracle(ctx):
+    sc = scenes.sheath_on_torso()
+    assert sc["shell_faces"].shape[0] == 41400
+    states, outs, stats = _drape(ctx, sc, "fp32", 9, SHEATH_SAMPLE)
+    assert all(s["status"] == 0 and s["all_finite"] and s["penetration_free"] for s in stats)
+    rows = _compare(sc, states, outs)
+    for k, r in zip(SHEATH_SAMPLE, rows):
+        assert abs(r["newton"][0] - r["newton"][1]) <= 1, (k, r)
+        assert r["rel"] < 1e-3, (k, r)

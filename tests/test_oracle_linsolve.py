@@ -163,3 +163,65 @@ def test_schwarz_domains_are_bfs_aggregates():
     counts = np.bincount(dom)
     assert counts.max() <= 16 and counts.sum() == 100 and nd == counts.size
     assert dom[0] == 0 and dom[1] == 0 and dom[10] == 0
+
+
+def _vector_laplacian(g, diag):
+    """Elliptic g x g vector Laplacian: `diag` on every scalar diagonal, -1 to the four grid
+    neighbours per component (the reference's multilevel test system)."""
+    r, c, v = [], [], []
+    idx = lambda i, j: j * g + i  # noqa: E731
+    for j in range(g):
+        for i in range(g):
+            a = idx(i, j)
+            for k in range(3):
+                r.append(3 * a + k); c.append(3 * a + k); v.append(diag)
+            for di, dj in ((1, 0), (-1, 0), (0, 1), (0, -1)):
+                ni, nj = i + di, j + dj
+                if 0 <= ni < g and 0 <= nj < g:
+                    w = idx(ni, nj)
+                    for k in range(3):
+                        r.append(3 * a + k); c.append(3 * w + k); v.append(-1.0)
+    return O.csr_from_triplets(3 * g * g, r, c, v)
+
+
+def test_multilevel_schwarz_solves_and_cuts_iterations():  # linsolve.rs:970-1027
+    g = 32
+    n = 3 * g * g
+    rp, ci, vv = _vector_laplacian(g, 4.01)
+    x_star = np.sin(np.arange(n, dtype=np.float32) * np.float32(0.03)).astype(np.float32)
+    b = O.spmv(n, rp, ci, vv, x_star)
+    x1, i1, _ = O.linear_solve(n, rp, ci, vv, b, 1e-8, 5000, "schwarz", 8)
+    x2, i2, _ = O.linear_solve_ml(n, rp, ci, vv, b, 1e-8, 5000, 8, 0.7)
+    assert np.abs(x2 - x_star).max() < 1e-3, "2-level Schwarz must solve"
+    assert i2 < i1, (i2, i1)
+    # a second solve on the same sparsity is identical
+    x3, _, _ = O.linear_solve_ml(n, rp, ci, vv, b, 1e-8, 5000, 8, 0.7)
+    assert np.array_equal(x2, x3)
+
+
+def test_multilevel_apply_is_level0_plus_weighted_coarse_correction():  # linsolve.rs:641-666
+    g = 12
+    n = 3 * g * g
+    rp, ci, vv = _vector_laplacian(g, 4.5)
+    r = np.cos(np.arange(n) * 0.37)
+    z0 = O.schwarz_apply(n, rp, ci, vv, 8, r)
+    agg, cdom, (crp, cci, cv) = O.schwarz_ml_plan(n, rp, ci, vv, 8)
+    nc = crp.size // 3
+    # Galerkin coarse operator: every fine entry summed into its (coarse row, coarse col)
+    dense = np.zeros((n, n))
+    for i in range(n):
+        dense[i, ci[rp[i]:rp[i + 1]]] = vv[rp[i]:rp[i + 1]]
+    C = np.zeros((3 * nc, n))
+    for v_ in range(g * g):
+        for k in range(3):
+            C[3 * agg[v_] + k, 3 * v_ + k] = 1.0
+    a1 = C @ dense @ C.T
+    cd = np.zeros((3 * nc, 3 * nc))
+    for i in range(3 * nc):
+        cd[i, cci[crp[i]:crp[i + 1]]] = cv[crp[i]:crp[i + 1]]
+    assert np.allclose(cd, a1, rtol=1e-6, atol=1e-5)
+    # z = S0 r + w C^T S1 (C r), S1 = one-level Schwarz over the coarse operator
+    ec = O.schwarz_apply(3 * nc, crp, cci, cv, 8, C @ r)
+    for w in (0.7, 1.0):
+        z = O.schwarz_ml_apply(n, rp, ci, vv, 8, w, r)
+        assert np.allclose(z, z0 + w * (C.T @ ec), rtol=1e-12, atol=1e-12)
