@@ -82,6 +82,11 @@ typedef struct {
  * Schwarz domain size in vertices (ignored for block Jacobi). */
 int mguso_linear_solver_create(mguso_ctx* ctx, int precond, uint32_t domain, int precision,
                                mguso_linear_solver** out);
+/* The two-level variant, SchwarzMlCpu::new(domain, weight) (linsolve.rs:779-836): z =
+ * S0 r + weight * C1^T S1 (C1 r), with the Galerkin coarse operator rebuilt from the matrix
+ * values at every solve (the reference's CLI default is domain 16, weight 0.7). */
+int mguso_linear_solver_create_ml(mguso_ctx* ctx, uint32_t domain, float weight, int precision,
+                                  mguso_linear_solver** out);
 int mguso_linear_solver_destroy(mguso_linear_solver* s);
 /* solve(a, b, tol, max_iter) -> x  (LinearSolver::solve). a, b, x host; x has a->n
  * entries. Stats as LinearSolver::last_stats. Reaching max_iter is reported in
@@ -132,6 +137,16 @@ int mguso_schwarz_factor(mguso_schwarz* s, void* stream);
 int mguso_schwarz_apply(mguso_schwarz* s, const float* r, float* z, void* stream);
 /* Domain id of every vertex (host, nb entries). */
 int mguso_schwarz_domains(const mguso_schwarz* s, uint32_t* dom_of_vertex);
+/* Two-level Galerkin additive Schwarz (MultilevelSchwarz, linsolve.rs:534-666):
+ * z = S0 r + weight * C1^T S1 (C1 r). S0 is the one-level apply above (here every vertex
+ * without off-diagonal blocks is a domain of its own, as in the reference); C1 sums a
+ * vertex's residual into its domain (one coarse node of three dofs per domain); S1 is a
+ * one-level Schwarz over the Galerkin operator A1 = C1 A C1^T whose domains are BFS groups of
+ * <= `domain` coarse nodes. mguso_schwarz_factor factors both levels (the coarse blocks are
+ * summed in FP32 in the order of the fine values, as coarse_matrix, linsolve.rs:618-630). */
+int mguso_schwarz_create_ml(mguso_bsr* a, uint32_t domain, float weight, mguso_schwarz** out);
+/* Coarse domain of every coarse node (= level-0 domain; host, one entry per domain). */
+int mguso_schwarz_coarse_domains(const mguso_schwarz* s, uint32_t* coarse_dom_of_domain);
 
 /* ---- LBVH broad phase (engine-gpu/src/{morton,radix,karras,bvh_aabb,bvh_traverse}.rs) */
 /* Triangle BVH: 30-bit (u32) or 63-bit (u64) Morton codes of the centroids normalised by
@@ -334,6 +349,10 @@ int mguso_adjoint_forward(mguso_adjoint* a, const double* theta, uint32_t nsteps
                           float* x_out, mguso_step_stats* stats);
 /* dl_dx f32[3 nv] (dL/dx_N) -> dl_dtheta f64[3 npanel + nseam], for the last forward. */
 int mguso_adjoint_backward(mguso_adjoint* a, const float* dl_dx, double* dl_dtheta);
+/* The last forward pass's states x_n and v_n, n = 0..nsteps, recomputed from its checkpoints
+ * exactly as the backward pass recomputes them: x_all and v_all host, (nsteps + 1) * 3 nv
+ * floats each (state n at offset 3 nv n). */
+int mguso_adjoint_states(mguso_adjoint* a, float* x_all, float* v_all);
 int mguso_read_positions(mguso_scene* s, float* out);   /* f32[3*nv] host */
 int mguso_write_positions(mguso_scene* s, const float* in);
 int mguso_read_velocities(mguso_scene* s, float* out);

@@ -469,6 +469,29 @@ int mguso_adjoint_forward(mguso_adjoint* a, const double* theta, uint32_t nsteps
   return MGUSO_OK;
 }
 
+int mguso_adjoint_states(mguso_adjoint* a, float* x_all, float* v_all) {
+  MG_CHECK_ARG(a && x_all && v_all && a->scene, "bad argument (forward first)");
+  MG_CUDA(cudaSetDevice(a->ctx->device));
+  Scene& s = a->scene->s;
+  cudaStream_t st = s.st;
+  const size_t n3 = 3 * (size_t)s.nv;
+  for (uint32_t c = 0; c < (uint32_t)a->ck_x.size(); ++c) {
+    const uint32_t n0 = c * a->every, n1 = std::min(a->nsteps, n0 + a->every);
+    MG_CUDA(cudaMemcpyAsync(s.x.p, a->ck_x[c]->p, 4 * n3, cudaMemcpyDeviceToDevice, st));
+    MG_CUDA(cudaMemcpyAsync(s.v.p, a->ck_v[c]->p, 4 * n3, cudaMemcpyDeviceToDevice, st));
+    for (uint32_t n = n0; n <= n1; ++n) {
+      MG_CUDA(cudaMemcpyAsync(x_all + n * n3, s.x.p, 4 * n3, cudaMemcpyDeviceToHost, st));
+      MG_CUDA(cudaMemcpyAsync(v_all + n * n3, s.v.p, 4 * n3, cudaMemcpyDeviceToHost, st));
+      MG_CUDA(cudaStreamSynchronize(st));
+      if (n < n1) {
+        mguso_step_stats stt{};
+        MG_TRY(scene_step(s, &stt));
+      }
+    }
+  }
+  return MGUSO_OK;
+}
+
 int mguso_adjoint_backward(mguso_adjoint* a, const float* dl_dx, double* dl_dtheta) {
   MG_CHECK_ARG(a && dl_dx && dl_dtheta && a->scene, "bad argument (forward first)");
   MG_CUDA(cudaSetDevice(a->ctx->device));

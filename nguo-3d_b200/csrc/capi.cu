@@ -1,5 +1,6 @@
 // extern "C" entry points declared in include/mguso_cuda.h (linear-algebra half).
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 
 #include "lbvh.cuh"
@@ -165,6 +166,29 @@ int mguso_schwarz_create(mguso_bsr* a, uint32_t domain, mguso_schwarz** out) {
   return MGUSO_OK;
 }
 
+int mguso_schwarz_create_ml(mguso_bsr* a, uint32_t domain, float weight, mguso_schwarz** out) {
+  MG_CHECK_ARG(a && out, "null argument");
+  MG_CHECK_ARG(domain >= 1 && domain <= 32, "Schwarz domain size must be in [1, 32] vertices");
+  MG_CHECK_ARG(std::isfinite(weight) && weight >= 0.f, "coarse weight must be finite and >= 0");
+  auto s = std::make_unique<mguso_schwarz>();
+  s->a = a;
+  s->domain = domain;
+  s->levels = 2;
+  s->weight = weight;
+  s->pack_singles = false;
+  MG_TRY(schwarz_build(s.get()));
+  *out = s.release();
+  return MGUSO_OK;
+}
+
+int mguso_schwarz_coarse_domains(const mguso_schwarz* s, uint32_t* coarse_dom_of_domain) {
+  MG_CHECK_ARG(s && coarse_dom_of_domain, "null argument");
+  MG_CHECK_ARG(s->levels == 2, "not a two-level Schwarz preconditioner");
+  for (uint32_t d = 0; d < s->ncdom; ++d)
+    for (uint32_t k = s->h_cdom_start[d]; k < s->h_cdom_start[d + 1]; ++k) coarse_dom_of_domain[s->h_cdom_nodes[k]] = d;
+  return MGUSO_OK;
+}
+
 int mguso_schwarz_destroy(mguso_schwarz* s) {
   delete s;
   return MGUSO_OK;
@@ -210,6 +234,15 @@ int mguso_linear_solver_create(mguso_ctx* ctx, int precond, uint32_t domain, int
   return MGUSO_OK;
 }
 
+int mguso_linear_solver_create_ml(mguso_ctx* ctx, uint32_t domain, float weight, int precision,
+                                  mguso_linear_solver** out) {
+  MG_CHECK_ARG(std::isfinite(weight) && weight >= 0.f, "coarse weight must be finite and >= 0");
+  MG_TRY(mguso_linear_solver_create(ctx, MGUSO_PRECOND_SCHWARZ, domain, precision, out));
+  (*out)->levels = 2;
+  (*out)->weight = weight;
+  return MGUSO_OK;
+}
+
 int mguso_linear_solver_destroy(mguso_linear_solver* s) {
   if (!s) return MGUSO_OK;
   delete s;
@@ -251,6 +284,9 @@ int mguso_linear_solve(mguso_linear_solver* s, const mguso_csr* a, const float* 
       s->schwarz = std::make_unique<mguso_schwarz>();
       s->schwarz->a = s->bsr.get();
       s->schwarz->domain = s->domain;
+      s->schwarz->levels = s->levels;
+      s->schwarz->weight = s->weight;
+      s->schwarz->pack_singles = s->levels != 2;  // two levels: every domain a coarse node, as the reference
       MG_TRY(schwarz_build(s->schwarz.get()));
     }
   } else {

@@ -88,6 +88,24 @@ struct mguso_schwarz {
   mg::DevBuf<__half> fac_h;
   mg::DevBuf<float> fac_scale;
   mg::DevBuf<uint32_t> status;
+  // Two-level Galerkin form (MultilevelSchwarz, linsolve.rs:534-666) when levels == 2: every
+  // level-0 domain is a coarse node (three dofs), coarse domains are BFS groups of <= domain
+  // coarse nodes over the coarse block graph, and each coarse domain's dense block of
+  // A1 = C1 A C1^T is factored like a level-0 domain (FP32 W1 tiles). Level-0 isolated
+  // vertices are packed only when pack_singles is set (the reference gives each its own domain).
+  uint32_t levels = 1;
+  float weight = 0.7f;
+  bool pack_singles = true;
+  uint32_t ncdom = 0, max_m1 = 0;
+  std::vector<uint32_t> h_cdom_start, h_cdom_nodes;
+  mg::DevBuf<uint32_t> cdom_start;  // ncdom + 1
+  mg::DevBuf<uint32_t> cdom_nodes;  // ndom: coarse nodes (level-0 domains) by coarse domain
+  mg::DevBuf<uint32_t> cdom_of;     // ndom: coarse domain of each coarse node
+  mg::DevBuf<uint32_t> cloc;        // ndom: local index of a coarse node in its coarse domain
+  mg::DevBuf<uint32_t> dom_sorted;  // nb: each level-0 domain's vertices in ascending order
+  mg::DevBuf<uint64_t> cfac_off;    // ncdom + 1
+  mg::DevBuf<float> cfac;           // W1 tiles
+  mg::DevBuf<float> ec;             // 3 * ndom: the coarse correction of the last apply
 };
 
 namespace mg {
@@ -183,6 +201,8 @@ struct mguso_linear_solver {
   int precond = MGUSO_PRECOND_SCHWARZ;
   uint32_t domain = 32;
   int precision = MGUSO_PRECISION_MIXED;
+  uint32_t levels = 1;  // 2: two-level Schwarz (SchwarzMlCpu)
+  float weight = 0.7f;
   // cached pattern (rebuild BSR/domains only when the scalar sparsity changes)
   std::vector<uint32_t> csr_row_ptr, csr_col;
   std::unique_ptr<mguso_bsr> bsr;

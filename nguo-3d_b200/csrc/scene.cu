@@ -567,6 +567,12 @@ int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>
     s.schwarz->domain = s.p.schwarz_domain;
     s.schwarz->half = s.fp16_factor;  // FP16 factor tiles: the apply moves half the bytes
     s.schwarz->inst_vert = s.inst_vert;
+    if (s.p.schwarz_levels == 2) {
+      // two-level Schwarz: single scenes, stepped with the per-kernel PCG
+      MG_CHECK_ARG(s.ninst == 1, "scene: two-level Schwarz is for single scenes, not batches");
+      s.schwarz->levels = 2;
+      s.schwarz->weight = s.p.schwarz_weight > 0.f ? s.p.schwarz_weight : 0.7f;
+    }
     MG_TRY(schwarz_build(s.schwarz.get()));
   } else {
     MG_TRY(s.bjinv.reserve(9 * (size_t)nv));

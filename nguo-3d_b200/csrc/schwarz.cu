@@ -19,6 +19,7 @@
 namespace mg {
 
 int schwarz_configure();
+int schwarz_build_coarse(mguso_schwarz* s);
 int schwarz_factor_with(mguso_schwarz* s, const uint32_t* c_rp, const uint32_t* c_col, const float* c_val,
                         cudaStream_t st);
 
@@ -43,7 +44,7 @@ int schwarz_build(mguso_schwarz* s) {
   // do not couple, so the packed domain's factor is block diagonal and the preconditioner
   // is unchanged (only the diagonal floor averages over the packed vertices).
   std::vector<uint32_t> singles;
-  for (uint32_t v = 0; v < nb; ++v) {
+  for (uint32_t v = 0; v < nb && s->pack_singles; ++v) {
     bool iso = true;
     for (uint32_t k = rp[v]; k < rp[v + 1] && iso; ++k) iso = cl[k] == v;
     if (iso) {
@@ -120,8 +121,81 @@ int schwarz_build(mguso_schwarz* s) {
   }
   MG_TRY(s->status.reserve(4));
   MG_CUDA(cudaMemsetAsync(s->status.p, 0, 16, st));
+  if (s->levels == 2) MG_TRY(schwarz_build_coarse(s));
   MG_CUDA(cudaStreamSynchronize(st));
   MG_TRY(schwarz_configure());
+  return MGUSO_OK;
+}
+
+// Coarse level of the two-level form (MultilevelSchwarz::build, linsolve.rs:555-608): coarse
+// node G = level-0 domain G; G and H are adjacent when some block (i, j) of the pattern has
+// i in G and j in H; coarse domains are the reference's greedy BFS over that adjacency
+// (seeds in node order, neighbours in ascending order, <= domain nodes each).
+int schwarz_build_coarse(mguso_schwarz* s) {
+  mguso_bsr* a = s->a;
+  const uint32_t nb = a->nb, nd = s->ndom;
+  const auto& rp = a->h_row_ptr;
+  const auto& cl = a->h_col;
+  std::vector<std::vector<uint32_t>> adj(nd);
+  for (uint32_t v = 0; v < nb; ++v) {
+    const uint32_t g = s->h_dom_of[v];
+    for (uint32_t k = rp[v]; k < rp[v + 1]; ++k) {
+      const uint32_t h = s->h_dom_of[cl[k]];
+      if (h != g) adj[g].push_back(h);
+    }
+  }
+  for (auto& x : adj) {
+    std::sort(x.begin(), x.end());
+    x.erase(std::unique(x.begin(), x.end()), x.end());
+  }
+  const uint32_t D = std::max<uint32_t>(s->domain, 1);
+  std::vector<uint8_t> assigned(nd, 0);
+  std::vector<uint32_t> cdom_of(nd, 0), cloc(nd, 0);
+  s->h_cdom_start.assign(1, 0);
+  s->h_cdom_nodes.clear();
+  s->max_m1 = 0;
+  for (uint32_t seed = 0; seed < nd; ++seed) {
+    if (assigned[seed]) continue;
+    const size_t base = s->h_cdom_nodes.size();
+    s->h_cdom_nodes.push_back(seed);
+    assigned[seed] = 1;
+    size_t fi = base;
+    while (s->h_cdom_nodes.size() - base < D && fi < s->h_cdom_nodes.size()) {
+      const uint32_t g = s->h_cdom_nodes[fi++];
+      for (uint32_t h : adj[g])
+        if (!assigned[h] && s->h_cdom_nodes.size() - base < D) {
+          assigned[h] = 1;
+          s->h_cdom_nodes.push_back(h);
+        }
+    }
+    const uint32_t d1 = (uint32_t)s->h_cdom_start.size() - 1;
+    for (size_t i = base; i < s->h_cdom_nodes.size(); ++i) {
+      cdom_of[s->h_cdom_nodes[i]] = d1;
+      cloc[s->h_cdom_nodes[i]] = (uint32_t)(i - base);
+    }
+    s->h_cdom_start.push_back((uint32_t)s->h_cdom_nodes.size());
+    s->max_m1 = std::max<uint32_t>(s->max_m1, 3 * (uint32_t)(s->h_cdom_nodes.size() - base));
+  }
+  s->ncdom = (uint32_t)s->h_cdom_start.size() - 1;
+  std::vector<uint64_t> off(s->ncdom + 1, 0);
+  for (uint32_t d = 0; d < s->ncdom; ++d) {
+    const uint64_t m = 3ull * (s->h_cdom_start[d + 1] - s->h_cdom_start[d]);
+    const uint64_t t = (m + 31) / 32;
+    off[d + 1] = off[d] + t * (t + 1) / 2 * TILE_FLOATS;
+  }
+  std::vector<uint32_t> sorted(s->h_dom_verts);
+  for (uint32_t d = 0; d < nd; ++d)
+    std::sort(sorted.begin() + s->h_dom_start[d], sorted.begin() + s->h_dom_start[d + 1]);
+  cudaStream_t st = a->ctx->stream;
+  MG_TRY(s->cdom_start.upload(s->h_cdom_start.data(), s->h_cdom_start.size(), st));
+  MG_TRY(s->cdom_nodes.upload(s->h_cdom_nodes.data(), std::max<size_t>(s->h_cdom_nodes.size(), 1), st));
+  MG_TRY(s->cdom_of.upload(cdom_of.data(), std::max<size_t>(nd, 1), st));
+  MG_TRY(s->cloc.upload(cloc.data(), std::max<size_t>(nd, 1), st));
+  MG_TRY(s->dom_sorted.upload(sorted.data(), std::max<size_t>(sorted.size(), 1), st));
+  MG_TRY(s->cfac_off.upload(off.data(), off.size(), st));
+  MG_TRY(s->cfac.reserve(std::max<uint64_t>(off[s->ncdom], 4)));
+  MG_TRY(s->ec.reserve(std::max<uint64_t>(3ull * nd, 4)));
+  MG_CUDA(cudaStreamSynchronize(st));
   return MGUSO_OK;
 }
 
@@ -173,6 +247,100 @@ __device__ double factor_amax(const double* A, int ld, int m, const double* diag
   return r > 0.0 ? r : 1.0;
 }
 
+// Steps 2-3 of the factorisation and the store, on the dense block A (m x m, leading
+// dimension ld, FP64 shared memory, lower triangle filled) of one domain: the reference's
+// diagonal floor, right-looking Cholesky with its pivot test (falling back to the floored
+// diagonal), W = L^-1, and W written to `out` as tiles (FP16 tiles: W / scale with the
+// scale in *scale_out). dinv and diag0 are m doubles of shared scratch each.
+template <class TS>
+__device__ void factor_dense_store(double* A, int ld, int m, double* dinv, double* diag0, TS* __restrict__ out,
+                                   float* scale_out, uint32_t* status) {
+  constexpr bool scaled = sizeof(TS) == 2;
+  __shared__ double s_floor;
+  __shared__ int s_fail;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  if (tid == 0) {
+    double tr = 0.0;
+    for (int k = 0; k < m; ++k) tr += A[k * ld + k];
+    s_floor = 1e-6 * (tr / (double)m) + 1e-8;
+    s_fail = 0;
+  }
+  __syncthreads();
+  for (int k = tid; k < m; k += nt) {
+    A[k * ld + k] += s_floor;
+    diag0[k] = A[k * ld + k];
+  }
+  __syncthreads();
+  // Cholesky: column k stays unscaled during its own trailing update (L_ik = A_ik / L_kk
+  // is applied after the loop), so one barrier per column suffices.
+  const int tx = tid & 31, ty = tid >> 5;
+  for (int k = 0; k < m; ++k) {
+    const double p = A[k * ld + k];
+    if (!(p > 1e-14)) {  // uniform: every thread reads the same pivot
+      if (tid == 0) s_fail = 1;
+      break;
+    }
+    const double ip = 1.0 / p;
+    for (int i = k + 1 + ty; i < m; i += 8) {
+      const double aik = A[i * ld + k] * ip;
+      for (int j = k + 1 + tx; j <= i; j += 32) A[i * ld + j] -= aik * A[j * ld + k];
+    }
+    if (tid == 0) {
+      const double l = sqrt(p);
+      dinv[k] = 1.0 / l;
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  const int T = (m + 31) / 32, nfl = T * (T + 1) / 2 * TILE_FLOATS;
+  if (s_fail) {
+    // reference fallback: L = diag(sqrt(ad_pp)) (1 where ad_pp <= 1e-14), i.e.
+    // W = diag(1 / sqrt(ad_pp))
+    const double sc = scaled ? factor_amax(A, ld, m, diag0, true) : 1.0;
+    if (scaled && tid == 0) *scale_out = (float)sc;
+    for (int e = tid; e < nfl; e += nt) out[e] = to_tile<TS>(0.0);
+    __syncthreads();
+    for (int r = tid; r < m; r += nt) {
+      double a = diag0[r];
+      const int I = r >> 5, lr = r & 31;
+      out[tile_index(I, I) * TILE_FLOATS + tile_offset(lr, lr)] = to_tile<TS>((a > 1e-14 ? 1.0 / sqrt(a) : 1.0) / sc);
+    }
+    if (tid == 0) atomicOr(status, 1u << 8);
+    return;
+  }
+  for (int i = ty; i < m; i += 8)
+    for (int k = tx; k < i; k += 32) A[i * ld + k] *= dinv[k];
+  __syncthreads();
+  // W = L^-1 by columns: thread j walks rows i > j; W_ij = -dinv_i * sum_{k=j}^{i-1} L_ik W_kj.
+  // W_kj (k >= j) lives at A[j * ld + k], the upper triangle and the diagonal.
+  for (int j = tid; j < m; j += nt) {
+    double* wj = A + (size_t)j * ld;
+    wj[j] = dinv[j];
+    for (int i = j + 1; i < m; ++i) {
+      const double* li = A + (size_t)i * ld;
+      double s0 = 0.0, s1 = 0.0;
+      int k = j;
+      for (; k + 1 < i; k += 2) {
+        s0 += li[k] * wj[k];
+        s1 += li[k + 1] * wj[k + 1];
+      }
+      if (k < i) s0 += li[k] * wj[k];
+      wj[i] = -(s0 + s1) * dinv[i];
+    }
+  }
+  __syncthreads();
+  const double inv_sc = scaled ? 1.0 / factor_amax(A, ld, m, diag0, false) : 1.0;
+  if (scaled && tid == 0) *scale_out = (float)(1.0 / inv_sc);
+  // tiles in storage order; e walks each tile's swizzled offsets so the stores coalesce
+  for (int e = tid; e < nfl; e += nt) {
+    const int t = e / TILE_FLOATS, o = e - t * TILE_FLOATS;
+    const int I = t >= 3 ? 2 : (t >= 1 ? 1 : 0), J = t - I * (I + 1) / 2;
+    const int c = o >> 5, r = (o & 31) ^ c;
+    const int gi = 32 * I + r, gj = 32 * J + c;
+    out[e] = to_tile<TS>((gi < m && gj <= gi) ? A[gj * ld + gi] * inv_sc : 0.0);
+  }
+}
+
 template <class TS>
 __global__ void __launch_bounds__(FACTOR_THREADS) k_schwarz_factor(
     const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ col, const float* __restrict__ val,
@@ -181,10 +349,7 @@ __global__ void __launch_bounds__(FACTOR_THREADS) k_schwarz_factor(
     TS* __restrict__ fac, float* __restrict__ fac_scale, uint32_t* status, const uint32_t* __restrict__ c_rp,
     const uint32_t* __restrict__ c_col, const float* __restrict__ c_val) {
   // FP16 tiles hold W / scale (scale: the domain's largest |W|); FP32 tiles hold W
-  constexpr bool scaled = sizeof(TS) == 2;
   extern __shared__ __align__(16) double sA[];
-  __shared__ double s_floor;
-  __shared__ int s_fail;
   const uint32_t d = blockIdx.x;
   const uint32_t vs = dom_start[d], nvd = dom_start[d + 1] - vs;
   const int m = 3 * (int)nvd;
@@ -225,87 +390,57 @@ __global__ void __launch_bounds__(FACTOR_THREADS) k_schwarz_factor(
     }
     __syncthreads();
   }
-  if (tid == 0) {
-    double tr = 0.0;
-    for (int k = 0; k < m; ++k) tr += A[k * ld + k];
-    s_floor = 1e-6 * (tr / (double)m) + 1e-8;
-    s_fail = 0;
-  }
+  factor_dense_store<TS>(A, ld, m, dinv, diag0, fac + fac_off[d], fac_scale ? fac_scale + d : nullptr, status);
+}
+
+// Coarse factorisation of the two-level form, one CTA per coarse domain: thread t owns
+// row t = 3a + r of the domain's dense Galerkin block (coarse node a, component r) and adds,
+// for every vertex i of node a in ascending order and every block (i, j) of the pattern and
+// of the contact matrix in column order whose column vertex lies in this coarse domain, the
+// block's row r. The sums run in FP32, entry by entry in the order of the fine values, as
+// the reference's coarse_matrix does (linsolve.rs:618-630); the block is then factored and
+// stored like a level-0 domain.
+__global__ void __launch_bounds__(FACTOR_THREADS) k_coarse_factor(
+    const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ col, const float* __restrict__ val,
+    const uint32_t* __restrict__ c_rp, const uint32_t* __restrict__ c_col, const float* __restrict__ c_val,
+    const uint32_t* __restrict__ dom_start, const uint32_t* __restrict__ dom_sorted,
+    const uint32_t* __restrict__ dom_of, const uint32_t* __restrict__ cdom_start,
+    const uint32_t* __restrict__ cdom_nodes, const uint32_t* __restrict__ cdom_of, const uint32_t* __restrict__ cloc,
+    const uint64_t* __restrict__ cfac_off, float* __restrict__ cfac, uint32_t* status) {
+  extern __shared__ __align__(16) double sA[];
+  const uint32_t d1 = blockIdx.x;
+  const uint32_t n0 = cdom_start[d1], mn = cdom_start[d1 + 1] - n0;
+  const int m = 3 * (int)mn, ld = m + 1;
+  double* A = sA;
+  double* dinv = sA + (size_t)m * ld;
+  double* diag0 = dinv + m;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int i = tid; i < m * ld; i += nt) A[i] = 0.0;
   __syncthreads();
-  for (int k = tid; k < m; k += nt) {
-    A[k * ld + k] += s_floor;
-    diag0[k] = A[k * ld + k];
-  }
-  __syncthreads();
-  // Cholesky: column k stays unscaled during its own trailing update (L_ik = A_ik / L_kk
-  // is applied after the loop), so one barrier per column suffices.
-  const int tx = tid & 31, ty = tid >> 5;
-  for (int k = 0; k < m; ++k) {
-    const double p = A[k * ld + k];
-    if (!(p > 1e-14)) {  // uniform: every thread reads the same pivot
-      if (tid == 0) s_fail = 1;
-      break;
-    }
-    const double ip = 1.0 / p;
-    for (int i = k + 1 + ty; i < m; i += 8) {
-      const double aik = A[i * ld + k] * ip;
-      for (int j = k + 1 + tx; j <= i; j += 32) A[i * ld + j] -= aik * A[j * ld + k];
-    }
-    if (tid == 0) {
-      const double l = sqrt(p);
-      dinv[k] = 1.0 / l;
-    }
-    __syncthreads();
-  }
-  __syncthreads();
-  TS* out = fac + fac_off[d];
-  const int T = (m + 31) / 32, nfl = T * (T + 1) / 2 * TILE_FLOATS;
-  if (s_fail) {
-    // reference fallback: L = diag(sqrt(ad_pp)) (1 where ad_pp <= 1e-14), i.e.
-    // W = diag(1 / sqrt(ad_pp))
-    const double sc = scaled ? factor_amax(A, ld, m, diag0, true) : 1.0;
-    if (scaled && tid == 0) fac_scale[d] = (float)sc;
-    for (int e = tid; e < nfl; e += nt) out[e] = to_tile<TS>(0.0);
-    __syncthreads();
-    for (int r = tid; r < m; r += nt) {
-      double a = diag0[r];
-      const int I = r >> 5, lr = r & 31;
-      out[tile_index(I, I) * TILE_FLOATS + tile_offset(lr, lr)] = to_tile<TS>((a > 1e-14 ? 1.0 / sqrt(a) : 1.0) / sc);
-    }
-    if (tid == 0) atomicOr(status, 1u << 8);
-    return;
-  }
-  for (int i = ty; i < m; i += 8)
-    for (int k = tx; k < i; k += 32) A[i * ld + k] *= dinv[k];
-  __syncthreads();
-  // W = L^-1 by columns: thread j walks rows i > j; W_ij = -dinv_i * sum_{k=j}^{i-1} L_ik W_kj.
-  // W_kj (k >= j) lives at A[j * ld + k], the upper triangle and the diagonal.
-  for (int j = tid; j < m; j += nt) {
-    double* wj = A + (size_t)j * ld;
-    wj[j] = dinv[j];
-    for (int i = j + 1; i < m; ++i) {
-      const double* li = A + (size_t)i * ld;
-      double s0 = 0.0, s1 = 0.0;
-      int k = j;
-      for (; k + 1 < i; k += 2) {
-        s0 += li[k] * wj[k];
-        s1 += li[k + 1] * wj[k + 1];
+  for (int t = tid; t < m; t += nt) {
+    const int a = t / 3, r = t - 3 * a;
+    const uint32_t g = cdom_nodes[n0 + a];
+    double* row = A + (size_t)t * ld;
+    for (uint32_t p = dom_start[g]; p < dom_start[g + 1]; ++p) {
+      const uint32_t i = dom_sorted[p];
+      uint32_t k1 = row_ptr[i];
+      const uint32_t e1 = row_ptr[i + 1];
+      uint32_t k2 = c_rp ? c_rp[i] : 0;
+      const uint32_t e2 = c_rp ? c_rp[i + 1] : 0;
+      while (k1 < e1 || k2 < e2) {
+        const bool from_c = k1 >= e1 || (k2 < e2 && c_col[k2] < col[k1]);
+        const uint32_t j = from_c ? c_col[k2] : col[k1];
+        const float* b = from_c ? c_val + 9 * (size_t)k2++ : val + 9 * (size_t)k1++;
+        const uint32_t h = dom_of[j];
+        if (cdom_of[h] != d1) continue;
+        const int q = 3 * (int)cloc[h];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) row[q + c] = (double)((float)row[q + c] + b[3 * r + c]);
       }
-      if (k < i) s0 += li[k] * wj[k];
-      wj[i] = -(s0 + s1) * dinv[i];
     }
   }
   __syncthreads();
-  const double inv_sc = scaled ? 1.0 / factor_amax(A, ld, m, diag0, false) : 1.0;
-  if (scaled && tid == 0) fac_scale[d] = (float)(1.0 / inv_sc);
-  // tiles in storage order; e walks each tile's swizzled offsets so the stores coalesce
-  for (int e = tid; e < nfl; e += nt) {
-    const int t = e / TILE_FLOATS, o = e - t * TILE_FLOATS;
-    const int I = t >= 3 ? 2 : (t >= 1 ? 1 : 0), J = t - I * (I + 1) / 2;
-    const int c = o >> 5, r = (o & 31) ^ c;
-    const int gi = 32 * I + r, gj = 32 * J + c;
-    out[e] = to_tile<TS>((gi < m && gj <= gi) ? A[gj * ld + gi] * inv_sc : 0.0);
-  }
+  factor_dense_store<float>(A, ld, m, dinv, diag0, cfac + cfac_off[d1], nullptr, status);
 }
 
 int schwarz_factor(mguso_schwarz* s, cudaStream_t st) {
@@ -326,6 +461,14 @@ int schwarz_factor_with(mguso_schwarz* s, const uint32_t* c_rp, const uint32_t* 
         a->row_ptr.p, a->col.p, a->val.p, s->dom_start.p, s->dom_verts.p, s->dom_of.p, s->loc.p, s->fac_off.p,
         s->fac.p, nullptr, s->status.p, c_col ? c_rp : nullptr, c_col, c_val);
   MG_CUDA(cudaGetLastError());
+  if (s->levels == 2 && s->ncdom) {
+    size_t smem1 = sizeof(double) * ((size_t)s->max_m1 * (s->max_m1 + 1) + 2 * (size_t)s->max_m1);
+    k_coarse_factor<<<s->ncdom, FACTOR_THREADS, smem1, st>>>(
+        a->row_ptr.p, a->col.p, a->val.p, c_col ? c_rp : nullptr, c_col, c_val, s->dom_start.p, s->dom_sorted.p,
+        s->dom_of.p, s->cdom_start.p, s->cdom_nodes.p, s->cdom_of.p, s->cloc.p, s->cfac_off.p, s->cfac.p,
+        s->status.p);
+    MG_CUDA(cudaGetLastError());
+  }
   return MGUSO_OK;
 }
 
@@ -401,7 +544,82 @@ __global__ void __launch_bounds__(32 * WARPS) k_schwarz_apply(
     }
     __syncwarp();  // every lane is done with buf before the next copy overwrites it
   }
-  if (with_dot) grid_dot_commit<Acc>(dot, acc);
+  if (with_dot == 1) grid_dot_commit<Acc>(dot, acc);
+}
+
+// Coarse level of the two-level apply, one warp per coarse domain: restriction
+// rc = sum of r over each coarse node's vertices (linsolve.rs:648-655), the domain's
+// z1 = W1^T (W1 rc) from its FP32 tiles, written as the coarse correction ec.
+__global__ void __launch_bounds__(32) k_coarse_apply(
+    const uint32_t* __restrict__ cdom_start, const uint32_t* __restrict__ cdom_nodes,
+    const uint32_t* __restrict__ dom_start, const uint32_t* __restrict__ dom_verts,
+    const uint64_t* __restrict__ cfac_off, const float* __restrict__ cfac, const float* __restrict__ r,
+    float* __restrict__ ec, uint32_t ncdom, const PcgScalars* done) {
+  __shared__ __align__(16) float buf[6 * TILE_FLOATS];
+  __shared__ float rd[96];
+  __shared__ double yd[96];
+  if (done && done->done) return;
+  const int lane = threadIdx.x;
+  for (uint32_t d1 = blockIdx.x; d1 < ncdom; d1 += gridDim.x) {
+    const uint32_t n0 = cdom_start[d1], mn = cdom_start[d1 + 1] - n0;
+    const int m = 3 * (int)mn;
+    const uint64_t off = cfac_off[d1];
+    const int nfl = (int)(cfac_off[d1 + 1] - off);
+    for (int e = lane; e < nfl; e += 32) buf[e] = cfac[off + e];
+    for (uint32_t a = 0; a < mn; ++a) {
+      const uint32_t g = cdom_nodes[n0 + a];
+      double s0 = 0, s1 = 0, s2 = 0;
+      for (uint32_t p = dom_start[g] + lane; p < dom_start[g + 1]; p += 32) {
+        const uint32_t v = dom_verts[p];
+        s0 += (double)r[3 * v];
+        s1 += (double)r[3 * v + 1];
+        s2 += (double)r[3 * v + 2];
+      }
+      s0 = warp_sum(s0);
+      s1 = warp_sum(s1);
+      s2 = warp_sum(s2);
+      if (lane == 0) {
+        rd[3 * a] = (float)s0;
+        rd[3 * a + 1] = (float)s1;
+        rd[3 * a + 2] = (float)s2;
+      }
+    }
+    for (int i = m + lane; i < 96; i += 32) rd[i] = 0.f;
+    __syncwarp();
+    double zz[3];
+    const int T = (m + 31) >> 5;
+    if (T == 3)
+      tiles_apply<3, double, float>(buf, rd, yd, zz, lane);
+    else if (T == 2)
+      tiles_apply<2, double, float>(buf, rd, yd, zz, lane);
+    else
+      tiles_apply<1, double, float>(buf, rd, yd, zz, lane);
+#pragma unroll
+    for (int J = 0; J < 3; ++J) {
+      const int i = 32 * J + lane;
+      if (i < m) ec[3 * cdom_nodes[n0 + i / 3] + i % 3] = (float)zz[J];
+    }
+    __syncwarp();
+  }
+}
+
+// z += w * ec[coarse node of the vertex] (the weighted prolongation, linsolve.rs:657-665),
+// with the fused r.z of the PCG.
+template <class Acc>
+__global__ void k_prolong(const float* __restrict__ r, float* __restrict__ z, const float* __restrict__ ec,
+                          const uint32_t* __restrict__ dom_of, uint32_t nb, float w, DotSink d, int with_dot) {
+  if (with_dot && d.sc->done) return;
+  Acc acc = 0;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nb; v += gridDim.x * blockDim.x) {
+    const uint32_t g = dom_of[v];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float zc = fmaf(w, ec[3 * g + c], z[3 * v + c]);
+      z[3 * v + c] = zc;
+      acc += (Acc)r[3 * v + c] * (Acc)zc;
+    }
+  }
+  if (with_dot) grid_dot_commit<Acc>(d, acc);
 }
 
 // Shared-memory opt-in for the largest domain (32 vertices, m = 96), set once outside any
@@ -412,6 +630,7 @@ int schwarz_configure() {
   size_t fsm = sizeof(double) * (96 * 97 + 2 * 96);
   MG_CUDA(cudaFuncSetAttribute(k_schwarz_factor<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
   MG_CUDA(cudaFuncSetAttribute(k_schwarz_factor<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
+  MG_CUDA(cudaFuncSetAttribute(k_coarse_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
   const int asm32 = (int)(128 + (size_t)APPLY_WARPS * apply_slice_bytes<float>());
   const int asm16 = (int)(128 + (size_t)APPLY_WARPS * apply_slice_bytes<__half>());
   MG_CUDA(cudaFuncSetAttribute(k_schwarz_apply<APPLY_WARPS, double, float>,
@@ -428,7 +647,9 @@ int schwarz_configure() {
 
 int schwarz_apply(mguso_schwarz* s, const float* r, float* z, cudaStream_t st, const DotSink* dot) {
   DotSink d{};
-  int with_dot = dot ? 1 : 0;
+  // two levels: the level-0 apply skips after convergence but leaves the r.z to the
+  // prolongation, which completes z
+  int with_dot = dot ? (s->levels == 2 ? 2 : 1) : 0;
   if (dot) d = *dot;
   bool mixed = dot && dot->mixed;
   if (s->max_m > 96) {
@@ -454,6 +675,18 @@ int schwarz_apply(mguso_schwarz* s, const float* r, float* z, cudaStream_t st, c
                   (void*)&nd, (void*)&stp, (void*)&d, (void*)&with_dot};
   if (grid == 0) return MGUSO_OK;
   MG_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(32 * APPLY_WARPS), args, smem, st));
+  if (s->levels != 2 || s->ncdom == 0) return MGUSO_OK;
+  const uint32_t cgrid = std::min<uint32_t>(s->ncdom, 16u * (uint32_t)s->a->ctx->sm_count);
+  k_coarse_apply<<<cgrid, 32, 0, st>>>(s->cdom_start.p, s->cdom_nodes.p, s->dom_start.p, s->dom_verts.p,
+                                       s->cfac_off.p, s->cfac.p, r, s->ec.p, s->ncdom, dot ? dot->sc : nullptr);
+  const uint32_t nb = s->a->nb;
+  const uint32_t pgrid = std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(nb, 256), 8u * (uint32_t)s->a->ctx->sm_count));
+  const int wd = dot ? 1 : 0;
+  if (mixed)
+    k_prolong<double><<<pgrid, 256, 0, st>>>(r, z, s->ec.p, s->dom_of.p, nb, s->weight, d, wd);
+  else
+    k_prolong<float><<<pgrid, 256, 0, st>>>(r, z, s->ec.p, s->dom_of.p, nb, s->weight, d, wd);
+  MG_CUDA(cudaGetLastError());
   return MGUSO_OK;
 }
 

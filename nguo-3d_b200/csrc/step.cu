@@ -126,7 +126,8 @@ static int linear_solve(Scene& s, uint32_t active, mguso_lin_stats* ls) {
   } else {
     MG_TRY(blockjacobi_factor(s.A.get(), s.bjinv.p, st));
   }
-  if (s.p.pcg_mode == 0 || s.p.pcg_mode == 2 || s.ninst > 1) {
+  const bool two_level = s.schwarz && s.schwarz->levels == 2;
+  if (!two_level && (s.p.pcg_mode == 0 || s.p.pcg_mode == 2 || s.ninst > 1)) {
     PcgInstResult r[PCG_MAX_INST] = {};
     int rc = s.p.pcg_mode == 2 ? pcg_persistent(s, s.inst_vert.data(), s.ninst, active, r)
                                : pcg_fused(s, s.inst_vert.data(), s.ninst, active, r);

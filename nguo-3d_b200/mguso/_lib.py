@@ -69,6 +69,7 @@ def load() -> C.CDLL:
         "mguso_ctx_destroy": (i32, [vp]),
         "mguso_ctx_stream": (vp, [vp]),
         "mguso_linear_solver_create": (i32, [vp, i32, u32, i32, P(vp)]),
+        "mguso_linear_solver_create_ml": (i32, [vp, u32, C.c_float, i32, P(vp)]),
         "mguso_linear_solver_destroy": (i32, [vp]),
         "mguso_linear_solve": (i32, [vp, P(CsrDesc), vp, f32, u32, vp, P(LinStats)]),
         "mguso_bsr_create_from_csr": (i32, [vp, P(CsrDesc), P(vp)]),
@@ -81,6 +82,8 @@ def load() -> C.CDLL:
         "mguso_bsr_autotune": (i32, [vp, P(f32)]),
         "mguso_bsr_kernel": (i32, [vp, P(C.c_int), P(C.c_int), P(C.c_int)]),
         "mguso_schwarz_create": (i32, [vp, u32, P(vp)]),
+        "mguso_schwarz_create_ml": (i32, [vp, u32, C.c_float, P(vp)]),
+        "mguso_schwarz_coarse_domains": (i32, [vp, vp]),
         "mguso_schwarz_destroy": (i32, [vp]),
         "mguso_schwarz_info": (i32, [vp, P(u32), P(u64)]),
         "mguso_schwarz_factor": (i32, [vp, vp]),

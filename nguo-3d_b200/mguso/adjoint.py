@@ -29,6 +29,7 @@ def _adj_sigs(lib):
         ("mguso_adjoint_destroy", i32, [vp]),
         ("mguso_adjoint_forward", i32, [vp, vp, C.c_uint32, C.c_uint32, vp, vp]),
         ("mguso_adjoint_backward", i32, [vp, vp, vp]),
+        ("mguso_adjoint_states", i32, [vp, vp, vp]),
     ]:
         fn = getattr(lib, name)
         fn.restype = res
@@ -89,6 +90,15 @@ class AdjointDrape:
         out = np.empty(self.nparams, np.float64)
         check(self.lib.mguso_adjoint_backward(self.h, ptr(g), ptr(out)))
         return out
+
+    def states(self):
+        """(x, v) of the last forward pass, each (nsteps + 1, nv, 3), recomputed from its
+        checkpoints as the backward pass recomputes them."""
+        n = len(self.stats)
+        x = np.empty((n + 1, self.nv, 3), np.float32)
+        v = np.empty((n + 1, self.nv, 3), np.float32)
+        check(self.lib.mguso_adjoint_states(self.h, ptr(x), ptr(v)))
+        return x, v
 
     def close(self):
         if self.h:

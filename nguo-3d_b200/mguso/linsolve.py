@@ -66,18 +66,23 @@ class Context:
 class CudaLinearSolver:
     """A ``LinearSolver`` whose solve is the device PCG.
 
-    ``precond`` is ``"schwarz"`` (SchwarzCpu(domain), linsolve.rs:463-520) or ``"block"``
-    (CgCpu's block Jacobi, linsolve.rs:413-442). ``precision`` is ``"mixed"`` (FP64 dot
-    products and norms) or ``"fp32"``.
+    ``precond`` is ``"schwarz"`` (SchwarzCpu(domain), linsolve.rs:463-520), ``"schwarz-ml"``
+    (SchwarzMlCpu(domain, weight), the two-level Galerkin form, linsolve.rs:779-836) or
+    ``"block"`` (CgCpu's block Jacobi, linsolve.rs:413-442). ``precision`` is ``"mixed"`` (FP64
+    dot products and norms) or ``"fp32"``.
     """
 
-    def __init__(self, ctx: Context, precond: str = "schwarz", domain: int = 32, precision: str = "mixed"):
+    def __init__(self, ctx: Context, precond: str = "schwarz", domain: int = 32, precision: str = "mixed",
+                 weight: float = 0.7):
         self.ctx = ctx
         self.lib = ctx.lib
-        pc = {"schwarz": _lib.PRECOND_SCHWARZ, "block": _lib.PRECOND_BLOCK_JACOBI}[precond]
         pr = {"mixed": _lib.PRECISION_MIXED, "fp32": _lib.PRECISION_FP32}[precision]
         h = C.c_void_p()
-        check(self.lib.mguso_linear_solver_create(ctx.h, pc, domain, pr, C.byref(h)))
+        if precond == "schwarz-ml":
+            check(self.lib.mguso_linear_solver_create_ml(ctx.h, domain, C.c_float(weight), pr, C.byref(h)))
+        else:
+            pc = {"schwarz": _lib.PRECOND_SCHWARZ, "block": _lib.PRECOND_BLOCK_JACOBI}[precond]
+            check(self.lib.mguso_linear_solver_create(ctx.h, pc, domain, pr, C.byref(h)))
         self.h = h
         self._stats = LinearStats()
 
@@ -179,13 +184,19 @@ class Bsr:
 
 
 class Schwarz:
-    """One-level additive Schwarz over a device BSR (linsolve.rs:126-258)."""
+    """Additive Schwarz over a device BSR: one level (linsolve.rs:126-258), or with
+    ``levels=2`` the two-level Galerkin form z = S0 r + weight C1^T S1 (C1 r)
+    (MultilevelSchwarz, linsolve.rs:534-666)."""
 
-    def __init__(self, a: Bsr, domain: int = 32):
+    def __init__(self, a: Bsr, domain: int = 32, levels: int = 1, weight: float = 0.7):
         self.a = a
         self.lib = a.lib
+        self.levels = levels
         h = C.c_void_p()
-        check(self.lib.mguso_schwarz_create(a.h, domain, C.byref(h)))
+        if levels == 2:
+            check(self.lib.mguso_schwarz_create_ml(a.h, domain, C.c_float(weight), C.byref(h)))
+        else:
+            check(self.lib.mguso_schwarz_create(a.h, domain, C.byref(h)))
         self.h = h
         nd, fb = C.c_uint32(), C.c_uint64()
         check(self.lib.mguso_schwarz_info(h, C.byref(nd), C.byref(fb)))
@@ -200,6 +211,12 @@ class Schwarz:
     def domains(self) -> np.ndarray:
         out = np.empty(self.a.nb, dtype=np.uint32)
         check(self.lib.mguso_schwarz_domains(self.h, ptr(out)))
+        return out
+
+    def coarse_domains(self) -> np.ndarray:
+        """Coarse domain of every coarse node (= level-0 domain); two levels only."""
+        out = np.empty(self.ndomains, dtype=np.uint32)
+        check(self.lib.mguso_schwarz_coarse_domains(self.h, ptr(out)))
         return out
 
     def close(self):

@@ -1728,7 +1728,9 @@ struct ImplicitSolver {
   }
 
   // self_collision_stencils (implicit.rs:678-753)
-  std::vector<Stencil<R>> self_collision_stencils(const std::vector<V>& x) const {
+  // kinds (optional, one per stencil, test infrastructure for the adjoint): 0 vertex-triangle,
+  // 1 vertex against a static collider triangle (signed, outside), 3 the same inside, 2 edge-edge
+  std::vector<Stencil<R>> self_collision_stencils(const std::vector<V>& x, std::vector<uint8_t>* kinds = nullptr) const {
     R dhat = params.contact_dhat;
     std::vector<Stencil<R>> out;
     auto mov = movable_mask();
@@ -1742,13 +1744,15 @@ struct ImplicitSolver {
       const Tri& t = collision_tris[pr.second];
       Stencil<R> s;
       s.idx[0] = pr.first; s.idx[1] = t[0]; s.idx[2] = t[1]; s.idx[3] = t[2];
-      if (is_collider_tri(s.idx))
+      const bool col = is_collider_tri(s.idx);
+      if (col)
         s.d = signed_point_tri_distance_grad(x[s.idx[0]], x[s.idx[1]], x[s.idx[2]], x[s.idx[3]], side[s.idx[0]] < 0, s.g);
       else
         s.d = point_tri_distance_grad(x[s.idx[0]], x[s.idx[1]], x[s.idx[2]], x[s.idx[3]], s.g);
       if (s.d >= dhat) continue;
       s.ghat = dhat;
       out.push_back(s);
+      if (kinds) kinds->push_back(col ? (side[s.idx[0]] < 0 ? 3 : 1) : 0);
     }
     R ee_search = dhat;  // max_edge_gap() + 2 * max_edge_offset() with face edges only
     std::vector<std::pair<uint32_t, uint32_t>> ee;
@@ -1765,6 +1769,7 @@ struct ImplicitSolver {
       if (s.d >= pair_ghat) continue;
       s.ghat = pair_ghat;
       out.push_back(s);
+      if (kinds) kinds->push_back(2);
     }
     return out;
   }
@@ -1776,7 +1781,9 @@ struct ImplicitSolver {
     std::vector<std::array<R, 9>> blocks;
     std::vector<std::array<R, 9>> diag;
     const std::vector<uint8_t>* pinned;
+    bool grad_only = false;
     void push(uint32_t r, uint32_t c, R v) {
+      if (grad_only) return;
       if (!diag.empty() && r / 3 == c / 3) diag[r / 3][3 * (r % 3) + (c % 3)] += v;
       if (!slots->empty()) {
         auto it = slots->find(((uint64_t)(r / 3) << 32) | (c / 3));
@@ -1811,6 +1818,60 @@ struct ImplicitSolver {
     return k > 0 ? k : params.contact_kappa;
   }
 
+  // Test infrastructure for the FP64 adjoint: the mass part of a stencil's Rayleigh
+  // stiffness, sum_a m_a w_a^2 / (sum_a w_a^2 d^2) (0 when the stiffness fell back to kappa).
+  R rayleigh_mass_part(const Stencil<R>& s, R k_used) const {
+    R nlen = s.g[0].length();
+    if (nlen < R(1.0e-12) || k_used == params.contact_kappa) return 0;
+    V nrm = s.g[0] / nlen;
+    R m_max = 0, ws = 0, acc = 0, mass[4], w[4];
+    for (int a = 0; a < 4; ++a) {
+      w[a] = s.g[a].dot(nrm);
+      R im = inv_mass[s.idx[a]];
+      mass[a] = im > 0 ? R(1) / im : R(0);
+      m_max = rmax(m_max, mass[a]);
+    }
+    for (int a = 0; a < 4; ++a) {
+      ws += w[a] * w[a];
+      acc += (mass[a] > 0 ? mass[a] : m_max) * w[a] * w[a];
+    }
+    return ws > 0 ? acc / ws / (s.d * s.d) : R(0);
+  }
+
+  // Adjoint support (test infrastructure): a frozen contact set, each stencil with its kind
+  // (as self_collision_stencils reports it) and its stiffness split into an elastic part held
+  // fixed and a mass part that goes as 1/d^2 from its value km at gap d0; when set, the
+  // assembly recomputes these stencils' gaps and gradients at its x instead of collecting
+  // stencils. grad_only skips the Hessian. record_contacts keeps (stiffness, mass part) of
+  // every stencil the assembly used.
+  struct FrozenContact {
+    uint32_t idx[4];
+    uint8_t kind;
+    R ghat, k_el, km, d0;
+  };
+  const std::vector<FrozenContact>* frozen = nullptr;
+  bool grad_only = false;
+  bool record_contacts = false;
+  std::vector<std::array<R, 2>> contact_rec;
+
+  std::vector<Stencil<R>> frozen_stencils(const std::vector<V>& x) const {
+    std::vector<Stencil<R>> out(frozen->size());
+    for (size_t i = 0; i < frozen->size(); ++i) {
+      const FrozenContact& f = (*frozen)[i];
+      Stencil<R>& s = out[i];
+      for (int a = 0; a < 4; ++a) s.idx[a] = f.idx[a];
+      const V &p0 = x[f.idx[0]], &p1 = x[f.idx[1]], &p2 = x[f.idx[2]], &p3 = x[f.idx[3]];
+      if (f.kind == 2)
+        s.d = segment_segment_distance_grad(p0, p1, p2, p3, s.g);
+      else if (f.kind == 0)
+        s.d = point_tri_distance_grad(p0, p1, p2, p3, s.g);
+      else
+        s.d = signed_point_tri_distance_grad(p0, p1, p2, p3, f.kind == 3, s.g);
+      s.ghat = f.ghat;
+    }
+    return out;
+  }
+
   // assemble (implicit.rs:2280-3155), restricted to the element kinds listed in the header
   CsrT<R> assemble(const std::vector<V>& x, const std::vector<V>& x_tilde, R inv_h2, std::vector<R>& rhs,
                    uint32_t* nstencils) {
@@ -1821,8 +1882,10 @@ struct ImplicitSolver {
     std::vector<R> grad(ndof, R(0));
     std::vector<uint8_t> pinned(n);
     for (size_t i = 0; i < n; ++i) pinned[i] = inv_mass[i] <= 0;
-    std::vector<Stencil<R>> sc = params.self_collision ? self_collision_stencils(x) : std::vector<Stencil<R>>();
+    std::vector<Stencil<R>> sc = frozen ? frozen_stencils(x)
+                                        : (params.self_collision ? self_collision_stencils(x) : std::vector<Stencil<R>>());
     if (nstencils) *nstencils = (uint32_t)sc.size();
+    if (record_contacts) contact_rec.clear();
     bool want_diag = !pins.empty() || !pulls.empty() || (!colliders.empty() && params.contact_rayleigh);
     std::unordered_map<uint64_t, size_t> slots;
     for (auto& f : sl_faces)
@@ -1845,6 +1908,7 @@ struct ImplicitSolver {
         }
     Asm trips;
     trips.sink = &sink;
+    trips.grad_only = grad_only;
     trips.slots = &slots;
     trips.blocks.assign(slots.size(), std::array<R, 9>{});
     if (want_diag) trips.diag.assign(n, std::array<R, 9>{});
@@ -2122,8 +2186,16 @@ struct ImplicitSolver {
     // self contact (implicit.rs:3026-3103)
     if (!sc.empty()) {
       auto blocks = trips.blocks;
-      for (auto& s : sc) {
-        R kk = self_contact_rayleigh(blocks, slots, s);
+      for (size_t si = 0; si < sc.size(); ++si) {
+        const Stencil<R>& s = sc[si];
+        R kk;
+        if (frozen) {
+          const FrozenContact& f = (*frozen)[si];
+          kk = f.k_el + (f.km > 0 ? f.km * (f.d0 * f.d0) / (s.d * s.d) : R(0));
+        } else {
+          kk = self_contact_rayleigh(blocks, slots, s);
+        }
+        if (record_contacts) contact_rec.push_back({kk, rayleigh_mass_part(s, kk)});
         BarrierKind kind = s.d < 0 ? BarrierKind::Cubic : params.barrier_kind;
         R e, bg, bh;
         if (!barrier_of(kind, s.d, s.ghat, kk, e, bg, bh)) continue;
@@ -2167,6 +2239,7 @@ struct ImplicitSolver {
     for (size_t i = 0; i < n; ++i)
       if (pinned[i])
         for (int c = 0; c < 3; ++c) rhs[3 * i + c] = 0;
+    if (grad_only) return CsrT<R>();
     return sink.finish(pinned);
   }
 

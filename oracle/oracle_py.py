@@ -296,6 +296,7 @@ def _step_sigs(lib):
         "oracle_vertex_contact": (None, [vp, u32, vp, f32, f32, f32, f32, vp, vp]),
         "oracle_dynamic_stiffness": (f32, [f32, f32, f32, f32, f32]),
         "oracle_stencil_friction": (i32, [vp, vp, f32, f32, f32, vp, vp]),
+        "oracle_adjoint_system": (i32, [vp, u32, u32, vp, vp, vp, vp, vp, vp, vp, vp, C.c_double, vp, vp]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -740,3 +741,56 @@ def membrane_materials(w, wu, wv, clamp=True):
     m9, m36 = np.zeros(9, np.float32), np.zeros(36, np.float32)
     lib.oracle_membrane_materials(_p(a), _p(b), _p(c), 1 if clamp else 0, _p(m9), _p(m36))
     return m9.reshape(3, 3), m36.reshape(4, 3, 3)
+
+
+def adjoint_system(o: "OracleSolver", scene: dict, theta, xn, vn, xn1, npanel=2, nseam=2, eps=1e-7):
+    """One step's adjoint system in FP64 (oracle_adjoint_system): H = dG/dx (n3 x n3) and
+    dG/dtheta ((3 npanel + nseam) x n3) of the step's equilibrium residual at x_{n+1}, with
+    the contact set and the stiffnesses' elastic parts of x_{n+1} held fixed; the stencil count."""
+    n3 = 3 * o.nv
+    npar = 3 * npanel + nseam
+    uv = np.ascontiguousarray(scene["shell_uv"], np.float32)
+    panel = np.ascontiguousarray(scene["shell_panel"], np.uint8)
+    seam = np.ascontiguousarray(scene["stitch_seam"], np.uint8)
+    k0 = np.ascontiguousarray(np.asarray(scene["stitch_kl"], np.float64)[:, 0])
+    th = np.ascontiguousarray(theta, np.float64)
+    H = np.empty((n3, n3), np.float64)
+    dG = np.empty((npar, n3), np.float64)
+    a = [np.ascontiguousarray(v, np.float64).reshape(-1) for v in (xn, vn, xn1)]
+    nst = o.lib.oracle_adjoint_system(o.h, npanel, nseam, _p(uv), _p(panel), _p(seam), _p(k0), _p(th), _p(a[0]),
+                                      _p(a[1]), _p(a[2]), C.c_double(eps), _p(H), _p(dG))
+    if nst < 0:
+        raise ValueError("the adjoint system needs an FP64 oracle solver")
+    return H, dG, nst
+
+
+def fp64_adjoint(scene: dict, theta, xs, vs, dl_dx, npanel=2, nseam=2, eps=1e-7):
+    """dL/dtheta of an N-step drape in FP64 on the CPU, along the given trajectory
+    (xs, vs: (N + 1, nv, 3), the states the GPU forward pass went through): backwards through
+    every step, w = H^-1 (a_x + a_v / h) by a dense LU of the free block of the
+    symmetrised H, dL/dtheta -= w . dG/dtheta, a_x <- M/h^2 w - a_v / h, a_v <- M/h w (pinned
+    rows 0). The same recursion the GPU adjoint runs, with every derivative in FP64."""
+    o = OracleSolver(scene, "f64")
+    im = np.asarray(scene["inv_mass"], np.float64)
+    free3 = np.repeat(im > 0, 3)
+    m3 = np.where(free3, 1.0 / np.where(im > 0, im, 1.0).repeat(3), 0.0)
+    h = float(scene["params"]["dt"])
+    ax = np.asarray(dl_dx, np.float64).reshape(-1).copy()
+    ax[~free3] = 0.0
+    av = np.zeros_like(ax)
+    grad = np.zeros(3 * npanel + nseam)
+    nstencils = []
+    f = np.flatnonzero(free3)
+    for n in range(len(xs) - 2, -1, -1):
+        H, dG, nst = adjoint_system(o, scene, theta, xs[n], vs[n], xs[n + 1], npanel, nseam, eps)
+        nstencils.append(nst)
+        Hf = H[np.ix_(f, f)]
+        Hf = 0.5 * (Hf + Hf.T)
+        b = ax + av / h
+        w = np.zeros_like(ax)
+        w[f] = np.linalg.solve(Hf, b[f])
+        grad -= dG @ w
+        ax = m3 / (h * h) * w - av / h
+        av = m3 / h * w
+    o.close()
+    return grad, nstencils[::-1]

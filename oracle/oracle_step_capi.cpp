@@ -858,4 +858,153 @@ void oracle_stitch(const double* x18, const double* w6, double l0, double lcap, 
     for (int c = 0; c < 3; ++c) grad18[3 * k + c] = g[k][c];
 }
 
+
+// ---- FP64 reference adjoint (test infrastructure) ---------------------------------------
+// One step's adjoint system, in FP64 on the oracle's assembly, at the converged state x_{n+1}
+// of step n (x_n, v_n its start): the Jacobian H = dG/dx and dG/dtheta of the step's
+// equilibrium residual G(x) = M/h^2 (x - x~) + grad Phi(x; theta) (implicit.rs:2280-3155
+// restated in FP64), x~ = x_n + h v_n + h^2 g on free vertices. The contact set is the one
+// collected at x_{n+1}, held fixed; each stencil's stiffness is split into its elastic part,
+// held fixed, and its mass part, which goes as 1/d^2 from its value at x_{n+1} (the
+// definition of the GPU adjoint's exact Hessian). Both derivatives are central differences
+// of G: H column by column, many columns at once by a distance-2 colouring of the vertices'
+// element graph (shells, hinges, stitches, stretch edges, stencils), step eps; dG/dtheta
+// parameter by parameter, step 1e-6 theta_j. theta = [stiff_p (P), warp_p, weft_p (2P),
+// seam_q (S)]: shell (mu, lambda) = base * stiff_p, rest shape = pattern triangle scaled by
+// (weft, warp) along (u, v), stitch stiffness = base * seam_q.
+// H is n3 x n3 row-major (pinned rows and columns 0), dG is (3P + S) x n3. Returns the
+// number of stencils, or -1 for a float solver.
+int oracle_adjoint_system(void* h, uint32_t npanel, uint32_t nseam, const float* uv, const uint8_t* panel,
+                          const uint8_t* seam, const double* stitch_k0, const double* theta, const double* xn,
+                          const double* vn, const double* xn1, double eps, double* H, double* dG) {
+  auto* any = (AnySolver*)h;
+  if (any->prec != 1) return -1;
+  ImplicitSolver<double>& s = *any->d;
+  using V = Vt<double>;
+  const size_t nv = s.positions.size(), n3 = 3 * nv;
+  const uint32_t P = npanel, S = nseam, np = 3 * P + S;
+  const double mu0 = s.params.shell_mu, lam0 = s.params.shell_lambda;
+  std::vector<double> th(theta, theta + np);
+  auto apply_theta = [&](const std::vector<double>& t) {
+    s.shell_k.resize(s.shells.size());
+    for (size_t f = 0; f < s.shells.size(); ++f) {
+      const uint32_t p = panel[f];
+      const double su = t[P + 2 * p + 1], sv = t[P + 2 * p];
+      const float* q = uv + 6 * f;
+      const double xx = su * ((double)q[2] - (double)q[0]), xy = sv * ((double)q[3] - (double)q[1]);
+      const double yx = su * ((double)q[4] - (double)q[0]), yy = sv * ((double)q[5] - (double)q[1]);
+      const double det = xx * yy - yx * xy;
+      s.shells[f].dm_inv = Mat2<double>{yy / det, -xy / det, -yx / det, xx / det};
+      s.shells[f].area = 0.5 * std::fabs(det);
+      s.shell_k[f] = {mu0 * t[p], lam0 * t[p]};
+    }
+    for (size_t i = 0; i < s.stitches.size(); ++i) s.stitches[i].stiffness = stitch_k0[i] * t[3 * P + seam[i]];
+  };
+  apply_theta(th);
+  const double dt = s.params.dt, inv_h2 = 1.0 / (dt * dt);
+  std::vector<V> x0(nv), x1(nv), xt(nv);
+  for (size_t i = 0; i < nv; ++i) {
+    x0[i] = V(xn[3 * i], xn[3 * i + 1], xn[3 * i + 2]);
+    x1[i] = V(xn1[3 * i], xn1[3 * i + 1], xn1[3 * i + 2]);
+    const V v(vn[3 * i], vn[3 * i + 1], vn[3 * i + 2]);
+    xt[i] = s.inv_mass[i] > 0 ? x0[i] + v * dt + s.params.gravity * (dt * dt) : x0[i];
+  }
+  // stencils at x_{n+1}, their kinds and the stiffnesses the step's assembly gives them
+  std::vector<uint8_t> kinds;
+  std::vector<Stencil<double>> sts =
+      s.params.self_collision ? s.self_collision_stencils(x1, &kinds) : std::vector<Stencil<double>>();
+  std::vector<double> rhs;
+  s.frozen = nullptr;
+  s.grad_only = false;
+  s.record_contacts = true;
+  s.assemble(x1, xt, inv_h2, rhs, nullptr);
+  s.record_contacts = false;
+  using FC = typename ImplicitSolver<double>::FrozenContact;
+  std::vector<FC> fr(sts.size());
+  for (size_t i = 0; i < sts.size(); ++i) {
+    FC& f = fr[i];
+    for (int a = 0; a < 4; ++a) f.idx[a] = sts[i].idx[a];
+    f.kind = kinds[i];
+    f.ghat = sts[i].ghat;
+    f.k_el = s.contact_rec[i][0] - s.contact_rec[i][1];
+    f.km = s.contact_rec[i][1];
+    f.d0 = sts[i].d;
+  }
+  s.frozen = &fr;
+  s.grad_only = true;
+  std::vector<double> gp(n3), gm(n3);
+  auto G = [&](const std::vector<V>& x, std::vector<double>& out) {
+    s.assemble(x, xt, inv_h2, rhs, nullptr);
+    for (size_t i = 0; i < n3; ++i) out[i] = -rhs[i];
+  };
+  // vertex coupling graph
+  std::vector<std::vector<uint32_t>> nb(nv);
+  auto couple = [&](const uint32_t* v, int k) {
+    for (int a = 0; a < k; ++a)
+      for (int b = 0; b < k; ++b) nb[v[a]].push_back(v[b]);
+  };
+  for (auto& sh : s.shells) couple(sh.v, 3);
+  for (auto& hg : s.hinges) couple(hg.v, 4);
+  for (auto& st : s.stitches) couple(st.index, 6);
+  for (auto& e : s.stretch_edges) couple(e.data(), 2);
+  for (auto& f : fr) couple(f.idx, 4);
+  for (size_t i = 0; i < nv; ++i) {
+    nb[i].push_back((uint32_t)i);
+    std::sort(nb[i].begin(), nb[i].end());
+    nb[i].erase(std::unique(nb[i].begin(), nb[i].end()), nb[i].end());
+  }
+  // greedy distance-2 colouring of the free vertices
+  std::vector<int> color(nv, -1);
+  int ncolor = 0;
+  std::vector<int> mark;
+  for (size_t j = 0; j < nv; ++j) {
+    if (!(s.inv_mass[j] > 0)) continue;
+    mark.assign(ncolor + 1, 0);
+    for (uint32_t a : nb[j])
+      for (uint32_t b : nb[a])
+        if (color[b] >= 0) mark[color[b]] = 1;
+    int c = 0;
+    while (mark[c]) ++c;
+    color[j] = c;
+    ncolor = std::max(ncolor, c + 1);
+  }
+  std::fill(H, H + n3 * n3, 0.0);
+  std::vector<V> xp(x1), xm(x1);
+  for (int c = 0; c < ncolor; ++c)
+    for (int k = 0; k < 3; ++k) {
+      xp = x1;
+      xm = x1;
+      for (size_t j = 0; j < nv; ++j)
+        if (color[j] == c) {
+          xp[j][k] += eps;
+          xm[j][k] -= eps;
+        }
+      G(xp, gp);
+      G(xm, gm);
+      for (size_t j = 0; j < nv; ++j) {
+        if (color[j] != c) continue;
+        for (uint32_t i : nb[j]) {
+          if (!(s.inv_mass[i] > 0)) continue;
+          for (int r = 0; r < 3; ++r) H[(3 * i + r) * n3 + 3 * j + k] = (gp[3 * i + r] - gm[3 * i + r]) / (2 * eps);
+        }
+      }
+    }
+  // parameter partials
+  for (uint32_t j = 0; j < np; ++j) {
+    const double d = 1e-6 * th[j];
+    std::vector<double> t = th;
+    t[j] = th[j] + d;
+    apply_theta(t);
+    G(x1, gp);
+    t[j] = th[j] - d;
+    apply_theta(t);
+    G(x1, gm);
+    for (size_t i = 0; i < n3; ++i) dG[(size_t)j * n3 + i] = (gp[i] - gm[i]) / (2 * d);
+  }
+  apply_theta(th);
+  s.frozen = nullptr;
+  s.grad_only = false;
+  return (int)fr.size();
+}
+
 }  // extern "C"

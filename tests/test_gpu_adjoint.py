@@ -1,9 +1,15 @@
-"""The adjoint of a drape (mguso_adjoint_forward/backward) against golden central finite
-differences (eps = 1e-4) of the FP64 oracle's landmark loss (tests/golden/make_adjoint_fd.py):
-the XS sheath at 5 cm edges draped onto its torso with self contact, 24 steps with checkpoints
-every 6, the 8 pattern parameters (2 panel stiffnesses, warp/weft
-rest scales of 2 panels, 2 seam stiffnesses), targets from a forward pass at parameters raised
-by 5%. Errors are relative to the largest finite difference."""
+"""The adjoint of a drape (mguso_adjoint_forward/backward) on the XS sheath at 5 cm edges
+draped onto its torso with self contact, 24 steps with checkpoints every 6, the 8 pattern
+parameters (2 panel stiffnesses, warp/weft rest scales of 2 panels, 2 seam stiffnesses),
+targets from a forward pass at parameters raised by 5%:
+
+- against the oracle's FP64 CPU adjoint (oracle_py.fp64_adjoint) along the same trajectory
+  (the GPU forward's states, recomputed from its checkpoints), within 1e-3 of the largest
+  entry: the same recursion with every derivative taken in FP64 by central differences of the
+  oracle's step residual;
+- against golden central finite differences (eps = 1e-4) of the FP64 oracle's landmark loss
+  (tests/golden/make_adjoint_fd.py), a sanity check at the differences' own noise level.
+Errors are relative to the largest entry of the reference."""
 import os
 import sys
 
@@ -48,3 +54,26 @@ def test_adjoint_matches_fp64_finite_differences(ctx, name):
     print(name, "adjoint", g, "\nfd at eps 1e-4", z["fd"], "\nfd at eps 1e-5", z["fd_fine"],
           "\nerror / max|fd| against", REF[name], err)
     assert err.max() <= TOL[name], err
+
+
+@pytest.mark.parametrize("name", ["coarse"])
+def test_adjoint_matches_fp64_cpu_adjoint(ctx, name):
+    import oracle_py as O
+
+    path = os.path.join(HERE, "golden", f"adjoint_fd_{name}.npz")
+    if not os.path.exists(path):
+        pytest.skip(f"no golden targets for {name}")
+    z = np.load(path)
+    sc, lm = adjoint_scene(name)
+    d = AdjointDrape(ctx, sc, "mixed")
+    x = d.forward(z["theta"], int(z["steps"]), int(z["every"]))
+    xs, vs = d.states()
+    assert np.array_equal(xs[-1], x)
+    dl = np.zeros_like(x)
+    dl[lm] = 2.0 * (x[lm] - z["target"])
+    g = d.backward(dl)
+    ref, nst = O.fp64_adjoint(sc, z["theta"], xs.astype(np.float64), vs.astype(np.float64), dl.astype(np.float64))
+    err = np.abs(g - ref) / np.abs(ref).max()
+    print(name, "adjoint", g, "\nfp64 cpu adjoint", ref, "\nstencils per step", nst, "\nerror / max|ref|", err)
+    assert max(nst) > 100
+    assert err.max() <= 1e-3, err
