@@ -388,6 +388,14 @@ int mguso_scene_profile(mguso_scene* s, int reps, float* us4, double* bytes4);
  * their algorithmic bytes per launch. Clobbers the PCG scratch (not the state). */
 int mguso_scene_profile_pcg(mguso_scene* s, int iters, float* us2, double* bytes2);
 
+/* The self-intersection scan behind mguso_step_stats.penetration_free
+ * (ImplicitSolver::has_self_intersection, implicit.rs:618-650): at positions x (host
+ * f32[3 nv]; the scene's positions are left at x), counts[k] gets instance k's number of
+ * (mesh edge, collision triangle) pairs that share no vertex, have a movable vertex, and
+ * where the edge crosses the triangle (edge_triangle_intersect, contact.rs:324-352). A step
+ * with self collision on runs the same scan at its committed positions. */
+int mguso_scene_self_intersections(mguso_scene* s, const float* x, uint32_t* counts);
+
 /* Assemble the Newton system once at positions x (f32[3 nv]) with inertia target x_tilde
    (f32[3 nv]; NULL means x), exactly as one Newton iteration of mguso_step does: contact
    stencils, elastic elements, colliders, contacts, right-hand side. The scene's positions

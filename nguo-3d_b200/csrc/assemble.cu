@@ -490,7 +490,8 @@ __global__ void k_contact_assemble(const Stencil* __restrict__ sts, uint32_t nst
                                    const uint32_t* __restrict__ ps_col, const float* __restrict__ vals,
                                    const uint32_t* __restrict__ pp_rp, const uint32_t* __restrict__ pp_col,
                                    const float* __restrict__ valp, float kappa, int barrier_kind, float mu, float feps,
-                                   float* __restrict__ ccb, unsigned long long* __restrict__ ckeys,
+                                   const float* __restrict__ kin_dx, float* __restrict__ ccb,
+                                   unsigned long long* __restrict__ ckeys,
                                    uint32_t* __restrict__ cids, float* __restrict__ cge,
                                    unsigned long long* __restrict__ gkeys, uint32_t* __restrict__ gids) {
   uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -515,7 +516,11 @@ __global__ void k_contact_assemble(const Stencil* __restrict__ sts, uint32_t nst
     V3<R> slip;
     for (int a = 0; a < 4; ++a) {
       w[a] = g[a].dot(n);
-      slip += (ld3<R>(x, S.idx[a]) - ld3<R>(x_start, S.idx[a])) * w[a];
+      // the slip is relative: a re-posed collider vertex adds the move it was given before
+      // this step (fdx_override, implicit.rs:3063-3078)
+      V3<R> dxa = ld3<R>(x, S.idx[a]) - ld3<R>(x_start, S.idx[a]);
+      if (kin_dx) dxa += ld3<R>(kin_dx, S.idx[a]);
+      slip += dxa * w[a];
     }
     fr = friction<R>(n * bg, slip, n, (R)mu, (R)feps, fg, fh);
     if (fr && fg.x == 0 && fg.y == 0 && fg.z == 0) fr = false;
@@ -845,14 +850,14 @@ int assemble_contacts(Scene& s, uint32_t nst) {
     k_contact_assemble<double><<<g, 64, 0, st>>>(s.stencils_sorted.p, nst, s.inv_mass.p, s.pinned.p, s.x.p, s.x0.p,
                                                  s.Ps.row_ptr.p, s.Ps.col.p, s.A->val.p, s.Pp.row_ptr.p, s.Pp.col.p,
                                                  s.valp.p, s.p.contact_kappa, s.p.barrier_kind, s.p.friction,
-                                                 s.p.friction_eps, s.ccblocks.p, s.ckeys.p, s.cids.p, s.cgentries.p,
-                                                 s.gkeys.p, s.gids.p);
+                                                 s.p.friction_eps, s.kin_dx_set ? s.kin_dx.p : nullptr, s.ccblocks.p,
+                                                 s.ckeys.p, s.cids.p, s.cgentries.p, s.gkeys.p, s.gids.p);
   else
     k_contact_assemble<float><<<g, 64, 0, st>>>(s.stencils_sorted.p, nst, s.inv_mass.p, s.pinned.p, s.x.p, s.x0.p,
                                                 s.Ps.row_ptr.p, s.Ps.col.p, s.A->val.p, s.Pp.row_ptr.p, s.Pp.col.p,
                                                 s.valp.p, s.p.contact_kappa, s.p.barrier_kind, s.p.friction,
-                                                s.p.friction_eps, s.ccblocks.p, s.ckeys.p, s.cids.p, s.cgentries.p,
-                                                s.gkeys.p, s.gids.p);
+                                                s.p.friction_eps, s.kin_dx_set ? s.kin_dx.p : nullptr, s.ccblocks.p,
+                                                s.ckeys.p, s.cids.p, s.cgentries.p, s.gkeys.p, s.gids.p);
   MG_CUDA(cudaGetLastError());
   // blocks: stable sort by (row, col); stencil order survives within equal keys
   MG_TRY(radix_sort_pairs(&s.sorter, s.ckeys.p, s.cids.p, mb, 64, st));

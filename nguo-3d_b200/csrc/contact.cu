@@ -102,6 +102,66 @@ int build_bvhs(Scene& s, const float* x) {
   return MGUSO_OK;
 }
 
+// ---- self intersection (has_self_intersection, implicit.rs:618-650) ------------------
+// edge_triangle_intersect (contact.rs:324-352) in FP32, in the reference's operation order
+// (this file is compiled without FMA contraction): the segment crosses the triangle's plane
+// strictly and the crossing point's barycentric coordinates are inside or on the boundary.
+__device__ __forceinline__ bool edge_triangle_intersect_f(V3<float> e0, V3<float> e1, V3<float> v0, V3<float> v1,
+                                                          V3<float> v2) {
+  const V3<float> d1 = v1 - v0, d2 = v2 - v0, a0 = e0 - v0, a1 = e1 - v0;
+  const V3<float> n = d1.cross(d2);
+  const float s1 = a0.dot(n), s2 = a1.dot(n);
+  if (!(s1 * s2 < 0.f)) return false;
+  const float t = s1 / (s1 - s2);
+  const V3<float> r = a0 * (1.f - t) + a1 * t;
+  const float a = d1.dot(d1), b = d1.dot(d2), c = d2.dot(d2);
+  const float det = a * c - b * b;
+  if (det == 0.f) return false;
+  const float p = d1.dot(r), q = d2.dot(r);
+  const float u = (c * p - b * q) / det, v = (a * q - b * p) / det;
+  return u >= 0.f && v >= 0.f && u + v <= 1.f;
+}
+
+// Every mesh edge against the triangles whose boxes overlap its own box (every piercing
+// pair is among them): pairs with a movable vertex that share no vertex, counted per
+// instance into red[RED_STRIDE k + 14].
+__global__ void k_self_intersect(BvhSet bv, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
+                                 const uint32_t* __restrict__ edges, const uint32_t* __restrict__ tris,
+                                 const float* __restrict__ im, uint32_t ne, unsigned int* __restrict__ red,
+                                 uint32_t* status) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ne) return;
+  const uint32_t e0 = edges[2 * j], e1 = edges[2 * j + 1];
+  float4 lo, hi;
+  edge_box(x, e0, e1, 0.f, lo, hi);
+  const bool emov = im[e0] > 0.f || im[e1] > 0.f;
+  const V3<float> p0 = ld3<float>(x, e0), p1 = ld3<float>(x, e1);
+  unsigned int hits = 0;
+  const bool ok = visit(bv, vinst[e0], lo, hi, [&](uint32_t t) {
+    const uint32_t a = tris[3 * t], b = tris[3 * t + 1], c = tris[3 * t + 2];
+    if (!emov && !(im[a] > 0.f || im[b] > 0.f || im[c] > 0.f)) return;
+    if (e0 == a || e0 == b || e0 == c || e1 == a || e1 == b || e1 == c) return;
+    if (edge_triangle_intersect_f(p0, p1, ld3<float>(x, a), ld3<float>(x, b), ld3<float>(x, c))) ++hits;
+  });
+  if (!ok) atomicOr(status, ST_STACK_OVERFLOW);
+  if (hits) atomicAdd(red + RED_STRIDE * vinst[e0] + 14, hits);
+}
+
+// Piercing (edge, triangle) pairs of every instance at the scene's positions x, counted into
+// red[RED_STRIDE k + 14] (which the caller zeroes); rebuilds the triangle BVHs at x.
+int self_intersections(Scene& s) {
+  if (s.n_edge == 0) return MGUSO_OK;
+  for (uint32_t k = 0; k < s.ninst; ++k) {
+    const uint32_t t0 = s.inst_tri[k];
+    MG_TRY(lbvh_build(s.tri_bvh[k].get(), s.x.p, s.nv, s.tris.p + 3 * (size_t)t0, s.inst_tri[k + 1] - t0, 30, s.st));
+  }
+  BvhSet tv = view_set(s.tri_bvh, s.inst_tri);
+  k_self_intersect<<<ceil_div(s.n_edge, 128), 128, 0, s.st>>>(tv, s.vinst.p, s.x.p, s.edges.p, s.tris.p, s.inv_mass.p,
+                                                             s.n_edge, s.red.p, s.status.p);
+  MG_CUDA(cudaGetLastError());
+  return MGUSO_OK;
+}
+
 // ---- collider sides ------------------------------------------------------------------
 // best (d2 bits, triangle) per non-static vertex over collider triangles within dhat; ties
 // go to the lowest triangle index, which is the first one the reference's triangle-major

@@ -735,14 +735,18 @@ int mguso_set_kinematic_collider_positions(mguso_scene* sc, const float* x) {
   MG_CUDA(cudaMemcpyAsync(vel.data(), s.v.p, 12 * (size_t)nv, cudaMemcpyDeviceToHost, s.st));
   MG_CUDA(cudaStreamSynchronize(s.st));
   const float inv_h = 1.0f / s.p.dt;
+  if (!s.kin_dx_set) s.h_kin_dx.assign(3 * (size_t)nv, 0.f);
   for (uint32_t i = 0; i < nv; ++i) {
     if (!s.h_static[i]) continue;
     for (int c = 0; c < 3; ++c) {
       const float dd = x[3 * i + c] - pos[3 * i + c];
       pos[3 * i + c] = x[3 * i + c];
       vel[3 * i + c] = dd * inv_h;
+      s.h_kin_dx[3 * i + c] += dd;  // accumulated until the next step consumes it
     }
   }
+  MG_TRY(s.kin_dx.upload(s.h_kin_dx.data(), s.h_kin_dx.size(), s.st));
+  s.kin_dx_set = true;
   std::vector<float> pn;
   collider_pseudonormals(pos.data(), nv, s.h_ctris, s.h_vinst, pn);
   MG_CUDA(cudaMemcpyAsync(s.x.p, pos.data(), 12 * (size_t)nv, cudaMemcpyHostToDevice, s.st));
@@ -998,5 +1002,27 @@ extern "C" int mguso_scene_profile_pcg(mguso_scene* sc, int iters, float* us2, d
     bytes2[1] = 36.0 * nv + 84.0 * nv;
   }
   return pcg_fused_profile(s, (uint32_t)iters, us2);
+}
+
+// Piercing (edge, triangle) pairs of every instance at positions x (host f32[3 nv]), the
+// self-intersection scan of penetration_free (has_self_intersection, implicit.rs:618-650);
+// the scene's positions are left at x.
+extern "C" int mguso_scene_self_intersections(mguso_scene* sc, const float* x, uint32_t* counts) {
+  MG_CHECK_ARG(sc && x && counts, "null argument");
+  Scene& s = sc->s;
+  MG_CUDA(cudaMemcpyAsync(s.x.p, x, 12 * (size_t)s.nv, cudaMemcpyHostToDevice, s.st));
+  MG_CUDA(cudaMemsetAsync(s.red.p, 0, 4 * RED_STRIDE * (size_t)s.ninst, s.st));
+  MG_TRY(self_intersections(s));
+  std::vector<unsigned int> h(RED_STRIDE * (size_t)s.ninst);
+  uint32_t st = 0;
+  MG_CUDA(cudaMemcpyAsync(h.data(), s.red.p, 4 * h.size(), cudaMemcpyDeviceToHost, s.st));
+  MG_CUDA(cudaMemcpyAsync(&st, s.status.p, 4, cudaMemcpyDeviceToHost, s.st));
+  MG_CUDA(cudaStreamSynchronize(s.st));
+  if (st & ST_STACK_OVERFLOW) {
+    set_error("self-intersection scan: BVH traversal stack overflow");
+    return MGUSO_ERR_BVH_STACK;
+  }
+  for (uint32_t k = 0; k < s.ninst; ++k) counts[k] = h[RED_STRIDE * k + 14];
+  return MGUSO_OK;
 }
 

@@ -80,6 +80,11 @@ struct Scene {
   // every vertex's instance (empty without a static collider)
   std::vector<uint8_t> h_static, h_vinst;
   std::vector<std::array<uint32_t, 3>> h_ctris;
+  // the collider's move since the last step (the friction slip of its vertices in the next
+  // step, implicit.rs:3063-3078), kept while kin_dx_set
+  std::vector<float> h_kin_dx;
+  DevBuf<float> kin_dx;
+  bool kin_dx_set = false;
   // Hessians the assembly writes: 0 the step's PSD-projected ones; 2 the exact ones (shells
   // without the eigenvalue clamp, stitches below rest length, hinges and barriers with their
   // second-derivative terms), the contact stiffness held at `contact_k` (2 per stencil:
@@ -197,6 +202,7 @@ int pcg_persistent(Scene& s, const uint32_t* h_inst_row, uint32_t ninst, uint32_
 int pcg_fused(Scene& s, const uint32_t* h_inst_row, uint32_t ninst, uint32_t active, PcgInstResult* out);
 int pcg_fused_profile(Scene& s, uint32_t iters, float* us2);
 int collect_stencils(Scene& s, uint32_t* nst);
+int self_intersections(Scene& s);  // piercing pairs per instance at s.x into red[RED_STRIDE k + 14]
 int ccd_step(Scene& s, uint32_t active, float* t_out, uint32_t* cap_hits);
 
 }  // namespace mg

@@ -278,6 +278,9 @@ int scene_step(Scene& s, mguso_step_stats* out) {
     k_collider_metrics<<<ceil_div(nv, 256), 256, 0, st>>>(s.x.p, s.inv_mass.p, s.vinst.p, nv, s.colliders.p, s.n_col,
                                                           s.p.contact_dhat, s.red.p);
   MG_CUDA(cudaGetLastError());
+  // the self-intersection scan of penetration_free (implicit.rs:2250-2258), with self
+  // collision on, at the committed positions
+  if (contacts) MG_TRY(self_intersections(s));
   MG_CUDA(cudaMemcpyAsync(hred.data(), s.red.p, 4 * hred.size(), cudaMemcpyDeviceToHost, st));
   uint32_t dev_status = 0;
   MG_CUDA(cudaMemcpyAsync(&dev_status, s.status.p, 4, cudaMemcpyDeviceToHost, st));
@@ -288,7 +291,7 @@ int scene_step(Scene& s, mguso_step_stats* out) {
     mguso_step_stats& o = stats[k];
     o.all_finite = m[11] == 0 ? 1 : 0;
     o.num_contacts = m[12];
-    o.penetration_free = (m[11] == 0 && m[13] == 0) ? 1 : 0;
+    o.penetration_free = (m[11] == 0 && m[13] == 0 && m[14] == 0) ? 1 : 0;
     o.status = m[11] ? MGUSO_ERR_NONFINITE : MGUSO_OK;
     if (dev_status & ST_STACK_OVERFLOW) o.status = MGUSO_ERR_BVH_STACK;
     if (dev_status & ST_WAIT_TIMEOUT) o.status = MGUSO_ERR_TIMEOUT;
@@ -297,6 +300,8 @@ int scene_step(Scene& s, mguso_step_stats* out) {
     if (out) out[k] = o;
   }
   MG_CUDA(cudaMemsetAsync(s.status.p, 0, 4, st));
+  // the collider move described this step only (implicit.rs:2065-2070)
+  s.kin_dx_set = false;
   return MGUSO_OK;
 }
 

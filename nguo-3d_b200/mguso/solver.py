@@ -64,6 +64,7 @@ def _sigs(lib):
         ("mguso_scene_ccd", i32, [vp, vp, vp, vp, vp]),
         ("mguso_scene_profile", i32, [vp, i32, vp, vp]),
         ("mguso_scene_profile_pcg", i32, [vp, i32, vp, vp]),
+        ("mguso_scene_self_intersections", i32, [vp, vp, vp]),
         ("mguso_batch_create", i32, [vp, vp, C.c_uint32, P(vp)]),
         ("mguso_scene_instances", i32, [vp, P(C.c_uint32), vp]),
         ("mguso_scene_system", i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
@@ -222,6 +223,14 @@ class ImplicitSolver:
         by = np.zeros(2, np.float64)
         check(self.lib.mguso_scene_profile_pcg(self.h, iters, ptr(us), ptr(by)))
         return {"rows": (float(us[0]), float(by[0])), "domains": (float(us[1]), float(by[1]))}
+
+    def self_intersections(self, x) -> np.ndarray:
+        """Piercing (edge, triangle) pairs per instance at positions ``x`` (the scan behind
+        penetration_free, implicit.rs:618-650); the scene's positions are left at ``x``."""
+        xx = np.ascontiguousarray(x, np.float32).reshape(self.nv, 3)
+        out = np.zeros(getattr(self, "ninst", 1), np.uint32)
+        check(self.lib.mguso_scene_self_intersections(self.h, ptr(xx), ptr(out)))
+        return out
 
     def ccd(self, x, dx):
         """Step fraction the CCD filter allows along ``dx`` from ``x`` (one per instance) and

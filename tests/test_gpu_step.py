@@ -27,10 +27,12 @@ def run_pair(ctx, sc, steps, precision="mixed"):
         g.positions = p0.astype(np.float32)
         g.velocities = v0.astype(np.float32)
         sg = g.step(1)[0]
-        so = o.step(1, check_intersection=False)[0]
+        so = o.step(1, check_intersection=True)[0]
         pg = g.positions.astype(np.float64)
         po = o.positions()
         disp = np.abs(po - p0).max() + 1e-12
+        # penetration_free includes the self-intersection scan on both sides
+        assert bool(sg["penetration_free"]) == bool(so["penetration_free"]), (k, sg, so)
         out.append((k, sg, so, np.abs(pg - po).max() / disp))
         print(f"step {k}: newton gpu {sg['newton_iters']} oracle {so['newton_iters']} stencils "
               f"{sg['stencils']}/{so['stencils']} t_min {sg['t_min']:.4f}/{so['t_min']:.4f} rel {out[-1][3]:.3e}")
@@ -316,3 +318,59 @@ def test_ccd_step_fraction_matches_oracle(ctx, precision):
         assert abs(float(t_gpu[0]) - t_o) <= 1e-4 * max(t_o, 1e-3), (mag, t_gpu, t_o)
     print(ts)
     assert min(t for _, _, t in ts) < 1.0  # some direction collides
+
+
+def _crossing_sheets(cross: bool, n=8):
+    """A horizontal sheet and a vertical one whose lower edge dips `cross`-ingly through it
+    (2 mm below the horizontal sheet) or stops 2 mm above it."""
+    sc = scenes.sheet_on_sphere(n, side=0.1, height=0.5, jitter=0.0, dhat=1e-3)
+    pos = sc["positions"].astype(np.float64)
+    v = pos.copy()
+    # rotate the copy into the vertical x-y plane through the sheet's middle
+    c = pos[:, [0, 2]].mean(0)
+    v[:, 1] = 0.5 + (pos[:, 2] - c[1]) + 0.05 + (-0.002 if cross else 0.002)
+    v[:, 2] = c[1] + 1e-4 * np.sin(7.0 * pos[:, 0])
+    sc["positions"] = np.concatenate([pos, v]).astype(np.float32)
+    sc["velocities"] = np.zeros_like(sc["positions"])
+    sc["tris"] = np.concatenate([sc["tris"], sc["tris"] + n * n]).astype(np.uint32)
+    sc["shell_faces"] = sc["tris"].copy()
+    sc["inv_mass"] = np.concatenate([sc["inv_mass"], sc["inv_mass"]])
+    sc["colliders"] = np.zeros((0, 8), np.float32)
+    return sc
+
+
+@pytest.mark.parametrize("cross", [True, False])
+def test_self_intersection_scan_matches_oracle(ctx, cross):
+    """has_self_intersection (implicit.rs:618-650) on the GPU (LBVH candidates, exact FP32
+    edge-triangle predicate) against the oracle's: two sheets that cross transversally and the
+    same sheets apart; then the flag through a step, where penetration_free must agree."""
+    sc = _crossing_sheets(cross)
+    g = ImplicitSolver(ctx, sc, "fp32")
+    o = O.OracleSolver(sc)
+    x = sc["positions"]
+    cnt = int(g.self_intersections(x)[0])
+    assert (cnt > 0) == o.self_intersects(x) == cross, (cnt, cross)
+    sg = g.step(1)[0]
+    so = o.step(1, check_intersection=True)[0]
+    assert bool(sg["penetration_free"]) == bool(so["penetration_free"]) == (not cross)
+
+
+def test_self_intersection_scan_on_perturbed_drapes(ctx):
+    """The scan's verdict equals the oracle's on a crumpled coarse sheath: its state after a
+    few steps (no crossing), then the same state with growing random displacements of the
+    free vertices (crossings appear)."""
+    sc = coarse_sheath()
+    g = ImplicitSolver(ctx, sc, "fp32")
+    o = O.OracleSolver(sc)
+    o.step(2, check_intersection=False)
+    x0 = o.positions().astype(np.float32)
+    free = np.asarray(sc["inv_mass"]) > 0
+    rng = np.random.default_rng(11)
+    verdicts = []
+    for mag in (0.0, 2e-3, 1e-2, 3e-2):
+        x = x0.copy()
+        x[free] += rng.normal(0, mag, (free.sum(), 3)).astype(np.float32)
+        cnt = int(g.self_intersections(x)[0])
+        assert (cnt > 0) == o.self_intersects(x), (mag, cnt)
+        verdicts.append(cnt > 0)
+    assert verdicts[0] is False and verdicts[-1] is True
