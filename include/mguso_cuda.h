@@ -243,6 +243,11 @@ typedef struct {
                               1 = FP32 tiles, 2 = FP16 tiles */
   uint32_t schwarz_levels; /* 1 (or 0): one-level Schwarz (SchwarzCpu, linsolve.rs:463-520);
                               2: two-level Galerkin Schwarz (SchwarzMlCpu, linsolve.rs:534-836) */
+  int pcg_variant;         /* kernels of the fused PCG (pcg_mode 0): 0 = chosen by the autotuner
+                              at the scene's first solve (cached per system size); v >= 1 fixes
+                              the rows kernel (v - 1) / 4 (2, 1 or 4 lanes per block row) and the
+                              Schwarz domain kernel (v - 1) % 4 (one warp per domain, 4 per CTA;
+                              three warps per domain, 1, 2 or 4 domains per CTA) */
   float schwarz_weight;    /* coarse-correction weight w of the two-level form
                               z = S0 r + w C1^T S1 (C1 r) (the CLI default 0.7, main.rs:761-763) */
 } mguso_params;

@@ -15,6 +15,8 @@
 // kernel launched after every instance converged returns at entry.
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "reduce.cuh"
@@ -24,8 +26,7 @@
 namespace mg {
 
 constexpr int FR_THREADS = 256;
-constexpr int FR_LPR = 2;          // lanes per block row (4 and 8 measured slower on the batch)
-constexpr int FD_WARPS = 4;        // Schwarz: warps (domains) per CTA
+constexpr int FD_WARPS = 4;        // Schwarz, one warp per domain: warps (domains) per CTA
 constexpr int FD_THREADS = 256;    // block Jacobi: vertices per CTA
 constexpr uint32_t FUSED_CHECK = 16;
 
@@ -74,7 +75,7 @@ __device__ __forceinline__ bool last_cta(uint32_t* counter) {
   return s_last;
 }
 
-template <class Acc>
+template <class Acc, int FR_LPR>
 __global__ void __launch_bounds__(FR_THREADS) k_fr_rows(FusedArgs a, const float* __restrict__ po,
                                                         float* __restrict__ pn) {
   if (a.ctl->all_done) return;
@@ -292,6 +293,165 @@ __global__ void __launch_bounds__(32 * FD_WARPS) k_fr_schwarz(FusedArgs a, const
   fd_finish(a, init != 0);
 }
 
+// Schwarz domains with three warps per domain, DOMS domains per CTA. The domain's tiles
+// (storage order (0,0), (1,0), (1,1), (2,0), (2,1), (2,2)) are split between the warps, warp
+// q taking tiles q and q + 3: each warp forms its tiles' partial W r rows, the partials are
+// summed per tile row in a fixed order into y = W r, each warp forms its tiles' partial
+// W^T y columns, and those are summed per tile column into z. Compared with one warp per
+// domain, the chain of dependent tile passes per domain is a third as long and three times
+// as many warps share the same shared memory. The sums are deterministic.
+template <class Acc, class TS>
+__host__ __device__ constexpr uint32_t f3_slice_bytes() {
+  return (6 * TILE_FLOATS * (uint32_t)sizeof(TS) + 96 * 4 + 3 * 2 * 32 * (uint32_t)sizeof(Acc) +
+          96 * (uint32_t)sizeof(Acc) + 127) / 128 * 128;
+}
+
+__device__ __forceinline__ void named_sync(int id, int threads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+
+// tile t's row and column block, and the tiles of warp q (slot 0, 1; -1 none) for T tile rows
+__device__ __forceinline__ int f3_tile_i(int t) { return t >= 3 ? 2 : (t >= 1 ? 1 : 0); }
+__device__ __forceinline__ int f3_tile_j(int t) { return t - f3_tile_i(t) * (f3_tile_i(t) + 1) / 2; }
+__device__ __forceinline__ int f3_tile(int T, int q, int slot) {
+  if (T == 3) return slot == 0 ? q : q + 3;
+  if (T == 2) return slot == 0 ? q : -1;
+  return (q == 0 && slot == 0) ? 0 : -1;
+}
+
+template <class Acc, class TS, int DOMS>
+__global__ void __launch_bounds__(96 * DOMS) k_fr_schwarz3(FusedArgs a, const float* __restrict__ pc,
+                                                          float* __restrict__ p_init, int init) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  if (!init && a.ctl->all_done) return;
+  const uint32_t K = a.ninst;
+  const int k = cta_instance(a.lay + 2 * LAY, K);
+  const uint32_t c0 = __ldg(a.lay + 2 * LAY + k);
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ld = wid / 3, q = wid - 3 * ld;
+  const uint32_t d = __ldg(a.lay + 3 * LAY + k) + (blockIdx.x - c0) * DOMS + ld;
+  const uint32_t dend = __ldg(a.lay + 3 * LAY + k + 1);
+  const bool upd = !init && a.inst[k].upd != 0;
+  const float al = (float)a.inst[k].alpha;
+  const bool skip = !init && a.inst[k].done != 0 && !upd;
+  const bool valid = d < dend && !skip;
+  uint64_t* bar = (uint64_t*)(smem + 16 * ld);
+  unsigned char* slice = smem + 128 + (size_t)ld * f3_slice_bytes<Acc, TS>();
+  TS* buf = (TS*)slice;
+  float* rd = (float*)(buf + 6 * TILE_FLOATS);
+  Acc* part = (Acc*)(rd + 96);  // [3][2][32]
+  Acc* yd = part + 3 * 2 * 32;
+  const int bid = 1 + ld;
+  Acc rr = 0, rz = 0;
+  uint32_t vs = 0;
+  int m = 0;
+  if (valid) {
+    vs = a.dom_start[d];
+    m = 3 * (int)(a.dom_start[d + 1] - vs);
+    if (q == 0 && lane == 0) {
+      const uint64_t off = a.fac_off[d];
+      const uint32_t bytes = (uint32_t)((a.fac_off[d + 1] - off) * sizeof(TS));
+      mbar_init(bar, 1);
+      fence_mbar_init();
+      fence_proxy_async();
+      mbar_arrive_expect_tx(bar, bytes);
+      bulk_g2s(buf, (const TS*)a.fac + off, bytes, bar);
+    }
+    const int i = 32 * q + lane;
+    float v = 0.f;
+    if (i < m) {
+      const uint32_t e = 3 * a.dom_verts[vs + i / 3] + i % 3;
+      if (init) {
+        v = a.b[e];
+        a.x[e] = 0.f;
+        a.r[e] = v;
+        p_init[e] = 0.f;
+      } else if (upd) {
+        a.x[e] = fmaf(al, pc[e], a.x[e]);
+        v = fmaf(-al, a.ap[e], a.r[e]);
+        a.r[e] = v;
+      } else {
+        v = a.r[e];
+      }
+    }
+    rd[i] = v;
+  }
+  named_sync(bid, 96);  // rd complete, the barrier initialised
+  bool ok = true;
+  if (valid) {
+    ok = mbar_wait(bar, 0);
+    if (!ok) {
+      if (q == 0 && lane == 0) atomicOr(&a.inst[k].status, ST_WAIT_TIMEOUT);
+      mbar_wait(bar, 0);  // bounded again: the copy may still land
+    }
+  }
+  const int T = (m + 31) >> 5;
+  // pass 1: partial rows of W r
+  if (valid && ok) {
+#pragma unroll
+    for (int slot = 0; slot < 2; ++slot) {
+      const int t = f3_tile(T, q, slot);
+      if (t < 0) continue;
+      const TS* w = buf + t * TILE_FLOATS;
+      const float* rj = rd + 32 * f3_tile_j(t);
+      Acc y = 0;
+#pragma unroll 8
+      for (int c = 0; c < 32; ++c) y += (Acc)tile_ld(w, tile_offset(lane, c)) * (Acc)rj[c];
+      part[(2 * q + slot) * 32 + lane] = y;
+    }
+  }
+  named_sync(bid, 96);
+  if (valid && ok && q < T) {  // y_q = sum of the partials of tile row q
+    Acc y = 0;
+    for (int p = 0; p < 3; ++p)
+      for (int slot = 0; slot < 2; ++slot) {
+        const int t = f3_tile(T, p, slot);
+        if (t >= 0 && f3_tile_i(t) == q) y += part[(2 * p + slot) * 32 + lane];
+      }
+    yd[32 * q + lane] = y;
+  }
+  named_sync(bid, 96);
+  // pass 2: partial columns of W^T y (into the partial buffer, now free)
+  if (valid && ok) {
+#pragma unroll
+    for (int slot = 0; slot < 2; ++slot) {
+      const int t = f3_tile(T, q, slot);
+      if (t < 0) continue;
+      const TS* w = buf + t * TILE_FLOATS;
+      const Acc* yi = yd + 32 * f3_tile_i(t);
+      Acc z = 0;
+#pragma unroll 8
+      for (int r = 0; r < 32; ++r) z += (Acc)tile_ld(w, tile_offset(r, lane)) * yi[r];
+      part[(2 * q + slot) * 32 + lane] = z;
+    }
+  }
+  named_sync(bid, 96);
+  if (valid && ok && q < T) {  // z_q = sum of the partials of tile column q
+    Acc z = 0;
+    for (int p = 0; p < 3; ++p)
+      for (int slot = 0; slot < 2; ++slot) {
+        const int t = f3_tile(T, p, slot);
+        if (t >= 0 && f3_tile_j(t) == q) z += part[(2 * p + slot) * 32 + lane];
+      }
+    const int i = 32 * q + lane;
+    if (i < m) {
+      const Acc sc = a.fac_scale ? (Acc)a.fac_scale[d] : (Acc)1;
+      const float zi = (float)(z * sc * sc);
+      a.z[3 * a.dom_verts[vs + i / 3] + i % 3] = zi;
+      rr = (Acc)rd[i] * (Acc)rd[i];
+      rz = (Acc)rd[i] * (Acc)zi;
+    }
+  }
+  const Acc s0 = block_sum<Acc>(rr);
+  const Acc s1 = block_sum<Acc>(rz);
+  if (threadIdx.x == 0) {
+    a.part[2 * blockIdx.x] = (double)s0;
+    a.part[2 * blockIdx.x + 1] = (double)s1;
+  }
+  if (!last_cta(&a.ctl->counter[1])) return;
+  fd_finish(a, init != 0);
+}
+
 // Block Jacobi: one thread per vertex. init: x = 0, r = b, p_init = 0.
 template <class Acc>
 __global__ void __launch_bounds__(FD_THREADS) k_fr_bj(FusedArgs a, const float* __restrict__ pc,
@@ -345,26 +505,73 @@ __global__ void __launch_bounds__(FD_THREADS) k_fr_bj(FusedArgs a, const float* 
 }
 
 namespace {
+// The fused kernels' variants the autotuner chooses between (per scene, cached per system
+// size): rows kernel with 2, 1 or 4 lanes per block row; Schwarz domain kernel with one warp
+// per domain (4 domains per CTA) or three warps per domain (1, 2 or 4 domains per CTA).
+constexpr int N_ROWS_VARIANTS = 3;
+constexpr int N_DOM_VARIANTS = 4;
+constexpr int ROWS_LPR[N_ROWS_VARIANTS] = {2, 1, 4};
+
 struct Launch {
   void* rows;
   void* dom;
   size_t dom_smem;
   uint32_t grid_rows, grid_dom;
+  uint32_t lpr, dom_threads, doms_per_cta;
 };
 
-Launch fused_kernels(const Scene& s) {
+template <class Acc>
+void* rows_fn(int rv) {
+  switch (rv) {
+    case 1: return (void*)k_fr_rows<Acc, 1>;
+    case 2: return (void*)k_fr_rows<Acc, 4>;
+    default: return (void*)k_fr_rows<Acc, 2>;
+  }
+}
+
+template <class Acc, class TS>
+void dom_fn(int dv, Launch& L) {
+  switch (dv) {
+    case 1:
+      L.dom = (void*)k_fr_schwarz3<Acc, TS, 1>;
+      L.doms_per_cta = 1;
+      L.dom_threads = 96;
+      L.dom_smem = 128 + f3_slice_bytes<Acc, TS>();
+      break;
+    case 2:
+      L.dom = (void*)k_fr_schwarz3<Acc, TS, 2>;
+      L.doms_per_cta = 2;
+      L.dom_threads = 192;
+      L.dom_smem = 128 + 2 * (size_t)f3_slice_bytes<Acc, TS>();
+      break;
+    case 3:
+      L.dom = (void*)k_fr_schwarz3<Acc, TS, 4>;
+      L.doms_per_cta = 4;
+      L.dom_threads = 384;
+      L.dom_smem = 128 + 4 * (size_t)f3_slice_bytes<Acc, TS>();
+      break;
+    default:
+      L.dom = (void*)k_fr_schwarz<Acc, TS>;
+      L.doms_per_cta = FD_WARPS;
+      L.dom_threads = 32 * FD_WARPS;
+      L.dom_smem = 128 + (size_t)FD_WARPS * apply_slice_bytes<TS>();
+  }
+}
+
+Launch fused_kernels(const Scene& s, int rv, int dv) {
   Launch L{};
   const bool sch = s.schwarz != nullptr;
-  L.rows = s.mixed ? (void*)k_fr_rows<double> : (void*)k_fr_rows<float>;
+  L.rows = s.mixed ? rows_fn<double>(rv) : rows_fn<float>(rv);
+  L.lpr = ROWS_LPR[rv];
   if (sch && s.schwarz->half) {
-    L.dom = s.mixed ? (void*)k_fr_schwarz<double, __half> : (void*)k_fr_schwarz<float, __half>;
-    L.dom_smem = 128 + (size_t)FD_WARPS * apply_slice_bytes<__half>();
+    if (s.mixed) dom_fn<double, __half>(dv, L); else dom_fn<float, __half>(dv, L);
   } else if (sch) {
-    L.dom = s.mixed ? (void*)k_fr_schwarz<double, float> : (void*)k_fr_schwarz<float, float>;
-    L.dom_smem = 128 + (size_t)FD_WARPS * apply_slice_bytes<float>();
+    if (s.mixed) dom_fn<double, float>(dv, L); else dom_fn<float, float>(dv, L);
   } else {
     L.dom = s.mixed ? (void*)k_fr_bj<double> : (void*)k_fr_bj<float>;
     L.dom_smem = 0;
+    L.dom_threads = FD_THREADS;
+    L.doms_per_cta = FD_THREADS;  // vertices per CTA
   }
   return L;
 }
@@ -376,9 +583,11 @@ static int fused_prepare(Scene& s, const uint32_t* h_inst_row, uint32_t K, uint3
   MG_CHECK_ARG(K >= 1 && K <= PCG_MAX_INST, "fused PCG: 1..8 instances");
   cudaStream_t st = s.st;
   PcgWork& w = s.work;
-  L = fused_kernels(s);
+  L = fused_kernels(s, s.fr_rows_variant, s.fr_dom_variant);
   // layout: rows, row-kernel CTAs, domain-kernel CTAs, domains (per instance)
   std::vector<uint32_t> key(h_inst_row, h_inst_row + K + 1);
+  key.push_back((uint32_t)s.fr_rows_variant);
+  key.push_back((uint32_t)s.fr_dom_variant);
   if (key != s.fr_key) {
     std::vector<uint32_t> lay(4 * LAY, 0);
     for (uint32_t k = 0; k <= K; ++k) lay[k] = h_inst_row[k];
@@ -395,8 +604,8 @@ static int fused_prepare(Scene& s, const uint32_t* h_inst_row, uint32_t K, uint3
     }
     for (uint32_t k = 0; k < K; ++k) {
       const uint32_t rows = h_inst_row[k + 1] - h_inst_row[k];
-      const uint32_t cr = std::max<uint32_t>(1, ceil_div(rows * FR_LPR, FR_THREADS));
-      const uint32_t cd = s.schwarz ? std::max<uint32_t>(1, ceil_div(dom[k + 1] - dom[k], FD_WARPS))
+      const uint32_t cr = std::max<uint32_t>(1, ceil_div(rows * L.lpr, FR_THREADS));
+      const uint32_t cd = s.schwarz ? std::max<uint32_t>(1, ceil_div(dom[k + 1] - dom[k], L.doms_per_cta))
                                     : std::max<uint32_t>(1, ceil_div(rows, FD_THREADS));
       lay[LAY + k + 1] = lay[LAY + k] + cr;
       lay[2 * LAY + k + 1] = lay[2 * LAY + k] + cd;
@@ -454,8 +663,7 @@ static int fused_prepare(Scene& s, const uint32_t* h_inst_row, uint32_t K, uint3
 
 static int launch_dom(const Scene& s, const Launch& L, FusedArgs& a, const float* pc, float* pinit, int init) {
   void* args[] = {(void*)&a, (void*)&pc, (void*)&pinit, (void*)&init};
-  MG_CUDA(cudaLaunchKernel(L.dom, dim3(L.grid_dom), dim3(s.schwarz ? 32 * FD_WARPS : FD_THREADS), args, L.dom_smem,
-                           s.st));
+  MG_CUDA(cudaLaunchKernel(L.dom, dim3(L.grid_dom), dim3(L.dom_threads), args, L.dom_smem, s.st));
   return MGUSO_OK;
 }
 
@@ -581,6 +789,73 @@ int pcg_fused_profile(Scene& s, uint32_t iters, float* us2) {
   MG_TRY(rc);
   us2[0] = (float)(1000.0 * t_rows / iters);
   us2[1] = (float)(1000.0 * t_dom / iters);
+  return MGUSO_OK;
+}
+
+// Autotuner of the fused kernels: every rows-kernel variant (with the current domain
+// kernel), then every domain-kernel variant (with the fastest rows kernel), each timed over
+// 12 iterations inside a solve of the scene's current system by pcg_fused_profile; the
+// fastest of each is kept. Choices are cached per system shape (vertices, pattern blocks,
+// instances, precision, factor storage, domains), so scenes of the same size share one
+// tuning. The solve that follows starts from scratch, so tuning leaves no trace in results
+// beyond the choice of kernels.
+static int fused_autotune(Scene& s) {
+  static std::mutex mu;
+  static std::map<std::vector<uint64_t>, std::pair<int, int>> cache;
+  std::vector<uint64_t> key = {s.nv, s.Ps.nnz, s.ninst, s.mixed ? 1u : 0u,
+                               s.schwarz ? (s.schwarz->half ? 2u : 1u) : 0u, s.schwarz ? s.schwarz->ndom : 0u,
+                               (uint64_t)s.ctx->device};
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+      s.fr_rows_variant = it->second.first;
+      s.fr_dom_variant = it->second.second;
+      return MGUSO_OK;
+    }
+  }
+  float us2[2];
+  float best = 0;
+  int br = 0;
+  s.fr_dom_variant = 0;
+  for (int rv = 0; rv < N_ROWS_VARIANTS; ++rv) {
+    s.fr_rows_variant = rv;
+    MG_TRY(pcg_fused_profile(s, 2, us2));  // warm-up (graph-free launches, attributes set)
+    MG_TRY(pcg_fused_profile(s, 12, us2));
+    if (rv == 0 || us2[0] < best) {
+      best = us2[0];
+      br = rv;
+    }
+  }
+  s.fr_rows_variant = br;
+  int bd = 0;
+  if (s.schwarz) {
+    for (int dv = 0; dv < N_DOM_VARIANTS; ++dv) {
+      s.fr_dom_variant = dv;
+      MG_TRY(pcg_fused_profile(s, 2, us2));
+      MG_TRY(pcg_fused_profile(s, 12, us2));
+      if (dv == 0 || us2[1] < best) {
+        best = us2[1];
+        bd = dv;
+      }
+    }
+  }
+  s.fr_dom_variant = bd;
+  std::lock_guard<std::mutex> lock(mu);
+  cache[key] = {br, bd};
+  return MGUSO_OK;
+}
+
+int pcg_fused_select(Scene& s) {
+  if (s.fr_tuned) return MGUSO_OK;
+  if (s.p.pcg_variant > 0) {
+    const int v = s.p.pcg_variant - 1;
+    s.fr_rows_variant = (v / N_DOM_VARIANTS) % N_ROWS_VARIANTS;
+    s.fr_dom_variant = s.schwarz ? v % N_DOM_VARIANTS : 0;
+  } else {
+    MG_TRY(fused_autotune(s));
+  }
+  s.fr_tuned = true;
   return MGUSO_OK;
 }
 

@@ -154,6 +154,8 @@ struct Scene {
   DevBuf<FusedCtl> fr_ctl;
   DevBuf<double> fr_part;
   cudaGraphExec_t fr_exec = nullptr;
+  int fr_rows_variant = 0, fr_dom_variant = 0;  // the fused kernels in use (see pcg_fused.cu)
+  bool fr_tuned = false;
   ~Scene() {
     if (fr_exec) cudaGraphExecDestroy(fr_exec);
   }
@@ -201,6 +203,7 @@ int build_bvhs(Scene& s, const float* x);
 int pcg_persistent(Scene& s, const uint32_t* h_inst_row, uint32_t ninst, uint32_t active, PcgInstResult* out);
 int pcg_fused(Scene& s, const uint32_t* h_inst_row, uint32_t ninst, uint32_t active, PcgInstResult* out);
 int pcg_fused_profile(Scene& s, uint32_t iters, float* us2);
+int pcg_fused_select(Scene& s);  // the fused kernels' variants: pcg_variant, or the autotuner's choice
 int collect_stencils(Scene& s, uint32_t* nst);
 int self_intersections(Scene& s);  // piercing pairs per instance at s.x into red[RED_STRIDE k + 14]
 int ccd_step(Scene& s, uint32_t active, float* t_out, uint32_t* cap_hits);

@@ -129,6 +129,7 @@ static int linear_solve(Scene& s, uint32_t active, mguso_lin_stats* ls) {
   const bool two_level = s.schwarz && s.schwarz->levels == 2;
   if (!two_level && (s.p.pcg_mode == 0 || s.p.pcg_mode == 2 || s.ninst > 1)) {
     PcgInstResult r[PCG_MAX_INST] = {};
+    if (s.p.pcg_mode != 2) MG_TRY(pcg_fused_select(s));
     int rc = s.p.pcg_mode == 2 ? pcg_persistent(s, s.inst_vert.data(), s.ninst, active, r)
                                : pcg_fused(s, s.inst_vert.data(), s.ninst, active, r);
     if (rc == MGUSO_OK) {

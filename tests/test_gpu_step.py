@@ -374,3 +374,28 @@ def test_self_intersection_scan_on_perturbed_drapes(ctx):
         assert (cnt > 0) == o.self_intersects(x), (mag, cnt)
         verdicts.append(cnt > 0)
     assert verdicts[0] is False and verdicts[-1] is True
+
+
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_fused_kernel_variants_agree(ctx, precision):
+    """Every variant of the fused PCG kernels the autotuner chooses between (rows kernel with
+    2, 1 or 4 lanes per block row; Schwarz domains with one warp each or three warps each at
+    1, 2 or 4 domains per CTA) runs the same iteration: two batched steps agree with the
+    first variant's to the Newton tolerance."""
+    from mguso import ImplicitBatch
+
+    scs = graded_coarse(2)
+    runs = []
+    for v in range(1, 13):
+        s2 = [dict(sc, params=dict(sc["params"], pcg_variant=v)) for sc in scs]
+        b = ImplicitBatch(ctx, s2, precision)
+        st = b.step(2)
+        runs.append((v, b.positions.astype(np.float64), st))
+        b.close()
+    _, p1, s1 = runs[0]
+    disp = np.abs(p1 - np.concatenate([sc["positions"] for sc in scs])).max()
+    for v, p, st in runs[1:]:
+        assert np.abs(p - p1).max() <= 1e-3 * disp, (v, np.abs(p - p1).max() / disp)
+        for a, b_ in zip(st, s1):
+            for x, y in zip(a, b_):
+                assert x["status"] == 0 and abs(x["newton_iters"] - y["newton_iters"]) <= 1, (v, x, y)
