@@ -88,6 +88,13 @@ struct mguso_schwarz {
   mg::DevBuf<__half> fac_h;
   mg::DevBuf<float> fac_scale;
   mg::DevBuf<uint32_t> status;
+  // Packed domains of vertices without off-diagonal blocks are block diagonal: each of their
+  // vertices is factored on its own, as the reference's one-vertex domain (floor from its
+  // own trace), and stores its 3x3 lower W_v (6 floats: w00 w10 w11 w20 w21 w22, in vfac at
+  // 6 v); such a domain has no tiles. dom_diag[d] marks them.
+  std::vector<uint8_t> h_dom_diag;
+  mg::DevBuf<uint8_t> dom_diag;
+  mg::DevBuf<float> vfac;
   // Two-level Galerkin form (MultilevelSchwarz, linsolve.rs:534-666) when levels == 2: every
   // level-0 domain is a coarse node (three dofs), coarse domains are BFS groups of <= domain
   // coarse nodes over the coarse block graph, and each coarse domain's dense block of

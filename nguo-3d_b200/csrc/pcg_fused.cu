@@ -42,6 +42,8 @@ struct FusedArgs {
   const uint64_t* fac_off;
   const void* fac;         // float or __half tiles
   const float* fac_scale;  // per domain (FP16 tiles), else null
+  const uint8_t* dom_diag;  // block-diagonal domains (per-vertex factors in vfac)
+  const float* vfac;
   const float* b;
   float *x, *r, *z, *ap;
   float tol;
@@ -231,7 +233,8 @@ __global__ void __launch_bounds__(32 * FD_WARPS) k_fr_schwarz(FusedArgs a, const
     const int m = 3 * (int)nvd;
     const uint64_t off = a.fac_off[d];
     const uint32_t bytes = (uint32_t)((a.fac_off[d + 1] - off) * sizeof(TS));
-    if (lane == 0) {
+    const bool diag = a.dom_diag[d] != 0;
+    if (lane == 0 && !diag) {
       mbar_init(bar, 1);
       fence_mbar_init();
       fence_proxy_async();
@@ -258,7 +261,20 @@ __global__ void __launch_bounds__(32 * FD_WARPS) k_fr_schwarz(FusedArgs a, const
       rd[i] = v;
     }
     __syncwarp();
-    if (!mbar_wait(bar, 0)) {
+    if (diag) {
+      if (lane < (int)nvd) {
+        const uint32_t v = a.dom_verts[vs + lane];
+        Acc zz[3];
+        vertex_apply<Acc>(a.vfac + 6 * (size_t)v, rd + 3 * lane, zz);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float zi = (float)zz[c];
+          a.z[3 * v + c] = zi;
+          rr += (Acc)rd[3 * lane + c] * (Acc)rd[3 * lane + c];
+          rz += (Acc)rd[3 * lane + c] * (Acc)zi;
+        }
+      }
+    } else if (!mbar_wait(bar, 0)) {
       if (lane == 0) atomicOr(&a.inst[k].status, ST_WAIT_TIMEOUT);
       mbar_wait(bar, 0);  // bounded again: the copy may still land
     } else {
@@ -345,10 +361,11 @@ __global__ void __launch_bounds__(96 * DOMS) k_fr_schwarz3(FusedArgs a, const fl
   Acc rr = 0, rz = 0;
   uint32_t vs = 0;
   int m = 0;
+  const bool diag = valid && a.dom_diag[d] != 0;
   if (valid) {
     vs = a.dom_start[d];
     m = 3 * (int)(a.dom_start[d + 1] - vs);
-    if (q == 0 && lane == 0) {
+    if (q == 0 && lane == 0 && !diag) {
       const uint64_t off = a.fac_off[d];
       const uint32_t bytes = (uint32_t)((a.fac_off[d + 1] - off) * sizeof(TS));
       mbar_init(bar, 1);
@@ -377,8 +394,21 @@ __global__ void __launch_bounds__(96 * DOMS) k_fr_schwarz3(FusedArgs a, const fl
     rd[i] = v;
   }
   named_sync(bid, 96);  // rd complete, the barrier initialised
+  if (diag && q == 0 && lane < m / 3) {
+    // block-diagonal domain: one lane per vertex
+    const uint32_t v = a.dom_verts[vs + lane];
+    Acc zz[3];
+    vertex_apply<Acc>(a.vfac + 6 * (size_t)v, rd + 3 * lane, zz);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float zi = (float)zz[c];
+      a.z[3 * v + c] = zi;
+      rr += (Acc)rd[3 * lane + c] * (Acc)rd[3 * lane + c];
+      rz += (Acc)rd[3 * lane + c] * (Acc)zi;
+    }
+  }
   bool ok = true;
-  if (valid) {
+  if (valid && !diag) {
     ok = mbar_wait(bar, 0);
     if (!ok) {
       if (q == 0 && lane == 0) atomicOr(&a.inst[k].status, ST_WAIT_TIMEOUT);
@@ -386,8 +416,9 @@ __global__ void __launch_bounds__(96 * DOMS) k_fr_schwarz3(FusedArgs a, const fl
     }
   }
   const int T = (m + 31) >> 5;
+  const bool tiles = valid && ok && !diag;
   // pass 1: partial rows of W r
-  if (valid && ok) {
+  if (tiles) {
 #pragma unroll
     for (int slot = 0; slot < 2; ++slot) {
       const int t = f3_tile(T, q, slot);
@@ -401,7 +432,7 @@ __global__ void __launch_bounds__(96 * DOMS) k_fr_schwarz3(FusedArgs a, const fl
     }
   }
   named_sync(bid, 96);
-  if (valid && ok && q < T) {  // y_q = sum of the partials of tile row q
+  if (tiles && q < T) {  // y_q = sum of the partials of tile row q
     Acc y = 0;
     for (int p = 0; p < 3; ++p)
       for (int slot = 0; slot < 2; ++slot) {
@@ -412,7 +443,7 @@ __global__ void __launch_bounds__(96 * DOMS) k_fr_schwarz3(FusedArgs a, const fl
   }
   named_sync(bid, 96);
   // pass 2: partial columns of W^T y (into the partial buffer, now free)
-  if (valid && ok) {
+  if (tiles) {
 #pragma unroll
     for (int slot = 0; slot < 2; ++slot) {
       const int t = f3_tile(T, q, slot);
@@ -426,7 +457,7 @@ __global__ void __launch_bounds__(96 * DOMS) k_fr_schwarz3(FusedArgs a, const fl
     }
   }
   named_sync(bid, 96);
-  if (valid && ok && q < T) {  // z_q = sum of the partials of tile column q
+  if (tiles && q < T) {  // z_q = sum of the partials of tile column q
     Acc z = 0;
     for (int p = 0; p < 3; ++p)
       for (int slot = 0; slot < 2; ++slot) {
@@ -646,6 +677,8 @@ static int fused_prepare(Scene& s, const uint32_t* h_inst_row, uint32_t K, uint3
     a.fac_off = sw->fac_off.p;
     a.fac = sw->half ? (const void*)sw->fac_h.p : (const void*)sw->fac.p;
     a.fac_scale = sw->half ? sw->fac_scale.p : nullptr;
+    a.dom_diag = sw->dom_diag.p;
+    a.vfac = sw->vfac.p;
   }
   a.b = w.b.p;
   a.x = w.x.p;

@@ -48,6 +48,8 @@ struct PersistentArgs {
   const uint64_t* fac_off;
   const void* fac;         // float or __half tiles
   const float* fac_scale;  // per domain (FP16 tiles), else null
+  const uint8_t* dom_diag;  // block-diagonal domains (per-vertex factors in vfac)
+  const float* vfac;
   uint32_t ndom;
   const float* b;
   float *x, *r, *z, *p, *p2, *ap;
@@ -201,7 +203,8 @@ __global__ void __launch_bounds__(PP_THREADS, 1) k_pcg_persistent(PersistentArgs
         const int m = 3 * (int)nvd;
         const uint64_t off = a.fac_off[d];
         const uint32_t bytes = (uint32_t)((a.fac_off[d + 1] - off) * sizeof(TS));
-        if (lane == 0) {
+        const bool diag = a.dom_diag[d] != 0;
+        if (lane == 0 && !diag) {
           fence_proxy_async();
           mbar_arrive_expect_tx(mbar, bytes);
           bulk_g2s(buf, (const TS*)a.fac + off, bytes, mbar);
@@ -226,6 +229,22 @@ __global__ void __launch_bounds__(PP_THREADS, 1) k_pcg_persistent(PersistentArgs
           rd[i] = v;
         }
         __syncwarp();
+        if (diag) {
+          if (lane < (int)nvd) {
+            const uint32_t v = a.dom_verts[vs + lane];
+            Acc zz[3];
+            vertex_apply<Acc>(a.vfac + 6 * (size_t)v, rd + 3 * lane, zz);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              const float zi = (float)zz[c];
+              a.z[3 * v + c] = zi;
+              acc[0] += (Acc)rd[3 * lane + c] * (Acc)rd[3 * lane + c];
+              acc[1] += (Acc)rd[3 * lane + c] * (Acc)zi;
+            }
+          }
+          __syncwarp();
+          continue;
+        }
         if (!mbar_wait(mbar, mphase)) {
           if (lane == 0) {
             atomicOr(a.bar + 2, ST_WAIT_TIMEOUT);
@@ -495,6 +514,8 @@ int pcg_persistent(Scene& s, const uint32_t* h_inst_row, uint32_t ninst, uint32_
     a.fac_off = sw->fac_off.p;
     a.fac = sw->half ? (const void*)sw->fac_h.p : (const void*)sw->fac.p;
     a.fac_scale = sw->half ? sw->fac_scale.p : nullptr;
+    a.dom_diag = sw->dom_diag.p;
+    a.vfac = sw->vfac.p;
     a.ndom = sw->ndom;
   }
   a.b = w.b.p;

@@ -947,15 +947,18 @@ extern "C" int mguso_scene_profile(mguso_scene* sc, int reps, float* us4, double
   if (rc == MGUSO_OK) rc = timed([&]() { return system_spmv(s, x.p, y.p, st, nullptr); }, &us4[0]);
   if (s.schwarz) {
     mguso_schwarz* sw = s.schwarz.get();
-    double packed = 0;
+    double packed = 0, vert = 0;
     for (uint32_t d = 0; d < sw->ndom; ++d) {
       double m = 3.0 * (sw->h_dom_start[d + 1] - sw->h_dom_start[d]);
-      packed += m * (m + 1) / 2;
+      if (sw->h_dom_diag[d])
+        vert += 24.0 * (sw->h_dom_start[d + 1] - sw->h_dom_start[d]);  // 6 FP32 per vertex
+      else
+        packed += m * (m + 1) / 2;
     }
     // factor entries at their stored width (2 bytes in FP16 plus a scale per domain)
     const double fe = sw->half ? 2.0 : 4.0, fs = sw->half ? 4.0 * sw->ndom : 0.0;
-    bytes4[1] = fe * packed + fs + 4.0 * s.nv + 24.0 * s.nv + 8.0 * (sw->ndom + 1);
-    bytes4[2] = 36.0 * nnz + fe * packed + fs;
+    bytes4[1] = fe * packed + vert + fs + 4.0 * s.nv + 24.0 * s.nv + 8.0 * (sw->ndom + 1);
+    bytes4[2] = 36.0 * nnz + fe * packed + vert + fs;
     if (rc == MGUSO_OK) rc = timed([&]() { return schwarz_apply(sw, x.p, y.p, st, nullptr); }, &us4[1]);
     if (rc == MGUSO_OK)
       rc = timed([&]() { return schwarz_factor_with(sw, s.c_row_ptr.p, s.c_col.p, s.c_val.p, st); }, &us4[2]);
@@ -992,13 +995,16 @@ extern "C" int mguso_scene_profile_pcg(mguso_scene* sc, int iters, float* us2, d
   bytes2[0] = 40.0 * ((double)s.Ps.nnz + nc) + 8.0 * (nv + 1) + 48.0 * nv;
   if (s.schwarz) {
     mguso_schwarz* sw = s.schwarz.get();
-    double packed = 0;
+    double packed = 0, vert = 0;
     for (uint32_t d = 0; d < sw->ndom; ++d) {
       const double m = 3.0 * (sw->h_dom_start[d + 1] - sw->h_dom_start[d]);
-      packed += m * (m + 1) / 2;
+      if (sw->h_dom_diag[d])
+        vert += 24.0 * (sw->h_dom_start[d + 1] - sw->h_dom_start[d]);  // 6 FP32 per vertex
+      else
+        packed += m * (m + 1) / 2;
     }
     const double fe = sw->half ? 2.0 : 4.0, fs = sw->half ? 4.0 * sw->ndom : 0.0;
-    bytes2[1] = fe * packed + fs + 88.0 * nv + 12.0 * sw->ndom;
+    bytes2[1] = fe * packed + vert + fs + 88.0 * nv + 13.0 * sw->ndom;
   } else {
     bytes2[1] = 36.0 * nv + 84.0 * nv;
   }

@@ -52,8 +52,10 @@ int schwarz_build(mguso_schwarz* s) {
       assigned[v] = 1;
     }
   }
-  auto close_domain = [&](size_t base) {
+  s->h_dom_diag.clear();
+  auto close_domain = [&](size_t base, bool diag = false) {
     uint32_t d = (uint32_t)s->h_dom_start.size() - 1;
+    s->h_dom_diag.push_back(diag ? 1 : 0);
     for (size_t i = base; i < s->h_dom_verts.size(); ++i) {
       s->h_dom_of[s->h_dom_verts[i]] = d;
       loc[s->h_dom_verts[i]] = (uint32_t)(i - base);
@@ -94,7 +96,7 @@ int schwarz_build(mguso_schwarz* s) {
   for (size_t i = si; i < se; i += D) {
     size_t base = s->h_dom_verts.size();
     for (size_t j = i; j < std::min(se, i + D); ++j) s->h_dom_verts.push_back(singles[j]);
-    close_domain(base);
+    close_domain(base, true);
   }
   si = se;
   }
@@ -103,10 +105,12 @@ int schwarz_build(mguso_schwarz* s) {
   std::vector<uint64_t> off(s->ndom + 1, 0);
   for (uint32_t d = 0; d < s->ndom; ++d) {
     uint64_t m = 3ull * (s->h_dom_start[d + 1] - s->h_dom_start[d]);
-    uint64_t t = (m + 31) / 32;
+    uint64_t t = s->h_dom_diag[d] ? 0 : (m + 31) / 32;
     off[d + 1] = off[d] + t * (t + 1) / 2 * TILE_FLOATS;
   }
   s->fac_floats = off[s->ndom];
+  MG_TRY(s->dom_diag.upload(s->h_dom_diag.data(), std::max<size_t>(s->h_dom_diag.size(), 1), a->ctx->stream));
+  MG_TRY(s->vfac.reserve(6 * (size_t)std::max<uint32_t>(nb, 1)));
   cudaStream_t st = a->ctx->stream;
   MG_TRY(s->dom_start.upload(s->h_dom_start.data(), s->h_dom_start.size(), st));
   MG_TRY(s->dom_verts.upload(s->h_dom_verts.data(), s->h_dom_verts.size(), st));
@@ -270,9 +274,18 @@ __device__ void factor_dense_store(double* A, int ld, int m, double* dinv, doubl
     A[k * ld + k] += s_floor;
     diag0[k] = A[k * ld + k];
   }
+  // the strict upper triangle becomes V (below), starting from the identity's zeros
+  for (int e = tid; e < m * m; e += nt) {
+    const int i = e / m, j = e - i * m;
+    if (j > i) A[i * ld + j] = 0.0;
+  }
   __syncthreads();
-  // Cholesky: column k stays unscaled during its own trailing update (L_ik = A_ik / L_kk
-  // is applied after the loop), so one barrier per column suffices.
+  // Cholesky A = U P U^T (U unit lower, U_ik = A_ik^(k) / p_k from the k-th Schur
+  // complement, P the pivots; L = U P^1/2) and, in the same sweep, V = U^-1 by row
+  // elimination: at step k, row i > k of V loses U_ik times row k, which is final by then.
+  // The Schur update writes the lower triangle (columns k < j <= i), the elimination the
+  // upper one (V_ij at A[j * ld + i], columns j <= k; V_kk = 1 is implicit), so one barrier
+  // per step suffices. Afterwards W = L^-1 = P^-1/2 V.
   const int tx = tid & 31, ty = tid >> 5;
   for (int k = 0; k < m; ++k) {
     const double p = A[k * ld + k];
@@ -284,6 +297,7 @@ __device__ void factor_dense_store(double* A, int ld, int m, double* dinv, doubl
     for (int i = k + 1 + ty; i < m; i += 8) {
       const double aik = A[i * ld + k] * ip;
       for (int j = k + 1 + tx; j <= i; j += 32) A[i * ld + j] -= aik * A[j * ld + k];
+      for (int j = tx; j <= k; j += 32) A[j * ld + i] -= aik * (j == k ? 1.0 : A[j * ld + k]);
     }
     if (tid == 0) {
       const double l = sqrt(p);
@@ -308,26 +322,9 @@ __device__ void factor_dense_store(double* A, int ld, int m, double* dinv, doubl
     if (tid == 0) atomicOr(status, 1u << 8);
     return;
   }
-  for (int i = ty; i < m; i += 8)
-    for (int k = tx; k < i; k += 32) A[i * ld + k] *= dinv[k];
-  __syncthreads();
-  // W = L^-1 by columns: thread j walks rows i > j; W_ij = -dinv_i * sum_{k=j}^{i-1} L_ik W_kj.
-  // W_kj (k >= j) lives at A[j * ld + k], the upper triangle and the diagonal.
-  for (int j = tid; j < m; j += nt) {
-    double* wj = A + (size_t)j * ld;
-    wj[j] = dinv[j];
-    for (int i = j + 1; i < m; ++i) {
-      const double* li = A + (size_t)i * ld;
-      double s0 = 0.0, s1 = 0.0;
-      int k = j;
-      for (; k + 1 < i; k += 2) {
-        s0 += li[k] * wj[k];
-        s1 += li[k + 1] * wj[k + 1];
-      }
-      if (k < i) s0 += li[k] * wj[k];
-      wj[i] = -(s0 + s1) * dinv[i];
-    }
-  }
+  // W_ij = dinv_i V_ij (j < i) and W_ii = dinv_i, in place at A[j * ld + i]
+  for (int j = ty; j < m; j += 8)
+    for (int i = j + tx; i < m; i += 32) A[j * ld + i] = i == j ? dinv[i] : A[j * ld + i] * dinv[i];
   __syncthreads();
   const double inv_sc = scaled ? 1.0 / factor_amax(A, ld, m, diag0, false) : 1.0;
   if (scaled && tid == 0) *scale_out = (float)(1.0 / inv_sc);
@@ -341,17 +338,71 @@ __device__ void factor_dense_store(double* A, int ld, int m, double* dinv, doubl
   }
 }
 
+// One vertex as its own domain (m = 3): the reference's floor 1e-6 (tr / 3) + 1e-8 on the
+// diagonal, the row-by-row Cholesky with its pivot test (linsolve.rs:80-99; a failed pivot
+// falls back to L = diag(sqrt(a_pp)), 1 where a_pp <= 1e-14), and W = L^-1 stored as its
+// lower triangle (w00 w10 w11 w20 w21 w22).
+__device__ void vertex_factor(double* a, float* __restrict__ w6, uint32_t* status) {
+  const double fl = 1e-6 * ((a[0] + a[4] + a[8]) / 3.0) + 1e-8;
+  a[0] += fl;
+  a[4] += fl;
+  a[8] += fl;
+  double l[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  bool ok = true;
+  for (int i = 0; i < 3 && ok; ++i)
+    for (int j = 0; j <= i; ++j) {
+      double sum = a[3 * i + j];
+      for (int k = 0; k < j; ++k) sum -= l[3 * i + k] * l[3 * j + k];
+      if (i == j) {
+        if (!(sum > 1e-14)) {
+          ok = false;
+          break;
+        }
+        l[3 * i + i] = sqrt(sum);
+      } else {
+        l[3 * i + j] = sum / l[3 * j + j];
+      }
+    }
+  if (!ok) {
+    for (int e = 0; e < 9; ++e) l[e] = 0.0;
+    for (int p = 0; p < 3; ++p) l[4 * p] = a[4 * p] > 1e-14 ? sqrt(a[4 * p]) : 1.0;
+    atomicOr(status, 1u << 8);
+  }
+  const double w00 = 1.0 / l[0], w11 = 1.0 / l[4], w22 = 1.0 / l[8];
+  const double w10 = -l[3] * w00 * w11;
+  const double w21 = -l[7] * w11 * w22;
+  const double w20 = -(l[6] * w00 + l[7] * w10) * w22;
+  w6[0] = (float)w00;
+  w6[1] = (float)w10;
+  w6[2] = (float)w11;
+  w6[3] = (float)w20;
+  w6[4] = (float)w21;
+  w6[5] = (float)w22;
+}
+
 template <class TS>
 __global__ void __launch_bounds__(FACTOR_THREADS) k_schwarz_factor(
     const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ col, const float* __restrict__ val,
     const uint32_t* __restrict__ dom_start, const uint32_t* __restrict__ dom_verts,
     const uint32_t* __restrict__ dom_of, const uint32_t* __restrict__ loc, const uint64_t* __restrict__ fac_off,
     TS* __restrict__ fac, float* __restrict__ fac_scale, uint32_t* status, const uint32_t* __restrict__ c_rp,
-    const uint32_t* __restrict__ c_col, const float* __restrict__ c_val) {
+    const uint32_t* __restrict__ c_col, const float* __restrict__ c_val, const uint8_t* __restrict__ dom_diag,
+    float* __restrict__ vfac) {
   // FP16 tiles hold W / scale (scale: the domain's largest |W|); FP32 tiles hold W
   extern __shared__ __align__(16) double sA[];
   const uint32_t d = blockIdx.x;
   const uint32_t vs = dom_start[d], nvd = dom_start[d + 1] - vs;
+  if (dom_diag[d]) {
+    for (uint32_t p = threadIdx.x; p < nvd; p += blockDim.x) {
+      const uint32_t v = dom_verts[vs + p];
+      double A9[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (uint32_t k = row_ptr[v]; k < row_ptr[v + 1]; ++k)
+        if (col[k] == v)
+          for (int e = 0; e < 9; ++e) A9[e] = (double)val[9 * (size_t)k + e];
+      vertex_factor(A9, vfac + 6 * (size_t)v, status);
+    }
+    return;
+  }
   const int m = 3 * (int)nvd;
   const int ld = m + 1;
   double* A = sA;
@@ -455,11 +506,11 @@ int schwarz_factor_with(mguso_schwarz* s, const uint32_t* c_rp, const uint32_t* 
   if (s->half)
     k_schwarz_factor<__half><<<s->ndom, FACTOR_THREADS, smem, st>>>(
         a->row_ptr.p, a->col.p, a->val.p, s->dom_start.p, s->dom_verts.p, s->dom_of.p, s->loc.p, s->fac_off.p,
-        s->fac_h.p, s->fac_scale.p, s->status.p, c_col ? c_rp : nullptr, c_col, c_val);
+        s->fac_h.p, s->fac_scale.p, s->status.p, c_col ? c_rp : nullptr, c_col, c_val, s->dom_diag.p, s->vfac.p);
   else
     k_schwarz_factor<float><<<s->ndom, FACTOR_THREADS, smem, st>>>(
         a->row_ptr.p, a->col.p, a->val.p, s->dom_start.p, s->dom_verts.p, s->dom_of.p, s->loc.p, s->fac_off.p,
-        s->fac.p, nullptr, s->status.p, c_col ? c_rp : nullptr, c_col, c_val);
+        s->fac.p, nullptr, s->status.p, c_col ? c_rp : nullptr, c_col, c_val, s->dom_diag.p, s->vfac.p);
   MG_CUDA(cudaGetLastError());
   if (s->levels == 2 && s->ncdom) {
     size_t smem1 = sizeof(double) * ((size_t)s->max_m1 * (s->max_m1 + 1) + 2 * (size_t)s->max_m1);
@@ -487,7 +538,8 @@ template <int WARPS, class Acc, class TS>
 __global__ void __launch_bounds__(32 * WARPS) k_schwarz_apply(
     const uint32_t* __restrict__ dom_start, const uint32_t* __restrict__ dom_verts,
     const uint64_t* __restrict__ fac_off, const TS* __restrict__ fac, const float* __restrict__ fac_scale,
-    const float* __restrict__ r, float* __restrict__ z, uint32_t ndom, uint32_t* status, DotSink dot, int with_dot) {
+    const float* __restrict__ r, float* __restrict__ z, uint32_t ndom, uint32_t* status, DotSink dot, int with_dot,
+    const uint8_t* __restrict__ dom_diag, const float* __restrict__ vfac) {
   extern __shared__ __align__(128) unsigned char smem[];
   if (with_dot && dot.sc->done) return;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -507,7 +559,8 @@ __global__ void __launch_bounds__(32 * WARPS) k_schwarz_apply(
     const int m = 3 * (int)nvd;
     const uint64_t off = fac_off[d];
     const uint32_t bytes = (uint32_t)((fac_off[d + 1] - off) * sizeof(TS));
-    if (lane == 0) {
+    const bool diag = dom_diag[d] != 0;
+    if (lane == 0 && !diag) {
       fence_proxy_async();
       mbar_arrive_expect_tx(bar, bytes);
       bulk_g2s(buf, fac + off, bytes, bar);
@@ -518,6 +571,21 @@ __global__ void __launch_bounds__(32 * WARPS) k_schwarz_apply(
       rd[i] = v;
     }
     __syncwarp();
+    if (diag) {
+      if (lane < (int)nvd) {
+        const uint32_t v = dom_verts[vs + lane];
+        Acc zz[3];
+        vertex_apply<Acc>(vfac + 6 * (size_t)v, rd + 3 * lane, zz);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float zi = (float)zz[c];
+          z[3 * v + c] = zi;
+          acc += (Acc)rd[3 * lane + c] * (Acc)zi;
+        }
+      }
+      __syncwarp();
+      continue;
+    }
     if (!mbar_wait(bar, phase)) {
       if (lane == 0) atomicOr(status, ST_WAIT_TIMEOUT);
       mbar_wait(bar, phase);  // the copy may still land: bounded second wait, then stop
@@ -671,8 +739,10 @@ int schwarz_apply(mguso_schwarz* s, const float* r, float* z, cudaStream_t st, c
   const float* a4 = h ? s->fac_scale.p : nullptr;
   uint32_t nd = s->ndom;
   uint32_t* stp = s->status.p;
+  const uint8_t* a5 = s->dom_diag.p;
+  const float* a6 = s->vfac.p;
   void* args[] = {(void*)&a0, (void*)&a1, (void*)&a2, (void*)&a3, (void*)&a4, (void*)&r, (void*)&z,
-                  (void*)&nd, (void*)&stp, (void*)&d, (void*)&with_dot};
+                  (void*)&nd, (void*)&stp, (void*)&d, (void*)&with_dot, (void*)&a5, (void*)&a6};
   if (grid == 0) return MGUSO_OK;
   MG_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(32 * APPLY_WARPS), args, smem, st));
   if (s->levels != 2 || s->ncdom == 0) return MGUSO_OK;

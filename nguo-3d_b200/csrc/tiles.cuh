@@ -79,4 +79,16 @@ __device__ __forceinline__ void tiles_apply(const TS* __restrict__ w, const floa
   z[2] = z2;
 }
 
+// z = W_v^T (W_v r) for one vertex of a block-diagonal domain (W_v lower triangular, 6 floats
+// w00 w10 w11 w20 w21 w22).
+template <class Acc>
+__device__ __forceinline__ void vertex_apply(const float* __restrict__ w6, const float* r3, Acc (&z)[3]) {
+  const Acc w00 = w6[0], w10 = w6[1], w11 = w6[2], w20 = w6[3], w21 = w6[4], w22 = w6[5];
+  const Acc r0 = r3[0], r1 = r3[1], r2 = r3[2];
+  const Acc y0 = w00 * r0, y1 = w10 * r0 + w11 * r1, y2 = w20 * r0 + w21 * r1 + w22 * r2;
+  z[0] = w00 * y0 + w10 * y1 + w20 * y2;
+  z[1] = w11 * y1 + w21 * y2;
+  z[2] = w22 * y2;
+}
+
 }  // namespace mg
