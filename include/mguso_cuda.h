@@ -57,6 +57,8 @@ size_t mguso_last_error(char* buf, size_t len);
 /* GPU context: selects `device` and owns a stream. The reference's GpuContext::new()
  * (engine-gpu/src/lib.rs:91-126). */
 int mguso_ctx_create(int device, mguso_ctx** out);
+/* Every object created on a context (solvers, operators, scenes, batches, BVHs, adjoints)
+ * uses its stream and must be destroyed before the context is. */
 int mguso_ctx_destroy(mguso_ctx* ctx);
 /* The context's CUDA stream (a cudaStream_t). */
 void* mguso_ctx_stream(mguso_ctx* ctx);

@@ -71,6 +71,7 @@ class AdjointDrape:
         h = C.c_void_p()
         check(self.lib.mguso_adjoint_create(ctx.h, C.byref(d), C.byref(spec), C.byref(h)))
         self.h = h
+        ctx.own(self)
 
     @property
     def nparams(self) -> int:

@@ -18,6 +18,7 @@ class Lbvh:
         h = C.c_void_p()
         check(self.lib.mguso_lbvh_create(ctx.h, C.byref(h)))
         self.h = h
+        ctx.own(self)
         self.nt = 0
 
     def build(self, pos_dev: int, nv: int, tris_dev: int, nt: int, key_bits: int = 30, stream: int = 0):

@@ -7,6 +7,7 @@ GPU through the C ABI. ``CsrMatrix`` mirrors ``engine_core::CsrMatrix`` (csr.rs:
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from dataclasses import dataclass
 
 import numpy as np
@@ -46,13 +47,24 @@ class Context:
         check(self.lib.mguso_ctx_create(device, C.byref(h)))
         self.h = h
         self.device = device
+        self._deps = weakref.WeakSet()
 
     @property
     def stream(self) -> int:
         return self.lib.mguso_ctx_stream(self.h)
 
+    def own(self, obj) -> None:
+        """Registers an object built on this context, to be closed before the context is
+        (the C objects use the context's stream, so they must not outlive it)."""
+        self._deps.add(obj)
+
     def close(self):
         if self.h:
+            for d in list(self._deps):
+                try:
+                    d.close()
+                except Exception:
+                    pass
             self.lib.mguso_ctx_destroy(self.h)
             self.h = None
 
@@ -84,6 +96,7 @@ class CudaLinearSolver:
             pc = {"schwarz": _lib.PRECOND_SCHWARZ, "block": _lib.PRECOND_BLOCK_JACOBI}[precond]
             check(self.lib.mguso_linear_solver_create(ctx.h, pc, domain, pr, C.byref(h)))
         self.h = h
+        ctx.own(self)
         self._stats = LinearStats()
 
     def solve(self, a: CsrMatrix, b: np.ndarray, tol: float, max_iter: int) -> np.ndarray:
@@ -127,6 +140,7 @@ class Bsr:
         check(self.lib.mguso_bsr_create(ctx.h, nb, ptr(rp), ptr(cl) if cl.size else None,
                                         ptr(vl) if vl.size else None, C.byref(h)))
         self.h = h
+        ctx.own(self)
         self.nb = nb
         self.nnzb = int(cl.size)
 
@@ -139,6 +153,7 @@ class Bsr:
         h = C.c_void_p()
         check(self.lib.mguso_bsr_create_from_csr(ctx.h, C.byref(desc), C.byref(h)))
         self.h = h
+        ctx.own(self)
         nb, nnzb = C.c_uint32(), C.c_uint32()
         check(self.lib.mguso_bsr_info(h, C.byref(nb), C.byref(nnzb)))
         self.nb, self.nnzb = nb.value, nnzb.value
@@ -198,6 +213,7 @@ class Schwarz:
         else:
             check(self.lib.mguso_schwarz_create(a.h, domain, C.byref(h)))
         self.h = h
+        a.ctx.own(self)
         nd, fb = C.c_uint32(), C.c_uint64()
         check(self.lib.mguso_schwarz_info(h, C.byref(nd), C.byref(fb)))
         self.ndomains, self.factor_bytes = nd.value, fb.value

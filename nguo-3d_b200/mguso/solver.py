@@ -151,6 +151,7 @@ class ImplicitSolver:
         h = C.c_void_p()
         check(self.lib.mguso_scene_create(ctx.h, C.byref(d), C.byref(h)))
         self.h = h
+        ctx.own(self)
         self.ninst = 1
         self.history: list[dict] = []
 
@@ -300,6 +301,7 @@ class ImplicitBatch(ImplicitSolver):
         h = C.c_void_p()
         check(self.lib.mguso_batch_create(ctx.h, arr, len(pairs), C.byref(h)))
         self.h = h
+        ctx.own(self)
         n = C.c_uint32()
         offs = np.zeros(len(pairs) + 1, np.uint32)
         check(self.lib.mguso_scene_instances(h, C.byref(n), ptr(offs)))
