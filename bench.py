@@ -376,7 +376,7 @@ def cpu_drape_window(which: str, warmup: int, seconds: float, states=None):
     steps = sum(n for n, _, _, _ in res)
     busy = max(dt for _, dt, _, _ in res)
     newton = [nw for _, _, nw, _ in res]
-    start = "from the GPU's post-warm-up states" if states is not None else f"after {warmup} untimed oracle steps"
+    start = "from the GPU's states before them" if states is not None else f"after {warmup} untimed oracle steps"
     desc = (f"oracle f32 implicit step, {'the 6 graded sizes' if k == 6 else 'the drape'} in {workers} concurrent "
             f"process{'es' if workers > 1 else ''}, steps {warmup + 1}..{warmup + max(n for n, _, _, _ in res)} "
             f"{start} ({busy:.1f} s timed, {wall:.1f} s wall); Newton iterations per timed step "
@@ -419,11 +419,12 @@ def time_steps(solver, steps, stream, dist):
     return dist.max(e0.elapsed_time(e1)), st
 
 
-def e2e_steps(solver, p0, v0, k, dist):
+def e2e_steps(solver, p0, v0, k, dist, record=None):
     """End to end through the C ABI, the same steps as the timed region: every step uploads
     its state (positions, velocities) from pinned host memory, steps once and downloads the
     new state, which is the next step's input. Returns (seconds per step, h2d and d2h bytes
-    per step)."""
+    per step). With `record` (a step index j of the window), the host state before step j and
+    the positions after it are kept in record_out (copies made outside the timed span)."""
     import torch
 
     import mguso
@@ -434,14 +435,25 @@ def e2e_steps(solver, p0, v0, k, dist):
     nbytes = pin_p.numel() * 4 + pin_v.numel() * 4
     torch.cuda.synchronize()
     dist.barrier()
+    span, kept = 0.0, {}
     t0 = time.perf_counter()
-    for _ in range(k):
+    for j in range(k):
+        if j == record:
+            span += time.perf_counter() - t0
+            kept["pre"] = (pin_p.numpy().copy(), pin_v.numpy().copy())
+            t0 = time.perf_counter()
         mguso._lib.check(lib.mguso_write_positions(solver.h, pin_p.data_ptr()))
         mguso._lib.check(lib.mguso_write_velocities(solver.h, pin_v.data_ptr()))
         solver.step(1)
         mguso._lib.check(lib.mguso_read_positions(solver.h, pin_p.data_ptr()))
         mguso._lib.check(lib.mguso_read_velocities(solver.h, pin_v.data_ptr()))
-    return dist.max(time.perf_counter() - t0) / k, nbytes, nbytes
+        if j == record:
+            span += time.perf_counter() - t0
+            kept["post"] = pin_p.numpy().copy()
+            t0 = time.perf_counter()
+    span += time.perf_counter() - t0
+    e2e_steps.kept = kept
+    return dist.max(span) / k, nbytes, nbytes
 
 
 def step_errors(x_start, x_test, x_ref):
@@ -517,10 +529,15 @@ def run_batch(args, dist: Dist):
     prof = b.profile(100)
     dom = max(fused, key=lambda k: fused[k][0])
     us, nbytes = fused[dom]
-    kname = {"rows": "k_fr_rows<double>", "domains": "k_fr_schwarz<double, __half>"}[dom]
+    kname = b.pcg_kernel_names()[dom]
     traffic, tsrc = traffic_from_profiles(kname)
+    # the window's representative step: the one whose mean Newton count (over the sizes) is
+    # the median of the window's; the CPU baseline and the FP64 error are taken there
+    per_step = [float(np.mean([s_["newton_iters"] for s_ in step])) for step in st_b]
+    j_med = int(np.argsort(per_step, kind="stable")[len(per_step) // 2])
     # end to end: the timed steps again from the same state, each step's state through host
-    e2e_s, h2d, d2h = e2e_steps(b, p_w, v_w, args.steps, dist)
+    e2e_s, h2d, d2h = e2e_steps(b, p_w, v_w, args.steps, dist, record=j_med)
+    kept = e2e_steps.kept
     nl = None if args.no_launch_count else count_launches(lambda: b.step(1))
     launches = None if nl is None else int(nl * args.steps)
     peak, peak_kind = load_peaks()
@@ -576,32 +593,33 @@ def run_batch(args, dist: Dist):
         "clocks": {k: clk[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
         "status": sorted(set(int(s_["status"]) for step in st_b for s_ in step)),
     }
+    step_no = args.warmup + 1 + j_med
+    res["config"]["newton_iters_per_step_batched"] = [round(x, 2) for x in per_step]
+    res["config"]["newton_iters_per_s_batched"] = round(float(np.sum(newton_b)) / (ms_b * 1e-3), 2)
     if dist.rank == 0 and not args.no_cpu_baseline:
-        # first timed step (warmup + 1) of every size from the GPU's post-warm-up state: the
-        # batch's result, the FP32 oracle's (timed: the CPU baseline) and the FP64 oracle's
-        b1 = mguso.ImplicitBatch(ctx, scs, "mixed")
-        b1.positions, b1.velocities = p_w, v_w
-        b1.step(1)
-        x_gpu = b1.positions
-        b1.close()
+        # the representative step of every size from the GPU's state before it: the batch's
+        # result, the FP32 oracle's (timed: the CPU baseline) and the FP64 oracle's
+        p_j, v_j = kept["pre"]
+        x_gpu = kept["post"]
         off = b.offsets
-        states = [(p_w[off[i]:off[i + 1]], v_w[off[i]:off[i + 1]]) for i in range(len(scs))]
-        sps, sample, cores, newton_cpu, x32 = cpu_drape_window("batch", args.warmup, args.cpu_seconds, states)
+        states = [(p_j[off[i]:off[i + 1]], v_j[off[i]:off[i + 1]]) for i in range(len(scs))]
+        sps, sample, cores, newton_cpu, x32 = cpu_drape_window("batch", step_no - 1, args.cpu_seconds, states)
         res["cpu_baseline"] = {"value": round(sps, 4), "unit": BATCH_UNIT, "cores": cores, "kind": "port",
-                               "sample": sample}
+                               "sample": sample,
+                               "newton_iters_per_s": round(sps * float(np.mean([n for nw in newton_cpu for n in nw])), 3)}
         if not args.no_fp64_check:
             jobs = [("batch", i, "f64", 0, 0.0, states[i]) for i in range(len(scs))]
             r64 = _pool_map(jobs, min(len(scs), os.cpu_count() or 1))
             table = []
             for i in range(len(scs)):
                 x64 = r64[i][3]
-                xs = p_w[off[i]:off[i + 1]]
-                table.append({"size": i, "step": args.warmup + 1,
+                xs = p_j[off[i]:off[i + 1]]
+                table.append({"size": i, "step": step_no,
                               "batch_mixed_vs_fp64": step_errors(xs, x_gpu[off[i]:off[i + 1]], x64),
                               "oracle_fp32_vs_fp64": step_errors(xs, x32[i], x64),
-                              "newton_batch_fp64_fp32": [int(st_b[0][i]["newton_iters"]), r64[i][2][0],
+                              "newton_batch_fp64_fp32": [int(st_b[j_med][i]["newton_iters"]), r64[i][2][0],
                                                          newton_cpu[i][0]]})
-            res["config"]["fp64_oracle_error_first_timed_step"] = table
+            res["config"]["fp64_oracle_error_representative_step"] = table
     b.close()
     ctx.close()
     return res
@@ -705,14 +723,16 @@ def run_reference(args, dist: Dist):
             "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": 1, "kind": "port", "sample": sample},
             "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }
-    sps, sample, cores, _, _ = cpu_drape_window(args.workload, args.warmup, max(1.0, min(args.cpu_seconds, 30.0)))
+    sps, sample, cores, newton, _ = cpu_drape_window(args.workload, args.warmup, max(1.0, min(args.cpu_seconds, 30.0)))
     _, desc = drape_scene(args.workload)
     unit = BATCH_UNIT if args.workload == "batch" else "steps/s"
+    nps = round(sps * float(np.mean([n for nw in newton for n in nw])), 3)
     return {
         "impl": "reference", "metric": METRIC, "value": round(sps, 4), "unit": unit, "n_gpus": dist.world,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": {"workload": desc},
-        "cpu_baseline": {"value": round(sps, 4), "unit": unit, "cores": cores, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": round(sps, 4), "unit": unit, "cores": cores, "kind": "port", "sample": sample,
+                         "newton_iters_per_s": nps},
         "e2e": {"value": round(sps, 4), "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 

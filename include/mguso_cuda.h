@@ -335,7 +335,8 @@ int mguso_scene_instances(mguso_scene* s, uint32_t* n, uint32_t* vert_offsets);
  * the stiffness of seam q's stitches. The backward pass solves, per step and in reverse,
  * H w = a_x + a_v / h with H the exact Hessian of the step at its converged positions
  * (symmetric, possibly indefinite: no eigenvalue clamps, with the second-derivative terms of
- * hinges and barriers) by MINRES to a relative residual of 1e-7, preconditioned by the
+ * hinges and barriers) by MINRES to a relative residual of 1e-10 (FP64 products with the
+ * stored FP32 blocks), preconditioned by the
  * step's own preconditioner factored from its projected matrix, recomputing the states
  * between checkpoints taken every `checkpoint_every` steps. A contact stiffness's dependence
  * on the gap enters H, its dependence on the elastic blocks does not; friction must be 0.
@@ -394,6 +395,11 @@ int mguso_scene_profile(mguso_scene* s, int reps, float* us4, double* bytes4);
  * SpMV, p.Ap), domain kernel (x/r update, preconditioner apply, r.r and r.z)}; bytes2 =
  * their algorithmic bytes per launch. Clobbers the PCG scratch (not the state). */
 int mguso_scene_profile_pcg(mguso_scene* s, int iters, float* us2, double* bytes2);
+/* The fused PCG kernels in use, as the autotuner (or pcg_variant) chose them: out2 = {rows
+ * kernel: 0 two lanes per block row, 1 one, 2 four; domain kernel: 0 one warp per domain and
+ * four domains per CTA, 1/2/3 three warps per domain and 1/2/4 domains per CTA}; -1 before
+ * the scene's first solve. */
+int mguso_scene_pcg_kernels(mguso_scene* s, int* out2);
 
 /* The self-intersection scan behind mguso_step_stats.penetration_free
  * (ImplicitSolver::has_self_intersection, implicit.rs:618-650): at positions x (host

@@ -17,6 +17,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "reduce.cuh"
@@ -316,10 +317,15 @@ __global__ void __launch_bounds__(32 * FD_WARPS) k_fr_schwarz(FusedArgs a, const
 // W^T y columns, and those are summed per tile column into z. Compared with one warp per
 // domain, the chain of dependent tile passes per domain is a third as long and three times
 // as many warps share the same shared memory. The sums are deterministic.
+// Accumulation type of the tile passes: FP32 over FP16 tiles (whose own rounding, 2^-11,
+// dwarfs FP32 sums of 32 terms), else the precision's type. The dot products stay in Acc.
+template <class Acc, class TS>
+using ApplyAcc = typename std::conditional<sizeof(TS) == 2, float, Acc>::type;
+
 template <class Acc, class TS>
 __host__ __device__ constexpr uint32_t f3_slice_bytes() {
-  return (6 * TILE_FLOATS * (uint32_t)sizeof(TS) + 96 * 4 + 3 * 2 * 32 * (uint32_t)sizeof(Acc) +
-          96 * (uint32_t)sizeof(Acc) + 127) / 128 * 128;
+  return (6 * TILE_FLOATS * (uint32_t)sizeof(TS) + 96 * 4 + 3 * 2 * 32 * (uint32_t)sizeof(ApplyAcc<Acc, TS>) +
+          96 * (uint32_t)sizeof(ApplyAcc<Acc, TS>) + 127) / 128 * 128;
 }
 
 __device__ __forceinline__ void named_sync(int id, int threads) {
@@ -353,10 +359,11 @@ __global__ void __launch_bounds__(96 * DOMS) k_fr_schwarz3(FusedArgs a, const fl
   const bool valid = d < dend && !skip;
   uint64_t* bar = (uint64_t*)(smem + 16 * ld);
   unsigned char* slice = smem + 128 + (size_t)ld * f3_slice_bytes<Acc, TS>();
+  using AA = ApplyAcc<Acc, TS>;
   TS* buf = (TS*)slice;
   float* rd = (float*)(buf + 6 * TILE_FLOATS);
-  Acc* part = (Acc*)(rd + 96);  // [3][2][32]
-  Acc* yd = part + 3 * 2 * 32;
+  AA* part = (AA*)(rd + 96);  // [3][2][32]
+  AA* yd = part + 3 * 2 * 32;
   const int bid = 1 + ld;
   Acc rr = 0, rz = 0;
   uint32_t vs = 0;
@@ -425,15 +432,15 @@ __global__ void __launch_bounds__(96 * DOMS) k_fr_schwarz3(FusedArgs a, const fl
       if (t < 0) continue;
       const TS* w = buf + t * TILE_FLOATS;
       const float* rj = rd + 32 * f3_tile_j(t);
-      Acc y = 0;
+      AA y = 0;
 #pragma unroll 8
-      for (int c = 0; c < 32; ++c) y += (Acc)tile_ld(w, tile_offset(lane, c)) * (Acc)rj[c];
+      for (int c = 0; c < 32; ++c) y += (AA)tile_ld(w, tile_offset(lane, c)) * (AA)rj[c];
       part[(2 * q + slot) * 32 + lane] = y;
     }
   }
   named_sync(bid, 96);
   if (tiles && q < T) {  // y_q = sum of the partials of tile row q
-    Acc y = 0;
+    AA y = 0;
     for (int p = 0; p < 3; ++p)
       for (int slot = 0; slot < 2; ++slot) {
         const int t = f3_tile(T, p, slot);
@@ -449,16 +456,16 @@ __global__ void __launch_bounds__(96 * DOMS) k_fr_schwarz3(FusedArgs a, const fl
       const int t = f3_tile(T, q, slot);
       if (t < 0) continue;
       const TS* w = buf + t * TILE_FLOATS;
-      const Acc* yi = yd + 32 * f3_tile_i(t);
-      Acc z = 0;
+      const AA* yi = yd + 32 * f3_tile_i(t);
+      AA z = 0;
 #pragma unroll 8
-      for (int r = 0; r < 32; ++r) z += (Acc)tile_ld(w, tile_offset(r, lane)) * yi[r];
+      for (int r = 0; r < 32; ++r) z += (AA)tile_ld(w, tile_offset(r, lane)) * yi[r];
       part[(2 * q + slot) * 32 + lane] = z;
     }
   }
   named_sync(bid, 96);
   if (tiles && q < T) {  // z_q = sum of the partials of tile column q
-    Acc z = 0;
+    AA z = 0;
     for (int p = 0; p < 3; ++p)
       for (int slot = 0; slot < 2; ++slot) {
         const int t = f3_tile(T, p, slot);
@@ -466,7 +473,7 @@ __global__ void __launch_bounds__(96 * DOMS) k_fr_schwarz3(FusedArgs a, const fl
       }
     const int i = 32 * q + lane;
     if (i < m) {
-      const Acc sc = a.fac_scale ? (Acc)a.fac_scale[d] : (Acc)1;
+      const AA sc = a.fac_scale ? (AA)a.fac_scale[d] : (AA)1;
       const float zi = (float)(z * sc * sc);
       a.z[3 * a.dom_verts[vs + i / 3] + i % 3] = zi;
       rr = (Acc)rd[i] * (Acc)rd[i];

@@ -1033,3 +1033,13 @@ extern "C" int mguso_scene_self_intersections(mguso_scene* sc, const float* x, u
   return MGUSO_OK;
 }
 
+// The fused PCG kernels in use (after the autotuner, or pcg_variant): out2 = {rows variant
+// (0: 2 lanes per block row, 1: 1, 2: 4), domain variant (0: one warp per domain, 4 per CTA;
+// 1, 2, 3: three warps per domain, 1, 2 or 4 domains per CTA)}; -1 before the first solve.
+extern "C" int mguso_scene_pcg_kernels(mguso_scene* sc, int* out2) {
+  MG_CHECK_ARG(sc && out2, "null argument");
+  out2[0] = sc->s.fr_tuned ? sc->s.fr_rows_variant : -1;
+  out2[1] = sc->s.fr_tuned ? sc->s.fr_dom_variant : -1;
+  return MGUSO_OK;
+}
+

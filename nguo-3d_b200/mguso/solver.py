@@ -64,6 +64,7 @@ def _sigs(lib):
         ("mguso_scene_ccd", i32, [vp, vp, vp, vp, vp]),
         ("mguso_scene_profile", i32, [vp, i32, vp, vp]),
         ("mguso_scene_profile_pcg", i32, [vp, i32, vp, vp]),
+        ("mguso_scene_pcg_kernels", i32, [vp, vp]),
         ("mguso_scene_self_intersections", i32, [vp, vp, vp]),
         ("mguso_batch_create", i32, [vp, vp, C.c_uint32, P(vp)]),
         ("mguso_scene_instances", i32, [vp, P(C.c_uint32), vp]),
@@ -232,6 +233,19 @@ class ImplicitSolver:
         out = np.zeros(getattr(self, "ninst", 1), np.uint32)
         check(self.lib.mguso_scene_self_intersections(self.h, ptr(xx), ptr(out)))
         return out
+
+    def pcg_kernels(self) -> tuple:
+        """(rows variant, domain variant) of the fused PCG in use (-1 before the first solve)."""
+        out = np.zeros(2, np.int32)
+        check(self.lib.mguso_scene_pcg_kernels(self.h, ptr(out)))
+        return int(out[0]), int(out[1])
+
+    def pcg_kernel_names(self) -> dict:
+        """Kernel names of the fused PCG in use, for the mixed-precision FP16-tile step."""
+        rv, dv = self.pcg_kernels()
+        lpr = {0: 2, 1: 1, 2: 4}.get(rv, 2)
+        dom = "k_fr_schwarz<double, __half>" if dv <= 0 else f"k_fr_schwarz3<double, __half, {(1, 2, 4)[dv - 1]}>"
+        return {"rows": f"k_fr_rows<double, {lpr}>", "domains": dom}
 
     def ccd(self, x, dx):
         """Step fraction the CCD filter allows along ``dx`` from ``x`` (one per instance) and
