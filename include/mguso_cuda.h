@@ -250,6 +250,8 @@ typedef struct {
                               the rows kernel (v - 1) / 4 (2, 1 or 4 lanes per block row) and the
                               Schwarz domain kernel (v - 1) % 4 (one warp per domain, 4 per CTA;
                               three warps per domain, 1, 2 or 4 domains per CTA) */
+  float constraint_tol;    /* pin gap floor as a fraction of the pin's ghat (0 = 1e-2, the
+                              reference's default ImplicitParams::constraint_tol) */
   float schwarz_weight;    /* coarse-correction weight w of the two-level form
                               z = S0 r + w C1^T S1 (C1 r) (the CLI default 0.7, main.rs:761-763) */
 } mguso_params;
@@ -373,6 +375,21 @@ int mguso_write_velocities(mguso_scene* s, const float* in);
  * reference). Counterpart: ImplicitSolver::set_kinematic_collider_positions
  * (core-engine/crates/engine-core/src/implicit.rs:1368-1398). */
 int mguso_set_kinematic_collider_positions(mguso_scene* s, const float* x);
+/* set_pins (implicit.rs:826-838): n pins (the reference's FixPair, implicit.rs:230-262), each
+ * confining vertex index[i] to a ball of radius ghat[i] around target[3 i..] with the dynamic
+ * stiffness (H w).w / |w|^2 + m / gap^2 (w = x - target, H the vertex's elastic diagonal
+ * block, gap = max(ghat - |w|, constraint_tol ghat)); a kinematic pin's stiffness is scaled
+ * by stiffness[i] and takes no part in the CCD, a static pin's ball limits the step fraction
+ * (implicit.rs:1755-1789). kinematic and stiffness may be NULL (all static, 1). All or
+ * nothing: an index out of range or a ghat <= 0 returns MGUSO_ERR_INVALID_ARG and keeps the
+ * previous pins; n = 0 clears them. All pointers host. */
+int mguso_set_pins(mguso_scene* s, uint32_t n, const uint32_t* index, const float* target, const float* ghat,
+                   const uint8_t* kinematic, const float* stiffness);
+/* set_pulls (implicit.rs:852-864): n pulls (PullPair, implicit.rs:264-282), each adding
+ * weight[i] |x - target|^2 / 2 on vertex index[i]. All or nothing: an index out of range or
+ * a weight <= 0 returns MGUSO_ERR_INVALID_ARG and keeps the previous pulls; n = 0 clears
+ * them. All pointers host. */
+int mguso_set_pulls(mguso_scene* s, uint32_t n, const uint32_t* index, const float* target, const float* weight);
 /* Element counts: hinges, shells, unique edges, static collider triangles,
  * system blocks (free-free pattern), pinned-pattern blocks. */
 int mguso_scene_info(mguso_scene* s, uint32_t* out6);

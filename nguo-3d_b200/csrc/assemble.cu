@@ -401,7 +401,83 @@ __global__ void k_colliders(const uint32_t* __restrict__ free_verts, uint32_t n_
   grad[3 * i + 2] += (float)gsum.z;
 }
 
+// ---- pins and pulls (implicit.rs:2809-2872) -----------------------------------------------
+// One thread per vertex with pins or pulls, in push order (every pin of the vertex in the
+// order they were set, then its pulls): a pin's stiffness reads the vertex's diagonal block
+// as accumulated so far (the elastic blocks and the earlier pins), k = (H w).w / |w|^2 +
+// m / gap^2 with w = x - target, gap = max(ghat - |w|, constraint_tol ghat), times the pin's
+// stiffness when kinematic; gradient k w, k on the diagonal. A pull adds weight (x - target)
+// and weight on the diagonal.
+template <class R>
+__global__ void k_pins_pulls(const uint32_t* __restrict__ pv, uint32_t n_pv, const uint32_t* __restrict__ pv_pin,
+                             const uint32_t* __restrict__ pv_pull, const float* __restrict__ pin_target,
+                             const float* __restrict__ pin_ghat, const uint8_t* __restrict__ pin_kin,
+                             const float* __restrict__ pin_stiff, const float* __restrict__ pull_target,
+                             const float* __restrict__ pull_weight, const float* __restrict__ im,
+                             const float* __restrict__ x, const uint32_t* __restrict__ diag_slot,
+                             float* __restrict__ vals, float* __restrict__ grad, float ctol) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_pv) return;
+  const uint32_t i = pv[t];
+  if (!(im[i] > 0.f)) return;
+  const R m = R(1) / (R)im[i];
+  const V3<R> xi = ld3<R>(x, i);
+  float* dblk = vals + 9 * (size_t)diag_slot[i];
+  R el[9];
+  for (int q = 0; q < 9; ++q) el[q] = (R)dblk[q];
+  V3<R> g;
+  for (uint32_t p = pv_pin[t]; p < pv_pin[t + 1]; ++p) {
+    const V3<R> w = xi - ld3<R>(pin_target, p);
+    const R d = w.length();
+    const R gh = (R)pin_ghat[p];
+    const R gap = rmax(gh - d, (R)ctol * gh);
+    const R d2 = w.length_squared();
+    R tmp = 0;
+    if (d2 > 0) {
+      const V3<R> hw(el[0] * w.x + el[1] * w.y + el[2] * w.z, el[3] * w.x + el[4] * w.y + el[5] * w.z,
+                     el[6] * w.x + el[7] * w.y + el[8] * w.z);
+      tmp = hw.dot(w) / d2;
+    }
+    R kp = tmp + m / (gap * gap);
+    if (pin_kin[p]) kp *= (R)pin_stiff[p];
+    g += w * kp;
+    el[0] += kp;
+    el[4] += kp;
+    el[8] += kp;
+  }
+  for (uint32_t q = pv_pull[t]; q < pv_pull[t + 1]; ++q) {
+    const R wt = (R)pull_weight[q];
+    g += (xi - ld3<R>(pull_target, q)) * wt;
+    el[0] += wt;
+    el[4] += wt;
+    el[8] += wt;
+  }
+  dblk[0] = (float)el[0];
+  dblk[4] = (float)el[4];
+  dblk[8] = (float)el[8];
+  grad[3 * i] += (float)g.x;
+  grad[3 * i + 1] += (float)g.y;
+  grad[3 * i + 2] += (float)g.z;
+}
+
+static int assemble_pins(Scene& s) {
+  if (!s.n_pv) return MGUSO_OK;
+  const unsigned g = ceil_div(s.n_pv, 128);
+  const float ctol = s.p.constraint_tol > 0.f ? s.p.constraint_tol : 1.0e-2f;
+  if (s.mixed)
+    k_pins_pulls<double><<<g, 128, 0, s.st>>>(s.pv.p, s.n_pv, s.pv_pin.p, s.pv_pull.p, s.pin_target.p, s.pin_ghat.p,
+                                              s.pin_kin.p, s.pin_stiff.p, s.pull_target.p, s.pull_weight.p,
+                                              s.inv_mass.p, s.x.p, s.diag_slot.p, s.A->val.p, s.grad.p, ctol);
+  else
+    k_pins_pulls<float><<<g, 128, 0, s.st>>>(s.pv.p, s.n_pv, s.pv_pin.p, s.pv_pull.p, s.pin_target.p, s.pin_ghat.p,
+                                             s.pin_kin.p, s.pin_stiff.p, s.pull_target.p, s.pull_weight.p,
+                                             s.inv_mass.p, s.x.p, s.diag_slot.p, s.A->val.p, s.grad.p, ctol);
+  MG_CUDA(cudaGetLastError());
+  return MGUSO_OK;
+}
+
 int assemble_colliders(Scene& s) {
+  MG_TRY(assemble_pins(s));
   if (!s.n_col || !s.n_free) return MGUSO_OK;
   unsigned g = ceil_div(s.n_free, 128);
   float mu = s.p.friction;  // collider friction unset: the vertex coefficient stands

@@ -417,6 +417,31 @@ __global__ void k_ccd_colliders(const uint32_t* __restrict__ free_verts, uint32_
   if (t < 1.f) atomic_min_pos(red + RED_STRIDE * vinst[i] + 1, t);
 }
 
+// static pins: the radius interpolated linearly over the extended horizon 1.25 dx, clamped
+// to land on the pin's ghat sphere (implicit.rs:1755-1789)
+__global__ void k_ccd_pins(const uint32_t* __restrict__ pin_vert, uint32_t n_pin, const uint8_t* __restrict__ pin_kin,
+                           const float* __restrict__ pin_target, const float* __restrict__ pin_ghat,
+                           const float* __restrict__ im, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
+                           const float* __restrict__ dx, unsigned int* __restrict__ red) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n_pin || pin_kin[p]) return;
+  const uint32_t i = pin_vert[p];
+  if (!(im[i] > 0.f)) return;
+  const float LS_MAX_T = 1.25f;
+  const V3<float> tg = ld3<float>(pin_target, p);
+  const float gh = pin_ghat[p];
+  const float r0 = (ld3<float>(x, i) - tg).length();
+  if (r0 >= gh) return;
+  const float r1 = (ld3<float>(x, i) + ld3<float>(dx, i) * LS_MAX_T - tg).length();
+  if (r1 > gh) {
+    const float denom = r1 - r0;
+    if (denom != 0.f) {
+      const float t = LS_MAX_T * (gh - r0) / denom;
+      if (t < 1.f) atomic_min_pos(red + RED_STRIDE * vinst[i] + 1, fmaxf(t, 0.f));
+    }
+  }
+}
+
 // CCD candidate pruning: a pair whose accd_toi (contact.rs:378-437) would return max_t at
 // its first test cannot lower the step fraction, and traversal skips whole subtrees of such
 // pairs (lbvh_visit_ccd) from the primitives' displacement boxes, refitted per CCD call.
@@ -605,7 +630,7 @@ __global__ void k_ccd_ee(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vins
   if (nacc) atomicAdd(red + RED_STRIDE * k + 8, nacc);
 }
 
-// ccd_max_step (implicit.rs:1690-1947) without strain limiting or pins, per instance. The
+// ccd_max_step (implicit.rs:1690-1947) without strain limiting, per instance. The
 // search direction is s.dx; per instance k, red[RED_STRIDE k + 0] = max |dx|, + 1 collider t,
 // + 2 self t, + 3 caps. Instances outside `active` get t = 1 and no work. Each instance runs
 // the reference's widening-radius schedule on its own displacement and edge length; a pass
@@ -617,7 +642,7 @@ int ccd_step(Scene& s, uint32_t active, float* t_out, uint32_t* cap_hits) {
     t_out[k] = 1.f;
     cap_hits[k] = 0;
   }
-  if (s.n_col == 0 && !s.p.self_collision) return MGUSO_OK;
+  if (s.n_col == 0 && !s.p.self_collision && s.n_static_pin == 0) return MGUSO_OK;
   std::vector<unsigned int> init(RED_STRIDE * K, 0u);
   for (uint32_t k = 0; k < K; ++k) {
     init[RED_STRIDE * k + 1] = f2u_host(1.f);
@@ -629,6 +654,9 @@ int ccd_step(Scene& s, uint32_t active, float* t_out, uint32_t* cap_hits) {
   if (s.n_col && s.n_free)
     k_ccd_colliders<<<ceil_div(s.n_free, 128), 128, 0, st>>>(s.free_verts.p, s.n_free, s.vinst.p, s.x.p, s.dx.p,
                                                            s.colliders.p, s.n_col, s.red.p);
+  if (s.n_static_pin)
+    k_ccd_pins<<<ceil_div(s.n_pin, 128), 128, 0, st>>>(s.pin_vert.p, s.n_pin, s.pin_kin.p, s.pin_target.p,
+                                                      s.pin_ghat.p, s.inv_mass.p, s.vinst.p, s.x.p, s.dx.p, s.red.p);
   MG_CUDA(cudaGetLastError());
   std::vector<unsigned int> h(RED_STRIDE * K);
   MG_CUDA(cudaMemcpyAsync(h.data(), s.red.p, 4 * h.size(), cudaMemcpyDeviceToHost, st));

@@ -583,6 +583,62 @@ int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>
   return MGUSO_OK;
 }
 
+// Pins and pulls grouped by vertex, each vertex's in their order of setting (the order the
+// reference pushes them), onto the device.
+int upload_pins(Scene& s) {
+  std::vector<uint32_t> verts;
+  for (auto& p : s.h_pins) verts.push_back(p.index);
+  for (auto& p : s.h_pulls) verts.push_back(p.index);
+  std::sort(verts.begin(), verts.end());
+  verts.erase(std::unique(verts.begin(), verts.end()), verts.end());
+  const uint32_t nvp = (uint32_t)verts.size();
+  std::vector<uint32_t> pin_ptr(nvp + 1, 0), pull_ptr(nvp + 1, 0);
+  auto slot = [&](uint32_t v) { return (uint32_t)(std::lower_bound(verts.begin(), verts.end(), v) - verts.begin()); };
+  for (auto& p : s.h_pins) pin_ptr[slot(p.index) + 1]++;
+  for (auto& p : s.h_pulls) pull_ptr[slot(p.index) + 1]++;
+  for (uint32_t i = 0; i < nvp; ++i) {
+    pin_ptr[i + 1] += pin_ptr[i];
+    pull_ptr[i + 1] += pull_ptr[i];
+  }
+  std::vector<uint32_t> pc(pin_ptr.begin(), pin_ptr.end() - 1), qc(pull_ptr.begin(), pull_ptr.end() - 1);
+  const size_t np = s.h_pins.size(), nq = s.h_pulls.size();
+  std::vector<float> pt(3 * np + 1), pg(np + 1), pst(np + 1), qt(3 * nq + 1), qw(nq + 1);
+  std::vector<uint8_t> pk(np + 1);
+  std::vector<uint32_t> pvert(np + 1);
+  s.n_static_pin = 0;
+  for (auto& p : s.h_pins) {
+    const uint32_t j = pc[slot(p.index)]++;
+    for (int c = 0; c < 3; ++c) pt[3 * j + c] = p.target[c];
+    pg[j] = p.ghat;
+    pst[j] = p.stiffness;
+    pk[j] = p.kinematic;
+    pvert[j] = p.index;
+    if (!p.kinematic) s.n_static_pin++;
+  }
+  for (auto& p : s.h_pulls) {
+    const uint32_t j = qc[slot(p.index)]++;
+    for (int c = 0; c < 3; ++c) qt[3 * j + c] = p.target[c];
+    qw[j] = p.weight;
+  }
+  verts.push_back(0);
+  cudaStream_t st = s.st;
+  MG_TRY(s.pv.upload(verts.data(), verts.size(), st));
+  MG_TRY(s.pv_pin.upload(pin_ptr.data(), pin_ptr.size(), st));
+  MG_TRY(s.pv_pull.upload(pull_ptr.data(), pull_ptr.size(), st));
+  MG_TRY(s.pin_vert.upload(pvert.data(), pvert.size(), st));
+  MG_TRY(s.pin_target.upload(pt.data(), pt.size(), st));
+  MG_TRY(s.pin_ghat.upload(pg.data(), pg.size(), st));
+  MG_TRY(s.pin_stiff.upload(pst.data(), pst.size(), st));
+  MG_TRY(s.pin_kin.upload(pk.data(), pk.size(), st));
+  MG_TRY(s.pull_target.upload(qt.data(), qt.size(), st));
+  MG_TRY(s.pull_weight.upload(qw.data(), qw.size(), st));
+  MG_CUDA(cudaStreamSynchronize(st));
+  s.n_pv = nvp;
+  s.n_pin = (uint32_t)np;
+  s.n_pull = (uint32_t)nq;
+  return MGUSO_OK;
+}
+
 }  // namespace mg
 
 using namespace mg;
@@ -756,6 +812,46 @@ int mguso_set_kinematic_collider_positions(mguso_scene* sc, const float* x) {
   MG_CUDA(cudaStreamSynchronize(s.st));
   s.static_done = false;  // contributions of all-pinned elements move with the collider
   return MGUSO_OK;
+}
+
+// set_pins / set_pulls (implicit.rs:826-864): all or nothing.
+int mguso_set_pins(mguso_scene* sc, uint32_t n, const uint32_t* index, const float* target, const float* ghat,
+                   const uint8_t* kinematic, const float* stiffness) {
+  MG_CHECK_ARG(sc && (n == 0 || (index && target && ghat)), "null argument");
+  Scene& s = sc->s;
+  std::vector<Scene::HostPin> pins(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    MG_CHECK_ARG(index[i] < s.nv, "set_pins: a pin's vertex is out of range");
+    MG_CHECK_ARG(std::isfinite(ghat[i]) && ghat[i] > 0.f, "set_pins: a pin's ghat must be positive");
+    MG_CHECK_ARG(std::isfinite(target[3 * i]) && std::isfinite(target[3 * i + 1]) && std::isfinite(target[3 * i + 2]),
+                 "set_pins: a pin's target is not finite");
+    pins[i].index = index[i];
+    for (int c = 0; c < 3; ++c) pins[i].target[c] = target[3 * i + c];
+    pins[i].ghat = ghat[i];
+    pins[i].kinematic = kinematic ? (kinematic[i] ? 1 : 0) : 0;
+    pins[i].stiffness = stiffness ? stiffness[i] : 1.f;
+  }
+  MG_CUDA(cudaSetDevice(s.ctx->device));
+  s.h_pins = std::move(pins);
+  return upload_pins(s);
+}
+
+int mguso_set_pulls(mguso_scene* sc, uint32_t n, const uint32_t* index, const float* target, const float* weight) {
+  MG_CHECK_ARG(sc && (n == 0 || (index && target && weight)), "null argument");
+  Scene& s = sc->s;
+  std::vector<Scene::HostPull> pulls(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    MG_CHECK_ARG(index[i] < s.nv, "set_pulls: a pull's vertex is out of range");
+    MG_CHECK_ARG(std::isfinite(weight[i]) && weight[i] > 0.f, "set_pulls: a pull's weight must be positive");
+    MG_CHECK_ARG(std::isfinite(target[3 * i]) && std::isfinite(target[3 * i + 1]) && std::isfinite(target[3 * i + 2]),
+                 "set_pulls: a pull's target is not finite");
+    pulls[i].index = index[i];
+    for (int c = 0; c < 3; ++c) pulls[i].target[c] = target[3 * i + c];
+    pulls[i].weight = weight[i];
+  }
+  MG_CUDA(cudaSetDevice(s.ctx->device));
+  s.h_pulls = std::move(pulls);
+  return upload_pins(s);
 }
 
 int mguso_read_positions(mguso_scene* s, float* out) { return copy_state(s, s->s.x, out, nullptr); }

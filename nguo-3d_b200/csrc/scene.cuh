@@ -108,6 +108,24 @@ struct Scene {
   DevBuf<float> valp;                       // Pp values
   DevBuf<float> grad, rhs;
 
+  // pins (FixPair, implicit.rs:230-262) and pulls (PullPair, implicit.rs:264-282), grouped by
+  // vertex in their order of setting: pv the vertices having any, pv_pin / pv_pull the ranges
+  // (n_pv + 1 each) into the pin and pull arrays
+  struct HostPin {
+    uint32_t index;
+    float target[3], ghat, stiffness;
+    uint8_t kinematic;
+  };
+  struct HostPull {
+    uint32_t index;
+    float target[3], weight;
+  };
+  std::vector<HostPin> h_pins;
+  std::vector<HostPull> h_pulls;
+  uint32_t n_pv = 0, n_pin = 0, n_pull = 0, n_static_pin = 0;
+  DevBuf<uint32_t> pv, pv_pin, pv_pull, pin_vert;
+  DevBuf<float> pin_target, pin_ghat, pin_stiff, pull_target, pull_weight;
+  DevBuf<uint8_t> pin_kin;
   // colliders
   uint32_t n_col = 0;
   std::vector<float> h_colliders;
@@ -192,7 +210,8 @@ int scene_step(Scene& s, mguso_step_stats* out);
 
 // assembly (assemble.cu)
 int assemble_elastic(Scene& s);
-int assemble_colliders(Scene& s);
+int assemble_colliders(Scene& s);  // pins and pulls first, then the analytic colliders
+int upload_pins(Scene& s);          // groups h_pins / h_pulls by vertex onto the device
 int assemble_contacts(Scene& s, uint32_t nst);
 int contact_stiffness(Scene& s, uint32_t nst);  // records s.contact_k from the gathered blocks
 int finish_rhs(Scene& s);

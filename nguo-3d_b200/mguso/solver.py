@@ -24,7 +24,7 @@ _PARAM_FIELDS = [("dt", C.c_float), ("gravity", C.c_float * 3), ("newton_iters",
                  ("cg_max_iter", C.c_uint32), ("floor_y", C.c_float), ("newton_tol", C.c_float),
                  ("precond", C.c_int), ("schwarz_domain", C.c_uint32), ("precision", C.c_int),
                  ("pcg_mode", C.c_int), ("factor_storage", C.c_int), ("schwarz_levels", C.c_uint32),
-                 ("pcg_variant", C.c_int), ("schwarz_weight", C.c_float)]
+                 ("pcg_variant", C.c_int), ("constraint_tol", C.c_float), ("schwarz_weight", C.c_float)]
 
 
 class Params(C.Structure):
@@ -58,6 +58,8 @@ def _sigs(lib):
         ("mguso_read_velocities", i32, [vp, vp]),
         ("mguso_write_velocities", i32, [vp, vp]),
         ("mguso_set_kinematic_collider_positions", i32, [vp, vp]),
+        ("mguso_set_pins", i32, [vp, C.c_uint32, vp, vp, vp, vp, vp]),
+        ("mguso_set_pulls", i32, [vp, C.c_uint32, vp, vp, vp]),
         ("mguso_scene_info", i32, [vp, vp]),
         ("mguso_scene_spmv_time", i32, [vp, i32, P(C.c_float), P(C.c_double)]),
         ("mguso_scene_assemble", i32, [vp, vp, vp, vp]),
@@ -196,6 +198,29 @@ class ImplicitSolver:
         MgusoError, changing nothing, without a static collider or with a non-finite row."""
         a = np.ascontiguousarray(x, np.float32).reshape(self.nv, 3)
         check(self.lib.mguso_set_kinematic_collider_positions(self.h, ptr(a)))
+
+    def set_pins(self, pins) -> None:
+        """ImplicitSolver::set_pins (implicit.rs:826-838): each pin (index, target xyz, ghat,
+        kinematic, stiffness). All or nothing: raises MgusoError, keeping the previous pins,
+        for an index out of range or a ghat <= 0; an empty list clears them."""
+        n = len(pins)
+        idx = np.array([p[0] for p in pins], np.uint32)
+        tgt = np.array([p[1] for p in pins], np.float32).reshape(n, 3)
+        gh = np.array([p[2] for p in pins], np.float32)
+        kin = np.array([1 if p[3] else 0 for p in pins], np.uint8)
+        st = np.array([p[4] for p in pins], np.float32)
+        check(self.lib.mguso_set_pins(self.h, n, ptr(idx) if n else None, ptr(tgt) if n else None,
+                                      ptr(gh) if n else None, ptr(kin) if n else None, ptr(st) if n else None))
+
+    def set_pulls(self, pulls) -> None:
+        """ImplicitSolver::set_pulls (implicit.rs:852-864): each pull (index, target xyz,
+        weight); all or nothing as set_pins."""
+        n = len(pulls)
+        idx = np.array([p[0] for p in pulls], np.uint32)
+        tgt = np.array([p[1] for p in pulls], np.float32).reshape(n, 3)
+        w = np.array([p[2] for p in pulls], np.float32)
+        check(self.lib.mguso_set_pulls(self.h, n, ptr(idx) if n else None, ptr(tgt) if n else None,
+                                       ptr(w) if n else None))
 
     def info(self) -> dict:
         out = np.zeros(6, np.uint32)
