@@ -246,10 +246,11 @@ typedef struct {
   uint32_t schwarz_levels; /* 1 (or 0): one-level Schwarz (SchwarzCpu, linsolve.rs:463-520);
                               2: two-level Galerkin Schwarz (SchwarzMlCpu, linsolve.rs:534-836) */
   int pcg_variant;         /* kernels of the fused PCG (pcg_mode 0): 0 = chosen by the autotuner
-                              at the scene's first solve (cached per system size); v >= 1 fixes
-                              the rows kernel (v - 1) / 4 (2, 1 or 4 lanes per block row) and the
-                              Schwarz domain kernel (v - 1) % 4 (one warp per domain, 4 per CTA;
-                              three warps per domain, 1, 2 or 4 domains per CTA) */
+                              at the scene's first solve (cached per system size); v in 1..16
+                              fixes the rows kernel (v - 1) / 4 (0, 1, 2: 2, 1 or 4 lanes per
+                              block row over the BSR; 3: one lane per row over a sliced-ELL copy)
+                              and the Schwarz domain kernel (v - 1) % 4 (one warp per domain, 4
+                              per CTA; three warps per domain, 1, 2 or 4 domains per CTA) */
   float constraint_tol;    /* pin gap floor as a fraction of the pin's ghat (0 = 1e-2, the
                               reference's default ImplicitParams::constraint_tol) */
   float schwarz_weight;    /* coarse-correction weight w of the two-level form
@@ -413,7 +414,7 @@ int mguso_scene_profile(mguso_scene* s, int reps, float* us4, double* bytes4);
  * their algorithmic bytes per launch. Clobbers the PCG scratch (not the state). */
 int mguso_scene_profile_pcg(mguso_scene* s, int iters, float* us2, double* bytes2);
 /* The fused PCG kernels in use, as the autotuner (or pcg_variant) chose them: out2 = {rows
- * kernel: 0 two lanes per block row, 1 one, 2 four; domain kernel: 0 one warp per domain and
+ * kernel: 0 two lanes per block row, 1 one, 2 four, 3 sliced ELL; domain kernel: 0 one warp per domain and
  * four domains per CTA, 1/2/3 three warps per domain and 1/2/4 domains per CTA}; -1 before
  * the scene's first solve. */
 int mguso_scene_pcg_kernels(mguso_scene* s, int* out2);

@@ -45,6 +45,8 @@ struct FusedArgs {
   const float* fac_scale;  // per domain (FP16 tiles), else null
   const uint8_t* dom_diag;  // block-diagonal domains (per-vertex factors in vfac)
   const float* vfac;
+  const uint32_t *sell_base, *sell_inst, *sell_col;  // SELL rows variant
+  const float* sell_val;
   const float* b;
   float *x, *r, *z, *ap;
   float tol;
@@ -76,6 +78,37 @@ __device__ __forceinline__ bool last_cta(uint32_t* counter) {
   __syncthreads();
   if (s_last) __threadfence();
   return s_last;
+}
+
+// finish of the rows kernel: alpha per instance, partials summed in CTA order
+__device__ __forceinline__ void rows_finish(const FusedArgs& a) {
+  const uint32_t K = a.ninst;
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int w = tid >> 5;
+  for (uint32_t q = w; q < K; q += FR_THREADS / 32) {
+    const uint32_t cb = a.lay[LAY + q], ce = a.lay[LAY + q + 1];
+    double t = 0;
+    for (uint32_t c = cb + lane; c < ce; c += 32) t += ((volatile double*)a.part)[c];
+    t = warp_sum(t);
+    if (lane == 0) {
+      FusedInst& I = a.inst[q];
+      I.upd = 0;
+      if (!I.done) {
+        if (!(t > 0.0)) {
+          I.done = 1;
+          I.status |= ST_PCG_BREAKDOWN;
+        } else {
+          I.alpha = I.rz / t;
+          I.upd = 1;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    a.ctl->counter[0] = 0;
+    __threadfence();
+  }
 }
 
 template <class Acc, int FR_LPR>
@@ -138,32 +171,94 @@ __global__ void __launch_bounds__(FR_THREADS) k_fr_rows(FusedArgs a, const float
   const Acc s = block_sum<Acc>(acc);
   if (tid == 0) a.part[blockIdx.x] = (double)s;
   if (!last_cta(&a.ctl->counter[0])) return;
-  // alpha per instance, partials summed in CTA order
-  const int w = tid >> 5;
-  for (uint32_t q = w; q < K; q += FR_THREADS / 32) {
-    const uint32_t cb = a.lay[LAY + q], ce = a.lay[LAY + q + 1];
-    double t = 0;
-    for (uint32_t c = cb + lane; c < ce; c += 32) t += ((volatile double*)a.part)[c];
-    t = warp_sum(t);
-    if (lane == 0) {
-      FusedInst& I = a.inst[q];
-      I.upd = 0;
-      if (!I.done) {
-        if (!(t > 0.0)) {
-          I.done = 1;
-          I.status |= ST_PCG_BREAKDOWN;
-        } else {
-          I.alpha = I.rz / t;
-          I.upd = 1;
-        }
+  rows_finish(a);
+}
+
+// Rows kernel over the sliced-ELL copy of Ps: one warp per slice of 32 rows, one lane per
+// row; each slot's column and nine values are read as coalesced 128-byte rows of the slice
+// (padding slots have zero values and the row's own column), then the row's contact blocks.
+// Same iteration and finish as k_fr_rows.
+template <class Acc>
+__global__ void __launch_bounds__(FR_THREADS) k_fr_rows_sell(FusedArgs a, const float* __restrict__ po,
+                                                             float* __restrict__ pn) {
+  if (a.ctl->all_done) return;
+  const uint32_t K = a.ninst;
+  const int k = cta_instance(a.lay + LAY, K);
+  const uint32_t c0 = __ldg(a.lay + LAY + k), lc = blockIdx.x - c0;
+  const uint32_t row0 = __ldg(a.lay + k), row1 = __ldg(a.lay + k + 1);
+  const bool done = a.inst[k].done != 0;
+  const float be = (float)a.inst[k].beta;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  Acc acc = 0;
+  const uint32_t sl = lc * (FR_THREADS / 32) + w;  // slice within the instance
+  const uint32_t row = row0 + 32 * sl + lane;
+  if (!done && row0 + 32 * sl < row1) {
+    const uint32_t gs = __ldg(a.sell_inst + k) + sl;
+    const uint32_t b0 = __ldg(a.sell_base + gs), b1 = __ldg(a.sell_base + gs + 1);
+    Acc y0 = 0, y1 = 0, y2 = 0;
+    auto gather = [&](uint32_t c, Acc& x0, Acc& x1, Acc& x2) {
+      x0 = (Acc)fmaf(be, po[3 * c], a.z[3 * c]);
+      x1 = (Acc)fmaf(be, po[3 * c + 1], a.z[3 * c + 1]);
+      x2 = (Acc)fmaf(be, po[3 * c + 2], a.z[3 * c + 2]);
+    };
+    if (row < row1) {
+#pragma unroll 2
+      for (uint32_t b = b0; b < b1; ++b) {
+        const uint32_t c = __ldg(a.sell_col + 32 * (size_t)b + lane);
+        const float* m = a.sell_val + 288 * (size_t)b + lane;
+        Acc x0, x1, x2;
+        gather(c, x0, x1, x2);
+        y0 = fr_fma((Acc)__ldcs(m + 0), x0, y0);
+        y0 = fr_fma((Acc)__ldcs(m + 32), x1, y0);
+        y0 = fr_fma((Acc)__ldcs(m + 64), x2, y0);
+        y1 = fr_fma((Acc)__ldcs(m + 96), x0, y1);
+        y1 = fr_fma((Acc)__ldcs(m + 128), x1, y1);
+        y1 = fr_fma((Acc)__ldcs(m + 160), x2, y1);
+        y2 = fr_fma((Acc)__ldcs(m + 192), x0, y2);
+        y2 = fr_fma((Acc)__ldcs(m + 224), x1, y2);
+        y2 = fr_fma((Acc)__ldcs(m + 256), x2, y2);
       }
+      const uint32_t ce = __ldg(a.crp + row + 1);
+      for (uint32_t kk = __ldg(a.crp + row); kk < ce; ++kk) {
+        const float* m9 = a.cval + 9 * (size_t)kk;
+        Acc x0, x1, x2;
+        gather(__ldg(a.ccol + kk), x0, x1, x2);
+        y0 = fr_fma((Acc)__ldg(m9 + 0), x0, y0);
+        y0 = fr_fma((Acc)__ldg(m9 + 1), x1, y0);
+        y0 = fr_fma((Acc)__ldg(m9 + 2), x2, y0);
+        y1 = fr_fma((Acc)__ldg(m9 + 3), x0, y1);
+        y1 = fr_fma((Acc)__ldg(m9 + 4), x1, y1);
+        y1 = fr_fma((Acc)__ldg(m9 + 5), x2, y1);
+        y2 = fr_fma((Acc)__ldg(m9 + 6), x0, y2);
+        y2 = fr_fma((Acc)__ldg(m9 + 7), x1, y2);
+        y2 = fr_fma((Acc)__ldg(m9 + 8), x2, y2);
+      }
+      const float f0 = (float)y0, f1 = (float)y1, f2 = (float)y2;
+      const float q0 = fmaf(be, po[3 * row], a.z[3 * row]);
+      const float q1 = fmaf(be, po[3 * row + 1], a.z[3 * row + 1]);
+      const float q2 = fmaf(be, po[3 * row + 2], a.z[3 * row + 2]);
+      pn[3 * row] = q0;
+      pn[3 * row + 1] = q1;
+      pn[3 * row + 2] = q2;
+      a.ap[3 * row] = f0;
+      a.ap[3 * row + 1] = f1;
+      a.ap[3 * row + 2] = f2;
+      acc = (Acc)q0 * (Acc)f0 + (Acc)q1 * (Acc)f1 + (Acc)q2 * (Acc)f2;
     }
   }
-  __syncthreads();
-  if (tid == 0) {
-    a.ctl->counter[0] = 0;
-    __threadfence();
-  }
+  const Acc s = block_sum<Acc>(acc);
+  if (tid == 0) a.part[blockIdx.x] = (double)s;
+  if (!last_cta(&a.ctl->counter[0])) return;
+  rows_finish(a);
+}
+
+// Ps values into the sliced-ELL copy (after every assembly; padding slots stay zero)
+__global__ void k_sell_pack(const float* __restrict__ val, const uint32_t* __restrict__ pos, uint32_t nnz,
+                            float* __restrict__ sv) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 9 * nnz) return;
+  const uint32_t k = i / 9, q = i - 9 * k;
+  sv[pos[k] + 32 * q] = val[i];
 }
 
 // finish of the domain kernel (and of the initialisation): instance sums of r.r and r.z
@@ -544,11 +639,13 @@ __global__ void __launch_bounds__(FD_THREADS) k_fr_bj(FusedArgs a, const float* 
 
 namespace {
 // The fused kernels' variants the autotuner chooses between (per scene, cached per system
-// size): rows kernel with 2, 1 or 4 lanes per block row; Schwarz domain kernel with one warp
-// per domain (4 domains per CTA) or three warps per domain (1, 2 or 4 domains per CTA).
-constexpr int N_ROWS_VARIANTS = 3;
+// size): rows kernel with 2, 1 or 4 lanes per block row over the BSR, or one lane per row over
+// the sliced-ELL copy; Schwarz domain kernel with one warp per domain (4 domains per CTA) or
+// three warps per domain (1, 2 or 4 domains per CTA).
+constexpr int N_ROWS_VARIANTS = 4;
 constexpr int N_DOM_VARIANTS = 4;
-constexpr int ROWS_LPR[N_ROWS_VARIANTS] = {2, 1, 4};
+constexpr int ROWS_LPR[N_ROWS_VARIANTS] = {2, 1, 4, 1};
+constexpr int ROWS_SELL = 3;
 
 struct Launch {
   void* rows;
@@ -563,6 +660,7 @@ void* rows_fn(int rv) {
   switch (rv) {
     case 1: return (void*)k_fr_rows<Acc, 1>;
     case 2: return (void*)k_fr_rows<Acc, 4>;
+    case 3: return (void*)k_fr_rows_sell<Acc>;
     default: return (void*)k_fr_rows<Acc, 2>;
   }
 }
@@ -614,6 +712,44 @@ Launch fused_kernels(const Scene& s, int rv, int dv) {
   return L;
 }
 }  // namespace
+
+// The sliced-ELL copy of Ps (built once per scene: the pattern is fixed): slices of 32
+// consecutive rows of one instance, each as wide as its longest row.
+static int sell_build(Scene& s) {
+  const auto& rp = s.Ps.h_row_ptr;
+  const auto& cl = s.Ps.h_col;
+  const uint32_t K = s.ninst;
+  std::vector<uint32_t> base(1, 0), inst(K + 1, 0), col, pos(std::max<uint32_t>(s.Ps.nnz, 1), 0);
+  for (uint32_t k = 0; k < K; ++k) {
+    inst[k] = (uint32_t)base.size() - 1;
+    for (uint32_t r0 = s.inst_vert[k]; r0 < s.inst_vert[k + 1]; r0 += 32) {
+      const uint32_t r1 = std::min<uint32_t>(r0 + 32, s.inst_vert[k + 1]);
+      uint32_t w = 0;
+      for (uint32_t r = r0; r < r1; ++r) w = std::max<uint32_t>(w, rp[r + 1] - rp[r]);
+      const uint32_t b = base.back();
+      col.resize(32 * (size_t)(b + w));
+      for (uint32_t j = 0; j < w; ++j)
+        for (uint32_t l = 0; l < 32; ++l) {
+          const uint32_t r = r0 + l;
+          const bool has = r < r1 && rp[r] + j < rp[r + 1];
+          col[32 * (size_t)(b + j) + l] = has ? cl[rp[r] + j] : (r < r1 ? r : r0);
+          if (has) pos[rp[r] + j] = 288 * (b + j) + l;
+        }
+      base.push_back(b + w);
+    }
+  }
+  inst[K] = (uint32_t)base.size() - 1;
+  cudaStream_t st = s.st;
+  MG_TRY(s.sell_base.upload(base.data(), base.size(), st));
+  MG_TRY(s.sell_inst.upload(inst.data(), inst.size(), st));
+  MG_TRY(s.sell_col.upload(col.data(), std::max<size_t>(col.size(), 1), st));
+  MG_TRY(s.sell_pos.upload(pos.data(), pos.size(), st));
+  MG_TRY(s.sell_val.reserve(std::max<size_t>(288 * (size_t)base.back(), 1)));
+  MG_CUDA(cudaMemsetAsync(s.sell_val.p, 0, 4 * std::max<size_t>(288 * (size_t)base.back(), 1), st));
+  MG_CUDA(cudaStreamSynchronize(st));
+  s.sell_built = true;
+  return MGUSO_OK;
+}
 
 // Layout of the fused kernels over the scene's instances and the arguments of both; resets
 // the per-instance state (instances outside `active` start done) on the scene's stream.
@@ -686,6 +822,16 @@ static int fused_prepare(Scene& s, const uint32_t* h_inst_row, uint32_t K, uint3
     a.fac_scale = sw->half ? sw->fac_scale.p : nullptr;
     a.dom_diag = sw->dom_diag.p;
     a.vfac = sw->vfac.p;
+  }
+  if (s.fr_rows_variant == ROWS_SELL) {
+    if (!s.sell_built) MG_TRY(sell_build(s));
+    // the system's current values into the sliced-ELL copy
+    k_sell_pack<<<ceil_div(9 * (size_t)s.Ps.nnz, 256), 256, 0, st>>>(s.A->val.p, s.sell_pos.p, s.Ps.nnz, s.sell_val.p);
+    MG_CUDA(cudaGetLastError());
+    a.sell_base = s.sell_base.p;
+    a.sell_inst = s.sell_inst.p;
+    a.sell_col = s.sell_col.p;
+    a.sell_val = s.sell_val.p;
   }
   a.b = w.b.p;
   a.x = w.x.p;

@@ -112,7 +112,7 @@ static int validate_desc(const mguso_scene_desc* d) {
   MG_CHECK_ARG(d->params.pcg_mode >= 0 && d->params.pcg_mode <= 2, "scene: pcg_mode must be 0, 1 or 2");
   MG_CHECK_ARG(d->params.factor_storage >= 0 && d->params.factor_storage <= 2, "scene: factor_storage must be 0, 1 or 2");
   MG_CHECK_ARG(d->params.schwarz_levels <= 2, "scene: schwarz_levels must be 1 or 2");
-  MG_CHECK_ARG(d->params.pcg_variant >= 0 && d->params.pcg_variant <= 12, "scene: pcg_variant must be in [0, 12]");
+  MG_CHECK_ARG(d->params.pcg_variant >= 0 && d->params.pcg_variant <= 16, "scene: pcg_variant must be in [0, 16]");
   MG_CHECK_ARG(std::isfinite(d->params.schwarz_weight) && d->params.schwarz_weight >= 0.f,
                "scene: schwarz_weight must be finite and >= 0");
   return MGUSO_OK;

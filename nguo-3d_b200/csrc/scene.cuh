@@ -173,6 +173,13 @@ struct Scene {
   DevBuf<double> fr_part;
   cudaGraphExec_t fr_exec = nullptr;
   int fr_rows_variant = 0, fr_dom_variant = 0;  // the fused kernels in use (see pcg_fused.cu)
+  // sliced-ELL copy of Ps for the rows kernel's SELL variant: slices of 32 consecutive rows of
+  // one instance, slot base per slice (sell_base, nslices + 1), per instance the first slice
+  // (sell_inst, ninst + 1), columns (sell_col, 32 per slot), values SoA (288 floats per slot:
+  // entry q of the 32 rows at q * 32 + lane) and each Ps block's value offset (sell_pos)
+  bool sell_built = false;
+  DevBuf<uint32_t> sell_base, sell_inst, sell_col, sell_pos;
+  DevBuf<float> sell_val;
   bool fr_tuned = false;
   ~Scene() {
     if (fr_exec) cudaGraphExecDestroy(fr_exec);

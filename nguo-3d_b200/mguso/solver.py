@@ -268,9 +268,9 @@ class ImplicitSolver:
     def pcg_kernel_names(self) -> dict:
         """Kernel names of the fused PCG in use, for the mixed-precision FP16-tile step."""
         rv, dv = self.pcg_kernels()
-        lpr = {0: 2, 1: 1, 2: 4}.get(rv, 2)
+        rows = "k_fr_rows_sell<double>" if rv == 3 else f"k_fr_rows<double, {({0: 2, 1: 1, 2: 4}).get(rv, 2)}>"
         dom = "k_fr_schwarz<double, __half>" if dv <= 0 else f"k_fr_schwarz3<double, __half, {(1, 2, 4)[dv - 1]}>"
-        return {"rows": f"k_fr_rows<double, {lpr}>", "domains": dom}
+        return {"rows": rows, "domains": dom}
 
     def ccd(self, x, dx):
         """Step fraction the CCD filter allows along ``dx`` from ``x`` (one per instance) and
