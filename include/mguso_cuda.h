@@ -251,6 +251,11 @@ typedef struct {
                               block row over the BSR; 3: one lane per row over a sliced-ELL copy)
                               and the Schwarz domain kernel (v - 1) % 4 (one warp per domain, 4
                               per CTA; three warps per domain, 1, 2 or 4 domains per CTA) */
+  float membrane_warp;     /* Baraff-Witkin membrane stiffnesses (ImplicitParams::membrane_warp /
+                              _weft / _shear, implicit.rs:39-43): 0 = off. The membrane covers
+                              every triangle of tris, rest shape from the initial positions */
+  float membrane_weft;
+  float membrane_shear;
   float constraint_tol;    /* pin gap floor as a fraction of the pin's ghat (0 = 1e-2, the
                               reference's default ImplicitParams::constraint_tol) */
   float schwarz_weight;    /* coarse-correction weight w of the two-level form

@@ -402,6 +402,8 @@ int mguso_adjoint_create(mguso_ctx* ctx, const mguso_scene_desc* d, const mguso_
   MG_CHECK_ARG(d->nstitch == 0 || spec->stitch_seam, "adjoint: stitch seams required");
   MG_CHECK_ARG(d->positions && d->inv_mass && d->shell_faces, "adjoint: null arrays");
   MG_CHECK_ARG(!(d->params.friction > 0), "adjoint: friction is not differentiated (set friction = 0)");
+  MG_CHECK_ARG(!(d->params.membrane_warp > 0 || d->params.membrane_weft > 0 || d->params.membrane_shear > 0),
+               "adjoint: the Baraff-Witkin membrane is not differentiated (set its stiffnesses to 0)");
   auto a = std::make_unique<mguso_adjoint>();
   a->ctx = ctx;
   a->base = *d;

@@ -139,6 +139,35 @@ __global__ void k_spring(const uint32_t* __restrict__ act, uint32_t n, const uin
   g[3] = -ga.x; g[4] = -ga.y; g[5] = -ga.z;
 }
 
+// ---- Baraff-Witkin membrane (implicit.rs:2532-2596) ---------------------------------------
+// One element's 9 blocks (each the sum of its warp, weft and shear terms) and 3 gradient
+// entries, in FP32 as the reference.
+__global__ void __launch_bounds__(128) k_membrane(const uint32_t* __restrict__ act, uint32_t n,
+                                                  const uint32_t* __restrict__ mv, const float* __restrict__ dm,
+                                                  const float* __restrict__ area, float kw, float kf, float ks,
+                                                  const float* __restrict__ x, float* __restrict__ cb,
+                                                  float* __restrict__ ge) {
+  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const uint32_t e = act[q];
+  const V3<float> p[3] = {ld3<float>(x, mv[3 * e]), ld3<float>(x, mv[3 * e + 1]), ld3<float>(x, mv[3 * e + 2])};
+  const float d4[4] = {dm[4 * e], dm[4 * e + 1], dm[4 * e + 2], dm[4 * e + 3]};
+  V3<float> g[3];
+  float h[9][9];
+  membrane_grad_hess<float>(p, d4, area[e], kw, kf, ks, g, h);
+  float* blk = cb + 81 * (size_t)e;
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b)
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) blk[9 * (3 * a + b) + 3 * r + c] = h[3 * a + r][3 * b + c];
+  float* gg = ge + 9 * (size_t)e;
+  for (int a = 0; a < 3; ++a) {
+    gg[3 * a] = g[a].x;
+    gg[3 * a + 1] = g[a].y;
+    gg[3 * a + 2] = g[a].z;
+  }
+}
+
 // ---- StVK shells ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(128) k_shell(const uint32_t* __restrict__ act, uint32_t n,
                                                const uint32_t* __restrict__ sv, const float* __restrict__ dm,
@@ -286,7 +315,7 @@ int assemble_elastic(Scene& s) {
   // all-pinned elements once (their contributions never change), then the active ones
   if (!s.static_done) {
     // the full element lists, built from identity index arrays
-    std::vector<uint32_t> ids(std::max({s.n_stitch, s.n_spring, s.n_shell, s.n_hinge, 1u}));
+    std::vector<uint32_t> ids(std::max({s.n_stitch, s.n_spring, s.n_mem, s.n_shell, s.n_hinge, 1u}));
     for (uint32_t i = 0; i < ids.size(); ++i) ids[i] = i;
     DevBuf<uint32_t> all;
     MG_TRY(all.upload(ids.data(), ids.size(), st));
@@ -296,6 +325,10 @@ int assemble_elastic(Scene& s) {
     if (s.n_spring)
       k_spring<<<grid(s.n_spring), 128, 0, st>>>(all.p, s.n_spring, s.spring_v.p, s.spring_rest.p, s.p.stiffness,
                                                  s.x.p, cb + 9 * s.cb_spring, ge + 3 * s.gb_spring, ex_spring);
+    if (s.n_mem)
+      k_membrane<<<grid(s.n_mem), 128, 0, st>>>(all.p, s.n_mem, s.mem_v.p, s.mem_dm.p, s.mem_area.p,
+                                                s.p.membrane_warp, s.p.membrane_weft, s.p.membrane_shear, s.x.p,
+                                                cb + 9 * s.cb_mem, ge + 3 * s.gb_mem);
     if (s.n_shell)
       k_shell<<<grid(s.n_shell), 128, 0, st>>>(all.p, s.n_shell, s.shell_v.p, s.shell_dm.p, s.shell_area.p,
                                                s.shell_mu.p, s.shell_lam.p, s.p.eiganalysis_eps, s.x.p,
@@ -313,6 +346,10 @@ int assemble_elastic(Scene& s) {
     if (s.n_act_spring)
       k_spring<<<grid(s.n_act_spring), 128, 0, st>>>(s.act_spring.p, s.n_act_spring, s.spring_v.p, s.spring_rest.p,
                                                      s.p.stiffness, s.x.p, cb + 9 * s.cb_spring, ge + 3 * s.gb_spring, ex_spring);
+    if (s.n_act_mem)
+      k_membrane<<<grid(s.n_act_mem), 128, 0, st>>>(s.act_mem.p, s.n_act_mem, s.mem_v.p, s.mem_dm.p, s.mem_area.p,
+                                                    s.p.membrane_warp, s.p.membrane_weft, s.p.membrane_shear, s.x.p,
+                                                    cb + 9 * s.cb_mem, ge + 3 * s.gb_mem);
     if (s.n_act_shell)
       k_shell<<<grid(s.n_act_shell), 128, 0, st>>>(s.act_shell.p, s.n_act_shell, s.shell_v.p, s.shell_dm.p,
                                                    s.shell_area.p, s.shell_mu.p, s.shell_lam.p, s.p.eiganalysis_eps,

@@ -579,4 +579,115 @@ __device__ inline void dihedral_grad(const V3<R> p[4], V3<R> g[4]) {
   g[3] = g3;
 }
 
+// ---------------------------------------------------------------------------------------
+// Baraff-Witkin membrane (engine-core/src/membrane.rs): warp, weft and shear conditions of
+// the deformation's columns wu, wv (F = Ds Dm^-1, Dm^-1 row-major dm[4]): Cu = |wu| - 1,
+// Cv = |wv| - 1, Csh = wu.wv; energy area (kw Cu^2 + kf Cv^2 + ks Csh^2) / 2; the stretch
+// blocks use n n^T + max(0, 1 - 1/|w|)(I - n n^T) and the shear block its eigen-projected
+// 6x6 form (membrane.rs:100-205). Gradient per vertex (g[a]) and 3x3 blocks h[3 a + b].
+template <class R>
+__device__ void bw_add_outer(R m[3][3], const V3<R>& u, const V3<R>& v, R s) {
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) m[r][c] += s * u[r] * v[c];
+}
+
+template <class R>
+__device__ void bw_proj_perp(const V3<R>& w, R q[3][3]) {
+  const V3<R> n = w.normalize_or_zero();
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) q[r][c] = (r == c ? R(1) : R(0)) - n[r] * n[c];
+}
+
+template <class R>
+__device__ void bw_stretch_material(const V3<R>& w, R m[3][3]) {
+  const R s = w.length();
+  const V3<R> n = w.normalize_or_zero();
+  const R perp = s > R(1.0e-6) ? rmax(R(1) - R(1) / s, R(0)) : R(0);
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      const R nnt = n[r] * n[c];
+      m[r][c] = nnt + perp * ((r == c ? R(1) : R(0)) - nnt);
+    }
+}
+
+template <class R>
+__device__ void bw_shear_material(const V3<R>& wu, const V3<R>& wv, R m[4][3][3]) {
+  const R f = wu.dot(wv);
+  const R a = wu.length_squared() + wv.length_squared();
+  const R disc = sqrt(rmax(a * a + R(12) * f * f, R(0)));
+  const R mu[2] = {R(0.5) * (a + disc), R(0.5) * (a - disc)};
+  for (int b = 0; b < 4; ++b)
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) m[b][r][c] = 0;
+  for (int k = 0; k < 2; ++k) {
+    const V3<R> top = wv * mu[k] + wu * f, bot = wu * mu[k] + wv * f;
+    const R n = top.length_squared() + bot.length_squared();
+    if (n > R(1e-20)) {
+      const R sc = rmax(mu[k], R(0)) / n;
+      bw_add_outer(m[0], top, top, sc);
+      bw_add_outer(m[1], top, bot, sc);
+      bw_add_outer(m[2], bot, top, sc);
+      bw_add_outer(m[3], bot, bot, sc);
+    }
+  }
+  const R fp = R(0.5) * rmax(f, R(0));
+  if (fp != 0) {
+    R qp[3][3];
+    bw_proj_perp(wu + wv, qp);
+    for (int b = 0; b < 4; ++b)
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) m[b][r][c] += fp * qp[r][c];
+  }
+  const R fm = R(0.5) * rmax(-f, R(0));
+  if (fm != 0) {
+    R qm[3][3];
+    bw_proj_perp(wv - wu, qm);
+    const R sgn[4] = {R(1), R(-1), R(-1), R(1)};
+    for (int b = 0; b < 4; ++b)
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) m[b][r][c] += (sgn[b] * fm) * qm[r][c];
+  }
+}
+
+template <class R>
+__device__ void membrane_grad_hess(const V3<R> p[3], const R dm[4], R area, R kw, R kf, R ks, V3<R> g[3],
+                                   R h[9][9]) {
+  const V3<R> ds0 = p[1] - p[0], ds1 = p[2] - p[0];
+  const V3<R> wu = ds0 * dm[0] + ds1 * dm[2];
+  const V3<R> wv = ds0 * dm[1] + ds1 * dm[3];
+  const R cnd[3] = {wu.length() - R(1), wv.length() - R(1), wu.dot(wv)};
+  const R cu[3] = {-(dm[0] + dm[2]), dm[0], dm[2]};
+  const R cv[3] = {-(dm[1] + dm[3]), dm[1], dm[3]};
+  const V3<R> nu = wu.normalize_or_zero(), nv = wv.normalize_or_zero();
+  R mu_[3][3], mv_[3][3], sm[4][3][3];
+  bw_stretch_material(wu, mu_);
+  bw_stretch_material(wv, mv_);
+  bw_shear_material(wu, wv, sm);
+  for (int a = 0; a < 3; ++a) g[a] = V3<R>();
+  for (int i = 0; i < 9; ++i)
+    for (int j = 0; j < 9; ++j) h[i][j] = 0;
+  const R kc[3] = {kw, kf, ks};
+  for (int ci = 0; ci < 3; ++ci) {
+    const R ka = kc[ci] * area;
+    if (!(ka > 0)) continue;
+    for (int a = 0; a < 3; ++a) {
+      const V3<R> ga = ci == 0 ? nu * cu[a] : (ci == 1 ? nv * cv[a] : wv * cu[a] + wu * cv[a]);
+      g[a] += ga * (ka * cnd[ci]);
+      for (int b = 0; b < 3; ++b)
+        for (int r = 0; r < 3; ++r)
+          for (int c = 0; c < 3; ++c) {
+            R v;
+            if (ci == 0)
+              v = ka * cu[a] * cu[b] * mu_[r][c];
+            else if (ci == 1)
+              v = ka * cv[a] * cv[b] * mv_[r][c];
+            else
+              v = ka * (cu[a] * cu[b] * sm[0][r][c] + cu[a] * cv[b] * sm[1][r][c] + cv[a] * cu[b] * sm[2][r][c] +
+                        cv[a] * cv[b] * sm[3][r][c]);
+            h[3 * a + r][3 * b + c] += v;
+          }
+    }
+  }
+}
+
 }  // namespace mg

@@ -112,6 +112,10 @@ static int validate_desc(const mguso_scene_desc* d) {
   MG_CHECK_ARG(d->params.pcg_mode >= 0 && d->params.pcg_mode <= 2, "scene: pcg_mode must be 0, 1 or 2");
   MG_CHECK_ARG(d->params.factor_storage >= 0 && d->params.factor_storage <= 2, "scene: factor_storage must be 0, 1 or 2");
   MG_CHECK_ARG(d->params.schwarz_levels <= 2, "scene: schwarz_levels must be 1 or 2");
+  MG_CHECK_ARG(std::isfinite(d->params.membrane_warp) && std::isfinite(d->params.membrane_weft) &&
+                   std::isfinite(d->params.membrane_shear) && d->params.membrane_warp >= 0 &&
+                   d->params.membrane_weft >= 0 && d->params.membrane_shear >= 0,
+               "scene: membrane stiffnesses must be finite and >= 0");
   MG_CHECK_ARG(d->params.pcg_variant >= 0 && d->params.pcg_variant <= 16, "scene: pcg_variant must be in [0, 16]");
   MG_CHECK_ARG(std::isfinite(d->params.schwarz_weight) && d->params.schwarz_weight >= 0.f,
                "scene: schwarz_weight must be finite and >= 0");
@@ -239,6 +243,29 @@ int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>
     }
   }
   s.n_hinge = (uint32_t)hinge_rest.size();
+  // Baraff-Witkin membrane elements (membrane.rs:272-312) on every triangle, rest frame from
+  // the initial positions; degenerate triangles are skipped
+  std::vector<uint32_t> mem_v;
+  std::vector<float> mem_dm, mem_area;
+  if (s.p.membrane_warp > 0 || s.p.membrane_weft > 0 || s.p.membrane_shear > 0) {
+    for (auto& t : tris) {
+      HV x0 = hp(P, t[0]), x1 = hp(P, t[1]), x2 = hp(P, t[2]);
+      HV e1 = x1 - x0, e2 = x2 - x0;
+      const float a = e1.length();
+      HV n = e1.cross(e2);
+      const float area = 0.5f * n.length();
+      if (a < 1.0e-9f || area < 1.0e-12f) continue;
+      HV t1 = e1 / a;
+      HV t2 = n.cross(e1).normalize_or_zero();
+      const float b = e2.dot(t1), dd = e2.dot(t2);
+      const float det = a * dd;
+      if (std::fabs(det) < 1.0e-12f) continue;
+      mem_v.insert(mem_v.end(), {t[0], t[1], t[2]});
+      mem_dm.insert(mem_dm.end(), {1.0f / a, -b / (a * dd), 0.0f, 1.0f / dd});
+      mem_area.push_back(area);
+    }
+  }
+  s.n_mem = (uint32_t)mem_area.size();
   // shells (shell_model.rs:310-348), StVK, per-scene (mu, lambda)
   std::vector<uint32_t> shell_v;
   std::vector<float> shell_dm, shell_area, shell_mu, shell_lam;
@@ -297,6 +324,9 @@ int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>
     if (vec.empty()) return buf.reserve(1);
     return buf.upload(vec.data(), vec.size(), st);
   };
+  MG_TRY(up(s.mem_v, mem_v));
+  MG_TRY(up(s.mem_dm, mem_dm));
+  MG_TRY(up(s.mem_area, mem_area));
   MG_TRY(up(s.shell_v, shell_v));
   MG_TRY(up(s.shell_dm, shell_dm));
   MG_TRY(up(s.shell_area, shell_area));
@@ -320,6 +350,9 @@ int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>
     }
   };
   std::vector<uint32_t> act;
+  active(mem_v, 3, s.n_mem, act);
+  s.n_act_mem = (uint32_t)act.size();
+  MG_TRY(up(s.act_mem, act));
   active(shell_v, 3, s.n_shell, act);
   s.n_act_shell = (uint32_t)act.size();
   MG_TRY(up(s.act_shell, act));
@@ -360,6 +393,14 @@ int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>
     cb.push_back({b, b});
     cb.push_back({a, b});
     cb.push_back({b, a});
+  }
+  s.cb_mem = cb.size();
+  s.gb_mem = gvert.size();
+  for (uint32_t e = 0; e < s.n_mem; ++e) {
+    const uint32_t* mv = mem_v.data() + 3 * e;
+    for (int a = 0; a < 3; ++a) gvert.push_back(mv[a]);
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) cb.push_back({mv[a], mv[b]});
   }
   s.cb_shell = cb.size();
   s.gb_shell = gvert.size();

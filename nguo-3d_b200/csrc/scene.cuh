@@ -69,6 +69,11 @@ struct Scene {
   DevBuf<float> hinge_rest;
   DevBuf<uint32_t> spring_v;     // 2 per spring
   DevBuf<float> spring_rest;
+  DevBuf<uint32_t> mem_v;        // 3 per Baraff-Witkin membrane element
+  DevBuf<float> mem_dm, mem_area; // 4 per element (Dm^-1 row-major), area
+  uint32_t n_mem = 0, n_act_mem = 0;
+  DevBuf<uint32_t> act_mem;
+  uint64_t cb_mem = 0, gb_mem = 0;
   DevBuf<uint32_t> stitch_idx;   // 6 per stitch
   DevBuf<float> stitch_w, stitch_kl;
   // elements with at least one free vertex (recomputed every Newton iteration); the

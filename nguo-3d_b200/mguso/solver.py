@@ -24,7 +24,8 @@ _PARAM_FIELDS = [("dt", C.c_float), ("gravity", C.c_float * 3), ("newton_iters",
                  ("cg_max_iter", C.c_uint32), ("floor_y", C.c_float), ("newton_tol", C.c_float),
                  ("precond", C.c_int), ("schwarz_domain", C.c_uint32), ("precision", C.c_int),
                  ("pcg_mode", C.c_int), ("factor_storage", C.c_int), ("schwarz_levels", C.c_uint32),
-                 ("pcg_variant", C.c_int), ("constraint_tol", C.c_float), ("schwarz_weight", C.c_float)]
+                 ("pcg_variant", C.c_int), ("membrane_warp", C.c_float), ("membrane_weft", C.c_float),
+                 ("membrane_shear", C.c_float), ("constraint_tol", C.c_float), ("schwarz_weight", C.c_float)]
 
 
 class Params(C.Structure):
