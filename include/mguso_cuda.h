@@ -260,6 +260,15 @@ typedef struct {
                               reference's default ImplicitParams::constraint_tol) */
   float schwarz_weight;    /* coarse-correction weight w of the two-level form
                               z = S0 r + w C1^T S1 (C1 r) (the CLI default 0.7, main.rs:761-763) */
+  float strain_limit_ratio; /* one-sided edge strain limit (ImplicitParams::strain_limit_ratio,
+                               _k, _ratio_weft, implicit.rs:160-170; strain_limit.rs:24-63): on
+                               every stretch edge a spring of rest length ratio * rest and
+                               stiffness strain_limit_k, active only while the edge is longer;
+                               0 = off */
+  float strain_limit_k;
+  float strain_limit_ratio_weft; /* > 0 with per-vertex uvs: edges more V- than U-aligned in UV
+                                    space use this ratio instead (edge_strain_ratio,
+                                    implicit.rs:798-817) */
 } mguso_params;
 
 /* One scene (Scene::build_implicit + the set_* calls of implicit.rs). All pointers host;
@@ -289,6 +298,14 @@ typedef struct {
    * parameters of the adjoint. */
   const float* shell_rest;
   const float* shell_stiff;
+  /* Optional per-vertex pattern coordinates (SimState::uvs), f32[2*nv] or NULL: they choose
+   * each edge's strain-limit ratio (strain_limit_ratio_weft). */
+  const float* uvs;
+  /* Optional stretch edges (SimState::edges), u32[2*nstretch]: when nstretch > 0 the stretch
+   * springs and the edge strain limit act on these edges, rest lengths from the initial
+   * positions, instead of on the unique edges of tris. Collision edges stay those of tris. */
+  uint32_t nstretch;
+  const uint32_t* stretch_edges;
 } mguso_scene_desc;
 
 typedef struct {
@@ -396,6 +413,20 @@ int mguso_set_pins(mguso_scene* s, uint32_t n, const uint32_t* index, const floa
  * a weight <= 0 returns MGUSO_ERR_INVALID_ARG and keeps the previous pulls; n = 0 clears
  * them. All pointers host. */
 int mguso_set_pulls(mguso_scene* s, uint32_t n, const uint32_t* index, const float* target, const float* weight);
+/* set_strain_limit_faces (implicit.rs:1088-1121): the per-face strain-limit barrier
+ * (shell_model.rs:438-640) on n faces (u32[3 n]), each with its allowed principal-stretch
+ * excess limits[i] (0.05 = 5 %) and its mass masses[i]; the rest shape comes from the
+ * current positions. Faces with a limit or mass <= 0, and degenerate faces, are skipped;
+ * *kept (may be NULL) gets the number kept. Each kept face adds the barrier on
+ * max(sigma - 1) at the dynamic stiffness max(w.(H w), 0) + mass / d^2 (w the face's
+ * positions about their centroid, H the elastic blocks gathered so far, d the headroom),
+ * and limits the step fraction by bisection (implicit.rs:1709-1753). All or nothing:
+ * MGUSO_ERR_INVALID_ARG for an index out of range, a face across two instances of a batch
+ * or a non-finite limit or mass; MGUSO_ERR_UNSUPPORTED when a face has two vertices, one of
+ * them free, that share no element (the barrier's block would lie outside the scene's
+ * fixed Hessian pattern). n = 0 clears them. All pointers host. */
+int mguso_set_strain_limit_faces(mguso_scene* s, uint32_t n, const uint32_t* faces, const float* limits,
+                                 const float* masses, uint32_t* kept);
 /* Element counts: hinges, shells, unique edges, static collider triangles,
  * system blocks (free-free pattern), pinned-pattern blocks. */
 int mguso_scene_info(mguso_scene* s, uint32_t* out6);

@@ -104,9 +104,14 @@ __global__ void k_stitch(const uint32_t* __restrict__ act, uint32_t n, const uin
 }
 
 // ---- stretch springs (spring_block, implicit.rs:3240-3263) --------------------------------
+// With the edge strain limit on (slk > 0), each spring's blocks and gradient also carry the
+// one-sided limit spring on the same edge (strain_block, strain_limit.rs:31-63; pushed after
+// the stretch spring, implicit.rs:2508-2530): rest length slr[e] * rest, stiffness slk,
+// zero while the edge is no longer than that. Its Hessian is the clamped spring block, which
+// is already exact while it acts.
 __global__ void k_spring(const uint32_t* __restrict__ act, uint32_t n, const uint32_t* __restrict__ sv,
                          const float* __restrict__ rest, float k, const float* __restrict__ x, float* __restrict__ cb,
-                         float* __restrict__ ge, int exact) {
+                         float* __restrict__ ge, int exact, const float* __restrict__ slr, float slk) {
   uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
   uint32_t e = act[q];
@@ -126,6 +131,23 @@ __global__ void k_spring(const uint32_t* __restrict__ act, uint32_t n, const uin
         h[3 * i + j] = k * (nnt + ct * ((i == j ? 1.f : 0.f) - nnt));
       }
     ga = nrm * (k * (l - rest[e]));
+  }
+  if (slk > 0.f && slr[e] > 0.f) {
+    const float r = rest[e] * slr[e];
+    if (l > r) {  // spring_block at rest length r (l >= 1e-9 here unless r < 0)
+      if (l < 1e-9f) {
+        for (int i = 0; i < 9; ++i) h[i] += (i % 4 == 0) ? slk : 0.f;
+      } else {
+        V3<float> nrm = d / l;
+        const float ct = fmaxf(1.0f - r / l, 0.f);
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) {
+            float nnt = nrm[i] * nrm[j];
+            h[3 * i + j] += slk * (nnt + ct * ((i == j ? 1.f : 0.f) - nnt));
+          }
+        ga += nrm * (slk * (l - r));
+      }
+    }
   }
   float* blk = cb + 36 * (size_t)e;
   for (int i = 0; i < 9; ++i) {
@@ -324,7 +346,8 @@ int assemble_elastic(Scene& s) {
                                                  s.x.p, cb + 9 * s.cb_stitch, ge + 3 * s.gb_stitch, ex_stitch);
     if (s.n_spring)
       k_spring<<<grid(s.n_spring), 128, 0, st>>>(all.p, s.n_spring, s.spring_v.p, s.spring_rest.p, s.p.stiffness,
-                                                 s.x.p, cb + 9 * s.cb_spring, ge + 3 * s.gb_spring, ex_spring);
+                                                 s.x.p, cb + 9 * s.cb_spring, ge + 3 * s.gb_spring, ex_spring,
+                                                 s.spring_slr.p, s.edge_limit ? s.p.strain_limit_k : 0.f);
     if (s.n_mem)
       k_membrane<<<grid(s.n_mem), 128, 0, st>>>(all.p, s.n_mem, s.mem_v.p, s.mem_dm.p, s.mem_area.p,
                                                 s.p.membrane_warp, s.p.membrane_weft, s.p.membrane_shear, s.x.p,
@@ -345,7 +368,8 @@ int assemble_elastic(Scene& s) {
                                                      s.stitch_kl.p, s.x.p, cb + 9 * s.cb_stitch, ge + 3 * s.gb_stitch, ex_stitch);
     if (s.n_act_spring)
       k_spring<<<grid(s.n_act_spring), 128, 0, st>>>(s.act_spring.p, s.n_act_spring, s.spring_v.p, s.spring_rest.p,
-                                                     s.p.stiffness, s.x.p, cb + 9 * s.cb_spring, ge + 3 * s.gb_spring, ex_spring);
+                                                     s.p.stiffness, s.x.p, cb + 9 * s.cb_spring, ge + 3 * s.gb_spring, ex_spring,
+                                                     s.spring_slr.p, s.edge_limit ? s.p.strain_limit_k : 0.f);
     if (s.n_act_mem)
       k_membrane<<<grid(s.n_act_mem), 128, 0, st>>>(s.act_mem.p, s.n_act_mem, s.mem_v.p, s.mem_dm.p, s.mem_area.p,
                                                     s.p.membrane_warp, s.p.membrane_weft, s.p.membrane_shear, s.x.p,
@@ -513,7 +537,118 @@ static int assemble_pins(Scene& s) {
   return MGUSO_OK;
 }
 
+// ---- strain-limit barrier faces (implicit.rs:2743-2807) -----------------------------------
+// One thread per face: its elastic stiffness w.(H w) from the blocks gathered so far (every
+// elastic term and the inertia; w the face's positions about their centroid), then the
+// barrier's gradient and 9x9 Hessian at the dynamic stiffness (sl_face_grad_hess) into the
+// face's contribution (zeros when inactive). Every face reads the blocks before any face
+// adds to them, as the reference does.
+template <class R>
+__global__ void __launch_bounds__(128) k_sl_faces(uint32_t n, const uint32_t* __restrict__ fv,
+                                                  const float* __restrict__ fdm, const float* __restrict__ flim,
+                                                  const float* __restrict__ fmass, const uint32_t* __restrict__ fslot,
+                                                  const float* __restrict__ x, const float* __restrict__ vals,
+                                                  const float* __restrict__ valp, uint32_t nnz_s, int kind, float eps,
+                                                  float* __restrict__ out) {
+  const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= n) return;
+  V3<R> p[3];
+  for (int a = 0; a < 3; ++a) p[a] = ld3<R>(x, fv[3 * f + a]);
+  // centroid and offsets in FP32 (the reference's Vec3 arithmetic), then widened
+  const V3<float> pf[3] = {ld3<float>(x, fv[3 * f]), ld3<float>(x, fv[3 * f + 1]), ld3<float>(x, fv[3 * f + 2])};
+  const V3<float> cen = (pf[0] + pf[1] + pf[2]) / 3.0f;
+  V3<R> w[3];
+  for (int a = 0; a < 3; ++a) {
+    const V3<float> d = pf[a] - cen;
+    w[a] = V3<R>((R)d.x, (R)d.y, (R)d.z);
+  }
+  R ek = 0;
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      const uint32_t sl = fslot[9 * f + 3 * a + b];
+      if (sl == ~0u) continue;
+      const float* blk = sl < nnz_s ? vals + 9 * (size_t)sl : valp + 9 * (size_t)(sl - nnz_s);
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) ek += w[a][r] * (R)blk[3 * r + c] * w[b][c];
+    }
+  const M2<R> dm{(R)fdm[4 * f], (R)fdm[4 * f + 1], (R)fdm[4 * f + 2], (R)fdm[4 * f + 3]};
+  V3<R> g[3];
+  R h[81];
+  float* o = out + 90 * (size_t)f;
+  if (!sl_face_grad_hess<R>(p, dm, (R)flim[f], (R)fmass[f], ek, kind, (R)eps, g, h)) {
+    for (int q = 0; q < 90; ++q) o[q] = 0.f;
+    return;
+  }
+  for (int q = 0; q < 81; ++q) o[q] = (float)h[q];
+  for (int a = 0; a < 3; ++a) {
+    o[81 + 3 * a] = (float)g[a].x;
+    o[82 + 3 * a] = (float)g[a].y;
+    o[83 + 3 * a] = (float)g[a].z;
+  }
+}
+
+// One thread per touched slot: the faces' blocks added to it in face order.
+__global__ void k_sl_gather_blocks(uint32_t ns, const uint32_t* __restrict__ slots, const uint32_t* __restrict__ sptr,
+                                   const uint32_t* __restrict__ slist, const float* __restrict__ c, uint32_t nnz_s,
+                                   float* __restrict__ vals, float* __restrict__ valp) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ns) return;
+  const uint32_t sl = slots[t];
+  float* blk = sl < nnz_s ? vals + 9 * (size_t)sl : valp + 9 * (size_t)(sl - nnz_s);
+  float acc[9];
+  for (int q = 0; q < 9; ++q) acc[q] = blk[q];
+  for (uint32_t j = sptr[t]; j < sptr[t + 1]; ++j) {
+    const uint32_t e = slist[j], f = e / 9, a = (e % 9) / 3, b = e % 3;
+    const float* h = c + 90 * (size_t)f;
+    for (int r = 0; r < 3; ++r)
+      for (int cc = 0; cc < 3; ++cc) acc[3 * r + cc] += h[(3 * a + r) * 9 + 3 * b + cc];
+  }
+  for (int q = 0; q < 9; ++q) blk[q] = acc[q];
+}
+
+// One thread per touched vertex: the faces' gradient entries added in face order.
+__global__ void k_sl_gather_grad(uint32_t nvt, const uint32_t* __restrict__ verts, const uint32_t* __restrict__ vptr,
+                                 const uint32_t* __restrict__ vlist, const float* __restrict__ c,
+                                 float* __restrict__ grad) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nvt) return;
+  const uint32_t v = verts[t];
+  float g0 = grad[3 * v], g1 = grad[3 * v + 1], g2 = grad[3 * v + 2];
+  for (uint32_t j = vptr[t]; j < vptr[t + 1]; ++j) {
+    const uint32_t e = vlist[j], f = e / 3, a = e % 3;
+    const float* g = c + 90 * (size_t)f + 81 + 3 * a;
+    g0 += g[0];
+    g1 += g[1];
+    g2 += g[2];
+  }
+  grad[3 * v] = g0;
+  grad[3 * v + 1] = g1;
+  grad[3 * v + 2] = g2;
+}
+
+static int assemble_strain_limit(Scene& s) {
+  if (!s.n_sl) return MGUSO_OK;
+  const unsigned g = ceil_div(s.n_sl, 128);
+  if (s.mixed)
+    k_sl_faces<double><<<g, 128, 0, s.st>>>(s.n_sl, s.sl_v.p, s.sl_dm.p, s.sl_limit.p, s.sl_mass.p, s.sl_slot.p,
+                                            s.x.p, s.A->val.p, s.valp.p, s.Ps.nnz, s.p.barrier_kind,
+                                            s.p.eiganalysis_eps, s.sl_c.p);
+  else
+    k_sl_faces<float><<<g, 128, 0, s.st>>>(s.n_sl, s.sl_v.p, s.sl_dm.p, s.sl_limit.p, s.sl_mass.p, s.sl_slot.p,
+                                           s.x.p, s.A->val.p, s.valp.p, s.Ps.nnz, s.p.barrier_kind,
+                                           s.p.eiganalysis_eps, s.sl_c.p);
+  if (s.n_sl_slots)
+    k_sl_gather_blocks<<<ceil_div(s.n_sl_slots, 128), 128, 0, s.st>>>(s.n_sl_slots, s.sl_slots.p, s.sl_sptr.p,
+                                                                      s.sl_slist.p, s.sl_c.p, s.Ps.nnz, s.A->val.p,
+                                                                      s.valp.p);
+  k_sl_gather_grad<<<ceil_div(s.n_sl_verts, 128), 128, 0, s.st>>>(s.n_sl_verts, s.sl_verts.p, s.sl_vptr.p,
+                                                                  s.sl_vlist.p, s.sl_c.p, s.grad.p);
+  MG_CUDA(cudaGetLastError());
+  return MGUSO_OK;
+}
+
 int assemble_colliders(Scene& s) {
+  MG_TRY(assemble_strain_limit(s));
   MG_TRY(assemble_pins(s));
   if (!s.n_col || !s.n_free) return MGUSO_OK;
   unsigned g = ceil_div(s.n_free, 128);

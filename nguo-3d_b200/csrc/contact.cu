@@ -442,6 +442,41 @@ __global__ void k_ccd_pins(const uint32_t* __restrict__ pin_vert, uint32_t n_pin
   }
 }
 
+// Strain-limit line search (implicit.rs:1709-1753): per face, bisect the step fraction on
+// max(sigma(x + t dx) - 1) < limit over [0, 1.25] until the bisection window stops
+// shrinking (at most 64 halvings); a face already inside its limit at 1.25 does not limit.
+__global__ void k_ccd_sl(uint32_t n, const uint32_t* __restrict__ fv, const float* __restrict__ fdm,
+                         const float* __restrict__ flim, const uint8_t* __restrict__ vinst,
+                         const float* __restrict__ x, const float* __restrict__ dx, unsigned int* __restrict__ red) {
+  const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= n) return;
+  const float LS_MAX_T = 1.25f;
+  const M2<float> dm{fdm[4 * f], fdm[4 * f + 1], fdm[4 * f + 2], fdm[4 * f + 3]};
+  const float limit = flim[f];
+  V3<float> x0[3], d0[3];
+  for (int a = 0; a < 3; ++a) {
+    x0[a] = ld3<float>(x, fv[3 * f + a]);
+    d0[a] = ld3<float>(dx, fv[3 * f + a]);
+  }
+  auto at = [&](float frac) {
+    V3<float> p[3] = {x0[0] + d0[0] * frac, x0[1] + d0[1] * frac, x0[2] + d0[2] * frac};
+    return max_stretch_excess<float>(p, dm);
+  };
+  if (at(LS_MAX_T) < limit) return;
+  float lo = 0.f, hi = LS_MAX_T, window = hi - lo;
+  for (int it = 0; it < 64; ++it) {
+    const float mid = 0.5f * (lo + hi);
+    if (at(mid) - limit < 0.f)
+      lo = mid;
+    else
+      hi = mid;
+    const float w = hi - lo;
+    if (w == window) break;
+    window = w;
+  }
+  if (lo < 1.f) atomic_min_pos(red + RED_STRIDE * vinst[fv[3 * f]] + 1, lo);
+}
+
 // CCD candidate pruning: a pair whose accd_toi (contact.rs:378-437) would return max_t at
 // its first test cannot lower the step fraction, and traversal skips whole subtrees of such
 // pairs (lbvh_visit_ccd) from the primitives' displacement boxes, refitted per CCD call.
@@ -642,7 +677,7 @@ int ccd_step(Scene& s, uint32_t active, float* t_out, uint32_t* cap_hits) {
     t_out[k] = 1.f;
     cap_hits[k] = 0;
   }
-  if (s.n_col == 0 && !s.p.self_collision && s.n_static_pin == 0) return MGUSO_OK;
+  if (s.n_col == 0 && !s.p.self_collision && s.n_static_pin == 0 && s.n_sl == 0) return MGUSO_OK;
   std::vector<unsigned int> init(RED_STRIDE * K, 0u);
   for (uint32_t k = 0; k < K; ++k) {
     init[RED_STRIDE * k + 1] = f2u_host(1.f);
@@ -657,6 +692,9 @@ int ccd_step(Scene& s, uint32_t active, float* t_out, uint32_t* cap_hits) {
   if (s.n_static_pin)
     k_ccd_pins<<<ceil_div(s.n_pin, 128), 128, 0, st>>>(s.pin_vert.p, s.n_pin, s.pin_kin.p, s.pin_target.p,
                                                       s.pin_ghat.p, s.inv_mass.p, s.vinst.p, s.x.p, s.dx.p, s.red.p);
+  if (s.n_sl)
+    k_ccd_sl<<<ceil_div(s.n_sl, 128), 128, 0, st>>>(s.n_sl, s.sl_v.p, s.sl_dm.p, s.sl_limit.p, s.vinst.p, s.x.p,
+                                                   s.dx.p, s.red.p);
   MG_CUDA(cudaGetLastError());
   std::vector<unsigned int> h(RED_STRIDE * K);
   MG_CUDA(cudaMemcpyAsync(h.data(), s.red.p, 4 * h.size(), cudaMemcpyDeviceToHost, st));

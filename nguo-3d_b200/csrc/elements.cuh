@@ -452,32 +452,15 @@ __device__ inline void shell_grad(const V3<R> p[3], const M2<R>& dm, R area, R m
   grad[2] = g2;
 }
 
-// StVK shell element: gradient (shell_model.rs:366-380) and eigen-projected Hessian
-// (shell_model.rs:178-290 + :403-438). dm = inverse rest shape (column-major 2x2).
-// project = false keeps the negative eigenvalues: the exact Hessian (the six eigenpairs
-// span the 3x2 deformation gradients).
+// scale * dF/dx^T d2Psi/dF2 dF/dx over a triangle from the principal-stretch derivatives
+// (shell_d2psi_df2_from_derivs, shell_model.rs:242-290 with the eigenpairs of :188-240;
+// dF/dx of :384-400). deda = dPsi/dsigma, d2 = d2Psi/dsigma2 (2x2, row-major). project = false
+// keeps the negative eigenvalues: the exact Hessian (the six eigenpairs span the 3x2
+// deformation gradients).
 template <class R>
-__device__ inline void shell_grad_hess(const V3<R> p[3], const M2<R>& dm, R area, R mu, R lambda, R eps, V3<R> grad[3],
-                                       R* h /*81*/, bool project = true) {
-  M32<R> f = M32<R>{p[1] - p[0], p[2] - p[0]}.mul(dm);
-  M32<R> u;
-  R s[2];
-  M2<R> v;
-  svd3x2(f, u, s, v);
-  R j = s[0] * s[1];
-  R s0m = s[0] - R(1), s1m = s[1] - R(1);
-  R deda[2] = {mu * (s0m * (s0m * s0m)) + lambda * s[1] * (j - R(1)),
-               mu * (s1m * (s1m * s1m)) + lambda * s[0] * (j - R(1))};
-  // gradient
-  M32<R> pk1 = M32<R>{u.c0 * deda[0], u.c1 * deda[1]}.mul(v.transpose());
-  M32<R> hh = pk1.mul(dm.transpose());
-  V3<R> g1 = hh.c0 * area, g2 = hh.c1 * area;
-  grad[0] = -(g1 + g2);
-  grad[1] = g1;
-  grad[2] = g2;
-  // eigen-projected d2Psi/dF2
-  R cross = lambda * (R(2) * s[0] * s[1] - R(1));
-  R d2[4] = {R(3) * mu * s0m * s0m + lambda * s[1] * s[1], cross, cross, R(3) * mu * s1m * s1m + lambda * s[0] * s[0]};
+__device__ inline void shell_hess_from_derivs(const M32<R>& u, const R s[2], const M2<R>& v, const R deda[2],
+                                              const R d2[4], R eps, const M2<R>& dm, R scale, R* h /*81*/,
+                                              bool project) {
   R ev[2];
   M2<R> evec;
   sym_eig2(d2[0], d2[1], d2[3], ev, evec);
@@ -529,8 +512,102 @@ __device__ inline void shell_grad_hess(const V3<R> p[3], const M2<R>& dm, R area
     for (int c = 0; c < 9; ++c) {
       R acc = 0;
       for (int k = 0; k < 6; ++k) acc += bm[k * 9 + r] * ab[k * 9 + c];
-      h[r * 9 + c] = area * acc;
+      h[r * 9 + c] = scale * acc;
     }
+}
+
+// StVK shell element: gradient (shell_model.rs:366-380) and eigen-projected Hessian
+// (shell_model.rs:178-290 + :403-438). dm = inverse rest shape (column-major 2x2).
+// project = false keeps the negative eigenvalues: the exact Hessian.
+template <class R>
+__device__ inline void shell_grad_hess(const V3<R> p[3], const M2<R>& dm, R area, R mu, R lambda, R eps, V3<R> grad[3],
+                                       R* h /*81*/, bool project = true) {
+  M32<R> f = M32<R>{p[1] - p[0], p[2] - p[0]}.mul(dm);
+  M32<R> u;
+  R s[2];
+  M2<R> v;
+  svd3x2(f, u, s, v);
+  R j = s[0] * s[1];
+  R s0m = s[0] - R(1), s1m = s[1] - R(1);
+  R deda[2] = {mu * (s0m * (s0m * s0m)) + lambda * s[1] * (j - R(1)),
+               mu * (s1m * (s1m * s1m)) + lambda * s[0] * (j - R(1))};
+  // gradient
+  M32<R> pk1 = M32<R>{u.c0 * deda[0], u.c1 * deda[1]}.mul(v.transpose());
+  M32<R> hh = pk1.mul(dm.transpose());
+  V3<R> g1 = hh.c0 * area, g2 = hh.c1 * area;
+  grad[0] = -(g1 + g2);
+  grad[1] = g1;
+  grad[2] = g2;
+  // eigen-projected d2Psi/dF2
+  R cross = lambda * (R(2) * s[0] * s[1] - R(1));
+  R d2[4] = {R(3) * mu * s0m * s0m + lambda * s[1] * s[1], cross, cross, R(3) * mu * s1m * s1m + lambda * s[0] * s[0]};
+  shell_hess_from_derivs(u, s, v, deda, d2, eps, dm, area, h, project);
+}
+
+// ---- face strain limit (shell_model.rs:438-640) -------------------------------------------
+// The barrier argument never drops below this fraction of the limit (SL_GAP_FLOOR,
+// shell_model.rs:444).
+#define MG_SL_GAP_FLOOR 1.0e-3
+
+// strain_limit_derivs (shell_model.rs:456-484): energy derivatives over the two principal
+// stretch excesses a = sigma - 1 (deda, diagonal d2); false when neither exceeds rest.
+template <class R>
+__device__ inline bool sl_derivs(const R s[2], R limit, int kind, R deda[2], R d2[4]) {
+  if (!(limit > 0)) return false;
+  deda[0] = deda[1] = R(0);
+  d2[0] = d2[1] = d2[2] = d2[3] = R(0);
+  bool active = false;
+  for (int i = 0; i < 2; ++i) {
+    const R a = s[i] - R(1);
+    if (a <= 0) continue;
+    const R y = rmax(limit - a, R(MG_SL_GAP_FLOOR) * limit);
+    R g, h;
+    if (barrier_of<R>(kind, y, limit, R(1), g, h)) {
+      deda[i] = -g;
+      d2[3 * i] = h;
+      active = true;
+    }
+  }
+  return active;
+}
+
+// The largest principal-stretch excess max(sigma - 1) of a face (what the strain-limit line
+// search bisects on, implicit.rs:1719-1729).
+template <class R>
+__device__ inline R max_stretch_excess(const V3<R> p[3], const M2<R>& dm) {
+  M32<R> f = M32<R>{p[1] - p[0], p[2] - p[0]}.mul(dm);
+  R lam[2];
+  M2<R> v;
+  sym_eig2(f.c0.dot(f.c0), f.c0.dot(f.c1), f.c1.dot(f.c1), lam, v);
+  const R s0 = sqrt(rmax(lam[0], R(0))), s1 = sqrt(rmax(lam[1], R(0)));
+  return rmax(s0 - R(1), s1 - R(1));
+}
+
+// strain_limit_assembly (shell_model.rs:582-640): the face barrier's gradient and 9x9
+// Hessian at the dynamic stiffness max(elastic_k, 0) + face_mass / d^2, d the headroom
+// limit - max(sigma - 1) floored at the gap floor. False when inactive.
+template <class R>
+__device__ inline bool sl_face_grad_hess(const V3<R> p[3], const M2<R>& dm, R limit, R face_mass, R elastic_k,
+                                         int kind, R eps, V3<R> grad[3], R* h /*81*/) {
+  M32<R> f = M32<R>{p[1] - p[0], p[2] - p[0]}.mul(dm);
+  M32<R> u;
+  R s[2];
+  M2<R> v;
+  svd3x2(f, u, s, v);
+  R deda[2], d2[4];
+  if (!sl_derivs(s, limit, kind, deda, d2)) return false;
+  const R max_a = rmax(s[0] - R(1), s[1] - R(1));
+  const R d = rmax(limit - max_a, R(MG_SL_GAP_FLOOR) * limit);
+  const R stiffness = rmax(elastic_k, R(0)) + face_mass / (d * d);
+  if (!(stiffness > 0)) return false;
+  M32<R> pk1 = M32<R>{u.c0 * deda[0], u.c1 * deda[1]}.mul(v.transpose());
+  M32<R> hg = pk1.mul(dm.transpose());
+  const V3<R> g1 = hg.c0 * stiffness, g2 = hg.c1 * stiffness;
+  grad[0] = -(g1 + g2);
+  grad[1] = g1;
+  grad[2] = g2;
+  shell_hess_from_derivs(u, s, v, deda, d2, eps, dm, stiffness, h, true);
+  return true;
 }
 
 // ---------------------------------------------------------------------------------------

@@ -80,6 +80,26 @@ float host_dihedral(const HV p[4]) {
   return std::atan2(s, c);
 }
 
+// build_shells (shell_model.rs:310-348) for one triangle: the inverse rest shape dm
+// (column-major 2x2) in the triangle's own in-plane frame and the rest area; false for a
+// degenerate triangle.
+bool shell_rest_shape(const HV& p0, const HV& p1, const HV& p2, float dm[4], float& area) {
+  HV e1 = p1 - p0, e2 = p2 - p0;
+  area = 0.5f * e1.cross(e2).length();
+  if (area <= 1e-12f) return false;
+  HV ax = e1.normalize();
+  HV ay = (e2 - ax * e2.dot(ax)).normalize();
+  float xx = e1.dot(ax), xy = e1.dot(ay), yx = e2.dot(ax), yy = e2.dot(ay);
+  float det = xx * yy - yx * xy;
+  if (std::fabs(det) < 1e-20f) return false;
+  float inv = 1.f / det;
+  dm[0] = yy * inv;
+  dm[1] = xy * -inv;
+  dm[2] = yx * -inv;
+  dm[3] = xx * inv;
+  return true;
+}
+
 struct Contribution {
   uint32_t row, col;
 };
@@ -119,6 +139,13 @@ static int validate_desc(const mguso_scene_desc* d) {
   MG_CHECK_ARG(d->params.pcg_variant >= 0 && d->params.pcg_variant <= 16, "scene: pcg_variant must be in [0, 16]");
   MG_CHECK_ARG(std::isfinite(d->params.schwarz_weight) && d->params.schwarz_weight >= 0.f,
                "scene: schwarz_weight must be finite and >= 0");
+  MG_CHECK_ARG(std::isfinite(d->params.strain_limit_ratio) && std::isfinite(d->params.strain_limit_k) &&
+                   std::isfinite(d->params.strain_limit_ratio_weft) && d->params.strain_limit_ratio >= 0 &&
+                   d->params.strain_limit_k >= 0 && d->params.strain_limit_ratio_weft >= 0,
+               "scene: strain limit ratios and stiffness must be finite and >= 0");
+  MG_CHECK_ARG(d->nstretch == 0 || d->stretch_edges, "scene: null arrays");
+  for (uint32_t e = 0; e < 2 * d->nstretch; ++e)
+    MG_CHECK_ARG(d->stretch_edges[e] < nv, "scene: stretch edge index out of range");
   return MGUSO_OK;
 }
 
@@ -282,33 +309,45 @@ int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>
         shell_lam.push_back(s.p.shell_lambda * k);
         continue;
       }
-      HV p0 = hp(P, fv[0]), p1 = hp(P, fv[1]), p2 = hp(P, fv[2]);
-      HV e1 = p1 - p0, e2 = p2 - p0;
-      float area = 0.5f * e1.cross(e2).length();
-      if (area <= 1e-12f) continue;
-      HV ax = e1.normalize();
-      HV ay = (e2 - ax * e2.dot(ax)).normalize();
-      float xx = e1.dot(ax), xy = e1.dot(ay), yx = e2.dot(ax), yy = e2.dot(ay);
-      float det = xx * yy - yx * xy;
-      if (std::fabs(det) < 1e-20f) continue;
-      float inv = 1.f / det;
+      float dm[4], area;
+      if (!shell_rest_shape(hp(P, fv[0]), hp(P, fv[1]), hp(P, fv[2]), dm, area)) continue;
       shell_v.insert(shell_v.end(), {fv[0], fv[1], fv[2]});
-      shell_dm.insert(shell_dm.end(), {yy * inv, xy * -inv, yx * -inv, xx * inv});
+      shell_dm.insert(shell_dm.end(), {dm[0], dm[1], dm[2], dm[3]});
       shell_area.push_back(area);
       shell_mu.push_back(s.p.shell_mu * k);
       shell_lam.push_back(s.p.shell_lambda * k);
     }
   }
   s.n_shell = (uint32_t)shell_area.size();
-  // stretch springs on the unique edges (state.rs:37-61), rest = initial length. At zero
-  // stiffness every spring block and gradient entry is exactly 0, so they are left out.
-  std::vector<uint32_t> spring_v;
-  std::vector<float> spring_rest;
-  for (auto& e : s.p.stiffness != 0.f ? edges : std::vector<std::array<uint32_t, 2>>()) {
-    spring_v.insert(spring_v.end(), {e[0], e[1]});
-    spring_rest.push_back((hp(P, e[0]) - hp(P, e[1])).length());
+  // stretch springs on the unique edges (state.rs:37-61), or on the description's stretch
+  // edges, rest = initial length. At zero stiffness, with the edge strain limit off, every
+  // spring block and gradient entry is exactly 0, so they are left out. Each spring carries
+  // its strain-limit ratio (edge_strain_ratio, implicit.rs:798-817): warp, or with a weft
+  // ratio and uvs, weft for an edge less U- than V-aligned in UV space.
+  std::vector<std::array<uint32_t, 2>> stretch = edges;
+  if (d->nstretch) {
+    stretch.resize(d->nstretch);
+    for (uint32_t e = 0; e < d->nstretch; ++e) stretch[e] = {d->stretch_edges[2 * e], d->stretch_edges[2 * e + 1]};
+    for (auto& e : stretch)
+      MG_CHECK_ARG(vinst[e[0]] == vinst[e[1]], "scene: a stretch edge spans two instances");
   }
+  const bool edge_limit = s.p.strain_limit_ratio > 0.f && s.p.strain_limit_k > 0.f;
+  std::vector<uint32_t> spring_v;
+  std::vector<float> spring_rest, spring_slr;
+  if (s.p.stiffness != 0.f || edge_limit)
+    for (auto& e : stretch) {
+      spring_v.insert(spring_v.end(), {e[0], e[1]});
+      spring_rest.push_back((hp(P, e[0]) - hp(P, e[1])).length());
+      float ratio = s.p.strain_limit_ratio;
+      if (s.p.strain_limit_ratio_weft > 0.f && d->uvs) {
+        const float du = std::fabs(d->uvs[2 * e[0]] - d->uvs[2 * e[1]]);
+        const float dv = std::fabs(d->uvs[2 * e[0] + 1] - d->uvs[2 * e[1] + 1]);
+        if (!(du >= dv)) ratio = s.p.strain_limit_ratio_weft;
+      }
+      spring_slr.push_back(ratio);
+    }
   s.n_spring = (uint32_t)spring_rest.size();
+  s.edge_limit = edge_limit;
   // stitches with stiffness > 0 (implicit.rs:2456-2485 skips the rest)
   std::vector<uint32_t> stitch_idx;
   std::vector<float> stitch_w, stitch_kl;
@@ -336,6 +375,7 @@ int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>
   MG_TRY(up(s.hinge_rest, hinge_rest));
   MG_TRY(up(s.spring_v, spring_v));
   MG_TRY(up(s.spring_rest, spring_rest));
+  MG_TRY(up(s.spring_slr, spring_slr));
   MG_TRY(up(s.stitch_idx, stitch_idx));
   MG_TRY(up(s.stitch_w, stitch_w));
   MG_TRY(up(s.stitch_kl, stitch_kl));
@@ -680,6 +720,18 @@ int upload_pins(Scene& s) {
   return MGUSO_OK;
 }
 
+// The gather slot of block (r, c): Ps when both vertices are free, else Pp (numbered after
+// Ps); -1 when the pattern has no such block.
+int slot_of_pair(const Scene& s, uint32_t r, uint32_t c) {
+  const bool sys = !s.h_pinned[r] && !s.h_pinned[c];
+  const BlockPattern& pat = sys ? s.Ps : s.Pp;
+  auto b = pat.h_col.begin() + pat.h_row_ptr[r], e = pat.h_col.begin() + pat.h_row_ptr[r + 1];
+  auto it = std::lower_bound(b, e, c);
+  if (it == e || *it != c) return -1;
+  const uint32_t local = (uint32_t)(it - pat.h_col.begin());
+  return (int)(sys ? local : s.Ps.nnz + local);
+}
+
 }  // namespace mg
 
 using namespace mg;
@@ -729,9 +781,16 @@ int mguso_batch_create(mguso_ctx* ctx, const mguso_scene_desc* descs, uint32_t n
     MG_CHECK_ARG(!d.shell_rest && !d.shell_stiff, "batch: per-shell overrides are not supported");
   }
   MG_CHECK_ARG(nv < (1u << 30), "batch: too many vertices");
-  std::vector<float> pos, vel, im, skl, sw;
-  std::vector<uint32_t> tri, shf, sidx, inst{0};
+  std::vector<float> pos, vel, im, skl, sw, uvs;
+  std::vector<uint32_t> tri, shf, sidx, sedge, inst{0};
   std::vector<uint8_t> mask;
+  bool any_uv = false, any_stretch = false;
+  for (uint32_t k = 0; k < n; ++k) {
+    any_uv = any_uv || descs[k].uvs;
+    any_stretch = any_stretch || descs[k].nstretch;
+  }
+  MG_CHECK_ARG(!any_stretch || std::all_of(descs, descs + n, [](const mguso_scene_desc& d) { return d.nstretch > 0; }),
+               "batch: give stretch edges for every instance or for none");
   pos.reserve(3 * nv);
   for (uint32_t k = 0; k < n; ++k) {
     const mguso_scene_desc& d = descs[k];
@@ -764,6 +823,18 @@ int mguso_batch_create(mguso_ctx* ctx, const mguso_scene_desc* descs, uint32_t n
       sw.insert(sw.end(), d.stitch_w, d.stitch_w + 6 * (size_t)d.nstitch);
       skl.insert(skl.end(), d.stitch_kl, d.stitch_kl + 3 * (size_t)d.nstitch);
     }
+    // an instance without uvs reads zeros, which give every edge the warp ratio, as no uvs do
+    if (any_uv) {
+      if (d.uvs)
+        uvs.insert(uvs.end(), d.uvs, d.uvs + 2 * (size_t)d.nv);
+      else
+        uvs.insert(uvs.end(), 2 * (size_t)d.nv, 0.f);
+    }
+    MG_CHECK_ARG(d.nstretch == 0 || d.stretch_edges, "batch: null arrays");
+    for (uint64_t i = 0; i < 2ull * d.nstretch; ++i) {
+      MG_CHECK_ARG(d.stretch_edges[i] < d.nv, "batch: stretch edge index out of range");
+      sedge.push_back(d.stretch_edges[i] + o);
+    }
     inst.push_back(o + d.nv);
   }
   mguso_scene_desc u = d0;
@@ -780,6 +851,9 @@ int mguso_batch_create(mguso_ctx* ctx, const mguso_scene_desc* descs, uint32_t n
   u.stitch_idx = sidx.empty() ? nullptr : sidx.data();
   u.stitch_w = sw.empty() ? nullptr : sw.data();
   u.stitch_kl = skl.empty() ? nullptr : skl.data();
+  u.uvs = any_uv ? uvs.data() : nullptr;
+  u.nstretch = (uint32_t)(sedge.size() / 2);
+  u.stretch_edges = sedge.empty() ? nullptr : sedge.data();
   MG_CUDA(cudaSetDevice(ctx->device));
   auto sc = std::make_unique<mguso_scene>();
   sc->s.ctx = ctx;
@@ -893,6 +967,99 @@ int mguso_set_pulls(mguso_scene* sc, uint32_t n, const uint32_t* index, const fl
   MG_CUDA(cudaSetDevice(s.ctx->device));
   s.h_pulls = std::move(pulls);
   return upload_pins(s);
+}
+
+// set_strain_limit_faces (implicit.rs:1088-1121): all or nothing.
+int mguso_set_strain_limit_faces(mguso_scene* sc, uint32_t n, const uint32_t* faces, const float* limits,
+                                 const float* masses, uint32_t* kept) {
+  MG_CHECK_ARG(sc && (n == 0 || (faces && limits && masses)), "null argument");
+  Scene& s = sc->s;
+  std::vector<uint8_t> vinst(s.nv);
+  for (uint32_t k = 0; k < s.ninst; ++k)
+    for (uint32_t v = s.inst_vert[k]; v < s.inst_vert[k + 1]; ++v) vinst[v] = (uint8_t)k;
+  for (uint32_t i = 0; i < n; ++i) {
+    const uint32_t* f = faces + 3 * i;
+    MG_CHECK_ARG(f[0] < s.nv && f[1] < s.nv && f[2] < s.nv, "set_strain_limit_faces: a face index is out of range");
+    MG_CHECK_ARG(vinst[f[0]] == vinst[f[1]] && vinst[f[0]] == vinst[f[2]],
+                 "set_strain_limit_faces: a face spans two instances");
+    MG_CHECK_ARG(std::isfinite(limits[i]) && std::isfinite(masses[i]),
+                 "set_strain_limit_faces: a limit or mass is not finite");
+  }
+  MG_CUDA(cudaSetDevice(s.ctx->device));
+  std::vector<float> pos(3 * (size_t)s.nv);
+  MG_CUDA(cudaMemcpyAsync(pos.data(), s.x.p, 12 * (size_t)s.nv, cudaMemcpyDeviceToHost, s.st));
+  MG_CUDA(cudaStreamSynchronize(s.st));
+  std::vector<uint32_t> fv, fslot;
+  std::vector<float> fdm, flim, fmass;
+  for (uint32_t i = 0; i < n; ++i) {
+    if (limits[i] <= 0.f || masses[i] <= 0.f) continue;
+    const uint32_t* f = faces + 3 * i;
+    float dm[4], area;
+    if (!shell_rest_shape(hp(pos.data(), f[0]), hp(pos.data(), f[1]), hp(pos.data(), f[2]), dm, area)) continue;
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        const int sl = slot_of_pair(s, f[a], f[b]);
+        if (sl < 0 && (!s.h_pinned[f[a]] || !s.h_pinned[f[b]])) {
+          set_error("set_strain_limit_faces: a face's vertex pair shares no element, so its block lies "
+                    "outside the scene's Hessian pattern");
+          return MGUSO_ERR_UNSUPPORTED;
+        }
+        fslot.push_back(sl < 0 ? ~0u : (uint32_t)sl);
+      }
+    fv.insert(fv.end(), {f[0], f[1], f[2]});
+    fdm.insert(fdm.end(), {dm[0], dm[1], dm[2], dm[3]});
+    flim.push_back(limits[i]);
+    fmass.push_back(masses[i]);
+  }
+  const uint32_t m = (uint32_t)flim.size();
+  // contributions per touched slot and per touched vertex, in face order
+  std::vector<uint32_t> slots, verts;
+  for (uint32_t x : fslot)
+    if (x != ~0u) slots.push_back(x);
+  std::sort(slots.begin(), slots.end());
+  slots.erase(std::unique(slots.begin(), slots.end()), slots.end());
+  verts = fv;
+  std::sort(verts.begin(), verts.end());
+  verts.erase(std::unique(verts.begin(), verts.end()), verts.end());
+  std::vector<uint32_t> sptr(slots.size() + 1, 0), vptr(verts.size() + 1, 0);
+  auto rank = [](const std::vector<uint32_t>& v, uint32_t x) {
+    return (uint32_t)(std::lower_bound(v.begin(), v.end(), x) - v.begin());
+  };
+  for (uint32_t x : fslot)
+    if (x != ~0u) sptr[rank(slots, x) + 1]++;
+  for (uint32_t x : fv) vptr[rank(verts, x) + 1]++;
+  for (size_t k = 0; k < slots.size(); ++k) sptr[k + 1] += sptr[k];
+  for (size_t k = 0; k < verts.size(); ++k) vptr[k + 1] += vptr[k];
+  std::vector<uint32_t> slist(sptr.back()), vlist(vptr.back());
+  {
+    std::vector<uint32_t> sc2(sptr.begin(), sptr.end() - 1), vc(vptr.begin(), vptr.end() - 1);
+    for (uint32_t e = 0; e < 9 * m; ++e)
+      if (fslot[e] != ~0u) slist[sc2[rank(slots, fslot[e])]++] = e;
+    for (uint32_t e = 0; e < 3 * m; ++e) vlist[vc[rank(verts, fv[e])]++] = e;
+  }
+  cudaStream_t st = s.st;
+  auto up = [&](auto& buf, const auto& vec) -> int {
+    if (vec.empty()) return buf.reserve(1);
+    return buf.upload(vec.data(), vec.size(), st);
+  };
+  MG_TRY(up(s.sl_v, fv));
+  MG_TRY(up(s.sl_slot, fslot));
+  MG_TRY(up(s.sl_dm, fdm));
+  MG_TRY(up(s.sl_limit, flim));
+  MG_TRY(up(s.sl_mass, fmass));
+  MG_TRY(up(s.sl_slots, slots));
+  MG_TRY(up(s.sl_sptr, sptr));
+  MG_TRY(up(s.sl_slist, slist));
+  MG_TRY(up(s.sl_verts, verts));
+  MG_TRY(up(s.sl_vptr, vptr));
+  MG_TRY(up(s.sl_vlist, vlist));
+  MG_TRY(s.sl_c.reserve(90 * (size_t)std::max<uint32_t>(m, 1)));
+  MG_CUDA(cudaStreamSynchronize(st));
+  s.n_sl = m;
+  s.n_sl_slots = (uint32_t)slots.size();
+  s.n_sl_verts = (uint32_t)verts.size();
+  if (kept) *kept = m;
+  return MGUSO_OK;
 }
 
 int mguso_read_positions(mguso_scene* s, float* out) { return copy_state(s, s->s.x, out, nullptr); }

@@ -69,6 +69,8 @@ struct Scene {
   DevBuf<float> hinge_rest;
   DevBuf<uint32_t> spring_v;     // 2 per spring
   DevBuf<float> spring_rest;
+  DevBuf<float> spring_slr;      // per spring: its edge strain-limit ratio (used when edge_limit)
+  bool edge_limit = false;       // strain_limit_ratio > 0 and strain_limit_k > 0
   DevBuf<uint32_t> mem_v;        // 3 per Baraff-Witkin membrane element
   DevBuf<float> mem_dm, mem_area; // 4 per element (Dm^-1 row-major), area
   uint32_t n_mem = 0, n_act_mem = 0;
@@ -131,6 +133,15 @@ struct Scene {
   DevBuf<uint32_t> pv, pv_pin, pv_pull, pin_vert;
   DevBuf<float> pin_target, pin_ghat, pin_stiff, pull_target, pull_weight;
   DevBuf<uint8_t> pin_kin;
+  // strain-limit barrier faces (implicit.rs:1088-1121): vertices (3 per face), inverse rest
+  // shape (4, column-major as shells), limit and mass; per face its 9 block slots (a, b) in
+  // the slot numbering of the gather (~0u: absent, both vertices pinned) and its
+  // contribution (81 Hessian entries, row-major 9x9, then 9 gradient entries). The touched
+  // slots and vertices have their contributions listed in face order (entry = 9 face + 3 a
+  // + b for blocks, 3 face + a for gradients).
+  uint32_t n_sl = 0, n_sl_slots = 0, n_sl_verts = 0;
+  DevBuf<uint32_t> sl_v, sl_slot, sl_slots, sl_sptr, sl_slist, sl_verts, sl_vptr, sl_vlist;
+  DevBuf<float> sl_dm, sl_limit, sl_mass, sl_c;
   // colliders
   uint32_t n_col = 0;
   std::vector<float> h_colliders;
@@ -222,8 +233,9 @@ int scene_step(Scene& s, mguso_step_stats* out);
 
 // assembly (assemble.cu)
 int assemble_elastic(Scene& s);
-int assemble_colliders(Scene& s);  // pins and pulls first, then the analytic colliders
+int assemble_colliders(Scene& s);  // strain-limit faces, pins and pulls first, then the analytic colliders
 int upload_pins(Scene& s);          // groups h_pins / h_pulls by vertex onto the device
+int slot_of_pair(const Scene& s, uint32_t r, uint32_t c);  // gather slot of block (r, c), -1 if absent
 int assemble_contacts(Scene& s, uint32_t nst);
 int contact_stiffness(Scene& s, uint32_t nst);  // records s.contact_k from the gathered blocks
 int finish_rhs(Scene& s);

@@ -25,7 +25,9 @@ _PARAM_FIELDS = [("dt", C.c_float), ("gravity", C.c_float * 3), ("newton_iters",
                  ("precond", C.c_int), ("schwarz_domain", C.c_uint32), ("precision", C.c_int),
                  ("pcg_mode", C.c_int), ("factor_storage", C.c_int), ("schwarz_levels", C.c_uint32),
                  ("pcg_variant", C.c_int), ("membrane_warp", C.c_float), ("membrane_weft", C.c_float),
-                 ("membrane_shear", C.c_float), ("constraint_tol", C.c_float), ("schwarz_weight", C.c_float)]
+                 ("membrane_shear", C.c_float), ("constraint_tol", C.c_float), ("schwarz_weight", C.c_float),
+                 ("strain_limit_ratio", C.c_float), ("strain_limit_k", C.c_float),
+                 ("strain_limit_ratio_weft", C.c_float)]
 
 
 class Params(C.Structure):
@@ -38,7 +40,8 @@ class SceneDesc(C.Structure):
                 ("nshell", C.c_uint32), ("shell_faces", C.c_void_p), ("nstitch", C.c_uint32),
                 ("stitch_idx", C.c_void_p), ("stitch_w", C.c_void_p), ("stitch_kl", C.c_void_p),
                 ("ncollider", C.c_uint32), ("colliders", C.c_void_p), ("params", Params),
-                ("shell_rest", C.c_void_p), ("shell_stiff", C.c_void_p)]
+                ("shell_rest", C.c_void_p), ("shell_stiff", C.c_void_p), ("uvs", C.c_void_p),
+                ("nstretch", C.c_uint32), ("stretch_edges", C.c_void_p)]
 
 
 class StepStats(C.Structure):
@@ -61,6 +64,7 @@ def _sigs(lib):
         ("mguso_set_kinematic_collider_positions", i32, [vp, vp]),
         ("mguso_set_pins", i32, [vp, C.c_uint32, vp, vp, vp, vp, vp]),
         ("mguso_set_pulls", i32, [vp, C.c_uint32, vp, vp, vp]),
+        ("mguso_set_strain_limit_faces", i32, [vp, C.c_uint32, vp, vp, vp, vp]),
         ("mguso_scene_info", i32, [vp, vp]),
         ("mguso_scene_spmv_time", i32, [vp, i32, P(C.c_float), P(C.c_double)]),
         ("mguso_scene_assemble", i32, [vp, vp, vp, vp]),
@@ -112,10 +116,14 @@ def _desc(scene: dict, precision: str):
     d.ncollider = keep["colliders"].shape[0]
     d.colliders = ptr(keep["colliders"]) if d.ncollider else None
     d.params = make_params(scene["params"], precision)
-    for name in ("shell_rest", "shell_stiff"):
+    for name in ("shell_rest", "shell_stiff", "uvs"):
         if scene.get(name) is not None:
             keep[name] = np.ascontiguousarray(scene[name], np.float32)
             setattr(d, name, ptr(keep[name]))
+    if scene.get("stretch_edges") is not None:
+        keep["stretch_edges"] = np.ascontiguousarray(scene["stretch_edges"], np.uint32).reshape(-1, 2)
+        d.nstretch = keep["stretch_edges"].shape[0]
+        d.stretch_edges = ptr(keep["stretch_edges"]) if d.nstretch else None
     return d, keep
 
 
@@ -222,6 +230,25 @@ class ImplicitSolver:
         w = np.array([p[2] for p in pulls], np.float32)
         check(self.lib.mguso_set_pulls(self.h, n, ptr(idx) if n else None, ptr(tgt) if n else None,
                                        ptr(w) if n else None))
+
+    def set_strain_limit_faces(self, faces, limits, masses) -> int:
+        """ImplicitSolver::set_strain_limit_faces (implicit.rs:1088-1121): the strain-limit
+        barrier on each face (u32 (n, 3)) with its limit (allowed principal-stretch excess)
+        and mass, rest shape from the current positions; faces with a limit or mass <= 0 and
+        degenerate faces are skipped. Returns the number kept. Raises ValueError when the
+        arrays' lengths disagree (the reference's Err), MgusoError for an index out of range
+        or a face whose vertex pair shares no element."""
+        f = np.ascontiguousarray(faces, np.uint32).reshape(-1, 3)
+        lim = np.ascontiguousarray(limits, np.float32).reshape(-1)
+        m = np.ascontiguousarray(masses, np.float32).reshape(-1)
+        if lim.size != f.shape[0] or m.size != f.shape[0]:
+            raise ValueError(f"strain-limit arrays must match the face count: {f.shape[0]} faces, "
+                             f"{lim.size} limits, {m.size} masses")
+        n = f.shape[0]
+        kept = C.c_uint32()
+        check(self.lib.mguso_set_strain_limit_faces(self.h, n, ptr(f) if n else None, ptr(lim) if n else None,
+                                                    ptr(m) if n else None, C.byref(kept)))
+        return int(kept.value)
 
     def info(self) -> dict:
         out = np.zeros(6, np.uint32)
