@@ -1117,11 +1117,10 @@ int assemble_contacts(Scene& s, uint32_t nst) {
   k_contact_heads<<<ceil_div(mb, 256), 256, 0, st>>>(s.ckeys.p, s.cids.p, mb, s.ccblocks.p, s.Ps.row_ptr.p,
                                                     s.Ps.col.p, s.A->val.p, is_new.p);
   MG_TRY(scan_u32(s, is_new.p, rank.p, mb, s.c_count.p, tmp));
-  uint32_t nc = 0;
-  MG_CUDA(cudaMemcpyAsync(&nc, s.c_count.p, 4, cudaMemcpyDeviceToHost, st));
-  MG_CUDA(cudaStreamSynchronize(st));
-  if (nc > s.cap_c || !s.c_col.p) {
-    s.cap_c = std::max(nc, s.cap_c) * 2;
+  // C has at most one block per stencil block: sized by that bound, its count (c_count)
+  // stays on the device
+  if (mb > s.cap_c || !s.c_col.p) {
+    s.cap_c = std::max(mb, 2 * s.cap_c);
     s.work.drop_graph();
   }
   MG_TRY(s.c_row.reserve(s.cap_c));

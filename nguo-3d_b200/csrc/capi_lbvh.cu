@@ -45,7 +45,6 @@ int mguso_lbvh_download(mguso_lbvh* b, uint64_t* keys, uint32_t* perm, uint32_t*
                         float* node_boxes) {
   MG_CHECK_ARG(b, "null lbvh");
   Lbvh& L = b->b;
-  cudaStream_t s = L.ctx->stream;
   MG_CUDA(cudaDeviceSynchronize());
   uint32_t nt = L.nt;
   if (keys && nt) {
@@ -71,7 +70,6 @@ int mguso_lbvh_download(mguso_lbvh* b, uint64_t* keys, uint32_t* perm, uint32_t*
       }
     }
   }
-  (void)s;
   return MGUSO_OK;
 }
 

@@ -77,6 +77,29 @@ struct DevBuf {
   }
 };
 
+// A typed page-locked host allocation (the target of device-to-host copies that must not
+// block the host), grown on demand and freed with the object.
+template <class T>
+struct PinnedBuf {
+  T* p = nullptr;
+  size_t cap = 0;
+  PinnedBuf() = default;
+  PinnedBuf(const PinnedBuf&) = delete;
+  PinnedBuf& operator=(const PinnedBuf&) = delete;
+  ~PinnedBuf() {
+    if (p) cudaFreeHost(p);
+  }
+  int reserve(size_t n) {
+    if (n <= cap && p) return MGUSO_OK;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    MG_CUDA(cudaMallocHost((void**)&p, n * sizeof(T)));
+    cap = n;
+    return MGUSO_OK;
+  }
+};
+
 inline unsigned ceil_div(size_t a, size_t b) { return (unsigned)((a + b - 1) / b); }
 
 inline unsigned int f2u_host(float f) {

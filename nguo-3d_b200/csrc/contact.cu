@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 
 #include "elements.cuh"
 #include "scene.cuh"
@@ -524,7 +525,7 @@ __device__ __forceinline__ int first_pass_edge(const CcdPass& cp, uint32_t k, co
 }
 
 template <class R>
-__global__ void k_ccd_vt(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
+__global__ void k_ccd_vt(BvhSet bv, const CcdPass* __restrict__ cpp, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
                          const float* __restrict__ dx, const uint32_t* __restrict__ tris,
                          const uint8_t* __restrict__ ctri, const float* __restrict__ im,
                          const uint32_t* __restrict__ ex_ptr, const uint32_t* __restrict__ ex_list,
@@ -533,6 +534,7 @@ __global__ void k_ccd_vt(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vins
                          unsigned int* __restrict__ acc, uint32_t* __restrict__ status) {
   uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= nv) return;
+  const CcdPass& cp = *cpp;
   const uint32_t k = vinst[v];
   if (!((cp.todo >> k) & 1u)) return;
   const int np = (int)cp.npass[k];
@@ -596,12 +598,13 @@ __global__ void k_ccd_vt(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vins
 }
 
 template <class R>
-__global__ void k_ccd_ee(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
+__global__ void k_ccd_ee(BvhSet bv, const CcdPass* __restrict__ cpp, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
                          const float* __restrict__ dx, const uint32_t* __restrict__ edges, const float* __restrict__ im,
                          uint32_t ne, uint32_t max_iter, unsigned int* __restrict__ red,
                          unsigned int* __restrict__ acc, uint32_t* __restrict__ status) {
   uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ne) return;
+  const CcdPass& cp = *cpp;
   uint32_t b0 = edges[2 * j], b1 = edges[2 * j + 1];
   const uint32_t k = vinst[b0];
   if (!((cp.todo >> k) & 1u)) return;
@@ -670,143 +673,252 @@ __global__ void k_ccd_ee(BvhSet bv, CcdPass cp, const uint8_t* __restrict__ vins
 // + 2 self t, + 3 caps. Instances outside `active` get t = 1 and no work. Each instance runs
 // the reference's widening-radius schedule on its own displacement and edge length; a pass
 // covers every instance that still needs one.
-int ccd_step(Scene& s, uint32_t active, float* t_out, uint32_t* cap_hits) {
+// ---- the CCD schedule on the device -----------------------------------------------------
+// The widening search of ccd_max_step (implicit.rs:1829-1947) per instance: the first launch
+// runs the schedule's first radius alone, each later one up to CCD_CHUNK further radii
+// (allowed, 4 allowed, ... up to the instance's largest displacement); an instance is settled
+// by the first radius whose step fraction keeps every move inside it, or by the full radius.
+// Plan, traversals and settle run as the body of a conditional while node, so the host never
+// waits on the schedule; CcdState holds it all.
+struct CcdState {
+  CcdPass cp;  // the current launch's radii
+  float sched[PCG_MAX_INST][CCD_CHUNK];
+  float allowed[PCG_MAX_INST], max_disp[PCG_MAX_INST], half_len[PCG_MAX_INST];
+  float t[PCG_MAX_INST];  // step fraction per instance (0 for inactive ones)
+  uint32_t caps[PCG_MAX_INST];
+  uint32_t launch, todo;
+};
+
+__global__ void k_red_init(unsigned int* __restrict__ red, uint32_t K) {
+  const uint32_t i = threadIdx.x;
+  if (i >= RED_STRIDE * K) return;
+  const uint32_t q = i % RED_STRIDE;
+  red[i] = (q == 1 || q == 2) ? __float_as_uint(1.f) : 0u;
+}
+
+// Per instance: the step fraction the colliders, pins and strain limits allow (red + 1), the
+// largest displacement (red + 0) and the first allowed radius; todo = the instances whose
+// self contact is still to be checked.
+__global__ void k_ccd_start(CcdState* __restrict__ cs, const unsigned int* __restrict__ red, uint32_t K,
+                            uint32_t active, int self) {
+  const uint32_t k = threadIdx.x;
+  if (k < PCG_MAX_INST) {
+    const bool on = k < K && ((active >> k) & 1u);
+    const float md = k < K ? __uint_as_float(red[RED_STRIDE * k]) : 0.f;
+    cs->max_disp[k] = md;
+    cs->t[k] = on ? __uint_as_float(red[RED_STRIDE * k + 1]) : 0.f;
+    cs->caps[k] = 0;
+    cs->allowed[k] = fmaxf(fminf(cs->half_len[k], md), 1.0e-9f);
+  }
+  if (k == 0) {
+    cs->launch = 0;
+    cs->todo = self ? active : 0u;
+  }
+}
+
+// This launch's radii per undecided instance, and fresh accumulators.
+__global__ void k_ccd_plan(CcdState* __restrict__ cs, unsigned int* __restrict__ acc, float fixed) {
+  const uint32_t k = threadIdx.x;
+  if (k < PCG_MAX_INST * CCD_CHUNK) {
+    acc[2 * k] = __float_as_uint(1.f);
+    acc[2 * k + 1] = 0u;
+  }
+  if (k >= PCG_MAX_INST) return;
+  if (k == 0) cs->cp.todo = cs->todo;
+  if (!((cs->todo >> k) & 1u)) {
+    cs->cp.npass[k] = 0;
+    return;
+  }
+  const float md = cs->max_disp[k];
+  float a = cs->allowed[k];
+  uint32_t n = 0;
+  for (;;) {
+    cs->sched[k][n] = a;
+    cs->cp.search[k][n] = fixed + 2.0f * a;
+    ++n;
+    if (cs->launch == 0 || n == (uint32_t)CCD_CHUNK || a >= md) break;
+    a = fminf(a * 4.0f, md);
+  }
+  cs->cp.npass[k] = n;
+}
+
+// Settles every instance whose launch decided it, widens the others, and sets the loop's
+// condition: go on while an instance is undecided, for at most 64 launches.
+__global__ void k_ccd_settle(CcdState* __restrict__ cs, const unsigned int* __restrict__ acc,
+                             cudaGraphConditionalHandle h) {
+  __shared__ uint32_t settled_mask;
+  const uint32_t k = threadIdx.x;
+  if (k == 0) settled_mask = 0;
+  __syncthreads();
+  if (k < PCG_MAX_INST && ((cs->cp.todo >> k) & 1u)) {
+    const uint32_t np = cs->cp.npass[k];
+    const float md = cs->max_disp[k];
+    bool settled = false;
+    for (uint32_t i = 0; i < np && !settled; ++i) {
+      const bool full = cs->sched[k][i] >= md;
+      const float t_self = __uint_as_float(acc[2 * (CCD_CHUNK * k + i)]);
+      if (full || t_self * md <= cs->sched[k][i]) {
+        cs->caps[k] = acc[2 * (CCD_CHUNK * k + i) + 1];
+        cs->t[k] = fminf(cs->t[k], t_self);
+        settled = true;
+      }
+    }
+    if (settled)
+      atomicOr(&settled_mask, 1u << k);
+    else
+      cs->allowed[k] = fminf(cs->sched[k][np - 1] * 4.0f, md);
+  }
+  __syncthreads();
+  if (k == 0) {
+    cs->todo &= ~settled_mask;
+    cs->launch += 1;
+    cudaGraphSetConditional(h, (cs->todo && cs->launch < 64) ? 1u : 0u);
+  }
+}
+
+__global__ void k_ccd_clamp(CcdState* __restrict__ cs) {
+  const uint32_t k = threadIdx.x;
+  if (k < PCG_MAX_INST) cs->t[k] = fminf(fmaxf(cs->t[k], 0.f), 1.f);
+}
+
+// The self-contact schedule's graph: one conditional while node around plan, the two
+// traversals and settle. Rebuilt when a by-value argument changes.
+static int ccd_graph(Scene& s, const BvhSet& tv, const BvhSet& ev, CcdState* cs) {
+  cudaStream_t st = s.st;
+  const float dhat = s.p.contact_dhat;
+  const float fixed = dhat;  // max_edge_gap() + 2 * max_edge_offset() for face edges
+  const uint32_t iters = std::max<uint32_t>(s.p.ccd_max_iter, 1);
+  std::vector<unsigned char> key(2 * sizeof(BvhSet) + 8 * sizeof(void*) + 16);
+  unsigned char* q = key.data();
+  auto put = [&](const void* p, size_t n) {
+    std::memcpy(q, p, n);
+    q += n;
+  };
+  put(&tv, sizeof(BvhSet));
+  put(&ev, sizeof(BvhSet));
+  const void* ptrs[8] = {s.x.p, s.dx.p, s.tris.p, s.edges.p, s.ccd_acc.p, s.red.p, s.side_best.p, cs};
+  put(ptrs, sizeof(ptrs));
+  const uint32_t misc[4] = {s.nv, s.n_edge, iters, s.mixed ? 1u : 0u};
+  put(misc, sizeof(misc));
+  if (s.ccd_exec && key == s.ccd_key) return MGUSO_OK;
+  if (s.ccd_exec) cudaGraphExecDestroy(s.ccd_exec);
+  s.ccd_exec = nullptr;
+  cudaGraph_t g = nullptr;
+  MG_CUDA(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle cond;
+  cudaGraphNodeParams cp = {};
+  cudaGraphNode_t node;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault);
+  if (e == cudaSuccess) {
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    e = cudaGraphAddNode(&node, g, nullptr, 0, &cp);
+  }
+  if (e == cudaSuccess)
+    e = cudaStreamBeginCaptureToGraph(st, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    MG_CUDA(e);
+  }
+  const CcdPass* cpp = &cs->cp;
+  k_ccd_plan<<<1, PCG_MAX_INST * CCD_CHUNK, 0, st>>>(cs, s.ccd_acc.p, fixed);
+  if (s.mixed) {
+    k_ccd_vt<double><<<ceil_div(s.nv, 128), 128, 0, st>>>(
+        tv, cpp, s.vinst.p, s.x.p, s.dx.p, s.tris.p, s.collider_tri.p, s.inv_mass.p, s.ex_ptr.p, s.ex_list.p,
+        s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.red.p, s.ccd_acc.p, s.status.p);
+    if (s.n_edge)
+      k_ccd_ee<double><<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, cpp, s.vinst.p, s.x.p, s.dx.p, s.edges.p,
+                                                               s.inv_mass.p, s.n_edge, iters, s.red.p, s.ccd_acc.p,
+                                                               s.status.p);
+  } else {
+    k_ccd_vt<float><<<ceil_div(s.nv, 128), 128, 0, st>>>(
+        tv, cpp, s.vinst.p, s.x.p, s.dx.p, s.tris.p, s.collider_tri.p, s.inv_mass.p, s.ex_ptr.p, s.ex_list.p,
+        s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.red.p, s.ccd_acc.p, s.status.p);
+    if (s.n_edge)
+      k_ccd_ee<float><<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, cpp, s.vinst.p, s.x.p, s.dx.p, s.edges.p,
+                                                              s.inv_mass.p, s.n_edge, iters, s.red.p, s.ccd_acc.p,
+                                                              s.status.p);
+  }
+  k_ccd_settle<<<1, 32, 0, st>>>(cs, s.ccd_acc.p, cond);
+  const cudaError_t le = cudaGetLastError();
+  cudaGraph_t body = nullptr;
+  e = cudaStreamEndCapture(st, &body);
+  if (le != cudaSuccess || e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    MG_CUDA(le);
+    MG_CUDA(e);
+  }
+  const cudaError_t ie = cudaGraphInstantiate(&s.ccd_exec, g, 0);
+  cudaGraphDestroy(g);
+  MG_CUDA(ie);
+  s.ccd_key = key;
+  return MGUSO_OK;
+}
+
+// The step fraction along s.dx from s.x for every instance in `active` (ccd_max_step,
+// implicit.rs:1690-1947): analytic colliders, static pins and strain-limit faces in single
+// launches, then with self collision the widening schedule as one graph launch. Everything is
+// enqueued on the scene's stream with no host wait; the results land in the device state
+// (read by k_advance through ccd_t) and in a pinned copy that ccd_results reads once the
+// stream has passed it.
+int ccd_step(Scene& s, uint32_t active) {
   cudaStream_t st = s.st;
   const uint32_t K = s.ninst;
-  for (uint32_t k = 0; k < K; ++k) {
-    t_out[k] = 1.f;
-    cap_hits[k] = 0;
+  MG_TRY(s.ccd_state.reserve(sizeof(CcdState)));
+  MG_TRY(s.ccd_acc.reserve(2 * CCD_CHUNK * PCG_MAX_INST));
+  MG_TRY(s.ccd_out.reserve(sizeof(CcdState)));
+  CcdState* cs = (CcdState*)s.ccd_state.p;
+  if (!s.ccd_half_set) {
+    float hl[PCG_MAX_INST] = {};
+    for (uint32_t k = 0; k < K; ++k) hl[k] = 0.5f * s.char_len[k];
+    MG_CUDA(cudaMemcpyAsync(cs->half_len, hl, sizeof(hl), cudaMemcpyHostToDevice, st));
+    s.ccd_half_set = true;
   }
-  if (s.n_col == 0 && !s.p.self_collision && s.n_static_pin == 0 && s.n_sl == 0) return MGUSO_OK;
-  std::vector<unsigned int> init(RED_STRIDE * K, 0u);
-  for (uint32_t k = 0; k < K; ++k) {
-    init[RED_STRIDE * k + 1] = f2u_host(1.f);
-    init[RED_STRIDE * k + 2] = f2u_host(1.f);
+  const bool self = s.p.self_collision != 0;
+  k_red_init<<<1, RED_STRIDE * PCG_MAX_INST, 0, st>>>(s.red.p, K);
+  if (s.n_col || self || s.n_static_pin || s.n_sl) {
+    const int sms = s.ctx->sm_count;
+    k_max_norm<<<std::min<uint32_t>(ceil_div(s.nv, 256), sms * 4), 256, 0, st>>>(s.dx.p, s.vinst.p, s.nv, s.red.p);
+    if (s.n_col && s.n_free)
+      k_ccd_colliders<<<ceil_div(s.n_free, 128), 128, 0, st>>>(s.free_verts.p, s.n_free, s.vinst.p, s.x.p, s.dx.p,
+                                                             s.colliders.p, s.n_col, s.red.p);
+    if (s.n_static_pin)
+      k_ccd_pins<<<ceil_div(s.n_pin, 128), 128, 0, st>>>(s.pin_vert.p, s.n_pin, s.pin_kin.p, s.pin_target.p,
+                                                        s.pin_ghat.p, s.inv_mass.p, s.vinst.p, s.x.p, s.dx.p, s.red.p);
+    if (s.n_sl)
+      k_ccd_sl<<<ceil_div(s.n_sl, 128), 128, 0, st>>>(s.n_sl, s.sl_v.p, s.sl_dm.p, s.sl_limit.p, s.vinst.p, s.x.p,
+                                                     s.dx.p, s.red.p);
   }
-  MG_CUDA(cudaMemcpyAsync(s.red.p, init.data(), 4 * init.size(), cudaMemcpyHostToDevice, st));
-  int sms = s.ctx->sm_count;
-  k_max_norm<<<std::min<uint32_t>(ceil_div(s.nv, 256), sms * 4), 256, 0, st>>>(s.dx.p, s.vinst.p, s.nv, s.red.p);
-  if (s.n_col && s.n_free)
-    k_ccd_colliders<<<ceil_div(s.n_free, 128), 128, 0, st>>>(s.free_verts.p, s.n_free, s.vinst.p, s.x.p, s.dx.p,
-                                                           s.colliders.p, s.n_col, s.red.p);
-  if (s.n_static_pin)
-    k_ccd_pins<<<ceil_div(s.n_pin, 128), 128, 0, st>>>(s.pin_vert.p, s.n_pin, s.pin_kin.p, s.pin_target.p,
-                                                      s.pin_ghat.p, s.inv_mass.p, s.vinst.p, s.x.p, s.dx.p, s.red.p);
-  if (s.n_sl)
-    k_ccd_sl<<<ceil_div(s.n_sl, 128), 128, 0, st>>>(s.n_sl, s.sl_v.p, s.sl_dm.p, s.sl_limit.p, s.vinst.p, s.x.p,
-                                                   s.dx.p, s.red.p);
+  k_ccd_start<<<1, 32, 0, st>>>(cs, s.red.p, K, active, self ? 1 : 0);
   MG_CUDA(cudaGetLastError());
-  std::vector<unsigned int> h(RED_STRIDE * K);
-  MG_CUDA(cudaMemcpyAsync(h.data(), s.red.p, 4 * h.size(), cudaMemcpyDeviceToHost, st));
-  MG_CUDA(cudaStreamSynchronize(st));
-  float max_disp[PCG_MAX_INST], allowed[PCG_MAX_INST];
-  for (uint32_t k = 0; k < K; ++k) {
-    max_disp[k] = u2f_host(h[RED_STRIDE * k]);
-    if ((active >> k) & 1u) t_out[k] = u2f_host(h[RED_STRIDE * k + 1]);
-  }
-  if (s.p.self_collision) {
-    const float dhat = s.p.contact_dhat;
-    const float fixed = dhat;  // max_edge_gap() + 2 * max_edge_offset() for face edges
-    uint32_t todo = active;
-    for (uint32_t k = 0; k < K; ++k) allowed[k] = std::max(std::min(0.5f * s.char_len[k], max_disp[k]), 1.0e-9f);
-    uint32_t iters = std::max<uint32_t>(s.p.ccd_max_iter, 1);
+  if (self) {
     // the trees' displacement boxes (the trees were built at this iterate)
     for (uint32_t k = 0; k < K; ++k) {
       MG_TRY(lbvh_refit_disp(s.tri_bvh[k].get(), s.dx.p, s.tris.p + 3 * (size_t)s.inst_tri[k], st));
       MG_TRY(lbvh_refit_disp(s.edge_bvh[k].get(), s.dx.p, s.edge_tris.p + 3 * (size_t)s.inst_edge[k], st));
     }
     const BvhSet tv = view_set(s.tri_bvh, s.inst_tri), ev = view_set(s.edge_bvh, s.inst_edge);
-    static const bool trace = std::getenv("MGUSO_TRACE") && std::getenv("MGUSO_TRACE")[0] == '2';
-    cudaEvent_t ev3[3];
-    if (trace)
-      for (auto& e : ev3) MG_CUDA(cudaEventCreate(&e));
-    MG_TRY(s.ccd_acc.reserve(2 * CCD_CHUNK * PCG_MAX_INST));
-    std::vector<unsigned int> acc0(2 * CCD_CHUNK * PCG_MAX_INST), acc(2 * CCD_CHUNK * PCG_MAX_INST);
-    for (int i = 0; i < CCD_CHUNK * PCG_MAX_INST; ++i) {
-      acc0[2 * i] = f2u_host(1.f);
-      acc0[2 * i + 1] = 0u;
-    }
-    // launch 0 runs the schedule's first pass alone (often decisive, and cheap); each later
-    // launch runs up to CCD_CHUNK further passes of every undecided instance in one traversal
-    float sched[PCG_MAX_INST][CCD_CHUNK];
-    for (int launch = 0; launch < 64 && todo; ++launch) {
-      if (trace) MG_CUDA(cudaEventRecord(ev3[0], st));
-      CcdPass cp{};
-      cp.todo = todo;
-      for (uint32_t k = 0; k < K; ++k) {
-        if (!((todo >> k) & 1u)) continue;
-        float a_ = allowed[k];
-        uint32_t n = 0;
-        for (;;) {
-          sched[k][n] = a_;
-          cp.search[k][n] = fixed + 2.0f * a_;
-          ++n;
-          if (launch == 0 || n == (uint32_t)CCD_CHUNK || a_ >= max_disp[k]) break;
-          a_ = std::min(a_ * 4.0f, max_disp[k]);
-        }
-        cp.npass[k] = n;
-      }
-      MG_CUDA(cudaMemcpyAsync(s.ccd_acc.p, acc0.data(), 4 * acc0.size(), cudaMemcpyHostToDevice, st));
-      if (s.mixed) {
-        k_ccd_vt<double><<<ceil_div(s.nv, 128), 128, 0, st>>>(
-            tv, cp, s.vinst.p, s.x.p, s.dx.p, s.tris.p, s.collider_tri.p, s.inv_mass.p, s.ex_ptr.p, s.ex_list.p,
-            s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.red.p, s.ccd_acc.p,
-            s.status.p);
-        if (trace) MG_CUDA(cudaEventRecord(ev3[1], st));
-        if (s.n_edge)
-          k_ccd_ee<double><<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, cp, s.vinst.p, s.x.p, s.dx.p, s.edges.p,
-                                                                   s.inv_mass.p, s.n_edge, iters, s.red.p,
-                                                                   s.ccd_acc.p, s.status.p);
-      } else {
-        k_ccd_vt<float><<<ceil_div(s.nv, 128), 128, 0, st>>>(
-            tv, cp, s.vinst.p, s.x.p, s.dx.p, s.tris.p, s.collider_tri.p, s.inv_mass.p, s.ex_ptr.p, s.ex_list.p,
-            s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.red.p, s.ccd_acc.p,
-            s.status.p);
-        if (trace) MG_CUDA(cudaEventRecord(ev3[1], st));
-        if (s.n_edge)
-          k_ccd_ee<float><<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, cp, s.vinst.p, s.x.p, s.dx.p, s.edges.p,
-                                                                  s.inv_mass.p, s.n_edge, iters, s.red.p,
-                                                                  s.ccd_acc.p, s.status.p);
-      }
-      MG_CUDA(cudaGetLastError());
-      if (trace) MG_CUDA(cudaEventRecord(ev3[2], st));
-      MG_CUDA(cudaMemcpyAsync(acc.data(), s.ccd_acc.p, 4 * acc.size(), cudaMemcpyDeviceToHost, st));
-      MG_CUDA(cudaMemcpyAsync(h.data(), s.red.p, 4 * h.size(), cudaMemcpyDeviceToHost, st));
-      MG_CUDA(cudaStreamSynchronize(st));
-      if (trace) {
-        float ms_all = 0, ms_vt = 0;
-        MG_CUDA(cudaEventElapsedTime(&ms_all, ev3[0], ev3[2]));
-        MG_CUDA(cudaEventElapsedTime(&ms_vt, ev3[0], ev3[1]));
-        unsigned long long lv = 0, av = 0, le = 0, ae = 0;
-        for (uint32_t k = 0; k < K; ++k) {
-          lv += h[RED_STRIDE * k + 5];
-          av += h[RED_STRIDE * k + 6];
-          le += h[RED_STRIDE * k + 7];
-          ae += h[RED_STRIDE * k + 8];
-        }
-        fprintf(stderr, "[mguso]   ccd launch %d todo %x passes %u: vt %.3f ms (leaves %llu, accd %llu), ee %.3f ms "
-                "(leaves %llu, accd %llu)\n", launch, todo, cp.npass[0], ms_vt, lv, av, ms_all - ms_vt, le, ae);
-      }
-      for (uint32_t k = 0; k < K; ++k) {
-        if (!((todo >> k) & 1u)) continue;
-        bool settled = false;
-        for (uint32_t i = 0; i < cp.npass[k] && !settled; ++i) {
-          const bool full = sched[k][i] >= max_disp[k];
-          const float t_self = u2f_host(acc[2 * (CCD_CHUNK * k + i)]);
-          if (full || t_self * max_disp[k] <= sched[k][i]) {
-            cap_hits[k] = acc[2 * (CCD_CHUNK * k + i) + 1];
-            t_out[k] = std::min(t_out[k], t_self);
-            todo &= ~(1u << k);
-            settled = true;
-          }
-        }
-        if (!settled) allowed[k] = std::min(sched[k][cp.npass[k] - 1] * 4.0f, max_disp[k]);
-      }
-    }
-    if (trace)
-      for (auto& e : ev3) cudaEventDestroy(e);
+    MG_TRY(ccd_graph(s, tv, ev, cs));
+    MG_CUDA(cudaGraphLaunch(s.ccd_exec, st));
   }
-  for (uint32_t k = 0; k < K; ++k) t_out[k] = std::min(std::max(t_out[k], 0.f), 1.f);
+  k_ccd_clamp<<<1, 32, 0, st>>>(cs);
+  MG_CUDA(cudaGetLastError());
+  MG_CUDA(cudaMemcpyAsync(s.ccd_out.p, cs, sizeof(CcdState), cudaMemcpyDeviceToHost, st));
+  return MGUSO_OK;
+}
+
+const float* ccd_t(Scene& s) { return ((CcdState*)s.ccd_state.p)->t; }
+
+int ccd_results(Scene& s, float* t_out, uint32_t* cap_hits) {
+  MG_CUDA(cudaStreamSynchronize(s.st));
+  const CcdState* cs = (const CcdState*)s.ccd_out.p;
+  for (uint32_t k = 0; k < s.ninst; ++k) {
+    t_out[k] = cs->t[k];
+    cap_hits[k] = cs->caps[k];
+  }
   return MGUSO_OK;
 }
 

@@ -174,7 +174,7 @@ struct FusedInst {
 struct FusedCtl {
   uint32_t counter[2];
   uint32_t all_done;
-  uint32_t pad;
+  uint32_t rounds;  // graph bodies of FUSED_CHECK iterations run (device-driven loop)
 };
 
 struct PcgInstResult {

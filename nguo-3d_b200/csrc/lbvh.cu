@@ -177,7 +177,19 @@ template <class K>
 __global__ void __launch_bounds__(RS_THREADS) k_onesweep(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                          K* __restrict__ kout, uint32_t* __restrict__ vout,
                                                          uint32_t n, int shift, const uint32_t* __restrict__ gofs,
-                                                         uint32_t* status, uint32_t* tile_counter, uint32_t* err) {
+                                                         uint32_t* status, uint32_t* tile_counter, uint32_t* err,
+                                                         const uint32_t* __restrict__ phist) {
+  // phist (the pass's digit histogram, or null): when every key has the same digit the pass
+  // keeps the order, and each CTA only copies its tile (the same decision in every CTA, so
+  // no look-back is started); the host then never reads the histogram back
+  if (phist && phist[(uint32_t)((kin[0] >> shift) & 0xff)] == n) {
+    const uint32_t b0 = blockIdx.x * RS_TILE, b1 = min(b0 + RS_TILE, n);
+    for (uint32_t j = b0 + threadIdx.x; j < b1; j += RS_THREADS) {
+      kout[j] = kin[j];
+      vout[j] = vin[j];
+    }
+    return;
+  }
   __shared__ uint32_t whist[RS_WARPS][256];
   __shared__ uint32_t tile_excl[256], g_pref[256];
   __shared__ K skeys[RS_TILE];
@@ -497,28 +509,20 @@ static int sort_impl(Lbvh* b, K* keys, uint32_t* vals, uint32_t n, int key_bits,
   k_rs_hist<K><<<std::min<uint32_t>(ceil_div(n, 256), sms * 8), 256, 0, s>>>(keys, n, passes, b->rs_hist.p);
   k_rs_scan<<<passes, 256, 0, s>>>(b->rs_hist.p, b->rs_ofs.p);
   MG_CUDA(cudaGetLastError());
-  // passes whose digit is the same for every key leave the order unchanged: skip them
-  std::vector<uint32_t> h(passes * 256);
-  MG_CUDA(cudaMemcpyAsync(h.data(), b->rs_hist.p, 4 * passes * 256, cudaMemcpyDeviceToHost, s));
-  MG_CUDA(cudaStreamSynchronize(s));
+  // every pass is launched; a pass whose digit is the same for every key finds that out on
+  // the device and only copies, so the sort needs no readback
   K* kA = keys;
   uint32_t* vA = vals;
   K* kB = (K*)b->rs_tmpk.p;
   uint32_t* vB = b->rs_tmpv.p;
-  b->last_sort_passes = 0;
   for (int p = 0; p < passes; ++p) {
-    bool trivial = false;
-    for (int d = 0; d < 256; ++d)
-      if (h[p * 256 + d] == n) trivial = true;
-    if (trivial) continue;
     MG_CUDA(cudaMemsetAsync(b->rs_status.p, 0, 4 * (size_t)ntiles * 256, s));
     MG_CUDA(cudaMemsetAsync(b->rs_counter.p, 0, 4, s));
     k_onesweep<K><<<ntiles, RS_THREADS, 0, s>>>(kA, vA, kB, vB, n, 8 * p, b->rs_ofs.p + p * 256, b->rs_status.p,
-                                               b->rs_counter.p, b->status.p);
+                                               b->rs_counter.p, b->status.p, b->rs_hist.p + p * 256);
     MG_CUDA(cudaGetLastError());
     std::swap(kA, kB);
     std::swap(vA, vB);
-    b->last_sort_passes++;
   }
   if (kA != keys) {
     MG_CUDA(cudaMemcpyAsync(keys, kA, sizeof(K) * (size_t)n, cudaMemcpyDeviceToDevice, s));
@@ -705,7 +709,8 @@ static int noalloc_sort(unsigned char* sc, K* keys, uint32_t* vals, uint32_t n, 
   for (int p = 0; p < passes; ++p) {
     MG_CUDA(cudaMemsetAsync(status, 0, 4 * (size_t)ntiles * 256, s));
     MG_CUDA(cudaMemsetAsync(counter, 0, 4, s));
-    k_onesweep<K><<<ntiles, RS_THREADS, 0, s>>>(kA, vA, kB, vB, n, 8 * p, ofs + p * 256, status, counter, err);
+    k_onesweep<K><<<ntiles, RS_THREADS, 0, s>>>(kA, vA, kB, vB, n, 8 * p, ofs + p * 256, status, counter, err,
+                                               nullptr);
     MG_CUDA(cudaGetLastError());
     std::swap(kA, kB);
     std::swap(vA, vB);

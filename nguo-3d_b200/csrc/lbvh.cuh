@@ -24,7 +24,6 @@ struct Lbvh {
   // radix-sort scratch
   DevBuf<uint32_t> rs_hist, rs_ofs, rs_status, rs_counter, rs_tmpv;
   DevBuf<unsigned char> rs_tmpk;
-  int last_sort_passes = 0;
   // query scratch
   DevBuf<float4> qbox;
   DevBuf<uint32_t> qkeys, qorder;

@@ -751,6 +751,15 @@ static int sell_build(Scene& s) {
   return MGUSO_OK;
 }
 
+__global__ void k_fr_reset(FusedInst* __restrict__ inst, FusedCtl* __restrict__ ctl, uint32_t K, uint32_t active) {
+  const uint32_t k = threadIdx.x;
+  if (k < K) {
+    inst[k] = FusedInst{};
+    inst[k].done = ((active >> k) & 1u) ? 0u : 1u;
+  }
+  if (k == 0) *ctl = FusedCtl{};
+}
+
 // Layout of the fused kernels over the scene's instances and the arguments of both; resets
 // the per-instance state (instances outside `active` start done) on the scene's stream.
 static int fused_prepare(Scene& s, const uint32_t* h_inst_row, uint32_t K, uint32_t active, FusedArgs& a, Launch& L) {
@@ -796,12 +805,9 @@ static int fused_prepare(Scene& s, const uint32_t* h_inst_row, uint32_t K, uint3
   MG_TRY(s.fr_inst.reserve(PCG_MAX_INST));
   MG_TRY(s.fr_ctl.reserve(1));
   MG_TRY(s.fr_part.reserve(2ull * std::max(L.grid_rows, L.grid_dom)));
-  FusedInst hi[PCG_MAX_INST] = {};
-  for (uint32_t k = 0; k < K; ++k) hi[k].done = ((active >> k) & 1u) ? 0u : 1u;
-  FusedCtl hc{};
-  MG_CUDA(cudaMemcpyAsync(s.fr_inst.p, hi, sizeof(FusedInst) * K, cudaMemcpyHostToDevice, st));
-  // pageable sources: the copies are staged before cudaMemcpyAsync returns
-  MG_CUDA(cudaMemcpyAsync(s.fr_ctl.p, &hc, sizeof(FusedCtl), cudaMemcpyHostToDevice, st));
+  // per-instance state and loop control reset on the device (no host copy to wait for)
+  k_fr_reset<<<1, 32, 0, st>>>(s.fr_inst.p, s.fr_ctl.p, K, active);
+  MG_CUDA(cudaGetLastError());
 
   a = FusedArgs{};
   a.ninst = K;
@@ -847,6 +853,15 @@ static int fused_prepare(Scene& s, const uint32_t* h_inst_row, uint32_t K, uint3
   return MGUSO_OK;
 }
 
+// The device-driven loop's condition: after each body of FUSED_CHECK iterations, go on while
+// an instance is still iterating and fewer than max_rounds bodies have run (the bound the
+// host-driven loop had: cg_max_iter + FUSED_CHECK iterations launched).
+__global__ void k_fr_continue(FusedCtl* __restrict__ ctl, cudaGraphConditionalHandle h, uint32_t max_rounds) {
+  const uint32_t r = ctl->rounds + 1;
+  ctl->rounds = r;
+  cudaGraphSetConditional(h, (!ctl->all_done && r < max_rounds) ? 1u : 0u);
+}
+
 static int launch_dom(const Scene& s, const Launch& L, FusedArgs& a, const float* pc, float* pinit, int init) {
   void* args[] = {(void*)&a, (void*)&pc, (void*)&pinit, (void*)&init};
   MG_CUDA(cudaLaunchKernel(L.dom, dim3(L.grid_dom), dim3(L.dom_threads), args, L.dom_smem, s.st));
@@ -878,11 +893,33 @@ int pcg_fused(Scene& s, const uint32_t* h_inst_row, uint32_t K, uint32_t active,
   std::memcpy(gk.data() + sizeof(FusedArgs) + sizeof(void*), &p1, sizeof(void*));
   std::memcpy(gk.data() + sizeof(FusedArgs) + 2 * sizeof(void*), &L.grid_rows, 4);
   std::memcpy(gk.data() + sizeof(FusedArgs) + 2 * sizeof(void*) + 4, &L.grid_dom, 4);
+  // The whole solve is one graph launch: a conditional while node whose body runs FUSED_CHECK
+  // iterations and then k_fr_continue, which decides on the device whether to go on, so the
+  // host neither waits nor reads anything until the solve has finished.
+  const uint32_t max_rounds = ceil_div(s.p.cg_max_iter + FUSED_CHECK, FUSED_CHECK);
   if (gk != s.fr_graph_key || !s.fr_exec) {
     if (s.fr_exec) cudaGraphExecDestroy(s.fr_exec);
     s.fr_exec = nullptr;
     cudaGraph_t g = nullptr;
-    MG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    MG_CUDA(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle cond;
+    cudaGraphNodeParams cp = {};
+    cudaGraphNode_t node;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) {
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = cond;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      e = cudaGraphAddNode(&node, g, nullptr, 0, &cp);
+    }
+    if (e == cudaSuccess)
+      e = cudaStreamBeginCaptureToGraph(st, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(g);
+      MG_CUDA(e);
+    }
     int rc = MGUSO_OK;
     for (uint32_t i = 0; i < FUSED_CHECK && rc == MGUSO_OK; ++i) {
       const float* po = (i & 1) ? p1 : p0;
@@ -890,27 +927,33 @@ int pcg_fused(Scene& s, const uint32_t* h_inst_row, uint32_t K, uint32_t active,
       rc = launch_rows(s, L, a, po, pn);
       if (rc == MGUSO_OK) rc = launch_dom(s, L, a, pn, pn, 0);
     }
-    cudaError_t e = cudaStreamEndCapture(st, &g);
-    if (rc != MGUSO_OK) {
-      if (g) cudaGraphDestroy(g);
-      return rc;
+    if (rc == MGUSO_OK) {
+      k_fr_continue<<<1, 1, 0, st>>>(s.fr_ctl.p, cond, max_rounds);
+      if (cudaGetLastError() != cudaSuccess) rc = MGUSO_ERR_CUDA;
     }
-    MG_CUDA(e);
+    cudaGraph_t body = nullptr;
+    e = cudaStreamEndCapture(st, &body);
+    if (rc != MGUSO_OK || e != cudaSuccess) {
+      cudaGraphDestroy(g);
+      if (rc != MGUSO_OK) return rc;
+      MG_CUDA(e);
+    }
     cudaError_t ie = cudaGraphInstantiate(&s.fr_exec, g, 0);
     cudaGraphDestroy(g);
     MG_CUDA(ie);
     s.fr_graph_key = gk;
   }
-  FusedCtl h{};
-  for (uint32_t launched = 0; launched < s.p.cg_max_iter + FUSED_CHECK; launched += FUSED_CHECK) {
-    MG_CUDA(cudaGraphLaunch(s.fr_exec, st));
-    MG_CUDA(cudaMemcpyAsync(&h, s.fr_ctl.p, sizeof(FusedCtl), cudaMemcpyDeviceToHost, st));
-    MG_CUDA(cudaStreamSynchronize(st));
-    if (h.all_done) break;
-  }
-  FusedInst hi[PCG_MAX_INST] = {};
-  MG_CUDA(cudaMemcpyAsync(hi, s.fr_inst.p, sizeof(FusedInst) * K, cudaMemcpyDeviceToHost, st));
-  MG_CUDA(cudaStreamSynchronize(st));
+  MG_CUDA(cudaGraphLaunch(s.fr_exec, st));
+  MG_TRY(s.fr_out.reserve(PCG_MAX_INST));
+  MG_CUDA(cudaMemcpyAsync(s.fr_out.p, s.fr_inst.p, sizeof(FusedInst) * K, cudaMemcpyDeviceToHost, st));
+  if (!out) return MGUSO_OK;  // deferred: the caller syncs the stream, then pcg_fused_results
+  return pcg_fused_results(s, K, out);
+}
+
+// The per-instance results of the last pcg_fused, once the stream has passed its copy.
+int pcg_fused_results(Scene& s, uint32_t K, PcgInstResult* out) {
+  MG_CUDA(cudaStreamSynchronize(s.st));
+  const FusedInst* hi = s.fr_out.p;
   for (uint32_t k = 0; k < K; ++k) {
     out[k].iters = hi[k].iters;
     out[k].residual = hi[k].residual;

@@ -1129,7 +1129,8 @@ extern "C" int mguso_scene_ccd(mguso_scene* sc, const float* x, const float* dx,
   }
   std::vector<float> t(s.ninst, 1.f);
   std::vector<uint32_t> caps(s.ninst, 0u);
-  MG_TRY(ccd_step(s, (s.ninst >= 32 ? ~0u : ((1u << s.ninst) - 1u)), t.data(), caps.data()));
+  MG_TRY(ccd_step(s, (s.ninst >= 32 ? ~0u : ((1u << s.ninst) - 1u))));
+  MG_TRY(ccd_results(s, t.data(), caps.data()));
   MG_CUDA(cudaStreamSynchronize(st));
   for (uint32_t k = 0; k < s.ninst; ++k) {
     t_out[k] = t[k];

@@ -186,6 +186,7 @@ struct Scene {
   uint32_t fr_grid_rows = 0, fr_grid_dom = 0;
   DevBuf<FusedInst> fr_inst;
   DevBuf<FusedCtl> fr_ctl;
+  PinnedBuf<FusedInst> fr_out;  // the last solve's per-instance results, copied back without a wait
   DevBuf<double> fr_part;
   cudaGraphExec_t fr_exec = nullptr;
   int fr_rows_variant = 0, fr_dom_variant = 0;  // the fused kernels in use (see pcg_fused.cu)
@@ -199,6 +200,7 @@ struct Scene {
   bool fr_tuned = false;
   ~Scene() {
     if (fr_exec) cudaGraphExecDestroy(fr_exec);
+    if (ccd_exec) cudaGraphExecDestroy(ccd_exec);
   }
   DevBuf<unsigned long long> st_keys;
   DevBuf<uint32_t> st_ids;
@@ -218,6 +220,11 @@ struct Scene {
   // reductions / CCD
   DevBuf<unsigned int> red;                 // per-iteration reductions (float bits), RED_STRIDE per instance
   DevBuf<unsigned int> ccd_acc;             // CCD per (instance, pass): step fraction bits, caps
+  DevBuf<unsigned char> ccd_state;          // the device-driven CCD schedule (contact.cu)
+  PinnedBuf<unsigned char> ccd_out;         // its copy for the host, read after the stream passes it
+  bool ccd_half_set = false;                // half the characteristic lengths uploaded into it
+  cudaGraphExec_t ccd_exec = nullptr;       // the self-contact schedule's conditional graph
+  std::vector<unsigned char> ccd_key;
   DevBuf<uint32_t> status;
 
   // linear solve
@@ -244,12 +251,20 @@ int system_spmv(Scene& s, const float* p, float* ap, cudaStream_t st, const DotS
 // contact (contact.cu)
 int build_bvhs(Scene& s, const float* x);
 int pcg_persistent(Scene& s, const uint32_t* h_inst_row, uint32_t ninst, uint32_t active, PcgInstResult* out);
+// out == null defers the results: the caller synchronises the stream later and reads them with
+// pcg_fused_results (the solve itself never waits on the host)
 int pcg_fused(Scene& s, const uint32_t* h_inst_row, uint32_t ninst, uint32_t active, PcgInstResult* out);
+int pcg_fused_results(Scene& s, uint32_t ninst, PcgInstResult* out);
 int pcg_fused_profile(Scene& s, uint32_t iters, float* us2);
 int pcg_fused_select(Scene& s);  // the fused kernels' variants: pcg_variant, or the autotuner's choice
 int collect_stencils(Scene& s, uint32_t* nst);
 int self_intersections(Scene& s);  // piercing pairs per instance at s.x into red[RED_STRIDE k + 14]
-int ccd_step(Scene& s, uint32_t active, float* t_out, uint32_t* cap_hits);
+// CCD step fractions of the instances in `active` along s.dx, enqueued without a host wait:
+// ccd_t is the device array of fractions (0 for inactive instances), ccd_results waits for
+// the stream and gives fractions and ACCD cap hits per instance
+int ccd_step(Scene& s, uint32_t active);
+const float* ccd_t(Scene& s);
+int ccd_results(Scene& s, float* t_out, uint32_t* cap_hits);
 
 }  // namespace mg
 

@@ -28,25 +28,28 @@ __global__ void k_predict(const float* __restrict__ x0, const float* __restrict_
   }
 }
 
-// per-instance floats passed by value (step fractions, rescales)
-struct InstF {
-  float v[PCG_MAX_INST];
-};
-
-__global__ void k_scale_copy(const float* __restrict__ in, InstF sc, const uint8_t* __restrict__ vinst, uint32_t n,
-                             float* __restrict__ out) {
+// dx = s_k * x on instance k's rows; with red given, s_k = min(max_dx / |x|_max, 1) from
+// instance k's largest vertex norm red[RED_STRIDE k] (float bits; 0 leaves x alone), the
+// uniform max_dx rescale of implicit.rs:1996-2004 decided on the device
+__global__ void k_scale_copy(const float* __restrict__ in, const unsigned int* __restrict__ red, float max_dx,
+                             const uint8_t* __restrict__ vinst, uint32_t n, float* __restrict__ out) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const float s = sc.v[vinst[i / 3]];
+  float s = 1.f;
+  if (red) {
+    const float m = __uint_as_float(red[RED_STRIDE * vinst[i / 3]]);
+    if (m > 0.f) s = fminf(max_dx / m, 1.0f);
+  }
   out[i] = s == 1.f ? in[i] : in[i] * s;
 }
 
-// x += t_k dx on instance k's vertices; red[RED_STRIDE k + 9] = max |t dx_i| (float bits)
-__global__ void k_advance(float* __restrict__ x, const float* __restrict__ dx, InstF t, const uint8_t* __restrict__ vinst,
-                          uint32_t nv, unsigned int* __restrict__ red) {
+// x += t_k dx on instance k's vertices, t the CCD's device array of step fractions (0 for
+// inactive instances); red[RED_STRIDE k + 9] = max |t dx_i| (float bits)
+__global__ void k_advance(float* __restrict__ x, const float* __restrict__ dx, const float* __restrict__ t,
+                          const uint8_t* __restrict__ vinst, uint32_t nv, unsigned int* __restrict__ red) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x) {
     const uint32_t k = vinst[i];
-    const float tk = t.v[k];
+    const float tk = t[k];
     if (tk == 0.f) continue;
     float d0 = dx[3 * i] * tk, d1 = dx[3 * i + 1] * tk, d2 = dx[3 * i + 2] * tk;
     x[3 * i] += d0;
@@ -117,9 +120,19 @@ __global__ void k_max_norm(const float* __restrict__ dx, const uint8_t* __restri
 int schwarz_factor_with(mguso_schwarz* s, const uint32_t* c_rp, const uint32_t* c_col, const float* c_val,
                         cudaStream_t st);
 
+static void fused_stats(const Scene& s, const PcgInstResult* r, mguso_lin_stats* ls) {
+  for (uint32_t k = 0; k < s.ninst; ++k) {
+    ls[k].iters = r[k].iters;
+    ls[k].residual = r[k].residual;
+    ls[k].status = (r[k].residual <= s.p.cg_tol || (r[k].status & ST_PCG_BREAKDOWN)) ? MGUSO_OK : MGUSO_ERR_PCG_CAP;
+  }
+}
+
 // Factorises the preconditioner and solves every instance in `active` (the others get
-// dx = 0); ls[k] = instance k's PCG statistics.
-static int linear_solve(Scene& s, uint32_t active, mguso_lin_stats* ls) {
+// dx = 0); ls[k] = instance k's PCG statistics. With `deferred` given, the fused PCG leaves
+// its statistics to be read after the caller's next stream synchronisation
+// (pcg_fused_results) and sets *deferred; ls is then not written.
+static int linear_solve(Scene& s, uint32_t active, mguso_lin_stats* ls, bool* deferred = nullptr) {
   cudaStream_t st = s.st;
   if (s.schwarz) {
     MG_TRY(schwarz_factor_with(s.schwarz.get(), s.c_row_ptr.p, s.c_col.p, s.c_val.p, st));
@@ -130,14 +143,14 @@ static int linear_solve(Scene& s, uint32_t active, mguso_lin_stats* ls) {
   if (!two_level && (s.p.pcg_mode == 0 || s.p.pcg_mode == 2 || s.ninst > 1)) {
     PcgInstResult r[PCG_MAX_INST] = {};
     if (s.p.pcg_mode != 2) MG_TRY(pcg_fused_select(s));
+    const bool defer = deferred && s.p.pcg_mode != 2;
     int rc = s.p.pcg_mode == 2 ? pcg_persistent(s, s.inst_vert.data(), s.ninst, active, r)
-                               : pcg_fused(s, s.inst_vert.data(), s.ninst, active, r);
+                               : pcg_fused(s, s.inst_vert.data(), s.ninst, active, defer ? nullptr : r);
     if (rc == MGUSO_OK) {
-      for (uint32_t k = 0; k < s.ninst; ++k) {
-        ls[k].iters = r[k].iters;
-        ls[k].residual = r[k].residual;
-        ls[k].status = (r[k].residual <= s.p.cg_tol || (r[k].status & ST_PCG_BREAKDOWN)) ? MGUSO_OK : MGUSO_ERR_PCG_CAP;
-      }
+      if (defer)
+        *deferred = true;
+      else
+        fused_stats(s, r, ls);
       return MGUSO_OK;
     }
     if (rc != MGUSO_ERR_UNSUPPORTED) return rc;
@@ -217,44 +230,43 @@ int scene_step(Scene& s, mguso_step_stats* out) {
     MG_TRY(finish_rhs(s));
     ph[2] = mark();
     mguso_lin_stats ls[PCG_MAX_INST] = {};
-    MG_TRY(linear_solve(s, active, ls));
+    bool deferred = false;
+    MG_TRY(linear_solve(s, active, ls, &deferred));
     ph[3] = mark();
-    InstF rescale;
+    // uniform max_dx rescale per instance (implicit.rs:1996-2004); INFINITY leaves dx alone
+    const bool cap_dx = std::isfinite(s.p.max_dx);
+    if (cap_dx) {
+      MG_CUDA(cudaMemsetAsync(s.red.p, 0, 4 * RED_STRIDE * K, st));
+      k_max_norm<<<std::min<uint32_t>(ceil_div(nv, 256), sms * 4), 256, 0, st>>>(s.work.x.p, s.vinst.p, nv, s.red.p);
+    }
+    k_scale_copy<<<ceil_div(n3, 256), 256, 0, st>>>(s.work.x.p, cap_dx ? s.red.p : nullptr, s.p.max_dx, s.vinst.p, n3,
+                                                    s.dx.p);
+    MG_CUDA(cudaGetLastError());
+    MG_TRY(ccd_step(s, active));
+    MG_CUDA(cudaMemsetAsync(s.red.p, 0, 4 * RED_STRIDE * K, st));
+    k_advance<<<std::min<uint32_t>(ceil_div(nv, 256), sms * 4), 256, 0, st>>>(s.x.p, s.dx.p, ccd_t(s), s.vinst.p, nv,
+                                                                             s.red.p);
+    MG_CUDA(cudaMemcpyAsync(hred.data(), s.red.p, 4 * hred.size(), cudaMemcpyDeviceToHost, st));
+    // the iteration's one wait: its step lengths, with the CCD's and the PCG's results
+    float t[PCG_MAX_INST];
+    uint32_t caps[PCG_MAX_INST];
+    MG_TRY(ccd_results(s, t, caps));
     for (uint32_t k = 0; k < K; ++k) {
-      rescale.v[k] = 1.f;
+      if (!((active >> k) & 1u)) continue;
+      stats[k].ccd_cap_hits += caps[k];
+      stats[k].t_min = std::min(stats[k].t_min, (double)t[k]);
+    }
+    if (deferred) {  // the stream has passed the PCG's result copy
+      PcgInstResult r[PCG_MAX_INST] = {};
+      MG_TRY(pcg_fused_results(s, K, r));
+      fused_stats(s, r, ls);
+    }
+    for (uint32_t k = 0; k < K; ++k) {
       if (!((active >> k) & 1u)) continue;
       stats[k].stencils = std::max(stats[k].stencils, nst);
       stats[k].max_reresid = std::max(stats[k].max_reresid, ls[k].residual);
       stats[k].max_cg_iters = std::max(stats[k].max_cg_iters, ls[k].iters);
     }
-    // uniform max_dx rescale per instance (implicit.rs:1996-2004); INFINITY leaves dx alone
-    if (std::isfinite(s.p.max_dx)) {
-      MG_CUDA(cudaMemsetAsync(s.red.p, 0, 4 * RED_STRIDE * K, st));
-      k_max_norm<<<std::min<uint32_t>(ceil_div(nv, 256), sms * 4), 256, 0, st>>>(s.work.x.p, s.vinst.p, nv, s.red.p);
-      MG_CUDA(cudaMemcpyAsync(hred.data(), s.red.p, 4 * hred.size(), cudaMemcpyDeviceToHost, st));
-      MG_CUDA(cudaStreamSynchronize(st));
-      for (uint32_t k = 0; k < K; ++k) {
-        const float max_norm = u2f_host(hred[RED_STRIDE * k]);
-        if (max_norm > 0.f) rescale.v[k] = std::min(s.p.max_dx / max_norm, 1.0f);
-      }
-    }
-    k_scale_copy<<<ceil_div(n3, 256), 256, 0, st>>>(s.work.x.p, rescale, s.vinst.p, n3, s.dx.p);
-    MG_CUDA(cudaGetLastError());
-    float t[PCG_MAX_INST];
-    uint32_t caps[PCG_MAX_INST];
-    MG_TRY(ccd_step(s, active, t, caps));
-    InstF tk;
-    for (uint32_t k = 0; k < K; ++k) {
-      tk.v[k] = ((active >> k) & 1u) ? t[k] : 0.f;
-      if (!((active >> k) & 1u)) continue;
-      stats[k].ccd_cap_hits += caps[k];
-      stats[k].t_min = std::min(stats[k].t_min, (double)t[k]);
-    }
-    MG_CUDA(cudaMemsetAsync(s.red.p, 0, 4 * RED_STRIDE * K, st));
-    k_advance<<<std::min<uint32_t>(ceil_div(nv, 256), sms * 4), 256, 0, st>>>(s.x.p, s.dx.p, tk, s.vinst.p, nv,
-                                                                             s.red.p);
-    MG_CUDA(cudaMemcpyAsync(hred.data(), s.red.p, 4 * hred.size(), cudaMemcpyDeviceToHost, st));
-    MG_CUDA(cudaStreamSynchronize(st));
     for (uint32_t k = 0; k < K; ++k) {
       if (!((active >> k) & 1u)) continue;
       const float max_step = u2f_host(hred[RED_STRIDE * k + 9]);
