@@ -473,11 +473,12 @@ def traffic_from_profiles(kernel: str):
     import glob
     import re
 
-    pat = re.compile(r"traffic_bytes_per_launch\s+(\S+)\s*=\s*([0-9.eE+]+)")
+    pat = re.compile(r"traffic_bytes_per_launch\s+`?(.+?)`?\s*=\s*([0-9.eE+]+)")
+    want = kernel.replace(" ", "")
     for f in sorted(glob.glob(os.path.join(REPO, "profiles", "*.md"))):
         for line in open(f):
             m = pat.search(line)
-            if m and m.group(1) == kernel:
+            if m and m.group(1).replace(" ", "") == want:
                 return float(m.group(2)), os.path.basename(f)
     return None, None
 
