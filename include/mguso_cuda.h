@@ -246,11 +246,13 @@ typedef struct {
   uint32_t schwarz_levels; /* 1 (or 0): one-level Schwarz (SchwarzCpu, linsolve.rs:463-520);
                               2: two-level Galerkin Schwarz (SchwarzMlCpu, linsolve.rs:534-836) */
   int pcg_variant;         /* kernels of the fused PCG (pcg_mode 0): 0 = chosen by the autotuner
-                              at the scene's first solve (cached per system size); v in 1..16
-                              fixes the rows kernel (v - 1) / 4 (0, 1, 2: 2, 1 or 4 lanes per
+                              at the scene's first solve (cached per system size); v in 1..24
+                              fixes the rows kernel (v - 1) / 6 (0, 1, 2: 2, 1 or 4 lanes per
                               block row over the BSR; 3: one lane per row over a sliced-ELL copy)
-                              and the Schwarz domain kernel (v - 1) % 4 (one warp per domain, 4
-                              per CTA; three warps per domain, 1, 2 or 4 domains per CTA) */
+                              and the Schwarz domain kernel (v - 1) % 6 (0: one warp per domain,
+                              4 per CTA; 1, 2, 3: three warps per domain, 1, 2 or 4 domains per
+                              CTA; 4, 5: FP16 tiles on the tensor cores, one warp per domain, 4
+                              or 8 per CTA, else as 0) */
   float membrane_warp;     /* Baraff-Witkin membrane stiffnesses (ImplicitParams::membrane_warp /
                               _weft / _shear, implicit.rs:39-43): 0 = off. The membrane covers
                               every triangle of tris, rest shape from the initial positions */

@@ -124,8 +124,9 @@ int PcgWork::reserve(uint32_t n_) {
   MG_TRY(b.reserve(n));
   MG_TRY(x.reserve(n));
   MG_TRY(r.reserve(n));
-  MG_TRY(z.reserve(n));
-  MG_TRY(p.reserve(n));
+  // z and the directions have room for 4 floats per vertex (the fused PCG's padded layout)
+  MG_TRY(z.reserve(4 * ((size_t)n / 3 + 1)));
+  MG_TRY(p.reserve(4 * ((size_t)n / 3 + 1)));
   MG_TRY(ap.reserve(n));
   size_t after = (size_t)b.p + (size_t)x.p + (size_t)r.p + (size_t)z.p + (size_t)p.p + (size_t)ap.p;
   if (before != after) drop_graph();

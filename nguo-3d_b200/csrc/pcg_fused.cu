@@ -31,6 +31,16 @@ constexpr int FD_WARPS = 4;        // Schwarz, one warp per domain: warps (domai
 constexpr int FD_THREADS = 256;    // block Jacobi: vertices per CTA
 constexpr uint32_t FUSED_CHECK = 16;
 
+// z and the search directions are stored with 4 floats per vertex (xyz, w unused): a
+// neighbour's z and p_old are two 16-byte loads in the SpMV gather. x, r, b and Ap keep 3.
+__device__ __forceinline__ uint32_t zpos(uint32_t e) { return 4 * (e / 3) + e % 3; }
+__device__ __forceinline__ float4 ld_v4(const float* __restrict__ v, uint32_t i) {
+  return __ldg(reinterpret_cast<const float4*>(v) + i);
+}
+__device__ __forceinline__ void st_v4(float* __restrict__ v, uint32_t i, float x, float y, float z) {
+  reinterpret_cast<float4*>(v)[i] = make_float4(x, y, z, 0.f);
+}
+
 struct FusedArgs {
   uint32_t ninst;
   const uint32_t* lay;  // [0, K] rows, [9 ..] row-kernel CTAs, [18 ..] domain-kernel CTAs, [27 ..] domains
@@ -129,9 +139,10 @@ __global__ void __launch_bounds__(FR_THREADS) k_fr_rows(FusedArgs a, const float
     for (uint32_t row = row0 + (lc * FR_THREADS + tid) / FR_LPR; row < row1; row += nc * FR_THREADS / FR_LPR) {
       Acc y0 = 0, y1 = 0, y2 = 0;
       auto block = [&](const float* __restrict__ m9, uint32_t c) {
-        const Acc x0 = (Acc)fmaf(be, po[3 * c], a.z[3 * c]);
-        const Acc x1 = (Acc)fmaf(be, po[3 * c + 1], a.z[3 * c + 1]);
-        const Acc x2 = (Acc)fmaf(be, po[3 * c + 2], a.z[3 * c + 2]);
+        const float4 zc = ld_v4(a.z, c), pc4 = ld_v4(po, c);
+        const Acc x0 = (Acc)fmaf(be, pc4.x, zc.x);
+        const Acc x1 = (Acc)fmaf(be, pc4.y, zc.y);
+        const Acc x2 = (Acc)fmaf(be, pc4.z, zc.z);
         y0 = fr_fma((Acc)__ldg(m9 + 0), x0, y0);
         y0 = fr_fma((Acc)__ldg(m9 + 1), x1, y0);
         y0 = fr_fma((Acc)__ldg(m9 + 2), x2, y0);
@@ -155,12 +166,11 @@ __global__ void __launch_bounds__(FR_THREADS) k_fr_rows(FusedArgs a, const float
       }
       if (sub == 0) {
         const float f0 = (float)y0, f1 = (float)y1, f2 = (float)y2;
-        const float q0 = fmaf(be, po[3 * row], a.z[3 * row]);
-        const float q1 = fmaf(be, po[3 * row + 1], a.z[3 * row + 1]);
-        const float q2 = fmaf(be, po[3 * row + 2], a.z[3 * row + 2]);
-        pn[3 * row] = q0;
-        pn[3 * row + 1] = q1;
-        pn[3 * row + 2] = q2;
+        const float4 zr = ld_v4(a.z, row), pr = ld_v4(po, row);
+        const float q0 = fmaf(be, pr.x, zr.x);
+        const float q1 = fmaf(be, pr.y, zr.y);
+        const float q2 = fmaf(be, pr.z, zr.z);
+        st_v4(pn, row, q0, q1, q2);
         a.ap[3 * row] = f0;
         a.ap[3 * row + 1] = f1;
         a.ap[3 * row + 2] = f2;
@@ -197,9 +207,10 @@ __global__ void __launch_bounds__(FR_THREADS) k_fr_rows_sell(FusedArgs a, const 
     const uint32_t b0 = __ldg(a.sell_base + gs), b1 = __ldg(a.sell_base + gs + 1);
     Acc y0 = 0, y1 = 0, y2 = 0;
     auto gather = [&](uint32_t c, Acc& x0, Acc& x1, Acc& x2) {
-      x0 = (Acc)fmaf(be, po[3 * c], a.z[3 * c]);
-      x1 = (Acc)fmaf(be, po[3 * c + 1], a.z[3 * c + 1]);
-      x2 = (Acc)fmaf(be, po[3 * c + 2], a.z[3 * c + 2]);
+      const float4 zc = ld_v4(a.z, c), pc4 = ld_v4(po, c);
+      x0 = (Acc)fmaf(be, pc4.x, zc.x);
+      x1 = (Acc)fmaf(be, pc4.y, zc.y);
+      x2 = (Acc)fmaf(be, pc4.z, zc.z);
     };
     if (row < row1) {
 #pragma unroll 2
@@ -234,12 +245,11 @@ __global__ void __launch_bounds__(FR_THREADS) k_fr_rows_sell(FusedArgs a, const 
         y2 = fr_fma((Acc)__ldg(m9 + 8), x2, y2);
       }
       const float f0 = (float)y0, f1 = (float)y1, f2 = (float)y2;
-      const float q0 = fmaf(be, po[3 * row], a.z[3 * row]);
-      const float q1 = fmaf(be, po[3 * row + 1], a.z[3 * row + 1]);
-      const float q2 = fmaf(be, po[3 * row + 2], a.z[3 * row + 2]);
-      pn[3 * row] = q0;
-      pn[3 * row + 1] = q1;
-      pn[3 * row + 2] = q2;
+      const float4 zr = ld_v4(a.z, row), pr = ld_v4(po, row);
+      const float q0 = fmaf(be, pr.x, zr.x);
+      const float q1 = fmaf(be, pr.y, zr.y);
+      const float q2 = fmaf(be, pr.z, zr.z);
+      st_v4(pn, row, q0, q1, q2);
       a.ap[3 * row] = f0;
       a.ap[3 * row + 1] = f1;
       a.ap[3 * row + 2] = f2;
@@ -345,9 +355,9 @@ __global__ void __launch_bounds__(32 * FD_WARPS) k_fr_schwarz(FusedArgs a, const
           v = a.b[e];
           a.x[e] = 0.f;
           a.r[e] = v;
-          p_init[e] = 0.f;
+          p_init[zpos(e)] = 0.f;
         } else if (upd) {
-          a.x[e] = fmaf(al, pc[e], a.x[e]);
+          a.x[e] = fmaf(al, pc[zpos(e)], a.x[e]);
           v = fmaf(-al, a.ap[e], a.r[e]);
           a.r[e] = v;
         } else {
@@ -365,7 +375,7 @@ __global__ void __launch_bounds__(32 * FD_WARPS) k_fr_schwarz(FusedArgs a, const
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           const float zi = (float)zz[c];
-          a.z[3 * v + c] = zi;
+          a.z[4 * v + c] = zi;
           rr += (Acc)rd[3 * lane + c] * (Acc)rd[3 * lane + c];
           rz += (Acc)rd[3 * lane + c] * (Acc)zi;
         }
@@ -388,7 +398,107 @@ __global__ void __launch_bounds__(32 * FD_WARPS) k_fr_schwarz(FusedArgs a, const
         const int i = 32 * J + lane;
         if (i < m) {
           const float zi = (float)(zz[J] * sc * sc);
-          a.z[3 * a.dom_verts[vs + i / 3] + i % 3] = zi;
+          a.z[4 * a.dom_verts[vs + i / 3] + i % 3] = zi;
+          rr += (Acc)rd[i] * (Acc)rd[i];
+          rz += (Acc)rd[i] * (Acc)zi;
+        }
+      }
+    }
+  }
+  const Acc s0 = block_sum<Acc>(rr);
+  const Acc s1 = block_sum<Acc>(rz);
+  if (threadIdx.x == 0) {
+    a.part[2 * blockIdx.x] = (double)s0;
+    a.part[2 * blockIdx.x + 1] = (double)s1;
+  }
+  if (!last_cta(&a.ctl->counter[1])) return;
+  fd_finish(a, init != 0);
+}
+
+// Schwarz domains on the tensor cores (FP16 tiles): one warp per domain, DOMS domains per CTA;
+// the domain's apply is tc_apply (mma.sync over 16 x 16 blocks of its tiles, the vectors split
+// into three FP16 terms, FP32 accumulation). Otherwise as k_fr_schwarz.
+constexpr uint32_t TC_SLICE_BYTES = 6 * TILE_FLOATS * 2 + 3 * 96 * 4;  // tiles, r, y, z
+
+template <class Acc, int DOMS>
+__global__ void __launch_bounds__(32 * DOMS) k_fr_schwarz_tc(FusedArgs a, const float* __restrict__ pc,
+                                                            float* __restrict__ p_init, int init) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  if (!init && a.ctl->all_done) return;
+  const uint32_t K = a.ninst;
+  const int k = cta_instance(a.lay + 2 * LAY, K);
+  const uint32_t c0 = __ldg(a.lay + 2 * LAY + k);
+  const uint32_t d = __ldg(a.lay + 3 * LAY + k) + (blockIdx.x - c0) * DOMS + (threadIdx.x >> 5);
+  const uint32_t dend = __ldg(a.lay + 3 * LAY + k + 1);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const bool upd = !init && a.inst[k].upd != 0;
+  const float al = (float)a.inst[k].alpha;
+  const bool skip = !init && a.inst[k].done != 0 && !upd;
+  uint64_t* bar = (uint64_t*)(smem + 16 * w);
+  __half* buf = (__half*)(smem + 128 + (size_t)w * TC_SLICE_BYTES);
+  float* rd = (float*)(buf + 6 * TILE_FLOATS);
+  float* ys = rd + 96;
+  float* zs = ys + 96;
+  Acc rr = 0, rz = 0;
+  if (d < dend && !skip) {
+    const uint32_t vs = a.dom_start[d], nvd = a.dom_start[d + 1] - vs;
+    const int m = 3 * (int)nvd;
+    const uint64_t off = a.fac_off[d];
+    const uint32_t bytes = (uint32_t)((a.fac_off[d + 1] - off) * sizeof(__half));
+    const bool diag = a.dom_diag[d] != 0;
+    if (lane == 0 && !diag) {
+      mbar_init(bar, 1);
+      fence_mbar_init();
+      fence_proxy_async();
+      mbar_arrive_expect_tx(bar, bytes);
+      bulk_g2s(buf, (const __half*)a.fac + off, bytes, bar);
+    }
+    for (int i = lane; i < 96; i += 32) {
+      float v = 0.f;
+      if (i < m) {
+        const uint32_t e = 3 * a.dom_verts[vs + i / 3] + i % 3;
+        if (init) {
+          v = a.b[e];
+          a.x[e] = 0.f;
+          a.r[e] = v;
+          p_init[zpos(e)] = 0.f;
+        } else if (upd) {
+          a.x[e] = fmaf(al, pc[zpos(e)], a.x[e]);
+          v = fmaf(-al, a.ap[e], a.r[e]);
+          a.r[e] = v;
+        } else {
+          v = a.r[e];
+        }
+      }
+      rd[i] = v;
+    }
+    __syncwarp();
+    if (diag) {
+      if (lane < (int)nvd) {
+        const uint32_t v = a.dom_verts[vs + lane];
+        Acc zz[3];
+        vertex_apply<Acc>(a.vfac + 6 * (size_t)v, rd + 3 * lane, zz);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float zi = (float)zz[c];
+          a.z[4 * v + c] = zi;
+          rr += (Acc)rd[3 * lane + c] * (Acc)rd[3 * lane + c];
+          rz += (Acc)rd[3 * lane + c] * (Acc)zi;
+        }
+      }
+    } else if (!mbar_wait(bar, 0)) {
+      if (lane == 0) atomicOr(&a.inst[k].status, ST_WAIT_TIMEOUT);
+      mbar_wait(bar, 0);  // bounded again: the copy may still land
+    } else {
+      float zz[3];
+      tc_apply(buf, rd, ys, zs, m, zz, lane);
+      const float sc = a.fac_scale[d];
+#pragma unroll
+      for (int J = 0; J < 3; ++J) {
+        const int i = 32 * J + lane;
+        if (i < m) {
+          const float zi = (float)((Acc)zz[J] * (Acc)sc * (Acc)sc);
+          a.z[4 * a.dom_verts[vs + i / 3] + i % 3] = zi;
           rr += (Acc)rd[i] * (Acc)rd[i];
           rz += (Acc)rd[i] * (Acc)zi;
         }
@@ -484,9 +594,9 @@ __global__ void __launch_bounds__(96 * DOMS) k_fr_schwarz3(FusedArgs a, const fl
         v = a.b[e];
         a.x[e] = 0.f;
         a.r[e] = v;
-        p_init[e] = 0.f;
+        p_init[zpos(e)] = 0.f;
       } else if (upd) {
-        a.x[e] = fmaf(al, pc[e], a.x[e]);
+        a.x[e] = fmaf(al, pc[zpos(e)], a.x[e]);
         v = fmaf(-al, a.ap[e], a.r[e]);
         a.r[e] = v;
       } else {
@@ -504,7 +614,7 @@ __global__ void __launch_bounds__(96 * DOMS) k_fr_schwarz3(FusedArgs a, const fl
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const float zi = (float)zz[c];
-      a.z[3 * v + c] = zi;
+      a.z[4 * v + c] = zi;
       rr += (Acc)rd[3 * lane + c] * (Acc)rd[3 * lane + c];
       rz += (Acc)rd[3 * lane + c] * (Acc)zi;
     }
@@ -529,7 +639,7 @@ __global__ void __launch_bounds__(96 * DOMS) k_fr_schwarz3(FusedArgs a, const fl
       const float* rj = rd + 32 * f3_tile_j(t);
       AA y = 0;
 #pragma unroll 8
-      for (int c = 0; c < 32; ++c) y += (AA)tile_ld(w, tile_offset(lane, c)) * (AA)rj[c];
+      for (int c = 0; c < 32; ++c) y += (AA)tile_ld(w, tile_off<TS>(lane, c)) * (AA)rj[c];
       part[(2 * q + slot) * 32 + lane] = y;
     }
   }
@@ -554,7 +664,7 @@ __global__ void __launch_bounds__(96 * DOMS) k_fr_schwarz3(FusedArgs a, const fl
       const AA* yi = yd + 32 * f3_tile_i(t);
       AA z = 0;
 #pragma unroll 8
-      for (int r = 0; r < 32; ++r) z += (AA)tile_ld(w, tile_offset(r, lane)) * yi[r];
+      for (int r = 0; r < 32; ++r) z += (AA)tile_ld(w, tile_off<TS>(r, lane)) * yi[r];
       part[(2 * q + slot) * 32 + lane] = z;
     }
   }
@@ -570,7 +680,7 @@ __global__ void __launch_bounds__(96 * DOMS) k_fr_schwarz3(FusedArgs a, const fl
     if (i < m) {
       const AA sc = a.fac_scale ? (AA)a.fac_scale[d] : (AA)1;
       const float zi = (float)(z * sc * sc);
-      a.z[3 * a.dom_verts[vs + i / 3] + i % 3] = zi;
+      a.z[4 * a.dom_verts[vs + i / 3] + i % 3] = zi;
       rr = (Acc)rd[i] * (Acc)rd[i];
       rz = (Acc)rd[i] * (Acc)zi;
     }
@@ -608,9 +718,9 @@ __global__ void __launch_bounds__(FD_THREADS) k_fr_bj(FusedArgs a, const float* 
         q[c] = a.b[e];
         a.x[e] = 0.f;
         a.r[e] = q[c];
-        p_init[e] = 0.f;
+        p_init[zpos(e)] = 0.f;
       } else if (upd) {
-        a.x[e] = fmaf(al, pc[e], a.x[e]);
+        a.x[e] = fmaf(al, pc[zpos(e)], a.x[e]);
         q[c] = fmaf(-al, a.ap[e], a.r[e]);
         a.r[e] = q[c];
       } else {
@@ -621,9 +731,9 @@ __global__ void __launch_bounds__(FD_THREADS) k_fr_bj(FusedArgs a, const float* 
     const float z0 = m9[0] * q[0] + m9[1] * q[1] + m9[2] * q[2];
     const float z1 = m9[3] * q[0] + m9[4] * q[1] + m9[5] * q[2];
     const float z2 = m9[6] * q[0] + m9[7] * q[1] + m9[8] * q[2];
-    a.z[3 * v] = z0;
-    a.z[3 * v + 1] = z1;
-    a.z[3 * v + 2] = z2;
+    a.z[4 * v] = z0;
+    a.z[4 * v + 1] = z1;
+    a.z[4 * v + 2] = z2;
     rr = (Acc)q[0] * (Acc)q[0] + (Acc)q[1] * (Acc)q[1] + (Acc)q[2] * (Acc)q[2];
     rz = (Acc)q[0] * (Acc)z0 + (Acc)q[1] * (Acc)z1 + (Acc)q[2] * (Acc)z2;
   }
@@ -640,10 +750,13 @@ __global__ void __launch_bounds__(FD_THREADS) k_fr_bj(FusedArgs a, const float* 
 namespace {
 // The fused kernels' variants the autotuner chooses between (per scene, cached per system
 // size): rows kernel with 2, 1 or 4 lanes per block row over the BSR, or one lane per row over
-// the sliced-ELL copy; Schwarz domain kernel with one warp per domain (4 domains per CTA) or
-// three warps per domain (1, 2 or 4 domains per CTA).
+// the sliced-ELL copy; Schwarz domain kernel with one warp per domain (4 domains per CTA),
+// three warps per domain (1, 2 or 4 domains per CTA), or, for FP16 tiles, one warp per domain
+// on the tensor cores (4 or 8 domains per CTA; with FP32 tiles these two fall back to the
+// first).
 constexpr int N_ROWS_VARIANTS = 4;
-constexpr int N_DOM_VARIANTS = 4;
+constexpr int N_DOM_VARIANTS = 6;
+constexpr int DOM_TC4 = 4, DOM_TC8 = 5;
 constexpr int ROWS_LPR[N_ROWS_VARIANTS] = {2, 1, 4, 1};
 constexpr int ROWS_SELL = 3;
 
@@ -667,6 +780,14 @@ void* rows_fn(int rv) {
 
 template <class Acc, class TS>
 void dom_fn(int dv, Launch& L) {
+  if (sizeof(TS) == 2 && (dv == DOM_TC4 || dv == DOM_TC8)) {
+    const int n = dv == DOM_TC4 ? 4 : 8;
+    L.dom = n == 4 ? (void*)k_fr_schwarz_tc<Acc, 4> : (void*)k_fr_schwarz_tc<Acc, 8>;
+    L.doms_per_cta = n;
+    L.dom_threads = 32 * n;
+    L.dom_smem = 128 + (size_t)n * TC_SLICE_BYTES;
+    return;
+  }
   switch (dv) {
     case 1:
       L.dom = (void*)k_fr_schwarz3<Acc, TS, 1>;
@@ -1059,7 +1180,7 @@ static int fused_autotune(Scene& s) {
   s.fr_rows_variant = br;
   int bd = 0;
   if (s.schwarz) {
-    for (int dv = 0; dv < N_DOM_VARIANTS; ++dv) {
+    for (int dv = 0; dv < (s.schwarz->half ? N_DOM_VARIANTS : DOM_TC4); ++dv) {
       s.fr_dom_variant = dv;
       MG_TRY(pcg_fused_profile(s, 2, us2));
       MG_TRY(pcg_fused_profile(s, 12, us2));

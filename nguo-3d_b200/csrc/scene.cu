@@ -136,7 +136,7 @@ static int validate_desc(const mguso_scene_desc* d) {
                    std::isfinite(d->params.membrane_shear) && d->params.membrane_warp >= 0 &&
                    d->params.membrane_weft >= 0 && d->params.membrane_shear >= 0,
                "scene: membrane stiffnesses must be finite and >= 0");
-  MG_CHECK_ARG(d->params.pcg_variant >= 0 && d->params.pcg_variant <= 16, "scene: pcg_variant must be in [0, 16]");
+  MG_CHECK_ARG(d->params.pcg_variant >= 0 && d->params.pcg_variant <= 24, "scene: pcg_variant must be in [0, 24]");
   MG_CHECK_ARG(std::isfinite(d->params.schwarz_weight) && d->params.schwarz_weight >= 0.f,
                "scene: schwarz_weight must be finite and >= 0");
   MG_CHECK_ARG(std::isfinite(d->params.strain_limit_ratio) && std::isfinite(d->params.strain_limit_k) &&

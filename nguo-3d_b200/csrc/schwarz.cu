@@ -317,7 +317,7 @@ __device__ void factor_dense_store(double* A, int ld, int m, double* dinv, doubl
     for (int r = tid; r < m; r += nt) {
       double a = diag0[r];
       const int I = r >> 5, lr = r & 31;
-      out[tile_index(I, I) * TILE_FLOATS + tile_offset(lr, lr)] = to_tile<TS>((a > 1e-14 ? 1.0 / sqrt(a) : 1.0) / sc);
+      out[tile_index(I, I) * TILE_FLOATS + tile_off<TS>(lr, lr)] = to_tile<TS>((a > 1e-14 ? 1.0 / sqrt(a) : 1.0) / sc);
     }
     if (tid == 0) atomicOr(status, 1u << 8);
     return;
@@ -332,7 +332,8 @@ __device__ void factor_dense_store(double* A, int ld, int m, double* dinv, doubl
   for (int e = tid; e < nfl; e += nt) {
     const int t = e / TILE_FLOATS, o = e - t * TILE_FLOATS;
     const int I = t >= 3 ? 2 : (t >= 1 ? 1 : 0), J = t - I * (I + 1) / 2;
-    const int c = o >> 5, r = (o & 31) ^ c;
+    int r, c;
+    tile_rc<TS>(o, r, c);
     const int gi = 32 * I + r, gj = 32 * J + c;
     out[e] = to_tile<TS>((gi < m && gj <= gi) ? A[gj * ld + gi] * inv_sc : 0.0);
   }
@@ -528,7 +529,7 @@ int schwarz_factor_with(mguso_schwarz* s, const uint32_t* c_rp, const uint32_t* 
 // W tiles into its shared slice, gathers r, then
 //   pass 1: y = W r    lane = row within a row tile, loop over columns c;
 //   pass 2: z = W^T y  lane = column within a column tile, loop over rows r.
-// The swizzled tile offset c*32 + (r ^ c) makes both passes free of bank conflicts. Every
+// The FP32 tile layout (c*32 + (r ^ c)) makes both passes free of bank conflicts. Every
 // lane carries one accumulator per tile row/column (<= 3), so there are no long serial
 // chains. Acc = double (mixed precision) accumulates in FP64.
 // ---------------------------------------------------------------------------------------

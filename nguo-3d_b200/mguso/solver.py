@@ -297,7 +297,10 @@ class ImplicitSolver:
         """Kernel names of the fused PCG in use, for the mixed-precision FP16-tile step."""
         rv, dv = self.pcg_kernels()
         rows = "k_fr_rows_sell<double>" if rv == 3 else f"k_fr_rows<double, {({0: 2, 1: 1, 2: 4}).get(rv, 2)}>"
-        dom = "k_fr_schwarz<double, __half>" if dv <= 0 else f"k_fr_schwarz3<double, __half, {(1, 2, 4)[dv - 1]}>"
+        if dv >= 4:
+            dom = f"k_fr_schwarz_tc<double, {4 if dv == 4 else 8}>"
+        else:
+            dom = "k_fr_schwarz<double, __half>" if dv <= 0 else f"k_fr_schwarz3<double, __half, {(1, 2, 4)[dv - 1]}>"
         return {"rows": rows, "domains": dom}
 
     def ccd(self, x, dx):

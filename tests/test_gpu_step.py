@@ -387,14 +387,15 @@ def test_self_intersection_scan_on_perturbed_drapes(ctx):
 @pytest.mark.parametrize("precision", ["fp32", "mixed"])
 def test_fused_kernel_variants_agree(ctx, precision):
     """Every variant of the fused PCG kernels the autotuner chooses between (rows kernel with
-    2, 1 or 4 lanes per block row, or over the sliced-ELL copy; Schwarz domains with one warp each or three warps each at
-    1, 2 or 4 domains per CTA) runs the same iteration: two batched steps agree with the
-    first variant's to the Newton tolerance."""
+    2, 1 or 4 lanes per block row, or over the sliced-ELL copy; Schwarz domains with one warp
+    each, three warps each at 1, 2 or 4 domains per CTA, or on the tensor cores at 4 or 8
+    domains per CTA) runs the same iteration: two batched steps agree with the first
+    variant's to the Newton tolerance."""
     from mguso import ImplicitBatch
 
     scs = graded_coarse(2)
     runs = []
-    for v in range(1, 17):
+    for v in range(1, 25):
         s2 = [dict(sc, params=dict(sc["params"], pcg_variant=v)) for sc in scs]
         b = ImplicitBatch(ctx, s2, precision)
         st = b.step(2)
