@@ -495,6 +495,8 @@ def run_batch(args, dist: Dist):
     ctx = mguso.Context(dist.local)
     stream = torch.cuda.ExternalStream(ctx.stream)
     scs = scenes.graded_sheaths()
+    if args.pcg_variant:
+        scs = [dict(sc, params=dict(sc["params"], pcg_variant=args.pcg_variant)) for sc in scs]
     ntri = [int(sc["shell_faces"].shape[0]) for sc in scs]
     clocks = ClockSampler(dist.local)
     clocks.start()
@@ -750,6 +752,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-check", action="store_true", help="skip the FP64-oracle error of the first timed step")
     ap.add_argument("--no-launch-count", action="store_true", help="skip the traced launch count (under ncu)")
+    ap.add_argument("--pcg-variant", type=int, default=0,
+                    help="fused PCG kernels (mguso_params.pcg_variant; 0 = the autotuner's choice), to profile "
+                         "one variant reproducibly")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

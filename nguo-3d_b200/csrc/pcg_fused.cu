@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(FR_THREADS) k_fr_rows(FusedArgs a, const float
 // (padding slots have zero values and the row's own column), then the row's contact blocks.
 // Same iteration and finish as k_fr_rows.
 template <class Acc>
-__global__ void __launch_bounds__(FR_THREADS) k_fr_rows_sell(FusedArgs a, const float* __restrict__ po,
+__global__ void __launch_bounds__(FR_THREADS, 4) k_fr_rows_sell(FusedArgs a, const float* __restrict__ po,
                                                              float* __restrict__ pn) {
   if (a.ctl->all_done) return;
   const uint32_t K = a.ninst;

@@ -172,7 +172,7 @@ __device__ __forceinline__ float tc_scale_exp(const float* v, int lane, float& s
   float mx = fmaxf(fmaxf(fabsf(v[lane]), fabsf(v[lane + 32])), fabsf(v[lane + 64]));
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-  if (!(mx > 0.f) || !isfinite(mx)) {
+  if (!(mx > 1e-30f) || !isfinite(mx)) {  // a (near) zero vector: z = 0 (and no 2^-e overflow)
     sc = 0.f;
     return 0.f;
   }

@@ -2368,36 +2368,88 @@ struct ImplicitSolver {
   }
 
   // has_self_intersection (implicit.rs:618-650) via a plain grid over edge/triangle boxes.
+  // positions_self_intersect (implicit.rs:618-643) over any_edge_triangle_pair
+  // (broadphase.rs:609-751): a grid of cell size max(char_len, mean edge length, mean
+  // triangle extent); pass A hashes the movable edges into the cells of their boxes padded by
+  // char_len and scans every triangle's padded cells, pass B hashes the movable triangles and
+  // scans the edges with no movable vertex. Pairs sharing a vertex are skipped; true at the
+  // first piercing pair.
   bool positions_self_intersect(const std::vector<V>& x) const {
-    if (edges.empty()) return false;
-    auto mov = movable_mask();
-    bool hit = false;
-    // candidate edges within `char_len` of a triangle: reuse the vertex-triangle grid over
-    // edge midpoints with a search radius covering half an edge plus char_len
-    R ml = mean_edge_len(x, edges);
-    std::vector<V> mids(edges.size());
-    std::vector<std::vector<uint32_t>> none(edges.size());
-    for (size_t i = 0; i < edges.size(); ++i) mids[i] = (x[edges[i][0]] + x[edges[i][1]]) * R(0.5);
-    std::vector<uint8_t> emov;
-    if (!mov.empty()) {
-      emov.resize(edges.size());
-      for (size_t i = 0; i < edges.size(); ++i) emov[i] = mov[edges[i][0]] || mov[edges[i][1]];
+    if (edges.empty() || collision_tris.empty()) return false;
+    const auto mov = movable_mask();
+    const R search = char_len;
+    const R cell = grid_cell(search, rmax(mean_edge_len(x, edges), mean_tri_extent(x, collision_tris)));
+    const R inv = R(1) / cell;
+    auto key = [&](R v) { return floor_i32((double)(v * inv)); };
+    const V pad(search, search, search);
+    auto edge_box = [&](const Edge& e, CellKey& lo, CellKey& hi) {
+      const V p = x[e[0]], q = x[e[1]];
+      const V l = p.vmin(q) - pad, h = p.vmax(q) + pad;
+      lo = CellKey{key(l.x), key(l.y), key(l.z)};
+      hi = CellKey{key(h.x), key(h.y), key(h.z)};
+    };
+    auto tri_box = [&](const Tri& t, CellKey& lo, CellKey& hi) {
+      const V a = x[t[0]], b = x[t[1]], c = x[t[2]];
+      const V l = a.vmin(b).vmin(c) - pad, h = a.vmax(b).vmax(c) + pad;
+      lo = CellKey{key(l.x), key(l.y), key(l.z)};
+      hi = CellKey{key(h.x), key(h.y), key(h.z)};
+    };
+    auto e_mov = [&](const Edge& e) { return mov.empty() || mov[e[0]] || mov[e[1]]; };
+    auto t_mov = [&](const Tri& t) { return mov.empty() || mov[t[0]] || mov[t[1]] || mov[t[2]]; };
+    auto pierces = [&](const Edge& e, const Tri& t) {
+      if (e[0] == t[0] || e[0] == t[1] || e[0] == t[2] || e[1] == t[0] || e[1] == t[1] || e[1] == t[2])
+        return false;  // shared vertex: adjacent
+      return edge_triangle_intersect(x[e[0]], x[e[1]], x[t[0]], x[t[1]], x[t[2]]);
+    };
+    // pass A: movable edges indexed, every triangle scanned
+    std::vector<std::pair<CellKey, uint32_t>> ins;
+    for (size_t ei = 0; ei < edges.size(); ++ei) {
+      if (!e_mov(edges[ei])) continue;
+      CellKey lo, hi;
+      edge_box(edges[ei], lo, hi);
+      for (int32_t cx = lo.x; cx <= hi.x; ++cx)
+        for (int32_t cy = lo.y; cy <= hi.y; ++cy)
+          for (int32_t cz = lo.z; cz <= hi.z; ++cz) ins.push_back({CellKey{cx, cy, cz}, (uint32_t)ei});
     }
-    R maxlen = 0;
-    for (auto& e : edges) maxlen = rmax(maxlen, (x[e[0]] - x[e[1]]).length());
-    (void)ml;
-    for_each_vertex_triangle_pair<R>(mids, collision_tris, R(0.5) * maxlen + char_len, none, {},
-                                     [&](uint32_t ei, uint32_t ti) {
-                                       if (hit) return;
-                                       const Edge& e = edges[ei];
-                                       const Tri& t = collision_tris[ti];
-                                       if (!emov.empty() && !emov[ei] && !(mov[t[0]] || mov[t[1]] || mov[t[2]])) return;
-                                       if (e[0] == t[0] || e[0] == t[1] || e[0] == t[2] || e[1] == t[0] ||
-                                           e[1] == t[1] || e[1] == t[2])
-                                         return;
-                                       if (edge_triangle_intersect(x[e[0]], x[e[1]], x[t[0]], x[t[1]], x[t[2]]))
-                                         hit = true;
-                                     });
+    CellGrid grid;
+    grid.build(ins);
+    bool hit = false;
+    for (size_t ti = 0; ti < collision_tris.size() && !hit; ++ti) {
+      const Tri& t = collision_tris[ti];
+      CellKey lo, hi;
+      tri_box(t, lo, hi);
+      for (int32_t cx = lo.x; cx <= hi.x && !hit; ++cx)
+        for (int32_t cy = lo.y; cy <= hi.y && !hit; ++cy)
+          for (int32_t cz = lo.z; cz <= hi.z && !hit; ++cz)
+            grid.each(CellKey{cx, cy, cz}, [&](uint32_t ei) {
+              if (!hit && pierces(edges[ei], t)) hit = true;
+            });
+    }
+    if (hit || mov.empty()) return hit;
+    // pass B: movable triangles indexed, the edges with no movable vertex scanned
+    ins.clear();
+    for (size_t ti = 0; ti < collision_tris.size(); ++ti) {
+      if (!t_mov(collision_tris[ti])) continue;
+      CellKey lo, hi;
+      tri_box(collision_tris[ti], lo, hi);
+      for (int32_t cx = lo.x; cx <= hi.x; ++cx)
+        for (int32_t cy = lo.y; cy <= hi.y; ++cy)
+          for (int32_t cz = lo.z; cz <= hi.z; ++cz) ins.push_back({CellKey{cx, cy, cz}, (uint32_t)ti});
+    }
+    CellGrid tgrid;
+    tgrid.build(ins);
+    for (size_t ei = 0; ei < edges.size() && !hit; ++ei) {
+      const Edge& e = edges[ei];
+      if (e_mov(e)) continue;
+      CellKey lo, hi;
+      edge_box(e, lo, hi);
+      for (int32_t cx = lo.x; cx <= hi.x && !hit; ++cx)
+        for (int32_t cy = lo.y; cy <= hi.y && !hit; ++cy)
+          for (int32_t cz = lo.z; cz <= hi.z && !hit; ++cz)
+            tgrid.each(CellKey{cx, cy, cz}, [&](uint32_t ti) {
+              if (!hit && pierces(e, collision_tris[ti])) hit = true;
+            });
+    }
     return hit;
   }
 

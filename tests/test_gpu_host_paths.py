@@ -42,7 +42,10 @@ class Recording(ImplicitSolver):
 def _check_against_oracle(sc, rec):
     res = oracle_steps_from(sc, rec.pre)
     for k, ((p0, _), pg, sg, (po, so)) in enumerate(zip(rec.pre, rec.post, rec.stats, res)):
-        rel = np.abs(pg - po).max() / (np.abs(po - p0).max() + 1e-12)
+        # relative to the step's displacement, floored at the Newton loop's own stopping step
+        # (1e-7 m): a step the CCD clamps to nothing (the sample garment starts with its
+        # panels touching, so its first step barely moves) is compared absolutely
+        rel = np.abs(pg - po).max() / max(np.abs(po - p0).max(), 1e-7)
         print(k, sg["newton_iters"], so["newton_iters"], rel)
         assert sg["status"] == 0 and abs(sg["newton_iters"] - so["newton_iters"]) <= 1, (k, sg, so)
         assert rel < 1e-3, (k, rel)
