@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <cstdlib>
 #include <vector>
 
 #include "../../include/mguso_cuda.h"
@@ -114,6 +115,18 @@ inline float u2f_host(unsigned int u) {
 }
 
 int device_sm_count();
+
+// MGUSO_PLAIN_LAUNCHES=1: the step's device-driven loops (the PCG solve and the CCD schedule,
+// conditional-while CUDA graphs) run as plain kernel launches driven by the host instead, with
+// the same kernels and iterations; for profilers, which cannot see the kernels of graphs with
+// conditional nodes.
+inline bool plain_launches() {
+  static const bool on = [] {
+    const char* e = std::getenv("MGUSO_PLAIN_LAUNCHES");
+    return e && e[0] && e[0] != '0';
+  }();
+  return on;
+}
 
 // ---------------------------------------------------------------------------------------
 // PTX wrappers: mbarrier + 1-D bulk (TMA) global -> shared copies.

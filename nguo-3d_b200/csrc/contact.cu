@@ -745,7 +745,7 @@ __global__ void k_ccd_plan(CcdState* __restrict__ cs, unsigned int* __restrict__
 // Settles every instance whose launch decided it, widens the others, and sets the loop's
 // condition: go on while an instance is undecided, for at most 64 launches.
 __global__ void k_ccd_settle(CcdState* __restrict__ cs, const unsigned int* __restrict__ acc,
-                             cudaGraphConditionalHandle h) {
+                             cudaGraphConditionalHandle h, int cond) {
   __shared__ uint32_t settled_mask;
   const uint32_t k = threadIdx.x;
   if (k == 0) settled_mask = 0;
@@ -772,7 +772,7 @@ __global__ void k_ccd_settle(CcdState* __restrict__ cs, const unsigned int* __re
   if (k == 0) {
     cs->todo &= ~settled_mask;
     cs->launch += 1;
-    cudaGraphSetConditional(h, (cs->todo && cs->launch < 64) ? 1u : 0u);
+    if (cond) cudaGraphSetConditional(h, (cs->todo && cs->launch < 64) ? 1u : 0u);
   }
 }
 
@@ -781,12 +781,37 @@ __global__ void k_ccd_clamp(CcdState* __restrict__ cs) {
   if (k < PCG_MAX_INST) cs->t[k] = fminf(fmaxf(cs->t[k], 0.f), 1.f);
 }
 
+// One launch of the self-contact schedule: plan, then the two traversals (settle follows).
+static void ccd_body(Scene& s, const BvhSet& tv, const BvhSet& ev, CcdState* cs) {
+  cudaStream_t st = s.st;
+  const float dhat = s.p.contact_dhat;
+  const float fixed = dhat;  // max_edge_gap() + 2 * max_edge_offset() for face edges
+  const uint32_t iters = std::max<uint32_t>(s.p.ccd_max_iter, 1);
+  const CcdPass* cpp = &cs->cp;
+  k_ccd_plan<<<1, PCG_MAX_INST * CCD_CHUNK, 0, st>>>(cs, s.ccd_acc.p, fixed);
+  if (s.mixed) {
+    k_ccd_vt<double><<<ceil_div(s.nv, 128), 128, 0, st>>>(
+        tv, cpp, s.vinst.p, s.x.p, s.dx.p, s.tris.p, s.collider_tri.p, s.inv_mass.p, s.ex_ptr.p, s.ex_list.p,
+        s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.red.p, s.ccd_acc.p, s.status.p);
+    if (s.n_edge)
+      k_ccd_ee<double><<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, cpp, s.vinst.p, s.x.p, s.dx.p, s.edges.p,
+                                                               s.inv_mass.p, s.n_edge, iters, s.red.p, s.ccd_acc.p,
+                                                               s.status.p);
+  } else {
+    k_ccd_vt<float><<<ceil_div(s.nv, 128), 128, 0, st>>>(
+        tv, cpp, s.vinst.p, s.x.p, s.dx.p, s.tris.p, s.collider_tri.p, s.inv_mass.p, s.ex_ptr.p, s.ex_list.p,
+        s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.red.p, s.ccd_acc.p, s.status.p);
+    if (s.n_edge)
+      k_ccd_ee<float><<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, cpp, s.vinst.p, s.x.p, s.dx.p, s.edges.p,
+                                                              s.inv_mass.p, s.n_edge, iters, s.red.p, s.ccd_acc.p,
+                                                              s.status.p);
+  }
+}
+
 // The self-contact schedule's graph: one conditional while node around plan, the two
 // traversals and settle. Rebuilt when a by-value argument changes.
 static int ccd_graph(Scene& s, const BvhSet& tv, const BvhSet& ev, CcdState* cs) {
   cudaStream_t st = s.st;
-  const float dhat = s.p.contact_dhat;
-  const float fixed = dhat;  // max_edge_gap() + 2 * max_edge_offset() for face edges
   const uint32_t iters = std::max<uint32_t>(s.p.ccd_max_iter, 1);
   std::vector<unsigned char> key(2 * sizeof(BvhSet) + 8 * sizeof(void*) + 16);
   unsigned char* q = key.data();
@@ -823,26 +848,8 @@ static int ccd_graph(Scene& s, const BvhSet& tv, const BvhSet& ev, CcdState* cs)
     cudaGraphDestroy(g);
     MG_CUDA(e);
   }
-  const CcdPass* cpp = &cs->cp;
-  k_ccd_plan<<<1, PCG_MAX_INST * CCD_CHUNK, 0, st>>>(cs, s.ccd_acc.p, fixed);
-  if (s.mixed) {
-    k_ccd_vt<double><<<ceil_div(s.nv, 128), 128, 0, st>>>(
-        tv, cpp, s.vinst.p, s.x.p, s.dx.p, s.tris.p, s.collider_tri.p, s.inv_mass.p, s.ex_ptr.p, s.ex_list.p,
-        s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.red.p, s.ccd_acc.p, s.status.p);
-    if (s.n_edge)
-      k_ccd_ee<double><<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, cpp, s.vinst.p, s.x.p, s.dx.p, s.edges.p,
-                                                               s.inv_mass.p, s.n_edge, iters, s.red.p, s.ccd_acc.p,
-                                                               s.status.p);
-  } else {
-    k_ccd_vt<float><<<ceil_div(s.nv, 128), 128, 0, st>>>(
-        tv, cpp, s.vinst.p, s.x.p, s.dx.p, s.tris.p, s.collider_tri.p, s.inv_mass.p, s.ex_ptr.p, s.ex_list.p,
-        s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.red.p, s.ccd_acc.p, s.status.p);
-    if (s.n_edge)
-      k_ccd_ee<float><<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, cpp, s.vinst.p, s.x.p, s.dx.p, s.edges.p,
-                                                              s.inv_mass.p, s.n_edge, iters, s.red.p, s.ccd_acc.p,
-                                                              s.status.p);
-  }
-  k_ccd_settle<<<1, 32, 0, st>>>(cs, s.ccd_acc.p, cond);
+  ccd_body(s, tv, ev, cs);
+  k_ccd_settle<<<1, 32, 0, st>>>(cs, s.ccd_acc.p, cond, 1);
   const cudaError_t le = cudaGetLastError();
   cudaGraph_t body = nullptr;
   e = cudaStreamEndCapture(st, &body);
@@ -901,8 +908,21 @@ int ccd_step(Scene& s, uint32_t active) {
       MG_TRY(lbvh_refit_disp(s.edge_bvh[k].get(), s.dx.p, s.edge_tris.p + 3 * (size_t)s.inst_edge[k], st));
     }
     const BvhSet tv = view_set(s.tri_bvh, s.inst_tri), ev = view_set(s.edge_bvh, s.inst_edge);
-    MG_TRY(ccd_graph(s, tv, ev, cs));
-    MG_CUDA(cudaGraphLaunch(s.ccd_exec, st));
+    if (plain_launches()) {
+      // the same launches driven by the host (for profilers)
+      for (int launch = 0; launch < 64; ++launch) {
+        ccd_body(s, tv, ev, cs);
+        k_ccd_settle<<<1, 32, 0, st>>>(cs, s.ccd_acc.p, cudaGraphConditionalHandle{}, 0);
+        MG_CUDA(cudaGetLastError());
+        uint32_t todo = 0;
+        MG_CUDA(cudaMemcpyAsync(&todo, &cs->todo, 4, cudaMemcpyDeviceToHost, st));
+        MG_CUDA(cudaStreamSynchronize(st));
+        if (!todo) break;
+      }
+    } else {
+      MG_TRY(ccd_graph(s, tv, ev, cs));
+      MG_CUDA(cudaGraphLaunch(s.ccd_exec, st));
+    }
   }
   k_ccd_clamp<<<1, 32, 0, st>>>(cs);
   MG_CUDA(cudaGetLastError());

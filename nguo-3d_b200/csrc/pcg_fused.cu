@@ -638,8 +638,14 @@ __global__ void __launch_bounds__(96 * DOMS) k_fr_schwarz3(FusedArgs a, const fl
       const TS* w = buf + t * TILE_FLOATS;
       const float* rj = rd + 32 * f3_tile_j(t);
       AA y = 0;
-#pragma unroll 8
-      for (int c = 0; c < 32; ++c) y += (AA)tile_ld(w, tile_off<TS>(lane, c)) * (AA)rj[c];
+#pragma unroll 2
+      for (int c0 = 0; c0 < 32; c0 += 4) {  // r_j as broadcast float4 loads, the sum in column order
+        const float4 r4 = *reinterpret_cast<const float4*>(rj + c0);
+        y += (AA)tile_ld(w, tile_off<TS>(lane, c0)) * (AA)r4.x;
+        y += (AA)tile_ld(w, tile_off<TS>(lane, c0 + 1)) * (AA)r4.y;
+        y += (AA)tile_ld(w, tile_off<TS>(lane, c0 + 2)) * (AA)r4.z;
+        y += (AA)tile_ld(w, tile_off<TS>(lane, c0 + 3)) * (AA)r4.w;
+      }
       part[(2 * q + slot) * 32 + lane] = y;
     }
   }
@@ -663,8 +669,32 @@ __global__ void __launch_bounds__(96 * DOMS) k_fr_schwarz3(FusedArgs a, const fl
       const TS* w = buf + t * TILE_FLOATS;
       const AA* yi = yd + 32 * f3_tile_i(t);
       AA z = 0;
+      if constexpr (sizeof(TS) == 2) {
+        // FP16 tiles: column `lane` as four 16-byte chunks (rows 8 kk .. 8 kk + 7 each), read
+        // in row order, their y entries as broadcast float4 loads; the sum runs over r in order
+        const uint4* col = reinterpret_cast<const uint4*>(w + 32 * lane);
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+          const uint4 v = col[kk ^ ((lane >> 1) & 3)];
+          const float4 ya = *reinterpret_cast<const float4*>(yi + 8 * kk);
+          const float4 yb = *reinterpret_cast<const float4*>(yi + 8 * kk + 4);
+          float2 f = __half22float2(*reinterpret_cast<const __half2*>(&v.x));
+          z += f.x * ya.x;
+          z += f.y * ya.y;
+          f = __half22float2(*reinterpret_cast<const __half2*>(&v.y));
+          z += f.x * ya.z;
+          z += f.y * ya.w;
+          f = __half22float2(*reinterpret_cast<const __half2*>(&v.z));
+          z += f.x * yb.x;
+          z += f.y * yb.y;
+          f = __half22float2(*reinterpret_cast<const __half2*>(&v.w));
+          z += f.x * yb.z;
+          z += f.y * yb.w;
+        }
+      } else {
 #pragma unroll 8
-      for (int r = 0; r < 32; ++r) z += (AA)tile_ld(w, tile_off<TS>(r, lane)) * yi[r];
+        for (int r = 0; r < 32; ++r) z += (AA)tile_ld(w, tile_off<TS>(r, lane)) * yi[r];
+      }
       part[(2 * q + slot) * 32 + lane] = z;
     }
   }
@@ -922,7 +952,7 @@ static int fused_prepare(Scene& s, const uint32_t* h_inst_row, uint32_t K, uint3
   }
   L.grid_rows = s.fr_grid_rows;
   L.grid_dom = s.fr_grid_dom;
-  MG_TRY(w.p2.reserve(w.n));
+  MG_TRY(w.p2.reserve(4 * ((size_t)w.n / 3 + 1)));  // the second direction, 4 floats per vertex
   MG_TRY(s.fr_inst.reserve(PCG_MAX_INST));
   MG_TRY(s.fr_ctl.reserve(1));
   MG_TRY(s.fr_part.reserve(2ull * std::max(L.grid_rows, L.grid_dom)));
@@ -1018,6 +1048,26 @@ int pcg_fused(Scene& s, const uint32_t* h_inst_row, uint32_t K, uint32_t active,
   // iterations and then k_fr_continue, which decides on the device whether to go on, so the
   // host neither waits nor reads anything until the solve has finished.
   const uint32_t max_rounds = ceil_div(s.p.cg_max_iter + FUSED_CHECK, FUSED_CHECK);
+  if (plain_launches()) {
+    // every kernel launched on its own and the loop driven by the host (profilers cannot see
+    // the kernels inside conditional graphs): the same iterations and the same bound
+    FusedCtl h{};
+    for (uint32_t r = 0; r < max_rounds; ++r) {
+      for (uint32_t i = 0; i < FUSED_CHECK; ++i) {
+        const float* po = (i & 1) ? p1 : p0;
+        float* pn = (i & 1) ? p0 : p1;
+        MG_TRY(launch_rows(s, L, a, po, pn));
+        MG_TRY(launch_dom(s, L, a, pn, pn, 0));
+      }
+      MG_CUDA(cudaMemcpyAsync(&h, s.fr_ctl.p, sizeof(FusedCtl), cudaMemcpyDeviceToHost, st));
+      MG_CUDA(cudaStreamSynchronize(st));
+      if (h.all_done) break;
+    }
+    MG_TRY(s.fr_out.reserve(PCG_MAX_INST));
+    MG_CUDA(cudaMemcpyAsync(s.fr_out.p, s.fr_inst.p, sizeof(FusedInst) * K, cudaMemcpyDeviceToHost, st));
+    if (!out) return MGUSO_OK;
+    return pcg_fused_results(s, K, out);
+  }
   if (gk != s.fr_graph_key || !s.fr_exec) {
     if (s.fr_exec) cudaGraphExecDestroy(s.fr_exec);
     s.fr_exec = nullptr;
