@@ -472,6 +472,11 @@ int mguso_scene_self_intersections(mguso_scene* s, const float* x, uint32_t* cou
    Parity and diagnostics entry; the reference counterpart is the triplet assembly of
    ImplicitSolver::step (core-engine/crates/engine-core/src/implicit.rs:2280-3155). */
 int mguso_scene_assemble(mguso_scene* scene, const float* x, const float* x_tilde, uint32_t out3[3]);
+/* The exact Hessian the adjoint's backward pass solves with, at x (no eigenvalue clamps; the
+ * hinges' and barriers' second-derivative terms; each contact stiffness recorded from the
+ * projected system at x, its mass part differentiated in the gap), assembled like
+ * mguso_scene_assemble into the system mguso_scene_system downloads. */
+int mguso_scene_assemble_exact(mguso_scene* scene, const float* x, const float* x_tilde, uint32_t out3[3]);
 
 /* The step fraction the CCD filter allows for search direction dx (f32[3 nv]) from positions
    x (f32[3 nv]; the scene's positions are left at x): t_out f32[instances] (one per instance

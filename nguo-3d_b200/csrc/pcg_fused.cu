@@ -30,6 +30,7 @@ constexpr int FR_THREADS = 256;
 constexpr int FD_WARPS = 4;        // Schwarz, one warp per domain: warps (domains) per CTA
 constexpr int FD_THREADS = 256;    // block Jacobi: vertices per CTA
 constexpr uint32_t FUSED_CHECK = 16;
+constexpr int FR_BATCH = 4;  // blocks per lane whose loads the rows kernel issues together
 
 // z and the search directions are stored with 4 floats per vertex (xyz, w unused): a
 // neighbour's z and p_old are two 16-byte loads in the SpMV gather. x, r, b and Ap keep 3.
@@ -138,8 +139,7 @@ __global__ void __launch_bounds__(FR_THREADS) k_fr_rows(FusedArgs a, const float
   if (!done) {
     for (uint32_t row = row0 + (lc * FR_THREADS + tid) / FR_LPR; row < row1; row += nc * FR_THREADS / FR_LPR) {
       Acc y0 = 0, y1 = 0, y2 = 0;
-      auto block = [&](const float* __restrict__ m9, uint32_t c) {
-        const float4 zc = ld_v4(a.z, c), pc4 = ld_v4(po, c);
+      auto block_x = [&](const float* __restrict__ m9, const float4& zc, const float4& pc4) {
         const Acc x0 = (Acc)fmaf(be, pc4.x, zc.x);
         const Acc x1 = (Acc)fmaf(be, pc4.y, zc.y);
         const Acc x2 = (Acc)fmaf(be, pc4.z, zc.z);
@@ -153,9 +153,28 @@ __global__ void __launch_bounds__(FR_THREADS) k_fr_rows(FusedArgs a, const float
         y2 = fr_fma((Acc)__ldg(m9 + 7), x1, y2);
         y2 = fr_fma((Acc)__ldg(m9 + 8), x2, y2);
       };
+      auto block = [&](const float* __restrict__ m9, uint32_t c) { block_x(m9, ld_v4(a.z, c), ld_v4(po, c)); };
       const uint32_t ke = __ldg(a.rp + row + 1);
-#pragma unroll 4
-      for (uint32_t kk = __ldg(a.rp + row) + sub; kk < ke; kk += FR_LPR) block(a.val + 9 * (size_t)kk, __ldg(a.col + kk));
+      // the row's blocks in batches of FR_BATCH per lane: every column, then every gather,
+      // issued before the first product (the same blocks in the same order as one at a time)
+      for (uint32_t kk = __ldg(a.rp + row) + sub; kk < ke; kk += FR_BATCH * FR_LPR) {
+        uint32_t cc[FR_BATCH];
+        bool ok[FR_BATCH];
+#pragma unroll
+        for (int u = 0; u < FR_BATCH; ++u) {
+          ok[u] = kk + u * FR_LPR < ke;
+          cc[u] = ok[u] ? __ldg(a.col + kk + u * FR_LPR) : row;
+        }
+        float4 zz[FR_BATCH], pp[FR_BATCH];
+#pragma unroll
+        for (int u = 0; u < FR_BATCH; ++u) {
+          zz[u] = ld_v4(a.z, cc[u]);
+          pp[u] = ld_v4(po, cc[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < FR_BATCH; ++u)
+          if (ok[u]) block_x(a.val + 9 * (size_t)(kk + u * FR_LPR), zz[u], pp[u]);
+      }
       const uint32_t ce = __ldg(a.crp + row + 1);
       for (uint32_t kk = __ldg(a.crp + row) + sub; kk < ce; kk += FR_LPR) block(a.cval + 9 * (size_t)kk, __ldg(a.ccol + kk));
 #pragma unroll

@@ -1165,6 +1165,44 @@ extern "C" int mguso_scene_assemble(mguso_scene* sc, const float* x, const float
   return MGUSO_OK;
 }
 
+// The adjoint's exact Hessian at x (inertia target x_tilde, x when null), as the backward
+// pass of mguso_adjoint_backward assembles it: the step's projected system first, for the
+// contact stiffnesses it records, then the exact one (no eigenvalue clamps, second-derivative
+// terms of hinges and barriers, the contact stiffnesses' gap dependence) into the same Ps + C
+// that mguso_scene_system downloads; the right-hand side is the negative gradient.
+extern "C" int mguso_scene_assemble_exact(mguso_scene* sc, const float* x, const float* x_tilde, uint32_t* out3) {
+  MG_CHECK_ARG(sc && x && out3, "bad argument");
+  Scene& s = sc->s;
+  cudaStream_t st = s.st;
+  const size_t bytes = 12 * (size_t)s.nv;
+  MG_CUDA(cudaMemcpyAsync(s.x.p, x, bytes, cudaMemcpyHostToDevice, st));
+  MG_CUDA(cudaMemcpyAsync(s.xt.p, x_tilde ? x_tilde : x, bytes, cudaMemcpyHostToDevice, st));
+  uint32_t nst = 0;
+  if (s.p.self_collision) {
+    MG_TRY(build_bvhs(s, s.x.p));
+    MG_TRY(collect_stencils(s, &nst));
+  }
+  s.hess_mode = 0;
+  MG_TRY(assemble_elastic(s));
+  MG_TRY(assemble_colliders(s));
+  MG_TRY(contact_stiffness(s, nst));
+  s.hess_mode = 2;
+  int rc = assemble_elastic(s);
+  if (rc == MGUSO_OK) rc = assemble_colliders(s);
+  if (rc == MGUSO_OK) rc = assemble_contacts(s, nst);
+  s.hess_mode = 0;
+  MG_TRY(rc);
+  MG_TRY(finish_rhs(s));
+  uint32_t nc = 0;
+  MG_CUDA(cudaMemcpyAsync(&nc, s.c_count.p, 4, cudaMemcpyDeviceToHost, st));
+  MG_CUDA(cudaStreamSynchronize(st));
+  out3[0] = s.Ps.nnz;
+  out3[1] = nc;
+  out3[2] = nst;
+  s.last_nst = nst;
+  return MGUSO_OK;
+}
+
 // The contact stencils of the last mguso_scene_assemble, in assembly order: participants
 // u32[4 n], kind u32[n] (0 vertex-triangle, 1 edge-edge), gap f64[n]. Writes min(n, cap).
 extern "C" int mguso_scene_stencils(mguso_scene* sc, uint32_t cap, uint32_t* idx4, uint32_t* kind, double* d,

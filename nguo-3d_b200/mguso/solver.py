@@ -68,6 +68,7 @@ def _sigs(lib):
         ("mguso_scene_info", i32, [vp, vp]),
         ("mguso_scene_spmv_time", i32, [vp, i32, P(C.c_float), P(C.c_double)]),
         ("mguso_scene_assemble", i32, [vp, vp, vp, vp]),
+        ("mguso_scene_assemble_exact", i32, [vp, vp, vp, vp]),
         ("mguso_scene_ccd", i32, [vp, vp, vp, vp, vp]),
         ("mguso_scene_profile", i32, [vp, i32, vp, vp]),
         ("mguso_scene_profile_pcg", i32, [vp, i32, vp, vp]),
@@ -314,15 +315,17 @@ class ImplicitSolver:
         check(self.lib.mguso_scene_ccd(self.h, ptr(xx), ptr(dd), ptr(t), ptr(caps)))
         return t, caps
 
-    def assemble(self, x, x_tilde=None) -> dict:
+    def assemble(self, x, x_tilde=None, exact: bool = False) -> dict:
         """One Newton-system assembly at positions ``x`` (inertia target ``x_tilde``, ``x``
         when None), downloaded as the fixed-pattern blocks ``ps`` and the contact-only
         blocks ``c`` (each ``(row_ptr, col, val[nnz, 3, 3])``) plus ``rhs``; the scene's
-        positions are left at ``x``."""
+        positions are left at ``x``. ``exact``: the adjoint's exact Hessian instead of the
+        step's projected one (mguso_scene_assemble_exact)."""
         xx = np.ascontiguousarray(x, np.float32)
         xt = None if x_tilde is None else np.ascontiguousarray(x_tilde, np.float32)
         n3 = np.zeros(3, np.uint32)
-        check(self.lib.mguso_scene_assemble(self.h, ptr(xx), ptr(xt) if xt is not None else None, ptr(n3)))
+        fn = self.lib.mguso_scene_assemble_exact if exact else self.lib.mguso_scene_assemble
+        check(fn(self.h, ptr(xx), ptr(xt) if xt is not None else None, ptr(n3)))
         nps, nc, nst = (int(v) for v in n3)
         ps_rp = np.empty(self.nv + 1, np.uint32)
         ps_col = np.empty(nps, np.uint32)

@@ -874,6 +874,11 @@ void oracle_stitch(const double* x18, const double* w6, double l0, double lcap, 
 // (weft, warp) along (u, v), stitch stiffness = base * seam_q.
 // H is n3 x n3 row-major (pinned rows and columns 0), dG is (3P + S) x n3. Returns the
 // number of stencils, or -1 for a float solver.
+// Diagnostics of the reference adjoint: 0 freezes each contact stiffness whole (no 1/d^2 mass
+// part), to measure how much that part of the exact Hessian moves a gradient.
+static int g_adjoint_km = 1;
+void oracle_adjoint_set_km(int on) { g_adjoint_km = on; }
+
 int oracle_adjoint_system(void* h, uint32_t npanel, uint32_t nseam, const float* uv, const uint8_t* panel,
                           const uint8_t* seam, const double* stitch_k0, const double* theta, const double* xn,
                           const double* vn, const double* xn1, double eps, double* H, double* dG) {
@@ -926,8 +931,8 @@ int oracle_adjoint_system(void* h, uint32_t npanel, uint32_t nseam, const float*
     for (int a = 0; a < 4; ++a) f.idx[a] = sts[i].idx[a];
     f.kind = kinds[i];
     f.ghat = sts[i].ghat;
-    f.k_el = s.contact_rec[i][0] - s.contact_rec[i][1];
-    f.km = s.contact_rec[i][1];
+    f.km = g_adjoint_km ? s.contact_rec[i][1] : 0.0;
+    f.k_el = s.contact_rec[i][0] - f.km;
     f.d0 = sts[i].d;
   }
   s.frozen = &fr;

@@ -42,13 +42,15 @@ class Recording(ImplicitSolver):
 def _check_against_oracle(sc, rec):
     res = oracle_steps_from(sc, rec.pre)
     for k, ((p0, _), pg, sg, (po, so)) in enumerate(zip(rec.pre, rec.post, rec.stats, res)):
-        # relative to the step's displacement, floored at the Newton loop's own stopping step
-        # (1e-7 m): a step the CCD clamps to nothing (the sample garment starts with its
-        # panels touching, so its first step barely moves) is compared absolutely
-        rel = np.abs(pg - po).max() / max(np.abs(po - p0).max(), 1e-7)
-        print(k, sg["newton_iters"], so["newton_iters"], rel)
+        disp = np.abs(po - p0).max()
+        print(k, sg["newton_iters"], so["newton_iters"], disp, np.abs(pg - po).max())
         assert sg["status"] == 0 and abs(sg["newton_iters"] - so["newton_iters"]) <= 1, (k, sg, so)
-        assert rel < 1e-3, (k, rel)
+        if so["t_min"] < 1e-6:
+            # the CCD clamps the step to nothing (the sample garment starts with its panels
+            # touching): both sides stay put, to within a micrometre
+            assert disp < 1e-6 and np.abs(pg - p0).max() < 1e-6, (k, disp, np.abs(pg - p0).max())
+        else:
+            assert np.abs(pg - po).max() < 1e-3 * disp, (k, np.abs(pg - po).max() / disp)
 
 
 def test_bridge_drapes_a_sewn_garment_on_the_cuda_step(ctx):
