@@ -532,7 +532,10 @@ def run_batch(args, dist: Dist):
     prof = b.profile(100)
     dom = max(fused, key=lambda k: fused[k][0])
     us, nbytes = fused[dom]
-    kname = b.pcg_kernel_names()[dom]
+    knames = b.pcg_kernel_names()
+    kname = knames[dom]
+    rv_, dv_ = b.pcg_kernels()
+    pvar = 6 * rv_ + dv_ + 1  # the mguso_params.pcg_variant that fixes these kernels
     traffic, tsrc = traffic_from_profiles(kname)
     # the window's representative step: the one whose mean Newton count (over the sizes) is
     # the median of the window's; the CPU baseline and the FP64 error are taken there
@@ -585,8 +588,9 @@ def run_batch(args, dist: Dist):
             "traffic_source": tsrc, "peak_kind": f"{peak_kind} (burst copy)",
             "kernel": kname + " (fused PCG, timed inside a solve of the last Newton system)",
             "us_per_launch": round(us, 2), "bytes_per_launch": int(nbytes),
-            "fused": {k: {"us": round(v[0], 2), "bytes": int(v[1]), "GB/s": round(v[1] / (v[0] * 1e-6) / 1e9, 1)}
-                      for k, v in fused.items()},
+            "fused": {k: {"kernel": knames[k], "us": round(v[0], 2), "bytes": int(v[1]),
+                          "GB/s": round(v[1] / (v[0] * 1e-6) / 1e9, 1)} for k, v in fused.items()},
+            "pcg_variant": int(pvar),
             "per_kernel_alone": {k: {"us": round(v[0], 2), "bytes": int(v[1]),
                                      "GB/s": round(v[1] / (v[0] * 1e-6) / 1e9, 1)} for k, v in prof.items()},
         },

@@ -875,7 +875,9 @@ __global__ void k_contact_exact(const Stencil* __restrict__ sts, uint32_t nst, c
       for (int j = 0; j < 12; ++j) H[12 * i + j] = coef * S.g[i] * S.g[j];
     V3<double> p[4];
     for (int a = 0; a < 4; ++a) p[a] = ld3<double>(x, S.idx[a]);
-    const double eps = fmax(1e-4 * fabs(d), 1e-9);
+    // a small step: the gap gradient of nearly parallel edges (a seam's two sides) changes
+    // region within 1e-4 |d|, and a difference across that switch is no derivative
+    const double eps = fmax(1e-6 * fabs(d), 1e-12);
     const bool inside = d < 0;
     for (int i = 0; i < 12; ++i) {
       double gp[12], gm[12];

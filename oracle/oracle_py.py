@@ -743,10 +743,14 @@ def membrane_materials(w, wu, wv, clamp=True):
     return m9.reshape(3, 3), m36.reshape(4, 3, 3)
 
 
-def adjoint_system(o: "OracleSolver", scene: dict, theta, xn, vn, xn1, npanel=2, nseam=2, eps=1e-7):
+def adjoint_system(o: "OracleSolver", scene: dict, theta, xn, vn, xn1, npanel=2, nseam=2, eps=3e-9):
     """One step's adjoint system in FP64 (oracle_adjoint_system): H = dG/dx (n3 x n3) and
     dG/dtheta ((3 npanel + nseam) x n3) of the step's equilibrium residual at x_{n+1}, with
-    the contact set and the stiffnesses' elastic parts of x_{n+1} held fixed; the stencil count."""
+    the contact set and the stiffnesses' elastic parts of x_{n+1} held fixed; the stencil count.
+    eps is the central-difference step of H in metres: at 1e-7 the seam's contact stencils
+    (edges 1 mm apart, nearly parallel) put differences across region switches of the gap
+    into H; from 1e-8 down H is symmetric to 1e-4 and stops changing (3e-9 and 1e-9 agree to
+    1e-4 of its entries of ~1e3)."""
     n3 = 3 * o.nv
     npar = 3 * npanel + nseam
     uv = np.ascontiguousarray(scene["shell_uv"], np.float32)
@@ -764,7 +768,7 @@ def adjoint_system(o: "OracleSolver", scene: dict, theta, xn, vn, xn1, npanel=2,
     return H, dG, nst
 
 
-def fp64_adjoint(scene: dict, theta, xs, vs, dl_dx, npanel=2, nseam=2, eps=1e-7):
+def fp64_adjoint(scene: dict, theta, xs, vs, dl_dx, npanel=2, nseam=2, eps=3e-9):
     """dL/dtheta of an N-step drape in FP64 on the CPU, along the given trajectory
     (xs, vs: (N + 1, nv, 3), the states the GPU forward pass went through): backwards through
     every step, w = H^-1 (a_x + a_v / h) by a dense LU of the free block of the
