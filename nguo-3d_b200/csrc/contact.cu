@@ -93,14 +93,46 @@ __device__ __forceinline__ void edge_box(const float* x, uint32_t a, uint32_t b,
   hi = make_float4(h[0], h[1], h[2], 0.f);
 }
 
-int build_bvhs(Scene& s, const float* x) {
-  for (uint32_t k = 0; k < s.ninst; ++k) {
-    const uint32_t t0 = s.inst_tri[k], e0 = s.inst_edge[k];
-    MG_TRY(lbvh_build(s.tri_bvh[k].get(), x, s.nv, s.tris.p + 3 * (size_t)t0, s.inst_tri[k + 1] - t0, 30, s.st));
-    MG_TRY(lbvh_build(s.edge_bvh[k].get(), x, s.nv, s.edge_tris.p + 3 * (size_t)e0, s.inst_edge[k + 1] - e0, 30,
-                      s.st));
+// Side streams: the work enqueued on them after aux_fork runs after everything on s.st so
+// far, and s.st's work after aux_join runs after all of theirs.
+static constexpr int N_AUX = 4;
+static int aux_fork(Scene& s) {
+  if (s.aux.empty()) {
+    s.aux.resize(N_AUX);
+    s.aux_ev.resize(N_AUX);
+    for (int i = 0; i < N_AUX; ++i) {
+      MG_CUDA(cudaStreamCreateWithFlags(&s.aux[i], cudaStreamNonBlocking));
+      MG_CUDA(cudaEventCreateWithFlags(&s.aux_ev[i], cudaEventDisableTiming));
+    }
+    MG_CUDA(cudaEventCreateWithFlags(&s.fork_ev, cudaEventDisableTiming));
+  }
+  MG_CUDA(cudaEventRecord(s.fork_ev, s.st));
+  for (int i = 0; i < N_AUX; ++i) MG_CUDA(cudaStreamWaitEvent(s.aux[i], s.fork_ev, 0));
+  return MGUSO_OK;
+}
+static int aux_join(Scene& s) {
+  for (int i = 0; i < N_AUX; ++i) {
+    MG_CUDA(cudaEventRecord(s.aux_ev[i], s.aux[i]));
+    MG_CUDA(cudaStreamWaitEvent(s.st, s.aux_ev[i], 0));
   }
   return MGUSO_OK;
+}
+
+// The instances' triangle and edge LBVHs at x, built concurrently on the side streams (each
+// tree has its own scratch).
+int build_bvhs(Scene& s, const float* x) {
+  MG_TRY(aux_fork(s));
+  int rc = MGUSO_OK;
+  for (uint32_t k = 0; k < s.ninst && rc == MGUSO_OK; ++k) {
+    const uint32_t t0 = s.inst_tri[k], e0 = s.inst_edge[k];
+    rc = lbvh_build(s.tri_bvh[k].get(), x, s.nv, s.tris.p + 3 * (size_t)t0, s.inst_tri[k + 1] - t0, 30,
+                    s.aux[(2 * k) % N_AUX]);
+    if (rc == MGUSO_OK)
+      rc = lbvh_build(s.edge_bvh[k].get(), x, s.nv, s.edge_tris.p + 3 * (size_t)e0, s.inst_edge[k + 1] - e0, 30,
+                      s.aux[(2 * k + 1) % N_AUX]);
+  }
+  MG_TRY(aux_join(s));
+  return rc;
 }
 
 // ---- self intersection (has_self_intersection, implicit.rs:618-650) ------------------
@@ -152,10 +184,15 @@ __global__ void k_self_intersect(BvhSet bv, const uint8_t* __restrict__ vinst, c
 // red[RED_STRIDE k + 14] (which the caller zeroes); rebuilds the triangle BVHs at x.
 int self_intersections(Scene& s) {
   if (s.n_edge == 0) return MGUSO_OK;
-  for (uint32_t k = 0; k < s.ninst; ++k) {
+  MG_TRY(aux_fork(s));
+  int rc = MGUSO_OK;
+  for (uint32_t k = 0; k < s.ninst && rc == MGUSO_OK; ++k) {
     const uint32_t t0 = s.inst_tri[k];
-    MG_TRY(lbvh_build(s.tri_bvh[k].get(), s.x.p, s.nv, s.tris.p + 3 * (size_t)t0, s.inst_tri[k + 1] - t0, 30, s.st));
+    rc = lbvh_build(s.tri_bvh[k].get(), s.x.p, s.nv, s.tris.p + 3 * (size_t)t0, s.inst_tri[k + 1] - t0, 30,
+                    s.aux[k % N_AUX]);
   }
+  MG_TRY(aux_join(s));
+  MG_TRY(rc);
   BvhSet tv = view_set(s.tri_bvh, s.inst_tri);
   k_self_intersect<<<ceil_div(s.n_edge, 128), 128, 0, s.st>>>(tv, s.vinst.p, s.x.p, s.edges.p, s.tris.p, s.inv_mass.p,
                                                              s.n_edge, s.red.p, s.status.p);
@@ -285,23 +322,29 @@ __global__ void k_vt_stencils(BvhSet bv, const uint8_t* __restrict__ vinst, cons
   if (!ok) atomicOr(status, ST_STACK_OVERFLOW);
 }
 
+// Edge-edge pairs: thread t (edge t) takes the pairs (t, p) with p > t, the lower-indexed
+// edge first in the stencil and its key, so each pair is seen once. An edge in its instance's
+// static tail (every edge from there on has both vertices pinned) has no partner above it
+// that can move, and skips its traversal.
 __global__ void k_ee_stencils(BvhSet bv, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
-                              const uint32_t* __restrict__ edges,
+                              const uint32_t* __restrict__ edges, const uint32_t* __restrict__ ee_tail,
                               const float* __restrict__ im, uint32_t ne, float search, float dhat, int mixed,
                               Stencil* out, unsigned long long* keys, uint32_t* ids, unsigned long long* counter,
                               uint32_t cap, uint32_t* status) {
-  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= ne) return;
-  uint32_t b0 = edges[2 * j], b1 = edges[2 * j + 1];
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ne) return;
+  const uint32_t b0 = edges[2 * t], b1 = edges[2 * t + 1];
+  const uint32_t k = vinst[b0];
+  if (t >= ee_tail[k]) return;
   float4 lo, hi;
   edge_box(x, b0, b1, search, lo, hi);
-  bool jmov = im[b0] > 0.f || im[b1] > 0.f;
-  bool ok = visit(bv, vinst[b0], lo, hi, [&](uint32_t i) {
-    if (i >= j) return;
-    uint32_t a0 = edges[2 * i], a1 = edges[2 * i + 1];
-    if (!(jmov || im[a0] > 0.f || im[a1] > 0.f)) return;
+  const bool tmov = im[b0] > 0.f || im[b1] > 0.f;
+  bool ok = visit(bv, k, lo, hi, [&](uint32_t p) {
+    if (p <= t) return;
+    const uint32_t a0 = edges[2 * p], a1 = edges[2 * p + 1];
+    if (!(tmov || im[a0] > 0.f || im[a1] > 0.f)) return;
     if (a0 == b0 || a0 == b1 || a1 == b0 || a1 == b1) return;
-    uint32_t idx[4] = {a0, a1, b0, b1};
+    uint32_t idx[4] = {b0, b1, a0, a1};
     double g[12];
     float gf[12];
     float df = ee_distance<float>(x, idx, gf);
@@ -310,7 +353,7 @@ __global__ void k_ee_stencils(BvhSet bv, const uint8_t* __restrict__ vinst, cons
     if (mixed && df < 10.f * dhat) d = ee_distance<double>(x, idx, g);
     double ghat = (double)(0.5f * (dhat + dhat));
     if (!(d < ghat)) return;
-    emit_stencil(out, keys, ids, counter, cap, status, 1, i, j, idx, d, ghat, g);
+    emit_stencil(out, keys, ids, counter, cap, status, 1, t, p, idx, d, ghat, g);
   });
   if (!ok) atomicOr(status, ST_STACK_OVERFLOW);
 }
@@ -342,7 +385,7 @@ int collect_stencils(Scene& s, uint32_t* nst_out) {
                                                      s.st_keys.p, s.st_ids.p, s.counters.p, s.cap_stencils,
                                                      s.status.p);
     if (s.n_edge)
-      k_ee_stencils<<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, s.vinst.p, s.x.p, s.edges.p, s.inv_mass.p, s.n_edge, dhat, dhat,
+      k_ee_stencils<<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, s.vinst.p, s.x.p, s.edges.p, s.ee_tail.p, s.inv_mass.p, s.n_edge, dhat, dhat,
                                                            s.mixed ? 1 : 0, s.stencils.p, s.st_keys.p, s.st_ids.p,
                                                            s.counters.p, s.cap_stencils, s.status.p);
     MG_CUDA(cudaGetLastError());
@@ -597,17 +640,20 @@ __global__ void k_ccd_vt(BvhSet bv, const CcdPass* __restrict__ cpp, const uint8
   if (nacc) atomicAdd(red + RED_STRIDE * k + 6, nacc);
 }
 
+// As k_ee_stencils: thread t takes the pairs (t, p) with p > t (the lower-indexed edge first),
+// and an edge of its instance's static tail skips its traversal.
 template <class R>
 __global__ void k_ccd_ee(BvhSet bv, const CcdPass* __restrict__ cpp, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
-                         const float* __restrict__ dx, const uint32_t* __restrict__ edges, const float* __restrict__ im,
+                         const float* __restrict__ dx, const uint32_t* __restrict__ edges,
+                         const uint32_t* __restrict__ ee_tail, const float* __restrict__ im,
                          uint32_t ne, uint32_t max_iter, unsigned int* __restrict__ red,
                          unsigned int* __restrict__ acc, uint32_t* __restrict__ status) {
-  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ne) return;
   const CcdPass& cp = *cpp;
-  uint32_t b0 = edges[2 * j], b1 = edges[2 * j + 1];
+  const uint32_t b0 = edges[2 * j], b1 = edges[2 * j + 1];
   const uint32_t k = vinst[b0];
-  if (!((cp.todo >> k) & 1u)) return;
+  if (!((cp.todo >> k) & 1u) || j >= ee_tail[k]) return;
   const int np = (int)cp.npass[k];
   float4 lo, hi, qlo, qhi;
   edge_box(x, b0, b1, cp.search[k][np - 1], lo, hi);
@@ -629,7 +675,7 @@ __global__ void k_ccd_ee(BvhSet bv, const CcdPass* __restrict__ cpp, const uint8
   uint32_t nleaf = 0, nacc = 0;
   bool ok = visit_ccd(bv, k, lo, hi, qlo, qhi, cq, rq, [&](uint32_t i) {
     ++nleaf;
-    if (i >= j) return;
+    if (i <= j) return;
     uint32_t a0 = edges[2 * i], a1 = edges[2 * i + 1];
     if (!(jmov || im[a0] > 0.f || im[a1] > 0.f)) return;
     if (a0 == b0 || a0 == b1 || a1 == b0 || a1 == b1) return;
@@ -641,7 +687,7 @@ __global__ void k_ccd_ee(BvhSet bv, const CcdPass* __restrict__ cpp, const uint8
     }
     const int i0 = first_pass_edge(cp, k, x, b0, b1, plo, phi);
     if (i0 >= np) return;
-    uint32_t idx[4] = {a0, a1, b0, b1};
+    uint32_t idx[4] = {b0, b1, a0, a1};
     V3<R> x0[4], dd[4];
     for (int q = 0; q < 4; ++q) {
       x0[q] = ld3<R>(x, idx[q]);
@@ -795,7 +841,7 @@ static void ccd_body(Scene& s, const BvhSet& tv, const BvhSet& ev, CcdState* cs)
         s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.red.p, s.ccd_acc.p, s.status.p);
     if (s.n_edge)
       k_ccd_ee<double><<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, cpp, s.vinst.p, s.x.p, s.dx.p, s.edges.p,
-                                                               s.inv_mass.p, s.n_edge, iters, s.red.p, s.ccd_acc.p,
+                                                               s.ee_tail.p, s.inv_mass.p, s.n_edge, iters, s.red.p, s.ccd_acc.p,
                                                                s.status.p);
   } else {
     k_ccd_vt<float><<<ceil_div(s.nv, 128), 128, 0, st>>>(
@@ -803,7 +849,7 @@ static void ccd_body(Scene& s, const BvhSet& tv, const BvhSet& ev, CcdState* cs)
         s.side_best.p, s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, iters, s.red.p, s.ccd_acc.p, s.status.p);
     if (s.n_edge)
       k_ccd_ee<float><<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, cpp, s.vinst.p, s.x.p, s.dx.p, s.edges.p,
-                                                              s.inv_mass.p, s.n_edge, iters, s.red.p, s.ccd_acc.p,
+                                                              s.ee_tail.p, s.inv_mass.p, s.n_edge, iters, s.red.p, s.ccd_acc.p,
                                                               s.status.p);
   }
 }
@@ -903,10 +949,16 @@ int ccd_step(Scene& s, uint32_t active) {
   MG_CUDA(cudaGetLastError());
   if (self) {
     // the trees' displacement boxes (the trees were built at this iterate)
-    for (uint32_t k = 0; k < K; ++k) {
-      MG_TRY(lbvh_refit_disp(s.tri_bvh[k].get(), s.dx.p, s.tris.p + 3 * (size_t)s.inst_tri[k], st));
-      MG_TRY(lbvh_refit_disp(s.edge_bvh[k].get(), s.dx.p, s.edge_tris.p + 3 * (size_t)s.inst_edge[k], st));
+    MG_TRY(aux_fork(s));
+    int rc = MGUSO_OK;
+    for (uint32_t k = 0; k < K && rc == MGUSO_OK; ++k) {
+      rc = lbvh_refit_disp(s.tri_bvh[k].get(), s.dx.p, s.tris.p + 3 * (size_t)s.inst_tri[k], s.aux[(2 * k) % N_AUX]);
+      if (rc == MGUSO_OK)
+        rc = lbvh_refit_disp(s.edge_bvh[k].get(), s.dx.p, s.edge_tris.p + 3 * (size_t)s.inst_edge[k],
+                             s.aux[(2 * k + 1) % N_AUX]);
     }
+    MG_TRY(aux_join(s));
+    MG_TRY(rc);
     const BvhSet tv = view_set(s.tri_bvh, s.inst_tri), ev = view_set(s.edge_bvh, s.inst_edge);
     if (plain_launches()) {
       // the same launches driven by the host (for profilers)

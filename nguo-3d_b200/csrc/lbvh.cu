@@ -536,6 +536,12 @@ int radix_sort_pairs(Lbvh* b, void* keys, uint32_t* vals, uint32_t n, int key_bi
   return sort_impl<uint64_t>(b, (uint64_t*)keys, vals, n, key_bits, s);
 }
 
+// the centroid-bounds accumulator's start (ordered bits): the three minima at their highest
+// value, the three maxima at their lowest
+__global__ void k_ord_init(uint32_t* __restrict__ ord) {
+  if (threadIdx.x < 6) ord[threadIdx.x] = threadIdx.x < 3 ? 0xffffffffu : 0u;
+}
+
 template <class K>
 static int build_impl(Lbvh* b, const float* pos, const uint32_t* tris, uint32_t nt, int key_bits, cudaStream_t s) {
   b->nt = nt;
@@ -553,8 +559,7 @@ static int build_impl(Lbvh* b, const float* pos, const uint32_t* tris, uint32_t 
   MG_TRY(b->ord.reserve(8));
   MG_TRY(b->status.reserve(4));
   if (nt == 0) return MGUSO_OK;
-  uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0, 0, 0};
-  MG_CUDA(cudaMemcpyAsync(b->ord.p, init, sizeof(init), cudaMemcpyHostToDevice, s));
+  k_ord_init<<<1, 32, 0, s>>>(b->ord.p);
   int sms = device_sm_count();
   k_centroid_bounds<<<std::min<uint32_t>(ceil_div(nt, 256), sms * 8), 256, 0, s>>>(pos, tris, nt, b->ord.p);
   k_bounds_finish<<<1, 32, 0, s>>>(b->ord.p, b->params.p);

@@ -561,6 +561,15 @@ int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>
   }
   MG_TRY(up(s.edges, ev));
   MG_TRY(up(s.edge_tris, etris));
+  {
+    std::vector<uint32_t> tail(PCG_MAX_INST, 0);
+    for (uint32_t k = 0; k < s.ninst; ++k) {
+      uint32_t t = s.inst_edge[k + 1];
+      while (t > s.inst_edge[k] && s.h_pinned[edges[t - 1][0]] && s.h_pinned[edges[t - 1][1]]) --t;
+      tail[k] = t;
+    }
+    MG_TRY(up(s.ee_tail, tail));
+  }
   // 1-ring exclusion: the vertex and its triangle neighbours, sorted
   std::vector<std::vector<uint32_t>> ex(nv);
   for (uint32_t i = 0; i < nv; ++i) ex[i].push_back(i);

@@ -151,6 +151,8 @@ struct Scene {
   uint32_t n_edge = 0;
   DevBuf<uint32_t> tris, edge_tris;         // edges as degenerate triangles (a, b, b)
   DevBuf<uint32_t> edges;                   // 2 per edge
+  DevBuf<uint32_t> ee_tail;                 // per instance: first edge of its static tail (all
+                                            // later edges of the instance have both ends pinned)
   DevBuf<uint32_t> ex_ptr, ex_list;         // 1-ring exclusion (broadphase.rs:756-775)
   DevBuf<uint8_t> static_vert, collider_tri;
   bool has_static = false;
@@ -198,9 +200,17 @@ struct Scene {
   DevBuf<uint32_t> sell_base, sell_inst, sell_col, sell_pos;
   DevBuf<float> sell_val;
   bool fr_tuned = false;
+  // side streams for the instances' independent BVH builds and refits (forked from and joined
+  // back into st with events), created on first use
+  std::vector<cudaStream_t> aux;
+  std::vector<cudaEvent_t> aux_ev;
+  cudaEvent_t fork_ev = nullptr;
   ~Scene() {
     if (fr_exec) cudaGraphExecDestroy(fr_exec);
     if (ccd_exec) cudaGraphExecDestroy(ccd_exec);
+    for (auto e : aux_ev) cudaEventDestroy(e);
+    for (auto q : aux) cudaStreamDestroy(q);
+    if (fork_ev) cudaEventDestroy(fork_ev);
   }
   DevBuf<unsigned long long> st_keys;
   DevBuf<uint32_t> st_ids;

@@ -77,3 +77,50 @@ def test_adjoint_matches_fp64_cpu_adjoint(ctx, name):
     print(name, "adjoint", g, "\nfp64 cpu adjoint", ref, "\nstencils per step", nst, "\nerror / max|ref|", err)
     assert max(nst) > 100
     assert err.max() <= 1e-3, err
+
+
+def test_exact_hessian_matches_fp64_cpu_hessian(ctx):
+    """The Hessian the backward pass solves with (mguso_scene_assemble_exact) at the end of
+    the drape's second step (802 contact stencils, the seam's sides 1 mm apart) against the
+    oracle's FP64 Jacobian of the step's residual with the same frozen contact set: every
+    entry within 1e-4 of the largest, and the same (positive) smallest eigenvalue."""
+    import scipy.sparse as sp
+
+    import oracle_py as O
+    from mguso import ImplicitSolver
+    from mguso.adjoint import pattern_rest
+
+    sc, lm = adjoint_scene("coarse")
+    d = AdjointDrape(ctx, sc, "mixed")
+    theta = np.ones(8)
+    d.forward(theta, 2, 2)
+    xs, vs = d.states()
+    d.close()
+    rest, k = pattern_rest(sc["shell_uv"], sc["shell_panel"], theta, 2)
+    gs = dict(sc, shell_rest=rest.astype(np.float32), shell_stiff=k.astype(np.float32),
+              params=dict(sc["params"], factor_storage=1))
+    g = ImplicitSolver(ctx, gs, "mixed")
+    h = float(sc["params"]["dt"])
+    grav = np.array(sc["params"]["gravity"], np.float32)
+    im = sc["inv_mass"]
+    xt = (xs[1] + (vs[1] * h + grav * h * h) * (im > 0)[:, None]).astype(np.float32)
+    a = g.assemble(xs[2], xt, exact=True)
+    n3 = 3 * len(im)
+    m = sp.bsr_matrix((a["ps"][2].astype(np.float64), a["ps"][1].astype(np.int64), a["ps"][0].astype(np.int64)),
+                      shape=(n3, n3))
+    if len(a["c"][1]):
+        m = m + sp.bsr_matrix((a["c"][2].astype(np.float64), a["c"][1].astype(np.int64),
+                               a["c"][0].astype(np.int64)), shape=(n3, n3))
+    f = np.flatnonzero(np.repeat(im > 0, 3))
+    hg = m.toarray()[np.ix_(f, f)]
+    o = O.OracleSolver(sc, "f64")
+    H, _, nst = O.adjoint_system(o, sc, theta, xs[1].astype(np.float64), vs[1].astype(np.float64),
+                                 xs[2].astype(np.float64))
+    o.close()
+    hc = H[np.ix_(f, f)]
+    hc = 0.5 * (hc + hc.T)
+    assert abs(a["stencils"] - nst) <= 2 and nst > 100
+    err = np.abs(hg - hc).max() / np.abs(hc).max()
+    eg, ec = np.linalg.eigvalsh(0.5 * (hg + hg.T))[0], np.linalg.eigvalsh(hc)[0]
+    print("max |H_gpu - H_cpu| / max |H|", err, "smallest eigenvalues", eg, ec)
+    assert err < 1e-4 and ec > 0 and abs(eg - ec) < 1e-2 * ec
