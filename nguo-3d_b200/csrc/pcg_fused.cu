@@ -657,13 +657,31 @@ __global__ void __launch_bounds__(96 * DOMS) k_fr_schwarz3(FusedArgs a, const fl
       const TS* w = buf + t * TILE_FLOATS;
       const float* rj = rd + 32 * f3_tile_j(t);
       AA y = 0;
+      if constexpr (sizeof(TS) == 2) {
+        // row `lane` of an FP16 tile: element (lane, c) sits at c * 32 + off[(c >> 1) & 3] (the
+        // chunk permutation repeats every 8 columns), so with the column loop unrolled every
+        // load is a register base plus an immediate
+        const __half* wh = reinterpret_cast<const __half*>(w);
+        const __half* row[4];
+#pragma unroll
+        for (int qq = 0; qq < 4; ++qq) row[qq] = wh + ((((lane >> 3) ^ qq) & 3) << 3) + (lane & 7);
+#pragma unroll
+        for (int c0 = 0; c0 < 32; c0 += 4) {  // r_j as broadcast float4 loads, the sum in column order
+          const float4 r4 = *reinterpret_cast<const float4*>(rj + c0);
+          y += __half2float(row[(c0 >> 1) & 3][c0 * 32]) * r4.x;
+          y += __half2float(row[((c0 + 1) >> 1) & 3][(c0 + 1) * 32]) * r4.y;
+          y += __half2float(row[((c0 + 2) >> 1) & 3][(c0 + 2) * 32]) * r4.z;
+          y += __half2float(row[((c0 + 3) >> 1) & 3][(c0 + 3) * 32]) * r4.w;
+        }
+      } else {
 #pragma unroll 2
-      for (int c0 = 0; c0 < 32; c0 += 4) {  // r_j as broadcast float4 loads, the sum in column order
-        const float4 r4 = *reinterpret_cast<const float4*>(rj + c0);
-        y += (AA)tile_ld(w, tile_off<TS>(lane, c0)) * (AA)r4.x;
-        y += (AA)tile_ld(w, tile_off<TS>(lane, c0 + 1)) * (AA)r4.y;
-        y += (AA)tile_ld(w, tile_off<TS>(lane, c0 + 2)) * (AA)r4.z;
-        y += (AA)tile_ld(w, tile_off<TS>(lane, c0 + 3)) * (AA)r4.w;
+        for (int c0 = 0; c0 < 32; c0 += 4) {  // r_j as broadcast float4 loads, the sum in column order
+          const float4 r4 = *reinterpret_cast<const float4*>(rj + c0);
+          y += (AA)tile_ld(w, tile_off<TS>(lane, c0)) * (AA)r4.x;
+          y += (AA)tile_ld(w, tile_off<TS>(lane, c0 + 1)) * (AA)r4.y;
+          y += (AA)tile_ld(w, tile_off<TS>(lane, c0 + 2)) * (AA)r4.z;
+          y += (AA)tile_ld(w, tile_off<TS>(lane, c0 + 3)) * (AA)r4.w;
+        }
       }
       part[(2 * q + slot) * 32 + lane] = y;
     }
