@@ -232,21 +232,32 @@ __global__ void __launch_bounds__(FR_THREADS, 4) k_fr_rows_sell(FusedArgs a, con
       x2 = (Acc)fmaf(be, pc4.z, zc.z);
     };
     if (row < row1) {
-#pragma unroll 2
-      for (uint32_t b = b0; b < b1; ++b) {
-        const uint32_t c = __ldg(a.sell_col + 32 * (size_t)b + lane);
-        const float* m = a.sell_val + 288 * (size_t)b + lane;
-        Acc x0, x1, x2;
-        gather(c, x0, x1, x2);
-        y0 = fr_fma((Acc)__ldcs(m + 0), x0, y0);
-        y0 = fr_fma((Acc)__ldcs(m + 32), x1, y0);
-        y0 = fr_fma((Acc)__ldcs(m + 64), x2, y0);
-        y1 = fr_fma((Acc)__ldcs(m + 96), x0, y1);
-        y1 = fr_fma((Acc)__ldcs(m + 128), x1, y1);
-        y1 = fr_fma((Acc)__ldcs(m + 160), x2, y1);
-        y2 = fr_fma((Acc)__ldcs(m + 192), x0, y2);
-        y2 = fr_fma((Acc)__ldcs(m + 224), x1, y2);
-        y2 = fr_fma((Acc)__ldcs(m + 256), x2, y2);
+      // the slice's slots in pairs: both columns, then both gathers, then the products (the
+      // same slots in the same order as one at a time)
+      for (uint32_t b = b0; b < b1; b += 2) {
+        const bool two = b + 1 < b1;
+        const uint32_t cA = __ldg(a.sell_col + 32 * (size_t)b + lane);
+        const uint32_t cB = two ? __ldg(a.sell_col + 32 * (size_t)(b + 1) + lane) : cA;
+        const float4 zA = ld_v4(a.z, cA), pA = ld_v4(po, cA), zB = ld_v4(a.z, cB), pB = ld_v4(po, cB);
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          if (u == 1 && !two) break;
+          const float* m = a.sell_val + 288 * (size_t)(b + u) + lane;
+          const float4& zc = u ? zB : zA;
+          const float4& pc4 = u ? pB : pA;
+          const Acc x0 = (Acc)fmaf(be, pc4.x, zc.x);
+          const Acc x1 = (Acc)fmaf(be, pc4.y, zc.y);
+          const Acc x2 = (Acc)fmaf(be, pc4.z, zc.z);
+          y0 = fr_fma((Acc)__ldcs(m + 0), x0, y0);
+          y0 = fr_fma((Acc)__ldcs(m + 32), x1, y0);
+          y0 = fr_fma((Acc)__ldcs(m + 64), x2, y0);
+          y1 = fr_fma((Acc)__ldcs(m + 96), x0, y1);
+          y1 = fr_fma((Acc)__ldcs(m + 128), x1, y1);
+          y1 = fr_fma((Acc)__ldcs(m + 160), x2, y1);
+          y2 = fr_fma((Acc)__ldcs(m + 192), x0, y2);
+          y2 = fr_fma((Acc)__ldcs(m + 224), x1, y2);
+          y2 = fr_fma((Acc)__ldcs(m + 256), x2, y2);
+        }
       }
       const uint32_t ce = __ldg(a.crp + row + 1);
       for (uint32_t kk = __ldg(a.crp + row); kk < ce; ++kk) {
