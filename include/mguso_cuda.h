@@ -185,6 +185,9 @@ int mguso_lbvh_build_query(mguso_ctx* ctx, const float* positions, uint32_t nv, 
  * u32 keys when key_bits <= 32, u64 keys otherwise. Replaces GpuRadixSort::sort_pairs
  * (radix.rs:112-352), which is limited to 65 536 keys. */
 int mguso_radix_sort_pairs(mguso_ctx* ctx, void* keys, uint32_t* vals, uint32_t n, int key_bits, void* stream);
+/* Waits for the device, then reports whether the last mguso_radix_sort_pairs of this context
+ * gave up a bounded look-back wait (MGUSO_ERR_TIMEOUT; its output is then not sorted). */
+int mguso_radix_sort_status(mguso_ctx* ctx);
 /* Allocation-free variant of mguso_radix_sort_pairs, with no counterpart in the reference.
  * For callers that may not allocate device memory once they are running (a host engine
  * that gives all of the GPU's memory to its own pool at start-up, or a per-frame path that

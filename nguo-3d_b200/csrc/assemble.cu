@@ -927,7 +927,7 @@ __global__ void k_contact_exact(const Stencil* __restrict__ sts, uint32_t nst, c
 
 int contact_stiffness(Scene& s, uint32_t nst) {
   if (nst == 0) return MGUSO_OK;
-  MG_TRY(s.contact_k.reserve(2 * (size_t)nst));
+  MG_TRY(s.contact_k.grow(2 * (size_t)nst));
   unsigned g = ceil_div(nst, 64);
   if (s.mixed)
     k_contact_stiffness<double><<<g, 64, 0, s.st>>>(s.stencils_sorted.p, nst, s.inv_mass.p, s.pinned.p,
@@ -1068,7 +1068,7 @@ __global__ void k_scan_add(uint32_t* __restrict__ out, uint32_t n, const uint32_
 
 static int scan_u32(Scene& s, const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* total, DevBuf<uint32_t>& tmp) {
   uint32_t nb = std::max<uint32_t>(ceil_div(n, 1024), 1);
-  MG_TRY(tmp.reserve(nb + 1));
+  MG_TRY(tmp.grow(nb + 1));
   if (n) k_scan_block<<<nb, 1024, 0, s.st>>>(in, out, n, tmp.p);
   else MG_CUDA(cudaMemsetAsync(tmp.p, 0, 4, s.st));
   k_scan_sums<<<1, 32, 0, s.st>>>(tmp.p, n ? nb : 1, total);
@@ -1086,12 +1086,12 @@ int assemble_contacts(Scene& s, uint32_t nst) {
     return MGUSO_OK;
   }
   const uint32_t mb = 32 * nst, mg_ = 8 * nst;
-  MG_TRY(s.ccblocks.reserve(9 * (size_t)mb));
-  MG_TRY(s.ckeys.reserve(mb));
-  MG_TRY(s.cids.reserve(mb));
-  MG_TRY(s.cgentries.reserve(3 * (size_t)mg_));
-  MG_TRY(s.gkeys.reserve(mg_));
-  MG_TRY(s.gids.reserve(mg_));
+  MG_TRY(s.ccblocks.grow(9 * (size_t)mb));
+  MG_TRY(s.ckeys.grow(mb));
+  MG_TRY(s.cids.grow(mb));
+  MG_TRY(s.cgentries.grow(3 * (size_t)mg_));
+  MG_TRY(s.gkeys.grow(mg_));
+  MG_TRY(s.gids.grow(mg_));
   unsigned g = ceil_div(nst, 64);
   if (s.hess_mode == 2 && (s.exact_terms & EXACT_CONTACTS))
     k_contact_exact<<<g, 64, 0, st>>>(s.stencils_sorted.p, nst, s.pinned.p, s.x.p, s.contact_k.p, s.p.barrier_kind,
@@ -1114,8 +1114,8 @@ int assemble_contacts(Scene& s, uint32_t nst) {
   DevBuf<uint32_t>& is_new = s.is_new;
   DevBuf<uint32_t>& rank = s.rank;
   DevBuf<uint32_t>& tmp = s.scan_tmp;
-  MG_TRY(is_new.reserve(mb));
-  MG_TRY(rank.reserve(mb));
+  MG_TRY(is_new.grow(mb));
+  MG_TRY(rank.grow(mb));
   k_contact_heads<<<ceil_div(mb, 256), 256, 0, st>>>(s.ckeys.p, s.cids.p, mb, s.ccblocks.p, s.Ps.row_ptr.p,
                                                     s.Ps.col.p, s.A->val.p, is_new.p);
   MG_TRY(scan_u32(s, is_new.p, rank.p, mb, s.c_count.p, tmp));

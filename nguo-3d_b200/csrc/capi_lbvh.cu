@@ -150,4 +150,17 @@ int mguso_radix_sort_pairs(mguso_ctx* ctx, void* keys, uint32_t* vals, uint32_t 
   return radix_sort_pairs(L, keys, vals, n, key_bits, (cudaStream_t)stream);
 }
 
+int mguso_radix_sort_status(mguso_ctx* ctx) {
+  MG_CHECK_ARG(ctx, "null argument");
+  if (!ctx->sort_scratch || !ctx->sort_scratch->status.p) return MGUSO_OK;
+  MG_CUDA(cudaDeviceSynchronize());
+  uint32_t st = 0;
+  MG_CUDA(cudaMemcpy(&st, ctx->sort_scratch->status.p, 4, cudaMemcpyDeviceToHost));
+  if (st & ST_WAIT_TIMEOUT) {
+    set_error("radix sort look-back wait timed out");
+    return MGUSO_ERR_TIMEOUT;
+  }
+  return MGUSO_OK;
+}
+
 }  // extern "C"

@@ -2,6 +2,7 @@
 // buffers and the PTX wrappers (mbarrier, 1-D TMA bulk copy) the staged kernels use.
 #pragma once
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <stdint.h>
 
 #include <cstdio>
@@ -71,6 +72,10 @@ struct DevBuf {
     cap = n;
     return MGUSO_OK;
   }
+  // reserve for buffers sized by a count that varies between calls (contact stencils,
+  // sort lengths): a cudaMalloc of tens of MB takes milliseconds to tens of milliseconds,
+  // so the capacity at least doubles when it has to grow
+  int grow(size_t n) { return reserve(n <= cap && p ? n : std::max(n, 2 * cap)); }
   int upload(const T* h, size_t n, cudaStream_t s) {
     MG_TRY(reserve(n));
     if (n && h) MG_CUDA(cudaMemcpyAsync(p, h, n * sizeof(T), cudaMemcpyHostToDevice, s));

@@ -57,17 +57,6 @@ static BvhSet view_set(const std::vector<std::unique_ptr<Lbvh>>& b, const std::v
   return s;
 }
 
-// search box (lo, hi) against the position boxes, the pruning test with the query's own box
-// (qlo, qhi) and displacement ball (cq, rq) against the displacement boxes
-template <class F>
-__device__ __forceinline__ bool visit_ccd(const BvhSet& bs, uint32_t k, float4 lo, float4 hi, float4 qlo, float4 qhi,
-                                          float3 cq, float rq, F&& f) {
-  const BvhView& bv = bs.t[k];
-  const uint32_t base = bs.base[k];
-  return lbvh_visit_ccd(bv.left, bv.right, bv.node, bv.leaf, bv.dnode, bv.dleaf, bv.prim, bv.n, lo, hi, qlo, qhi, cq,
-                        rq, [&](uint32_t local) { f(base + local); });
-}
-
 template <class F>
 __device__ __forceinline__ bool visit(const BvhSet& bs, uint32_t k, float4 lo, float4 hi, F&& f) {
   const BvhView& bv = bs.t[k];
@@ -523,7 +512,7 @@ __global__ void k_ccd_sl(uint32_t n, const uint32_t* __restrict__ fv, const floa
 
 // CCD candidate pruning: a pair whose accd_toi (contact.rs:378-437) would return max_t at
 // its first test cannot lower the step fraction, and traversal skips whole subtrees of such
-// pairs (lbvh_visit_ccd) from the primitives' displacement boxes, refitted per CCD call.
+// pairs (CcdWalk) from the primitives' displacement boxes, refitted per CCD call.
 
 // Per-instance CCD passes of one launch: up to CCD_CHUNK consecutive search radii of the
 // widening schedule (ascending). The traversal uses the largest; each candidate pair's ACCD
@@ -567,151 +556,260 @@ __device__ __forceinline__ int first_pass_edge(const CcdPass& cp, uint32_t k, co
   return n;
 }
 
-template <class R>
-__global__ void k_ccd_vt(BvhSet bv, const CcdPass* __restrict__ cpp, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
-                         const float* __restrict__ dx, const uint32_t* __restrict__ tris,
-                         const uint8_t* __restrict__ ctri, const float* __restrict__ im,
-                         const uint32_t* __restrict__ ex_ptr, const uint32_t* __restrict__ ex_list,
-                         const unsigned long long* __restrict__ best, const float* __restrict__ pn, int has_static,
-                         uint32_t nv, float dhat, uint32_t max_iter, unsigned int* __restrict__ red,
-                         unsigned int* __restrict__ acc, uint32_t* __restrict__ status) {
-  uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= nv) return;
-  const CcdPass& cp = *cpp;
-  const uint32_t k = vinst[v];
-  if (!((cp.todo >> k) & 1u)) return;
-  const int np = (int)cp.npass[k];
-  float4 lo, hi, qlo, qhi;
-  point_box(x, v, cp.search[k][np - 1], lo, hi);
-  point_box(x, v, 0.f, qlo, qhi);
-  const float3 cq = make_float3(dx[3 * v], dx[3 * v + 1], dx[3 * v + 2]);
-  bool vmov = im[v] > 0.f;
-  float side = 2.f;
-  float tloc[CCD_CHUNK];
-  uint32_t ncap[CCD_CHUNK];
-#pragma unroll
-  for (int i = 0; i < CCD_CHUNK; ++i) {
-    tloc[i] = 1.f;
-    ncap[i] = 0;
+// ---- warp-pooled root solves ----------------------------------------------------------------
+// Each lane walks its query's tree (CcdWalk) and pushes the leaves it reaches, as (query,
+// primitive) pairs, onto its warp's queue in shared memory; whenever 32 are queued the whole
+// warp takes them, one per lane, through the remaining filters and accd_toi. The walks stay
+// per lane, but the root solves (the bulk of the work) run on full warps instead of on the
+// few lanes whose walk happens to sit on a leaf. Results are per (instance, pass) minima and
+// sums, so the order in which the pairs are solved does not change them.
+constexpr int CCD_WARPS = 4;  // 128-thread blocks
+constexpr int CCD_QCAP = 96;  // < 32 left over + 2 leaves per lane and step
+
+__device__ __forceinline__ void wq_push(uint2* q, int& n, bool has, uint2 e) {
+  const unsigned m = __ballot_sync(0xffffffffu, has);
+  if (has) q[n + __popc(m & ((1u << (threadIdx.x & 31)) - 1u))] = e;
+  n += __popc(m);
+}
+
+// Takes batches of up to 32 queued pairs while at least min_n are queued (n is warp-uniform).
+template <class F>
+__device__ __forceinline__ void wq_take(uint2* q, int& n, int min_n, F&& solve) {
+  const int lane = (int)(threadIdx.x & 31);
+  __syncwarp();
+  while (n >= min_n && n > 0) {
+    const int take = n < 32 ? n : 32;
+    const bool has = lane < take;
+    const uint2 e = has ? q[n - take + lane] : make_uint2(0u, 0u);
+    __syncwarp();
+    n -= take;
+    if (has) solve(e);
   }
-  uint32_t nleaf = 0, nacc = 0;
-  bool ok = visit_ccd(bv, k, lo, hi, qlo, qhi, cq, 0.f, [&](uint32_t t) {
-    ++nleaf;
-    uint32_t a = tris[3 * t], b = tris[3 * t + 1], c = tris[3 * t + 2];
-    bool tmov = im[a] > 0.f || im[b] > 0.f || im[c] > 0.f;
-    if (!tmov && !vmov) return;
-    if (excluded(ex_ptr, ex_list, v, a, b, c)) return;
-    if (has_static && ctri[t]) {
-      if (side == 2.f) side = side_of(v, best, x, tris, pn, dhat);
-      if (side < 0.f) return;
+}
+
+// A lane's step fractions and cap counts per pass for one instance at a time, flushed to the
+// per (instance, pass) accumulators when the instance changes and at the end.
+struct CcdAcc {
+  uint32_t k;
+  float t[CCD_CHUNK];
+  uint32_t cap[CCD_CHUNK];
+  uint32_t solves;
+  __device__ __forceinline__ void reset(uint32_t kk) {
+    k = kk;
+    solves = 0;
+#pragma unroll
+    for (int i = 0; i < CCD_CHUNK; ++i) {
+      t[i] = 1.f;
+      cap[i] = 0;
     }
-    float plo[3], phi[3];
-    for (int q = 0; q < 3; ++q) {
-      const float pa = x[3 * a + q], pb = x[3 * b + q], pc = x[3 * c + q];
-      plo[q] = fminf(fminf(pa, pb), pc);
-      phi[q] = fmaxf(fmaxf(pa, pb), pc);
+  }
+  __device__ __forceinline__ void flush(const CcdPass& cp, unsigned int* acc, unsigned int* red, int solve_slot) {
+    if (k == 0xffffffffu) return;
+    const int np = (int)cp.npass[k];
+#pragma unroll
+    for (int i = 0; i < CCD_CHUNK; ++i) {
+      if (i < np && t[i] < 1.f) atomic_min_pos(ccd_slot(acc, k, i), t[i]);
+      if (i < np && cap[i]) atomicAdd(ccd_slot(acc, k, i) + 1, cap[i]);
     }
-    const int i0 = first_pass_point(cp, k, x, v, plo, phi);
-    if (i0 >= np) return;
-    uint32_t idx[4] = {v, a, b, c};
-    V3<R> x0[4], dd[4];
-    for (int q = 0; q < 4; ++q) {
-      x0[q] = ld3<R>(x, idx[q]);
-      dd[q] = ld3<R>(dx, idx[q]);
+    if (solves) atomicAdd(red + RED_STRIDE * k + solve_slot, solves);
+  }
+  __device__ __forceinline__ void add(uint32_t kk, int i0, float tt, bool capped, const CcdPass& cp,
+                                      unsigned int* acc, unsigned int* red, int solve_slot) {
+    if (kk != k) {
+      flush(cp, acc, red, solve_slot);
+      reset(kk);
     }
-    bool cap = false;
-    ++nacc;
-    R toi = accd_toi<R>(x0, dd, R(0), R(1.25), R(0.01), max_iter, 0, &cap);
-    const float tt = (float)(toi / R(1.25));
+    ++solves;
 #pragma unroll
     for (int i = 0; i < CCD_CHUNK; ++i)
       if (i >= i0) {
-        tloc[i] = fminf(tloc[i], tt);
-        ncap[i] += cap ? 1u : 0u;
+        t[i] = fminf(t[i], tt);
+        cap[i] += capped ? 1u : 0u;
       }
-  });
-  if (!ok) atomicOr(status, ST_STACK_OVERFLOW);
-#pragma unroll
-  for (int i = 0; i < CCD_CHUNK; ++i) {
-    if (i < np && tloc[i] < 1.f) atomic_min_pos(ccd_slot(acc, k, i), tloc[i]);
-    if (i < np && ncap[i]) atomicAdd(ccd_slot(acc, k, i) + 1, ncap[i]);
   }
-  if (nleaf) atomicAdd(red + RED_STRIDE * k + 5, nleaf);
-  if (nacc) atomicAdd(red + RED_STRIDE * k + 6, nacc);
+};
+
+__device__ __forceinline__ void walk_init(CcdWalk& w, const BvhSet& bs, uint32_t k, float4 lo, float4 hi, float4 qlo,
+                                          float4 qhi, float3 cq, float rq) {
+  const BvhView& bv = bs.t[k];
+  w.left = bv.left;
+  w.right = bv.right;
+  w.prim = bv.prim;
+  w.node = bv.node;
+  w.leaf = bv.leaf;
+  w.dnode = bv.dnode;
+  w.dleaf = bv.dleaf;
+  w.nt = bv.n;
+  w.slo = lo;
+  w.shi = hi;
+  w.qlo = qlo;
+  w.qhi = qhi;
+  w.cq = cq;
+  w.rq = rq;
 }
 
-// As k_ee_stencils: thread t takes the pairs (t, p) with p > t (the lower-indexed edge first),
-// and an edge of its instance's static tail skips its traversal.
+// Vertex-triangle passes: lane v walks the triangles near vertex v.
 template <class R>
-__global__ void k_ccd_ee(BvhSet bv, const CcdPass* __restrict__ cpp, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
-                         const float* __restrict__ dx, const uint32_t* __restrict__ edges,
-                         const uint32_t* __restrict__ ee_tail, const float* __restrict__ im,
-                         uint32_t ne, uint32_t max_iter, unsigned int* __restrict__ red,
-                         unsigned int* __restrict__ acc, uint32_t* __restrict__ status) {
-  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= ne) return;
+__global__ void __launch_bounds__(CCD_WARPS * 32) k_ccd_vt(
+    BvhSet bv, const CcdPass* __restrict__ cpp, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
+    const float* __restrict__ dx, const uint32_t* __restrict__ tris, const uint8_t* __restrict__ ctri,
+    const float* __restrict__ im, const uint32_t* __restrict__ ex_ptr, const uint32_t* __restrict__ ex_list,
+    const unsigned long long* __restrict__ best, const float* __restrict__ pn, int has_static, uint32_t nv, float dhat,
+    uint32_t max_iter, unsigned int* __restrict__ red, unsigned int* __restrict__ acc, uint32_t* __restrict__ status) {
+  __shared__ uint2 qbuf[CCD_WARPS][CCD_QCAP];
+  uint2* q = qbuf[threadIdx.x >> 5];
+  int qn = 0;
   const CcdPass& cp = *cpp;
-  const uint32_t b0 = edges[2 * j], b1 = edges[2 * j + 1];
-  const uint32_t k = vinst[b0];
-  if (!((cp.todo >> k) & 1u) || j >= ee_tail[k]) return;
-  const int np = (int)cp.npass[k];
-  float4 lo, hi, qlo, qhi;
-  edge_box(x, b0, b1, cp.search[k][np - 1], lo, hi);
-  edge_box(x, b0, b1, 0.f, qlo, qhi);
-  // the query edge's displacements lie in the ball around their midpoint
-  const float3 d0 = make_float3(dx[3 * b0], dx[3 * b0 + 1], dx[3 * b0 + 2]);
-  const float3 d1 = make_float3(dx[3 * b1], dx[3 * b1 + 1], dx[3 * b1 + 2]);
-  const float3 cq = make_float3(0.5f * (d0.x + d1.x), 0.5f * (d0.y + d1.y), 0.5f * (d0.z + d1.z));
-  const float ex = d1.x - d0.x, ey = d1.y - d0.y, ez = d1.z - d0.z;
-  const float rq = 0.5f * sqrtf(ex * ex + ey * ey + ez * ez) * 1.0001f;
-  bool jmov = im[b0] > 0.f || im[b1] > 0.f;
-  float tloc[CCD_CHUNK];
-  uint32_t ncap[CCD_CHUNK];
-#pragma unroll
-  for (int i = 0; i < CCD_CHUNK; ++i) {
-    tloc[i] = 1.f;
-    ncap[i] = 0;
+  const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t k = 0xffffffffu, base = 0, nleaf = 0;
+  bool done = true;
+  float side = 2.f;
+  CcdWalk walk;
+  walk.ok = true;
+  uint32_t out[2];
+  int nout = 0;
+  if (v < nv) {
+    const uint32_t kv = vinst[v];
+    if ((cp.todo >> kv) & 1u) {
+      k = kv;
+      base = bv.base[k];
+      float4 lo, hi, qlo, qhi;
+      point_box(x, v, cp.search[k][cp.npass[k] - 1], lo, hi);
+      point_box(x, v, 0.f, qlo, qhi);
+      walk_init(walk, bv, k, lo, hi, qlo, qhi, make_float3(dx[3 * v], dx[3 * v + 1], dx[3 * v + 2]), 0.f);
+      nout = walk.start(done, out);
+    }
   }
-  uint32_t nleaf = 0, nacc = 0;
-  bool ok = visit_ccd(bv, k, lo, hi, qlo, qhi, cq, rq, [&](uint32_t i) {
-    ++nleaf;
-    if (i <= j) return;
-    uint32_t a0 = edges[2 * i], a1 = edges[2 * i + 1];
-    if (!(jmov || im[a0] > 0.f || im[a1] > 0.f)) return;
+  CcdAcc a;
+  a.reset(0xffffffffu);
+  auto solve = [&](uint2 e) {
+    const uint32_t qv = e.x, t = e.y, kq = vinst[qv];
+    const uint32_t ta = tris[3 * t], tb = tris[3 * t + 1], tc = tris[3 * t + 2];
+    if (!(im[qv] > 0.f || im[ta] > 0.f || im[tb] > 0.f || im[tc] > 0.f)) return;
+    if (excluded(ex_ptr, ex_list, qv, ta, tb, tc)) return;
+    float plo[3], phi[3];
+    for (int c = 0; c < 3; ++c) {
+      const float pa = x[3 * ta + c], pb = x[3 * tb + c], pc = x[3 * tc + c];
+      plo[c] = fminf(fminf(pa, pb), pc);
+      phi[c] = fmaxf(fmaxf(pa, pb), pc);
+    }
+    const int i0 = first_pass_point(cp, kq, x, qv, plo, phi);
+    if (i0 >= (int)cp.npass[kq]) return;
+    const uint32_t idx[4] = {qv, ta, tb, tc};
+    V3<R> x0[4], dd[4];
+    for (int c = 0; c < 4; ++c) {
+      x0[c] = ld3<R>(x, idx[c]);
+      dd[c] = ld3<R>(dx, idx[c]);
+    }
+    bool capped = false;
+    const R toi = accd_toi<R>(x0, dd, R(0), R(1.25), R(0.01), max_iter, 0, &capped);
+    a.add(kq, i0, (float)(toi / R(1.25)), capped, cp, acc, red, 6);
+  };
+  for (;;) {
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      bool has = c < nout;
+      const uint32_t t = has ? base + out[c] : 0u;
+      if (has) {
+        ++nleaf;
+        // a collider triangle only counts on the vertex's outer side (lazily, once per vertex)
+        if (has_static && ctri[t]) {
+          if (side == 2.f) side = side_of(v, best, x, tris, pn, dhat);
+          if (side < 0.f) has = false;
+        }
+      }
+      wq_push(q, qn, has, make_uint2(v, t));
+    }
+    wq_take(q, qn, 32, solve);
+    if (!__any_sync(0xffffffffu, !done)) break;
+    nout = done ? 0 : walk.step(done, out);
+  }
+  wq_take(q, qn, 1, solve);
+  a.flush(cp, acc, red, 6);
+  if (!walk.ok) atomicOr(status, ST_STACK_OVERFLOW);
+  if (nleaf) atomicAdd(red + RED_STRIDE * k + 5, nleaf);
+}
+
+// Edge-edge passes. As k_ee_stencils: lane j takes the pairs (j, i) with i > j (the
+// lower-indexed edge first), and an edge of its instance's static tail skips its walk.
+template <class R>
+__global__ void __launch_bounds__(CCD_WARPS * 32) k_ccd_ee(
+    BvhSet bv, const CcdPass* __restrict__ cpp, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
+    const float* __restrict__ dx, const uint32_t* __restrict__ edges, const uint32_t* __restrict__ ee_tail,
+    const float* __restrict__ im, uint32_t ne, uint32_t max_iter, unsigned int* __restrict__ red,
+    unsigned int* __restrict__ acc, uint32_t* __restrict__ status) {
+  __shared__ uint2 qbuf[CCD_WARPS][CCD_QCAP];
+  uint2* q = qbuf[threadIdx.x >> 5];
+  int qn = 0;
+  const CcdPass& cp = *cpp;
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t k = 0xffffffffu, base = 0, nleaf = 0;
+  bool done = true;
+  CcdWalk walk;
+  walk.ok = true;
+  uint32_t out[2];
+  int nout = 0;
+  if (j < ne) {
+    const uint32_t b0 = edges[2 * j], b1 = edges[2 * j + 1];
+    const uint32_t kj = vinst[b0];
+    if (((cp.todo >> kj) & 1u) && j < ee_tail[kj]) {
+      k = kj;
+      base = bv.base[k];
+      float4 lo, hi, qlo, qhi;
+      edge_box(x, b0, b1, cp.search[k][cp.npass[k] - 1], lo, hi);
+      edge_box(x, b0, b1, 0.f, qlo, qhi);
+      // the query edge's displacements lie in the ball around their midpoint
+      const float3 d0 = make_float3(dx[3 * b0], dx[3 * b0 + 1], dx[3 * b0 + 2]);
+      const float3 d1 = make_float3(dx[3 * b1], dx[3 * b1 + 1], dx[3 * b1 + 2]);
+      const float3 cq = make_float3(0.5f * (d0.x + d1.x), 0.5f * (d0.y + d1.y), 0.5f * (d0.z + d1.z));
+      const float ex = d1.x - d0.x, ey = d1.y - d0.y, ez = d1.z - d0.z;
+      const float rq = 0.5f * sqrtf(ex * ex + ey * ey + ez * ez) * 1.0001f;
+      walk_init(walk, bv, k, lo, hi, qlo, qhi, cq, rq);
+      nout = walk.start(done, out);
+    }
+  }
+  CcdAcc a;
+  a.reset(0xffffffffu);
+  auto solve = [&](uint2 e) {
+    const uint32_t qj = e.x, i = e.y;
+    const uint32_t b0 = edges[2 * qj], b1 = edges[2 * qj + 1], a0 = edges[2 * i], a1 = edges[2 * i + 1];
+    const uint32_t kq = vinst[b0];
+    if (!(im[b0] > 0.f || im[b1] > 0.f || im[a0] > 0.f || im[a1] > 0.f)) return;
     if (a0 == b0 || a0 == b1 || a1 == b0 || a1 == b1) return;
     float plo[3], phi[3];
-    for (int q = 0; q < 3; ++q) {
-      const float pa = x[3 * a0 + q], pb = x[3 * a1 + q];
-      plo[q] = fminf(pa, pb);
-      phi[q] = fmaxf(pa, pb);
+    for (int c = 0; c < 3; ++c) {
+      const float pa = x[3 * a0 + c], pb = x[3 * a1 + c];
+      plo[c] = fminf(pa, pb);
+      phi[c] = fmaxf(pa, pb);
     }
-    const int i0 = first_pass_edge(cp, k, x, b0, b1, plo, phi);
-    if (i0 >= np) return;
-    uint32_t idx[4] = {b0, b1, a0, a1};
+    const int i0 = first_pass_edge(cp, kq, x, b0, b1, plo, phi);
+    if (i0 >= (int)cp.npass[kq]) return;
+    const uint32_t idx[4] = {b0, b1, a0, a1};
     V3<R> x0[4], dd[4];
-    for (int q = 0; q < 4; ++q) {
-      x0[q] = ld3<R>(x, idx[q]);
-      dd[q] = ld3<R>(dx, idx[q]);
+    for (int c = 0; c < 4; ++c) {
+      x0[c] = ld3<R>(x, idx[c]);
+      dd[c] = ld3<R>(dx, idx[c]);
     }
-    bool cap = false;
-    ++nacc;
-    R toi = accd_toi<R>(x0, dd, R(0), R(1.25), R(0.01), max_iter, 1, &cap);
-    const float tt = (float)(toi / R(1.25));
+    bool capped = false;
+    const R toi = accd_toi<R>(x0, dd, R(0), R(1.25), R(0.01), max_iter, 1, &capped);
+    a.add(kq, i0, (float)(toi / R(1.25)), capped, cp, acc, red, 8);
+  };
+  for (;;) {
 #pragma unroll
-    for (int q = 0; q < CCD_CHUNK; ++q)
-      if (q >= i0) {
-        tloc[q] = fminf(tloc[q], tt);
-        ncap[q] += cap ? 1u : 0u;
-      }
-  });
-  if (!ok) atomicOr(status, ST_STACK_OVERFLOW);
-#pragma unroll
-  for (int i = 0; i < CCD_CHUNK; ++i) {
-    if (i < np && tloc[i] < 1.f) atomic_min_pos(ccd_slot(acc, k, i), tloc[i]);
-    if (i < np && ncap[i]) atomicAdd(ccd_slot(acc, k, i) + 1, ncap[i]);
+    for (int c = 0; c < 2; ++c) {
+      const bool leaf = c < nout;
+      const uint32_t i = leaf ? base + out[c] : 0u;
+      nleaf += leaf ? 1u : 0u;
+      wq_push(q, qn, leaf && i > j, make_uint2(j, i));
+    }
+    wq_take(q, qn, 32, solve);
+    if (!__any_sync(0xffffffffu, !done)) break;
+    nout = done ? 0 : walk.step(done, out);
   }
+  wq_take(q, qn, 1, solve);
+  a.flush(cp, acc, red, 8);
+  if (!walk.ok) atomicOr(status, ST_STACK_OVERFLOW);
   if (nleaf) atomicAdd(red + RED_STRIDE * k + 7, nleaf);
-  if (nacc) atomicAdd(red + RED_STRIDE * k + 8, nacc);
 }
 
 // ccd_max_step (implicit.rs:1690-1947) without strain limiting, per instance. The
@@ -722,14 +820,20 @@ __global__ void k_ccd_ee(BvhSet bv, const CcdPass* __restrict__ cpp, const uint8
 // ---- the CCD schedule on the device -----------------------------------------------------
 // The widening search of ccd_max_step (implicit.rs:1829-1947) per instance: the first launch
 // runs the schedule's first radius alone, each later one up to CCD_CHUNK further radii
-// (allowed, 4 allowed, ... up to the instance's largest displacement); an instance is settled
-// by the first radius whose step fraction keeps every move inside it, or by the full radius.
+// (allowed, 4 allowed, ... up to the instance's largest displacement, and no further than the
+// first radius that the previous launch's fraction already settles: the traversal runs at the
+// chunk's largest radius, so a chunk that overshot it would only search a larger box for a
+// result the sequential schedule never looks at); an instance is settled by the first radius
+// whose step fraction keeps every move inside it, or by the full radius.
 // Plan, traversals and settle run as the body of a conditional while node, so the host never
 // waits on the schedule; CcdState holds it all.
 struct CcdState {
   CcdPass cp;  // the current launch's radii
   float sched[PCG_MAX_INST][CCD_CHUNK];
   float allowed[PCG_MAX_INST], max_disp[PCG_MAX_INST], half_len[PCG_MAX_INST];
+  // the radius from which on a pass is sure to settle: t_i md <= r_i holds once r_i >= t md
+  // for the fraction t of any smaller radius, since t_i only falls as the radius grows
+  float reach[PCG_MAX_INST];
   float t[PCG_MAX_INST];  // step fraction per instance (0 for inactive ones)
   uint32_t caps[PCG_MAX_INST];
   uint32_t launch, todo;
@@ -755,6 +859,7 @@ __global__ void k_ccd_start(CcdState* __restrict__ cs, const unsigned int* __res
     cs->t[k] = on ? __uint_as_float(red[RED_STRIDE * k + 1]) : 0.f;
     cs->caps[k] = 0;
     cs->allowed[k] = fmaxf(fminf(cs->half_len[k], md), 1.0e-9f);
+    cs->reach[k] = md;
   }
   if (k == 0) {
     cs->launch = 0;
@@ -782,7 +887,7 @@ __global__ void k_ccd_plan(CcdState* __restrict__ cs, unsigned int* __restrict__
     cs->sched[k][n] = a;
     cs->cp.search[k][n] = fixed + 2.0f * a;
     ++n;
-    if (cs->launch == 0 || n == (uint32_t)CCD_CHUNK || a >= md) break;
+    if (cs->launch == 0 || n == (uint32_t)CCD_CHUNK || a >= md || a >= cs->reach[k]) break;
     a = fminf(a * 4.0f, md);
   }
   cs->cp.npass[k] = n;
@@ -809,10 +914,12 @@ __global__ void k_ccd_settle(CcdState* __restrict__ cs, const unsigned int* __re
         settled = true;
       }
     }
-    if (settled)
+    if (settled) {
       atomicOr(&settled_mask, 1u << k);
-    else
+    } else {
       cs->allowed[k] = fminf(cs->sched[k][np - 1] * 4.0f, md);
+      cs->reach[k] = fminf(cs->reach[k], __uint_as_float(acc[2 * (CCD_CHUNK * k + np - 1)]) * md);
+    }
   }
   __syncthreads();
   if (k == 0) {
@@ -983,6 +1090,8 @@ int ccd_step(Scene& s, uint32_t active) {
 }
 
 const float* ccd_t(Scene& s) { return ((CcdState*)s.ccd_state.p)->t; }
+
+uint32_t ccd_launches(Scene& s) { return ((const CcdState*)s.ccd_out.p)->launch; }
 
 int ccd_results(Scene& s, float* t_out, uint32_t* cap_hits) {
   MG_CUDA(cudaStreamSynchronize(s.st));

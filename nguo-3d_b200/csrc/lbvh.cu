@@ -500,10 +500,10 @@ static int sort_impl(Lbvh* b, K* keys, uint32_t* vals, uint32_t n, int key_bits,
   MG_TRY(b->rs_hist.reserve(8 * 256));
   MG_TRY(b->rs_ofs.reserve(8 * 256));
   uint32_t ntiles = ceil_div(n, RS_TILE);
-  MG_TRY(b->rs_status.reserve((size_t)ntiles * 256));
+  MG_TRY(b->rs_status.grow((size_t)ntiles * 256));
   MG_TRY(b->rs_counter.reserve(8));
-  MG_TRY(b->rs_tmpk.reserve((size_t)n * sizeof(K)));
-  MG_TRY(b->rs_tmpv.reserve(n));
+  MG_TRY(b->rs_tmpk.grow((size_t)n * sizeof(K)));
+  MG_TRY(b->rs_tmpv.grow(n));
   MG_CUDA(cudaMemsetAsync(b->rs_hist.p, 0, 4 * 8 * 256, s));
   int sms = device_sm_count();
   k_rs_hist<K><<<std::min<uint32_t>(ceil_div(n, 256), sms * 8), 256, 0, s>>>(keys, n, passes, b->rs_hist.p);
@@ -519,7 +519,8 @@ static int sort_impl(Lbvh* b, K* keys, uint32_t* vals, uint32_t n, int key_bits,
     MG_CUDA(cudaMemsetAsync(b->rs_status.p, 0, 4 * (size_t)ntiles * 256, s));
     MG_CUDA(cudaMemsetAsync(b->rs_counter.p, 0, 4, s));
     k_onesweep<K><<<ntiles, RS_THREADS, 0, s>>>(kA, vA, kB, vB, n, 8 * p, b->rs_ofs.p + p * 256, b->rs_status.p,
-                                               b->rs_counter.p, b->status.p, b->rs_hist.p + p * 256);
+                                               b->rs_counter.p, b->err_sink ? b->err_sink : b->status.p,
+                                               b->rs_hist.p + p * 256);
     MG_CUDA(cudaGetLastError());
     std::swap(kA, kB);
     std::swap(vA, vB);

@@ -21,6 +21,7 @@ struct Lbvh {
   DevBuf<float> params;             // centroid lo.xyz, inv.xyz
   DevBuf<uint32_t> ord;
   DevBuf<uint32_t> status;
+  uint32_t* err_sink = nullptr;     // when set, the sort's wait-timeout bit goes here instead of status
   // radix-sort scratch
   DevBuf<uint32_t> rs_hist, rs_ofs, rs_status, rs_counter, rs_tmpv;
   DevBuf<unsigned char> rs_tmpk;
@@ -116,13 +117,23 @@ __device__ __forceinline__ bool lbvh_visit(const uint32_t* __restrict__ left, co
 // u_max <= max(2 rq, diag D, rq + farthest(cq, D)); and d0 >= the distance between the
 // query's box (qlo, qhi) and the subtree's position box. The subtree is skipped when
 // 1.3 u_bound < 0.98 distance (4% margin over 1.25 for rounding).
-template <class F>
-__device__ __forceinline__ bool lbvh_visit_ccd(const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
-                                               const float4* __restrict__ node, const float4* __restrict__ leaf,
-                                               const float4* __restrict__ dnode, const float4* __restrict__ dleaf,
-                                               const uint32_t* __restrict__ prim, uint32_t nt, float4 slo, float4 shi,
-                                               float4 qlo, float4 qhi, float3 cq, float rq, F&& f) {
-  auto enter = [&](const float4* pb, const float4* db) {
+//
+// The walk is resumable: start() and each step() hand back at most two leaf primitives, so
+// the lanes of a warp can advance their walks in lockstep and pool the leaves they reach
+// (the root solves then run on full warps). 64-entry stack; ok turns false on overflow.
+struct CcdWalk {
+  const uint32_t *left, *right, *prim;
+  const float4 *node, *leaf, *dnode, *dleaf;
+  uint32_t nt;
+  float4 slo, shi, qlo, qhi;
+  float3 cq;
+  float rq;
+  uint32_t stack[64];
+  int sp;
+  uint32_t cur;
+  bool ok;
+
+  __device__ __forceinline__ bool enter(const float4* pb, const float4* db) const {
     const float4 lo = __ldg(pb), hi = __ldg(pb + 1);
     if (!(slo.x <= hi.x && slo.y <= hi.y && slo.z <= hi.z && lo.x <= shi.x && lo.y <= shi.y && lo.z <= shi.z))
       return false;
@@ -138,28 +149,39 @@ __device__ __forceinline__ bool lbvh_visit_ccd(const uint32_t* __restrict__ left
     const float ex = dhi.x - dlo.x, ey = dhi.y - dlo.y, ez = dhi.z - dlo.z;
     const float u = fmaxf(fmaxf(2.f * rq, sqrtf(ex * ex + ey * ey + ez * ez)), rq + sqrtf(fx * fx + fy * fy + fz * fz));
     return !(1.3f * u < 0.98f * sqrtf(gap2));
-  };
-  if (nt == 0) return true;
-  if (nt == 1) {
-    if (enter(leaf, dleaf)) f(prim[0]);
-    return true;
   }
-  if (!enter(node, dnode)) return true;
-  uint32_t stack[64];
-  int sp = 0;
-  uint32_t cur = 0;
-  bool ok = true;
-  for (;;) {
-    uint32_t ch[2] = {__ldg(left + cur), __ldg(right + cur)};
+  // Begins the walk; returns the number of leaves written to out (the single leaf of a
+  // one-primitive tree) and sets done when nothing is left to visit.
+  __device__ __forceinline__ int start(bool& done, uint32_t out[2]) {
+    sp = 0;
+    cur = 0;
+    ok = true;
+    done = true;
+    if (nt == 0) return 0;
+    if (nt == 1) {
+      if (enter(leaf, dleaf)) {
+        out[0] = prim[0];
+        return 1;
+      }
+      return 0;
+    }
+    done = !enter(node, dnode);
+    return 0;
+  }
+  // Visits the children of the current node: entered leaves go to out (returned count),
+  // an entered inner child becomes the next node (the second is stacked).
+  __device__ __forceinline__ int step(bool& done, uint32_t out[2]) {
+    int n = 0;
+    const uint32_t ch[2] = {__ldg(left + cur), __ldg(right + cur)};
     uint32_t next = 0xffffffffu;
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
-      uint32_t x = ch[c];
+      const uint32_t x = ch[c];
       const bool lf = (x & 0x80000000u) != 0;
       const uint32_t i = x & 0x7fffffffu;
       if (!(lf ? enter(leaf + 2 * i, dleaf + 2 * i) : enter(node + 2 * i, dnode + 2 * i))) continue;
       if (lf) {
-        f(prim[i]);
+        out[n++] = prim[i];
       } else if (next == 0xffffffffu) {
         next = x;
       } else if (sp < 64) {
@@ -173,10 +195,10 @@ __device__ __forceinline__ bool lbvh_visit_ccd(const uint32_t* __restrict__ left
     } else if (sp > 0) {
       cur = stack[--sp];
     } else {
-      break;
+      done = true;
     }
+    return n;
   }
-  return ok;
-}
+};
 
 }  // namespace mg

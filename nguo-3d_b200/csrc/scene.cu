@@ -645,6 +645,9 @@ int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>
   MG_TRY(s.red.reserve(RED_STRIDE * s.ninst));
   MG_TRY(s.status.reserve(4));
   MG_CUDA(cudaMemsetAsync(s.status.p, 0, 16, st));
+  // the sorts and BVH builds of the step report a look-back timeout in the step's status
+  s.sorter.err_sink = s.status.p;
+  for (uint32_t k = 0; k < s.ninst; ++k) s.tri_bvh[k]->err_sink = s.edge_bvh[k]->err_sink = s.status.p;
   s.cap_c = std::max<uint32_t>(1u << 14, 4 * nv);
   MG_TRY(s.c_row_ptr.reserve(nv + 1));
   MG_TRY(s.c_count.reserve(4));

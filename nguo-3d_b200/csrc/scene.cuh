@@ -275,6 +275,7 @@ int self_intersections(Scene& s);  // piercing pairs per instance at s.x into re
 int ccd_step(Scene& s, uint32_t active);
 const float* ccd_t(Scene& s);
 int ccd_results(Scene& s, float* t_out, uint32_t* cap_hits);
+uint32_t ccd_launches(Scene& s);  // self-contact schedule launches of the last ccd_step (after ccd_results)
 
 }  // namespace mg
 

@@ -243,6 +243,11 @@ int scene_step(Scene& s, mguso_step_stats* out) {
                                                     s.dx.p);
     MG_CUDA(cudaGetLastError());
     MG_TRY(ccd_step(s, active));
+    std::vector<unsigned int> hccd;
+    if (trace_phases) {  // the self-contact traversals' leaf and root-solve counts
+      hccd.resize(RED_STRIDE * K);
+      MG_CUDA(cudaMemcpyAsync(hccd.data(), s.red.p, 4 * hccd.size(), cudaMemcpyDeviceToHost, st));
+    }
     MG_CUDA(cudaMemsetAsync(s.red.p, 0, 4 * RED_STRIDE * K, st));
     k_advance<<<std::min<uint32_t>(ceil_div(nv, 256), sms * 4), 256, 0, st>>>(s.x.p, s.dx.p, ccd_t(s), s.vinst.p, nv,
                                                                              s.red.p);
@@ -282,6 +287,14 @@ int scene_step(Scene& s, mguso_step_stats* out) {
       ph[4] = mark();
       std::fprintf(stderr, "[mguso]   ms: stencils %.3f assembly %.3f solve %.3f ccd+advance %.3f\n", ph[1] - ph[0],
                    ph[2] - ph[1], ph[3] - ph[2], ph[4] - ph[3]);
+      unsigned long long c[5] = {0, 0, 0, 0, 0};
+      for (uint32_t k = 0; k < K; ++k) {
+        for (int q = 0; q < 4; ++q) c[q] += hccd[RED_STRIDE * k + 5 + q];
+        c[4] += caps[k];
+      }
+      std::fprintf(stderr,
+                   "[mguso]   ccd: launches %u vt leaves %llu solves %llu ee leaves %llu solves %llu caps %llu\n",
+                   ccd_launches(s), c[0], c[1], c[2], c[3], c[4]);
     }
   }
   MG_CUDA(cudaMemsetAsync(s.red.p, 0, 4 * RED_STRIDE * K, st));

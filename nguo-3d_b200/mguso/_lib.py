@@ -98,6 +98,7 @@ def load() -> C.CDLL:
         "mguso_lbvh_stage_times": (i32, [vp, i32, vp]),
         "mguso_lbvh_build_query": (i32, [vp, vp, u32, vp, u32, i32, f32, vp, vp, vp, u64, P(u64)]),
         "mguso_radix_sort_pairs": (i32, [vp, vp, vp, u32, i32, vp]),
+        "mguso_radix_sort_status": (i32, [vp]),
         "mguso_radix_sort_pairs_noalloc": (i32, [vp, vp, u32, i32, vp]),
     }
     for name, (res, args) in sigs.items():

@@ -86,6 +86,11 @@ def radix_sort_pairs(ctx, keys_dev: int, vals_dev: int, n: int, key_bits: int, s
     check(ctx.lib.mguso_radix_sort_pairs(ctx.h, keys_dev, vals_dev, n, key_bits, stream))
 
 
+def radix_sort_status(ctx):
+    """Waits for the device; raises if the last radix_sort_pairs gave up its look-back wait."""
+    check(ctx.lib.mguso_radix_sort_status(ctx.h))
+
+
 # The allocation-free sort keeps its temporaries in a fixed device array of the library.
 NOALLOC_MAX_PAIRS = 1 << 18
 

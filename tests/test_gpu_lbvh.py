@@ -87,7 +87,8 @@ def test_onesweep_sort_stable(ctx, bits):
     import torch
     from mguso.lbvh import radix_sort_pairs
     rng = np.random.default_rng(7)
-    for n in (1, 3, 2047, 2048, 2049, 100_003, 3_000_000):
+    # sizes in the order of a growing buffer: each larger n reallocates the scratch
+    for n in (1, 3, 2047, 2048, 2049, 100_003, 1_054_816, 3_000_000, 1_044_128):
         if bits == 32:
             keys = rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32)
             keys[: n // 3] = keys[: n // 3] % 500  # duplicate-heavy prefix
@@ -98,7 +99,7 @@ def test_onesweep_sort_stable(ctx, bits):
             kt = torch.from_numpy(keys.view(np.int64)).cuda()
         vt = torch.arange(n, dtype=torch.int32, device="cuda")
         radix_sort_pairs(ctx, kt.data_ptr(), vt.data_ptr(), n, bits, torch.cuda.current_stream().cuda_stream)
-        torch.cuda.synchronize()
+        lbvh.radix_sort_status(ctx)  # no look-back wait gave up
         gk = kt.cpu().numpy().view(np.uint32 if bits == 32 else np.uint64)
         gv = vt.cpu().numpy().view(np.uint32)
         order = np.argsort(keys, kind="stable")
