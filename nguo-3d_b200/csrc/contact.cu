@@ -113,6 +113,7 @@ int build_bvhs(Scene& s, const float* x) {
   MG_TRY(aux_fork(s));
   int rc = MGUSO_OK;
   for (uint32_t k = 0; k < s.ninst && rc == MGUSO_OK; ++k) {
+    if (!((s.iter_active >> k) & 1u)) continue;  // an instance the batch no longer iterates
     const uint32_t t0 = s.inst_tri[k], e0 = s.inst_edge[k];
     rc = lbvh_build(s.tri_bvh[k].get(), x, s.nv, s.tris.p + 3 * (size_t)t0, s.inst_tri[k + 1] - t0, 30,
                     s.aux[(2 * k) % N_AUX]);
@@ -197,9 +198,9 @@ __global__ void k_side_best(BvhSet bv, const uint8_t* __restrict__ vinst, const 
                             const uint8_t* __restrict__ ctri, const uint8_t* __restrict__ svert,
                             const float* __restrict__ im, const uint32_t* __restrict__ ex_ptr,
                             const uint32_t* __restrict__ ex_list, uint32_t nv, float dhat,
-                            unsigned long long* __restrict__ best, uint32_t* __restrict__ status) {
+                            unsigned long long* __restrict__ best, uint32_t* __restrict__ status, uint32_t active) {
   uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= nv) return;
+  if (v >= nv || !((active >> vinst[v]) & 1u)) return;
   unsigned long long b = ~0ull;
   if (!svert[v] && im[v] > 0.f) {
     float4 lo, hi;
@@ -283,9 +284,9 @@ __global__ void k_vt_stencils(BvhSet bv, const uint8_t* __restrict__ vinst, cons
                               const uint32_t* __restrict__ ex_ptr, const uint32_t* __restrict__ ex_list,
                               const unsigned long long* __restrict__ best, const float* __restrict__ pn, int has_static,
                               uint32_t nv, float dhat, int mixed, Stencil* out, unsigned long long* keys, uint32_t* ids,
-                              unsigned long long* counter, uint32_t cap, uint32_t* status) {
+                              unsigned long long* counter, uint32_t cap, uint32_t* status, uint32_t active) {
   uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= nv) return;
+  if (v >= nv || !((active >> vinst[v]) & 1u)) return;
   float4 lo, hi;
   point_box(x, v, dhat, lo, hi);
   bool vmov = im[v] > 0.f;
@@ -319,12 +320,12 @@ __global__ void k_ee_stencils(BvhSet bv, const uint8_t* __restrict__ vinst, cons
                               const uint32_t* __restrict__ edges, const uint32_t* __restrict__ ee_tail,
                               const float* __restrict__ im, uint32_t ne, float search, float dhat, int mixed,
                               Stencil* out, unsigned long long* keys, uint32_t* ids, unsigned long long* counter,
-                              uint32_t cap, uint32_t* status) {
+                              uint32_t cap, uint32_t* status, uint32_t active) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ne) return;
   const uint32_t b0 = edges[2 * t], b1 = edges[2 * t + 1];
   const uint32_t k = vinst[b0];
-  if (t >= ee_tail[k]) return;
+  if (t >= ee_tail[k] || !((active >> k) & 1u)) return;
   float4 lo, hi;
   edge_box(x, b0, b1, search, lo, hi);
   const bool tmov = im[b0] > 0.f || im[b1] > 0.f;
@@ -360,7 +361,7 @@ int collect_stencils(Scene& s, uint32_t* nst_out) {
   if (s.has_static) {
     k_side_best<<<ceil_div(s.nv, 128), 128, 0, st>>>(tv, s.vinst.p, s.x.p, s.tris.p, s.collider_tri.p, s.static_vert.p,
                                                    s.inv_mass.p, s.ex_ptr.p, s.ex_list.p, s.nv, dhat, s.side_best.p,
-                                                   s.status.p);
+                                                   s.status.p, s.iter_active);
   }
   for (int attempt = 0; attempt < 4; ++attempt) {
     MG_TRY(s.stencils.reserve(s.cap_stencils));
@@ -372,11 +373,11 @@ int collect_stencils(Scene& s, uint32_t* nst_out) {
                                                      s.ex_ptr.p, s.ex_list.p, s.side_best.p, s.collider_pn.p,
                                                      s.has_static ? 1 : 0, s.nv, dhat, s.mixed ? 1 : 0, s.stencils.p,
                                                      s.st_keys.p, s.st_ids.p, s.counters.p, s.cap_stencils,
-                                                     s.status.p);
+                                                     s.status.p, s.iter_active);
     if (s.n_edge)
       k_ee_stencils<<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, s.vinst.p, s.x.p, s.edges.p, s.ee_tail.p, s.inv_mass.p, s.n_edge, dhat, dhat,
                                                            s.mixed ? 1 : 0, s.stencils.p, s.st_keys.p, s.st_ids.p,
-                                                           s.counters.p, s.cap_stencils, s.status.p);
+                                                           s.counters.p, s.cap_stencils, s.status.p, s.iter_active);
     MG_CUDA(cudaGetLastError());
     unsigned long long cnt = 0;
     MG_CUDA(cudaMemcpyAsync(&cnt, s.counters.p, 8, cudaMemcpyDeviceToHost, st));
@@ -1059,6 +1060,7 @@ int ccd_step(Scene& s, uint32_t active) {
     MG_TRY(aux_fork(s));
     int rc = MGUSO_OK;
     for (uint32_t k = 0; k < K && rc == MGUSO_OK; ++k) {
+      if (!((active >> k) & 1u)) continue;  // its self contact is not checked
       rc = lbvh_refit_disp(s.tri_bvh[k].get(), s.dx.p, s.tris.p + 3 * (size_t)s.inst_tri[k], s.aux[(2 * k) % N_AUX]);
       if (rc == MGUSO_OK)
         rc = lbvh_refit_disp(s.edge_bvh[k].get(), s.dx.p, s.edge_tris.p + 3 * (size_t)s.inst_edge[k],

@@ -95,6 +95,10 @@ struct mguso_schwarz {
   std::vector<uint8_t> h_dom_diag;
   mg::DevBuf<uint8_t> dom_diag;
   mg::DevBuf<float> vfac;
+  // each domain's instance; the factorisation skips the domains of instances outside
+  // `active` (their factors keep their last values; a batch step sets it per Newton iteration)
+  mg::DevBuf<uint8_t> dom_inst;
+  uint32_t active = 0xffffffffu;
   // Two-level Galerkin form (MultilevelSchwarz, linsolve.rs:534-666) when levels == 2: every
   // level-0 domain is a coarse node (three dofs), coarse domains are BFS groups of <= domain
   // coarse nodes over the coarse block graph, and each coarse domain's dense block of

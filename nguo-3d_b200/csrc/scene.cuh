@@ -168,6 +168,9 @@ struct Scene {
 
   // self-contact working set
   uint32_t cap_pairs = 0, cap_stencils = 0;
+  // the instances the current Newton iteration of a step works on (all outside a step): BVH
+  // builds, stencil collection and collider sides skip the others
+  uint32_t iter_active = 0xffffffffu;
   DevBuf<uint32_t> pairs;                   // 2 per candidate
   DevBuf<unsigned long long> counters;      // [0] vt pairs, [1] stencils, [2] ee candidates, [3] unique keys
   DevBuf<unsigned long long> side_best;     // per vertex (d2 bits << 32 | tri)

@@ -110,6 +110,14 @@ int schwarz_build(mguso_schwarz* s) {
   }
   s->fac_floats = off[s->ndom];
   MG_TRY(s->dom_diag.upload(s->h_dom_diag.data(), std::max<size_t>(s->h_dom_diag.size(), 1), a->ctx->stream));
+  // each domain's instance (the range of its first vertex), for factorisations that skip
+  // the instances a batch no longer iterates
+  std::vector<uint8_t> dom_inst(std::max<uint32_t>(s->ndom, 1), 0);
+  for (uint32_t d = 0; d < s->ndom; ++d) {
+    const uint32_t v = s->h_dom_verts[s->h_dom_start[d]];
+    dom_inst[d] = (uint8_t)(std::upper_bound(ranges.begin(), ranges.end(), v) - ranges.begin() - 1);
+  }
+  MG_TRY(s->dom_inst.upload(dom_inst.data(), dom_inst.size(), a->ctx->stream));
   MG_TRY(s->vfac.reserve(6 * (size_t)std::max<uint32_t>(nb, 1)));
   cudaStream_t st = a->ctx->stream;
   MG_TRY(s->dom_start.upload(s->h_dom_start.data(), s->h_dom_start.size(), st));
@@ -207,11 +215,12 @@ int schwarz_build_coarse(mguso_schwarz* s) {
 // Factorisation: one CTA per domain, FP64 in shared memory, in place in one m x ld buffer
 // (ld = m + 1, so column walks are free of bank conflicts):
 //   1. gather the dense block and add the reference's diagonal floor;
-//   2. right-looking Cholesky on the lower triangle. The k-th pivot is the k-th Schur
-//      complement diagonal, the value the reference's row-by-row Cholesky tests against
-//      1e-14 (linsolve.rs:88-92), so the same blocks fall back to the diagonal;
-//   3. W = L^-1, one thread per column (forward substitution), written transposed into the
-//      upper triangle.
+//   2. blocked right-looking Cholesky on the lower triangle over 32-column panels. The k-th
+//      pivot is the k-th Schur complement diagonal, the value the reference's row-by-row
+//      Cholesky tests against 1e-14 (linsolve.rs:88-92), so the same blocks fall back to the
+//      diagonal;
+//   3. W = L^-1, the diagonal blocks inverted per panel, the others by block forward
+//      substitution, written transposed into the upper triangle.
 // Stored: W in FP32 as swizzled tiles (layout above). The apply forms z = W^T (W r), so
 // the FP32 preconditioner W~^T W~ is symmetric positive definite for any rounding of W.
 // (An explicitly stored FP32 inverse is not: with stiff seams a domain block reaches a
@@ -251,6 +260,29 @@ __device__ double factor_amax(const double* A, int ld, int m, const double* diag
   return r > 0.0 ? r : 1.0;
 }
 
+// acc[r][c] += sum over k in [k0, k1) of a(i0 + r, k) b(k, j0 + c): a 4 x 4 register tile of
+// a small FP64 product in shared memory (a and b return 0 outside their structure)
+__device__ __forceinline__ void mt4_zero(double (&acc)[4][4]) {
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
+}
+template <class FA, class FB>
+__device__ __forceinline__ void mt4(double (&acc)[4][4], int i0, int j0, int k0, int k1, FA&& a, FB&& b) {
+  for (int k = k0; k < k1; ++k) {
+    double av[4], bv[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) av[r] = a(i0 + r, k);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) bv[c] = b(k, j0 + c);
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[r][c] = fma(av[r], bv[c], acc[r][c]);
+  }
+}
+
 // Steps 2-3 of the factorisation and the store, on the dense block A (m x m, leading
 // dimension ld, FP64 shared memory, lower triangle filled) of one domain: the reference's
 // diagonal floor, right-looking Cholesky with its pivot test (falling back to the floored
@@ -274,39 +306,162 @@ __device__ void factor_dense_store(double* A, int ld, int m, double* dinv, doubl
     A[k * ld + k] += s_floor;
     diag0[k] = A[k * ld + k];
   }
-  // the strict upper triangle becomes V (below), starting from the identity's zeros
+  // the strict upper triangle receives W's off-diagonal entries (W_ij at A[j * ld + i], i > j)
   for (int e = tid; e < m * m; e += nt) {
     const int i = e / m, j = e - i * m;
     if (j > i) A[i * ld + j] = 0.0;
   }
   __syncthreads();
-  // Cholesky A = U P U^T (U unit lower, U_ik = A_ik^(k) / p_k from the k-th Schur
-  // complement, P the pivots; L = U P^1/2) and, in the same sweep, V = U^-1 by row
-  // elimination: at step k, row i > k of V loses U_ik times row k, which is final by then.
-  // The Schur update writes the lower triangle (columns k < j <= i), the elimination the
-  // upper one (V_ij at A[j * ld + i], columns j <= k; V_kk = 1 is implicit), so one barrier
-  // per step suffices. Afterwards W = L^-1 = P^-1/2 V.
+  // Blocked right-looking Cholesky A = L L^T over 32-column panels, L in the lower triangle:
+  // per panel, warp 0 factors the diagonal block column by column (the k-th pivot is the
+  // k-th Schur complement diagonal, tested against 1e-14 as the reference's row-by-row
+  // Cholesky does) and inverts it (W_PP = L_PP^-1, one lane per column); then the rows below
+  // become L_IP = A_IP W_PP^T and the trailing blocks lose L_IP L_JP^T, as 4 x 4 register
+  // tiles per thread. About four barriers per panel instead of one per column.
   const int tx = tid & 31, ty = tid >> 5;
-  for (int k = 0; k < m; ++k) {
-    const double p = A[k * ld + k];
-    if (!(p > 1e-14)) {  // uniform: every thread reads the same pivot
-      if (tid == 0) s_fail = 1;
-      break;
-    }
-    const double ip = 1.0 / p;
-    for (int i = k + 1 + ty; i < m; i += 8) {
-      const double aik = A[i * ld + k] * ip;
-      for (int j = k + 1 + tx; j <= i; j += 32) A[i * ld + j] -= aik * A[j * ld + k];
-      for (int j = tx; j <= k; j += 32) A[j * ld + i] -= aik * (j == k ? 1.0 : A[j * ld + k]);
-    }
-    if (tid == 0) {
-      const double l = sqrt(p);
-      dinv[k] = 1.0 / l;
+  const int T = (m + 31) >> 5;
+  for (int P = 0; P < T; ++P) {
+    const int c0 = 32 * P, nb = min(32, m - c0), r0 = c0 + nb, R = m - r0;
+    if (ty == 0) {
+      // the diagonal block in registers, lane i holding row i; column k of the factor is
+      // broadcast by shuffles, so a step costs no shared-memory round trips
+      double row[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) row[j] = (tx < nb && j <= tx) ? A[(c0 + tx) * ld + c0 + j] : 0.0;
+      bool fail = false;
+#pragma unroll
+      for (int k = 0; k < 32; ++k) {
+        if (k < nb && !fail) {  // uniform
+          const double p = __shfl_sync(0xffffffffu, row[k], k);
+          if (!(p > 1e-14)) {  // every lane sees the same pivot
+            fail = true;
+          } else {
+            const double il = rsqrt(p), lkk = p * il;  // 1 / L_kk and L_kk
+            const double lik = tx > k ? row[k] * il : (tx == k ? lkk : 0.0);
+            if (tx >= k) row[k] = lik;
+            if (tx == k) dinv[c0 + k] = il;
+#pragma unroll
+            for (int j = k + 1; j < 32; ++j) {
+              const double ljk = __shfl_sync(0xffffffffu, lik, j);
+              if (tx >= j) row[j] = fma(-lik, ljk, row[j]);
+            }
+          }
+        }
+      }
+      if (!fail) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+          if (tx < nb && j <= tx) A[(c0 + tx) * ld + c0 + j] = row[j];
+        __syncwarp();
+        // W_PP = L_PP^-1, lane j holding column j: W_jj = 1 / L_jj and, for i > j,
+        // W_ij = -(sum_{j <= q < i} L_iq W_qj) / L_ii, L's rows read as broadcasts
+        double wcol[32];
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+          if (i < nb) {
+            const double* li = A + (size_t)(c0 + i) * ld + c0;
+            double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+            for (int q = 0; q < i; ++q) {
+              const double t = q >= tx ? wcol[q] : 0.0;
+              if (q & 1)
+                a1 = fma(li[q], t, a1);
+              else
+                a0 = fma(li[q], t, a0);
+            }
+            const double di = dinv[c0 + i];
+            wcol[i] = i == tx ? di : (i > tx ? -(a0 + a1) * di : 0.0);
+          } else {
+            wcol[i] = 0.0;
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < 32; ++i)
+          if (i > tx && i < nb) A[(c0 + tx) * ld + c0 + i] = wcol[i];
+      }
+      if (tx == 0) s_fail = fail ? 1 : 0;
     }
     __syncthreads();
+    if (s_fail) break;  // uniform
+    if (R > 0) {
+      // panel: L_ij = sum_{c <= j} A_ic W_jc for the rows below (nb = 32 here)
+      const int ntr = (R + 3) >> 2, items = ntr * 8;
+      double acc[4][4];
+      const int t = tid;
+      const int ti = t >> 3, tj = t & 7;
+      const int i0 = r0 + 4 * ti, j0 = 4 * tj;
+      const bool mine = t < items;
+      if (mine) {
+        mt4_zero(acc);
+        mt4(acc, i0, j0, 0, j0 + 4,
+            [&](int i, int c) { return i < m ? A[i * ld + c0 + c] : 0.0; },
+            [&](int c, int j) { return c == j ? dinv[c0 + j] : (c < j ? A[(c0 + c) * ld + c0 + j] : 0.0); });
+      }
+      __syncthreads();
+      if (mine)
+        for (int r = 0; r < 4; ++r)
+          if (i0 + r < m)
+            for (int c = 0; c < 4; ++c) A[(i0 + r) * ld + c0 + j0 + c] = acc[r][c];
+      __syncthreads();
+      // trailing update of the lower triangle: A_ij -= sum_c L_ic L_jc (i >= j >= r0)
+      const int pairs = ntr * (ntr + 1) / 2;
+      for (int u = tid; u < pairs; u += nt) {
+        int a = (int)((sqrtf(8.f * (float)u + 1.f) - 1.f) * 0.5f);
+        while ((a + 1) * (a + 2) / 2 <= u) ++a;
+        while (a * (a + 1) / 2 > u) --a;
+        const int b = u - a * (a + 1) / 2;  // tile row a >= tile column b
+        const int ii = r0 + 4 * a, jj = r0 + 4 * b;
+        double up[4][4];
+        mt4_zero(up);
+        mt4(up, ii, jj, 0, 32, [&](int i, int c) { return i < m ? A[i * ld + c0 + c] : 0.0; },
+            [&](int c, int j) { return j < m ? A[j * ld + c0 + c] : 0.0; });
+        for (int r = 0; r < 4; ++r)
+          for (int c = 0; c < 4; ++c)
+            if (ii + r < m && jj + c <= ii + r) A[(ii + r) * ld + jj + c] -= up[r][c];
+      }
+      __syncthreads();
+    }
   }
   __syncthreads();
-  const int T = (m + 31) / 32, nfl = T * (T + 1) / 2 * TILE_FLOATS;
+  if (!s_fail) {
+    // off-diagonal blocks of W = L^-1, block row by block row:
+    // W_IJ = -W_II S_IJ with S_IJ = sum_{J <= K < I} L_IK W_KJ; S is formed in W_IJ's place
+    for (int I = 1; I < T; ++I) {
+      const int i0 = 32 * I, ni = min(32, m - i0), ntr = (ni + 3) >> 2, items = I * ntr * 8;
+      for (int u = tid; u < items; u += nt) {
+        const int J = u / (ntr * 8), rem = u - J * ntr * 8, ti = rem >> 3, tj = rem & 7;
+        const int j0 = 32 * J, ia = i0 + 4 * ti, ja = j0 + 4 * tj;
+        double acc[4][4];
+        mt4_zero(acc);
+        mt4(acc, ia, ja, j0, i0, [&](int i, int k) { return i < m ? A[i * ld + k] : 0.0; },
+            [&](int k, int j) { return k == j ? dinv[k] : (k > j ? A[j * ld + k] : 0.0); });
+        for (int r = 0; r < 4; ++r)
+          if (ia + r < m)
+            for (int c = 0; c < 4; ++c) A[(ja + c) * ld + ia + r] = acc[r][c];
+      }
+      __syncthreads();
+      double res[4][4];
+      int ia = 0, ja = 0;
+      const bool mine = tid < items;
+      if (mine) {
+        const int J = tid / (ntr * 8), rem = tid - J * ntr * 8, ti = rem >> 3, tj = rem & 7;
+        ia = i0 + 4 * ti;
+        ja = 32 * J + 4 * tj;
+        mt4_zero(res);
+        mt4(res, ia, ja, i0, min(m, ia + 4),
+            [&](int i, int q) { return (i < m && q <= i) ? (q == i ? dinv[i] : A[q * ld + i]) : 0.0; },
+            [&](int q, int j) { return A[j * ld + q]; });
+      }
+      __syncthreads();
+      if (mine)
+        for (int r = 0; r < 4; ++r)
+          if (ia + r < m)
+            for (int c = 0; c < 4; ++c) A[(ja + c) * ld + ia + r] = -res[r][c];
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  const int nfl = T * (T + 1) / 2 * TILE_FLOATS;
   if (s_fail) {
     // reference fallback: L = diag(sqrt(ad_pp)) (1 where ad_pp <= 1e-14), i.e.
     // W = diag(1 / sqrt(ad_pp))
@@ -322,9 +477,7 @@ __device__ void factor_dense_store(double* A, int ld, int m, double* dinv, doubl
     if (tid == 0) atomicOr(status, 1u << 8);
     return;
   }
-  // W_ij = dinv_i V_ij (j < i) and W_ii = dinv_i, in place at A[j * ld + i]
-  for (int j = ty; j < m; j += 8)
-    for (int i = j + tx; i < m; i += 32) A[j * ld + i] = i == j ? dinv[i] : A[j * ld + i] * dinv[i];
+  for (int i = tid; i < m; i += nt) A[i * ld + i] = dinv[i];  // W's diagonal joins its upper-triangle copy
   __syncthreads();
   const double inv_sc = scaled ? 1.0 / factor_amax(A, ld, m, diag0, false) : 1.0;
   if (scaled && tid == 0) *scale_out = (float)(1.0 / inv_sc);
@@ -382,16 +535,17 @@ __device__ void vertex_factor(double* a, float* __restrict__ w6, uint32_t* statu
 }
 
 template <class TS>
-__global__ void __launch_bounds__(FACTOR_THREADS) k_schwarz_factor(
+__global__ void __launch_bounds__(FACTOR_THREADS, 2) k_schwarz_factor(
     const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ col, const float* __restrict__ val,
     const uint32_t* __restrict__ dom_start, const uint32_t* __restrict__ dom_verts,
     const uint32_t* __restrict__ dom_of, const uint32_t* __restrict__ loc, const uint64_t* __restrict__ fac_off,
     TS* __restrict__ fac, float* __restrict__ fac_scale, uint32_t* status, const uint32_t* __restrict__ c_rp,
     const uint32_t* __restrict__ c_col, const float* __restrict__ c_val, const uint8_t* __restrict__ dom_diag,
-    float* __restrict__ vfac) {
+    float* __restrict__ vfac, const uint8_t* __restrict__ dom_inst, uint32_t active) {
   // FP16 tiles hold W / scale (scale: the domain's largest |W|); FP32 tiles hold W
   extern __shared__ __align__(16) double sA[];
   const uint32_t d = blockIdx.x;
+  if (!((active >> dom_inst[d]) & 1u)) return;  // an instance the batch no longer iterates
   const uint32_t vs = dom_start[d], nvd = dom_start[d + 1] - vs;
   if (dom_diag[d]) {
     for (uint32_t p = threadIdx.x; p < nvd; p += blockDim.x) {
@@ -507,11 +661,13 @@ int schwarz_factor_with(mguso_schwarz* s, const uint32_t* c_rp, const uint32_t* 
   if (s->half)
     k_schwarz_factor<__half><<<s->ndom, FACTOR_THREADS, smem, st>>>(
         a->row_ptr.p, a->col.p, a->val.p, s->dom_start.p, s->dom_verts.p, s->dom_of.p, s->loc.p, s->fac_off.p,
-        s->fac_h.p, s->fac_scale.p, s->status.p, c_col ? c_rp : nullptr, c_col, c_val, s->dom_diag.p, s->vfac.p);
+        s->fac_h.p, s->fac_scale.p, s->status.p, c_col ? c_rp : nullptr, c_col, c_val, s->dom_diag.p, s->vfac.p,
+        s->dom_inst.p, s->active);
   else
     k_schwarz_factor<float><<<s->ndom, FACTOR_THREADS, smem, st>>>(
         a->row_ptr.p, a->col.p, a->val.p, s->dom_start.p, s->dom_verts.p, s->dom_of.p, s->loc.p, s->fac_off.p,
-        s->fac.p, nullptr, s->status.p, c_col ? c_rp : nullptr, c_col, c_val, s->dom_diag.p, s->vfac.p);
+        s->fac.p, nullptr, s->status.p, c_col ? c_rp : nullptr, c_col, c_val, s->dom_diag.p, s->vfac.p,
+        s->dom_inst.p, s->active);
   MG_CUDA(cudaGetLastError());
   if (s->levels == 2 && s->ncdom) {
     size_t smem1 = sizeof(double) * ((size_t)s->max_m1 * (s->max_m1 + 1) + 2 * (size_t)s->max_m1);

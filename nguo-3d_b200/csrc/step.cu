@@ -135,7 +135,11 @@ static void fused_stats(const Scene& s, const PcgInstResult* r, mguso_lin_stats*
 static int linear_solve(Scene& s, uint32_t active, mguso_lin_stats* ls, bool* deferred = nullptr) {
   cudaStream_t st = s.st;
   if (s.schwarz) {
-    MG_TRY(schwarz_factor_with(s.schwarz.get(), s.c_row_ptr.p, s.c_col.p, s.c_val.p, st));
+    // only the instances still iterating need their domains factored
+    s.schwarz->active = active;
+    const int rc = schwarz_factor_with(s.schwarz.get(), s.c_row_ptr.p, s.c_col.p, s.c_val.p, st);
+    s.schwarz->active = 0xffffffffu;
+    MG_TRY(rc);
   } else {
     MG_TRY(blockjacobi_factor(s.A.get(), s.bjinv.p, st));
   }
@@ -214,7 +218,13 @@ int scene_step(Scene& s, mguso_step_stats* out) {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
   };
   std::vector<unsigned int> hred(RED_STRIDE * K);
+  // the instances each Newton iteration works on; every exit restores "all"
+  struct ActiveGuard {
+    Scene& s;
+    ~ActiveGuard() { s.iter_active = 0xffffffffu; }
+  } active_guard{s};
   for (uint32_t it = 0; it < cap && active; ++it) {
+    s.iter_active = active;
     for (uint32_t k = 0; k < K; ++k)
       if ((active >> k) & 1u) stats[k].newton_iters++;
     uint32_t nst = 0;
@@ -297,6 +307,7 @@ int scene_step(Scene& s, mguso_step_stats* out) {
                    ccd_launches(s), c[0], c[1], c[2], c[3], c[4]);
     }
   }
+  s.iter_active = 0xffffffffu;
   MG_CUDA(cudaMemsetAsync(s.red.p, 0, 4 * RED_STRIDE * K, st));
   k_check_finite<<<ceil_div(nv, 256), 256, 0, st>>>(s.x.p, s.inv_mass.p, s.vinst.p, nv, s.p.floor_y, s.red.p);
   k_commit<<<ceil_div(nv, 256), 256, 0, st>>>(s.x.p, s.x0.p, s.v.p, s.inv_mass.p, s.vinst.p, nv, 1.0f / h, s.red.p);
