@@ -402,17 +402,20 @@ def count_launches(fn):
         return None
 
 
-def time_steps(solver, steps, stream, dist):
-    """Device time (ms) of `steps` steps on the solver's stream, CUDA events, barrier-bracketed."""
+def time_steps(solver, steps, stream, dist, name="timed"):
+    """Device time (ms) of `steps` steps on the solver's stream, CUDA events, barrier-bracketed.
+    The steps run inside an NVTX range `name` (a profiler can restrict itself to it)."""
     import torch
 
     torch.cuda.synchronize()
     dist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push(name)
     e0.record(stream)
     st = solver.step(steps)
     e1.record(stream)
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     dist.barrier()
     torch.cuda.synchronize()
@@ -504,7 +507,7 @@ def run_batch(args, dist: Dist):
     b = mguso.ImplicitBatch(ctx, scs, "mixed")
     b.step(args.warmup)
     p_w, v_w = b.positions.copy(), b.velocities.copy()
-    ms_b, st_b = time_steps(b, args.steps, stream, dist)
+    ms_b, st_b = time_steps(b, args.steps, stream, dist, "batch")
     clk = clocks.stop()
     # batched, mixed precision with FP32 factor tiles (the apply in FP32 storage), same steps
     scs32 = [dict(sc, params=dict(sc["params"], factor_storage=1)) for sc in scs]

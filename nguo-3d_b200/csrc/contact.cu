@@ -651,7 +651,7 @@ __device__ __forceinline__ void walk_init(CcdWalk& w, const BvhSet& bs, uint32_t
 
 // Vertex-triangle passes: lane v walks the triangles near vertex v.
 template <class R>
-__global__ void __launch_bounds__(CCD_WARPS * 32) k_ccd_vt(
+__global__ void __launch_bounds__(CCD_WARPS * 32, 4) k_ccd_vt(
     BvhSet bv, const CcdPass* __restrict__ cpp, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
     const float* __restrict__ dx, const uint32_t* __restrict__ tris, const uint8_t* __restrict__ ctri,
     const float* __restrict__ im, const uint32_t* __restrict__ ex_ptr, const uint32_t* __restrict__ ex_list,
@@ -734,7 +734,7 @@ __global__ void __launch_bounds__(CCD_WARPS * 32) k_ccd_vt(
 // Edge-edge passes. As k_ee_stencils: lane j takes the pairs (j, i) with i > j (the
 // lower-indexed edge first), and an edge of its instance's static tail skips its walk.
 template <class R>
-__global__ void __launch_bounds__(CCD_WARPS * 32) k_ccd_ee(
+__global__ void __launch_bounds__(CCD_WARPS * 32, 4) k_ccd_ee(
     BvhSet bv, const CcdPass* __restrict__ cpp, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
     const float* __restrict__ dx, const uint32_t* __restrict__ edges, const uint32_t* __restrict__ ee_tail,
     const float* __restrict__ im, uint32_t ne, uint32_t max_iter, unsigned int* __restrict__ red,
