@@ -195,10 +195,12 @@ __global__ void __launch_bounds__(128) k_shell(const uint32_t* __restrict__ act,
                                                const uint32_t* __restrict__ sv, const float* __restrict__ dm,
                                                const float* __restrict__ area, const float* __restrict__ mu,
                                                const float* __restrict__ lam, float eps, const float* __restrict__ x,
-                                               float* __restrict__ cb, float* __restrict__ ge, int exact) {
+                                               float* __restrict__ cb, float* __restrict__ ge, int exact,
+                                               const uint8_t* __restrict__ vinst, uint32_t active) {
   uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
   uint32_t e = act[q];
+  if (!((active >> vinst[sv[3 * e]]) & 1u)) return;  // an instance the batch no longer iterates
   V3<float> p[3] = {ld3<float>(x, sv[3 * e]), ld3<float>(x, sv[3 * e + 1]), ld3<float>(x, sv[3 * e + 2])};
   M2<float> D{dm[4 * e], dm[4 * e + 1], dm[4 * e + 2], dm[4 * e + 3]};
   V3<float> g[3];
@@ -228,10 +230,11 @@ __global__ void __launch_bounds__(128) k_shell(const uint32_t* __restrict__ act,
 // ---- hinges ----------------------------------------------------------------------------------
 __global__ void k_hinge(const uint32_t* __restrict__ act, uint32_t n, const uint32_t* __restrict__ hv,
                         const float* __restrict__ rest, float kb, const float* __restrict__ x, float* __restrict__ cb,
-                        float* __restrict__ ge, int exact) {
+                        float* __restrict__ ge, int exact, const uint8_t* __restrict__ vinst, uint32_t active) {
   uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
   uint32_t e = act[q];
+  if (!((active >> vinst[hv[4 * e]]) & 1u)) return;  // an instance the batch no longer iterates
   V3<float> p[4];
   for (int a = 0; a < 4; ++a) p[a] = ld3<float>(x, hv[4 * e + a]);
   float theta = dihedral_angle<float>(p);
@@ -239,9 +242,16 @@ __global__ void k_hinge(const uint32_t* __restrict__ act, uint32_t n, const uint
   dihedral_grad<float>(p, g);
   float kwt = kb * 1.0f;  // hinge weight w = 1 (bending.rs:150-156)
   float gval = theta - rest[e];
-  float* gg = ge + 12 * (size_t)e;
+  // the hinge's 12 gradient entries and 144 block entries are 16-byte aligned runs (48 e and
+  // 576 e bytes): stored as float4, a quarter of the store instructions of scalar stores
+  float gv[12];
+#pragma unroll
   for (int a = 0; a < 4; ++a)
-    for (int c = 0; c < 3; ++c) gg[3 * a + c] = kwt * gval * g[a][c];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) gv[3 * a + c] = kwt * gval * g[a][c];
+  float4* gg4 = reinterpret_cast<float4*>(ge + 12 * (size_t)e);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) gg4[i] = make_float4(gv[4 * i], gv[4 * i + 1], gv[4 * i + 2], gv[4 * i + 3]);
   float* blk = cb + 144 * (size_t)e;
   if (exact) {
     // k (grad theta grad theta^T + (theta - theta0) hess theta), hess theta from FP64
@@ -272,18 +282,27 @@ __global__ void k_hinge(const uint32_t* __restrict__ act, uint32_t n, const uint
           for (int c = 0; c < 3; ++c) blk[9 * (4 * a + b) + 3 * r + c] = (float)(kwt * H[12 * (3 * a + r) + 3 * b + c]);
     return;
   }
-  for (int a = 0; a < 4; ++a)
-    for (int b = 0; b < 4; ++b)
-      for (int r = 0; r < 3; ++r)
-        for (int c = 0; c < 3; ++c) blk[9 * (4 * a + b) + 3 * r + c] = kwt * g[a][r] * g[b][c];
+  float4* blk4 = reinterpret_cast<float4*>(blk);
+#pragma unroll
+  for (int i = 0; i < 36; ++i) {
+    float v4[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int f = 4 * i + u, ab = f / 9, rc = f - 9 * ab;  // block (a, b), entry (r, c)
+      const int a = ab >> 2, b = ab & 3, r = rc / 3, c = rc - 3 * r;
+      v4[u] = kwt * g[a][r] * g[b][c];
+    }
+    blk4[i] = make_float4(v4[0], v4[1], v4[2], v4[3]);
+  }
 }
 
 // ---- gathers ---------------------------------------------------------------------------------
 __global__ void k_gather_blocks(const uint32_t* __restrict__ slot_ptr, const uint32_t* __restrict__ slot_list,
                                 const float* __restrict__ cb, uint32_t nslots, uint32_t nnz_s,
-                                float* __restrict__ vals, float* __restrict__ valp) {
+                                float* __restrict__ vals, float* __restrict__ valp,
+                                const uint8_t* __restrict__ slot_inst, uint32_t active) {
   uint32_t sl = blockIdx.x * blockDim.x + threadIdx.x;
-  if (sl >= nslots) return;
+  if (sl >= nslots || !((active >> slot_inst[sl]) & 1u)) return;
   float acc[9];
 #pragma unroll
   for (int k = 0; k < 9; ++k) acc[k] = 0.f;
@@ -298,9 +317,10 @@ __global__ void k_gather_blocks(const uint32_t* __restrict__ slot_ptr, const uin
 }
 
 __global__ void k_gather_grad(const uint32_t* __restrict__ gv_ptr, const uint32_t* __restrict__ gv_list,
-                              const float* __restrict__ ge, uint32_t nv, float* __restrict__ grad) {
+                              const float* __restrict__ ge, uint32_t nv, float* __restrict__ grad,
+                              const uint8_t* __restrict__ vinst, uint32_t active) {
   uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= nv) return;
+  if (v >= nv || !((active >> vinst[v]) & 1u)) return;
   float a0 = 0.f, a1 = 0.f, a2 = 0.f;
   for (uint32_t j = gv_ptr[v]; j < gv_ptr[v + 1]; ++j) {
     const float* g = ge + 3 * (size_t)gv_list[j];
@@ -355,10 +375,12 @@ int assemble_elastic(Scene& s) {
     if (s.n_shell)
       k_shell<<<grid(s.n_shell), 128, 0, st>>>(all.p, s.n_shell, s.shell_v.p, s.shell_dm.p, s.shell_area.p,
                                                s.shell_mu.p, s.shell_lam.p, s.p.eiganalysis_eps, s.x.p,
-                                               cb + 9 * s.cb_shell, ge + 3 * s.gb_shell, ex_shell);
+                                               cb + 9 * s.cb_shell, ge + 3 * s.gb_shell, ex_shell, s.vinst.p,
+                                               0xffffffffu);
     if (s.n_hinge)
       k_hinge<<<grid(s.n_hinge), 128, 0, st>>>(all.p, s.n_hinge, s.hinge_v.p, s.hinge_rest.p, s.p.bend_stiffness,
-                                               s.x.p, cb + 9 * s.cb_hinge, ge + 3 * s.gb_hinge, ex_hinge);
+                                               s.x.p, cb + 9 * s.cb_hinge, ge + 3 * s.gb_hinge, ex_hinge,
+                                               s.vinst.p, 0xffffffffu);
     MG_CUDA(cudaGetLastError());
     MG_CUDA(cudaStreamSynchronize(st));
     s.static_done = true;
@@ -377,16 +399,18 @@ int assemble_elastic(Scene& s) {
     if (s.n_act_shell)
       k_shell<<<grid(s.n_act_shell), 128, 0, st>>>(s.act_shell.p, s.n_act_shell, s.shell_v.p, s.shell_dm.p,
                                                    s.shell_area.p, s.shell_mu.p, s.shell_lam.p, s.p.eiganalysis_eps,
-                                                   s.x.p, cb + 9 * s.cb_shell, ge + 3 * s.gb_shell, ex_shell);
+                                                   s.x.p, cb + 9 * s.cb_shell, ge + 3 * s.gb_shell, ex_shell, s.vinst.p,
+                                               s.iter_active);
     if (s.n_act_hinge)
       k_hinge<<<grid(s.n_act_hinge), 128, 0, st>>>(s.act_hinge.p, s.n_act_hinge, s.hinge_v.p, s.hinge_rest.p,
-                                                   s.p.bend_stiffness, s.x.p, cb + 9 * s.cb_hinge, ge + 3 * s.gb_hinge, ex_hinge);
+                                                   s.p.bend_stiffness, s.x.p, cb + 9 * s.cb_hinge, ge + 3 * s.gb_hinge, ex_hinge,
+                                               s.vinst.p, s.iter_active);
   }
   MG_CUDA(cudaGetLastError());
   uint32_t nslots = s.Ps.nnz + s.Pp.nnz;
   k_gather_blocks<<<grid(nslots), 128, 0, st>>>(s.slot_ptr.p, s.slot_list.p, cb, nslots, s.Ps.nnz, s.A->val.p,
-                                                s.valp.p);
-  k_gather_grad<<<grid(s.nv), 128, 0, st>>>(s.gv_ptr.p, s.gv_list.p, ge, s.nv, s.grad.p);
+                                                s.valp.p, s.slot_inst.p, s.iter_active);
+  k_gather_grad<<<grid(s.nv), 128, 0, st>>>(s.gv_ptr.p, s.gv_list.p, ge, s.nv, s.grad.p, s.vinst.p, s.iter_active);
   k_pinned_identity<<<grid(s.nv), 128, 0, st>>>(s.Ps.row_ptr.p, s.Ps.col.p, s.pinned.p, s.nv, s.A->val.p);
   MG_CUDA(cudaGetLastError());
   return MGUSO_OK;

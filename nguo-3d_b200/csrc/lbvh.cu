@@ -649,10 +649,11 @@ int lbvh_query_points(Lbvh* b, const float* pts, uint32_t np, float dhat, uint32
 // radix_sort_pairs, with its temporaries in one fixed file-scope device array instead of
 // buffers that grow on demand.
 //
-// Differences from radix_sort_pairs: every digit pass runs (no host read-back of the
-// histogram to skip passes whose digit is constant; such a pass is the identity for a
-// stable sort, so the output is the same), and the call waits for the sort to finish so it
-// can report a look-back timeout from the scratch's error word.
+// Differences from radix_sort_pairs: every digit pass runs the full scatter (radix_sort_pairs
+// turns a pass whose digit is the same for every key into a tile copy, found on the device;
+// such a pass is the identity for a stable sort, so the output is the same), and the call
+// waits for the sort to finish so it can report a look-back timeout from the scratch's
+// error word.
 // ---------------------------------------------------------------------------------------
 constexpr uint32_t NOALLOC_MAX_PAIRS = 1u << 18;  // 262 144 pairs
 constexpr size_t NA_TMPK = 0;                                         // u64 keys, ping-pong

@@ -294,10 +294,11 @@ __global__ void __launch_bounds__(FR_THREADS, 4) k_fr_rows_sell(FusedArgs a, con
 
 // Ps values into the sliced-ELL copy (after every assembly; padding slots stay zero)
 __global__ void k_sell_pack(const float* __restrict__ val, const uint32_t* __restrict__ pos, uint32_t nnz,
-                            float* __restrict__ sv) {
+                            float* __restrict__ sv, const uint8_t* __restrict__ slot_inst, uint32_t active) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= 9 * nnz) return;
   const uint32_t k = i / 9, q = i - 9 * k;
+  if (!((active >> slot_inst[k]) & 1u)) return;  // an instance the batch no longer iterates
   sv[pos[k] + 32 * q] = val[i];
 }
 
@@ -1031,7 +1032,8 @@ static int fused_prepare(Scene& s, const uint32_t* h_inst_row, uint32_t K, uint3
   if (s.fr_rows_variant == ROWS_SELL) {
     if (!s.sell_built) MG_TRY(sell_build(s));
     // the system's current values into the sliced-ELL copy
-    k_sell_pack<<<ceil_div(9 * (size_t)s.Ps.nnz, 256), 256, 0, st>>>(s.A->val.p, s.sell_pos.p, s.Ps.nnz, s.sell_val.p);
+    k_sell_pack<<<ceil_div(9 * (size_t)s.Ps.nnz, 256), 256, 0, st>>>(s.A->val.p, s.sell_pos.p, s.Ps.nnz, s.sell_val.p,
+                                                                    s.slot_inst.p, s.iter_active);
     MG_CUDA(cudaGetLastError());
     a.sell_base = s.sell_base.p;
     a.sell_inst = s.sell_inst.p;

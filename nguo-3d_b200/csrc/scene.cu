@@ -103,6 +103,7 @@ bool shell_rest_shape(const HV& p0, const HV& p1, const HV& p2, float dm[4], flo
 struct Contribution {
   uint32_t row, col;
 };
+constexpr uint32_t PAD_ENTRY = 0xffffffffu;  // alignment padding in the contribution lists
 
 }  // namespace
 
@@ -450,6 +451,10 @@ int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>
     for (int a = 0; a < 3; ++a)
       for (int b = 0; b < 3; ++b) cb.push_back({sv[a], sv[b]});
   }
+  // the hinges' blocks and gradient entries start 16-byte aligned (k_hinge stores them as
+  // float4): padding entries before them, which no slot and no vertex gathers
+  while (cb.size() % 4) cb.push_back({PAD_ENTRY, PAD_ENTRY});
+  while (gvert.size() % 4) gvert.push_back(PAD_ENTRY);
   s.cb_hinge = cb.size();
   s.gb_hinge = gvert.size();
   for (uint32_t e = 0; e < s.n_hinge; ++e) {
@@ -466,6 +471,7 @@ int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>
   std::vector<uint64_t> ks, kp;
   ks.reserve(cb.size() + nv);
   for (auto& c : cb) {
+    if (c.row == PAD_ENTRY) continue;
     if (vfree(c.row) && vfree(c.col))
       ks.push_back(key(c.row, c.col));
     else
@@ -504,19 +510,27 @@ int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>
   uint32_t nslots = s.Ps.nnz + s.Pp.nnz;
   std::vector<uint32_t> slot_ptr(nslots + 1, 0), slot_of_c(cb.size());
   for (size_t i = 0; i < cb.size(); ++i) {
+    if (cb[i].row == PAD_ENTRY) {
+      slot_of_c[i] = PAD_ENTRY;
+      continue;
+    }
     slot_of_c[i] = slot_of(cb[i].row, cb[i].col);
     slot_ptr[slot_of_c[i] + 1]++;
   }
   for (uint32_t k = 0; k < nslots; ++k) slot_ptr[k + 1] += slot_ptr[k];
-  std::vector<uint32_t> cursor(slot_ptr.begin(), slot_ptr.end() - 1), slot_list(cb.size());
-  for (size_t i = 0; i < cb.size(); ++i) slot_list[cursor[slot_of_c[i]]++] = (uint32_t)i;
+  std::vector<uint32_t> cursor(slot_ptr.begin(), slot_ptr.end() - 1),
+      slot_list(std::max<uint32_t>(slot_ptr[nslots], 1));
+  for (size_t i = 0; i < cb.size(); ++i)
+    if (slot_of_c[i] != PAD_ENTRY) slot_list[cursor[slot_of_c[i]]++] = (uint32_t)i;
   MG_TRY(up(s.slot_ptr, slot_ptr));
   MG_TRY(up(s.slot_list, slot_list));
-  std::vector<uint32_t> gv_ptr(nv + 1, 0), gv_list(gvert.size());
-  for (uint32_t v : gvert) gv_ptr[v + 1]++;
+  std::vector<uint32_t> gv_ptr(nv + 1, 0);
+  for (uint32_t v : gvert)
+    if (v != PAD_ENTRY) gv_ptr[v + 1]++;
   for (uint32_t k = 0; k < nv; ++k) gv_ptr[k + 1] += gv_ptr[k];
-  std::vector<uint32_t> gcur(gv_ptr.begin(), gv_ptr.end() - 1);
-  for (size_t i = 0; i < gvert.size(); ++i) gv_list[gcur[gvert[i]]++] = (uint32_t)i;
+  std::vector<uint32_t> gcur(gv_ptr.begin(), gv_ptr.end() - 1), gv_list(std::max<uint32_t>(gv_ptr[nv], 1));
+  for (size_t i = 0; i < gvert.size(); ++i)
+    if (gvert[i] != PAD_ENTRY) gv_list[gcur[gvert[i]]++] = (uint32_t)i;
   MG_TRY(up(s.gv_ptr, gv_ptr));
   MG_TRY(up(s.gv_list, gv_list));
   std::vector<uint32_t> diag(nv);
@@ -530,6 +544,14 @@ int scene_build(Scene& s, const mguso_scene_desc* d, const std::vector<uint32_t>
     }
   }
   MG_TRY(up(s.diag_slot, diag));
+  // each slot's instance (its row's), for gathers that skip the instances a batch no longer
+  // iterates
+  std::vector<uint8_t> slot_inst(std::max<uint32_t>(nslots, 1), 0);
+  for (uint32_t r = 0; r < nv; ++r) {
+    for (uint32_t k = s.Ps.h_row_ptr[r]; k < s.Ps.h_row_ptr[r + 1]; ++k) slot_inst[k] = vinst[r];
+    for (uint32_t k = s.Pp.h_row_ptr[r]; k < s.Pp.h_row_ptr[r + 1]; ++k) slot_inst[s.Ps.nnz + k] = vinst[r];
+  }
+  MG_TRY(s.slot_inst.upload(slot_inst.data(), slot_inst.size(), st));
   MG_TRY(s.cblocks.reserve(9 * std::max<uint64_t>(s.n_cblocks, 1)));
   MG_TRY(s.gentries.reserve(3 * std::max<uint64_t>(s.n_gentries, 1)));
   MG_CUDA(cudaMemsetAsync(s.cblocks.p, 0, 36 * std::max<uint64_t>(s.n_cblocks, 1), st));

@@ -109,6 +109,7 @@ struct Scene {
   // patterns + gather lists (slot < Ps.nnz: Ps; else Pp)
   BlockPattern Ps, Pp;
   DevBuf<uint32_t> slot_ptr, slot_list;     // contributions per slot, push order
+  DevBuf<uint8_t> slot_inst;                // instance of each slot (Ps, then Pp)
   DevBuf<uint32_t> gv_ptr, gv_list;         // gradient entries per vertex, push order
   DevBuf<uint32_t> diag_slot;               // per vertex: its diagonal slot (Ps if free, Pp if pinned)
   std::unique_ptr<mguso_bsr> A;             // Ps values live in A->val
