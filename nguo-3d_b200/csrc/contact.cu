@@ -259,6 +259,38 @@ __device__ __forceinline__ void emit_stencil(Stencil* out, unsigned long long* k
   ids[at] = (uint32_t)at;
 }
 
+// ---- warp-pooled narrow phase ---------------------------------------------------------------
+// Each lane walks its query's tree (BoxWalk, CcdWalk) and pushes the leaves it reaches, as
+// (query, primitive) pairs, onto its warp's queue in shared memory; whenever 32 are queued the
+// whole warp takes them, one per lane, through the remaining filters and the narrow phase
+// (distances, accd_toi). The walks stay per lane, but the narrow phase (the bulk of the work)
+// runs on full warps instead of on the few lanes whose walk happens to sit on a leaf. Its
+// results are order-free: stencils are sorted by their pair key afterwards, CCD results are
+// per (instance, pass) minima and sums.
+constexpr int WQ_WARPS = 4;   // 128-thread blocks
+constexpr int WQ_QCAP = 96;   // < 32 left over + 2 leaves per lane and step
+
+__device__ __forceinline__ void wq_push(uint2* q, int& n, bool has, uint2 e) {
+  const unsigned m = __ballot_sync(0xffffffffu, has);
+  if (has) q[n + __popc(m & ((1u << (threadIdx.x & 31)) - 1u))] = e;
+  n += __popc(m);
+}
+
+// Takes batches of up to 32 queued pairs while at least min_n are queued (n is warp-uniform).
+template <class F>
+__device__ __forceinline__ void wq_take(uint2* q, int& n, int min_n, F&& solve) {
+  const int lane = (int)(threadIdx.x & 31);
+  __syncwarp();
+  while (n >= min_n && n > 0) {
+    const int take = n < 32 ? n : 32;
+    const bool has = lane < take;
+    const uint2 e = has ? q[n - take + lane] : make_uint2(0u, 0u);
+    __syncwarp();
+    n -= take;
+    if (has) solve(e);
+  }
+}
+
 template <class R>
 __device__ __forceinline__ R vt_distance(const float* x, const uint32_t idx[4], bool collider, bool inside, R g[12]) {
   V3<R> gg[4];
@@ -312,40 +344,70 @@ __global__ void k_vt_stencils(BvhSet bv, const uint8_t* __restrict__ vinst, cons
   if (!ok) atomicOr(status, ST_STACK_OVERFLOW);
 }
 
-// Edge-edge pairs: thread t (edge t) takes the pairs (t, p) with p > t, the lower-indexed
-// edge first in the stencil and its key, so each pair is seen once. An edge in its instance's
-// static tail (every edge from there on has both vertices pinned) has no partner above it
-// that can move, and skips its traversal.
-__global__ void k_ee_stencils(BvhSet bv, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
-                              const uint32_t* __restrict__ edges, const uint32_t* __restrict__ ee_tail,
-                              const float* __restrict__ im, uint32_t ne, float search, float dhat, int mixed,
-                              Stencil* out, unsigned long long* keys, uint32_t* ids, unsigned long long* counter,
-                              uint32_t cap, uint32_t* status, uint32_t active) {
+// Edge-edge pairs: lane t (edge t) takes the pairs (t, p) with p > t, the lower-indexed edge
+// first in the stencil and its key, so each pair is seen once. An edge in its instance's static
+// tail (every edge from there on has both vertices pinned) has no partner above it that can
+// move, and skips its walk. The distances run pooled per warp.
+__global__ void __launch_bounds__(WQ_WARPS * 32) k_ee_stencils(
+    BvhSet bv, const uint8_t* __restrict__ vinst, const float* __restrict__ x, const uint32_t* __restrict__ edges,
+    const uint32_t* __restrict__ ee_tail, const float* __restrict__ im, uint32_t ne, float search, float dhat,
+    int mixed, Stencil* out, unsigned long long* keys, uint32_t* ids, unsigned long long* counter, uint32_t cap,
+    uint32_t* status, uint32_t active) {
+  __shared__ uint2 qbuf[WQ_WARPS][WQ_QCAP];
+  uint2* q = qbuf[threadIdx.x >> 5];
+  int qn = 0;
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ne) return;
-  const uint32_t b0 = edges[2 * t], b1 = edges[2 * t + 1];
-  const uint32_t k = vinst[b0];
-  if (t >= ee_tail[k] || !((active >> k) & 1u)) return;
-  float4 lo, hi;
-  edge_box(x, b0, b1, search, lo, hi);
-  const bool tmov = im[b0] > 0.f || im[b1] > 0.f;
-  bool ok = visit(bv, k, lo, hi, [&](uint32_t p) {
-    if (p <= t) return;
-    const uint32_t a0 = edges[2 * p], a1 = edges[2 * p + 1];
-    if (!(tmov || im[a0] > 0.f || im[a1] > 0.f)) return;
+  uint32_t base = 0;
+  bool done = true;
+  BoxWalk walk;
+  walk.ok = true;
+  uint32_t outp[2];
+  int nout = 0;
+  if (t < ne) {
+    const uint32_t b0 = edges[2 * t], b1 = edges[2 * t + 1];
+    const uint32_t k = vinst[b0];
+    if (t < ee_tail[k] && ((active >> k) & 1u)) {
+      const BvhView& tv = bv.t[k];
+      base = bv.base[k];
+      walk.left = tv.left;
+      walk.right = tv.right;
+      walk.prim = tv.prim;
+      walk.node = tv.node;
+      walk.leaf = tv.leaf;
+      walk.nt = tv.n;
+      edge_box(x, b0, b1, search, walk.qlo, walk.qhi);
+      nout = walk.start(done, outp);
+    }
+  }
+  auto solve = [&](uint2 e) {
+    const uint32_t qt = e.x, p = e.y;
+    const uint32_t b0 = edges[2 * qt], b1 = edges[2 * qt + 1], a0 = edges[2 * p], a1 = edges[2 * p + 1];
+    if (!(im[b0] > 0.f || im[b1] > 0.f || im[a0] > 0.f || im[a1] > 0.f)) return;
     if (a0 == b0 || a0 == b1 || a1 == b0 || a1 == b1) return;
     uint32_t idx[4] = {b0, b1, a0, a1};
     double g[12];
     float gf[12];
     float df = ee_distance<float>(x, idx, gf);
     double d = df;
-    for (int k = 0; k < 12; ++k) g[k] = gf[k];
+    for (int c = 0; c < 12; ++c) g[c] = gf[c];
     if (mixed && df < 10.f * dhat) d = ee_distance<double>(x, idx, g);
     double ghat = (double)(0.5f * (dhat + dhat));
     if (!(d < ghat)) return;
-    emit_stencil(out, keys, ids, counter, cap, status, 1, t, p, idx, d, ghat, g);
-  });
-  if (!ok) atomicOr(status, ST_STACK_OVERFLOW);
+    emit_stencil(out, keys, ids, counter, cap, status, 1, qt, p, idx, d, ghat, g);
+  };
+  for (;;) {
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const bool leaf = c < nout;
+      const uint32_t p = leaf ? base + outp[c] : 0u;
+      wq_push(q, qn, leaf && p > t, make_uint2(t, p));
+    }
+    wq_take(q, qn, 32, solve);
+    if (!__any_sync(0xffffffffu, !done)) break;
+    nout = done ? 0 : walk.step(done, outp);
+  }
+  wq_take(q, qn, 1, solve);
+  if (!walk.ok) atomicOr(status, ST_STACK_OVERFLOW);
 }
 
 __global__ void k_permute_stencils(const Stencil* __restrict__ in, const uint32_t* __restrict__ ids, uint32_t n,
@@ -557,37 +619,6 @@ __device__ __forceinline__ int first_pass_edge(const CcdPass& cp, uint32_t k, co
   return n;
 }
 
-// ---- warp-pooled root solves ----------------------------------------------------------------
-// Each lane walks its query's tree (CcdWalk) and pushes the leaves it reaches, as (query,
-// primitive) pairs, onto its warp's queue in shared memory; whenever 32 are queued the whole
-// warp takes them, one per lane, through the remaining filters and accd_toi. The walks stay
-// per lane, but the root solves (the bulk of the work) run on full warps instead of on the
-// few lanes whose walk happens to sit on a leaf. Results are per (instance, pass) minima and
-// sums, so the order in which the pairs are solved does not change them.
-constexpr int CCD_WARPS = 4;  // 128-thread blocks
-constexpr int CCD_QCAP = 96;  // < 32 left over + 2 leaves per lane and step
-
-__device__ __forceinline__ void wq_push(uint2* q, int& n, bool has, uint2 e) {
-  const unsigned m = __ballot_sync(0xffffffffu, has);
-  if (has) q[n + __popc(m & ((1u << (threadIdx.x & 31)) - 1u))] = e;
-  n += __popc(m);
-}
-
-// Takes batches of up to 32 queued pairs while at least min_n are queued (n is warp-uniform).
-template <class F>
-__device__ __forceinline__ void wq_take(uint2* q, int& n, int min_n, F&& solve) {
-  const int lane = (int)(threadIdx.x & 31);
-  __syncwarp();
-  while (n >= min_n && n > 0) {
-    const int take = n < 32 ? n : 32;
-    const bool has = lane < take;
-    const uint2 e = has ? q[n - take + lane] : make_uint2(0u, 0u);
-    __syncwarp();
-    n -= take;
-    if (has) solve(e);
-  }
-}
-
 // A lane's step fractions and cap counts per pass for one instance at a time, flushed to the
 // per (instance, pass) accumulators when the instance changes and at the end.
 struct CcdAcc {
@@ -651,13 +682,13 @@ __device__ __forceinline__ void walk_init(CcdWalk& w, const BvhSet& bs, uint32_t
 
 // Vertex-triangle passes: lane v walks the triangles near vertex v.
 template <class R>
-__global__ void __launch_bounds__(CCD_WARPS * 32, 4) k_ccd_vt(
+__global__ void __launch_bounds__(WQ_WARPS * 32, 4) k_ccd_vt(
     BvhSet bv, const CcdPass* __restrict__ cpp, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
     const float* __restrict__ dx, const uint32_t* __restrict__ tris, const uint8_t* __restrict__ ctri,
     const float* __restrict__ im, const uint32_t* __restrict__ ex_ptr, const uint32_t* __restrict__ ex_list,
     const unsigned long long* __restrict__ best, const float* __restrict__ pn, int has_static, uint32_t nv, float dhat,
     uint32_t max_iter, unsigned int* __restrict__ red, unsigned int* __restrict__ acc, uint32_t* __restrict__ status) {
-  __shared__ uint2 qbuf[CCD_WARPS][CCD_QCAP];
+  __shared__ uint2 qbuf[WQ_WARPS][WQ_QCAP];
   uint2* q = qbuf[threadIdx.x >> 5];
   int qn = 0;
   const CcdPass& cp = *cpp;
@@ -734,12 +765,12 @@ __global__ void __launch_bounds__(CCD_WARPS * 32, 4) k_ccd_vt(
 // Edge-edge passes. As k_ee_stencils: lane j takes the pairs (j, i) with i > j (the
 // lower-indexed edge first), and an edge of its instance's static tail skips its walk.
 template <class R>
-__global__ void __launch_bounds__(CCD_WARPS * 32, 4) k_ccd_ee(
+__global__ void __launch_bounds__(WQ_WARPS * 32, 4) k_ccd_ee(
     BvhSet bv, const CcdPass* __restrict__ cpp, const uint8_t* __restrict__ vinst, const float* __restrict__ x,
     const float* __restrict__ dx, const uint32_t* __restrict__ edges, const uint32_t* __restrict__ ee_tail,
     const float* __restrict__ im, uint32_t ne, uint32_t max_iter, unsigned int* __restrict__ red,
     unsigned int* __restrict__ acc, uint32_t* __restrict__ status) {
-  __shared__ uint2 qbuf[CCD_WARPS][CCD_QCAP];
+  __shared__ uint2 qbuf[WQ_WARPS][WQ_QCAP];
   uint2* q = qbuf[threadIdx.x >> 5];
   int qn = 0;
   const CcdPass& cp = *cpp;

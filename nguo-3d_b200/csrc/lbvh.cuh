@@ -106,6 +106,71 @@ __device__ __forceinline__ bool lbvh_visit(const uint32_t* __restrict__ left, co
   return ok;
 }
 
+// Resumable walk over the leaves whose boxes overlap [qlo, qhi] (the predicate of
+// lbvh_visit): start() and each step() hand back at most two leaf primitives, so a warp's
+// lanes can advance their walks in lockstep and pool the leaves they reach. 64-entry stack;
+// ok turns false on overflow.
+struct BoxWalk {
+  const uint32_t *left, *right, *prim;
+  const float4 *node, *leaf;
+  uint32_t nt;
+  float4 qlo, qhi;
+  uint32_t stack[64];
+  int sp;
+  uint32_t cur;
+  bool ok;
+
+  __device__ __forceinline__ bool enter(const float4* pb) const {
+    const float4 lo = __ldg(pb), hi = __ldg(pb + 1);
+    return qlo.x <= hi.x && qlo.y <= hi.y && qlo.z <= hi.z && lo.x <= qhi.x && lo.y <= qhi.y && lo.z <= qhi.z;
+  }
+  __device__ __forceinline__ int start(bool& done, uint32_t out[2]) {
+    sp = 0;
+    cur = 0;
+    ok = true;
+    done = true;
+    if (nt == 0) return 0;
+    if (nt == 1) {
+      if (enter(leaf)) {
+        out[0] = prim[0];
+        return 1;
+      }
+      return 0;
+    }
+    done = !enter(node);
+    return 0;
+  }
+  __device__ __forceinline__ int step(bool& done, uint32_t out[2]) {
+    int n = 0;
+    const uint32_t ch[2] = {__ldg(left + cur), __ldg(right + cur)};
+    uint32_t next = 0xffffffffu;
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const uint32_t x = ch[c];
+      const bool lf = (x & 0x80000000u) != 0;
+      const uint32_t i = x & 0x7fffffffu;
+      if (!enter(lf ? leaf + 2 * i : node + 2 * i)) continue;
+      if (lf) {
+        out[n++] = prim[i];
+      } else if (next == 0xffffffffu) {
+        next = x;
+      } else if (sp < 64) {
+        stack[sp++] = x;
+      } else {
+        ok = false;
+      }
+    }
+    if (next != 0xffffffffu) {
+      cur = next;
+    } else if (sp > 0) {
+      cur = stack[--sp];
+    } else {
+      done = true;
+    }
+    return n;
+  }
+};
+
 // CCD traversal (ccd_max_step's broad phase, implicit.rs:1690-1947, with exact pruning).
 // A subtree is entered when the search box overlaps its position box (node, leaf) and its
 // pairs with the query are not all settled by accd_toi's first test (contact.rs:378-437),
