@@ -34,11 +34,13 @@ struct BvhView {
   const float4 *node, *leaf;
   uint32_t n;
   const float4 *dnode, *dleaf;  // displacement boxes of the same tree (CCD only)
+  const float4 *cbox, *dcbox;   // children's position and displacement boxes per inner node
 };
 
 static BvhView view(const Lbvh& b) {
   return BvhView{b.left.p, b.right.p, b.perm.p, (const float4*)b.node.p, (const float4*)b.leaf.p, b.nt,
-                 (const float4*)b.dnode.p, (const float4*)b.dleaf.p};
+                 (const float4*)b.dnode.p, (const float4*)b.dleaf.p, (const float4*)b.cbox.p,
+                 (const float4*)b.dcbox.p};
 }
 
 // One tree per instance over that instance's primitives (a query only meets its own
@@ -108,18 +110,26 @@ static int aux_join(Scene& s) {
 }
 
 // The instances' triangle and edge LBVHs at x, built concurrently on the side streams (each
-// tree has its own scratch).
-int build_bvhs(Scene& s, const float* x) {
+// tree has its own scratch). With refit, a tree keeps the shape of its last build and gets
+// its boxes at x (leaf boxes and one climb instead of bounds, keys, sort, Karras and climb):
+// the traversals' leaf sets are defined by box overlap with exact node unions, so they are
+// the same for any shape over the same primitives, and within a step the shape built at its
+// first iterate stays a close fit.
+int build_bvhs(Scene& s, const float* x, bool refit) {
   MG_TRY(aux_fork(s));
   int rc = MGUSO_OK;
   for (uint32_t k = 0; k < s.ninst && rc == MGUSO_OK; ++k) {
     if (!((s.iter_active >> k) & 1u)) continue;  // an instance the batch no longer iterates
     const uint32_t t0 = s.inst_tri[k], e0 = s.inst_edge[k];
-    rc = lbvh_build(s.tri_bvh[k].get(), x, s.nv, s.tris.p + 3 * (size_t)t0, s.inst_tri[k + 1] - t0, 30,
-                    s.aux[(2 * k) % N_AUX]);
+    const uint32_t nt = s.inst_tri[k + 1] - t0, ne = s.inst_edge[k + 1] - e0;
+    Lbvh* tb = s.tri_bvh[k].get();
+    Lbvh* eb = s.edge_bvh[k].get();
+    const uint32_t* tt = s.tris.p + 3 * (size_t)t0;
+    const uint32_t* et = s.edge_tris.p + 3 * (size_t)e0;
+    cudaStream_t ts = s.aux[(2 * k) % N_AUX], es = s.aux[(2 * k + 1) % N_AUX];
+    rc = (refit && tb->shaped && tb->nt == nt) ? lbvh_refit_pos(tb, x, tt, ts) : lbvh_build(tb, x, s.nv, tt, nt, 30, ts);
     if (rc == MGUSO_OK)
-      rc = lbvh_build(s.edge_bvh[k].get(), x, s.nv, s.edge_tris.p + 3 * (size_t)e0, s.inst_edge[k + 1] - e0, 30,
-                      s.aux[(2 * k + 1) % N_AUX]);
+      rc = (refit && eb->shaped && eb->nt == ne) ? lbvh_refit_pos(eb, x, et, es) : lbvh_build(eb, x, s.nv, et, ne, 30, es);
   }
   MG_TRY(aux_join(s));
   return rc;
@@ -172,14 +182,16 @@ __global__ void k_self_intersect(BvhSet bv, const uint8_t* __restrict__ vinst, c
 
 // Piercing (edge, triangle) pairs of every instance at the scene's positions x, counted into
 // red[RED_STRIDE k + 14] (which the caller zeroes); rebuilds the triangle BVHs at x.
-int self_intersections(Scene& s) {
+int self_intersections(Scene& s, bool refit) {
   if (s.n_edge == 0) return MGUSO_OK;
   MG_TRY(aux_fork(s));
   int rc = MGUSO_OK;
   for (uint32_t k = 0; k < s.ninst && rc == MGUSO_OK; ++k) {
-    const uint32_t t0 = s.inst_tri[k];
-    rc = lbvh_build(s.tri_bvh[k].get(), s.x.p, s.nv, s.tris.p + 3 * (size_t)t0, s.inst_tri[k + 1] - t0, 30,
-                    s.aux[k % N_AUX]);
+    const uint32_t t0 = s.inst_tri[k], nt = s.inst_tri[k + 1] - t0;
+    Lbvh* tb = s.tri_bvh[k].get();
+    const uint32_t* tt = s.tris.p + 3 * (size_t)t0;
+    rc = (refit && tb->shaped && tb->nt == nt) ? lbvh_refit_pos(tb, s.x.p, tt, s.aux[k % N_AUX])
+                                 : lbvh_build(tb, s.x.p, s.nv, tt, nt, 30, s.aux[k % N_AUX]);
   }
   MG_TRY(aux_join(s));
   MG_TRY(rc);
@@ -311,37 +323,70 @@ __device__ __forceinline__ R ee_distance(const float* x, const uint32_t idx[4], 
   return d;
 }
 
-__global__ void k_vt_stencils(BvhSet bv, const uint8_t* __restrict__ vinst, const float* __restrict__ x, const uint32_t* __restrict__ tris,
-                              const uint8_t* __restrict__ ctri, const float* __restrict__ im,
-                              const uint32_t* __restrict__ ex_ptr, const uint32_t* __restrict__ ex_list,
-                              const unsigned long long* __restrict__ best, const float* __restrict__ pn, int has_static,
-                              uint32_t nv, float dhat, int mixed, Stencil* out, unsigned long long* keys, uint32_t* ids,
-                              unsigned long long* counter, uint32_t cap, uint32_t* status, uint32_t active) {
-  uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= nv || !((active >> vinst[v]) & 1u)) return;
-  float4 lo, hi;
-  point_box(x, v, dhat, lo, hi);
-  bool vmov = im[v] > 0.f;
-  float side = 2.f;  // computed lazily
-  bool ok = visit(bv, vinst[v], lo, hi, [&](uint32_t t) {
-    uint32_t a = tris[3 * t], b = tris[3 * t + 1], c = tris[3 * t + 2];
-    bool tmov = im[a] > 0.f || im[b] > 0.f || im[c] > 0.f;
-    if (!tmov && !vmov) return;
-    if (excluded(ex_ptr, ex_list, v, a, b, c)) return;
-    uint32_t idx[4] = {v, a, b, c};
-    bool collider = has_static && ctri[t];
-    if (collider && side == 2.f) side = side_of(v, best, x, tris, pn, dhat);
-    bool inside = collider && side < 0.f;
+// Vertex-triangle pairs: lane v walks the triangles near vertex v; the distances run pooled
+// per warp. A static collider triangle needs v's side of the collider, which depends on v
+// alone (side_of), so the lane that takes the pair evaluates it.
+__global__ void __launch_bounds__(WQ_WARPS * 32) k_vt_stencils(
+    BvhSet bv, const uint8_t* __restrict__ vinst, const float* __restrict__ x, const uint32_t* __restrict__ tris,
+    const uint8_t* __restrict__ ctri, const float* __restrict__ im, const uint32_t* __restrict__ ex_ptr,
+    const uint32_t* __restrict__ ex_list, const unsigned long long* __restrict__ best, const float* __restrict__ pn,
+    int has_static, uint32_t nv, float dhat, int mixed, Stencil* out, unsigned long long* keys, uint32_t* ids,
+    unsigned long long* counter, uint32_t cap, uint32_t* status, uint32_t active) {
+  __shared__ uint2 qbuf[WQ_WARPS][WQ_QCAP];
+  uint2* q = qbuf[threadIdx.x >> 5];
+  int qn = 0;
+  const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t base = 0;
+  bool done = true;
+  BoxWalk walk;
+  walk.ok = true;
+  uint32_t outp[2];
+  int nout = 0;
+  if (v < nv) {
+    const uint32_t k = vinst[v];
+    if ((active >> k) & 1u) {
+      const BvhView& tv = bv.t[k];
+      base = bv.base[k];
+      walk.left = tv.left;
+      walk.right = tv.right;
+      walk.prim = tv.prim;
+      walk.node = tv.node;
+      walk.leaf = tv.leaf;
+      walk.cbox = tv.cbox;
+      walk.nt = tv.n;
+      point_box(x, v, dhat, walk.qlo, walk.qhi);
+      nout = walk.start(done, outp);
+    }
+  }
+  auto solve = [&](uint2 e) {
+    const uint32_t qv = e.x, t = e.y;
+    const uint32_t a = tris[3 * t], b = tris[3 * t + 1], c = tris[3 * t + 2];
+    if (!(im[qv] > 0.f || im[a] > 0.f || im[b] > 0.f || im[c] > 0.f)) return;
+    if (excluded(ex_ptr, ex_list, qv, a, b, c)) return;
+    uint32_t idx[4] = {qv, a, b, c};
+    const bool collider = has_static && ctri[t];
+    const bool inside = collider && side_of(qv, best, x, tris, pn, dhat) < 0.f;
     double g[12];
     float gf[12];
     float df = vt_distance<float>(x, idx, collider, inside, gf);
     double d = df;
-    for (int k = 0; k < 12; ++k) g[k] = gf[k];
+    for (int cc = 0; cc < 12; ++cc) g[cc] = gf[cc];
     if (mixed && df < 10.f * dhat) d = vt_distance<double>(x, idx, collider, inside, g);
     if (!(d < (double)dhat)) return;
-    emit_stencil(out, keys, ids, counter, cap, status, 0, v, t, idx, d, dhat, g);
-  });
-  if (!ok) atomicOr(status, ST_STACK_OVERFLOW);
+    emit_stencil(out, keys, ids, counter, cap, status, 0, qv, t, idx, d, dhat, g);
+  };
+  for (;;) {
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const bool leaf = c < nout;
+      wq_push(q, qn, leaf, make_uint2(v, leaf ? base + outp[c] : 0u));
+    }
+    wq_take(q, qn, 32, solve);
+    if (!__any_sync(0xffffffffu, !done)) break;
+    nout = done ? 0 : walk.step(done, outp);
+  }
+  wq_take(q, qn, 1, solve);
+  if (!walk.ok) atomicOr(status, ST_STACK_OVERFLOW);
 }
 
 // Edge-edge pairs: lane t (edge t) takes the pairs (t, p) with p > t, the lower-indexed edge
@@ -374,6 +419,7 @@ __global__ void __launch_bounds__(WQ_WARPS * 32) k_ee_stencils(
       walk.prim = tv.prim;
       walk.node = tv.node;
       walk.leaf = tv.leaf;
+      walk.cbox = tv.cbox;
       walk.nt = tv.n;
       edge_box(x, b0, b1, search, walk.qlo, walk.qhi);
       nout = walk.start(done, outp);
@@ -431,16 +477,19 @@ int collect_stencils(Scene& s, uint32_t* nst_out) {
     MG_TRY(s.st_keys.reserve(s.cap_stencils));
     MG_TRY(s.st_ids.reserve(s.cap_stencils));
     MG_CUDA(cudaMemsetAsync(s.counters.p, 0, 8 * 8, st));
-    k_vt_stencils<<<ceil_div(s.nv, 128), 128, 0, st>>>(tv, s.vinst.p, s.x.p, s.tris.p, s.collider_tri.p, s.inv_mass.p,
-                                                     s.ex_ptr.p, s.ex_list.p, s.side_best.p, s.collider_pn.p,
-                                                     s.has_static ? 1 : 0, s.nv, dhat, s.mixed ? 1 : 0, s.stencils.p,
-                                                     s.st_keys.p, s.st_ids.p, s.counters.p, s.cap_stencils,
-                                                     s.status.p, s.iter_active);
+    // the two kinds run concurrently on side streams (they share the output through its
+    // atomic counter; the stencils are put in key order below)
+    MG_TRY(aux_fork(s));
+    k_vt_stencils<<<ceil_div(s.nv, 128), 128, 0, s.aux[0]>>>(
+        tv, s.vinst.p, s.x.p, s.tris.p, s.collider_tri.p, s.inv_mass.p, s.ex_ptr.p, s.ex_list.p, s.side_best.p,
+        s.collider_pn.p, s.has_static ? 1 : 0, s.nv, dhat, s.mixed ? 1 : 0, s.stencils.p, s.st_keys.p, s.st_ids.p,
+        s.counters.p, s.cap_stencils, s.status.p, s.iter_active);
     if (s.n_edge)
-      k_ee_stencils<<<ceil_div(s.n_edge, 128), 128, 0, st>>>(ev, s.vinst.p, s.x.p, s.edges.p, s.ee_tail.p, s.inv_mass.p, s.n_edge, dhat, dhat,
-                                                           s.mixed ? 1 : 0, s.stencils.p, s.st_keys.p, s.st_ids.p,
-                                                           s.counters.p, s.cap_stencils, s.status.p, s.iter_active);
+      k_ee_stencils<<<ceil_div(s.n_edge, 128), 128, 0, s.aux[1]>>>(
+          ev, s.vinst.p, s.x.p, s.edges.p, s.ee_tail.p, s.inv_mass.p, s.n_edge, dhat, dhat, s.mixed ? 1 : 0,
+          s.stencils.p, s.st_keys.p, s.st_ids.p, s.counters.p, s.cap_stencils, s.status.p, s.iter_active);
     MG_CUDA(cudaGetLastError());
+    MG_TRY(aux_join(s));
     unsigned long long cnt = 0;
     MG_CUDA(cudaMemcpyAsync(&cnt, s.counters.p, 8, cudaMemcpyDeviceToHost, st));
     MG_CUDA(cudaStreamSynchronize(st));
@@ -671,6 +720,8 @@ __device__ __forceinline__ void walk_init(CcdWalk& w, const BvhSet& bs, uint32_t
   w.leaf = bv.leaf;
   w.dnode = bv.dnode;
   w.dleaf = bv.dleaf;
+  w.cbox = bv.cbox;
+  w.dcbox = bv.dcbox;
   w.nt = bv.n;
   w.slo = lo;
   w.shi = hi;

@@ -394,9 +394,11 @@ __device__ __forceinline__ void child_box(uint32_t c, const float4* leaf, const 
   hi = __ldcg(src + 1);
 }
 
+// cb (4 float4 per internal node) receives each node's two children's boxes as read.
 __global__ void k_refit(const uint32_t* __restrict__ parent_leaf, const uint32_t* __restrict__ parent_int,
                         const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
-                        const float4* __restrict__ leaf, float4* node, uint32_t* flags, uint32_t nt) {
+                        const float4* __restrict__ leaf, float4* node, float4* __restrict__ cb, uint32_t* flags,
+                        uint32_t nt) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nt || nt < 2) return;
   uint32_t p = parent_leaf[i];
@@ -412,6 +414,11 @@ __global__ void k_refit(const uint32_t* __restrict__ parent_leaf, const uint32_t
     float4 hi = make_float4(fmaxf(a1.x, b1.x), fmaxf(a1.y, b1.y), fmaxf(a1.z, b1.z), 0.f);
     __stcg(node + 2 * p, lo);
     __stcg(node + 2 * p + 1, hi);
+    float4* c4 = cb + 4 * (size_t)p;
+    c4[0] = a0;
+    c4[1] = a1;
+    c4[2] = b0;
+    c4[3] = b1;
     p = parent_int[p];
   }
 }
@@ -545,6 +552,7 @@ __global__ void k_ord_init(uint32_t* __restrict__ ord) {
 
 template <class K>
 static int build_impl(Lbvh* b, const float* pos, const uint32_t* tris, uint32_t nt, int key_bits, cudaStream_t s) {
+  b->shaped = false;
   b->nt = nt;
   b->key_bits = key_bits;
   MG_TRY(b->keys.reserve((size_t)std::max<uint32_t>(nt, 1) * sizeof(K)));
@@ -555,6 +563,7 @@ static int build_impl(Lbvh* b, const float* pos, const uint32_t* tris, uint32_t 
   MG_TRY(b->parent_leaf.reserve(std::max<uint32_t>(nt, 1)));
   MG_TRY(b->leaf.reserve(2 * (size_t)std::max<uint32_t>(nt, 1)));
   MG_TRY(b->node.reserve(2 * (size_t)std::max<uint32_t>(nt, 2)));
+  MG_TRY(b->cbox.reserve(4 * (size_t)std::max<uint32_t>(nt, 2)));
   MG_TRY(b->flags.reserve(std::max<uint32_t>(nt, 2)));
   MG_TRY(b->params.reserve(8));
   MG_TRY(b->ord.reserve(8));
@@ -579,10 +588,12 @@ static int build_impl(Lbvh* b, const float* pos, const uint32_t* tris, uint32_t 
   if (nt > 1) {
     MG_CUDA(cudaMemsetAsync(b->flags.p, 0, 4 * (size_t)(nt - 1), s));
     k_refit<<<ceil_div(nt, 256), 256, 0, s>>>(b->parent_leaf.p, b->parent_int.p, b->left.p, b->right.p,
-                                             (const float4*)b->leaf.p, (float4*)b->node.p, b->flags.p, nt);
+                                             (const float4*)b->leaf.p, (float4*)b->node.p, b->cbox.p, b->flags.p,
+                                             nt);
   }
   MG_CUDA(cudaGetLastError());
   if (b->ev_on) cudaEventRecord(b->ev[4], s);
+  b->shaped = true;
   return MGUSO_OK;
 }
 
@@ -590,12 +601,33 @@ int lbvh_refit_disp(Lbvh* b, const float* dx, const uint32_t* tris, cudaStream_t
   const uint32_t nt = b->nt;
   MG_TRY(b->dleaf.reserve(2 * (size_t)std::max<uint32_t>(nt, 1)));
   MG_TRY(b->dnode.reserve(2 * (size_t)std::max<uint32_t>(nt, 2)));
+  MG_TRY(b->dcbox.reserve(4 * (size_t)std::max<uint32_t>(nt, 2)));
   if (nt == 0) return MGUSO_OK;
   k_leaf_disp_boxes<<<ceil_div(nt, 256), 256, 0, s>>>(dx, tris, b->perm.p, nt, b->dleaf.p);
   if (nt > 1) {
     MG_CUDA(cudaMemsetAsync(b->flags.p, 0, 4 * (size_t)(nt - 1), s));
     k_refit<<<ceil_div(nt, 256), 256, 0, s>>>(b->parent_leaf.p, b->parent_int.p, b->left.p, b->right.p, b->dleaf.p,
-                                             b->dnode.p, b->flags.p, nt);
+                                             b->dnode.p, b->dcbox.p, b->flags.p, nt);
+  }
+  MG_CUDA(cudaGetLastError());
+  return MGUSO_OK;
+}
+
+int lbvh_refit_pos(Lbvh* b, const float* pos, const uint32_t* tris, cudaStream_t s) {
+  const uint32_t nt = b->nt;
+  MG_CHECK_ARG(b->shaped, "LBVH refit before a complete build");
+  if (nt == 0) return MGUSO_OK;
+  // sized by the last build already (these only check, unless that build stopped early)
+  MG_TRY(b->leaf.reserve(2 * (size_t)nt));
+  MG_TRY(b->node.reserve(2 * (size_t)std::max<uint32_t>(nt, 2)));
+  MG_TRY(b->cbox.reserve(4 * (size_t)std::max<uint32_t>(nt, 2)));
+  MG_TRY(b->flags.reserve(std::max<uint32_t>(nt, 2)));
+  k_leaf_boxes<<<ceil_div(nt, 256), 256, 0, s>>>(pos, tris, b->perm.p, nt, (float4*)b->leaf.p);
+  if (nt > 1) {
+    MG_CUDA(cudaMemsetAsync(b->flags.p, 0, 4 * (size_t)(nt - 1), s));
+    k_refit<<<ceil_div(nt, 256), 256, 0, s>>>(b->parent_leaf.p, b->parent_int.p, b->left.p, b->right.p,
+                                             (const float4*)b->leaf.p, (float4*)b->node.p, b->cbox.p, b->flags.p,
+                                             nt);
   }
   MG_CUDA(cudaGetLastError());
   return MGUSO_OK;

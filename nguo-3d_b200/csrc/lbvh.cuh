@@ -11,12 +11,16 @@ struct Lbvh {
   mguso_ctx* ctx = nullptr;
   uint32_t nt = 0;
   int key_bits = 30;
+  bool shaped = false;              // the last build enqueued its whole shape (refits may follow)
   DevBuf<unsigned char> keys;       // nt keys (u32 or u64), sorted after build
   DevBuf<uint32_t> perm;            // sorted leaf -> triangle
   DevBuf<uint32_t> left, right;     // nt - 1 internal nodes
   DevBuf<uint32_t> parent_int, parent_leaf;
   DevBuf<float4> leaf, node;        // 2 float4 per box (lo, hi)
   DevBuf<float4> dleaf, dnode;      // displacement boxes of the same tree (CCD pruning)
+  // per internal node, its two children's boxes side by side (left lo, hi, right lo, hi), so
+  // that a walk reads a node's child indices and their boxes in one round of loads
+  DevBuf<float4> cbox, dcbox;
   DevBuf<uint32_t> flags;
   DevBuf<float> params;             // centroid lo.xyz, inv.xyz
   DevBuf<uint32_t> ord;
@@ -37,6 +41,12 @@ struct Lbvh {
 int radix_sort_pairs(Lbvh* b, void* keys, uint32_t* vals, uint32_t n, int key_bits, cudaStream_t s);
 int lbvh_build(Lbvh* b, const float* pos, uint32_t nv, const uint32_t* tris, uint32_t nt, int key_bits,
                cudaStream_t s);
+// Leaf and node boxes at pos over the tree's existing shape (keys, permutation and children
+// from the last lbvh_build, which must have had the same primitives; MGUSO_ERR_INVALID_ARG
+// when that build did not complete): the boxes are exact
+// unions again, so every overlap query returns the same leaves as after a rebuild at pos,
+// only the shape fits pos less tightly.
+int lbvh_refit_pos(Lbvh* b, const float* pos, const uint32_t* tris, cudaStream_t s);
 // Displacement boxes (AABB of dx over each primitive's vertices, refitted up the tree) into
 // dleaf/dnode, for the CCD's pruning test.
 int lbvh_refit_disp(Lbvh* b, const float* dx, const uint32_t* tris, cudaStream_t s);
@@ -112,7 +122,7 @@ __device__ __forceinline__ bool lbvh_visit(const uint32_t* __restrict__ left, co
 // ok turns false on overflow.
 struct BoxWalk {
   const uint32_t *left, *right, *prim;
-  const float4 *node, *leaf;
+  const float4 *node, *leaf, *cbox;
   uint32_t nt;
   float4 qlo, qhi;
   uint32_t stack[64];
@@ -120,10 +130,10 @@ struct BoxWalk {
   uint32_t cur;
   bool ok;
 
-  __device__ __forceinline__ bool enter(const float4* pb) const {
-    const float4 lo = __ldg(pb), hi = __ldg(pb + 1);
+  __device__ __forceinline__ bool over(const float4& lo, const float4& hi) const {
     return qlo.x <= hi.x && qlo.y <= hi.y && qlo.z <= hi.z && lo.x <= qhi.x && lo.y <= qhi.y && lo.z <= qhi.z;
   }
+  __device__ __forceinline__ bool enter(const float4* pb) const { return over(__ldg(pb), __ldg(pb + 1)); }
   __device__ __forceinline__ int start(bool& done, uint32_t out[2]) {
     sp = 0;
     cur = 0;
@@ -143,13 +153,15 @@ struct BoxWalk {
   __device__ __forceinline__ int step(bool& done, uint32_t out[2]) {
     int n = 0;
     const uint32_t ch[2] = {__ldg(left + cur), __ldg(right + cur)};
+    const float4* cb = cbox + 4 * (size_t)cur;
+    const bool in[2] = {over(__ldg(cb), __ldg(cb + 1)), over(__ldg(cb + 2), __ldg(cb + 3))};
     uint32_t next = 0xffffffffu;
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
       const uint32_t x = ch[c];
       const bool lf = (x & 0x80000000u) != 0;
       const uint32_t i = x & 0x7fffffffu;
-      if (!enter(lf ? leaf + 2 * i : node + 2 * i)) continue;
+      if (!in[c]) continue;
       if (lf) {
         out[n++] = prim[i];
       } else if (next == 0xffffffffu) {
@@ -188,7 +200,7 @@ struct BoxWalk {
 // (the root solves then run on full warps). 64-entry stack; ok turns false on overflow.
 struct CcdWalk {
   const uint32_t *left, *right, *prim;
-  const float4 *node, *leaf, *dnode, *dleaf;
+  const float4 *node, *leaf, *dnode, *dleaf, *cbox, *dcbox;
   uint32_t nt;
   float4 slo, shi, qlo, qhi;
   float3 cq;
@@ -199,7 +211,11 @@ struct CcdWalk {
   bool ok;
 
   __device__ __forceinline__ bool enter(const float4* pb, const float4* db) const {
-    const float4 lo = __ldg(pb), hi = __ldg(pb + 1);
+    return enter_box(__ldg(pb), __ldg(pb + 1), db);
+  }
+  // the test of enter() with the position box given (db: the displacement box, read only
+  // when the pruning bound is needed)
+  __device__ __forceinline__ bool enter_box(const float4 lo, const float4 hi, const float4* db) const {
     if (!(slo.x <= hi.x && slo.y <= hi.y && slo.z <= hi.z && lo.x <= shi.x && lo.y <= shi.y && lo.z <= shi.z))
       return false;
     const float gx = fmaxf(fmaxf(qlo.x - hi.x, lo.x - qhi.x), 0.f);
@@ -238,13 +254,16 @@ struct CcdWalk {
   __device__ __forceinline__ int step(bool& done, uint32_t out[2]) {
     int n = 0;
     const uint32_t ch[2] = {__ldg(left + cur), __ldg(right + cur)};
+    const float4* cb = cbox + 4 * (size_t)cur;
+    const float4* db = dcbox + 4 * (size_t)cur;
+    const bool in[2] = {enter_box(__ldg(cb), __ldg(cb + 1), db), enter_box(__ldg(cb + 2), __ldg(cb + 3), db + 2)};
     uint32_t next = 0xffffffffu;
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
       const uint32_t x = ch[c];
       const bool lf = (x & 0x80000000u) != 0;
       const uint32_t i = x & 0x7fffffffu;
-      if (!(lf ? enter(leaf + 2 * i, dleaf + 2 * i) : enter(node + 2 * i, dnode + 2 * i))) continue;
+      if (!in[c]) continue;
       if (lf) {
         out[n++] = prim[i];
       } else if (next == 0xffffffffu) {

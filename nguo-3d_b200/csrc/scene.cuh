@@ -263,7 +263,9 @@ int finish_rhs(Scene& s);
 int system_spmv(Scene& s, const float* p, float* ap, cudaStream_t st, const DotSink* d);
 
 // contact (contact.cu)
-int build_bvhs(Scene& s, const float* x);
+// The instances' triangle and edge LBVHs at x; refit = true keeps each tree's shape from its
+// last build (the Newton iterations after a step's first) and only recomputes its boxes at x.
+int build_bvhs(Scene& s, const float* x, bool refit = false);
 int pcg_persistent(Scene& s, const uint32_t* h_inst_row, uint32_t ninst, uint32_t active, PcgInstResult* out);
 // out == null defers the results: the caller synchronises the stream later and reads them with
 // pcg_fused_results (the solve itself never waits on the host)
@@ -272,7 +274,9 @@ int pcg_fused_results(Scene& s, uint32_t ninst, PcgInstResult* out);
 int pcg_fused_profile(Scene& s, uint32_t iters, float* us2);
 int pcg_fused_select(Scene& s);  // the fused kernels' variants: pcg_variant, or the autotuner's choice
 int collect_stencils(Scene& s, uint32_t* nst);
-int self_intersections(Scene& s);  // piercing pairs per instance at s.x into red[RED_STRIDE k + 14]
+// piercing pairs per instance at s.x into red[RED_STRIDE k + 14]; refit = true refits the
+// triangle LBVHs built earlier in the step instead of rebuilding them
+int self_intersections(Scene& s, bool refit = false);
 // CCD step fractions of the instances in `active` along s.dx, enqueued without a host wait:
 // ccd_t is the device array of fractions (0 for inactive instances), ccd_results waits for
 // the stream and gives fractions and ACCD cap hits per instance

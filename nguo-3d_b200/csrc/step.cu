@@ -230,7 +230,8 @@ int scene_step(Scene& s, mguso_step_stats* out) {
     uint32_t nst = 0;
     ph[0] = mark();
     if (contacts) {
-      MG_TRY(build_bvhs(s, s.x.p));
+      // the first iterate's tree shapes serve the step's later iterations (boxes refitted)
+      MG_TRY(build_bvhs(s, s.x.p, it > 0));
       MG_TRY(collect_stencils(s, &nst));
     }
     ph[1] = mark();
@@ -316,8 +317,8 @@ int scene_step(Scene& s, mguso_step_stats* out) {
                                                           s.p.contact_dhat, s.red.p);
   MG_CUDA(cudaGetLastError());
   // the self-intersection scan of penetration_free (implicit.rs:2250-2258), with self
-  // collision on, at the committed positions
-  if (contacts) MG_TRY(self_intersections(s));
+  // collision on, at the committed positions (over the triangle trees built in this step)
+  if (contacts) MG_TRY(self_intersections(s, true));
   MG_CUDA(cudaMemcpyAsync(hred.data(), s.red.p, 4 * hred.size(), cudaMemcpyDeviceToHost, st));
   uint32_t dev_status = 0;
   MG_CUDA(cudaMemcpyAsync(&dev_status, s.status.p, 4, cudaMemcpyDeviceToHost, st));
