@@ -196,9 +196,10 @@ int mguso_radix_sort_status(mguso_ctx* ctx);
  * (on every device that loads it, until the process exits), which limits n to 262 144
  * pairs; larger n returns MGUSO_ERR_INVALID_ARG. Sorts the same (key, payload) pairs in
  * place on the current device, stably, with the same result as mguso_radix_sort_pairs, and
- * returns when the sort has finished on `stream`. The first call on each device looks up
- * the array's device address once and keeps it for the life of the process: after
- * cudaDeviceReset on a device it is stale, so a process that resets a device must not call
+ * returns when the sort has finished on `stream`. The first call on each device does a
+ * one-time set-up: it looks up the array's device address and keeps it for the life of the
+ * process, so make that first call before any stream capture begins. After cudaDeviceReset
+ * on a device the kept address is stale, so a process that resets a device must not call
  * this function on it again. All calls share the one array, so calls that overlap on the
  * GPU (other streams, other host threads) race and must be serialised by the caller. */
 int mguso_radix_sort_pairs_noalloc(void* keys, uint32_t* vals, uint32_t n, int key_bits, void* stream);
