@@ -68,7 +68,7 @@ def test_sphere_contact_steps_match_oracle(ctx):
     for k, sg, so, rel in out:
         assert sg["status"] == 0 and sg["all_finite"] and sg["penetration_free"]
         assert abs(sg["newton_iters"] - so["newton_iters"]) <= 1, (k, sg["newton_iters"], so["newton_iters"])
-        assert rel < 2e-2, (k, rel)
+        assert rel < 1e-3, (k, rel)
     assert any(so["num_contacts"] > 0 for _, _, so, _ in out)
 
 
@@ -85,7 +85,11 @@ def test_drape_invariants_on_gpu(ctx):
 @pytest.mark.parametrize("precision", ["fp32", "mixed"])
 def test_self_contact_stencils_and_step(ctx, precision):
     """Two stacked sheets 0.6 mm apart: self-contact stencils active from the first
-    iteration; the GPU step matches the oracle's from the same state."""
+    iteration; the GPU step matches the oracle's from the same state. The first step (11 Newton
+    iterations over 1 286 stencils at 0.6 mm, d-hat 1 mm) has measured 1.9e-4 (FP32) and
+    3.4e-4 (mixed) of its displacement away from the oracle's, against 1e-5 or less for the
+    other steps: its barrier stiffness magnifies the rounding-level differences of the PCG
+    solutions (tolerance 1e-4 per Newton iteration) into the iterate, so the bound is 2e-3."""
     rng = np.random.default_rng(4)
     n = 10
     sc = scenes.sheet_on_sphere(n, side=0.05, height=0.5, jitter=0.0, dhat=1e-3)
@@ -104,7 +108,7 @@ def test_self_contact_stencils_and_step(ctx, precision):
     for k, sg, so, rel in out:
         assert sg["stencils"] == so["stencils"], (k, sg["stencils"], so["stencils"])
         assert abs(sg["newton_iters"] - so["newton_iters"]) <= 1
-        assert rel < 2e-2, (k, rel)
+        assert rel < 2e-3, (k, rel)
 
 
 def coarse_sheath(**kw):
