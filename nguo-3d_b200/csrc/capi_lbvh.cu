@@ -12,6 +12,7 @@ int mguso_lbvh_create(mguso_ctx* ctx, mguso_lbvh** out) {
   MG_CUDA(cudaSetDevice(ctx->device));
   auto* b = new mguso_lbvh();
   b->b.ctx = ctx;
+  b->b.child_boxes = false;  // its point and box queries walk node and leaf boxes only
   *out = b;
   return MGUSO_OK;
 }

@@ -394,7 +394,8 @@ __device__ __forceinline__ void child_box(uint32_t c, const float4* leaf, const 
   hi = __ldcg(src + 1);
 }
 
-// cb (4 float4 per internal node) receives each node's two children's boxes as read.
+// cb (4 float4 per internal node; may be null) receives each node's two children's boxes as
+// read.
 __global__ void k_refit(const uint32_t* __restrict__ parent_leaf, const uint32_t* __restrict__ parent_int,
                         const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
                         const float4* __restrict__ leaf, float4* node, float4* __restrict__ cb, uint32_t* flags,
@@ -414,11 +415,13 @@ __global__ void k_refit(const uint32_t* __restrict__ parent_leaf, const uint32_t
     float4 hi = make_float4(fmaxf(a1.x, b1.x), fmaxf(a1.y, b1.y), fmaxf(a1.z, b1.z), 0.f);
     __stcg(node + 2 * p, lo);
     __stcg(node + 2 * p + 1, hi);
-    float4* c4 = cb + 4 * (size_t)p;
-    c4[0] = a0;
-    c4[1] = a1;
-    c4[2] = b0;
-    c4[3] = b1;
+    if (cb) {
+      float4* c4 = cb + 4 * (size_t)p;
+      c4[0] = a0;
+      c4[1] = a1;
+      c4[2] = b0;
+      c4[3] = b1;
+    }
     p = parent_int[p];
   }
 }
@@ -563,7 +566,7 @@ static int build_impl(Lbvh* b, const float* pos, const uint32_t* tris, uint32_t 
   MG_TRY(b->parent_leaf.reserve(std::max<uint32_t>(nt, 1)));
   MG_TRY(b->leaf.reserve(2 * (size_t)std::max<uint32_t>(nt, 1)));
   MG_TRY(b->node.reserve(2 * (size_t)std::max<uint32_t>(nt, 2)));
-  MG_TRY(b->cbox.reserve(4 * (size_t)std::max<uint32_t>(nt, 2)));
+  if (b->child_boxes) MG_TRY(b->cbox.reserve(4 * (size_t)std::max<uint32_t>(nt, 2)));
   MG_TRY(b->flags.reserve(std::max<uint32_t>(nt, 2)));
   MG_TRY(b->params.reserve(8));
   MG_TRY(b->ord.reserve(8));
@@ -588,8 +591,8 @@ static int build_impl(Lbvh* b, const float* pos, const uint32_t* tris, uint32_t 
   if (nt > 1) {
     MG_CUDA(cudaMemsetAsync(b->flags.p, 0, 4 * (size_t)(nt - 1), s));
     k_refit<<<ceil_div(nt, 256), 256, 0, s>>>(b->parent_leaf.p, b->parent_int.p, b->left.p, b->right.p,
-                                             (const float4*)b->leaf.p, (float4*)b->node.p, b->cbox.p, b->flags.p,
-                                             nt);
+                                             (const float4*)b->leaf.p, (float4*)b->node.p,
+                                             b->child_boxes ? b->cbox.p : nullptr, b->flags.p, nt);
   }
   MG_CUDA(cudaGetLastError());
   if (b->ev_on) cudaEventRecord(b->ev[4], s);
@@ -601,13 +604,13 @@ int lbvh_refit_disp(Lbvh* b, const float* dx, const uint32_t* tris, cudaStream_t
   const uint32_t nt = b->nt;
   MG_TRY(b->dleaf.reserve(2 * (size_t)std::max<uint32_t>(nt, 1)));
   MG_TRY(b->dnode.reserve(2 * (size_t)std::max<uint32_t>(nt, 2)));
-  MG_TRY(b->dcbox.reserve(4 * (size_t)std::max<uint32_t>(nt, 2)));
+  if (b->child_boxes) MG_TRY(b->dcbox.reserve(4 * (size_t)std::max<uint32_t>(nt, 2)));
   if (nt == 0) return MGUSO_OK;
   k_leaf_disp_boxes<<<ceil_div(nt, 256), 256, 0, s>>>(dx, tris, b->perm.p, nt, b->dleaf.p);
   if (nt > 1) {
     MG_CUDA(cudaMemsetAsync(b->flags.p, 0, 4 * (size_t)(nt - 1), s));
     k_refit<<<ceil_div(nt, 256), 256, 0, s>>>(b->parent_leaf.p, b->parent_int.p, b->left.p, b->right.p, b->dleaf.p,
-                                             b->dnode.p, b->dcbox.p, b->flags.p, nt);
+                                             b->dnode.p, b->child_boxes ? b->dcbox.p : nullptr, b->flags.p, nt);
   }
   MG_CUDA(cudaGetLastError());
   return MGUSO_OK;
@@ -620,14 +623,14 @@ int lbvh_refit_pos(Lbvh* b, const float* pos, const uint32_t* tris, cudaStream_t
   // sized by the last build already (these only check, unless that build stopped early)
   MG_TRY(b->leaf.reserve(2 * (size_t)nt));
   MG_TRY(b->node.reserve(2 * (size_t)std::max<uint32_t>(nt, 2)));
-  MG_TRY(b->cbox.reserve(4 * (size_t)std::max<uint32_t>(nt, 2)));
+  if (b->child_boxes) MG_TRY(b->cbox.reserve(4 * (size_t)std::max<uint32_t>(nt, 2)));
   MG_TRY(b->flags.reserve(std::max<uint32_t>(nt, 2)));
   k_leaf_boxes<<<ceil_div(nt, 256), 256, 0, s>>>(pos, tris, b->perm.p, nt, (float4*)b->leaf.p);
   if (nt > 1) {
     MG_CUDA(cudaMemsetAsync(b->flags.p, 0, 4 * (size_t)(nt - 1), s));
     k_refit<<<ceil_div(nt, 256), 256, 0, s>>>(b->parent_leaf.p, b->parent_int.p, b->left.p, b->right.p,
-                                             (const float4*)b->leaf.p, (float4*)b->node.p, b->cbox.p, b->flags.p,
-                                             nt);
+                                             (const float4*)b->leaf.p, (float4*)b->node.p,
+                                             b->child_boxes ? b->cbox.p : nullptr, b->flags.p, nt);
   }
   MG_CUDA(cudaGetLastError());
   return MGUSO_OK;

@@ -19,8 +19,10 @@ struct Lbvh {
   DevBuf<float4> leaf, node;        // 2 float4 per box (lo, hi)
   DevBuf<float4> dleaf, dnode;      // displacement boxes of the same tree (CCD pruning)
   // per internal node, its two children's boxes side by side (left lo, hi, right lo, hi), so
-  // that a walk reads a node's child indices and their boxes in one round of loads
+  // that a walk reads a node's child indices and their boxes in one round of loads; kept only
+  // when child_boxes is set (the scene's trees, whose walks read them)
   DevBuf<float4> cbox, dcbox;
+  bool child_boxes = true;
   DevBuf<uint32_t> flags;
   DevBuf<float> params;             // centroid lo.xyz, inv.xyz
   DevBuf<uint32_t> ord;
