@@ -138,8 +138,10 @@ def triangle_soup(nt: int, seed: int = 3, edge: float = 2.0e-3):
 # (engine-core/src/implicit.rs:30-229).
 # ---------------------------------------------------------------------------------------
 def lame_from_young_poisson(young: float, poisson: float):
-    """material::lame_from_young_poisson (engine-core/src/material.rs:31-45), in f32."""
-    nu = np.float32(min(max(poisson, 1.0e-6), 0.5 - 1.0e-4))
+    """material::lame_from_young_poisson (engine-core/src/material.rs:31-45), in f32: the
+    Poisson ratio clamped into [1e-6, 0.5 - 1e-4], a non-finite one replaced by 0.35."""
+    p = float(poisson)
+    nu = np.float32(min(max(p, 1.0e-6), 0.5 - 1.0e-4)) if np.isfinite(p) else np.float32(0.35)
     y = np.float32(young)
     mu = y / (np.float32(2.0) * (np.float32(1.0) + nu))
     lam = y * nu / ((np.float32(1.0) + nu) * (np.float32(1.0) - np.float32(2.0) * nu))

@@ -1399,6 +1399,139 @@ inline void for_each_edge_edge_pair(const std::vector<Vt<R>>& pos, const std::ve
   }
 }
 
+// The cells of an edge's or a triangle's box padded by `search` (the edge/triangle grids of
+// broadphase.rs:523-751 key a coordinate as floor(v / cell) in the scalar type).
+template <class R>
+struct EtCells {
+  const std::vector<Vt<R>>& pos;
+  R search, inv;
+  CellKey key(const Vt<R>& p) const {
+    return CellKey{floor_i32((double)(p.x * inv)), floor_i32((double)(p.y * inv)), floor_i32((double)(p.z * inv))};
+  }
+  void edge(const std::array<uint32_t, 2>& e, CellKey& lo, CellKey& hi) const {
+    const Vt<R> p = pos[e[0]], q = pos[e[1]], pad(search, search, search);
+    lo = key(p.vmin(q) - pad);
+    hi = key(p.vmax(q) + pad);
+  }
+  void tri(const std::array<uint32_t, 3>& t, CellKey& lo, CellKey& hi) const {
+    const Vt<R> a = pos[t[0]], b = pos[t[1]], c = pos[t[2]], pad(search, search, search);
+    lo = key(a.vmin(b).vmin(c) - pad);
+    hi = key(a.vmax(b).vmax(c) + pad);
+  }
+};
+
+inline bool et_adjacent(const std::array<uint32_t, 2>& e, const std::array<uint32_t, 3>& t) {
+  return e[0] == t[0] || e[0] == t[1] || e[0] == t[2] || e[1] == t[0] || e[1] == t[1] || e[1] == t[2];
+}
+
+// edge_triangle_pairs (broadphase.rs:523-585): every edge hashed into the cells of its box
+// padded by search, every triangle's padded cells scanned; pairs sharing a vertex skipped;
+// the (edge, triangle) pairs sorted and deduplicated. Cell size: grid_cell(search,
+// max(mean edge length, mean triangle extent)).
+template <class R>
+inline std::vector<std::pair<uint32_t, uint32_t>> edge_triangle_pairs(const std::vector<Vt<R>>& pos,
+                                                                      const std::vector<std::array<uint32_t, 2>>& edges,
+                                                                      const std::vector<std::array<uint32_t, 3>>& tris,
+                                                                      R search) {
+  std::vector<std::pair<uint32_t, uint32_t>> pairs;
+  if (edges.empty() || tris.empty()) return pairs;
+  const R cell = grid_cell(search, rmax(mean_edge_len(pos, edges), mean_tri_extent(pos, tris)));
+  const EtCells<R> cells{pos, search, R(1) / cell};
+  std::vector<std::pair<CellKey, uint32_t>> ins;
+  for (size_t ei = 0; ei < edges.size(); ++ei) {
+    CellKey lo, hi;
+    cells.edge(edges[ei], lo, hi);
+    for (int32_t cx = lo.x; cx <= hi.x; ++cx)
+      for (int32_t cy = lo.y; cy <= hi.y; ++cy)
+        for (int32_t cz = lo.z; cz <= hi.z; ++cz) ins.push_back({CellKey{cx, cy, cz}, (uint32_t)ei});
+  }
+  CellGrid grid;
+  grid.build(ins);
+  for (size_t ti = 0; ti < tris.size(); ++ti) {
+    CellKey lo, hi;
+    cells.tri(tris[ti], lo, hi);
+    for (int32_t cx = lo.x; cx <= hi.x; ++cx)
+      for (int32_t cy = lo.y; cy <= hi.y; ++cy)
+        for (int32_t cz = lo.z; cz <= hi.z; ++cz)
+          grid.each(CellKey{cx, cy, cz}, [&](uint32_t ei) {
+            if (!et_adjacent(edges[ei], tris[ti])) pairs.push_back({ei, (uint32_t)ti});
+          });
+  }
+  std::sort(pairs.begin(), pairs.end());
+  pairs.erase(std::unique(pairs.begin(), pairs.end()), pairs.end());
+  return pairs;
+}
+
+// any_edge_triangle_pair (broadphase.rs:587-751): the candidates of edge_triangle_pairs
+// streamed to hit(edge, triangle) until it returns true (the return value). With a movable
+// mask (u8 per vertex; empty = unfiltered) it runs two passes, each indexing only the
+// movable primitives of one kind: pass A hashes the edges with a movable vertex and scans
+// every triangle, pass B hashes the triangles with a movable vertex and scans the edges
+// with none, so pairs whose every vertex is immovable are never offered. A pair may be
+// offered more than once (an edge and a triangle sharing several cells).
+template <class R, class F>
+inline bool any_edge_triangle_pair(const std::vector<Vt<R>>& pos, const std::vector<std::array<uint32_t, 2>>& edges,
+                                   const std::vector<std::array<uint32_t, 3>>& tris, R search,
+                                   const std::vector<uint8_t>& movable, F hit) {
+  if (edges.empty() || tris.empty()) return false;
+  const R cell = grid_cell(search, rmax(mean_edge_len(pos, edges), mean_tri_extent(pos, tris)));
+  const EtCells<R> cells{pos, search, R(1) / cell};
+  auto e_mov = [&](const std::array<uint32_t, 2>& e) { return movable.empty() || movable[e[0]] || movable[e[1]]; };
+  auto t_mov = [&](const std::array<uint32_t, 3>& t) {
+    return movable.empty() || movable[t[0]] || movable[t[1]] || movable[t[2]];
+  };
+  // pass A: movable edges indexed, every triangle scanned
+  std::vector<std::pair<CellKey, uint32_t>> ins;
+  for (size_t ei = 0; ei < edges.size(); ++ei) {
+    if (!e_mov(edges[ei])) continue;
+    CellKey lo, hi;
+    cells.edge(edges[ei], lo, hi);
+    for (int32_t cx = lo.x; cx <= hi.x; ++cx)
+      for (int32_t cy = lo.y; cy <= hi.y; ++cy)
+        for (int32_t cz = lo.z; cz <= hi.z; ++cz) ins.push_back({CellKey{cx, cy, cz}, (uint32_t)ei});
+  }
+  bool found = false;
+  {
+    CellGrid grid;
+    grid.build(ins);
+    for (size_t ti = 0; ti < tris.size() && !found; ++ti) {
+      CellKey lo, hi;
+      cells.tri(tris[ti], lo, hi);
+      for (int32_t cx = lo.x; cx <= hi.x && !found; ++cx)
+        for (int32_t cy = lo.y; cy <= hi.y && !found; ++cy)
+          for (int32_t cz = lo.z; cz <= hi.z && !found; ++cz)
+            grid.each(CellKey{cx, cy, cz}, [&](uint32_t ei) {
+              if (!found && !et_adjacent(edges[ei], tris[ti]) && hit(ei, (uint32_t)ti)) found = true;
+            });
+    }
+  }
+  if (found || movable.empty()) return found;
+  // pass B: movable triangles indexed, the edges with no movable vertex scanned
+  ins.clear();
+  for (size_t ti = 0; ti < tris.size(); ++ti) {
+    if (!t_mov(tris[ti])) continue;
+    CellKey lo, hi;
+    cells.tri(tris[ti], lo, hi);
+    for (int32_t cx = lo.x; cx <= hi.x; ++cx)
+      for (int32_t cy = lo.y; cy <= hi.y; ++cy)
+        for (int32_t cz = lo.z; cz <= hi.z; ++cz) ins.push_back({CellKey{cx, cy, cz}, (uint32_t)ti});
+  }
+  CellGrid tgrid;
+  tgrid.build(ins);
+  for (size_t ei = 0; ei < edges.size() && !found; ++ei) {
+    if (e_mov(edges[ei])) continue;  // pass A offered it against every triangle
+    CellKey lo, hi;
+    cells.edge(edges[ei], lo, hi);
+    for (int32_t cx = lo.x; cx <= hi.x && !found; ++cx)
+      for (int32_t cy = lo.y; cy <= hi.y && !found; ++cy)
+        for (int32_t cz = lo.z; cz <= hi.z && !found; ++cz)
+          tgrid.each(CellKey{cx, cy, cz}, [&](uint32_t ti) {
+            if (!found && !et_adjacent(edges[ei], tris[ti]) && hit((uint32_t)ei, ti)) found = true;
+          });
+  }
+  return found;
+}
+
 inline std::vector<std::vector<uint32_t>> one_ring_exclusion(size_t nv, const std::vector<std::array<uint32_t, 3>>& tris) {
   std::vector<std::vector<uint32_t>> ex(nv);
   for (size_t i = 0; i < nv; ++i) ex[i].push_back((uint32_t)i);
@@ -2367,90 +2500,18 @@ struct ImplicitSolver {
     return rclamp(t, T_MIN, R(1));
   }
 
-  // has_self_intersection (implicit.rs:618-650) via a plain grid over edge/triangle boxes.
-  // positions_self_intersect (implicit.rs:618-643) over any_edge_triangle_pair
-  // (broadphase.rs:609-751): a grid of cell size max(char_len, mean edge length, mean
-  // triangle extent); pass A hashes the movable edges into the cells of their boxes padded by
-  // char_len and scans every triangle's padded cells, pass B hashes the movable triangles and
-  // scans the edges with no movable vertex. Pairs sharing a vertex are skipped; true at the
-  // first piercing pair.
+  // has_self_intersection (implicit.rs:618-650): positions_self_intersect (implicit.rs:618-643)
+  // streams the candidates of any_edge_triangle_pair (broadphase.rs:587-751) at search =
+  // char_len over the movable mask and stops at the first pair that edge_triangle_intersect
+  // reports piercing.
   bool positions_self_intersect(const std::vector<V>& x) const {
     if (edges.empty() || collision_tris.empty()) return false;
-    const auto mov = movable_mask();
-    const R search = char_len;
-    const R cell = grid_cell(search, rmax(mean_edge_len(x, edges), mean_tri_extent(x, collision_tris)));
-    const R inv = R(1) / cell;
-    auto key = [&](R v) { return floor_i32((double)(v * inv)); };
-    const V pad(search, search, search);
-    auto edge_box = [&](const Edge& e, CellKey& lo, CellKey& hi) {
-      const V p = x[e[0]], q = x[e[1]];
-      const V l = p.vmin(q) - pad, h = p.vmax(q) + pad;
-      lo = CellKey{key(l.x), key(l.y), key(l.z)};
-      hi = CellKey{key(h.x), key(h.y), key(h.z)};
-    };
-    auto tri_box = [&](const Tri& t, CellKey& lo, CellKey& hi) {
-      const V a = x[t[0]], b = x[t[1]], c = x[t[2]];
-      const V l = a.vmin(b).vmin(c) - pad, h = a.vmax(b).vmax(c) + pad;
-      lo = CellKey{key(l.x), key(l.y), key(l.z)};
-      hi = CellKey{key(h.x), key(h.y), key(h.z)};
-    };
-    auto e_mov = [&](const Edge& e) { return mov.empty() || mov[e[0]] || mov[e[1]]; };
-    auto t_mov = [&](const Tri& t) { return mov.empty() || mov[t[0]] || mov[t[1]] || mov[t[2]]; };
-    auto pierces = [&](const Edge& e, const Tri& t) {
-      if (e[0] == t[0] || e[0] == t[1] || e[0] == t[2] || e[1] == t[0] || e[1] == t[1] || e[1] == t[2])
-        return false;  // shared vertex: adjacent
-      return edge_triangle_intersect(x[e[0]], x[e[1]], x[t[0]], x[t[1]], x[t[2]]);
-    };
-    // pass A: movable edges indexed, every triangle scanned
-    std::vector<std::pair<CellKey, uint32_t>> ins;
-    for (size_t ei = 0; ei < edges.size(); ++ei) {
-      if (!e_mov(edges[ei])) continue;
-      CellKey lo, hi;
-      edge_box(edges[ei], lo, hi);
-      for (int32_t cx = lo.x; cx <= hi.x; ++cx)
-        for (int32_t cy = lo.y; cy <= hi.y; ++cy)
-          for (int32_t cz = lo.z; cz <= hi.z; ++cz) ins.push_back({CellKey{cx, cy, cz}, (uint32_t)ei});
-    }
-    CellGrid grid;
-    grid.build(ins);
-    bool hit = false;
-    for (size_t ti = 0; ti < collision_tris.size() && !hit; ++ti) {
-      const Tri& t = collision_tris[ti];
-      CellKey lo, hi;
-      tri_box(t, lo, hi);
-      for (int32_t cx = lo.x; cx <= hi.x && !hit; ++cx)
-        for (int32_t cy = lo.y; cy <= hi.y && !hit; ++cy)
-          for (int32_t cz = lo.z; cz <= hi.z && !hit; ++cz)
-            grid.each(CellKey{cx, cy, cz}, [&](uint32_t ei) {
-              if (!hit && pierces(edges[ei], t)) hit = true;
-            });
-    }
-    if (hit || mov.empty()) return hit;
-    // pass B: movable triangles indexed, the edges with no movable vertex scanned
-    ins.clear();
-    for (size_t ti = 0; ti < collision_tris.size(); ++ti) {
-      if (!t_mov(collision_tris[ti])) continue;
-      CellKey lo, hi;
-      tri_box(collision_tris[ti], lo, hi);
-      for (int32_t cx = lo.x; cx <= hi.x; ++cx)
-        for (int32_t cy = lo.y; cy <= hi.y; ++cy)
-          for (int32_t cz = lo.z; cz <= hi.z; ++cz) ins.push_back({CellKey{cx, cy, cz}, (uint32_t)ti});
-    }
-    CellGrid tgrid;
-    tgrid.build(ins);
-    for (size_t ei = 0; ei < edges.size() && !hit; ++ei) {
-      const Edge& e = edges[ei];
-      if (e_mov(e)) continue;
-      CellKey lo, hi;
-      edge_box(e, lo, hi);
-      for (int32_t cx = lo.x; cx <= hi.x && !hit; ++cx)
-        for (int32_t cy = lo.y; cy <= hi.y && !hit; ++cy)
-          for (int32_t cz = lo.z; cz <= hi.z && !hit; ++cz)
-            tgrid.each(CellKey{cx, cy, cz}, [&](uint32_t ti) {
-              if (!hit && pierces(e, collision_tris[ti])) hit = true;
-            });
-    }
-    return hit;
+    return any_edge_triangle_pair<R>(x, edges, collision_tris, char_len, movable_mask(),
+                                     [&](uint32_t ei, uint32_t ti) {
+                                       const Edge& e = edges[ei];
+                                       const Tri& t = collision_tris[ti];
+                                       return edge_triangle_intersect(x[e[0]], x[e[1]], x[t[0]], x[t[1]], x[t[2]]);
+                                     });
   }
 
   // step (implicit.rs:1951-2191)

@@ -288,6 +288,11 @@ def _step_sigs(lib):
         "oracle_ee_pairs": (C.c_uint64, [u32, vp, u32, vp, f32, vp, vp, C.c_uint64]),
         "oracle_unique_edges": (u32, [u32, vp, vp]),
         "oracle_grid_cell": (f32, [f32, f32]),
+        "oracle_et_pairs": (C.c_uint64, [u32, vp, u32, vp, u32, vp, f32, vp, C.c_uint64]),
+        "oracle_sym_eig2": (None, [vp, vp, vp]),
+        "oracle_svd3x2": (None, [vp, vp, vp, vp]),
+        "oracle_stvk_density": (f32, [vp, f32, f32, vp, vp]),
+        "oracle_et_any": (i32, [u32, vp, u32, vp, u32, vp, f32, vp, i32, vp, C.c_uint64, vp]),
         "oracle_edge_triangle_intersect": (i32, [vp]),
         "oracle_closest_point": (None, [vp, vp, vp]),
         "oracle_ee_witness": (None, [vp, vp]),
@@ -639,6 +644,68 @@ def ee_pairs(pos, edges, search, movable=None):
     e = np.ascontiguousarray(edges, np.uint32).reshape(-1, 2)
     m = None if movable is None or len(movable) == 0 else np.ascontiguousarray(movable, np.uint8)
     return _pairs(lib.oracle_ee_pairs, p.shape[0], _p(p), e.shape[0], _p(e), search, _p(m))
+
+
+def sym_eig2(p, q, r):
+    """sym_eig2 (shell_model.rs:60-78) of [[p, q], [q, r]] in f32: (eigenvalues descending,
+    eigenvectors as the columns of a 2x2)."""
+    a = np.array([p, q, r], np.float32)
+    lam = np.zeros(2, np.float32)
+    v = np.zeros(4, np.float32)
+    _lib_elem().oracle_sym_eig2(_p(a), _p(lam), _p(v))
+    return lam, v.reshape(2, 2).T
+
+
+def svd3x2(f):
+    """svd3x2 (shell_model.rs:84-106) of a 3x2 F in f32: (U 3x2, sigma descending, V 2x2)."""
+    fc = np.ascontiguousarray(np.asarray(f, np.float32).T)
+    u = np.zeros(6, np.float32)
+    s = np.zeros(2, np.float32)
+    v = np.zeros(4, np.float32)
+    _lib_elem().oracle_svd3x2(_p(fc), _p(u), _p(s), _p(v))
+    return u.reshape(2, 3).T, s, v.reshape(2, 2).T
+
+
+def stvk_density(sigma, mu, lam):
+    """The StVK shell density over principal stretches (shell_model.rs:131-176) in f32:
+    (psi, gradient 2, Hessian 2x2)."""
+    s = np.ascontiguousarray(sigma, np.float32)
+    g = np.zeros(2, np.float32)
+    h = np.zeros(4, np.float32)
+    e = _lib_elem().oracle_stvk_density(_p(s), mu, lam, _p(g), _p(h))
+    return float(e), g, h.reshape(2, 2)
+
+
+def et_pairs(pos, edges, tris, search):
+    """edge_triangle_pairs (broadphase.rs:523-585): sorted unique (edge, triangle) candidates."""
+    lib = _lib_elem()
+    p = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+    e = np.ascontiguousarray(edges, np.uint32).reshape(-1, 2)
+    t = np.ascontiguousarray(tris, np.uint32).reshape(-1, 3)
+    return _pairs(lib.oracle_et_pairs, p.shape[0], _p(p), e.shape[0], _p(e), t.shape[0], _p(t), search)
+
+
+ET_NEVER, ET_FIRST, ET_PIERCE = 0, 1, 2
+
+
+def et_any(pos, edges, tris, search, movable=None, mode=ET_NEVER):
+    """any_edge_triangle_pair (broadphase.rs:587-751) with the predicate `mode`: ET_NEVER (never
+    matches; the candidates offered are returned, repeats included), ET_FIRST (matches the first
+    candidate) or ET_PIERCE (edge_triangle_intersect). Returns (matched, offered): offered is
+    the list of (edge, triangle) pairs for ET_NEVER, else the number of candidates seen."""
+    lib = _lib_elem()
+    p = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+    e = np.ascontiguousarray(edges, np.uint32).reshape(-1, 2)
+    t = np.ascontiguousarray(tris, np.uint32).reshape(-1, 3)
+    m = None if movable is None or len(movable) == 0 else np.ascontiguousarray(movable, np.uint8)
+    n = np.zeros(1, np.uint64)
+    args = (p.shape[0], _p(p), e.shape[0], _p(e), t.shape[0], _p(t), search, _p(m), mode)
+    found = lib.oracle_et_any(*args, None, 0, _p(n))
+    if mode != ET_NEVER:
+        return bool(found), int(n[0])
+    out = np.empty((max(int(n[0]), 1), 2), np.uint32)
+    found = lib.oracle_et_any(*args, _p(out), int(n[0]), _p(n))
+    return bool(found), [tuple(r) for r in out[:int(n[0])].tolist()]
 
 
 def unique_edges(tris):

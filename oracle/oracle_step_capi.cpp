@@ -695,6 +695,91 @@ uint64_t oracle_ee_pairs(uint32_t nv, const float* pos, uint32_t ne, const uint3
   return pr.size();
 }
 
+// sym_eig2 (shell_model.rs:60-78) in f32 of the symmetric [[p, q], [q, r]] (a3 = p, q, r):
+// eigenvalues descending into l2, eigenvectors as the columns of v4 (column-major).
+void oracle_sym_eig2(const float* a3, float* l2, float* v4) {
+  Mat2<float> a{a3[0], a3[1], a3[1], a3[2]}, v{};
+  sym_eig2(a, l2, v);
+  v4[0] = v.xx;
+  v4[1] = v.xy;
+  v4[2] = v.yx;
+  v4[3] = v.yy;
+}
+
+// svd3x2 (shell_model.rs:84-106) in f32 of F (f6: column 0 xyz, then column 1 xyz): U's two
+// columns into u6 the same way, sigma descending into s2, V column-major into v4.
+void oracle_svd3x2(const float* f6, float* u6, float* s2, float* v4) {
+  Mat3x2<float> f{Vt<float>(f6[0], f6[1], f6[2]), Vt<float>(f6[3], f6[4], f6[5])}, u{};
+  Mat2<float> v{};
+  svd3x2(f, u, s2, v);
+  const float uu[6] = {u.c0.x, u.c0.y, u.c0.z, u.c1.x, u.c1.y, u.c1.z};
+  for (int k = 0; k < 6; ++k) u6[k] = uu[k];
+  v4[0] = v.xx;
+  v4[1] = v.xy;
+  v4[2] = v.yx;
+  v4[3] = v.yy;
+}
+
+// The StVK shell density over principal stretches (shell_model.rs:131-176) in f32: returns
+// psi(s2), its gradient into g2 and its Hessian (row-major 2x2) into h4.
+float oracle_stvk_density(const float* s2, float mu, float lambda, float* g2, float* h4) {
+  stvk_dpsi(s2, mu, lambda, g2);
+  stvk_d2psi(s2, mu, lambda, h4);
+  return stvk_density(s2, mu, lambda);
+}
+
+// edge_triangle_pairs (broadphase.rs:523-585) in f32: the sorted unique (edge, triangle)
+// candidate pairs into out (2 u32 each, up to cap); returns the count.
+uint64_t oracle_et_pairs(uint32_t nv, const float* pos, uint32_t ne, const uint32_t* edges, uint32_t nt,
+                         const uint32_t* tris, float search, uint32_t* out, uint64_t cap) {
+  std::vector<Vt<float>> P(nv);
+  for (uint32_t i = 0; i < nv; ++i) P[i] = Vt<float>(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+  std::vector<std::array<uint32_t, 2>> E(ne);
+  for (uint32_t e = 0; e < ne; ++e) E[e] = {edges[2 * e], edges[2 * e + 1]};
+  std::vector<std::array<uint32_t, 3>> T(nt);
+  for (uint32_t t = 0; t < nt; ++t) T[t] = {tris[3 * t], tris[3 * t + 1], tris[3 * t + 2]};
+  const auto pr = edge_triangle_pairs<float>(P, E, T, search);
+  for (size_t i = 0; i < pr.size() && i < cap; ++i) {
+    out[2 * i] = pr[i].first;
+    out[2 * i + 1] = pr[i].second;
+  }
+  return pr.size();
+}
+
+// any_edge_triangle_pair (broadphase.rs:587-751) in f32 with one of three predicates: mode 0
+// never matches (every candidate offered is written to out, repeats included, up to cap),
+// mode 1 matches the first candidate offered, mode 2 is edge_triangle_intersect. movable
+// (u8 per vertex) may be null. *offered = the number of candidates the predicate saw; returns
+// 1 when it matched.
+int oracle_et_any(uint32_t nv, const float* pos, uint32_t ne, const uint32_t* edges, uint32_t nt,
+                  const uint32_t* tris, float search, const uint8_t* movable, int mode, uint32_t* out, uint64_t cap,
+                  uint64_t* offered) {
+  std::vector<Vt<float>> P(nv);
+  for (uint32_t i = 0; i < nv; ++i) P[i] = Vt<float>(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+  std::vector<std::array<uint32_t, 2>> E(ne);
+  for (uint32_t e = 0; e < ne; ++e) E[e] = {edges[2 * e], edges[2 * e + 1]};
+  std::vector<std::array<uint32_t, 3>> T(nt);
+  for (uint32_t t = 0; t < nt; ++t) T[t] = {tris[3 * t], tris[3 * t + 1], tris[3 * t + 2]};
+  std::vector<uint8_t> mov = movable ? std::vector<uint8_t>(movable, movable + nv) : std::vector<uint8_t>();
+  uint64_t n = 0;
+  const bool found = any_edge_triangle_pair<float>(P, E, T, search, mov, [&](uint32_t ei, uint32_t ti) {
+    if (mode == 0 && out && n < cap) {
+      out[2 * n] = ei;
+      out[2 * n + 1] = ti;
+    }
+    ++n;
+    if (mode == 1) return true;
+    if (mode == 2) {
+      const auto& e = E[ei];
+      const auto& t = T[ti];
+      return edge_triangle_intersect(P[e[0]], P[e[1]], P[t[0]], P[t[1]], P[t[2]]);
+    }
+    return false;
+  });
+  if (offered) *offered = n;
+  return found ? 1 : 0;
+}
+
 // unique_edges (broadphase.rs:332-343) into out (2 u32 each, room for 3 nt); returns the count.
 uint32_t oracle_unique_edges(uint32_t nt, const uint32_t* tris, uint32_t* out) {
   std::vector<std::array<uint32_t, 3>> T(nt);

@@ -69,6 +69,17 @@ def test_parses_param_toml_from_text(tmp_path):  # golden.rs:1984-2001
     assert p["cg_tol"] == 1.0e-3  # unparsable: the default stays
 
 
+def test_friction_mode_parsing_falls_back_to_the_reference_default(tmp_path):  # contact.rs:1144-1165
+    """The spellings of FrictionMode::from_str_or_default's test as param.toml values (the
+    reader trims the value and its quotes as golden.rs:514-522 does); the default is min."""
+    for text, want in (("max", "max"), ('"max"', "max"), (" mean ", "mean"), ("min", "min"),
+                       ("wobble", "min"), ("", "min")):
+        (tmp_path / "param.toml").write_text(f"[param]\nfriction_mode = {text}\n")
+        assert cap.read_param_toml(str(tmp_path))["friction_mode"] == want, text
+    (tmp_path / "param.toml").write_text("[param]\ndt = 0.002\n")
+    assert cap.read_param_toml(str(tmp_path))["friction_mode"] == "min"
+
+
 def test_reads_material_means_from_synthetic(tmp_path):  # golden.rs:2003-2028
     d = tmp_path / "input_bin" / "param"
     d.mkdir(parents=True)

@@ -1,7 +1,9 @@
 """The oracle's uniform-grid broad phase (broadphase.rs restated in oracle/implicit_oracle.hpp)
 against the reference's own broad-phase tests: candidates are a superset of brute force,
-the movable filter drops exactly the inert pairs, and the edge-edge candidate count of the
-reference's fixture is its pinned number (broadphase.rs:994-1002: 268 075 over 5 162 edges).
+the movable filter drops exactly the inert pairs, the edge-edge candidate count of the
+reference's fixture is its pinned number (broadphase.rs:994-1002: 268 075 over 5 162 edges),
+and the self-intersection predicate's streamed edge-triangle candidates equal the
+materialised list, stop at the first match and see cloth-through-body pierces only.
 """
 import numpy as np
 import oracle_py as O
@@ -184,3 +186,75 @@ def test_edge_triangle_intersect_cases():  # contact.rs:1816-1853
     assert not O.edge_triangle_intersect((0.25, 0.25, 1), (0.25, 0.25, 0.5), a, b, c)  # same side
     assert not O.edge_triangle_intersect((2, 0.25, 1), (2, 0.25, -1), a, b, c)  # outside the triangle
     assert not O.edge_triangle_intersect((-1, 0.25, 0), (2, 0.25, 0), a, b, c)  # coplanar
+
+
+def stabbed_sheet():
+    """broadphase.rs:1011-1033: a 7 x 7 sheet at 0.1 spacing and a vertical edge through it
+    near its middle, appended after the sheet's unique edges."""
+    p, t = _grid(7, 0.1, 0.0, 0, True)
+    base = len(p)
+    pos = np.array(p + [(0.32, -0.2, 0.31), (0.32, 0.2, 0.31)], f32)
+    tris = np.array(t, np.uint32)
+    edges = np.concatenate([O.unique_edges(tris), np.array([[base, base + 1]], np.uint32)])
+    return pos, edges, tris
+
+
+def test_streaming_offers_the_same_candidate_set_as_the_materialised_list():  # broadphase.rs:1036-1066
+    pos, edges, tris = stabbed_sheet()
+    for search in (0.05, 0.15, 0.4):
+        want = O.et_pairs(pos, edges, tris, search)
+        found, got = O.et_any(pos, edges, tris, search, mode=O.ET_NEVER)
+        assert not found, "a never-matching predicate must exhaust the candidates"
+        assert sorted(set(got)) == want, search
+        assert want, search
+
+
+def test_streaming_short_circuits_on_the_first_match():  # broadphase.rs:1068-1086
+    pos, edges, tris = stabbed_sheet()
+    total = len(O.et_pairs(pos, edges, tris, 0.4))
+    found, seen = O.et_any(pos, edges, tris, 0.4, mode=O.ET_FIRST)
+    assert found and seen == 1
+    assert total > 10
+
+
+def test_streaming_agrees_on_whether_an_edge_pierces():  # broadphase.rs:1088-1117
+    pos, edges, tris = stabbed_sheet()
+    assert O.et_any(pos, edges, tris, 0.15, mode=O.ET_PIERCE)[0], "the spike through the sheet must be detected"
+    pos[-2, 1] = 0.2
+    pos[-1, 1] = 0.6
+    assert not O.et_any(pos, edges, tris, 0.15, mode=O.ET_PIERCE)[0], "a spike clear of the sheet must not be"
+
+
+def test_the_intersection_predicate_sees_cloth_through_body_but_not_body_through_body():  # broadphase.rs:1279-1346
+    pos, tris, edges, movable = two_sheets()
+
+    def pierced(pos, edges, movable):
+        return O.et_any(pos, edges, tris, 0.05, movable=movable, mode=O.ET_PIERCE)[0]
+
+    assert not pierced(pos, edges, movable), "the undisturbed two-sheet scene must not intersect"
+    # a movable spike through the static lower sheet, ending below the movable upper one
+    base = len(pos)
+    pos = np.concatenate([pos, np.array([(0.12, 0.015, 0.13), (0.12, -0.03, 0.13)], f32)])
+    movable = np.concatenate([movable, np.ones(2, np.uint8)])
+    edges = np.concatenate([edges, np.array([[base, base + 1]], np.uint32)])
+    assert pierced(pos, edges, movable), "a movable edge piercing the static body must be reported"
+    # the same spike static: a pierce between immovable primitives only is not reported ...
+    movable[base] = movable[base + 1] = 0
+    assert not pierced(pos, edges, movable)
+    # ... although it is there: unfiltered, it is found
+    assert pierced(pos, edges, None)
+    # a static edge through the movable upper sheet (the second pass's case)
+    base = len(pos)
+    pos = np.concatenate([pos, np.array([(0.07, 0.05, 0.08), (0.07, 0.008, 0.08)], f32)])
+    movable = np.concatenate([movable, np.zeros(2, np.uint8)])
+    edges = np.concatenate([edges, np.array([[base, base + 1]], np.uint32)])
+    assert pierced(pos, edges, movable), "a static edge piercing a movable triangle must be reported"
+
+
+def test_edges_are_unique_and_deterministic():  # geometry.rs:50-63
+    tris = np.array([[0, 1, 2], [2, 1, 3]], np.uint32)
+    e = O.unique_edges(tris)
+    assert len(e) == 5
+    assert np.array_equal(e, O.unique_edges(tris))
+    assert sum(1 for a, b in e.tolist() if (a, b) == (1, 2)) == 1
+    assert e.tolist() == sorted(e.tolist())
