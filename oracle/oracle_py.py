@@ -290,6 +290,7 @@ def _step_sigs(lib):
         "oracle_grid_cell": (f32, [f32, f32]),
         "oracle_et_pairs": (C.c_uint64, [u32, vp, u32, vp, u32, vp, f32, vp, C.c_uint64]),
         "oracle_sym_eig2": (None, [vp, vp, vp]),
+        "oracle_asm_blocks": (None, [u32, u32, vp, u32, vp, vp, vp]),
         "oracle_svd3x2": (None, [vp, vp, vp, vp]),
         "oracle_stvk_density": (f32, [vp, f32, f32, vp, vp]),
         "oracle_et_any": (i32, [u32, vp, u32, vp, u32, vp, f32, vp, i32, vp, C.c_uint64, vp]),
@@ -644,6 +645,17 @@ def ee_pairs(pos, edges, search, movable=None):
     e = np.ascontiguousarray(edges, np.uint32).reshape(-1, 2)
     m = None if movable is None or len(movable) == 0 else np.ascontiguousarray(movable, np.uint8)
     return _pairs(lib.oracle_ee_pairs, p.shape[0], _p(p), e.shape[0], _p(e), search, _p(m))
+
+
+def asm_blocks(nv, slot_pairs, triplets):
+    """The assembler's elastic-block gather: triplets (row, col, value) pushed in order with
+    the vertex pairs slot_pairs requested; returns one row-major 3x3 block per slot."""
+    keys = np.ascontiguousarray(slot_pairs, np.uint32).reshape(-1, 2)
+    rc = np.ascontiguousarray([(r, c) for r, c, _ in triplets], np.uint32).reshape(-1, 2)
+    v = np.ascontiguousarray([t[2] for t in triplets], np.float32)
+    out = np.zeros((len(keys), 3, 3), np.float32)
+    _lib_elem().oracle_asm_blocks(nv, len(keys), _p(keys), len(v), _p(rc), _p(v), _p(out))
+    return out
 
 
 def sym_eig2(p, q, r):

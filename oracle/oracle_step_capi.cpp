@@ -695,6 +695,28 @@ uint64_t oracle_ee_pairs(uint32_t nv, const float* pos, uint32_t ne, const uint3
   return pr.size();
 }
 
+// The assembler's elastic-block gather (Asm::push into its requested blocks, implicit.rs
+// Asm; the blocks the Rayleigh stiffnesses read): the n_trips triplets (row trip_rc[2k],
+// column trip_rc[2k + 1], value trip_v[k], scalar indices) pushed in order over nv vertices
+// with the vertex pairs (slot_keys[2s], slot_keys[2s + 1]) requested as slots s; each slot's
+// row-major 3x3 block into out (9 floats per slot).
+void oracle_asm_blocks(uint32_t nv, uint32_t n_slots, const uint32_t* slot_keys, uint32_t n_trips,
+                       const uint32_t* trip_rc, const float* trip_v, float* out) {
+  std::unordered_map<uint64_t, size_t> slots;
+  for (uint32_t k = 0; k < n_slots; ++k) slots[((uint64_t)slot_keys[2 * k] << 32) | slot_keys[2 * k + 1]] = k;
+  TripletSinkT<float> sink;
+  sink.begin(3 * (size_t)nv);
+  std::vector<uint8_t> pinned(nv, 0);
+  ImplicitSolver<float>::Asm a;
+  a.sink = &sink;
+  a.slots = &slots;
+  a.blocks.assign(n_slots, std::array<float, 9>{});
+  a.pinned = &pinned;
+  for (uint32_t k = 0; k < n_trips; ++k) a.push(trip_rc[2 * k], trip_rc[2 * k + 1], trip_v[k]);
+  for (uint32_t k = 0; k < n_slots; ++k)
+    for (int q = 0; q < 9; ++q) out[9 * k + q] = a.blocks[k][q];
+}
+
 // sym_eig2 (shell_model.rs:60-78) in f32 of the symmetric [[p, q], [q, r]] (a3 = p, q, r):
 // eigenvalues descending into l2, eigenvectors as the columns of v4 (column-major).
 void oracle_sym_eig2(const float* a3, float* l2, float* v4) {

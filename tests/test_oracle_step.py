@@ -494,3 +494,18 @@ def test_kinematic_collider_repose_moves_only_the_collider_and_sets_its_velocity
     assert st[0]["penetration_free"] and np.all(np.isfinite(o.positions()))
     free = dict(sc, static_mask=None)
     assert not O.OracleSolver(free, "f64").set_kinematic_collider_positions(x)
+
+
+def test_elastic_block_gather_handles_off_diagonals_and_duplicates():  # implicit.rs:6330-6388
+    """The assembler's requested blocks (the Rayleigh stiffnesses' gathers): off-diagonal
+    blocks at their own local (row, column), duplicates accumulated, unrequested pairs
+    ignored."""
+    trips = [(1, 2, 5.0), (0, 3, 1.5), (0, 3, 2.5), (5, 1, -7.0), (6, 8, 9.0), (9, 9, 100.0), (3, 6, 100.0)]
+    b = O.asm_blocks(4, [(0, 0), (0, 1), (1, 0), (2, 2)], trips)
+    assert b.shape == (4, 3, 3)
+    assert b[0][1, 2] == 5.0 and np.count_nonzero(b[0]) == 1
+    assert b[1][0, 0] == 4.0, "duplicate triplets must accumulate"
+    assert b[2][2, 1] == -7.0
+    assert not np.array_equal(b[1], b[2]), "(0,1) and (1,0) must be distinct blocks"
+    assert b[3][0, 2] == 9.0
+    assert np.abs(b).sum() == 5.0 + 4.0 + 7.0 + 9.0, "unrequested pairs must be ignored"
