@@ -32,7 +32,7 @@ def two_layer_mesh(n=40, gap=0.03):
 
 @pytest.mark.parametrize("bits", [30, 63])
 @pytest.mark.parametrize("case", ["two_layer", "soup", "degenerate"])
-def test_lbvh_bit_exact(ctx, bits, case):
+def test_lbvh_bit_exact(ctx, bits, case):  # engine-gpu morton.rs:272-328 (codes, then the radix sort)
     if case == "two_layer":
         pos, tris = two_layer_mesh()
         dhat = 0.05

@@ -21,7 +21,7 @@ def small_grid(n=12, seed=5):
 
 
 @pytest.mark.parametrize("variant", [1, 2, 3])
-def test_spmv_matches_oracle_small(ctx, variant):
+def test_spmv_matches_oracle_small(ctx, variant):  # engine-gpu pcg.rs:791-807 (gpu_spmv_matches_cpu)
     nb, rp, col, val, N, srp, sci, svv = small_grid(37)
     a = Bsr(ctx, nb, rp, col, val)
     a.set_kernel(variant)
@@ -97,7 +97,7 @@ def test_schwarz_domains_equal_oracle(ctx):
     assert np.array_equal(s.domains(), want)
 
 
-def test_schwarz_apply_matches_oracle(ctx):
+def test_schwarz_apply_matches_oracle(ctx):  # engine-gpu schwarz.rs:404-430
     import torch
     nb, rp, col, val, N, srp, sci, svv = small_grid(23)
     a = Bsr(ctx, nb, rp, col, val)
@@ -115,7 +115,7 @@ def test_schwarz_apply_matches_oracle(ctx):
 
 @pytest.mark.parametrize("precond,kind", [("schwarz", "schwarz"), ("block", "block")])
 @pytest.mark.parametrize("precision", ["mixed", "fp32"])
-def test_pcg_matches_oracle(ctx, precond, kind, precision):
+def test_pcg_matches_oracle(ctx, precond, kind, precision):  # engine-gpu pcg.rs:809-836, schwarz.rs:434-463
     nb, rp, col, val, N, srp, sci, svv = small_grid(30)
     A = CsrMatrix(N, srp, sci, svv)
     xs = np.sin(np.arange(N, dtype=np.float32) * np.float32(0.05)).astype(np.float32)
@@ -139,7 +139,8 @@ def test_pcg_reports_cap_and_breakdown(ctx):
     s = CudaLinearSolver(ctx, precond="block")
     s.solve(A, b, 1e-12, 3)
     assert s.last_stats().iters == 3 and s.last_stats().status == 4  # PCG_CAP
-    x = s.solve(A, np.zeros(N, np.float32), 1e-6, 100)  # b = 0: pAp = 0 -> break, x = 0
+    # b = 0: pAp = 0 -> break, x = 0 (engine-gpu pcg.rs:838-846, pcg_zero_rhs_is_zero)
+    x = s.solve(A, np.zeros(N, np.float32), 1e-6, 100)
     assert np.all(x == 0) and s.last_stats().iters == 0
 
 

@@ -55,7 +55,7 @@ def test_scene_topology_matches_oracle(ctx):
     assert gi["hinges"] == oi["hinges"] and gi["shells"] == oi["shells"] and gi["edges"] == oi["edges"]
 
 
-def test_free_fall_step_matches_oracle(ctx):
+def test_free_fall_step_matches_oracle(ctx):  # engine-gpu pcg.rs:848-901 (the GPU-solved step vs the CPU one)
     sc = sphere_scene(12, height=0.6)
     g, o, out = run_pair(ctx, sc, 3)
     for k, sg, so, rel in out:
@@ -179,7 +179,7 @@ def test_sheath_assembly_matches_oracle_fp32(ctx):
     assert np.abs(a["rhs"] - orhs).max() <= 1e-5 * np.abs(orhs).max()
 
 
-def test_sheath_steps_match_oracle(ctx):
+def test_sheath_steps_match_oracle(ctx):  # engine-gpu pcg.rs:905-965 (Schwarz-solved steps vs the CPU)
     """Seamed sheath steps from identical states: Newton counts within +-1, positions within
     1e-3 of the step's displacement (FP32 and mixed)."""
     sc = coarse_sheath()
