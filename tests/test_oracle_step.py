@@ -509,3 +509,37 @@ def test_elastic_block_gather_handles_off_diagonals_and_duplicates():  # implici
     assert not np.array_equal(b[1], b[2]), "(0,1) and (1,0) must be distinct blocks"
     assert b[3][0, 2] == 9.0
     assert np.abs(b).sum() == 5.0 + 4.0 + 7.0 + 9.0, "unrequested pairs must be ignored"
+
+
+def test_shell_energy_is_rigid_motion_invariant_and_its_hessian_annihilates_translations():
+    """shell_model.rs:1112-1147 and 1200-1250 on the StVK model this path runs (the reference
+    tests ARAP there): the unit triangle's rest state is stress-free and its area 1/2, the
+    deformed energy is unchanged by the tests' rotation and shift, the forces sum to zero, and
+    the element Hessian is symmetric, PSD and has the three translations as null modes; a
+    degenerate triangle builds no element."""
+    rest = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float64)
+    mu, lam = 400.0, 250.0
+    e, g, _ = O.shell(rest, rest, mu, lam, f64=False)
+    assert abs(e) < 1e-5 and np.abs(g).max() < 1e-3
+    flat = np.array([[0, 0, 0], [1, 0, 0], [2, 0, 0]], np.float64)
+    assert O.shell(flat, flat, mu, lam) is None  # a degenerate rest triangle builds no element
+    deformed = np.array([[0.01, -0.02, 0.0], [1.25, 0.05, 0.03], [-0.04, 0.88, -0.02]], np.float64)
+    base, g, _ = O.shell(rest, deformed, mu, lam)
+    assert base > 1e-3
+    assert np.abs(g.sum(axis=0)).max() < 1e-9 * max(1.0, np.abs(g).max())
+    a, b, c = 0.8, -1.2, 0.4  # glam's EulerRot::XYZ: R = Rx(a) Ry(b) Rz(c)
+    rx = np.array([[1, 0, 0], [0, np.cos(a), -np.sin(a)], [0, np.sin(a), np.cos(a)]])
+    ry = np.array([[np.cos(b), 0, np.sin(b)], [0, 1, 0], [-np.sin(b), 0, np.cos(b)]])
+    rz = np.array([[np.cos(c), -np.sin(c), 0], [np.sin(c), np.cos(c), 0], [0, 0, 1]])
+    moved = deformed @ (rx @ ry @ rz).T + np.array([-3.0, 4.0, 2.0])
+    after = O.shell(rest, moved, mu, lam)[0]
+    assert abs(after - base) < 1e-3 * max(base, 1.0), (base, after)
+    p = np.array([[0, 0, 0], [1.22, 0.05, 0.0], [0.03, 0.9, 0.02]], np.float64)
+    _, _, h = O.shell(rest, p, mu, lam)
+    scale = max(1.0, np.abs(h).max())
+    assert np.abs(h - h.T).max() < 1e-4 * scale
+    assert np.linalg.eigvalsh(0.5 * (h + h.T)).min() > -1e-3 * scale
+    for axis in range(3):
+        t = np.zeros(9)
+        t[axis::3] = 1.0
+        assert np.abs(h @ t).max() < 1e-3 * scale, axis
