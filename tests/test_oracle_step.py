@@ -513,8 +513,7 @@ def test_elastic_block_gather_handles_off_diagonals_and_duplicates():  # implici
 
 def test_shell_energy_is_rigid_motion_invariant_and_its_hessian_annihilates_translations():
     """shell_model.rs:1112-1147 and 1200-1250 on the StVK model this path runs (the reference
-    tests ARAP there): the unit triangle's rest state is stress-free and its area 1/2, the
-    deformed energy is unchanged by the tests' rotation and shift, the forces sum to zero, and
+    tests ARAP there): the unit triangle's rest state is stress-free, the deformed energy is unchanged by the tests' rotation and shift, the forces sum to zero, and
     the element Hessian is symmetric, PSD and has the three translations as null modes; a
     degenerate triangle builds no element."""
     rest = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float64)
