@@ -69,6 +69,17 @@ def test_parses_param_toml_from_text(tmp_path):  # golden.rs:1984-2001
     assert p["cg_tol"] == 1.0e-3  # unparsable: the default stays
 
 
+def test_u64_index_decoders_refuse_to_truncate():  # golden.rs:1410-1455 (the triangle and index-list decoders)
+    poison = 0x1_0000_0005  # narrows to 5, a plausible in-range vertex
+    tri = np.array([0, 1, poison], "<u8").tobytes()
+    for decode in (cap.decode_tris_u64, cap.decode_u64_list):
+        with pytest.raises(cap.CaptureError, match="exceeds u32"):
+            decode(tri)
+    ok = np.array([7, 8, 9, 10, 11, 12], "<u8").tobytes()
+    assert cap.decode_tris_u64(ok).tolist() == [[7, 8, 9], [10, 11, 12]]
+    assert cap.decode_u64_list(ok[:16]).tolist() == [7, 8]
+
+
 def test_friction_mode_parsing_falls_back_to_the_reference_default(tmp_path):  # contact.rs:1144-1165
     """The spellings of FrictionMode::from_str_or_default's test as param.toml values (the
     reader trims the value and its quotes as golden.rs:514-522 does); the default is min."""
