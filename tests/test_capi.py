@@ -17,6 +17,26 @@ def test_library_exports_every_header_symbol():
     assert not missing, f"declared in include/mguso_cuda.h but not exported: {missing}"
 
 
+def test_header_is_plain_c_and_cpp():
+    """The boundary header compiles as strict C99 and as C++17 on its own: plain pointers,
+    sizes and opaque handles, no CUDA or torch types in the signatures."""
+    import os
+    import shutil
+    import subprocess
+
+    import pytest
+
+    hdr = os.path.join(os.path.dirname(_lib.LIB_PATH), "..", "..", "include", "mguso_cuda.h")
+    for cc, args in (("gcc", ["-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-x", "c"]),
+                     ("g++", ["-std=c++17", "-Wall", "-Werror", "-x", "c++"])):
+        if shutil.which(cc) is None:
+            pytest.skip(f"{cc} not found")
+        subprocess.run([cc, *args, "-fsyntax-only", hdr], check=True)
+    text = open(hdr).read()
+    assert "#include <cuda" not in text and "#include \"cuda" not in text
+    assert "torch" not in text.lower()
+
+
 def test_version_and_last_error_without_gpu():
     lib = _lib.load()
     assert lib.mguso_version() >= 100
